@@ -1,0 +1,197 @@
+/* C ABI of the B200 multi-fluid Hall-MHD step (libmercury_mhd.so).
+ *
+ * The library replaces the body of the reference's explicit step,
+ * MercurySolver::StepOnce() (Z4_Mercury/src/MercurySolver_Driver.cpp:21-61),
+ * and its derived-field refresh UpdateDerivedFields_()
+ * (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:309-321).  The reference has
+ * no plugin or FFI layer; its seam is the C++ class interfaces the step uses:
+ *   Field::field(fid, ib) / FieldBlock::operator()(i,j,k,m)
+ *       (include/3_field/Field.h:45-52, include/3_field/FieldBlock.h:38-49)
+ *       -> mhd_upload_field / mhd_download_field, same index space and layout;
+ *   MercuryBoundary::Sync(group) (Z4_Mercury/include/1_Boundary.h:32) and
+ *   Halo::sync_group / sync_owner_alias_group (include/4_halo/Halo.h:28-37)
+ *       -> mhd_sync_tables (flattened halo and owner copies per group);
+ *   ReduceEdgeAliasCandidatesToOwners_ (Z4_Mercury/src/physics/MercurySolver_Current.cpp:3-57)
+ *       -> mhd_alias_classes;
+ *   calc_physical_constant (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:3-48)
+ *       -> mhd_constants.
+ *
+ * Conventions: plain C types only; every call returns an int status
+ * (MHD_OK = 0) and never exits or throws — the reference's exit(-1) on dt
+ * underflow (Z4_Mercury/src/physics/MercurySolver_Timestep.cpp:129-140) becomes
+ * MHD_ERR_DT, its KSP failure throw becomes MHD_ERR_SOLVE.  A context owns one
+ * CUDA stream; calls on one context are synchronous with respect to the host
+ * unless stated, and a context is not shared between host threads.
+ */
+#ifndef MERCURY_MHD_H
+#define MERCURY_MHD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum mhd_status {
+  MHD_OK = 0,
+  MHD_ERR_ARG = 1,      /* invalid argument */
+  MHD_ERR_CUDA = 2,     /* CUDA runtime error (see mhd_last_error) */
+  MHD_ERR_OOM = 3,      /* device allocation failed */
+  MHD_ERR_DT = 4,       /* dt non-finite or below 1e-7 (reference aborts) */
+  MHD_ERR_NONFINITE = 5,/* non-finite state detected */
+  MHD_ERR_SOLVE = 6,    /* implicit solve did not converge */
+  MHD_ERR_STATE = 7     /* call out of order (e.g. step before prepare) */
+};
+
+/* Field identifiers: the reference's catalog names
+ * (Z4_Mercury/include/0_MercuryFieldCatalog.h:70-202 and the geometry fields of
+ * src/7_metric/Metric.cpp:14-73).  ncomp / location in mhd_field_info(). */
+enum mhd_field {
+  /* state */
+  MHD_U_H = 0, MHD_U_NA, MHD_B_XI, MHD_B_ETA, MHD_B_ZETA,
+  /* derived (refreshed by the step) */
+  MHD_PV_H, MHD_PV_NA, MHD_U_PLUS, MHD_B_CELL, MHD_BIND_CELL, MHD_J_CELL,
+  MHD_J_XI, MHD_J_ETA, MHD_J_ZETA,
+  /* work (readable for diagnostics) */
+  MHD_E_XI, MHD_E_ETA, MHD_E_ZETA, MHD_EHALL_XI, MHD_EHALL_ETA, MHD_EHALL_ZETA,
+  MHD_EFACE_XI, MHD_EFACE_ETA, MHD_EFACE_ZETA, MHD_EHC, MHD_HALL_BETA,
+  /* static geometry and sources (uploaded once) */
+  MHD_JAC, MHD_JDXI, MHD_JDET, MHD_JDZE, MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA,
+  MHD_DL_XI, MHD_DL_ETA, MHD_DL_ZETA, MHD_DR_XI, MHD_DR_ETA, MHD_DR_ZETA,
+  MHD_HODGE_FACE_XI, MHD_HODGE_FACE_ETA, MHD_HODGE_FACE_ZETA,      /* beta = |l*|/|S| */
+  MHD_HODGE_EDGE_XI, MHD_HODGE_EDGE_ETA, MHD_HODGE_EDGE_ZETA,      /* alpha = |e|/|S*| */
+  MHD_BCELL_W, MHD_JCELL_W, MHD_BADD_XI, MHD_BADD_ETA, MHD_BADD_ZETA, MHD_PHOTO,
+  MHD_CELL_X, MHD_CELL_Y, MHD_CELL_Z,                              /* cell centres */
+  MHD_TAPER_XI, MHD_TAPER_ETA, MHD_TAPER_ZETA,                     /* Hall radial taper per edge */
+  MHD_NUM_FIELDS
+};
+
+enum mhd_location { MHD_CELL = 0, MHD_FACE_XI, MHD_FACE_ETA, MHD_FACE_ZETA, MHD_EDGE_XI, MHD_EDGE_ETA, MHD_EDGE_ZETA };
+
+/* Sync groups: MercuryBoundary::Sync names (Z4_Mercury/src/boundary/Boundary_Build.cpp:564-703). */
+enum mhd_group { MHD_SYNC_UCELL = 0, MHD_SYNC_BFACE, MHD_SYNC_EHALL, MHD_SYNC_EEDGE, MHD_SYNC_B_CELL,
+                 MHD_SYNC_JEDGE, MHD_SYNC_J_CELL, MHD_NUM_GROUPS };
+
+/* Physical constants as calc_physical_constant derives them (Tools.cpp:3-48). */
+typedef struct mhd_constants {
+  double gamma, M_H, M_Na, M_ref, T_ref, L_ref, U_ref, B_ref, n_ref, rho_ref, m_Na, k_Boltz, q_e, mu0;
+  double state_coeff_H, state_coeff_Na, CFL, hall_coef, momentum_induce_coeff, momentum_hall_coeff;
+  double inver_MA2, ne_hall_floor;
+  int32_t ambipolar; /* is_Ambipolar_Efield */
+  int32_t pad_;
+} mhd_constants;
+
+/* One DOF reference in the FieldBlock index space. */
+typedef struct mhd_dof {
+  int32_t field, block, i, j, k, comp;
+} mhd_dof;
+
+/* One flattened copy dst <- sign * src.  A group's halo copies are applied
+ * first (all reading pre-sync values), then its owner copies, exactly the
+ * stage order of MercuryBoundary::Sync_ (Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110). */
+typedef struct mhd_copy {
+  mhd_dof dst, src;
+  double sign;
+} mhd_copy;
+
+typedef struct mhd_sync_group {
+  int32_t n_halo, n_owner;
+  const mhd_copy *halo;
+  const mhd_copy *owner;
+} mhd_sync_group;
+
+/* Edge alias classes (global_id order): class c has members
+ * member[offset[c] .. offset[c+1]) with orientation signs, written to
+ * owner[c] as owner_sign * (sum_m sign_m * value_m) / count. */
+typedef struct mhd_alias_classes {
+  int32_t n_classes;
+  const int32_t *offset;      /* n_classes + 1 */
+  const mhd_dof *member;      /* offset[n_classes] (field = location axis 0/1/2) */
+  const double *member_sign;
+  const mhd_dof *owner;       /* n_classes */
+  const double *owner_sign;
+} mhd_alias_classes;
+
+typedef struct mhd_desc {
+  int32_t n_blocks;
+  const int32_t *cells;   /* n_blocks * 3: cells per axis (mx, my, mz) */
+  int32_t nghost;         /* runtime ghost width ngg (4 in production) */
+  int32_t precision;      /* 0 = FP64 (parity path); 1 = mixed (FP32 state/flux, FP64 metric) */
+  mhd_constants constants;
+  mhd_sync_group groups[MHD_NUM_GROUPS];
+  mhd_alias_classes edge_aliases;
+} mhd_desc;
+
+typedef struct mhd_ctx mhd_ctx;
+
+/* Replaces the MercurySolver constructor's device-side duties: allocates the
+ * device field arena (SoA, one array per component), uploads the sync and
+ * alias tables.  Fields are uploaded separately. */
+int mhd_ctx_create(const mhd_desc *desc, mhd_ctx **out);
+int mhd_ctx_destroy(mhd_ctx *ctx);
+
+/* Field::field(fid, ib) data exchange.  `data` is the FieldBlock storage of
+ * that field: AoS, offset ((i-lo0)*e1 + (j-lo1))*e2*ncomp + (k-lo2)*ncomp + m
+ * (include/3_field/FieldArray.h:126-128), for the logical range [lo, hi). */
+int mhd_upload_field(mhd_ctx *ctx, int field, int block, const double *data, const int32_t lo[3],
+                     const int32_t hi[3], int ncomp);
+int mhd_download_field(mhd_ctx *ctx, int field, int block, double *data, const int32_t lo[3],
+                       const int32_t hi[3], int ncomp);
+
+/* The preamble of MercurySolver::Advance (Z4_Mercury/src/MercurySolver_Driver.cpp:6-13):
+ * UpdateDerivedFields_ on the uploaded state.  Sets time/step. */
+int mhd_prepare(mhd_ctx *ctx, double time, int64_t step);
+
+/* nsteps calls of StepOnce.  dt_out (optional) receives the last dt.  The
+ * steps are captured once into a CUDA graph and replayed. */
+int mhd_step(mhd_ctx *ctx, int nsteps, double *dt_out);
+
+/* Same as mhd_step but returns without waiting for the GPU (status is
+ * checked on the next synchronous call). */
+int mhd_step_async(mhd_ctx *ctx, int nsteps);
+int mhd_synchronize(mhd_ctx *ctx);
+
+/* MercuryBoundary::Sync(group) on device data. */
+int mhd_sync(mhd_ctx *ctx, int group);
+
+typedef struct mhd_info {
+  double time, dt;
+  int64_t step;
+  int32_t status;      /* sticky device status (mhd_status) */
+  int32_t pad_;
+  int64_t device_bytes;
+} mhd_info;
+int mhd_get_info(mhd_ctx *ctx, mhd_info *info);
+
+/* Static description of a field id: ncomp and mhd_location. */
+int mhd_field_info(int field, int32_t *ncomp, int32_t *location);
+
+/* CUDA stream the context runs on (cudaStream_t as void*). */
+void *mhd_stream(mhd_ctx *ctx);
+
+/* Number of kernels one mhd_step(ctx, 1) launches (for launch accounting). */
+int mhd_kernels_per_step(mhd_ctx *ctx);
+
+/* Raw device pointer of one field component array of a block, with the box
+ * layout: element (i,j,k) at base[(i+G)*si + (j+G)*sj + (k+G)]. */
+int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base, int32_t *G, int64_t *si,
+                    int64_t *sj, int32_t ext[3]);
+
+/* Text of the last error on this thread. */
+const char *mhd_last_error(void);
+
+/* ---- host-side topology builders (C++ in the library, no device work) ----
+ * Flattened sync tables and edge alias classes for ONE block of n^3 cells,
+ * periodic in every direction (the reference's periodic inner patches with
+ * negative block ids, src/1_grid/1_MPCNS_Grid.cpp:455-464).  The tables are
+ * owned by the returned handle. */
+typedef struct mhd_topology mhd_topology;
+int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghost, mhd_topology **out);
+int mhd_topology_fill_desc(const mhd_topology *topo, mhd_desc *desc);
+int mhd_topology_destroy(mhd_topology *topo);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MERCURY_MHD_H */

@@ -1,0 +1,239 @@
+"""ctypes binding of the C ABI in include/mercury_mhd.h (libmercury_mhd.so).
+
+The structures mirror the header one for one.  The library is loaded from the
+package directory; there is no fallback: a missing or unloadable library is
+an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmercury_mhd.so")
+
+# enum mhd_field, in header order
+FIELDS = [
+    "U_H", "U_NA", "B_XI", "B_ETA", "B_ZETA",
+    "PV_H", "PV_NA", "U_PLUS", "B_CELL", "BIND_CELL", "J_CELL", "J_XI", "J_ETA", "J_ZETA",
+    "E_XI", "E_ETA", "E_ZETA", "EHALL_XI", "EHALL_ETA", "EHALL_ZETA",
+    "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA",
+    "JAC", "JDXI", "JDET", "JDZE", "AREA_XI", "AREA_ETA", "AREA_ZETA",
+    "DL_XI", "DL_ETA", "DL_ZETA", "DR_XI", "DR_ETA", "DR_ZETA",
+    "HODGE_FACE_XI", "HODGE_FACE_ETA", "HODGE_FACE_ZETA",
+    "HODGE_EDGE_XI", "HODGE_EDGE_ETA", "HODGE_EDGE_ZETA",
+    "BCELL_W", "JCELL_W", "BADD_XI", "BADD_ETA", "BADD_ZETA", "PHOTO",
+    "CELL_X", "CELL_Y", "CELL_Z", "TAPER_XI", "TAPER_ETA", "TAPER_ZETA",
+]
+FIELD_ID = {name: i for i, name in enumerate(FIELDS)}
+
+# Reference catalog name -> mhd_field (Z4_Mercury/include/0_MercuryFieldCatalog.h,
+# src/7_metric/Metric.cpp:14-73)
+REF_FIELD = {
+    "U_H": "U_H", "U_Na": "U_NA", "B_xi": "B_XI", "B_eta": "B_ETA", "B_zeta": "B_ZETA",
+    "PV_H": "PV_H", "PV_Na": "PV_NA", "U_plus": "U_PLUS", "B_cell": "B_CELL", "Bind_cell": "BIND_CELL",
+    "J_cell": "J_CELL", "J_xi": "J_XI", "J_eta": "J_ETA", "J_zeta": "J_ZETA",
+    "E_xi": "E_XI", "E_eta": "E_ETA", "E_zeta": "E_ZETA",
+    "Ehall_xi": "EHALL_XI", "Ehall_eta": "EHALL_ETA", "Ehall_zeta": "EHALL_ZETA",
+    "Eface_xi": "EFACE_XI", "Eface_eta": "EFACE_ETA", "Eface_zeta": "EFACE_ZETA",
+    "Jac": "JAC", "JDxi": "JDXI", "JDet": "JDET", "JDze": "JDZE",
+    "Area_xi": "AREA_XI", "Area_eta": "AREA_ETA", "Area_zeta": "AREA_ZETA",
+    "dl_xi": "DL_XI", "dl_eta": "DL_ETA", "dl_zeta": "DL_ZETA",
+    "dr_xi": "DR_XI", "dr_eta": "DR_ETA", "dr_zeta": "DR_ZETA",
+    "Hodge_star_2form_to_1form_face_xi_lumped": "HODGE_FACE_XI",
+    "Hodge_star_2form_to_1form_face_eta_lumped": "HODGE_FACE_ETA",
+    "Hodge_star_2form_to_1form_face_zeta_lumped": "HODGE_FACE_ZETA",
+    "Hodge_star_inverse_2form_to_1form_edge_xi_lumped": "HODGE_EDGE_XI",
+    "Hodge_star_inverse_2form_to_1form_edge_eta_lumped": "HODGE_EDGE_ETA",
+    "Hodge_star_inverse_2form_to_1form_edge_zeta_lumped": "HODGE_EDGE_ZETA",
+    "Bcell_from_Bface_w": "BCELL_W", "Jcell_from_Jedge_w": "JCELL_W",
+    "Badd_xi": "BADD_XI", "Badd_eta": "BADD_ETA", "Badd_zeta": "BADD_ZETA", "Photo_rate": "PHOTO",
+    "taper_xi": "TAPER_XI", "taper_eta": "TAPER_ETA", "taper_zeta": "TAPER_ZETA",
+}
+
+GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL"]
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_DT", 5: "ERR_NONFINITE", 6: "ERR_SOLVE",
+          7: "ERR_STATE"}
+
+
+class MhdConstants(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "gamma", "M_H", "M_Na", "M_ref", "T_ref", "L_ref", "U_ref", "B_ref", "n_ref", "rho_ref", "m_Na",
+        "k_Boltz", "q_e", "mu0", "state_coeff_H", "state_coeff_Na", "CFL", "hall_coef",
+        "momentum_induce_coeff", "momentum_hall_coeff", "inver_MA2", "ne_hall_floor")] + [
+        ("ambipolar", ctypes.c_int32), ("pad_", ctypes.c_int32)]
+
+
+class MhdDof(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("field", "block", "i", "j", "k", "comp")]
+
+
+class MhdCopy(ctypes.Structure):
+    _fields_ = [("dst", MhdDof), ("src", MhdDof), ("sign", ctypes.c_double)]
+
+
+class MhdSyncGroup(ctypes.Structure):
+    _fields_ = [("n_halo", ctypes.c_int32), ("n_owner", ctypes.c_int32),
+                ("halo", ctypes.POINTER(MhdCopy)), ("owner", ctypes.POINTER(MhdCopy))]
+
+
+class MhdAliasClasses(ctypes.Structure):
+    _fields_ = [("n_classes", ctypes.c_int32), ("offset", ctypes.POINTER(ctypes.c_int32)),
+                ("member", ctypes.POINTER(MhdDof)), ("member_sign", ctypes.POINTER(ctypes.c_double)),
+                ("owner", ctypes.POINTER(MhdDof)), ("owner_sign", ctypes.POINTER(ctypes.c_double))]
+
+
+class MhdDesc(ctypes.Structure):
+    _fields_ = [("n_blocks", ctypes.c_int32), ("cells", ctypes.POINTER(ctypes.c_int32)),
+                ("nghost", ctypes.c_int32), ("precision", ctypes.c_int32), ("constants", MhdConstants),
+                ("groups", MhdSyncGroup * 7), ("edge_aliases", MhdAliasClasses)]
+
+
+class MhdInfo(ctypes.Structure):
+    _fields_ = [("time", ctypes.c_double), ("dt", ctypes.c_double), ("step", ctypes.c_int64),
+                ("status", ctypes.c_int32), ("pad_", ctypes.c_int32), ("device_bytes", ctypes.c_int64)]
+
+
+EXPORTS = [
+    "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
+    "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
+    "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
+    "mhd_topology_fill_desc", "mhd_topology_destroy",
+]
+
+_lib = None
+
+
+class MhdError(RuntimeError):
+    def __init__(self, code, where):
+        self.code = code
+        msg = _lib.mhd_last_error().decode() if _lib is not None else ""
+        super().__init__(f"{where}: {STATUS.get(code, code)} {msg}")
+
+
+def lib() -> ctypes.CDLL:
+    """Load libmercury_mhd.so (building it first if it is missing and nvcc is
+    present).  Raises if the library cannot be loaded."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    L.mhd_ctx_create.argtypes = [ctypes.POINTER(MhdDesc), ctypes.POINTER(P)]
+    L.mhd_ctx_destroy.argtypes = [P]
+    L.mhd_upload_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p, ctypes.c_int]
+    L.mhd_download_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p, ctypes.c_int]
+    L.mhd_prepare.argtypes = [P, ctypes.c_double, ctypes.c_int64]
+    L.mhd_step.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.mhd_step_async.argtypes = [P, ctypes.c_int]
+    L.mhd_synchronize.argtypes = [P]
+    L.mhd_sync.argtypes = [P, ctypes.c_int]
+    L.mhd_get_info.argtypes = [P, ctypes.POINTER(MhdInfo)]
+    L.mhd_field_info.argtypes = [ctypes.c_int, i32p, i32p]
+    L.mhd_stream.argtypes = [P]
+    L.mhd_stream.restype = ctypes.c_void_p
+    L.mhd_kernels_per_step.argtypes = [P]
+    L.mhd_device_view.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                  i32p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), i32p]
+    L.mhd_last_error.restype = ctypes.c_char_p
+    L.mhd_topology_periodic_block.argtypes = [i32p, ctypes.c_int32, ctypes.POINTER(P)]
+    L.mhd_topology_fill_desc.argtypes = [P, ctypes.POINTER(MhdDesc)]
+    L.mhd_topology_destroy.argtypes = [P]
+    _lib = L
+    return L
+
+
+def check(rc, where):
+    if rc != 0:
+        raise MhdError(rc, where)
+
+
+def field_info(field: str):
+    nc, loc = ctypes.c_int32(), ctypes.c_int32()
+    check(lib().mhd_field_info(FIELD_ID[field], ctypes.byref(nc), ctypes.byref(loc)), "mhd_field_info")
+    return nc.value, loc.value
+
+
+def _i3(v):
+    return (ctypes.c_int32 * 3)(*[int(x) for x in v])
+
+
+class Context:
+    """One device-resident solve behind the C ABI (mhd_ctx)."""
+
+    def __init__(self, cells, nghost: int, constants: MhdConstants, topology=None, precision: int = 0):
+        L = lib()
+        self._cells = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
+        self.desc = MhdDesc()
+        self.desc.n_blocks = len(cells)
+        self.desc.cells = self._cells
+        self.desc.nghost = nghost
+        self.desc.precision = precision
+        self.desc.constants = constants
+        self._topo = ctypes.c_void_p()
+        if topology is None and len(cells) == 1:
+            check(L.mhd_topology_periodic_block(_i3(cells[0]), nghost, ctypes.byref(self._topo)),
+                  "mhd_topology_periodic_block")
+            check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
+        self.ctx = ctypes.c_void_p()
+        check(L.mhd_ctx_create(ctypes.byref(self.desc), ctypes.byref(self.ctx)), "mhd_ctx_create")
+
+    def upload(self, field: str, array: np.ndarray, lo, hi, block: int = 0):
+        a = np.ascontiguousarray(array, dtype=np.float64)
+        check(lib().mhd_upload_field(self.ctx, FIELD_ID[field], block, a.ctypes.data_as(ctypes.c_void_p),
+                                     _i3(lo), _i3(hi), a.shape[-1]), f"upload {field}")
+
+    def download(self, field: str, lo, hi, block: int = 0) -> np.ndarray:
+        nc, _ = field_info(field)
+        out = np.empty((hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], nc), dtype=np.float64)
+        check(lib().mhd_download_field(self.ctx, FIELD_ID[field], block, out.ctypes.data_as(ctypes.c_void_p),
+                                       _i3(lo), _i3(hi), nc), f"download {field}")
+        return out
+
+    def prepare(self, time: float = 0.0, step: int = 0):
+        check(lib().mhd_prepare(self.ctx, time, step), "mhd_prepare")
+
+    def step(self, n: int = 1) -> float:
+        dt = ctypes.c_double()
+        check(lib().mhd_step(self.ctx, n, ctypes.byref(dt)), "mhd_step")
+        return dt.value
+
+    def step_async(self, n: int = 1):
+        check(lib().mhd_step_async(self.ctx, n), "mhd_step_async")
+
+    def synchronize(self):
+        check(lib().mhd_synchronize(self.ctx), "mhd_synchronize")
+
+    def sync(self, group: str):
+        check(lib().mhd_sync(self.ctx, GROUPS.index(group)), f"mhd_sync {group}")
+
+    def info(self) -> MhdInfo:
+        inf = MhdInfo()
+        check(lib().mhd_get_info(self.ctx, ctypes.byref(inf)), "mhd_get_info")
+        return inf
+
+    def kernels_per_step(self) -> int:
+        return lib().mhd_kernels_per_step(self.ctx)
+
+    def stream(self) -> int:
+        return lib().mhd_stream(self.ctx)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            lib().mhd_ctx_destroy(self.ctx)
+            self.ctx = None
+        if getattr(self, "_topo", None):
+            lib().mhd_topology_destroy(self._topo)
+            self._topo = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,167 @@
+// Host-side topology builder: flattened sync tables and edge alias classes
+// for one block that is periodic in every direction.
+//
+// The reference builds the same connectivity from periodic inner patches
+// (negative block ids, src/1_grid/1_MPCNS_Grid.cpp:455-464) through its
+// topology and halo builders (src/2_topology/TopologyBuilder.cpp:436,
+// src/4_halo/core/HaloBuild.cpp:382-540).  On a periodic block those compose
+// to the following map, which the unique-code probe of the reference
+// reproduces DOF for DOF:
+//   halo  : a ghost DOF copies the DOF reached by wrapping every out-of-range
+//           index by +-n; along a node-like (staggered) axis the alias layer
+//           n is an owned DOF and is kept.  Corner1D groups (Ucell) fill only
+//           ghosts that are out of range along exactly one axis.
+//   owner : an owned alias DOF (node-like index == n) takes its owner's value
+//           (index 0), after the halo copies.
+// Edge alias classes (ReduceEdgeAliasCandidatesToOwners_,
+// Z4_Mercury/src/physics/MercurySolver_Current.cpp:3-57) group the 2 or 4
+// periodic images of a boundary edge; the owner is the image with all
+// node-like indices in [0, n) and members are listed in lexicographic (i, j, k)
+// order, the order the reference's topology stores them in.
+#include <cstdint>
+#include <new>
+#include <vector>
+
+#include "mercury_mhd.h"
+#include "mhd_layout.cuh"
+
+struct mhd_topology {
+  std::vector<mhd_copy> halo[MHD_NUM_GROUPS], owner[MHD_NUM_GROUPS];
+  std::vector<int32_t> alias_offset;
+  std::vector<mhd_dof> alias_member, alias_owner;
+  std::vector<double> alias_msign, alias_osign;
+};
+
+namespace {
+
+struct GroupSpec {
+  int group;
+  int corner1d;
+  std::vector<int> fields;
+};
+
+const GroupSpec kGroups[] = {
+    {MHD_SYNC_UCELL, 1, {MHD_U_H, MHD_U_NA}},
+    {MHD_SYNC_BFACE, 0, {MHD_B_XI, MHD_B_ETA, MHD_B_ZETA}},
+    {MHD_SYNC_EHALL, 0, {MHD_EHALL_XI, MHD_EHALL_ETA, MHD_EHALL_ZETA}},
+    {MHD_SYNC_EEDGE, 0, {MHD_E_XI, MHD_E_ETA, MHD_E_ZETA}},
+    {MHD_SYNC_B_CELL, 0, {MHD_B_CELL, MHD_BIND_CELL}},
+    {MHD_SYNC_JEDGE, 0, {MHD_J_XI, MHD_J_ETA, MHD_J_ZETA}},
+    {MHD_SYNC_J_CELL, 0, {MHD_J_CELL}},
+};
+
+void build_group(mhd_topology *t, const GroupSpec &gs, const int n[3], int g) {
+  for (int field : gs.fields) {
+    const int loc = mhd::kFieldSpec[field].loc;
+    const int nc = mhd::kFieldSpec[field].ncomp;
+    const int *st = mhd::kStagger[loc];
+    for (int i = -g; i < n[0] + st[0] + g; ++i)
+      for (int j = -g; j < n[1] + st[1] + g; ++j)
+        for (int k = -g; k < n[2] + st[2] + g; ++k) {
+          const int idx[3] = {i, j, k};
+          int src[3];
+          int nout = 0;
+          for (int a = 0; a < 3; ++a) nout += !(idx[a] >= 0 && idx[a] < n[a] + st[a]);
+          bool is_owner_copy = false;
+          if (nout == 0) {
+            bool alias = false;
+            for (int a = 0; a < 3; ++a) {
+              const bool al = st[a] && idx[a] == n[a];
+              src[a] = al ? 0 : idx[a];
+              alias = alias || al;
+            }
+            if (!alias) continue;
+            is_owner_copy = true;
+          } else {
+            if (gs.corner1d && nout > 1) continue;
+            for (int a = 0; a < 3; ++a) {
+              int v = idx[a];
+              if (st[a]) {
+                if (v < 0) v += n[a];
+                else if (v > n[a]) v -= n[a];
+              } else {
+                v = ((v % n[a]) + n[a]) % n[a];
+              }
+              src[a] = v;
+            }
+          }
+          for (int m = 0; m < nc; ++m) {
+            mhd_copy c;
+            c.dst = {field, 0, i, j, k, m};
+            c.src = {field, 0, src[0], src[1], src[2], m};
+            c.sign = 1.0;
+            (is_owner_copy ? t->owner : t->halo)[gs.group].push_back(c);
+          }
+        }
+  }
+}
+
+void build_alias(mhd_topology *t, const int n[3]) {
+  t->alias_offset.push_back(0);
+  const int locs[3] = {MHD_EDGE_XI, MHD_EDGE_ETA, MHD_EDGE_ZETA};
+  for (int axis = 0; axis < 3; ++axis) {
+    const int *st = mhd::kStagger[locs[axis]];
+    for (int i = 0; i < n[0] + st[0]; ++i)
+      for (int j = 0; j < n[1] + st[1]; ++j)
+        for (int k = 0; k < n[2] + st[2]; ++k) {
+          const int idx[3] = {i, j, k};
+          bool ok = true, dup = false;
+          int axes[3], na = 0;
+          for (int a = 0; a < 3; ++a) {
+            if (st[a] && idx[a] == n[a]) ok = false;
+            if (st[a] && idx[a] == 0) {
+              dup = true;
+              axes[na++] = a;
+            }
+          }
+          if (!ok || !dup) continue;
+          for (int c = 0; c < (1 << na); ++c) {
+            int p[3] = {i, j, k};
+            for (int b = 0; b < na; ++b)
+              if (c & (1 << (na - 1 - b))) p[axes[b]] = n[axes[b]];
+            t->alias_member.push_back({axis, 0, p[0], p[1], p[2], 0});
+            t->alias_msign.push_back(1.0);
+          }
+          t->alias_owner.push_back({axis, 0, i, j, k, 0});
+          t->alias_osign.push_back(1.0);
+          t->alias_offset.push_back((int32_t)t->alias_member.size());
+        }
+  }
+}
+
+}  // namespace
+
+extern "C" int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghost, mhd_topology **out) {
+  if (!cells || !out || nghost < 1) return MHD_ERR_ARG;
+  for (int a = 0; a < 3; ++a)
+    if (cells[a] < 2) return MHD_ERR_ARG;
+  auto *t = new (std::nothrow) mhd_topology();
+  if (!t) return MHD_ERR_OOM;
+  const int n[3] = {cells[0], cells[1], cells[2]};
+  for (const auto &gs : kGroups) build_group(t, gs, n, nghost);
+  build_alias(t, n);
+  *out = t;
+  return MHD_OK;
+}
+
+extern "C" int mhd_topology_fill_desc(const mhd_topology *t, mhd_desc *d) {
+  if (!t || !d) return MHD_ERR_ARG;
+  for (int g = 0; g < MHD_NUM_GROUPS; ++g) {
+    d->groups[g].n_halo = (int32_t)t->halo[g].size();
+    d->groups[g].halo = t->halo[g].data();
+    d->groups[g].n_owner = (int32_t)t->owner[g].size();
+    d->groups[g].owner = t->owner[g].data();
+  }
+  d->edge_aliases.n_classes = (int32_t)t->alias_owner.size();
+  d->edge_aliases.offset = t->alias_offset.data();
+  d->edge_aliases.member = t->alias_member.data();
+  d->edge_aliases.member_sign = t->alias_msign.data();
+  d->edge_aliases.owner = t->alias_owner.data();
+  d->edge_aliases.owner_sign = t->alias_osign.data();
+  return MHD_OK;
+}
+
+extern "C" int mhd_topology_destroy(mhd_topology *t) {
+  delete t;
+  return MHD_OK;
+}

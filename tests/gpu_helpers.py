@@ -1,0 +1,45 @@
+"""Shared helpers of the GPU parity tests: build a device solve from a
+reference dump and compare fields."""
+import numpy as np
+
+import mercury_oracle as mo
+from mpcns_mercury_b200 import Context, reference_constants
+from mpcns_mercury_b200.capi import REF_FIELD
+
+NGHOST = 4
+
+
+def context_from_dump(dump, n, tag="step0:", cfl=0.4):
+    """Upload the reference's step-0 state and static inputs into a new context."""
+    ctx = Context([(n, n, n)], NGHOST, reference_constants(cfl=cfl))
+    for name in mo.STATE_FIELDS:
+        r = dump[(tag + name, 0)]
+        ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
+    for name in mo.STATIC_FIELDS + ["taper_xi", "taper_eta", "taper_zeta"]:
+        r = dump[("static:" + name, 0)]
+        ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
+    # cell centres: the reference reads dual_x(i+1, j+1, k+1) for cell (i, j, k)
+    for ax, fld in zip("xyz", ("CELL_X", "CELL_Y", "CELL_Z")):
+        r = dump[("dual_" + ax, 0)]
+        lo = tuple(v - 1 for v in r.lo)
+        hi = tuple(v - 1 for v in r.hi)
+        ctx.upload(fld, r.data, lo, hi)
+    return ctx
+
+
+def owned(rec):
+    g = [-v for v in rec.lo]
+    return rec.data[g[0]:rec.hi[0], g[1]:rec.hi[1], g[2]:rec.hi[2]]
+
+
+def compare(ctx, dump, tag, names, tol):
+    """Max relative L2 over ``names`` (owned DOFs) of device vs dump."""
+    worst = {}
+    for name in names:
+        r = dump[(tag + name, 0)]
+        dev = ctx.download(REF_FIELD[name], r.lo, r.hi)
+        g = [-v for v in r.lo]
+        sl = (slice(g[0], r.hi[0]), slice(g[1], r.hi[1]), slice(g[2], r.hi[2]))
+        worst[name] = mo.rel_l2(dev[sl], r.data[sl])
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    return worst, bad
