@@ -152,6 +152,14 @@ int mhd_step(mhd_ctx *ctx, int nsteps, double *dt_out);
 int mhd_step_async(mhd_ctx *ctx, int nsteps);
 int mhd_synchronize(mhd_ctx *ctx);
 
+/* Profiling form of mhd_step (no graph): runs nsteps steps eagerly with a
+ * CUDA event after every kernel and returns, per kernel launch of one step
+ * (in launch order), its mean duration in ms and its name.  The reference
+ * has no counterpart (its only timer is RuntimeMonitor's CPU time per step,
+ * src/6_io/RuntimeMonitor.cpp:33-56). */
+int mhd_step_profiled(mhd_ctx *ctx, int nsteps, int max_kernels, float *kernel_ms, const char **kernel_names,
+                      int *n_kernels);
+
 /* MercuryBoundary::Sync(group) on device data. */
 int mhd_sync(mhd_ctx *ctx, int group);
 

@@ -99,6 +99,11 @@ struct mhd_ctx {
   size_t staging_elems = 0;
   double **comp_ptrs = nullptr;  // device array of component pointers for scatter/gather
   int kernels_per_step = 0;
+  // eager profiling: an event after every launch, labelled by kernel name
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_events;
+  std::vector<const char *> prof_names;
+  size_t prof_used = 0;
 
   BlockView view(int b, int cur) const {
     BlockView v;
@@ -135,6 +140,19 @@ struct mhd_ctx {
 };
 
 namespace {
+
+// After a launch: in profiling mode record an event labelled `name`.
+void mark(mhd_ctx *ctx, const char *name) {
+  if (!ctx->profiling) return;
+  if (ctx->prof_used == ctx->prof_events.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    ctx->prof_events.push_back(e);
+    ctx->prof_names.push_back(name);
+  }
+  ctx->prof_names[ctx->prof_used] = name;
+  cudaEventRecord(ctx->prof_events[ctx->prof_used++], ctx->stream);
+}
 
 int upload_table(const mhd_copy *tab, int n, const mhd_ctx *ctx, DevTable *out) {
   out->n = n;
@@ -211,11 +229,13 @@ int enqueue_sync(mhd_ctx *ctx, int g, int cur, int *nk) {
   const int64_t ucur_off = (int64_t)cur * ctx->ubuf;
   if (ctx->halo[g].n) {
     launch_copy(ctx->halo[g].dst, ctx->halo[g].src, ctx->halo[g].sign, ctx->halo[g].n, ctx->arena, ucur_off, ctx->stream);
+    mark(ctx, "k_copy(halo)");
     ++*nk;
   }
   if (ctx->owner[g].n) {
     launch_copy(ctx->owner[g].dst, ctx->owner[g].src, ctx->owner[g].sign, ctx->owner[g].n, ctx->arena, ucur_off,
                 ctx->stream);
+    mark(ctx, "k_copy(owner)");
     ++*nk;
   }
   return MHD_OK;
@@ -224,18 +244,31 @@ int enqueue_sync(mhd_ctx *ctx, int g, int cur, int *nk) {
 // UpdateDerivedFields_ (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:309-321) on buffer `cur`.
 void enqueue_derived(mhd_ctx *ctx, int cur, int *nk) {
   cudaStream_t st = ctx->stream;
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) launch_bcell(ctx->view(b, cur), ctx->S, b == 0, st);
+  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
+    launch_bcell(ctx->view(b, cur), ctx->S, b == 0, st);
+    mark(ctx, "k_bcell");
+  }
   enqueue_sync(ctx, MHD_SYNC_B_CELL, cur, nk);
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) launch_jedge(ctx->view(b, cur), st);
+  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
+    launch_jedge(ctx->view(b, cur), st);
+    mark(ctx, "k_jedge");
+  }
   if (ctx->aliasJ.n) {
     launch_alias(ctx->aliasJ.offset, ctx->aliasJ.member, ctx->aliasJ.msign, ctx->aliasJ.owner, ctx->aliasJ.osign,
                  ctx->aliasJ.n, ctx->arena, st);
+    mark(ctx, "k_alias(J)");
     ++*nk;
   }
   enqueue_sync(ctx, MHD_SYNC_JEDGE, cur, nk);
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) launch_jcell(ctx->view(b, cur), st);
+  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
+    launch_jcell(ctx->view(b, cur), st);
+    mark(ctx, "k_jcell");
+  }
   enqueue_sync(ctx, MHD_SYNC_J_CELL, cur, nk);
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) launch_pv_uplus(ctx->view(b, cur), ctx->consts, ctx->nghost, st);
+  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
+    launch_pv_uplus(ctx->view(b, cur), ctx->consts, ctx->nghost, st);
+    mark(ctx, "k_pv_uplus");
+  }
 }
 
 // StepOnce (Z4_Mercury/src/MercurySolver_Driver.cpp:21-61), state in buffer `cur`
@@ -243,22 +276,44 @@ void enqueue_derived(mhd_ctx *ctx, int cur, int *nk) {
 void enqueue_step(mhd_ctx *ctx, int cur, int *nk) {
   cudaStream_t st = ctx->stream;
   const int nb = ctx->nblocks;
-  for (int b = 0; b < nb; ++b, ++*nk) launch_timestep(ctx->view(b, cur), ctx->consts, ctx->S, st);
+  for (int b = 0; b < nb; ++b, ++*nk) {
+    launch_timestep(ctx->view(b, cur), ctx->consts, ctx->S, st);
+    mark(ctx, "k_timestep");
+  }
   // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171)
-  for (int b = 0; b < nb; ++b, ++*nk) launch_face_emf(ctx->view(b, cur), st);
-  for (int b = 0; b < nb; ++b, ++*nk) launch_edge_emf(ctx->view(b, cur), ctx->consts, st);
+  for (int b = 0; b < nb; ++b, ++*nk) {
+    launch_face_emf(ctx->view(b, cur), st);
+    mark(ctx, "k_face_emf");
+  }
+  for (int b = 0; b < nb; ++b, ++*nk) {
+    launch_edge_emf(ctx->view(b, cur), ctx->consts, st);
+    mark(ctx, "k_edge_emf");
+  }
   if (ctx->aliasE.n) {
     launch_alias(ctx->aliasE.offset, ctx->aliasE.member, ctx->aliasE.msign, ctx->aliasE.owner, ctx->aliasE.osign,
                  ctx->aliasE.n, ctx->arena, st);
+    mark(ctx, "k_alias(E)");
     ++*nk;
   }
-  for (int b = 0; b < nb; ++b, ++*nk) launch_hall_cell(ctx->view(b, cur), ctx->consts, ctx->nghost, st);
-  for (int b = 0; b < nb; ++b, ++*nk) launch_hall_edge(ctx->view(b, cur), st);
+  for (int b = 0; b < nb; ++b, ++*nk) {
+    launch_hall_cell(ctx->view(b, cur), ctx->consts, ctx->nghost, st);
+    mark(ctx, "k_hall_cell");
+  }
+  for (int b = 0; b < nb; ++b, ++*nk) {
+    launch_hall_edge(ctx->view(b, cur), st);
+    mark(ctx, "k_hall_edge");
+  }
   enqueue_sync(ctx, MHD_SYNC_EHALL, cur, nk);
-  for (int b = 0; b < nb; ++b, ++*nk) launch_add_hall(ctx->view(b, cur), st);
+  for (int b = 0; b < nb; ++b, ++*nk) {
+    launch_add_hall(ctx->view(b, cur), st);
+    mark(ctx, "k_add_hall");
+  }
   enqueue_sync(ctx, MHD_SYNC_EEDGE, cur, nk);
   // fluid RHS + Euler update into the other buffer, B_face update in place
-  for (int b = 0; b < nb; ++b, ++*nk) launch_update(ctx->view(b, cur), ctx->consts, ctx->S, b == 0, st);
+  for (int b = 0; b < nb; ++b, ++*nk) {
+    launch_update(ctx->view(b, cur), ctx->consts, ctx->S, b == 0, st);
+    mark(ctx, "k_update");
+  }
   const int nxt = cur ^ 1;
   enqueue_sync(ctx, MHD_SYNC_UCELL, nxt, nk);
   enqueue_sync(ctx, MHD_SYNC_BFACE, nxt, nk);
@@ -356,6 +411,7 @@ int mhd_ctx_destroy(mhd_ctx *ctx) {
   }
   free_alias(ctx->aliasE);
   free_alias(ctx->aliasJ);
+  for (auto e : ctx->prof_events) cudaEventDestroy(e);
   cudaFree(ctx->arena);
   cudaFree(ctx->S);
   cudaFree(ctx->staging);
@@ -494,6 +550,39 @@ int mhd_step(mhd_ctx *ctx, int nsteps, double *dt_out) {
     *dt_out = s.dt;
   }
   return MHD_OK;
+}
+
+int mhd_step_profiled(mhd_ctx *ctx, int nsteps, int max_kernels, float *kernel_ms, const char **kernel_names,
+                      int *n_kernels) {
+  if (!ctx || nsteps < 1 || !kernel_ms || !n_kernels) return fail(MHD_ERR_ARG, "mhd_step_profiled: bad arguments");
+  if (!ctx->prepared) return fail(MHD_ERR_STATE, "mhd_step_profiled before mhd_prepare");
+  std::vector<float> acc;
+  int per_step = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    ctx->profiling = true;
+    ctx->prof_used = 0;
+    mark(ctx, "start");
+    int nk = 0;
+    enqueue_step(ctx, ctx->ucur, &nk);
+    ctx->profiling = false;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ctx->ucur ^= 1;
+    per_step = (int)ctx->prof_used - 1;
+    if (acc.empty()) acc.assign(per_step, 0.0f);
+    for (int q = 0; q < per_step; ++q) {
+      float ms = 0.0f;
+      CUDA_TRY(cudaEventElapsedTime(&ms, ctx->prof_events[q], ctx->prof_events[q + 1]));
+      acc[q] += ms;
+    }
+  }
+  const int n = per_step < max_kernels ? per_step : max_kernels;
+  for (int q = 0; q < n; ++q) {
+    kernel_ms[q] = acc[q] / (float)nsteps;
+    if (kernel_names) kernel_names[q] = ctx->prof_names[q + 1];
+  }
+  *n_kernels = n;
+  return check_status(ctx);
 }
 
 int mhd_sync(mhd_ctx *ctx, int group) {

@@ -927,3 +927,12 @@ void oracle_bind(octx *c, int slot, double *p, const int *lo, const int *hi, int
 }
 double oracle_get_dt(const octx *c) { return c->dt; }
 double oracle_get_time(const octx *c) { return c->time; }
+
+/* MercuryBoundary::Sync("Ucell") and Sync("Bface") on the periodic block. */
+void oracle_sync_state(octx *c) {
+  sync_periodic(&c->UH, LOC_CELL, 1, c->n);
+  sync_periodic(&c->UN, LOC_CELL, 1, c->n);
+  sync_periodic(&c->Bx, LOC_FXI, 0, c->n);
+  sync_periodic(&c->By, LOC_FET, 0, c->n);
+  sync_periodic(&c->Bz, LOC_FZE, 0, c->n);
+}

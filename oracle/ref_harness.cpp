@@ -14,6 +14,7 @@
 // The job file holds "key value" lines; see oracle/mercury_oracle.py.
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -600,9 +601,25 @@ int main(int argc, char **argv) {
           }
       };
       dump_state(0);
+      double stepping = 0.0;
       for (long s = 1; s <= steps; ++s) {
+        const auto t0 = std::chrono::steady_clock::now();
         S.StepOnce();
+        stepping += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         dump_state(s);
+      }
+      {
+        // wall time of the StepOnce calls alone (setup and dumps excluded)
+        long cells = 0;
+        for (int ib = 0; ib < fld->num_blocks(); ++ib) {
+          FieldBlock &U = fld->field(S.fid_.fid_U_H, ib);
+          if (!U.is_allocated()) continue;
+          const Int3 h = U.inner_hi();
+          cells += (long)h.i * h.j * h.k;
+        }
+        const double meta[3] = {stepping, (double)steps, (double)cells};
+        const int l[3] = {0, 0, 0}, h[3] = {1, 1, 3};
+        d.rec("timing", -1, l, h, 1, meta);
       }
     }
   }

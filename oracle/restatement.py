@@ -105,3 +105,45 @@ class Restatement:
         if getattr(self, "ctx", None):
             lib().oracle_destroy(self.ctx)
             self.ctx = None
+
+
+# Extents of the derived and work fields, as the reference's catalog allocates
+# them (Z4_Mercury/include/0_MercuryFieldCatalog.h:70-202): (stagger, ncomp, nghost)
+_WORK = {
+    "PV_H": ((0, 0, 0), 5, 4), "PV_Na": ((0, 0, 0), 5, 4), "U_plus": ((0, 0, 0), 3, 4),
+    "B_cell": ((0, 0, 0), 3, 4), "Bind_cell": ((0, 0, 0), 3, 4), "J_cell": ((0, 0, 0), 3, 4),
+    "J_xi": ((0, 1, 1), 1, 4), "J_eta": ((1, 0, 1), 1, 4), "J_zeta": ((1, 1, 0), 1, 4),
+    "RHS_H": ((0, 0, 0), 5, 0), "RHS_Na": ((0, 0, 0), 5, 0),
+    "F_xi": ((1, 0, 0), 5, 0), "F_eta": ((0, 1, 0), 5, 0), "F_zeta": ((0, 0, 1), 5, 0),
+    "RHS_B_xi": ((1, 0, 0), 1, 0), "RHS_B_eta": ((0, 1, 0), 1, 0), "RHS_B_zeta": ((0, 0, 1), 1, 0),
+    "E_xi": ((0, 1, 1), 1, 4), "E_eta": ((1, 0, 1), 1, 4), "E_zeta": ((1, 1, 0), 1, 4),
+    "Ehall_xi": ((0, 1, 1), 1, 4), "Ehall_eta": ((1, 0, 1), 1, 4), "Ehall_zeta": ((1, 1, 0), 1, 4),
+    "Eface_xi": ((1, 0, 0), 3, 4), "Eface_eta": ((0, 1, 0), 3, 4), "Eface_zeta": ((0, 0, 1), 3, 4),
+    "Ehc": ((0, 0, 0), 3, 4), "hall_beta": ((0, 0, 0), 1, 4),
+}
+_SETUP_NAME = {"dual_x": None, "dual_y": None, "dual_z": None}
+
+
+def inputs_from_fields(n: int, fields: dict):
+    """Restatement slots from a case built by the package's host setup
+    ({reference field name: (lo, hi, data)} plus cell_x/y/z cell centres)."""
+    out = {}
+    for slot in SLOTS:
+        if slot in _WORK:
+            st, nc, g = _WORK[slot]
+            lo = (-g, -g, -g)
+            hi = tuple(n + st[a] + g for a in range(3))
+            out[slot] = (lo, hi, np.zeros(tuple(hi[a] - lo[a] for a in range(3)) + (nc,)))
+        elif slot in ("dual_x", "dual_y", "dual_z"):
+            lo, hi, data = fields["cell_" + slot[-1]]
+            # dual(i+1, j+1, k+1) is the centre of cell (i, j, k)
+            out[slot] = (tuple(v + 1 for v in lo), tuple(v + 1 for v in hi), data)
+        else:
+            out[slot] = fields[slot]
+    return out
+
+
+def sync_state(r: "Restatement"):
+    L = lib()
+    L.oracle_sync_state.argtypes = [ctypes.c_void_p]
+    L.oracle_sync_state(r.ctx)
