@@ -186,6 +186,43 @@ int mhd_kernels_per_step(mhd_ctx *ctx);
 int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base, int32_t *G, int64_t *si,
                     int64_t *sj, int32_t ext[3]);
 
+/* ---- Hall edge EMF without device allocation ----
+ * No counterpart in the reference: it exists for callers that may not call
+ * cudaMalloc / cudaFree themselves (a host framework that owns all device
+ * memory through its own pool, or a request loop that must not allocate per
+ * call).  The caller passes device pointers to its inputs and outputs in the
+ * box layout of mhd_device_view (element (i,j,k) at p[(i+G)*si + (j+G)*sj +
+ * (k+G)], G >= nghost + 1); the only intermediate — alpha (J x B) and
+ * |alpha||B| on the cells [-nghost, n + nghost)^3 — lives in a library-owned
+ * static device array of MHD_HALL_SCRATCH_MAX_CELLS cells x 4 doubles
+ * (32 MiB), held by every GPU that loads the library until the process exits.
+ * Blocks with more cells than that return MHD_ERR_ARG.  The first call on a
+ * device looks up the array's device address (once per device, with that
+ * device current); make that first call before any stream capture.  All calls
+ * share the one array and nothing in it needs to start at zero (every cell is
+ * written before it is read), but calls that overlap on the GPU race on it:
+ * serialise them (one stream, or one device at a time).  Writes the Hall EMF
+ * on the owned edges of all three families; launches asynchronously on
+ * `stream` (cudaStream_t as void*; NULL = default stream). */
+#define MHD_HALL_SCRATCH_MAX_CELLS (1 << 20)
+typedef struct mhd_hall_block {
+  int32_t n[3];        /* cells per axis */
+  int32_t nghost;      /* runtime ghost width (4) */
+  int32_t G;           /* box ghost width of the pointers (>= nghost + 1) */
+  int32_t pad_;
+  int64_t si, sj;      /* box strides (k contiguous) */
+  const double *rho_H, *rho_Na;                  /* U_H and U_Na component 0 (cells) */
+  const double *J_cell[3], *B_cell[3];           /* cells */
+  const double *B_face[3];                       /* induced face fluxes xi, eta, zeta */
+  const double *area[3];                         /* |S| of xi, eta, zeta faces */
+  const double *dl[3];                           /* |e| of xi, eta, zeta edges */
+  const double *dr_xi[3], *dr_eta[3], *dr_zeta[3];/* edge vectors, x/y/z components */
+  const double *taper[3];                        /* Hall radial taper per edge */
+  double hall_coef, M_H, M_Na, M_ref, ne_hall_floor;
+} mhd_hall_block;
+int mhd_hall_emf_static_scratch(const mhd_hall_block *in, double *out_xi, double *out_eta, double *out_zeta,
+                                void *stream);
+
 /* Text of the last error on this thread. */
 const char *mhd_last_error(void);
 
