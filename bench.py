@@ -130,6 +130,10 @@ def build_workload(name: str):
     if name == "cube32":
         geom, f = S.cube_case(32)
         return [(32, 32, 32)], [f], "config 1: periodic curvilinear 32^3 cube, Orszag-Tang, 2 ion fluids, Hall+p_e, FP64"
+    if name.startswith("cube"):
+        n = int(name[4:])
+        geom, f = S.cube_case(n)
+        return [(n, n, n)], [f], f"config-1 physics on a periodic curvilinear {n}^3 cube (size study), FP64"
     raise SystemExit(f"unknown workload {name}")
 
 

@@ -186,6 +186,13 @@ int mhd_kernels_per_step(mhd_ctx *ctx);
 int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base, int32_t *G, int64_t *si,
                     int64_t *sj, int32_t ext[3]);
 
+/* Seeded uniform draws of the synthetic workloads (host only): std::mt19937_64
+ * seeded with `seed`, u = (x >> 11) * 2^-53, out[t] = -a + 2 a u in draw order.
+ * No counterpart in the reference solver; it reproduces the seeding the
+ * workload definition states, so that host-generated initial states are
+ * byte-identical to the ones the CPU oracle generates. */
+int mhd_seeded_uniform(uint64_t seed, int64_t count, double a, double *out);
+
 /* ---- Hall edge EMF without device allocation ----
  * No counterpart in the reference: it exists for callers that may not call
  * cudaMalloc / cudaFree themselves (a host framework that owns all device

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmercury_mhd.so")
-SOURCES = ["mhd_step.cu", "mhd_ctx.cu", "mhd_topology.cpp", "mhd_noalloc.cu"]
+SOURCES = ["mhd_step.cu", "mhd_ctx.cu", "mhd_topology.cpp", "mhd_noalloc.cu", "mhd_host_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -432,18 +432,28 @@ def _reference_rho_small():
 
 
 class Uniform:
-    """std::mt19937_64 with seed 20261203 + solve_id; uniforms (x >> 11) * 2^-53."""
+    """std::mt19937_64 with seed 20261203 + solve_id; uniforms (x >> 11) * 2^-53.
+    Draws come from the library's host helper (mhd_seeded_uniform); the stream
+    continues across calls."""
 
     def __init__(self, solve_id: int = 0):
-        self.mt = _MT19937_64(20261203 + solve_id)
-
-    def next(self) -> float:
-        return (self.mt.next() >> 11) * 2.0 ** -53
+        self.seed = 20261203 + solve_id
+        self.used = 0
 
     def sym(self, a: float, count: int) -> np.ndarray:
-        out = np.empty(count)
-        for t in range(count):
-            out[t] = -a + 2.0 * a * self.next()
+        import ctypes
+
+        from .capi import check, lib
+
+        L = lib()
+        L.mhd_seeded_uniform.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p]
+        buf = np.empty(self.used + count)
+        check(L.mhd_seeded_uniform(self.seed, self.used + count, a, buf.ctypes.data_as(ctypes.c_void_p)),
+              "mhd_seeded_uniform")
+        # the stream is regenerated from its start (the draws before this call
+        # were produced with the same engine); amplitudes are per call
+        out = buf[self.used:].copy()
+        self.used += count
         return out
 
 

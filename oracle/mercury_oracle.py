@@ -156,3 +156,31 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.float64)
     den = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
+
+
+# Config-2 case: 6-panel cubed-sphere shell r in [1, 8], 48x48x96 cells per
+# panel (r_k = 8^(k/96)), inner wall (the reference's Coupled-Solid handlers),
+# outer Farfield; upstream v = (-4, 0, 0), n = 1, p = 0.1, IMF (0, 0, -0.2);
+# centred dipole, tilt 0, |B| = 1 at the surface equator (moment in A m^2 with
+# the reference's own nondimensionalisation, operators/Dipole.h:46-80);
+# two ion fluids, Na+ at 1e-3 number fraction; Hall on (the reference's
+# production taper r_min 1.1, r_max 1.2); CFL 0.4.
+SHELL_UPSTREAM = "1612400.0 1954409.5501563628 4E7 0.001 0.0 0.0 0.0 0.0 -2.0000000000000003e-10"
+SHELL_JOB = {
+    "case": "shell",
+    "na": 48,
+    "nr": 96,
+    "r_out": 8.0,
+    "cfl": 0.4,
+    "steps": 200,
+    "resistive": 0,
+    "ambipolar": 1,
+    "hall_r_min": 1.1,
+    "hall_r_max": 1.2,
+    "init": "na_fraction",
+    "na_fraction": 1e-3,
+    "num_of_dipole": 1,
+    "dipole_line": "0.0 0.0 0.0 0.0 0.0 -1.452678400462402e+17 0.0",
+    "initial_line": SHELL_UPSTREAM,
+    "farfield_line": "1612400.0 1954409.5501563628 4E7 0.0 0.0",
+}

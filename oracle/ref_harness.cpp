@@ -262,6 +262,146 @@ void write_cube_case(const fs::path &geo) {
   write_text(geo / "boundary_condition" / "inner   0.txt", in.str());
 }
 
+// Config "shell": 6-panel gnomonic (equiangular) cubed-sphere shell,
+// r in [1, r_out] with r_k = r_out^(k/nr); panel p has local axes
+// (i: xi angle, j: eta angle, k: radius), right-handed.  Shared panel-edge
+// nodes are bitwise identical (tan of the edge angles is set to +-1 exactly
+// and the angle grid is symmetric), so the reference's mesh transfer sees
+// conformal interfaces.  Inner boundary r = 1: "Coupled-Solid" (the name the
+// reference registers its solid-wall handlers under); outer r = r_out: Farfield.
+void shell_dir(int p, double ta, double tb, double d[3]) {
+  switch (p) {
+    case 0: d[0] = 1.0; d[1] = ta; d[2] = tb; break;
+    case 1: d[0] = -ta; d[1] = 1.0; d[2] = tb; break;
+    case 2: d[0] = -1.0; d[1] = -ta; d[2] = tb; break;
+    case 3: d[0] = ta; d[1] = -1.0; d[2] = tb; break;
+    case 4: d[0] = -tb; d[1] = ta; d[2] = 1.0; break;
+    default: d[0] = tb; d[1] = ta; d[2] = -1.0; break;
+  }
+}
+double shell_tan(int i, int n) {
+  const int q = 2 * i - n;
+  if (q == n) return 1.0;
+  if (q == -n) return -1.0;
+  return std::tan(((double)q / (double)n) * (std::acos(-1.0) / 4.0));
+}
+void shell_node(int p, int i, int j, int k, int na, int nr, double r_out, double out[3]) {
+  double d[3];
+  shell_dir(p, shell_tan(i, na), shell_tan(j, na), d);
+  const double inv = 1.0 / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double r = (k == 0) ? 1.0 : (k == nr ? r_out : std::pow(r_out, (double)k / (double)nr));
+  for (int a = 0; a < 3; ++a) out[a] = r * d[a] * inv;
+}
+
+void write_shell_case(const fs::path &geo) {
+  const int na = (int)job_int("na", 48), nr = (int)job_int("nr", 96);
+  const double r_out = job_dbl("r_out", 8.0);
+  const int ni = na + 1, nk = nr + 1;
+  std::vector<std::string> names(6, "Fluid");
+  std::vector<std::array<int, 3>> dims(6, {ni, ni, nk});
+  std::vector<std::vector<double>> xyz(6);
+  for (int p = 0; p < 6; ++p) {
+    auto &b = xyz[p];
+    b.resize((size_t)3 * ni * ni * nk);
+    const size_t npts = (size_t)ni * ni * nk;
+    for (int k = 0; k < nk; ++k)
+      for (int j = 0; j < ni; ++j)
+        for (int i = 0; i < ni; ++i) {
+          double x[3];
+          shell_node(p, i, j, k, na, nr, r_out, x);
+          const size_t o = ((size_t)k * ni + j) * ni + i;
+          b[o] = x[0];
+          b[npts + o] = x[1];
+          b[2 * npts + o] = x[2];
+        }
+  }
+  write_grid_binary(geo / "grid   0.grd", names, dims, xyz);
+
+  // panel edge e: 0 = (i = 0), 1 = (i = na), 2 = (j = 0), 3 = (j = na); nodes along the
+  // other angular index t at r = 1
+  auto edge_pt = [&](int p, int e, int t, double out[3]) {
+    const int i = e == 0 ? 0 : e == 1 ? na : t;
+    const int j = e == 2 ? 0 : e == 3 ? na : t;
+    shell_node(p, i, j, 0, na, nr, r_out, out);
+  };
+  struct Conn {
+    int q, f;
+    bool reversed;
+  };
+  Conn conn[6][4];
+  for (int p = 0; p < 6; ++p)
+    for (int e = 0; e < 4; ++e) {
+      bool found = false;
+      for (int q = 0; q < 6 && !found; ++q)
+        for (int f = 0; f < 4 && !found; ++f) {
+          if (q == p) continue;
+          for (int rev = 0; rev < 2 && !found; ++rev) {
+            bool ok = true;
+            for (int t = 0; t <= na && ok; ++t) {
+              double a[3], b[3];
+              edge_pt(p, e, t, a);
+              edge_pt(q, f, rev ? na - t : t, b);
+              ok = a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
+            }
+            if (ok) {
+              conn[p][e] = {q, f, rev != 0};
+              found = true;
+            }
+          }
+        }
+      if (!found) {
+        std::fprintf(stderr, "shell: panel %d edge %d has no partner\n", p, e);
+        std::exit(3);
+      }
+    }
+  // inner patches, 1-based node ranges; the normal dimension has sub == sup,
+  // the angular tangential is sign-marked (paired with the partner's angular
+  // tangential), the radial tangential is unmarked and runs 1..nk on both sides.
+  const std::string A = std::to_string(ni), K = std::to_string(nk);
+  auto ranges = [&](int e, bool rev) {
+    std::string r[3];
+    const bool on_i = (e == 0 || e == 1);
+    const std::string fixed = (e == 0 || e == 2) ? "1" : A;
+    const std::string ang = rev ? ("-" + A + "\t-1") : ("-1\t-" + A);
+    r[on_i ? 0 : 1] = fixed + "\t" + fixed;
+    r[on_i ? 1 : 0] = ang;
+    r[2] = "1\t" + K;
+    return r[0] + "\t" + r[1] + "\t" + r[2];
+  };
+  std::ostringstream in;
+  in << "\t24\n\t4\t4\t4\t4\t4\t4\nimin\timax\tjmin\tjmax\tkmin\tkmax\tid\tPhysic_Name\n";
+  // Each side of a connection must list, as its partner, exactly the range
+  // line the partner lists for itself (src/1_grid/1_MPCNS_Grid.cpp:473-509
+  // pairs patches by equal ranges); a reversed connection is therefore
+  // written descending on the side with the larger (panel, edge) key.
+  auto own_line = [&](int p, int e) {
+    const Conn &c = conn[p][e];
+    const bool upper = (p * 4 + e) > (c.q * 4 + c.f);
+    return ranges(e, upper && c.reversed);
+  };
+  for (int p = 0; p < 6; ++p)
+    for (int e = 0; e < 4; ++e) {
+      const Conn &c = conn[p][e];
+      in << own_line(p, e) << "\t" << (p + 1) << "\tFluid\n";
+      in << own_line(c.q, c.f) << "\t" << (c.q + 1) << "\tFluid\n";
+    }
+  fs::create_directories(geo / "boundary_condition");
+  write_text(geo / "boundary_condition" / "inner   0.txt", in.str());
+  std::ostringstream bc;
+  const std::string M = std::to_string(na), R = std::to_string(nr);
+  for (int p = 0; p < 6; ++p) {
+    bc << "\t2\n";
+    bc << "0\t" << M << "\t0\t" << M << "\t0\t0\t17\n";
+    bc << "0\t" << M << "\t0\t" << M << "\t" << R << "\t" << R << "\t4\n";
+  }
+  write_text(geo / "boundary_condition" / "boundary   0.txt", bc.str());
+  std::string fv = kFvbnd;
+  fv.replace(fv.find("BOUNDARIES"), 10, "Coupled-Solid\nBOUNDARIES");
+  write_text(geo / "boundary_condition" / "boundary_name.fvbnd", fv);
+  write_text(geo / "boundary_condition" / "parallel   0.txt",
+             "\t6\t0\n\t0\t0\t0\t0\t0\t0\nimin\timax\tjmin\tjmax\tkmin\tkmax\ts_r_id\ts_flag\tr_flag\tPhysic_Name\n");
+}
+
 void write_case(const fs::path &work) {
   fs::create_directories(work / "CASE" / "setup");
   fs::create_directories(work / "CASE" / "geometry");
@@ -274,6 +414,8 @@ void write_case(const fs::path &work) {
   const std::string kind = job_str("case", "cube");
   if (kind == "cube")
     write_cube_case(work / "CASE" / "geometry");
+  else if (kind == "shell")
+    write_shell_case(work / "CASE" / "geometry");
   else {
     std::fprintf(stderr, "unknown case %s\n", kind.c_str());
     std::exit(2);
@@ -432,6 +574,34 @@ void set_orszag_tang(MercurySolver &S) {
         Bz(i, j, k, 0) = (EX(i, j, k) - EX(i, j + 1, k)) + (EY(i + 1, j, k) - EY(i, j, k));
 }
 
+// Magnetosphere start: the reference's uniform solar wind (Common_Initial,
+// Z4_Mercury/include/2_Initial.h:134-215) for H+, and Na+ at a number-density
+// fraction f of it with the same velocity and temperature:
+// rho_Na = f (M_Na / M_H) rho_H, p_Na = f p_H, on every allocated cell.
+void set_na_fraction(MercurySolver &S) {
+  Field *fld = S.fld_;
+  const double f = job_dbl("na_fraction", 1e-3);
+  const double g = S.gamma_;
+  for (int ib = 0; ib < fld->num_blocks(); ++ib) {
+    FieldBlock &UH = fld->field(S.fid_.fid_U_H, ib);
+    FieldBlock &UN = fld->field(S.fid_.fid_U_Na, ib);
+    const Int3 lo = UH.get_lo(), hi = UH.get_hi();
+    for (int i = lo.i; i < hi.i; ++i)
+      for (int j = lo.j; j < hi.j; ++j)
+        for (int k = lo.k; k < hi.k; ++k) {
+          const double rho = UH(i, j, k, 0);
+          const double u = UH(i, j, k, 1) / rho, v = UH(i, j, k, 2) / rho, w = UH(i, j, k, 3) / rho;
+          const double p = (g - 1.0) * (UH(i, j, k, 4) - 0.5 * rho * (u * u + v * v + w * w));
+          const double rn = f * (S.M_Na / S.M_H) * rho, pn = f * p;
+          UN(i, j, k, 0) = rn;
+          UN(i, j, k, 1) = rn * u;
+          UN(i, j, k, 2) = rn * v;
+          UN(i, j, k, 3) = rn * w;
+          UN(i, j, k, 4) = pn / (g - 1.0) + 0.5 * rn * (u * u + v * v + w * w);
+        }
+  }
+}
+
 // ---------------------------------------------------------------- sync probe
 // Unique-code probe of one sync group, following the reference's own halo
 // test method (Z0_NULL/test/halo_comm/Z0_HaloCommTest.cpp:361-398): every
@@ -571,11 +741,14 @@ int main(int argc, char **argv) {
     Dumper d(out);
     const std::string mode = job_str("mode", "run");
     if (mode == "probe") {
+      if (job_int("dump_grid", 0)) dump_grid(d, grd);
       probe_group(S, job_str("probe_group"), d);
     } else if (mode == "classes") {
       dump_edge_classes(topology, d);
     } else {
-      if (job_str("init", "ot") == "ot") set_orszag_tang(S);
+      const std::string init = job_str("init", "ot");
+      if (init == "ot") set_orszag_tang(S);
+      if (init == "na_fraction") set_na_fraction(S);
       S.mercury_bound_.Sync("Ucell");
       S.mercury_bound_.Sync("Bface");
       // Advance() begins with UpdateDerivedFields_ and the step-0 control
