@@ -46,19 +46,19 @@ L2_BYTES = 126 * 1024 * 1024
 
 # Algorithmic HBM bytes per owned cell of each FP64 kernel: the distinct field
 # components it must read and write once per DOF (8 B each), as listed in
-# mhd_step.cu.  Kernels over the allocated range carry their own cell count.
+# mpcns_mercury_b200/csrc/mhd_kernels.cu.  Kernels over the allocated cell
+# range count the allocated cells.
 KERNEL_BYTES_PER_CELL = {
-    "k_timestep": 8 * (10 + 3 + 1 + 9),
-    "k_face_emf": 8 * (3 + 3 + 3 + 9 + 1 + 9),
-    "k_edge_emf": 8 * (9 + 3 + 9 + 1 + 3 + 2 + 2 + 3),
-    "k_hall_cell": 8 * (2 + 3 + 3 + 3 + 1),
-    "k_hall_edge": 8 * (3 + 1 + 9 + 3 + 3 + 3 + 3 + 3),
-    "k_add_hall": 8 * (3 + 3 + 3),
-    "k_update": 8 * (10 + 10 + 3 + 3 + 3 + 9 + 1 + 1 + 3 + 10 + 3 + 3 + 3),
-    "k_bcell": 8 * (3 + 3 + 18 + 3 + 3),
-    "k_jedge": 8 * (3 + 3 + 3 + 3),
-    "k_jcell": 8 * (3 + 36 + 3),
-    "k_pv_uplus": 8 * (10 + 10 + 3),
+    "k_face_emf": 8 * (3 + 3 + 3 + 9),                      # B, Badd, UCON -> Eface
+    "k_edge_emf": 8 * (9 + 3 + 3 + 2 + 2 + 3),              # Eface, UCON, B, p_e x2, rho x2 -> E
+    "k_hall_cell": 8 * (2 + 3 + 3 + 3 + 1),                 # rho x2, J_cell, B_cell -> EHC, beta
+    "k_hall_edge": 8 * (3 + 1 + 9 + 3 + 3 + 3 + 3 + 3),     # EHC, beta, dr, dl, Area, B, taper -> Ehall
+    "k_add_hall": 8 * (3 + 3 + 3),                          # E += Ehall
+    "k_fluid": 8 * (10 + 10 + 9 + 1 + 3 + 3 + 3 + 1 + 3 + 10),  # U, PV, JD, Jac, U+, B_cell, J_cell, Photo, xyz -> U'
+    "k_bface": 8 * (3 + 3 + 3),                             # B += dt curl E
+    "k_bcell_jedge": 8 * (3 + 3 + 18 + 3 + 3 + 3 + 3 + 3),  # B, Badd, W_B, beta, alpha -> B_cell, Bind, J edges
+    "k_jcell": 8 * (3 + 36 + 3),                            # J edges, W_J -> J_cell
+    "k_pv_uplus": 8 * (10 + 1 + 9 + 3 + 10 + 3 + 3),        # U, Jac, JD, B_cell -> PV, U+, UCON (+ dt)
 }
 ALLOCATED_RANGE_KERNELS = {"k_hall_cell", "k_pv_uplus"}
 
@@ -137,20 +137,7 @@ def build_workload(name: str):
     raise SystemExit(f"unknown workload {name}")
 
 
-UPLOAD_FIELDS = ["Jac", "JDxi", "JDet", "JDze", "Area_xi", "Area_eta", "Area_zeta", "dl_xi", "dl_eta", "dl_zeta",
-                 "dr_xi", "dr_eta", "dr_zeta", "beta_xi", "beta_eta", "beta_zeta", "alpha_xi", "alpha_eta",
-                 "alpha_zeta", "Bcell_from_Bface_w", "Jcell_from_Jedge_w", "Badd_xi", "Badd_eta", "Badd_zeta",
-                 "Photo_rate", "cell_x", "cell_y", "cell_z", "taper_xi", "taper_eta", "taper_zeta",
-                 "U_H", "U_Na", "B_xi", "B_eta", "B_zeta"]
-CAPI_NAME = {"beta_xi": "HODGE_FACE_XI", "beta_eta": "HODGE_FACE_ETA", "beta_zeta": "HODGE_FACE_ZETA",
-             "alpha_xi": "HODGE_EDGE_XI", "alpha_eta": "HODGE_EDGE_ETA", "alpha_zeta": "HODGE_EDGE_ZETA",
-             "cell_x": "CELL_X", "cell_y": "CELL_Y", "cell_z": "CELL_Z"}
-
-
-def capi_field(name):
-    from mpcns_mercury_b200.capi import REF_FIELD
-
-    return CAPI_NAME.get(name) or REF_FIELD[name]
+from mpcns_mercury_b200.workloads import UPLOAD_FIELDS, capi_field  # noqa: E402
 
 
 def make_context(cells, fields, pinned=None):

@@ -56,6 +56,7 @@ enum mhd_field {
   /* work (readable for diagnostics) */
   MHD_E_XI, MHD_E_ETA, MHD_E_ZETA, MHD_EHALL_XI, MHD_EHALL_ETA, MHD_EHALL_ZETA,
   MHD_EFACE_XI, MHD_EFACE_ETA, MHD_EFACE_ZETA, MHD_EHC, MHD_HALL_BETA,
+  MHD_UCON,                                   /* contravariant U_plus components along xi, eta, zeta */
   /* static geometry and sources (uploaded once) */
   MHD_JAC, MHD_JDXI, MHD_JDET, MHD_JDZE, MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA,
   MHD_DL_XI, MHD_DL_ETA, MHD_DL_ZETA, MHD_DR_XI, MHD_DR_ETA, MHD_DR_ZETA,
@@ -169,6 +170,7 @@ typedef struct mhd_info {
   int32_t status;      /* sticky device status (mhd_status) */
   int32_t pad_;
   int64_t device_bytes;
+  int64_t remaining;   /* steps of the current request not yet taken */
 } mhd_info;
 int mhd_get_info(mhd_ctx *ctx, mhd_info *info);
 
@@ -229,6 +231,45 @@ typedef struct mhd_hall_block {
 } mhd_hall_block;
 int mhd_hall_emf_static_scratch(const mhd_hall_block *in, double *out_xi, double *out_eta, double *out_zeta,
                                 void *stream);
+
+/* ---- batched solves (ensembles and request serving) ----
+ * No counterpart in the reference, which runs one solve per MPI job.  A batch
+ * holds up to `capacity` independent solves (slots) on one GPU and advances
+ * all of them with one CUDA graph per step: every kernel of the step is a
+ * persistent loop over the tiles of all active slots, so one launch covers
+ * every member and the graph stays valid while slots join and leave.  A slot
+ * is active while it has steps left in its request; slots with different
+ * block shapes, sync tables and constants share a batch.  mhd_ctx is a batch
+ * of capacity 1.  Calls on one batch are serialised by the caller. */
+typedef struct mhd_batch mhd_batch;
+int mhd_batch_create(int capacity, mhd_batch **out);
+int mhd_batch_destroy(mhd_batch *batch);
+/* Device bytes a solve of this descriptor occupies (arena and tables); -1 on
+ * a bad descriptor.  Lets a server admit requests against free HBM. */
+int64_t mhd_desc_device_bytes(const mhd_desc *desc);
+/* Adds a solve (allocates its arena, uploads its tables) into a free slot. */
+int mhd_batch_add(mhd_batch *batch, const mhd_desc *desc, int *slot);
+/* Frees a slot; the solve's memory is released in stream order. */
+int mhd_batch_remove(mhd_batch *batch, int slot);
+int mhd_batch_upload_field(mhd_batch *batch, int slot, int field, int block, const double *data,
+                           const int32_t lo[3], const int32_t hi[3], int ncomp);
+int mhd_batch_download_field(mhd_batch *batch, int slot, int field, int block, double *data,
+                             const int32_t lo[3], const int32_t hi[3], int ncomp);
+int mhd_batch_sync(mhd_batch *batch, int slot, int group);
+int mhd_batch_prepare(mhd_batch *batch, int slot, double time, int64_t step);
+/* Sets the slot's request to nsteps more steps (0 parks it). */
+int mhd_batch_request(mhd_batch *batch, int slot, int64_t nsteps);
+/* Enqueues nsteps graph launches of the batched step (asynchronous).  Each
+ * launch advances every slot that still has steps requested by one step. */
+int mhd_batch_run(mhd_batch *batch, int nsteps);
+/* Synchronises and fills infos[0 .. capacity) (empty slots read zero). */
+int mhd_batch_poll(mhd_batch *batch, mhd_info *infos);
+void *mhd_batch_stream(mhd_batch *batch);
+int mhd_batch_kernels_per_step(mhd_batch *batch);
+int mhd_batch_step_profiled(mhd_batch *batch, int nsteps, int max_kernels, float *kernel_ms,
+                            const char **kernel_names, int *n_kernels);
+int mhd_batch_device_view(mhd_batch *batch, int slot, int field, int block, int comp, double **base, int32_t *G,
+                          int64_t *si, int64_t *sj, int32_t ext[3]);
 
 /* Text of the last error on this thread. */
 const char *mhd_last_error(void);

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmercury_mhd.so")
-SOURCES = ["mhd_step.cu", "mhd_ctx.cu", "mhd_topology.cpp", "mhd_noalloc.cu", "mhd_host_setup.cpp"]
+SOURCES = ["mhd_kernels.cu", "mhd_ctx.cu", "mhd_topology.cpp", "mhd_noalloc.cu", "mhd_host_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -29,7 +29,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+    cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "--extended-lambda", "--threads", "0", "-Xcompiler", "-fPIC", "-shared",
            "-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp",
            *[os.path.join(CSRC, s) for s in SOURCES], "-lcudart"]
     if verbose:

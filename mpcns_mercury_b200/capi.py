@@ -19,7 +19,7 @@ FIELDS = [
     "U_H", "U_NA", "B_XI", "B_ETA", "B_ZETA",
     "PV_H", "PV_NA", "U_PLUS", "B_CELL", "BIND_CELL", "J_CELL", "J_XI", "J_ETA", "J_ZETA",
     "E_XI", "E_ETA", "E_ZETA", "EHALL_XI", "EHALL_ETA", "EHALL_ZETA",
-    "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA",
+    "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA", "UCON",
     "JAC", "JDXI", "JDET", "JDZE", "AREA_XI", "AREA_ETA", "AREA_ZETA",
     "DL_XI", "DL_ETA", "DL_ZETA", "DR_XI", "DR_ETA", "DR_ZETA",
     "HODGE_FACE_XI", "HODGE_FACE_ETA", "HODGE_FACE_ZETA",
@@ -93,14 +93,19 @@ class MhdDesc(ctypes.Structure):
 
 class MhdInfo(ctypes.Structure):
     _fields_ = [("time", ctypes.c_double), ("dt", ctypes.c_double), ("step", ctypes.c_int64),
-                ("status", ctypes.c_int32), ("pad_", ctypes.c_int32), ("device_bytes", ctypes.c_int64)]
+                ("status", ctypes.c_int32), ("pad_", ctypes.c_int32), ("device_bytes", ctypes.c_int64),
+                ("remaining", ctypes.c_int64)]
 
 
 EXPORTS = [
     "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
-    "mhd_topology_fill_desc", "mhd_topology_destroy",
+    "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy",
+    "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_remove", "mhd_batch_upload_field",
+    "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
+    "mhd_batch_poll", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
+    "mhd_batch_device_view",
 ]
 
 _lib = None
@@ -145,6 +150,28 @@ def lib() -> ctypes.CDLL:
     L.mhd_topology_periodic_block.argtypes = [i32p, ctypes.c_int32, ctypes.POINTER(P)]
     L.mhd_topology_fill_desc.argtypes = [P, ctypes.POINTER(MhdDesc)]
     L.mhd_topology_destroy.argtypes = [P]
+    L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(P)]
+    L.mhd_batch_destroy.argtypes = [P]
+    L.mhd_desc_device_bytes.argtypes = [ctypes.POINTER(MhdDesc)]
+    L.mhd_desc_device_bytes.restype = ctypes.c_int64
+    L.mhd_batch_add.argtypes = [P, ctypes.POINTER(MhdDesc), ctypes.POINTER(ctypes.c_int)]
+    L.mhd_batch_remove.argtypes = [P, ctypes.c_int]
+    L.mhd_batch_upload_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p,
+                                         ctypes.c_int]
+    L.mhd_batch_download_field.argtypes = L.mhd_batch_upload_field.argtypes
+    L.mhd_batch_sync.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.mhd_batch_prepare.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_int64]
+    L.mhd_batch_request.argtypes = [P, ctypes.c_int, ctypes.c_int64]
+    L.mhd_batch_run.argtypes = [P, ctypes.c_int]
+    L.mhd_batch_poll.argtypes = [P, ctypes.POINTER(MhdInfo)]
+    L.mhd_batch_stream.argtypes = [P]
+    L.mhd_batch_stream.restype = ctypes.c_void_p
+    L.mhd_batch_kernels_per_step.argtypes = [P]
+    L.mhd_batch_step_profiled.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                                          ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int)]
+    L.mhd_batch_device_view.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_void_p), i32p, ctypes.POINTER(ctypes.c_int64),
+                                        ctypes.POINTER(ctypes.c_int64), i32p]
     _lib = L
     return L
 
@@ -231,6 +258,103 @@ class Context:
         if getattr(self, "_topo", None):
             lib().mhd_topology_destroy(self._topo)
             self._topo = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolveDesc:
+    """A solve descriptor (mhd_desc) with the storage it points to kept alive."""
+
+    def __init__(self, cells, nghost: int, constants: MhdConstants, precision: int = 0):
+        L = lib()
+        self._cells = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
+        self.desc = MhdDesc()
+        self.desc.n_blocks = len(cells)
+        self.desc.cells = self._cells
+        self.desc.nghost = nghost
+        self.desc.precision = precision
+        self.desc.constants = constants
+        self._topo = ctypes.c_void_p()
+        if len(cells) == 1:
+            check(L.mhd_topology_periodic_block(_i3(cells[0]), nghost, ctypes.byref(self._topo)),
+                  "mhd_topology_periodic_block")
+            check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
+
+    def device_bytes(self) -> int:
+        return int(lib().mhd_desc_device_bytes(ctypes.byref(self.desc)))
+
+    def close(self):
+        if getattr(self, "_topo", None):
+            lib().mhd_topology_destroy(self._topo)
+            self._topo = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent solves advanced together by one CUDA graph per step (mhd_batch)."""
+
+    def __init__(self, capacity: int):
+        self.capacity = capacity
+        self.b = ctypes.c_void_p()
+        check(lib().mhd_batch_create(capacity, ctypes.byref(self.b)), "mhd_batch_create")
+
+    def add(self, desc: SolveDesc) -> int:
+        slot = ctypes.c_int()
+        check(lib().mhd_batch_add(self.b, ctypes.byref(desc.desc), ctypes.byref(slot)), "mhd_batch_add")
+        return slot.value
+
+    def remove(self, slot: int):
+        check(lib().mhd_batch_remove(self.b, slot), "mhd_batch_remove")
+
+    def upload(self, slot: int, field: str, array: np.ndarray, lo, hi, block: int = 0):
+        a = np.ascontiguousarray(array, dtype=np.float64)
+        check(lib().mhd_batch_upload_field(self.b, slot, FIELD_ID[field], block, a.ctypes.data_as(ctypes.c_void_p),
+                                           _i3(lo), _i3(hi), a.shape[-1]), f"upload {field}")
+
+    def download(self, slot: int, field: str, lo, hi, block: int = 0) -> np.ndarray:
+        nc, _ = field_info(field)
+        out = np.empty((hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], nc), dtype=np.float64)
+        check(lib().mhd_batch_download_field(self.b, slot, FIELD_ID[field], block,
+                                             out.ctypes.data_as(ctypes.c_void_p), _i3(lo), _i3(hi), nc),
+              f"download {field}")
+        return out
+
+    def sync(self, slot: int, group: str):
+        check(lib().mhd_batch_sync(self.b, slot, GROUPS.index(group)), f"mhd_batch_sync {group}")
+
+    def prepare(self, slot: int, time: float = 0.0, step: int = 0):
+        check(lib().mhd_batch_prepare(self.b, slot, time, step), "mhd_batch_prepare")
+
+    def request(self, slot: int, nsteps: int):
+        check(lib().mhd_batch_request(self.b, slot, nsteps), "mhd_batch_request")
+
+    def run(self, nsteps: int):
+        check(lib().mhd_batch_run(self.b, nsteps), "mhd_batch_run")
+
+    def poll(self):
+        infos = (MhdInfo * self.capacity)()
+        check(lib().mhd_batch_poll(self.b, infos), "mhd_batch_poll")
+        return list(infos)
+
+    def stream(self) -> int:
+        return lib().mhd_batch_stream(self.b)
+
+    def kernels_per_step(self) -> int:
+        return lib().mhd_batch_kernels_per_step(self.b)
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().mhd_batch_destroy(self.b)
+            self.b = None
 
     def __del__(self):
         try:

@@ -1,13 +1,18 @@
-// Context, device arena and C ABI of the MHD step (include/mercury_mhd.h).
+// Engine host side and C ABI (include/mercury_mhd.h).
 //
-// One context = one solve on one GPU: a device arena holding every field
-// component of every block (layout in mhd_layout.cuh), the flattened sync and
-// alias tables translated to arena offsets, a CUDA stream, and two CUDA graphs
-// (one per parity of the double-buffered conserved state) that each replay one
-// full StepOnce.
+// A batch owns a fixed-capacity device directory of solve slots
+// (mhd_engine.cuh), one CUDA stream and one CUDA graph of a full StepOnce over
+// every active slot.  Every kernel reads the directory from device memory and
+// runs a persistent grid, so the graph stays valid while solves join and
+// leave: adding or removing a solve only rewrites directory entries with
+// stream-ordered copies between graph launches.
+//
+// mhd_ctx (one solve) is a batch of capacity 1.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -15,8 +20,8 @@
 #include <vector>
 
 #include "mercury_mhd.h"
-#include "mhd_layout.cuh"
-#include "mhd_step.cuh"
+#include "mhd_engine.cuh"
+#include "mhd_kernels.cuh"
 
 using namespace mhd;
 
@@ -40,19 +45,7 @@ int fail(int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return fail(MHD_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
   } while (0)
 
-struct DevTable {
-  int64_t *dst = nullptr, *src = nullptr;
-  double *sign = nullptr;
-  int n = 0;
-};
-struct DevAlias {
-  int32_t *offset = nullptr;
-  int64_t *member = nullptr, *owner = nullptr;
-  double *msign = nullptr, *osign = nullptr;
-  int n = 0;
-};
-
-constexpr int64_t kUFlag = int64_t(1) << 62;
+constexpr unsigned long long kDtUnset = 0x54B249AD2594C37DULL;  // bit pattern of 1e100
 
 // AoS (FieldBlock) <-> SoA box scatter/gather for uploads and downloads.
 __global__ void k_scatter_aos(const double *__restrict__ aos, int lo0, int lo1, int lo2, int e0, int e1, int e2, int nc,
@@ -77,49 +70,37 @@ __global__ void k_gather_aos(double *__restrict__ aos, int lo0, int lo1, int lo2
   for (int m = 0; m < nc; ++m) aos[t * nc + m] = src_comp[m][off];
 }
 
-}  // namespace
+template <class T>
+int dev_upload(const std::vector<T> &h, T **d, cudaStream_t st) {
+  *d = nullptr;
+  if (h.empty()) return MHD_OK;
+  CUDA_TRY(cudaMallocAsync((void **)d, sizeof(T) * h.size(), st));
+  CUDA_TRY(cudaMemcpyAsync(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st));
+  return MHD_OK;
+}
 
-struct mhd_ctx {
+// One solve: its arena, tables and its directory entry's pointees.
+struct Solve {
   int nblocks = 0, nghost = 0;
-  std::vector<Box> boxes;
-  std::vector<int64_t> ubase, mbase;  // per-block offsets inside the U regions / main region
-  int64_t ubuf = 0;                   // elements of one U region (all blocks)
-  int64_t main_off = 0;               // element offset of the main region
-  int64_t arena_elems = 0;
-  double *arena = nullptr;
-  Scalars *S = nullptr;
-  Consts consts{};
-  cudaStream_t stream = nullptr;
-  DevTable halo[MHD_NUM_GROUPS], owner[MHD_NUM_GROUPS];
-  DevAlias aliasE, aliasJ;
-  int ucur = 0;
   bool prepared = false;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  double *staging = nullptr;  // upload / download staging (device)
-  size_t staging_elems = 0;
-  double **comp_ptrs = nullptr;  // device array of component pointers for scatter/gather
-  int kernels_per_step = 0;
-  // eager profiling: an event after every launch, labelled by kernel name
-  bool profiling = false;
-  std::vector<cudaEvent_t> prof_events;
-  std::vector<const char *> prof_names;
-  size_t prof_used = 0;
+  std::vector<Box> boxes;
+  std::vector<int64_t> ubase, mbase;
+  int64_t ubuf = 0, main_off = 0, arena_elems = 0, table_bytes = 0;
+  double *arena = nullptr;
+  DevBlock *dblocks = nullptr;
+  int *dtile_prefix[kNumRanges] = {};
+  int tiles[kNumRanges] = {};
+  int64_t *tab_dst[kMaxGroups][2] = {}, *tab_src[kMaxGroups][2] = {};
+  double *tab_sign[kMaxGroups][2] = {};
+  int tab_n[kMaxGroups][2] = {};
+  int32_t *al_off = nullptr;
+  int64_t *al_memE = nullptr, *al_ownE = nullptr, *al_memJ = nullptr, *al_ownJ = nullptr;
+  double *al_msign = nullptr, *al_osign = nullptr;
+  int al_n = 0;
+  Consts consts{};
 
-  BlockView view(int b, int cur) const {
-    BlockView v;
-    const Box &bx = boxes[b];
-    v.U = arena + (int64_t)cur * ubuf + ubase[b];
-    v.Unext = arena + (int64_t)(cur ^ 1) * ubuf + ubase[b];
-    v.M = arena + main_off + mbase[b];
-    v.total = bx.total;
-    v.si = bx.si;
-    v.sj = bx.sj;
-    v.G = bx.G;
-    for (int a = 0; a < 3; ++a) v.n[a] = bx.n[a];
-    return v;
-  }
-  // Arena offset of a DOF; U components relative to the U region with the flag bit.
-  int64_t dof_offset(const mhd_dof &d, bool *ok) const {
+  // block << 48 | comp << 40 | box offset
+  int64_t code(const mhd_dof &d, bool *ok) const {
     *ok = false;
     if (d.field < 0 || d.field >= MHD_NUM_FIELDS || d.block < 0 || d.block >= nblocks) return 0;
     if (d.comp < 0 || d.comp >= kFieldSpec[d.field].ncomp) return 0;
@@ -130,201 +111,319 @@ struct mhd_ctx {
     const int64_t off = (int64_t)(d.i + bx.G) * bx.si + (int64_t)(d.j + bx.G) * bx.sj + (d.k + bx.G);
     const int c = kComp.first[d.field] + d.comp;
     *ok = true;
-    if (c < kNumUComps) return (ubase[d.block] + (int64_t)c * bx.total + off) | kUFlag;
-    return main_off + mbase[d.block] + (int64_t)(c - kNumUComps) * bx.total + off;
+    return ((int64_t)d.block << 48) | ((int64_t)c << 40) | off;
   }
-  double *comp_ptr(int b, int c, int cur) const {
-    if (c < kNumUComps) return arena + (int64_t)cur * ubuf + ubase[b] + (int64_t)c * boxes[b].total;
+  double *comp_ptr(int b, int c, int buf) const {
+    if (c < kNumUComps) return arena + (int64_t)buf * ubuf + ubase[b] + (int64_t)c * boxes[b].total;
     return arena + main_off + mbase[b] + (int64_t)(c - kNumUComps) * boxes[b].total;
   }
 };
 
+}  // namespace
+
+struct mhd_batch {
+  int capacity = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<Solve *> slots;
+  // device directory (fixed addresses for the lifetime of the batch)
+  DevSolve *dsolves = nullptr;
+  SolveState *dstate = nullptr;
+  int *dprefix_tiles[kNumRanges] = {};
+  int *dprefix_copy[kMaxGroups][2] = {};
+  int *dprefix_aliasE = nullptr, *dprefix_aliasJ = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int kernels_per_step = 0;
+  double *staging = nullptr;
+  size_t staging_elems = 0;
+  double **comp_ptrs = nullptr;
+  SolveState *hstate = nullptr;  // pinned mirror of dstate
+  // eager profiling
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_events;
+  std::vector<const char *> prof_names;
+  size_t prof_used = 0;
+
+  Dir dir(int mode) const {
+    Dir d;
+    d.solves = dsolves;
+    d.state = dstate;
+    d.nsolves = capacity;
+    d.mode = mode;
+    for (int r = 0; r < kNumRanges; ++r) d.solve_tile_prefix[r] = dprefix_tiles[r];
+    for (int g = 0; g < kMaxGroups; ++g)
+      for (int p = 0; p < 2; ++p) d.copy_prefix[g][p] = dprefix_copy[g][p];
+    d.aliasE_prefix = dprefix_aliasE;
+    d.aliasJ_prefix = dprefix_aliasJ;
+    return d;
+  }
+};
+
+struct mhd_ctx {
+  mhd_batch *batch = nullptr;
+};
+
 namespace {
 
-// After a launch: in profiling mode record an event labelled `name`.
-void mark(mhd_ctx *ctx, const char *name) {
-  if (!ctx->profiling) return;
-  if (ctx->prof_used == ctx->prof_events.size()) {
+void mark(mhd_batch *b, const char *name) {
+  if (!b->profiling) return;
+  if (b->prof_used == b->prof_events.size()) {
     cudaEvent_t e;
     cudaEventCreate(&e);
-    ctx->prof_events.push_back(e);
-    ctx->prof_names.push_back(name);
+    b->prof_events.push_back(e);
+    b->prof_names.push_back(name);
   }
-  ctx->prof_names[ctx->prof_used] = name;
-  cudaEventRecord(ctx->prof_events[ctx->prof_used++], ctx->stream);
+  b->prof_names[b->prof_used] = name;
+  cudaEventRecord(b->prof_events[b->prof_used++], b->stream);
 }
 
-int upload_table(const mhd_copy *tab, int n, const mhd_ctx *ctx, DevTable *out) {
-  out->n = n;
-  if (n <= 0) return MHD_OK;
+void launch(mhd_batch *b, int mode, StepKernel k, int *nk, int a0 = 0, int a1 = 0) {
+  launch_step_kernel(k, b->dir(mode), b->stream, a0, a1);
+  ++*nk;
+  mark(b, step_kernel_name(k));
+}
+
+// MercuryBoundary::Sync(group) (Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110):
+// the group's halo copies, then its owner copies.
+void enqueue_sync(mhd_batch *b, int mode, int g, int *nk) {
+  launch(b, mode, SK_COPY, nk, g, 0);
+  launch(b, mode, SK_COPY, nk, g, 1);
+}
+
+// UpdateDerivedFields_ (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:309-321) plus the
+// contravariant velocities and the next step's CFL dt.
+void enqueue_derived(mhd_batch *b, int mode, int *nk) {
+  launch(b, mode, SK_BCELL_JEDGE, nk);
+  enqueue_sync(b, mode, MHD_SYNC_B_CELL, nk);
+  launch(b, mode, SK_ALIAS, nk, 1);
+  enqueue_sync(b, mode, MHD_SYNC_JEDGE, nk);
+  launch(b, mode, SK_JCELL, nk);
+  enqueue_sync(b, mode, MHD_SYNC_J_CELL, nk);
+  launch(b, mode, SK_PV_UPLUS, nk);
+}
+
+// StepOnce (Z4_Mercury/src/MercurySolver_Driver.cpp:21-61) for every active slot.
+void enqueue_step(mhd_batch *b, int *nk) {
+  const int m = 0;
+  // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171)
+  launch(b, m, SK_FACE_EMF, nk);
+  launch(b, m, SK_EDGE_EMF, nk);
+  launch(b, m, SK_ALIAS, nk, 0);
+  launch(b, m, SK_HALL_CELL, nk);
+  launch(b, m, SK_HALL_EDGE, nk);
+  enqueue_sync(b, m, MHD_SYNC_EHALL, nk);
+  launch(b, m, SK_ADD_HALL, nk);
+  enqueue_sync(b, m, MHD_SYNC_EEDGE, nk);
+  // AssembleRHS_Fluid_ + ApplyUpdate_Euler_ (state into the other buffer) and
+  // the constrained-transport face update (Z4_Mercury/src/physics/MercurySolver_Advance.cpp:73-147)
+  launch(b, m, SK_FLUID, nk);
+  launch(b, m, SK_BFACE, nk);
+  launch(b, m, SK_FLIP, nk);
+  enqueue_sync(b, m, MHD_SYNC_UCELL, nk);
+  enqueue_sync(b, m, MHD_SYNC_BFACE, nk);
+  enqueue_derived(b, m, nk);
+  launch(b, m, SK_RETIRE, nk);
+}
+
+int ensure_staging(mhd_batch *b, size_t elems) {
+  if (elems <= b->staging_elems) return MHD_OK;
+  if (b->staging) cudaFreeAsync(b->staging, b->stream);
+  b->staging = nullptr;
+  b->staging_elems = 0;
+  if (cudaMallocAsync((void **)&b->staging, sizeof(double) * elems, b->stream) != cudaSuccess)
+    return fail(MHD_ERR_OOM, "staging of %zu doubles", elems);
+  b->staging_elems = elems;
+  return MHD_OK;
+}
+
+// Rewrites the directory: per-range and per-table prefix sums over the slots
+// and every slot's DevSolve (empty slots contribute no items).
+int publish(mhd_batch *b) {
+  const int C = b->capacity;
+  std::vector<int> pre((size_t)C + 1);
+  auto put = [&](int *dst, auto count) -> int {
+    pre[0] = 0;
+    for (int s = 0; s < C; ++s) pre[s + 1] = pre[s] + (b->slots[s] ? count(b->slots[s]) : 0);
+    CUDA_TRY(cudaMemcpyAsync(dst, pre.data(), sizeof(int) * (C + 1), cudaMemcpyHostToDevice, b->stream));
+    return MHD_OK;
+  };
+  int rc;
+  for (int r = 0; r < kNumRanges; ++r)
+    if ((rc = put(b->dprefix_tiles[r], [&](const Solve *S) { return S->tiles[r]; }))) return rc;
+  for (int g = 0; g < kMaxGroups; ++g)
+    for (int p = 0; p < 2; ++p)
+      if ((rc = put(b->dprefix_copy[g][p], [&](const Solve *S) { return S->tab_n[g][p]; }))) return rc;
+  if ((rc = put(b->dprefix_aliasE, [](const Solve *S) { return S->al_n; }))) return rc;
+  if ((rc = put(b->dprefix_aliasJ, [](const Solve *S) { return S->al_n; }))) return rc;
+  std::vector<DevSolve> ds((size_t)C);
+  for (int s = 0; s < C; ++s) {
+    DevSolve &d = ds[s];
+    std::memset(&d, 0, sizeof d);
+    const Solve *S = b->slots[s];
+    if (!S) continue;
+    d.c = S->consts;
+    d.blocks = S->dblocks;
+    d.nblocks = S->nblocks;
+    for (int r = 0; r < kNumRanges; ++r) d.tile_prefix[r] = S->dtile_prefix[r];
+    for (int g = 0; g < kMaxGroups; ++g) {
+      d.halo[g] = DevTable{S->tab_dst[g][0], S->tab_src[g][0], S->tab_sign[g][0], S->tab_n[g][0]};
+      d.owner[g] = DevTable{S->tab_dst[g][1], S->tab_src[g][1], S->tab_sign[g][1], S->tab_n[g][1]};
+    }
+    d.aliasE = DevAlias{S->al_off, S->al_memE, S->al_msign, S->al_ownE, S->al_osign, S->al_n};
+    d.aliasJ = DevAlias{S->al_off, S->al_memJ, S->al_msign, S->al_ownJ, S->al_osign, S->al_n};
+  }
+  CUDA_TRY(cudaMemcpyAsync(b->dsolves, ds.data(), sizeof(DevSolve) * C, cudaMemcpyHostToDevice, b->stream));
+  return MHD_OK;
+}
+
+// One group phase's copy table, sorted by destination so that consecutive
+// threads write (and mostly read) consecutive k.  Destinations within one
+// phase are distinct and each phase reads values the phase does not write,
+// so the order of the copies does not change the result.
+int upload_copies(Solve *S, const mhd_copy *tab, int n, int g, int phase, cudaStream_t st) {
+  if (n < 0 || (n > 0 && !tab)) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, phase);
   std::vector<int64_t> dst(n), src(n);
   std::vector<double> sign(n);
+  std::vector<int> order(n);
   for (int t = 0; t < n; ++t) {
-    bool ok1, ok2;
-    dst[t] = ctx->dof_offset(tab[t].dst, &ok1);
-    src[t] = ctx->dof_offset(tab[t].src, &ok2);
-    if (!ok1 || !ok2) return fail(MHD_ERR_ARG, "sync table entry %d out of range", t);
+    bool o1, o2;
+    dst[t] = S->code(tab[t].dst, &o1);
+    src[t] = S->code(tab[t].src, &o2);
+    if (!o1 || !o2) return fail(MHD_ERR_ARG, "sync table entry %d out of range", t);
     sign[t] = tab[t].sign;
+    order[t] = t;
   }
-  CUDA_TRY(cudaMalloc(&out->dst, sizeof(int64_t) * n));
-  CUDA_TRY(cudaMalloc(&out->src, sizeof(int64_t) * n));
-  CUDA_TRY(cudaMalloc(&out->sign, sizeof(double) * n));
-  CUDA_TRY(cudaMemcpy(out->dst, dst.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(out->src, src.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(out->sign, sign.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return dst[a] < dst[c]; });
+  std::vector<int64_t> d2(n), s2(n);
+  std::vector<double> g2(n);
+  for (int t = 0; t < n; ++t) {
+    d2[t] = dst[order[t]];
+    s2[t] = src[order[t]];
+    g2[t] = sign[order[t]];
+  }
+  S->tab_n[g][phase] = n;
+  S->table_bytes += (int64_t)n * 24;
+  int rc;
+  if ((rc = dev_upload(d2, &S->tab_dst[g][phase], st)) || (rc = dev_upload(s2, &S->tab_src[g][phase], st)) ||
+      (rc = dev_upload(g2, &S->tab_sign[g][phase], st)))
+    return rc;
   return MHD_OK;
 }
 
-int upload_alias(const mhd_alias_classes &a, const int fields[3], const mhd_ctx *ctx, DevAlias *out) {
-  out->n = a.n_classes;
-  if (a.n_classes <= 0) return MHD_OK;
+int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
+  S->al_n = a.n_classes;
+  if (a.n_classes <= 0) {
+    S->al_n = 0;
+    return MHD_OK;
+  }
+  if (!a.offset || !a.member || !a.member_sign || !a.owner || !a.owner_sign)
+    return fail(MHD_ERR_ARG, "alias classes: null table");
   const int nm = a.offset[a.n_classes];
-  std::vector<int64_t> mem(nm), own(a.n_classes);
-  for (int q = 0; q < nm; ++q) {
-    mhd_dof d = a.member[q];
-    if (d.field < 0 || d.field > 2) return fail(MHD_ERR_ARG, "alias member %d: axis %d", q, d.field);
-    d.field = fields[d.field];
-    bool ok;
-    mem[q] = ctx->dof_offset(d, &ok);
-    if (!ok || (mem[q] & kUFlag)) return fail(MHD_ERR_ARG, "alias member %d out of range", q);
-  }
-  for (int c = 0; c < a.n_classes; ++c) {
-    mhd_dof d = a.owner[c];
-    if (d.field < 0 || d.field > 2) return fail(MHD_ERR_ARG, "alias owner %d: axis %d", c, d.field);
-    d.field = fields[d.field];
-    bool ok;
-    own[c] = ctx->dof_offset(d, &ok);
-    if (!ok) return fail(MHD_ERR_ARG, "alias owner %d out of range", c);
-  }
-  CUDA_TRY(cudaMalloc(&out->offset, sizeof(int32_t) * (a.n_classes + 1)));
-  CUDA_TRY(cudaMalloc(&out->member, sizeof(int64_t) * nm));
-  CUDA_TRY(cudaMalloc(&out->msign, sizeof(double) * nm));
-  CUDA_TRY(cudaMalloc(&out->owner, sizeof(int64_t) * a.n_classes));
-  CUDA_TRY(cudaMalloc(&out->osign, sizeof(double) * a.n_classes));
-  CUDA_TRY(cudaMemcpy(out->offset, a.offset, sizeof(int32_t) * (a.n_classes + 1), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(out->member, mem.data(), sizeof(int64_t) * nm, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(out->msign, a.member_sign, sizeof(double) * nm, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(out->owner, own.data(), sizeof(int64_t) * a.n_classes, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(out->osign, a.owner_sign, sizeof(double) * a.n_classes, cudaMemcpyHostToDevice));
+  std::vector<int64_t> mE(nm), mJ(nm), oE(a.n_classes), oJ(a.n_classes);
+  const int ef[3] = {MHD_E_XI, MHD_E_ETA, MHD_E_ZETA}, jf[3] = {MHD_J_XI, MHD_J_ETA, MHD_J_ZETA};
+  auto both = [&](mhd_dof d, int64_t *e, int64_t *j) {
+    if (d.field < 0 || d.field > 2) return false;
+    const int ax = d.field;
+    bool o1, o2;
+    d.field = ef[ax];
+    *e = S->code(d, &o1);
+    d.field = jf[ax];
+    *j = S->code(d, &o2);
+    return o1 && o2;
+  };
+  for (int q = 0; q < nm; ++q)
+    if (!both(a.member[q], &mE[q], &mJ[q])) return fail(MHD_ERR_ARG, "alias member %d out of range", q);
+  for (int c = 0; c < a.n_classes; ++c)
+    if (!both(a.owner[c], &oE[c], &oJ[c])) return fail(MHD_ERR_ARG, "alias owner %d out of range", c);
+  std::vector<int32_t> off(a.offset, a.offset + a.n_classes + 1);
+  std::vector<double> ms(a.member_sign, a.member_sign + nm), os(a.owner_sign, a.owner_sign + a.n_classes);
+  S->table_bytes += (int64_t)nm * 24 + (int64_t)a.n_classes * 28;
+  int rc;
+  if ((rc = dev_upload(off, &S->al_off, st)) || (rc = dev_upload(mE, &S->al_memE, st)) ||
+      (rc = dev_upload(mJ, &S->al_memJ, st)) || (rc = dev_upload(oE, &S->al_ownE, st)) ||
+      (rc = dev_upload(oJ, &S->al_ownJ, st)) || (rc = dev_upload(ms, &S->al_msign, st)) ||
+      (rc = dev_upload(os, &S->al_osign, st)))
+    return rc;
   return MHD_OK;
 }
 
-void free_table(DevTable &t) {
-  cudaFree(t.dst);
-  cudaFree(t.src);
-  cudaFree(t.sign);
-  t = DevTable{};
-}
-void free_alias(DevAlias &a) {
-  cudaFree(a.offset);
-  cudaFree(a.member);
-  cudaFree(a.msign);
-  cudaFree(a.owner);
-  cudaFree(a.osign);
-  a = DevAlias{};
+void free_solve(Solve *S, cudaStream_t st) {
+  if (!S) return;
+  auto f = [&](void *p) {
+    if (p) cudaFreeAsync(p, st);
+  };
+  f(S->arena);
+  f(S->dblocks);
+  for (int r = 0; r < kNumRanges; ++r) f(S->dtile_prefix[r]);
+  for (int g = 0; g < kMaxGroups; ++g)
+    for (int p = 0; p < 2; ++p) {
+      f(S->tab_dst[g][p]);
+      f(S->tab_src[g][p]);
+      f(S->tab_sign[g][p]);
+    }
+  for (void *p : {(void *)S->al_off, (void *)S->al_memE, (void *)S->al_ownE, (void *)S->al_memJ, (void *)S->al_ownJ,
+                  (void *)S->al_msign, (void *)S->al_osign})
+    f(p);
+  delete S;
 }
 
-// MercuryBoundary::Sync(group): halo copies then owner copies.
-int enqueue_sync(mhd_ctx *ctx, int g, int cur, int *nk) {
-  const int64_t ucur_off = (int64_t)cur * ctx->ubuf;
-  if (ctx->halo[g].n) {
-    launch_copy(ctx->halo[g].dst, ctx->halo[g].src, ctx->halo[g].sign, ctx->halo[g].n, ctx->arena, ucur_off, ctx->stream);
-    mark(ctx, "k_copy(halo)");
-    ++*nk;
-  }
-  if (ctx->owner[g].n) {
-    launch_copy(ctx->owner[g].dst, ctx->owner[g].src, ctx->owner[g].sign, ctx->owner[g].n, ctx->arena, ucur_off,
-                ctx->stream);
-    mark(ctx, "k_copy(owner)");
-    ++*nk;
-  }
+int set_state_field(mhd_batch *b, int slot, size_t offset, const void *src, size_t bytes) {
+  CUDA_TRY(cudaMemcpyAsync((char *)(b->dstate + slot) + offset, src, bytes, cudaMemcpyHostToDevice, b->stream));
   return MHD_OK;
 }
 
-// UpdateDerivedFields_ (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:309-321) on buffer `cur`.
-void enqueue_derived(mhd_ctx *ctx, int cur, int *nk) {
-  cudaStream_t st = ctx->stream;
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
-    launch_bcell(ctx->view(b, cur), ctx->S, b == 0, st);
-    mark(ctx, "k_bcell");
-  }
-  enqueue_sync(ctx, MHD_SYNC_B_CELL, cur, nk);
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
-    launch_jedge(ctx->view(b, cur), st);
-    mark(ctx, "k_jedge");
-  }
-  if (ctx->aliasJ.n) {
-    launch_alias(ctx->aliasJ.offset, ctx->aliasJ.member, ctx->aliasJ.msign, ctx->aliasJ.owner, ctx->aliasJ.osign,
-                 ctx->aliasJ.n, ctx->arena, st);
-    mark(ctx, "k_alias(J)");
-    ++*nk;
-  }
-  enqueue_sync(ctx, MHD_SYNC_JEDGE, cur, nk);
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
-    launch_jcell(ctx->view(b, cur), st);
-    mark(ctx, "k_jcell");
-  }
-  enqueue_sync(ctx, MHD_SYNC_J_CELL, cur, nk);
-  for (int b = 0; b < ctx->nblocks; ++b, ++*nk) {
-    launch_pv_uplus(ctx->view(b, cur), ctx->consts, ctx->nghost, st);
-    mark(ctx, "k_pv_uplus");
-  }
+int read_state(mhd_batch *b) {
+  CUDA_TRY(cudaMemcpyAsync(b->hstate, b->dstate, sizeof(SolveState) * b->capacity, cudaMemcpyDeviceToHost, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return MHD_OK;
 }
 
-// StepOnce (Z4_Mercury/src/MercurySolver_Driver.cpp:21-61), state in buffer `cur`
-// on entry and in buffer cur^1 on exit.
-void enqueue_step(mhd_ctx *ctx, int cur, int *nk) {
-  cudaStream_t st = ctx->stream;
-  const int nb = ctx->nblocks;
-  for (int b = 0; b < nb; ++b, ++*nk) {
-    launch_timestep(ctx->view(b, cur), ctx->consts, ctx->S, st);
-    mark(ctx, "k_timestep");
-  }
-  // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171)
-  for (int b = 0; b < nb; ++b, ++*nk) {
-    launch_face_emf(ctx->view(b, cur), st);
-    mark(ctx, "k_face_emf");
-  }
-  for (int b = 0; b < nb; ++b, ++*nk) {
-    launch_edge_emf(ctx->view(b, cur), ctx->consts, st);
-    mark(ctx, "k_edge_emf");
-  }
-  if (ctx->aliasE.n) {
-    launch_alias(ctx->aliasE.offset, ctx->aliasE.member, ctx->aliasE.msign, ctx->aliasE.owner, ctx->aliasE.osign,
-                 ctx->aliasE.n, ctx->arena, st);
-    mark(ctx, "k_alias(E)");
-    ++*nk;
-  }
-  for (int b = 0; b < nb; ++b, ++*nk) {
-    launch_hall_cell(ctx->view(b, cur), ctx->consts, ctx->nghost, st);
-    mark(ctx, "k_hall_cell");
-  }
-  for (int b = 0; b < nb; ++b, ++*nk) {
-    launch_hall_edge(ctx->view(b, cur), st);
-    mark(ctx, "k_hall_edge");
-  }
-  enqueue_sync(ctx, MHD_SYNC_EHALL, cur, nk);
-  for (int b = 0; b < nb; ++b, ++*nk) {
-    launch_add_hall(ctx->view(b, cur), st);
-    mark(ctx, "k_add_hall");
-  }
-  enqueue_sync(ctx, MHD_SYNC_EEDGE, cur, nk);
-  // fluid RHS + Euler update into the other buffer, B_face update in place
-  for (int b = 0; b < nb; ++b, ++*nk) {
-    launch_update(ctx->view(b, cur), ctx->consts, ctx->S, b == 0, st);
-    mark(ctx, "k_update");
-  }
-  const int nxt = cur ^ 1;
-  enqueue_sync(ctx, MHD_SYNC_UCELL, nxt, nk);
-  enqueue_sync(ctx, MHD_SYNC_BFACE, nxt, nk);
-  enqueue_derived(ctx, nxt, nk);
+int slot_check(mhd_batch *b, int slot) {
+  if (!b) return fail(MHD_ERR_ARG, "null batch");
+  if (slot < 0 || slot >= b->capacity || !b->slots[slot]) return fail(MHD_ERR_ARG, "slot %d is not in use", slot);
+  return MHD_OK;
 }
 
-int check_status(mhd_ctx *ctx) {
-  Scalars s;
-  CUDA_TRY(cudaMemcpyAsync(&s, ctx->S, sizeof s, cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  if (s.status) return fail(s.status, "device status %d at step %lld (dt=%g)", s.status, s.step, s.dt);
+// Runs `enqueue` over slot `slot` alone (the kernels' mode 1 selects slots by mask).
+template <class F>
+int targeted(mhd_batch *b, int slot, F &&enqueue) {
+  const int one = 1, zero = 0;
+  int rc = set_state_field(b, slot, offsetof(SolveState, mask), &one, sizeof one);
+  if (rc) return rc;
+  int nk = 0;
+  enqueue(&nk);
+  CUDA_TRY(cudaGetLastError());
+  return set_state_field(b, slot, offsetof(SolveState, mask), &zero, sizeof zero);
+}
+
+int build_graph(mhd_batch *b) {
+  if (b->graph) return MHD_OK;
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int nk = 0;
+  enqueue_step(b, &nk);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess) return fail(MHD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(MHD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  b->kernels_per_step = nk;
+  return MHD_OK;
+}
+
+int xfer(mhd_batch *b, int slot, int field, int block, const int32_t lo[3], const int32_t hi[3], int ncomp,
+         Solve **S_out) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  Solve *S = b->slots[slot];
+  if (field < 0 || field >= MHD_NUM_FIELDS || block < 0 || block >= S->nblocks || !lo || !hi)
+    return fail(MHD_ERR_ARG, "transfer: bad arguments");
+  if (ncomp != kFieldSpec[field].ncomp)
+    return fail(MHD_ERR_ARG, "field %d has %d components, got %d", field, kFieldSpec[field].ncomp, ncomp);
+  const Box &bx = S->boxes[block];
+  for (int a = 0; a < 3; ++a)
+    if (lo[a] < -bx.G || hi[a] > bx.n[a] + 1 + bx.G || hi[a] <= lo[a])
+      return fail(MHD_ERR_ARG, "transfer range [%d,%d) outside the block box on axis %d", lo[a], hi[a], a);
+  *S_out = S;
   return MHD_OK;
 }
 
@@ -341,293 +440,453 @@ int mhd_field_info(int field, int32_t *ncomp, int32_t *location) {
   return MHD_OK;
 }
 
-int mhd_ctx_create(const mhd_desc *desc, mhd_ctx **out) {
-  if (!desc || !out || desc->n_blocks < 1 || !desc->cells || desc->nghost < 1)
-    return fail(MHD_ERR_ARG, "mhd_ctx_create: bad descriptor");
-  if (desc->precision != 0) return fail(MHD_ERR_ARG, "mhd_ctx_create: precision %d not available", desc->precision);
-  auto *ctx = new (std::nothrow) mhd_ctx();
-  if (!ctx) return fail(MHD_ERR_OOM, "host allocation");
-  ctx->nblocks = desc->n_blocks;
-  ctx->nghost = desc->nghost;
-  int64_t u = 0, m = 0;
-  for (int b = 0; b < ctx->nblocks; ++b) {
+// ------------------------------------------------------------------ batch API
+int mhd_batch_create(int capacity, mhd_batch **out) {
+  if (!out || capacity < 1 || capacity > 65536) return fail(MHD_ERR_ARG, "mhd_batch_create: capacity %d", capacity);
+  *out = nullptr;
+  auto *b = new (std::nothrow) mhd_batch();
+  if (!b) return fail(MHD_ERR_OOM, "host allocation");
+  b->capacity = capacity;
+  b->slots.assign(capacity, nullptr);
+  auto bail = [&](int rc) {
+    mhd_batch_destroy(b);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(MHD_ERR_CUDA, "stream create"));
+  const size_t C1 = (size_t)capacity + 1;
+  if (cudaMalloc(&b->dsolves, sizeof(DevSolve) * capacity) != cudaSuccess ||
+      cudaMalloc(&b->dstate, sizeof(SolveState) * capacity) != cudaSuccess ||
+      cudaMalloc(&b->comp_ptrs, sizeof(double *) * 72) != cudaSuccess ||
+      cudaMallocHost(&b->hstate, sizeof(SolveState) * capacity) != cudaSuccess)
+    return bail(fail(MHD_ERR_OOM, "directory of %d slots", capacity));
+  for (int r = 0; r < kNumRanges; ++r)
+    if (cudaMalloc(&b->dprefix_tiles[r], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
+  for (int g = 0; g < kMaxGroups; ++g)
+    for (int p = 0; p < 2; ++p)
+      if (cudaMalloc(&b->dprefix_copy[g][p], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
+  if (cudaMalloc(&b->dprefix_aliasE, sizeof(int) * C1) != cudaSuccess ||
+      cudaMalloc(&b->dprefix_aliasJ, sizeof(int) * C1) != cudaSuccess)
+    return bail(fail(MHD_ERR_OOM, "prefix"));
+  if (cudaMemsetAsync(b->dstate, 0, sizeof(SolveState) * capacity, b->stream) != cudaSuccess)
+    return bail(fail(MHD_ERR_CUDA, "state init"));
+  int rc = publish(b);
+  if (rc) return bail(rc);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(fail(MHD_ERR_CUDA, "batch init"));
+  *out = b;
+  return MHD_OK;
+}
+
+int mhd_batch_destroy(mhd_batch *b) {
+  if (!b) return MHD_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (auto *S : b->slots) free_solve(S, b->stream);
+  if (b->staging) cudaFreeAsync(b->staging, b->stream);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  cudaFree(b->dsolves);
+  cudaFree(b->dstate);
+  cudaFree(b->comp_ptrs);
+  if (b->hstate) cudaFreeHost(b->hstate);
+  for (int r = 0; r < kNumRanges; ++r) cudaFree(b->dprefix_tiles[r]);
+  for (int g = 0; g < kMaxGroups; ++g)
+    for (int p = 0; p < 2; ++p) cudaFree(b->dprefix_copy[g][p]);
+  cudaFree(b->dprefix_aliasE);
+  cudaFree(b->dprefix_aliasJ);
+  for (auto e : b->prof_events) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return MHD_OK;
+}
+
+int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
+  if (!desc || desc->n_blocks < 1 || !desc->cells || desc->nghost < 1) return -1;
+  int64_t bytes = 0;
+  for (int b = 0; b < desc->n_blocks; ++b) {
     const int n[3] = {desc->cells[3 * b], desc->cells[3 * b + 1], desc->cells[3 * b + 2]};
-    if (n[0] < 2 || n[1] < 2 || n[2] < 2) {
-      delete ctx;
-      return fail(MHD_ERR_ARG, "block %d: cells %d %d %d", b, n[0], n[1], n[2]);
+    if (n[0] < 2 || n[1] < 2 || n[2] < 2) return -1;
+    const Box bx = make_box(n, desc->nghost);
+    bytes += (int64_t)(kNumComps + kNumUComps) * bx.total * (int64_t)sizeof(double);
+  }
+  for (int g = 0; g < MHD_NUM_GROUPS; ++g)
+    bytes += (int64_t)(desc->groups[g].n_halo + desc->groups[g].n_owner) * 24;
+  if (desc->edge_aliases.n_classes > 0 && desc->edge_aliases.offset)
+    bytes += (int64_t)desc->edge_aliases.offset[desc->edge_aliases.n_classes] * 24 +
+             (int64_t)desc->edge_aliases.n_classes * 28;
+  return bytes;
+}
+
+int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
+  if (!b || !desc || !slot_out || desc->n_blocks < 1 || !desc->cells || desc->nghost < 1)
+    return fail(MHD_ERR_ARG, "mhd_batch_add: bad descriptor");
+  if (desc->precision != 0) return fail(MHD_ERR_ARG, "precision %d not available", desc->precision);
+  if (desc->n_blocks >= (1 << 15)) return fail(MHD_ERR_ARG, "too many blocks (%d)", desc->n_blocks);
+  int slot = -1;
+  for (int s = 0; s < b->capacity; ++s)
+    if (!b->slots[s]) {
+      slot = s;
+      break;
     }
+  if (slot < 0) return fail(MHD_ERR_OOM, "mhd_batch_add: all %d slots in use", b->capacity);
+  auto *S = new (std::nothrow) Solve();
+  if (!S) return fail(MHD_ERR_OOM, "host allocation");
+  cudaStream_t st = b->stream;
+  auto bail = [&](int rc) {
+    free_solve(S, st);
+    return rc;
+  };
+  S->nblocks = desc->n_blocks;
+  S->nghost = desc->nghost;
+  int64_t u = 0, m = 0;
+  std::vector<int> prefix[kNumRanges];
+  for (int r = 0; r < kNumRanges; ++r) prefix[r].push_back(0);
+  for (int bi = 0; bi < S->nblocks; ++bi) {
+    const int n[3] = {desc->cells[3 * bi], desc->cells[3 * bi + 1], desc->cells[3 * bi + 2]};
+    if (n[0] < 2 || n[1] < 2 || n[2] < 2) return bail(fail(MHD_ERR_ARG, "block %d: cells %d %d %d", bi, n[0], n[1], n[2]));
     Box bx = make_box(n, desc->nghost);
-    ctx->boxes.push_back(bx);
-    ctx->ubase.push_back(u);
-    ctx->mbase.push_back(m);
+    if (bx.total >= (int64_t(1) << 40)) return bail(fail(MHD_ERR_ARG, "block %d too large", bi));
+    S->boxes.push_back(bx);
+    S->ubase.push_back(u);
+    S->mbase.push_back(m);
     u += (int64_t)kNumUComps * bx.total;
     m += (int64_t)(kNumComps - kNumUComps) * bx.total;
+    for (int r = 0; r < kNumRanges; ++r)
+      prefix[r].push_back(prefix[r].back() + tiles_of(range_of(r, n, desc->nghost), r));
   }
-  ctx->ubuf = u;
-  ctx->main_off = 2 * u;
-  ctx->arena_elems = 2 * u + m;
+  S->ubuf = u;
+  S->main_off = 2 * u;
+  S->arena_elems = 2 * u + m;
   const mhd_constants &k = desc->constants;
-  ctx->consts = Consts{k.gamma,  k.M_H,           k.M_Na,          k.M_ref, k.T_ref, k.L_ref, k.U_ref, k.B_ref,
-                       k.n_ref,  k.rho_ref,       k.m_Na,          k.k_Boltz, k.q_e, k.mu0, k.state_coeff_H,
-                       k.state_coeff_Na, k.CFL,   k.hall_coef,     k.momentum_induce_coeff, k.momentum_hall_coeff,
-                       k.inver_MA2, k.ne_hall_floor, k.ambipolar};
-  int rc = MHD_OK;
-  auto bail = [&](int code) {
-    mhd_ctx_destroy(ctx);
-    return code;
-  };
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return bail(fail(MHD_ERR_CUDA, "stream create"));
-  if (cudaMalloc(&ctx->arena, sizeof(double) * ctx->arena_elems) != cudaSuccess)
-    return bail(fail(MHD_ERR_OOM, "arena of %lld doubles", (long long)ctx->arena_elems));
-  if (cudaMemset(ctx->arena, 0, sizeof(double) * ctx->arena_elems) != cudaSuccess)
+  S->consts = Consts{k.gamma,         k.M_H,       k.M_Na,        k.M_ref,
+                     k.T_ref,         k.L_ref,     k.U_ref,       k.B_ref,
+                     k.n_ref,         k.rho_ref,   k.m_Na,        k.k_Boltz,
+                     k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
+                     k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
+                     k.inver_MA2,     k.ne_hall_floor, k.ambipolar, desc->nghost};
+  if (cudaMallocAsync((void **)&S->arena, sizeof(double) * S->arena_elems, st) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail(MHD_ERR_OOM, "arena of %lld doubles", (long long)S->arena_elems));
+  }
+  if (cudaMemsetAsync(S->arena, 0, sizeof(double) * S->arena_elems, st) != cudaSuccess)
     return bail(fail(MHD_ERR_CUDA, "arena memset"));
-  if (cudaMalloc(&ctx->S, sizeof(Scalars)) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "scalars"));
-  Scalars s0{};
-  s0.dt_bits = 0;
-  if (cudaMemcpy(ctx->S, &s0, sizeof s0, cudaMemcpyHostToDevice) != cudaSuccess)
-    return bail(fail(MHD_ERR_CUDA, "scalars init"));
-  if (cudaMalloc(&ctx->comp_ptrs, sizeof(double *) * 2 * 36) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "ptrs"));
-  for (int g = 0; g < MHD_NUM_GROUPS; ++g) {
-    if ((rc = upload_table(desc->groups[g].halo, desc->groups[g].n_halo, ctx, &ctx->halo[g])) != MHD_OK) return bail(rc);
-    if ((rc = upload_table(desc->groups[g].owner, desc->groups[g].n_owner, ctx, &ctx->owner[g])) != MHD_OK)
-      return bail(rc);
+  std::vector<DevBlock> blocks(S->nblocks);
+  for (int bi = 0; bi < S->nblocks; ++bi) {
+    const Box &bx = S->boxes[bi];
+    DevBlock &d = blocks[bi];
+    d.U[0] = S->arena + S->ubase[bi];
+    d.U[1] = S->arena + S->ubuf + S->ubase[bi];
+    d.M = S->arena + S->main_off + S->mbase[bi];
+    d.total = bx.total;
+    d.si = bx.si;
+    d.sj = bx.sj;
+    d.G = bx.G;
+    for (int a = 0; a < 3; ++a) d.n[a] = bx.n[a];
+    d.solve = slot;
   }
-  const int ef[3] = {MHD_E_XI, MHD_E_ETA, MHD_E_ZETA}, jf[3] = {MHD_J_XI, MHD_J_ETA, MHD_J_ZETA};
-  if ((rc = upload_alias(desc->edge_aliases, ef, ctx, &ctx->aliasE)) != MHD_OK) return bail(rc);
-  if ((rc = upload_alias(desc->edge_aliases, jf, ctx, &ctx->aliasJ)) != MHD_OK) return bail(rc);
-  *out = ctx;
-  return MHD_OK;
-}
-
-int mhd_ctx_destroy(mhd_ctx *ctx) {
-  if (!ctx) return MHD_OK;
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (auto &g : ctx->graph)
-    if (g) cudaGraphExecDestroy(g);
-  for (int g = 0; g < MHD_NUM_GROUPS; ++g) {
-    free_table(ctx->halo[g]);
-    free_table(ctx->owner[g]);
+  int rc;
+  if ((rc = dev_upload(blocks, &S->dblocks, st))) return bail(rc);
+  for (int r = 0; r < kNumRanges; ++r) {
+    S->tiles[r] = prefix[r].back();
+    if ((rc = dev_upload(prefix[r], &S->dtile_prefix[r], st))) return bail(rc);
   }
-  free_alias(ctx->aliasE);
-  free_alias(ctx->aliasJ);
-  for (auto e : ctx->prof_events) cudaEventDestroy(e);
-  cudaFree(ctx->arena);
-  cudaFree(ctx->S);
-  cudaFree(ctx->staging);
-  cudaFree(ctx->comp_ptrs);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  for (int g = 0; g < MHD_NUM_GROUPS; ++g) {
+    if ((rc = upload_copies(S, desc->groups[g].halo, desc->groups[g].n_halo, g, 0, st))) return bail(rc);
+    if ((rc = upload_copies(S, desc->groups[g].owner, desc->groups[g].n_owner, g, 1, st))) return bail(rc);
+  }
+  if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
+  SolveState s0{};
+  s0.dt_bits = kDtUnset;
+  if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
+  b->slots[slot] = S;
+  if ((rc = publish(b))) return rc;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  *slot_out = slot;
   return MHD_OK;
 }
 
-static int xfer_check(mhd_ctx *ctx, int field, int block, const int32_t lo[3], const int32_t hi[3], int ncomp) {
-  if (!ctx || field < 0 || field >= MHD_NUM_FIELDS || block < 0 || block >= ctx->nblocks || !lo || !hi)
-    return fail(MHD_ERR_ARG, "transfer: bad arguments");
-  if (ncomp != kFieldSpec[field].ncomp) return fail(MHD_ERR_ARG, "field %d has %d components, got %d", field,
-                                                    kFieldSpec[field].ncomp, ncomp);
-  const Box &bx = ctx->boxes[block];
-  for (int a = 0; a < 3; ++a)
-    if (lo[a] < -bx.G || hi[a] > bx.n[a] + 1 + bx.G || hi[a] <= lo[a])
-      return fail(MHD_ERR_ARG, "transfer range [%d,%d) outside the block box on axis %d", lo[a], hi[a], a);
+int mhd_batch_remove(mhd_batch *b, int slot) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  Solve *S = b->slots[slot];
+  b->slots[slot] = nullptr;
+  SolveState s0{};
+  if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return rc;
+  if ((rc = publish(b))) return rc;
+  free_solve(S, b->stream);
   return MHD_OK;
 }
 
-static int ensure_staging(mhd_ctx *ctx, size_t elems) {
-  if (elems <= ctx->staging_elems) return MHD_OK;
-  cudaFree(ctx->staging);
-  ctx->staging = nullptr;
-  ctx->staging_elems = 0;
-  if (cudaMalloc(&ctx->staging, sizeof(double) * elems) != cudaSuccess)
-    return fail(MHD_ERR_OOM, "staging of %zu doubles", elems);
-  ctx->staging_elems = elems;
-  return MHD_OK;
-}
-
-int mhd_upload_field(mhd_ctx *ctx, int field, int block, const double *data, const int32_t lo[3], const int32_t hi[3],
-                     int ncomp) {
-  int rc = xfer_check(ctx, field, block, lo, hi, ncomp);
+int mhd_batch_upload_field(mhd_batch *b, int slot, int field, int block, const double *data, const int32_t lo[3],
+                           const int32_t hi[3], int ncomp) {
+  Solve *S = nullptr;
+  int rc = xfer(b, slot, field, block, lo, hi, ncomp, &S);
   if (rc) return rc;
   if (!data) return fail(MHD_ERR_ARG, "upload: null data");
   const int e[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
   const size_t npts = (size_t)e[0] * e[1] * e[2];
-  if ((rc = ensure_staging(ctx, npts * ncomp))) return rc;
-  CUDA_TRY(cudaMemcpyAsync(ctx->staging, data, sizeof(double) * npts * ncomp, cudaMemcpyHostToDevice, ctx->stream));
-  // U components go to both buffers (ghost corners never written by the step
-  // must be identical in both).
+  if ((rc = ensure_staging(b, npts * ncomp))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(b->staging, data, sizeof(double) * npts * ncomp, cudaMemcpyHostToDevice, b->stream));
+  // U components go to both buffers: ghost corners the step never writes must
+  // be identical in both.
   const int c0 = kComp.first[field];
   const int ndst = c0 < kNumUComps ? 2 : 1;
   double *ptrs[72];
   for (int d = 0; d < ndst; ++d)
-    for (int m = 0; m < ncomp; ++m) ptrs[d * ncomp + m] = ctx->comp_ptr(block, c0 + m, d == 0 ? ctx->ucur : ctx->ucur ^ 1);
-  CUDA_TRY(cudaMemcpyAsync(ctx->comp_ptrs, ptrs, sizeof(double *) * ndst * ncomp, cudaMemcpyHostToDevice, ctx->stream));
-  const Box &bx = ctx->boxes[block];
-  k_scatter_aos<<<(unsigned)((npts + 255) / 256), 256, 0, ctx->stream>>>(ctx->staging, lo[0], lo[1], lo[2], e[0], e[1],
-                                                                         e[2], ncomp, ctx->comp_ptrs, ndst, bx.si, bx.sj,
-                                                                         bx.G);
+    for (int m = 0; m < ncomp; ++m) ptrs[d * ncomp + m] = S->comp_ptr(block, c0 + m, d);
+  CUDA_TRY(cudaMemcpyAsync(b->comp_ptrs, ptrs, sizeof(double *) * ndst * ncomp, cudaMemcpyHostToDevice, b->stream));
+  const Box &bx = S->boxes[block];
+  k_scatter_aos<<<(unsigned)((npts + 255) / 256), 256, 0, b->stream>>>(b->staging, lo[0], lo[1], lo[2], e[0], e[1], e[2],
+                                                                       ncomp, b->comp_ptrs, ndst, bx.si, bx.sj, bx.G);
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  ctx->prepared = false;
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  S->prepared = false;
   return MHD_OK;
 }
 
-int mhd_download_field(mhd_ctx *ctx, int field, int block, double *data, const int32_t lo[3], const int32_t hi[3],
-                       int ncomp) {
-  int rc = xfer_check(ctx, field, block, lo, hi, ncomp);
+int mhd_batch_download_field(mhd_batch *b, int slot, int field, int block, double *data, const int32_t lo[3],
+                             const int32_t hi[3], int ncomp) {
+  Solve *S = nullptr;
+  int rc = xfer(b, slot, field, block, lo, hi, ncomp, &S);
   if (rc) return rc;
   if (!data) return fail(MHD_ERR_ARG, "download: null data");
+  if ((rc = read_state(b))) return rc;
+  const int cur = b->hstate[slot].cur;
   const int e[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
   const size_t npts = (size_t)e[0] * e[1] * e[2];
-  if ((rc = ensure_staging(ctx, npts * ncomp))) return rc;
+  if ((rc = ensure_staging(b, npts * ncomp))) return rc;
   const int c0 = kComp.first[field];
   double *ptrs[36];
-  for (int m = 0; m < ncomp; ++m) ptrs[m] = ctx->comp_ptr(block, c0 + m, ctx->ucur);
-  CUDA_TRY(cudaMemcpyAsync(ctx->comp_ptrs, ptrs, sizeof(double *) * ncomp, cudaMemcpyHostToDevice, ctx->stream));
-  const Box &bx = ctx->boxes[block];
-  k_gather_aos<<<(unsigned)((npts + 255) / 256), 256, 0, ctx->stream>>>(ctx->staging, lo[0], lo[1], lo[2], e[0], e[1],
-                                                                        e[2], ncomp, ctx->comp_ptrs, bx.si, bx.sj, bx.G);
+  for (int m = 0; m < ncomp; ++m) ptrs[m] = S->comp_ptr(block, c0 + m, cur);
+  CUDA_TRY(cudaMemcpyAsync(b->comp_ptrs, ptrs, sizeof(double *) * ncomp, cudaMemcpyHostToDevice, b->stream));
+  const Box &bx = S->boxes[block];
+  k_gather_aos<<<(unsigned)((npts + 255) / 256), 256, 0, b->stream>>>(b->staging, lo[0], lo[1], lo[2], e[0], e[1], e[2],
+                                                                      ncomp, b->comp_ptrs, bx.si, bx.sj, bx.G);
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaMemcpyAsync(data, ctx->staging, sizeof(double) * npts * ncomp, cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(data, b->staging, sizeof(double) * npts * ncomp, cudaMemcpyDeviceToHost, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
   return MHD_OK;
 }
 
-int mhd_prepare(mhd_ctx *ctx, double time, int64_t step) {
-  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
-  Scalars s0{};
-  s0.dt_bits = (unsigned long long)0;
+int mhd_batch_sync(mhd_batch *b, int slot, int group) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  if (group < 0 || group >= MHD_NUM_GROUPS) return fail(MHD_ERR_ARG, "mhd_sync: bad group %d", group);
+  rc = targeted(b, slot, [&](int *nk) { enqueue_sync(b, 1, group, nk); });
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return MHD_OK;
+}
+
+int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  SolveState s0{};
+  s0.dt_bits = kDtUnset;
   s0.time = time;
   s0.step = step;
-  CUDA_TRY(cudaMemcpyAsync(ctx->S, &s0, sizeof s0, cudaMemcpyHostToDevice, ctx->stream));
-  int nk = 0;
-  enqueue_derived(ctx, ctx->ucur, &nk);
-  CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  ctx->prepared = true;
-  return MHD_OK;
-}
-
-static int build_graph(mhd_ctx *ctx, int cur) {
-  if (ctx->graph[cur]) return MHD_OK;
-  cudaGraph_t g = nullptr;
-  CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  int nk = 0;
-  enqueue_step(ctx, cur, &nk);
-  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-  if (e != cudaSuccess) return fail(MHD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&ctx->graph[cur], g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return fail(MHD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-  ctx->kernels_per_step = nk;
-  return MHD_OK;
-}
-
-int mhd_step_async(mhd_ctx *ctx, int nsteps) {
-  if (!ctx || nsteps < 0) return fail(MHD_ERR_ARG, "mhd_step: bad arguments");
-  if (!ctx->prepared) return fail(MHD_ERR_STATE, "mhd_step before mhd_prepare");
-  int rc;
-  for (int s = 0; s < nsteps; ++s) {
-    if ((rc = build_graph(ctx, ctx->ucur))) return rc;
-    CUDA_TRY(cudaGraphLaunch(ctx->graph[ctx->ucur], ctx->stream));
-    ctx->ucur ^= 1;
-  }
-  return MHD_OK;
-}
-
-int mhd_synchronize(mhd_ctx *ctx) {
-  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  return check_status(ctx);
-}
-
-int mhd_step(mhd_ctx *ctx, int nsteps, double *dt_out) {
-  int rc = mhd_step_async(ctx, nsteps);
+  // keep the current buffer index
+  if ((rc = read_state(b))) return rc;
+  s0.cur = b->hstate[slot].cur;
+  if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return rc;
+  rc = targeted(b, slot, [&](int *nk) { enqueue_derived(b, 1, nk); });
   if (rc) return rc;
-  if ((rc = mhd_synchronize(ctx))) return rc;
-  if (dt_out) {
-    Scalars s;
-    CUDA_TRY(cudaMemcpy(&s, ctx->S, sizeof s, cudaMemcpyDeviceToHost));
-    *dt_out = s.dt;
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  b->slots[slot]->prepared = true;
+  return MHD_OK;
+}
+
+int mhd_batch_request(mhd_batch *b, int slot, int64_t nsteps) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  if (nsteps < 0) return fail(MHD_ERR_ARG, "nsteps %lld", (long long)nsteps);
+  if (nsteps > 0 && !b->slots[slot]->prepared) return fail(MHD_ERR_STATE, "steps requested before prepare");
+  const long long n = nsteps;
+  return set_state_field(b, slot, offsetof(SolveState, remaining), &n, sizeof n);
+}
+
+int mhd_batch_run(mhd_batch *b, int nsteps) {
+  if (!b || nsteps < 0) return fail(MHD_ERR_ARG, "mhd_batch_run: bad arguments");
+  int rc = build_graph(b);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+  return MHD_OK;
+}
+
+int mhd_batch_poll(mhd_batch *b, mhd_info *infos) {
+  if (!b || !infos) return fail(MHD_ERR_ARG, "mhd_batch_poll: bad arguments");
+  int rc = read_state(b);
+  if (rc) return rc;
+  for (int s = 0; s < b->capacity; ++s) {
+    const SolveState &st = b->hstate[s];
+    std::memset(&infos[s], 0, sizeof(mhd_info));
+    infos[s].time = st.time;
+    infos[s].dt = st.dt;
+    infos[s].step = st.step;
+    infos[s].status = st.status;
+    infos[s].remaining = st.remaining;
+    const Solve *S = b->slots[s];
+    infos[s].device_bytes = S ? (int64_t)(S->arena_elems * sizeof(double)) + S->table_bytes : 0;
   }
   return MHD_OK;
 }
 
-int mhd_step_profiled(mhd_ctx *ctx, int nsteps, int max_kernels, float *kernel_ms, const char **kernel_names,
-                      int *n_kernels) {
-  if (!ctx || nsteps < 1 || !kernel_ms || !n_kernels) return fail(MHD_ERR_ARG, "mhd_step_profiled: bad arguments");
-  if (!ctx->prepared) return fail(MHD_ERR_STATE, "mhd_step_profiled before mhd_prepare");
+void *mhd_batch_stream(mhd_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+int mhd_batch_kernels_per_step(mhd_batch *b) {
+  if (!b) return -1;
+  if (build_graph(b) != MHD_OK) return -1;
+  return b->kernels_per_step;
+}
+
+int mhd_batch_step_profiled(mhd_batch *b, int nsteps, int max_kernels, float *kernel_ms, const char **kernel_names,
+                            int *n_kernels) {
+  if (!b || nsteps < 1 || !kernel_ms || !n_kernels) return fail(MHD_ERR_ARG, "mhd_step_profiled: bad arguments");
   std::vector<float> acc;
   int per_step = 0;
   for (int s = 0; s < nsteps; ++s) {
-    ctx->profiling = true;
-    ctx->prof_used = 0;
-    mark(ctx, "start");
+    b->profiling = true;
+    b->prof_used = 0;
+    mark(b, "start");
     int nk = 0;
-    enqueue_step(ctx, ctx->ucur, &nk);
-    ctx->profiling = false;
+    enqueue_step(b, &nk);
+    b->profiling = false;
     CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    ctx->ucur ^= 1;
-    per_step = (int)ctx->prof_used - 1;
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    per_step = (int)b->prof_used - 1;
     if (acc.empty()) acc.assign(per_step, 0.0f);
     for (int q = 0; q < per_step; ++q) {
       float ms = 0.0f;
-      CUDA_TRY(cudaEventElapsedTime(&ms, ctx->prof_events[q], ctx->prof_events[q + 1]));
+      CUDA_TRY(cudaEventElapsedTime(&ms, b->prof_events[q], b->prof_events[q + 1]));
       acc[q] += ms;
     }
   }
   const int n = per_step < max_kernels ? per_step : max_kernels;
   for (int q = 0; q < n; ++q) {
     kernel_ms[q] = acc[q] / (float)nsteps;
-    if (kernel_names) kernel_names[q] = ctx->prof_names[q + 1];
+    if (kernel_names) kernel_names[q] = b->prof_names[q + 1];
   }
   *n_kernels = n;
-  return check_status(ctx);
-}
-
-int mhd_sync(mhd_ctx *ctx, int group) {
-  if (!ctx || group < 0 || group >= MHD_NUM_GROUPS) return fail(MHD_ERR_ARG, "mhd_sync: bad arguments");
-  int nk = 0;
-  enqueue_sync(ctx, group, ctx->ucur, &nk);
-  CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return MHD_OK;
 }
 
-int mhd_get_info(mhd_ctx *ctx, mhd_info *info) {
-  if (!ctx || !info) return fail(MHD_ERR_ARG, "mhd_get_info: bad arguments");
-  Scalars s;
-  CUDA_TRY(cudaMemcpyAsync(&s, ctx->S, sizeof s, cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  info->time = s.time;
-  info->dt = s.dt;
-  info->step = s.step;
-  info->status = s.status;
-  info->device_bytes = (int64_t)(ctx->arena_elems * sizeof(double));
-  return MHD_OK;
-}
-
-void *mhd_stream(mhd_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
-
-int mhd_kernels_per_step(mhd_ctx *ctx) {
-  if (!ctx) return -1;
-  if (!ctx->kernels_per_step && build_graph(ctx, ctx->ucur) != MHD_OK) return -1;
-  return ctx->kernels_per_step;
-}
-
-int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base, int32_t *G, int64_t *si, int64_t *sj,
-                    int32_t ext[3]) {
-  if (!ctx || field < 0 || field >= MHD_NUM_FIELDS || block < 0 || block >= ctx->nblocks || comp < 0 ||
+int mhd_batch_device_view(mhd_batch *b, int slot, int field, int block, int comp, double **base, int32_t *G,
+                          int64_t *si, int64_t *sj, int32_t ext[3]) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  Solve *S = b->slots[slot];
+  if (field < 0 || field >= MHD_NUM_FIELDS || block < 0 || block >= S->nblocks || comp < 0 ||
       comp >= kFieldSpec[field].ncomp)
     return fail(MHD_ERR_ARG, "mhd_device_view: bad arguments");
-  const Box &bx = ctx->boxes[block];
-  if (base) *base = ctx->comp_ptr(block, kComp.first[field] + comp, ctx->ucur);
+  if ((rc = read_state(b))) return rc;
+  const Box &bx = S->boxes[block];
+  if (base) *base = S->comp_ptr(block, kComp.first[field] + comp, b->hstate[slot].cur);
   if (G) *G = bx.G;
   if (si) *si = bx.si;
   if (sj) *sj = bx.sj;
   if (ext)
     for (int a = 0; a < 3; ++a) ext[a] = bx.ext[a];
   return MHD_OK;
+}
+
+// ------------------------------------------------------------------ single solve
+int mhd_ctx_create(const mhd_desc *desc, mhd_ctx **out) {
+  if (!desc || !out) return fail(MHD_ERR_ARG, "mhd_ctx_create: bad descriptor");
+  auto *ctx = new (std::nothrow) mhd_ctx();
+  if (!ctx) return fail(MHD_ERR_OOM, "host allocation");
+  int rc = mhd_batch_create(1, &ctx->batch);
+  if (rc) {
+    delete ctx;
+    return rc;
+  }
+  int slot = -1;
+  if ((rc = mhd_batch_add(ctx->batch, desc, &slot))) {
+    const std::string err = g_last_error;
+    mhd_batch_destroy(ctx->batch);
+    delete ctx;
+    g_last_error = err;
+    return rc;
+  }
+  *out = ctx;
+  return MHD_OK;
+}
+
+int mhd_ctx_destroy(mhd_ctx *ctx) {
+  if (!ctx) return MHD_OK;
+  mhd_batch_destroy(ctx->batch);
+  delete ctx;
+  return MHD_OK;
+}
+
+int mhd_upload_field(mhd_ctx *ctx, int field, int block, const double *data, const int32_t lo[3], const int32_t hi[3],
+                     int ncomp) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_upload_field(ctx->batch, 0, field, block, data, lo, hi, ncomp);
+}
+
+int mhd_download_field(mhd_ctx *ctx, int field, int block, double *data, const int32_t lo[3], const int32_t hi[3],
+                       int ncomp) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_download_field(ctx->batch, 0, field, block, data, lo, hi, ncomp);
+}
+
+int mhd_prepare(mhd_ctx *ctx, double time, int64_t step) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_prepare(ctx->batch, 0, time, step);
+}
+
+int mhd_step_async(mhd_ctx *ctx, int nsteps) {
+  if (!ctx || nsteps < 0) return fail(MHD_ERR_ARG, "mhd_step: bad arguments");
+  int rc = mhd_batch_request(ctx->batch, 0, nsteps);
+  if (rc) return rc;
+  return mhd_batch_run(ctx->batch, nsteps);
+}
+
+int mhd_synchronize(mhd_ctx *ctx) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  int rc = read_state(ctx->batch);
+  if (rc) return rc;
+  const SolveState &s = ctx->batch->hstate[0];
+  if (s.status) return fail(s.status, "device status %d at step %lld", s.status, s.step);
+  return MHD_OK;
+}
+
+int mhd_step(mhd_ctx *ctx, int nsteps, double *dt_out) {
+  int rc = mhd_step_async(ctx, nsteps);
+  if (rc) return rc;
+  if ((rc = mhd_synchronize(ctx))) return rc;
+  if (dt_out) *dt_out = ctx->batch->hstate[0].dt;
+  return MHD_OK;
+}
+
+int mhd_step_profiled(mhd_ctx *ctx, int nsteps, int max_kernels, float *kernel_ms, const char **kernel_names,
+                      int *n_kernels) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  if (nsteps < 1) return fail(MHD_ERR_ARG, "mhd_step_profiled: bad arguments");
+  int rc = mhd_batch_request(ctx->batch, 0, nsteps);
+  if (rc) return rc;
+  rc = mhd_batch_step_profiled(ctx->batch, nsteps, max_kernels, kernel_ms, kernel_names, n_kernels);
+  if (rc) return rc;
+  return mhd_synchronize(ctx);
+}
+
+int mhd_sync(mhd_ctx *ctx, int group) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_sync(ctx->batch, 0, group);
+}
+
+int mhd_get_info(mhd_ctx *ctx, mhd_info *info) {
+  if (!ctx || !info) return fail(MHD_ERR_ARG, "mhd_get_info: bad arguments");
+  return mhd_batch_poll(ctx->batch, info);
+}
+
+void *mhd_stream(mhd_ctx *ctx) { return ctx ? mhd_batch_stream(ctx->batch) : nullptr; }
+
+int mhd_kernels_per_step(mhd_ctx *ctx) { return ctx ? mhd_batch_kernels_per_step(ctx->batch) : -1; }
+
+int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base, int32_t *G, int64_t *si, int64_t *sj,
+                    int32_t ext[3]) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_device_view(ctx->batch, 0, field, block, comp, base, G, si, sj, ext);
 }
 
 }  // extern "C"

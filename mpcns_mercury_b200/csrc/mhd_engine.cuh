@@ -1,0 +1,129 @@
+// Batched execution engine of the MHD step: device-resident directory of
+// solves, their blocks and their tile work-lists.
+//
+// Every step kernel is a persistent, grid-stride loop over work items of one
+// "range kind" (cells, faces+edges, the extended face range of the ideal EMF,
+// the allocated cell range).  A work item is a 32 (k) x 4 (j) x 2 (i) tile of
+// one block of one solve; the directory maps the global item index to
+// (solve, block, tile) through per-range prefix sums.  Grid sizes depend only
+// on the SM count, so one CUDA graph captured once runs any set of solves:
+// membership changes only rewrite the directory in device memory.
+#pragma once
+#include <cstdint>
+
+#include "mhd_layout.cuh"
+
+namespace mhd {
+
+// Range kinds of the work lists.
+enum RangeKind : int {
+  kCells = 0,    // owned cells [0, n)
+  kBox = 1,      // [0, n + 1): owned faces and edges of all families
+  kExt = 2,      // [-1, n + 2): face EMF candidates incl. one ghost layer
+  kAlloc = 3,    // [-g, n + g): allocated cell range
+  kCells2 = 4,   // owned cells, two work items per tile (one per ion species)
+  kNumRanges = 5
+};
+
+constexpr int kTileK = 32, kTileJ = 4, kTileI = 2, kTileThreads = kTileK * kTileJ * kTileI;
+
+// Per-block descriptor (device).
+struct DevBlock {
+  double *U[2];       // U_H, U_Na components (10) of buffer 0 / 1
+  double *M;          // all other components (kNumComps - 10)
+  int64_t total, si, sj;
+  int G, n[3];
+  int solve;          // index of the owning solve in the directory
+};
+
+// Per-solve constants, as calc_physical_constant derives them
+// (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:3-48).
+struct Consts {
+  double gamma, M_H, M_Na, M_ref, T_ref, L_ref, U_ref, B_ref, n_ref, rho_ref, m_Na, k_Boltz, q_e, mu0;
+  double state_coeff_H, state_coeff_Na, CFL, hall_coef, momentum_induce_coeff, momentum_hall_coeff;
+  double inver_MA2, ne_hall_floor;
+  int ambipolar;
+  int nghost;
+};
+
+// Per-solve device state.
+struct SolveState {
+  unsigned long long dt_bits;  // running min of the next step's CFL dt (positive double bits)
+  double dt, time;             // last dt used, simulated time
+  long long step;              // steps taken
+  long long remaining;         // steps still to take in the current request (0 = idle)
+  int status;                  // sticky mhd_status
+  int cur;                     // which U buffer holds the current state
+  int mask;                    // selected for a targeted pass (Dir::mode == 1)
+  int pad_;
+};
+
+// A flattened copy/alias table of one solve: entries encode (block, comp, cell
+// offset) as  block << 48 | comp << 40 | offset  (block local to the solve).
+struct DevTable {
+  const int64_t *dst = nullptr, *src = nullptr;
+  const double *sign = nullptr;
+  int n = 0;
+};
+struct DevAlias {
+  const int32_t *offset = nullptr;  // n + 1
+  const int64_t *member = nullptr;  // encoded E members
+  const double *msign = nullptr;
+  const int64_t *owner = nullptr;   // encoded E owners
+  const double *osign = nullptr;
+  int n = 0;
+};
+
+constexpr int kMaxGroups = MHD_NUM_GROUPS;
+
+// Directory entry of one solve (device).
+struct DevSolve {
+  Consts c;
+  const DevBlock *blocks;             // this solve's blocks (global array slice)
+  int nblocks;
+  const int *tile_prefix[kNumRanges]; // per range: nblocks + 1 prefix sums of tile counts
+  DevTable halo[kMaxGroups], owner[kMaxGroups];
+  DevAlias aliasE, aliasJ;
+};
+
+// The directory handed to every kernel (by value).
+struct Dir {
+  const DevSolve *solves;
+  SolveState *state;
+  int nsolves;
+  int mode;  // 0: solves with remaining steps (the step); 1: solves with mask set (prepare, sync)
+  const int *solve_tile_prefix[kNumRanges];  // nsolves + 1 per range
+  // sync tables: per group and phase (0 halo, 1 owner) prefix sums of entry counts over solves
+  const int *copy_prefix[kMaxGroups][2];
+  const int *aliasE_prefix, *aliasJ_prefix;
+};
+
+__host__ __device__ inline bool solve_active(const Dir &D, int s) {
+  return D.mode ? D.state[s].mask != 0 : D.state[s].remaining != 0;
+}
+
+// Tile grid of a block for a range kind.
+struct RangeBox {
+  int lo[3], hi[3];
+};
+__host__ __device__ inline RangeBox range_of(int kind, const int n[3], int g) {
+  RangeBox r;
+  for (int a = 0; a < 3; ++a) {
+    switch (kind) {
+      case kCells:
+      case kCells2: r.lo[a] = 0; r.hi[a] = n[a]; break;
+      case kBox: r.lo[a] = 0; r.hi[a] = n[a] + 1; break;
+      case kExt: r.lo[a] = -1; r.hi[a] = n[a] + 2; break;
+      default: r.lo[a] = -g; r.hi[a] = n[a] + g; break;
+    }
+  }
+  return r;
+}
+__host__ __device__ inline int tiles_of(const RangeBox &r, int kind) {
+  const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
+  const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
+  const int ti = (r.hi[0] - r.lo[0] + kTileI - 1) / kTileI;
+  return tk * tj * ti * (kind == kCells2 ? 2 : 1);
+}
+
+}  // namespace mhd

@@ -14,7 +14,7 @@
 // being allocated.
 //
 // The arithmetic is the same as the context path (k_hall_cell / k_hall_edge
-// in mhd_step.cu, i.e. BuildHallFaceEMF_Rusanov_diff_ of the reference,
+// in mhd_kernels.cu, i.e. BuildHallFaceEMF_Rusanov_diff_ of the reference,
 // Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:58-400), in the
 // same operation order, so the two agree bitwise on the edges both write.
 #include <cuda_runtime.h>

@@ -48,12 +48,14 @@ def _view(a: np.ndarray, a_lo, lo, hi, di=0, dj=0, dk=0):
 
 
 # ------------------------------------------------------------------ grids
-def cube_nodes(n: int, amp: float = 0.05):
-    """Nodes of the periodic curvilinear unit cube on [-G, n + 1 + G):
-    x_a = xi_a + amp * sin(2 pi xi_b) * sin(2 pi xi_c), (a, b, c) cyclic."""
+def cube_nodes(n, amp: float = 0.05):
+    """Nodes of the periodic curvilinear unit cube on [-G, n_a + 1 + G) per axis
+    (n an int or three cell counts): x_a = xi_a + amp * sin(2 pi xi_b) * sin(2 pi xi_c),
+    (a, b, c) cyclic, xi_a = index / n_a."""
     G = NODE_GHOST
-    idx = np.arange(-G, n + 1 + G, dtype=np.float64) / n
-    a, b, c = np.meshgrid(idx, idx, idx, indexing="ij")
+    ns = (n, n, n) if np.isscalar(n) else tuple(int(v) for v in n)
+    idx = [np.arange(-G, m + 1 + G, dtype=np.float64) / m for m in ns]
+    a, b, c = np.meshgrid(idx[0], idx[1], idx[2], indexing="ij")
     tp = 2.0 * math.pi
     x = a + amp * np.sin(tp * b) * np.sin(tp * c)
     y = b + amp * np.sin(tp * c) * np.sin(tp * a)
@@ -312,49 +314,49 @@ def _shift_sl(arr: Arr, lo, hi, d):
 def _pinv_sym3(M: np.ndarray) -> np.ndarray:
     """Pseudo-inverse of symmetric 3x3 matrices by cyclic Jacobi rotations
     (18 sweeps), dropping eigenvalues below 1e-10 of the largest — the
-    eigen_sym3 / Minv construction of ReconstructionSetup.cpp:33-66,123-133."""
-    A = M.copy()
-    shp = A.shape[:-2]
-    V = np.zeros(shp + (3, 3))
-    for a in range(3):
-        V[..., a, a] = 1.0
+    eigen_sym3 / Minv construction of ReconstructionSetup.cpp:33-66,123-133.
+    Works on component-major copies (A[p][q] contiguous over the cells)."""
+    shp = M.shape[:-2]
+    A = [[np.ascontiguousarray(M[..., p, q]) for q in range(3)] for p in range(3)]
+    one, zero = np.ones(shp), np.zeros(shp)
+    V = [[(one if a == c else zero).copy() for c in range(3)] for a in range(3)]
     for _ in range(18):
         for p in range(2):
             for q in range(p + 1, 3):
-                apq = A[..., p, q].copy()
-                skip = np.abs(apq) <= 1.0e-16 * (np.abs(A[..., p, p]) + np.abs(A[..., q, q]) + 1.0)
-                phi = 0.5 * np.arctan2(2.0 * apq, A[..., q, q] - A[..., p, p])
+                apq = A[p][q]
+                skip = np.abs(apq) <= 1.0e-16 * (np.abs(A[p][p]) + np.abs(A[q][q]) + 1.0)
+                phi = 0.5 * np.arctan2(2.0 * apq, A[q][q] - A[p][p])
                 c, s = np.cos(phi), np.sin(phi)
                 c = np.where(skip, 1.0, c)
                 s = np.where(skip, 0.0, s)
-                app, aqq = A[..., p, p].copy(), A[..., q, q].copy()
+                app, aqq = A[p][p], A[q][q]
                 r = 3 - p - q
-                akp, akq = A[..., r, p].copy(), A[..., r, q].copy()
+                akp, akq = A[r][p], A[r][q]
                 nkp = c * akp - s * akq
                 nkq = s * akp + c * akq
-                A[..., r, p] = np.where(skip, akp, nkp)
-                A[..., p, r] = A[..., r, p]
-                A[..., r, q] = np.where(skip, akq, nkq)
-                A[..., q, r] = A[..., r, q]
+                A[r][p] = np.where(skip, akp, nkp)
+                A[p][r] = A[r][p]
+                A[r][q] = np.where(skip, akq, nkq)
+                A[q][r] = A[r][q]
                 npp = c * c * app - 2.0 * s * c * apq + s * s * aqq
                 nqq = s * s * app + 2.0 * s * c * apq + c * c * aqq
-                A[..., p, p] = np.where(skip, app, npp)
-                A[..., q, q] = np.where(skip, aqq, nqq)
-                A[..., p, q] = np.where(skip, apq, 0.0)
-                A[..., q, p] = A[..., p, q]
+                A[p][p] = np.where(skip, app, npp)
+                A[q][q] = np.where(skip, aqq, nqq)
+                A[p][q] = np.where(skip, apq, 0.0)
+                A[q][p] = A[p][q]
                 for k in range(3):
-                    vkp, vkq = V[..., k, p].copy(), V[..., k, q].copy()
-                    V[..., k, p] = np.where(skip, vkp, c * vkp - s * vkq)
-                    V[..., k, q] = np.where(skip, vkq, s * vkp + c * vkq)
-    lam = np.stack([A[..., 0, 0], A[..., 1, 1], A[..., 2, 2]], axis=-1)
-    lmax = np.maximum(lam[..., 0], np.maximum(lam[..., 1], lam[..., 2]))
+                    vkp, vkq = V[k][p], V[k][q]
+                    V[k][p] = np.where(skip, vkp, c * vkp - s * vkq)
+                    V[k][q] = np.where(skip, vkq, s * vkp + c * vkq)
+    lam = [A[0][0], A[1][1], A[2][2]]
+    lmax = np.maximum(lam[0], np.maximum(lam[1], lam[2]))
     Minv = np.zeros(shp + (3, 3))
     for q in range(3):
         with np.errstate(divide="ignore"):
-            inv = np.where(lam[..., q] > 1.0e-10 * lmax, 1.0 / lam[..., q], 0.0)
+            inv = np.where(lam[q] > 1.0e-10 * lmax, 1.0 / lam[q], 0.0)
         for a in range(3):
             for c in range(3):
-                Minv[..., a, c] = Minv[..., a, c] + V[..., a, q] * inv * V[..., c, q]
+                Minv[..., a, c] = Minv[..., a, c] + V[a][q] * inv * V[c][q]
     Minv[lmax <= 1.0e-30] = 0.0
     return Minv
 
@@ -502,86 +504,88 @@ def orszag_tang_state(geom: Geometry, gamma: float = 1.6667, noise: float = 1e-3
     (ghost corners) keep the uniform solar-wind state, as in the reference.
     Returns {name: Arr} for U_H, U_Na, B_xi, B_eta, B_zeta."""
     n = geom.n
-    if not (n[0] == n[1] == n[2]):
-        raise ValueError("orszag_tang_state expects a cube")
-    m = n[0]
     g = geom.g
     pi = math.acos(-1.0)
     rng = Uniform(solve_id)
     qinf, qinfs = uniform_state(gamma=gamma)
-    shape = (m + 2 * g,) * 3
+    shape = tuple(m + 2 * g for m in n)
     UH = np.empty(shape + (5,))
     UN = np.empty(shape + (5,))
     UH[...] = qinf
     UN[...] = qinfs
-    xs, ys, _ = geom.D((0, 0, 0), (m, m, m), 1, 1, 1)
+    xs, ys, _ = geom.D((0, 0, 0), n, 1, 1, 1)
     rho, p = 1.0, 0.6
     u = -np.sin(2.0 * pi * ys)
     v = np.sin(2.0 * pi * xs)
     w = np.zeros_like(u)
     q = np.stack([np.full_like(u, rho), rho * u, rho * v, rho * w,
                   p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)], axis=-1)
-    nz = rng.sym(noise, m * m * m * 10).reshape(m, m, m, 2, 5)
-    UH[g:g + m, g:g + m, g:g + m] = q * (1.0 + nz[:, :, :, 0, :])
-    UN[g:g + m, g:g + m, g:g + m] = q * (1.0 + nz[:, :, :, 1, :])
+    ncell = n[0] * n[1] * n[2]
+    own = tuple(slice(g, g + m) for m in n)
+    nz = rng.sym(noise, ncell * 10).reshape(n + (2, 5))
+    UH[own] = q * (1.0 + nz[:, :, :, 0, :])
+    UN[own] = q * (1.0 + nz[:, :, :, 1, :])
 
     def Az(xx, yy):
         return (np.cos(4.0 * pi * xx) / (4.0 * pi) + np.cos(2.0 * pi * yy) / (2.0 * pi)) / math.sqrt(4.0 * pi)
 
-    lo, hi = (0, 0, 0), (m, m, m)
+    lo, hi = (0, 0, 0), n
     edges = []
     for off in ((1, 0, 0), (0, 1, 0), (0, 0, 1)):
         a = geom.N(lo, hi)
         b = geom.N(lo, hi, *off)
         val = Az(0.5 * (a[0] + b[0]), 0.5 * (a[1] + b[1])) * (b[2] - a[2])
-        edges.append(val * (1.0 + rng.sym(noise, m ** 3).reshape(m, m, m)))
+        edges.append(val * (1.0 + rng.sym(noise, ncell).reshape(n)))
     EX, EY, EZ = edges
     r = lambda A, di, dj, dk: np.roll(A, (-di, -dj, -dk), axis=(0, 1, 2))  # periodic shift: A[i+di]
     Bx = (EY - r(EY, 0, 0, 1)) + (r(EZ, 0, 1, 0) - EZ)
     By = (r(EX, 0, 0, 1) - EX) + (EZ - r(EZ, 1, 0, 0))
     Bz = (EX - r(EX, 0, 1, 0)) + (r(EY, 1, 0, 0) - EY)
-    out = {"U_H": Arr((-g,) * 3, (m + g,) * 3, UH), "U_Na": Arr((-g,) * 3, (m + g,) * 3, UN)}
+    hi_c = tuple(m + g for m in n)
+    out = {"U_H": Arr((-g,) * 3, hi_c, UH), "U_Na": Arr((-g,) * 3, hi_c, UN)}
     for name, Bv, ax in (("B_xi", Bx, 0), ("B_eta", By, 1), ("B_zeta", Bz, 2)):
-        ext = [m + 2 * g] * 3
+        ext = [m + 2 * g for m in n]
         ext[ax] += 1
         arr = np.zeros(tuple(ext) + (1,))
         full = np.concatenate([Bv, Bv[(slice(0, 1) if ax == 0 else slice(None),
                                        slice(0, 1) if ax == 1 else slice(None),
                                        slice(0, 1) if ax == 2 else slice(None))]], axis=ax)
-        sl = [slice(g, g + m)] * 3
-        sl[ax] = slice(g, g + m + 1)
+        sl = [slice(g, g + m) for m in n]
+        sl[ax] = slice(g, g + n[ax] + 1)
         arr[tuple(sl)] = full[..., None]
-        hi_ = [m + g] * 3
+        hi_ = list(hi_c)
         hi_[ax] += 1
         out[name] = Arr((-g,) * 3, tuple(hi_), arr)
     return out
 
 
-def cube_case(n: int = 32, amp: float = 0.05, solve_id: int = 0):
-    """Config 1: geometry, sources and initial state of the periodic cube.
+def cube_case(n=32, amp: float = 0.05, solve_id: int = 0):
+    """Config 1: geometry, sources and initial state of the periodic cube
+    (n cells per axis, or three per-axis counts for a periodic box).
     Returns (Geometry, {field name: Arr}) with every static input the step
     reads (reference names) and the initial state."""
-    lo, x, y, z = cube_nodes(n, amp)
-    geom = Geometry((n, n, n), lo, x, y, z)
+    ns = (n, n, n) if np.isscalar(n) else tuple(int(v) for v in n)
+    lo, x, y, z = cube_nodes(ns, amp)
+    geom = Geometry(ns, lo, x, y, z)
     f = dict(geom.fields)
     na, photo = photo_rate(geom)
     f["Na"] = na
     f["Photo_rate"] = photo
     g = NGHOST
     for name, ax in (("Badd_xi", 0), ("Badd_eta", 1), ("Badd_zeta", 2)):
-        ext = [n + 2 * g] * 3
+        ext = [m + 2 * g for m in ns]
         ext[ax] += 1
-        hi_ = [n + g] * 3
+        hi_ = [m + g for m in ns]
         hi_[ax] += 1
         f[name] = Arr((-g,) * 3, tuple(hi_), np.zeros(tuple(ext) + (1,)))
     for name, ax in (("taper_xi", 0), ("taper_eta", 1), ("taper_zeta", 2)):
-        ext = [n + 1 + 2 * g] * 3
+        ext = [m + 1 + 2 * g for m in ns]
         ext[ax] -= 1
         t = np.zeros(tuple(ext) + (1,))
-        sl = [slice(g, g + n + 1)] * 3
-        sl[ax] = slice(g, g + n)
+        sl = [slice(g, g + m + 1) for m in ns]
+        sl[ax] = slice(g, g + ns[ax])
         t[tuple(sl)] = 1.0  # Hall taper with r_min = r_max = 0 is 1 everywhere it is read
-        hi_ = [n + 1 + g] * 3
+        hi_ = [m + 1 + g for m in ns]
         hi_[ax] -= 1
         f[name] = Arr((-g,) * 3, tuple(hi_), t)
     f.update(orszag_tang_state(geom, solve_id=solve_id))

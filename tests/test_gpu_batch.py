@@ -1,0 +1,125 @@
+"""Batched solves (mhd_batch): every solve's result is the same alone and in
+the mix, bit for bit, including solves that join, finish and leave while
+others are running on the same CUDA graph.
+
+The single-solve path (mhd_ctx) is itself pinned against the reference in
+test_gpu_parity.py; here each batched solve is compared with a single-solve
+run of the same inputs, at tolerance 0 (same kernels, same operation order)."""
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+SIZES = {0: (8, 8, 8), 1: (10, 8, 12), 2: (12, 12, 12), 3: (8, 12, 10)}
+
+
+@pytest.fixture(scope="module")
+def cases():
+    if not has_gpu():
+        pytest.skip("no GPU")
+    from mpcns_mercury_b200 import workloads as W
+
+    return {sid: W.case_fields(n, solve_id=sid) for sid, n in SIZES.items()}
+
+
+def _single(fields, n, steps):
+    from mpcns_mercury_b200 import Context, reference_constants
+    from mpcns_mercury_b200 import workloads as W
+
+    ctx = Context([n], W.NGHOST, reference_constants(cfl=0.4))
+    W.upload_case(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), fields)
+    ctx.sync("UCELL")
+    ctx.sync("BFACE")
+    ctx.prepare()
+    if steps:
+        ctx.step(steps)
+    out = {name: ctx.download(W.capi_field(name), fields[name].lo, fields[name].hi) for name in W.STATE_FIELDS}
+    info = ctx.info()
+    ctx.close()
+    return out, info
+
+
+def _add(batch, fields, n):
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.capi import SolveDesc
+
+    d = SolveDesc([n], W.NGHOST, reference_constants(cfl=0.4))
+    slot = batch.add(d)
+    W.upload_case(lambda f, a, lo, hi, b: batch.upload(slot, f, a, lo, hi, block=b), fields)
+    batch.sync(slot, "UCELL")
+    batch.sync(slot, "BFACE")
+    batch.prepare(slot)
+    return slot, d
+
+
+def _state(batch, slot, fields):
+    from mpcns_mercury_b200 import workloads as W
+
+    return {name: batch.download(slot, W.capi_field(name), fields[name].lo, fields[name].hi)
+            for name in W.STATE_FIELDS}
+
+
+def _same(a, b):
+    return all(np.array_equal(a[k], b[k]) for k in a)
+
+
+def test_batch_equals_single(cases):
+    from mpcns_mercury_b200.capi import Batch
+
+    ref = {sid: _single(cases[sid], SIZES[sid], 4) for sid in (0, 1, 2)}
+    b = Batch(4)
+    slots = {sid: _add(b, cases[sid], SIZES[sid]) for sid in (0, 1, 2)}
+    for sid, (slot, _) in slots.items():
+        b.request(slot, 4)
+    b.run(4)
+    infos = b.poll()
+    for sid, (slot, _) in slots.items():
+        got = _state(b, slot, cases[sid])
+        assert _same(got, ref[sid][0]), f"solve {sid} differs from its single run"
+        assert infos[slot].step == 4 and infos[slot].remaining == 0 and infos[slot].status == 0
+        assert infos[slot].dt == ref[sid][1].dt and infos[slot].time == ref[sid][1].time
+    b.close()
+
+
+def test_batch_membership_changes(cases):
+    """Solves with different step counts; one leaves and a new one joins its
+    slot between graph launches; the survivors continue unaffected."""
+    from mpcns_mercury_b200.capi import Batch
+
+    b = Batch(3)
+    s0, d0 = _add(b, cases[0], SIZES[0])
+    s1, d1 = _add(b, cases[1], SIZES[1])
+    b.request(s0, 3)
+    b.request(s1, 5)
+    b.run(5)  # s0 idles for the last two launches
+    infos = b.poll()
+    assert infos[s0].step == 3 and infos[s1].step == 5
+    assert _same(_state(b, s0, cases[0]), _single(cases[0], SIZES[0], 3)[0])
+    assert _same(_state(b, s1, cases[1]), _single(cases[1], SIZES[1], 5)[0])
+    b.remove(s1)
+    s3, d3 = _add(b, cases[3], SIZES[3])
+    assert s3 == s1  # the freed slot is reused
+    b.request(s0, 2)
+    b.request(s3, 2)
+    b.run(2)
+    assert _same(_state(b, s0, cases[0]), _single(cases[0], SIZES[0], 5)[0])
+    assert _same(_state(b, s3, cases[3]), _single(cases[3], SIZES[3], 2)[0])
+    b.close()
+
+
+def test_batch_request_before_prepare_is_refused(cases):
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.capi import Batch, MhdError, SolveDesc
+
+    b = Batch(1)
+    d = SolveDesc([SIZES[0]], W.NGHOST, reference_constants(cfl=0.4))
+    slot = b.add(d)
+    with pytest.raises(MhdError):
+        b.request(slot, 1)
+    with pytest.raises(MhdError):
+        b.add(d)  # capacity 1 is full
+    b.close()
