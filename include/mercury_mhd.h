@@ -57,6 +57,7 @@ enum mhd_field {
   MHD_E_XI, MHD_E_ETA, MHD_E_ZETA, MHD_EHALL_XI, MHD_EHALL_ETA, MHD_EHALL_ZETA,
   MHD_EFACE_XI, MHD_EFACE_ETA, MHD_EFACE_ZETA, MHD_EHC, MHD_HALL_BETA,
   MHD_UCON,                                   /* contravariant U_plus components along xi, eta, zeta */
+  MHD_FNORM_XI, MHD_FNORM_ETA, MHD_FNORM_ZETA, /* unit normal (3) and |JD| of the faces, set by mhd_prepare */
   /* static geometry and sources (uploaded once) */
   MHD_JAC, MHD_JDXI, MHD_JDET, MHD_JDZE, MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA,
   MHD_DL_XI, MHD_DL_ETA, MHD_DL_ZETA, MHD_DR_XI, MHD_DR_ETA, MHD_DR_ZETA,
@@ -118,7 +119,7 @@ typedef struct mhd_desc {
   int32_t n_blocks;
   const int32_t *cells;   /* n_blocks * 3: cells per axis (mx, my, mz) */
   int32_t nghost;         /* runtime ghost width ngg (4 in production) */
-  int32_t precision;      /* 0 = FP64 (parity path); 1 = mixed (FP32 state/flux, FP64 metric) */
+  int32_t precision;      /* 0 = FP64 (parity path); 1 = mixed (FP32 state/flux, FP64 metric Jac/JD) */
   mhd_constants constants;
   mhd_sync_group groups[MHD_NUM_GROUPS];
   mhd_alias_classes edge_aliases;
@@ -184,7 +185,9 @@ void *mhd_stream(mhd_ctx *ctx);
 int mhd_kernels_per_step(mhd_ctx *ctx);
 
 /* Raw device pointer of one field component array of a block, with the box
- * layout: element (i,j,k) at base[(i+G)*si + (j+G)*sj + (k+G)]. */
+ * layout: element (i,j,k) at base[(i+G)*si + (j+G)*sj + (k+G)].  The
+ * elements are double, except in mixed precision (mhd_desc.precision = 1),
+ * where every field other than MHD_JAC and MHD_JD* holds float. */
 int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base, int32_t *G, int64_t *si,
                     int64_t *sj, int32_t ext[3]);
 
@@ -242,7 +245,12 @@ int mhd_hall_emf_static_scratch(const mhd_hall_block *in, double *out_xi, double
  * block shapes, sync tables and constants share a batch.  mhd_ctx is a batch
  * of capacity 1.  Calls on one batch are serialised by the caller. */
 typedef struct mhd_batch mhd_batch;
-int mhd_batch_create(int capacity, mhd_batch **out);
+/* precision: 0 = FP64 (every field double); 1 = mixed (state, work and
+ * static fields float, fluxes / EMFs / updates computed in float; the metric
+ * MHD_JAC and MHD_JD* stays double).  Every solve of a batch has the batch's
+ * precision (mhd_desc.precision).  Uploads and downloads always exchange
+ * doubles; mhd_batch_device_view returns a float array for float fields. */
+int mhd_batch_create(int capacity, int precision, mhd_batch **out);
 int mhd_batch_destroy(mhd_batch *batch);
 /* Device bytes a solve of this descriptor occupies (arena and tables); -1 on
  * a bad descriptor.  Lets a server admit requests against free HBM. */

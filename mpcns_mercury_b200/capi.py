@@ -12,14 +12,15 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmercury_mhd.so")
+# MERCURY_MHD_LIB selects another build of the library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("MERCURY_MHD_LIB") or os.path.join(HERE, "libmercury_mhd.so")
 
 # enum mhd_field, in header order
 FIELDS = [
     "U_H", "U_NA", "B_XI", "B_ETA", "B_ZETA",
     "PV_H", "PV_NA", "U_PLUS", "B_CELL", "BIND_CELL", "J_CELL", "J_XI", "J_ETA", "J_ZETA",
     "E_XI", "E_ETA", "E_ZETA", "EHALL_XI", "EHALL_ETA", "EHALL_ZETA",
-    "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA", "UCON",
+    "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA", "UCON", "FNORM_XI", "FNORM_ETA", "FNORM_ZETA",
     "JAC", "JDXI", "JDET", "JDZE", "AREA_XI", "AREA_ETA", "AREA_ZETA",
     "DL_XI", "DL_ETA", "DL_ZETA", "DR_XI", "DR_ETA", "DR_ZETA",
     "HODGE_FACE_XI", "HODGE_FACE_ETA", "HODGE_FACE_ZETA",
@@ -150,7 +151,7 @@ def lib() -> ctypes.CDLL:
     L.mhd_topology_periodic_block.argtypes = [i32p, ctypes.c_int32, ctypes.POINTER(P)]
     L.mhd_topology_fill_desc.argtypes = [P, ctypes.POINTER(MhdDesc)]
     L.mhd_topology_destroy.argtypes = [P]
-    L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(P)]
+    L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
     L.mhd_batch_destroy.argtypes = [P]
     L.mhd_desc_device_bytes.argtypes = [ctypes.POINTER(MhdDesc)]
     L.mhd_desc_device_bytes.restype = ctypes.c_int64
@@ -302,10 +303,11 @@ class SolveDesc:
 class Batch:
     """Independent solves advanced together by one CUDA graph per step (mhd_batch)."""
 
-    def __init__(self, capacity: int):
+    def __init__(self, capacity: int, precision: int = 0):
         self.capacity = capacity
+        self.precision = precision
         self.b = ctypes.c_void_p()
-        check(lib().mhd_batch_create(capacity, ctypes.byref(self.b)), "mhd_batch_create")
+        check(lib().mhd_batch_create(capacity, precision, ctypes.byref(self.b)), "mhd_batch_create")
 
     def add(self, desc: SolveDesc) -> int:
         slot = ctypes.c_int()

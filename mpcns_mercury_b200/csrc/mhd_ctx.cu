@@ -47,9 +47,10 @@ int fail(int code, const char *fmt, ...) {
 
 constexpr unsigned long long kDtUnset = 0x54B249AD2594C37DULL;  // bit pattern of 1e100
 
-// AoS (FieldBlock) <-> SoA box scatter/gather for uploads and downloads.
+// AoS (FieldBlock) <-> SoA box scatter/gather for uploads and downloads; the
+// device arrays hold doubles (fp32 = 0) or floats (fp32 = 1).
 __global__ void k_scatter_aos(const double *__restrict__ aos, int lo0, int lo1, int lo2, int e0, int e1, int e2, int nc,
-                              double *const *__restrict__ dst_comp, int ndst, int64_t si, int64_t sj, int G) {
+                              void *const *__restrict__ dst_comp, int ndst, int64_t si, int64_t sj, int G, int fp32) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t npts = (int64_t)e0 * e1 * e2;
   if (t >= npts) return;
@@ -57,17 +58,23 @@ __global__ void k_scatter_aos(const double *__restrict__ aos, int lo0, int lo1, 
   const int64_t off = (int64_t)(i + lo0 + G) * si + (int64_t)(j + lo1 + G) * sj + (k + lo2 + G);
   for (int m = 0; m < nc; ++m) {
     const double v = aos[t * nc + m];
-    for (int d = 0; d < ndst; ++d) dst_comp[d * nc + m][off] = v;
+    for (int d = 0; d < ndst; ++d) {
+      if (fp32)
+        ((float *)dst_comp[d * nc + m])[off] = (float)v;
+      else
+        ((double *)dst_comp[d * nc + m])[off] = v;
+    }
   }
 }
 __global__ void k_gather_aos(double *__restrict__ aos, int lo0, int lo1, int lo2, int e0, int e1, int e2, int nc,
-                             double *const *__restrict__ src_comp, int64_t si, int64_t sj, int G) {
+                             void *const *__restrict__ src_comp, int64_t si, int64_t sj, int G, int fp32) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t npts = (int64_t)e0 * e1 * e2;
   if (t >= npts) return;
   const int k = (int)(t % e2), j = (int)((t / e2) % e1), i = (int)(t / ((int64_t)e1 * e2));
   const int64_t off = (int64_t)(i + lo0 + G) * si + (int64_t)(j + lo1 + G) * sj + (k + lo2 + G);
-  for (int m = 0; m < nc; ++m) aos[t * nc + m] = src_comp[m][off];
+  for (int m = 0; m < nc; ++m)
+    aos[t * nc + m] = fp32 ? (double)((const float *)src_comp[m])[off] : ((const double *)src_comp[m])[off];
 }
 
 template <class T>
@@ -79,27 +86,36 @@ int dev_upload(const std::vector<T> &h, T **d, cudaStream_t st) {
   return MHD_OK;
 }
 
-// One solve: its arena, tables and its directory entry's pointees.
+// One solve: its arena, tables and its directory entry's pointees.  Arena
+// bytes: [U buffer 0 | U buffer 1 | M of every block], per block U = 10 real
+// arrays, M = 10 metric double arrays then kNumRComps real arrays.
 struct Solve {
-  int nblocks = 0, nghost = 0;
+  int nblocks = 0, nghost = 0, es = 8;  // es: bytes per real
   bool prepared = false;
   std::vector<Box> boxes;
-  std::vector<int64_t> ubase, mbase;
-  int64_t ubuf = 0, main_off = 0, arena_elems = 0, table_bytes = 0;
-  double *arena = nullptr;
+  std::vector<int64_t> ubase, mbase;  // bytes
+  int64_t ubuf = 0, main_off = 0, arena_bytes = 0, table_bytes = 0;
+  char *arena = nullptr;
   DevBlock *dblocks = nullptr;
   int *dtile_prefix[kNumRanges] = {};
   int tiles[kNumRanges] = {};
-  int64_t *tab_dst[kMaxGroups][2] = {}, *tab_src[kMaxGroups][2] = {};
-  double *tab_sign[kMaxGroups][2] = {};
-  int tab_n[kMaxGroups][2] = {};
+  int64_t *tab_seg[kMaxGroups][2] = {};
+  int tab_n[kMaxGroups][2] = {};  // segments
   int32_t *al_off = nullptr;
   int64_t *al_memE = nullptr, *al_ownE = nullptr, *al_memJ = nullptr, *al_ownJ = nullptr;
   double *al_msign = nullptr, *al_osign = nullptr;
   int al_n = 0;
   Consts consts{};
 
-  // block << 48 | comp << 40 | box offset
+  int comp_bytes(int c) const { return is_metric(c) ? 8 : es; }
+  // byte offset of component array c of block b (U comps in buffer `buf`)
+  int64_t comp_base(int b, int c, int buf) const {
+    const int64_t tot = boxes[b].total;
+    if (c < kNumUComps) return (int64_t)buf * ubuf + ubase[b] + (int64_t)c * tot * es;
+    if (is_metric(c)) return main_off + mbase[b] + (int64_t)(c - kMetricFirst) * tot * 8;
+    return main_off + mbase[b] + (int64_t)kNumMetric * tot * 8 + (int64_t)rslot(c) * tot * es;
+  }
+  // Arena code of a DOF (kCodeOffMask / kCodeUFlag in mhd_engine.cuh).
   int64_t code(const mhd_dof &d, bool *ok) const {
     *ok = false;
     if (d.field < 0 || d.field >= MHD_NUM_FIELDS || d.block < 0 || d.block >= nblocks) return 0;
@@ -110,19 +126,19 @@ struct Solve {
       if (q[a] < -bx.G || q[a] >= bx.n[a] + 1 + bx.G) return 0;
     const int64_t off = (int64_t)(d.i + bx.G) * bx.si + (int64_t)(d.j + bx.G) * bx.sj + (d.k + bx.G);
     const int c = kComp.first[d.field] + d.comp;
+    if (is_metric(c)) return 0;  // the metric is static and never synced
     *ok = true;
-    return ((int64_t)d.block << 48) | ((int64_t)c << 40) | off;
+    const int64_t code = comp_base(d.block, c, 0) + off * es;
+    return c < kNumUComps ? (kCodeUFlag | code) : code;
   }
-  double *comp_ptr(int b, int c, int buf) const {
-    if (c < kNumUComps) return arena + (int64_t)buf * ubuf + ubase[b] + (int64_t)c * boxes[b].total;
-    return arena + main_off + mbase[b] + (int64_t)(c - kNumUComps) * boxes[b].total;
-  }
+  void *comp_ptr(int b, int c, int buf) const { return arena + comp_base(b, c, buf); }
 };
 
 }  // namespace
 
 struct mhd_batch {
   int capacity = 0;
+  int precision = kFP64;
   cudaStream_t stream = nullptr;
   std::vector<Solve *> slots;
   // device directory (fixed addresses for the lifetime of the batch)
@@ -135,7 +151,7 @@ struct mhd_batch {
   int kernels_per_step = 0;
   double *staging = nullptr;
   size_t staging_elems = 0;
-  double **comp_ptrs = nullptr;
+  void **comp_ptrs = nullptr;
   SolveState *hstate = nullptr;  // pinned mirror of dstate
   // eager profiling
   bool profiling = false;
@@ -176,26 +192,41 @@ void mark(mhd_batch *b, const char *name) {
   cudaEventRecord(b->prof_events[b->prof_used++], b->stream);
 }
 
-void launch(mhd_batch *b, int mode, StepKernel k, int *nk, int a0 = 0, int a1 = 0) {
-  launch_step_kernel(k, b->dir(mode), b->stream, a0, a1);
+void launch(mhd_batch *b, int mode, StepKernel k, int *nk, const SyncOps *ops = nullptr) {
+  launch_step_kernel(k, b->dir(mode), b->stream, ops, b->precision);
   ++*nk;
   mark(b, step_kernel_name(k));
+}
+
+SyncOp copy_op(int g, int phase) { return SyncOp{SYNC_COPY, g, phase}; }
+SyncOp alias_op(int which) { return SyncOp{SYNC_ALIAS, which, 0}; }
+
+// One k_sync launch running one or two independent sync operations.
+void sync1(mhd_batch *b, int mode, SyncOp a, int *nk) {
+  SyncOps ops{{a, a}, 1};
+  launch(b, mode, SK_SYNC, nk, &ops);
+}
+void sync2(mhd_batch *b, int mode, SyncOp a, SyncOp c, int *nk) {
+  SyncOps ops{{a, c}, 2};
+  launch(b, mode, SK_SYNC, nk, &ops);
 }
 
 // MercuryBoundary::Sync(group) (Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110):
 // the group's halo copies, then its owner copies.
 void enqueue_sync(mhd_batch *b, int mode, int g, int *nk) {
-  launch(b, mode, SK_COPY, nk, g, 0);
-  launch(b, mode, SK_COPY, nk, g, 1);
+  sync1(b, mode, copy_op(g, 0), nk);
+  sync1(b, mode, copy_op(g, 1), nk);
 }
 
 // UpdateDerivedFields_ (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:309-321) plus the
-// contravariant velocities and the next step's CFL dt.
+// contravariant velocities and the next step's CFL dt.  Independent sync
+// stages share a launch: Sync(B_cell) runs beside the J alias reduction and
+// Sync(Jedge), in the same order per field as the reference.
 void enqueue_derived(mhd_batch *b, int mode, int *nk) {
   launch(b, mode, SK_BCELL_JEDGE, nk);
-  enqueue_sync(b, mode, MHD_SYNC_B_CELL, nk);
-  launch(b, mode, SK_ALIAS, nk, 1);
-  enqueue_sync(b, mode, MHD_SYNC_JEDGE, nk);
+  sync2(b, mode, copy_op(MHD_SYNC_B_CELL, 0), alias_op(1), nk);
+  sync2(b, mode, copy_op(MHD_SYNC_B_CELL, 1), copy_op(MHD_SYNC_JEDGE, 0), nk);
+  sync1(b, mode, copy_op(MHD_SYNC_JEDGE, 1), nk);
   launch(b, mode, SK_JCELL, nk);
   enqueue_sync(b, mode, MHD_SYNC_J_CELL, nk);
   launch(b, mode, SK_PV_UPLUS, nk);
@@ -204,13 +235,14 @@ void enqueue_derived(mhd_batch *b, int mode, int *nk) {
 // StepOnce (Z4_Mercury/src/MercurySolver_Driver.cpp:21-61) for every active slot.
 void enqueue_step(mhd_batch *b, int *nk) {
   const int m = 0;
-  // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171)
+  // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171);
+  // the E alias reduction (ideal EMF) and Sync(Ehall) touch different fields
   launch(b, m, SK_FACE_EMF, nk);
   launch(b, m, SK_EDGE_EMF, nk);
-  launch(b, m, SK_ALIAS, nk, 0);
   launch(b, m, SK_HALL_CELL, nk);
   launch(b, m, SK_HALL_EDGE, nk);
-  enqueue_sync(b, m, MHD_SYNC_EHALL, nk);
+  sync2(b, m, alias_op(0), copy_op(MHD_SYNC_EHALL, 0), nk);
+  sync1(b, m, copy_op(MHD_SYNC_EHALL, 1), nk);
   launch(b, m, SK_ADD_HALL, nk);
   enqueue_sync(b, m, MHD_SYNC_EEDGE, nk);
   // AssembleRHS_Fluid_ + ApplyUpdate_Euler_ (state into the other buffer) and
@@ -218,13 +250,13 @@ void enqueue_step(mhd_batch *b, int *nk) {
   launch(b, m, SK_FLUID, nk);
   launch(b, m, SK_BFACE, nk);
   launch(b, m, SK_FLIP, nk);
-  enqueue_sync(b, m, MHD_SYNC_UCELL, nk);
-  enqueue_sync(b, m, MHD_SYNC_BFACE, nk);
+  sync2(b, m, copy_op(MHD_SYNC_UCELL, 0), copy_op(MHD_SYNC_BFACE, 0), nk);
+  sync2(b, m, copy_op(MHD_SYNC_UCELL, 1), copy_op(MHD_SYNC_BFACE, 1), nk);
   enqueue_derived(b, m, nk);
   launch(b, m, SK_RETIRE, nk);
 }
 
-int ensure_staging(mhd_batch *b, size_t elems) {
+int ensure_staging(mhd_batch *b, size_t elems) {  // elems doubles
   if (elems <= b->staging_elems) return MHD_OK;
   if (b->staging) cudaFreeAsync(b->staging, b->stream);
   b->staging = nullptr;
@@ -252,8 +284,8 @@ int publish(mhd_batch *b) {
   for (int g = 0; g < kMaxGroups; ++g)
     for (int p = 0; p < 2; ++p)
       if ((rc = put(b->dprefix_copy[g][p], [&](const Solve *S) { return S->tab_n[g][p]; }))) return rc;
-  if ((rc = put(b->dprefix_aliasE, [](const Solve *S) { return S->al_n; }))) return rc;
-  if ((rc = put(b->dprefix_aliasJ, [](const Solve *S) { return S->al_n; }))) return rc;
+  if ((rc = put(b->dprefix_aliasE, [](const Solve *S) { return (S->al_n + 7) / 8; }))) return rc;
+  if ((rc = put(b->dprefix_aliasJ, [](const Solve *S) { return (S->al_n + 7) / 8; }))) return rc;
   std::vector<DevSolve> ds((size_t)C);
   for (int s = 0; s < C; ++s) {
     DevSolve &d = ds[s];
@@ -261,12 +293,15 @@ int publish(mhd_batch *b) {
     const Solve *S = b->slots[s];
     if (!S) continue;
     d.c = S->consts;
+    d.cf = to_float(S->consts);
     d.blocks = S->dblocks;
+    d.arena = S->arena;
+    d.ubuf = S->ubuf;
     d.nblocks = S->nblocks;
     for (int r = 0; r < kNumRanges; ++r) d.tile_prefix[r] = S->dtile_prefix[r];
     for (int g = 0; g < kMaxGroups; ++g) {
-      d.halo[g] = DevTable{S->tab_dst[g][0], S->tab_src[g][0], S->tab_sign[g][0], S->tab_n[g][0]};
-      d.owner[g] = DevTable{S->tab_dst[g][1], S->tab_src[g][1], S->tab_sign[g][1], S->tab_n[g][1]};
+      d.halo[g] = DevTable{S->tab_seg[g][0], S->tab_n[g][0]};
+      d.owner[g] = DevTable{S->tab_seg[g][1], S->tab_n[g][1]};
     }
     d.aliasE = DevAlias{S->al_off, S->al_memE, S->al_msign, S->al_ownE, S->al_osign, S->al_n};
     d.aliasJ = DevAlias{S->al_off, S->al_memJ, S->al_msign, S->al_ownJ, S->al_osign, S->al_n};
@@ -275,38 +310,58 @@ int publish(mhd_batch *b) {
   return MHD_OK;
 }
 
-// One group phase's copy table, sorted by destination so that consecutive
-// threads write (and mostly read) consecutive k.  Destinations within one
-// phase are distinct and each phase reads values the phase does not write,
-// so the order of the copies does not change the result.
+// One group phase's copy table as segments: sorted by destination (a
+// destination written twice keeps the later entry, as sequential
+// application would), then runs of consecutive destinations with
+// consecutive sources and the same sign merged, up to kSegMax elements.
+// Destinations of one phase are distinct and no copy of a phase reads a
+// value the phase writes, so the order of application does not change the
+// result.  Signs must be +1 or -1 (orientation flips).
 int upload_copies(Solve *S, const mhd_copy *tab, int n, int g, int phase, cudaStream_t st) {
   if (n < 0 || (n > 0 && !tab)) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, phase);
   std::vector<int64_t> dst(n), src(n);
-  std::vector<double> sign(n);
   std::vector<int> order(n);
+  std::vector<char> neg(n);
   for (int t = 0; t < n; ++t) {
     bool o1, o2;
     dst[t] = S->code(tab[t].dst, &o1);
     src[t] = S->code(tab[t].src, &o2);
-    if (!o1 || !o2) return fail(MHD_ERR_ARG, "sync table entry %d out of range", t);
-    sign[t] = tab[t].sign;
+    if (!o1 || !o2) return fail(MHD_ERR_ARG, "group %d phase %d: entry %d out of range", g, phase, t);
+    if (tab[t].sign != 1.0 && tab[t].sign != -1.0)
+      return fail(MHD_ERR_ARG, "group %d phase %d: entry %d has sign %g (must be +1 or -1)", g, phase, t, tab[t].sign);
+    neg[t] = tab[t].sign < 0.0;
     order[t] = t;
   }
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return dst[a] < dst[c]; });
-  std::vector<int64_t> d2(n), s2(n);
-  std::vector<double> g2(n);
-  for (int t = 0; t < n; ++t) {
-    d2[t] = dst[order[t]];
-    s2[t] = src[order[t]];
-    g2[t] = sign[order[t]];
+  std::vector<int64_t> seg;
+  seg.reserve(2 * (size_t)n);
+  int64_t sd = 0, ss = 0;
+  int len = 0;
+  bool sneg = false;
+  auto flush = [&]() {
+    if (!len) return;
+    seg.push_back(sd | ((int64_t)(len - 1) << kSegLenShift) | ((int64_t)sneg << kSegNegBit));
+    seg.push_back(ss);
+    len = 0;
+  };
+  for (int u = 0; u < n; ++u) {
+    const int t = order[u];
+    if (u + 1 < n && dst[order[u + 1]] == dst[t]) continue;  // a later entry overwrites this destination
+    if (len && len < kSegMax && dst[t] == sd + (int64_t)len * S->es && src[t] == ss + (int64_t)len * S->es &&
+        (bool)neg[t] == sneg) {
+      ++len;
+      continue;
+    }
+    flush();
+    sd = dst[t];
+    ss = src[t];
+    sneg = neg[t];
+    len = 1;
   }
-  S->tab_n[g][phase] = n;
-  S->table_bytes += (int64_t)n * 24;
-  int rc;
-  if ((rc = dev_upload(d2, &S->tab_dst[g][phase], st)) || (rc = dev_upload(s2, &S->tab_src[g][phase], st)) ||
-      (rc = dev_upload(g2, &S->tab_sign[g][phase], st)))
-    return rc;
-  return MHD_OK;
+  flush();
+  S->tab_n[g][phase] = (int)(seg.size() / 2);
+  S->table_bytes += (int64_t)seg.size() * 8;
+  return dev_upload(seg, &S->tab_seg[g][phase], st);
 }
 
 int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
@@ -356,9 +411,7 @@ void free_solve(Solve *S, cudaStream_t st) {
   for (int r = 0; r < kNumRanges; ++r) f(S->dtile_prefix[r]);
   for (int g = 0; g < kMaxGroups; ++g)
     for (int p = 0; p < 2; ++p) {
-      f(S->tab_dst[g][p]);
-      f(S->tab_src[g][p]);
-      f(S->tab_sign[g][p]);
+      f(S->tab_seg[g][p]);
     }
   for (void *p : {(void *)S->al_off, (void *)S->al_memE, (void *)S->al_ownE, (void *)S->al_memJ, (void *)S->al_ownJ,
                   (void *)S->al_msign, (void *)S->al_osign})
@@ -441,12 +494,14 @@ int mhd_field_info(int field, int32_t *ncomp, int32_t *location) {
 }
 
 // ------------------------------------------------------------------ batch API
-int mhd_batch_create(int capacity, mhd_batch **out) {
+int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
   if (!out || capacity < 1 || capacity > 65536) return fail(MHD_ERR_ARG, "mhd_batch_create: capacity %d", capacity);
+  if (precision != kFP64 && precision != kMixed) return fail(MHD_ERR_ARG, "mhd_batch_create: precision %d", precision);
   *out = nullptr;
   auto *b = new (std::nothrow) mhd_batch();
   if (!b) return fail(MHD_ERR_OOM, "host allocation");
   b->capacity = capacity;
+  b->precision = precision;
   b->slots.assign(capacity, nullptr);
   auto bail = [&](int rc) {
     mhd_batch_destroy(b);
@@ -457,7 +512,7 @@ int mhd_batch_create(int capacity, mhd_batch **out) {
   const size_t C1 = (size_t)capacity + 1;
   if (cudaMalloc(&b->dsolves, sizeof(DevSolve) * capacity) != cudaSuccess ||
       cudaMalloc(&b->dstate, sizeof(SolveState) * capacity) != cudaSuccess ||
-      cudaMalloc(&b->comp_ptrs, sizeof(double *) * 72) != cudaSuccess ||
+      cudaMalloc(&b->comp_ptrs, sizeof(void *) * 72) != cudaSuccess ||
       cudaMallocHost(&b->hstate, sizeof(SolveState) * capacity) != cudaSuccess)
     return bail(fail(MHD_ERR_OOM, "directory of %d slots", capacity));
   for (int r = 0; r < kNumRanges; ++r)
@@ -506,7 +561,8 @@ int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
     const int n[3] = {desc->cells[3 * b], desc->cells[3 * b + 1], desc->cells[3 * b + 2]};
     if (n[0] < 2 || n[1] < 2 || n[2] < 2) return -1;
     const Box bx = make_box(n, desc->nghost);
-    bytes += (int64_t)(kNumComps + kNumUComps) * bx.total * (int64_t)sizeof(double);
+    const int64_t es = desc->precision == kMixed ? 4 : 8;
+    bytes += ((int64_t)kNumMetric * 8 + (int64_t)(kNumRComps + 2 * kNumUComps) * es) * bx.total;
   }
   for (int g = 0; g < MHD_NUM_GROUPS; ++g)
     bytes += (int64_t)(desc->groups[g].n_halo + desc->groups[g].n_owner) * 24;
@@ -519,7 +575,8 @@ int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
 int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   if (!b || !desc || !slot_out || desc->n_blocks < 1 || !desc->cells || desc->nghost < 1)
     return fail(MHD_ERR_ARG, "mhd_batch_add: bad descriptor");
-  if (desc->precision != 0) return fail(MHD_ERR_ARG, "precision %d not available", desc->precision);
+  if (desc->precision != b->precision)
+    return fail(MHD_ERR_ARG, "solve precision %d differs from the batch's (%d)", desc->precision, b->precision);
   if (desc->n_blocks >= (1 << 15)) return fail(MHD_ERR_ARG, "too many blocks (%d)", desc->n_blocks);
   int slot = -1;
   for (int s = 0; s < b->capacity; ++s)
@@ -537,6 +594,7 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   };
   S->nblocks = desc->n_blocks;
   S->nghost = desc->nghost;
+  S->es = b->precision == kMixed ? 4 : 8;
   int64_t u = 0, m = 0;
   std::vector<int> prefix[kNumRanges];
   for (int r = 0; r < kNumRanges; ++r) prefix[r].push_back(0);
@@ -548,14 +606,14 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
     S->boxes.push_back(bx);
     S->ubase.push_back(u);
     S->mbase.push_back(m);
-    u += (int64_t)kNumUComps * bx.total;
-    m += (int64_t)(kNumComps - kNumUComps) * bx.total;
+    u += (int64_t)kNumUComps * bx.total * S->es;
+    m += ((int64_t)kNumMetric * 8 + (int64_t)kNumRComps * S->es) * bx.total;
     for (int r = 0; r < kNumRanges; ++r)
       prefix[r].push_back(prefix[r].back() + tiles_of(range_of(r, n, desc->nghost), r));
   }
   S->ubuf = u;
   S->main_off = 2 * u;
-  S->arena_elems = 2 * u + m;
+  S->arena_bytes = 2 * u + m;
   const mhd_constants &k = desc->constants;
   S->consts = Consts{k.gamma,         k.M_H,       k.M_Na,        k.M_ref,
                      k.T_ref,         k.L_ref,     k.U_ref,       k.B_ref,
@@ -563,11 +621,11 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
                      k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
                      k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
                      k.inver_MA2,     k.ne_hall_floor, k.ambipolar, desc->nghost};
-  if (cudaMallocAsync((void **)&S->arena, sizeof(double) * S->arena_elems, st) != cudaSuccess) {
+  if (cudaMallocAsync((void **)&S->arena, S->arena_bytes, st) != cudaSuccess) {
     cudaGetLastError();
-    return bail(fail(MHD_ERR_OOM, "arena of %lld doubles", (long long)S->arena_elems));
+    return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
   }
-  if (cudaMemsetAsync(S->arena, 0, sizeof(double) * S->arena_elems, st) != cudaSuccess)
+  if (cudaMemsetAsync(S->arena, 0, S->arena_bytes, st) != cudaSuccess)
     return bail(fail(MHD_ERR_CUDA, "arena memset"));
   std::vector<DevBlock> blocks(S->nblocks);
   for (int bi = 0; bi < S->nblocks; ++bi) {
@@ -630,13 +688,14 @@ int mhd_batch_upload_field(mhd_batch *b, int slot, int field, int block, const d
   // be identical in both.
   const int c0 = kComp.first[field];
   const int ndst = c0 < kNumUComps ? 2 : 1;
-  double *ptrs[72];
+  void *ptrs[72];
   for (int d = 0; d < ndst; ++d)
     for (int m = 0; m < ncomp; ++m) ptrs[d * ncomp + m] = S->comp_ptr(block, c0 + m, d);
-  CUDA_TRY(cudaMemcpyAsync(b->comp_ptrs, ptrs, sizeof(double *) * ndst * ncomp, cudaMemcpyHostToDevice, b->stream));
+  CUDA_TRY(cudaMemcpyAsync(b->comp_ptrs, ptrs, sizeof(void *) * ndst * ncomp, cudaMemcpyHostToDevice, b->stream));
   const Box &bx = S->boxes[block];
   k_scatter_aos<<<(unsigned)((npts + 255) / 256), 256, 0, b->stream>>>(b->staging, lo[0], lo[1], lo[2], e[0], e[1], e[2],
-                                                                       ncomp, b->comp_ptrs, ndst, bx.si, bx.sj, bx.G);
+                                                                       ncomp, b->comp_ptrs, ndst, bx.si, bx.sj, bx.G,
+                                                                       S->comp_bytes(c0) == 4);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(b->stream));
   S->prepared = false;
@@ -655,12 +714,13 @@ int mhd_batch_download_field(mhd_batch *b, int slot, int field, int block, doubl
   const size_t npts = (size_t)e[0] * e[1] * e[2];
   if ((rc = ensure_staging(b, npts * ncomp))) return rc;
   const int c0 = kComp.first[field];
-  double *ptrs[36];
+  void *ptrs[36];
   for (int m = 0; m < ncomp; ++m) ptrs[m] = S->comp_ptr(block, c0 + m, cur);
-  CUDA_TRY(cudaMemcpyAsync(b->comp_ptrs, ptrs, sizeof(double *) * ncomp, cudaMemcpyHostToDevice, b->stream));
+  CUDA_TRY(cudaMemcpyAsync(b->comp_ptrs, ptrs, sizeof(void *) * ncomp, cudaMemcpyHostToDevice, b->stream));
   const Box &bx = S->boxes[block];
   k_gather_aos<<<(unsigned)((npts + 255) / 256), 256, 0, b->stream>>>(b->staging, lo[0], lo[1], lo[2], e[0], e[1], e[2],
-                                                                      ncomp, b->comp_ptrs, bx.si, bx.sj, bx.G);
+                                                                      ncomp, b->comp_ptrs, bx.si, bx.sj, bx.G,
+                                                                      S->comp_bytes(c0) == 4);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemcpyAsync(data, b->staging, sizeof(double) * npts * ncomp, cudaMemcpyDeviceToHost, b->stream));
   CUDA_TRY(cudaStreamSynchronize(b->stream));
@@ -688,7 +748,10 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   if ((rc = read_state(b))) return rc;
   s0.cur = b->hstate[slot].cur;
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return rc;
-  rc = targeted(b, slot, [&](int *nk) { enqueue_derived(b, 1, nk); });
+  rc = targeted(b, slot, [&](int *nk) {
+    launch(b, 1, SK_FACE_NORMALS, nk);
+    enqueue_derived(b, 1, nk);
+  });
   if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(b->stream));
   b->slots[slot]->prepared = true;
@@ -725,7 +788,7 @@ int mhd_batch_poll(mhd_batch *b, mhd_info *infos) {
     infos[s].status = st.status;
     infos[s].remaining = st.remaining;
     const Solve *S = b->slots[s];
-    infos[s].device_bytes = S ? (int64_t)(S->arena_elems * sizeof(double)) + S->table_bytes : 0;
+    infos[s].device_bytes = S ? S->arena_bytes + S->table_bytes : 0;
   }
   return MHD_OK;
 }
@@ -779,7 +842,7 @@ int mhd_batch_device_view(mhd_batch *b, int slot, int field, int block, int comp
     return fail(MHD_ERR_ARG, "mhd_device_view: bad arguments");
   if ((rc = read_state(b))) return rc;
   const Box &bx = S->boxes[block];
-  if (base) *base = S->comp_ptr(block, kComp.first[field] + comp, b->hstate[slot].cur);
+  if (base) *base = (double *)S->comp_ptr(block, kComp.first[field] + comp, b->hstate[slot].cur);
   if (G) *G = bx.G;
   if (si) *si = bx.si;
   if (sj) *sj = bx.sj;
@@ -793,7 +856,8 @@ int mhd_ctx_create(const mhd_desc *desc, mhd_ctx **out) {
   if (!desc || !out) return fail(MHD_ERR_ARG, "mhd_ctx_create: bad descriptor");
   auto *ctx = new (std::nothrow) mhd_ctx();
   if (!ctx) return fail(MHD_ERR_OOM, "host allocation");
-  int rc = mhd_batch_create(1, &ctx->batch);
+  const int prec = desc->precision == kMixed ? kMixed : kFP64;
+  int rc = mhd_batch_create(1, prec, &ctx->batch);
   if (rc) {
     delete ctx;
     return rc;

@@ -27,10 +27,25 @@ enum RangeKind : int {
 
 constexpr int kTileK = 32, kTileJ = 4, kTileI = 2, kTileThreads = kTileK * kTileJ * kTileI;
 
-// Per-block descriptor (device).
+// Precision of a batch: every component array holds `real` values (double
+// or float) except the metric (Jac and the face area vectors JD), which is
+// always double.  In the FP64 path real = double throughout.
+enum Precision : int { kFP64 = 0, kMixed = 1 };
+constexpr int kMetricFirst = kComp.first[MHD_JAC];  // JAC, JDXI, JDET, JDZE are consecutive
+constexpr int kNumMetric = kComp.first[MHD_JDZE] + 3 - kMetricFirst;
+constexpr int kNumRComps = kNumComps - kNumUComps - kNumMetric;  // real-valued comps outside U
+static_assert(kNumMetric == 10, "metric components");
+__host__ __device__ constexpr bool is_metric(int comp) { return comp >= kMetricFirst && comp < kMetricFirst + kNumMetric; }
+// Index of a non-U, non-metric component among the real-valued M arrays.
+__host__ __device__ constexpr int rslot(int comp) {
+  return comp - kNumUComps - (comp >= kMetricFirst + kNumMetric ? kNumMetric : 0);
+}
+
+// Per-block descriptor (device).  Block memory: U buffers of 10 real arrays
+// each; M = [10 metric double arrays | kNumRComps real arrays].
 struct DevBlock {
-  double *U[2];       // U_H, U_Na components (10) of buffer 0 / 1
-  double *M;          // all other components (kNumComps - 10)
+  void *U[2];         // U_H, U_Na components (10) of buffer 0 / 1
+  char *M;
   int64_t total, si, sj;
   int G, n[3];
   int solve;          // index of the owning solve in the directory
@@ -38,13 +53,23 @@ struct DevBlock {
 
 // Per-solve constants, as calc_physical_constant derives them
 // (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:3-48).
-struct Consts {
-  double gamma, M_H, M_Na, M_ref, T_ref, L_ref, U_ref, B_ref, n_ref, rho_ref, m_Na, k_Boltz, q_e, mu0;
-  double state_coeff_H, state_coeff_Na, CFL, hall_coef, momentum_induce_coeff, momentum_hall_coeff;
-  double inver_MA2, ne_hall_floor;
+template <class T>
+struct ConstsT {
+  T gamma, M_H, M_Na, M_ref, T_ref, L_ref, U_ref, B_ref, n_ref, rho_ref, m_Na, k_Boltz, q_e, mu0;
+  T state_coeff_H, state_coeff_Na, CFL, hall_coef, momentum_induce_coeff, momentum_hall_coeff;
+  T inver_MA2, ne_hall_floor;
   int ambipolar;
   int nghost;
 };
+using Consts = ConstsT<double>;
+inline ConstsT<float> to_float(const Consts &c) {
+  return ConstsT<float>{(float)c.gamma, (float)c.M_H, (float)c.M_Na, (float)c.M_ref, (float)c.T_ref,
+                        (float)c.L_ref, (float)c.U_ref, (float)c.B_ref, (float)c.n_ref, (float)c.rho_ref,
+                        (float)c.m_Na, (float)c.k_Boltz, (float)c.q_e, (float)c.mu0, (float)c.state_coeff_H,
+                        (float)c.state_coeff_Na, (float)c.CFL, (float)c.hall_coef, (float)c.momentum_induce_coeff,
+                        (float)c.momentum_hall_coeff, (float)c.inver_MA2, (float)c.ne_hall_floor, c.ambipolar,
+                        c.nghost};
+}
 
 // Per-solve device state.
 struct SolveState {
@@ -58,20 +83,30 @@ struct SolveState {
   int pad_;
 };
 
-// A flattened copy/alias table of one solve: entries encode (block, comp, cell
-// offset) as  block << 48 | comp << 40 | offset  (block local to the solve).
+// Sync tables of one solve address DOFs by "codes": the byte offset from the
+// solve's arena base (bits 0..55); bit 60 marks a U component, whose offset
+// is taken in U buffer 0 and shifted by cur * ubuf bytes at run time.  All
+// synced components are real-valued.
+constexpr int64_t kCodeOffMask = (int64_t(1) << 56) - 1;
+constexpr int64_t kCodeUFlag = int64_t(1) << 60;
+// Copy segments: `len` (1..8) consecutive destinations dst.. <- sign * src..
+// (consecutive sources), stored as two int64: dst code with (len - 1) in bits
+// 56..58 and a negative sign in bit 59, and the src code.
+constexpr int kSegMax = 8;
+constexpr int kSegLenShift = 56, kSegNegBit = 59;
 struct DevTable {
-  const int64_t *dst = nullptr, *src = nullptr;
-  const double *sign = nullptr;
-  int n = 0;
+  const int64_t *seg = nullptr;  // 2 * n
+  int n = 0;                     // segments
 };
+// Edge alias classes: members member[offset[c] .. offset[c+1]) (codes and
+// signs), written to owner[c]; processed 8 classes per lane group.
 struct DevAlias {
   const int32_t *offset = nullptr;  // n + 1
-  const int64_t *member = nullptr;  // encoded E members
+  const int64_t *member = nullptr;
   const double *msign = nullptr;
-  const int64_t *owner = nullptr;   // encoded E owners
+  const int64_t *owner = nullptr;
   const double *osign = nullptr;
-  int n = 0;
+  int n = 0;                        // classes
 };
 
 constexpr int kMaxGroups = MHD_NUM_GROUPS;
@@ -79,7 +114,10 @@ constexpr int kMaxGroups = MHD_NUM_GROUPS;
 // Directory entry of one solve (device).
 struct DevSolve {
   Consts c;
-  const DevBlock *blocks;             // this solve's blocks (global array slice)
+  ConstsT<float> cf;                  // the same, rounded (mixed precision)
+  const DevBlock *blocks;             // this solve's blocks
+  char *arena;                        // base of the sync codes
+  int64_t ubuf;                       // bytes per U buffer
   int nblocks;
   const int *tile_prefix[kNumRanges]; // per range: nblocks + 1 prefix sums of tile counts
   DevTable halo[kMaxGroups], owner[kMaxGroups];
@@ -93,10 +131,18 @@ struct Dir {
   int nsolves;
   int mode;  // 0: solves with remaining steps (the step); 1: solves with mask set (prepare, sync)
   const int *solve_tile_prefix[kNumRanges];  // nsolves + 1 per range
-  // sync tables: per group and phase (0 halo, 1 owner) prefix sums of entry counts over solves
+  // sync tables: per group and phase (0 halo, 1 owner) prefix sums over the
+  // solves of their segment counts; alias tables: of their 8-class groups
   const int *copy_prefix[kMaxGroups][2];
   const int *aliasE_prefix, *aliasJ_prefix;
 };
+
+template <class R>
+__device__ __forceinline__ const ConstsT<R> &consts_of(const DevSolve &S);
+template <>
+__device__ __forceinline__ const ConstsT<double> &consts_of<double>(const DevSolve &S) { return S.c; }
+template <>
+__device__ __forceinline__ const ConstsT<float> &consts_of<float>(const DevSolve &S) { return S.cf; }
 
 __host__ __device__ inline bool solve_active(const Dir &D, int s) {
   return D.mode ? D.state[s].mask != 0 : D.state[s].remaining != 0;

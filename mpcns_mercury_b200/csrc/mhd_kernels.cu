@@ -34,6 +34,7 @@ constexpr int cEX = kComp.first[MHD_E_XI], cEY = kComp.first[MHD_E_ETA], cEZ = k
 constexpr int cHX = kComp.first[MHD_EHALL_XI], cHY = kComp.first[MHD_EHALL_ETA], cHZ = kComp.first[MHD_EHALL_ZETA];
 constexpr int cEFX = kComp.first[MHD_EFACE_XI], cEFY = kComp.first[MHD_EFACE_ETA], cEFZ = kComp.first[MHD_EFACE_ZETA];
 constexpr int cEHC = kComp.first[MHD_EHC], cHB = kComp.first[MHD_HALL_BETA], cUC = kComp.first[MHD_UCON];
+constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA], cFNZ = kComp.first[MHD_FNORM_ZETA];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
 constexpr int cAX = kComp.first[MHD_AREA_XI], cAY = kComp.first[MHD_AREA_ETA], cAZ = kComp.first[MHD_AREA_ZETA];
@@ -50,34 +51,47 @@ constexpr int cPHOTO = kComp.first[MHD_PHOTO], cCX = kComp.first[MHD_CELL_X], cC
 constexpr int cTPX = kComp.first[MHD_TAPER_XI], cTPY = kComp.first[MHD_TAPER_ETA], cTPZ = kComp.first[MHD_TAPER_ZETA];
 
 // std::max / std::min semantics (first argument wins ties, incl. signed zeros).
-__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
-__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+template <class R>
+__device__ __forceinline__ R dmax(R a, R b) { return (a < b) ? b : a; }
+template <class R>
+__device__ __forceinline__ R dmin(R a, R b) { return (b < a) ? b : a; }
 
-// One block's fields for the current step: U = current buffer.
+// One block's fields for the current step: U = current buffer, M = metric
+// (double) then the other real-valued components (mhd_engine.cuh).
+template <class R>
 struct V {
-  double *U, *Un, *M;
+  R *U, *Un;
+  char *M;
   int64_t total, si, sj;
   int G, n0, n1, n2;
-  __device__ __forceinline__ double *c(int comp) const {
-    return comp < kNumUComps ? U + (int64_t)comp * total : M + (int64_t)(comp - kNumUComps) * total;
+  // real-valued component (U or M)
+  __device__ __forceinline__ R *c(int comp) const {
+    return comp < kNumUComps ? U + (int64_t)comp * total
+                             : (R *)(M + (int64_t)kNumMetric * total * 8) + (int64_t)rslot(comp) * total;
   }
+  // metric component (JAC, JD*), double in every precision
+  __device__ __forceinline__ double *m(int comp) const { return (double *)M + (int64_t)(comp - kMetricFirst) * total; }
   __device__ __forceinline__ int64_t off(int i, int j, int k) const {
     return (int64_t)(i + G) * si + (int64_t)(j + G) * sj + (k + G);
   }
 };
 #define AT(cc, i, j, k) (B.c(cc)[B.off((i), (j), (k))])
+#define ATM(cc, i, j, k) (B.m(cc)[B.off((i), (j), (k))])
 
 struct Item {
   int s;       // solve
   int species; // kCells2 only
   int i, j, k;
   bool in;     // inside the kernel's range
+  int o[3];    // tile origin (i, j, k)
+  int hi[3];   // range upper bounds (exclusive)
+  int lo[3];   // range lower bounds
 };
 
 // Work-item loop: for every tile of range `KIND` of every active solve, call
 // f(S, B, item).  Tile lookup: two binary searches by thread 0, broadcast
 // through shared memory.
-template <int KIND, class F>
+template <class R, int KIND, class F>
 __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
   __shared__ int sh[3];
   const int total = D.solve_tile_prefix[KIND][D.nsolves];
@@ -120,14 +134,21 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
     const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
     const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
     const int bk = t % tk, bj = (t / tk) % tj, bi = t / (tk * tj);
-    it.k = r.lo[2] + bk * kTileK + (tid % kTileK);
-    it.j = r.lo[1] + bj * kTileJ + ((tid / kTileK) % kTileJ);
-    it.i = r.lo[0] + bi * kTileI + (tid / (kTileK * kTileJ));
+    it.o[0] = r.lo[0] + bi * kTileI;
+    it.o[1] = r.lo[1] + bj * kTileJ;
+    it.o[2] = r.lo[2] + bk * kTileK;
+    for (int a = 0; a < 3; ++a) {
+      it.hi[a] = r.hi[a];
+      it.lo[a] = r.lo[a];
+    }
+    it.k = it.o[2] + (tid % kTileK);
+    it.j = it.o[1] + ((tid / kTileK) % kTileJ);
+    it.i = it.o[0] + (tid / (kTileK * kTileJ));
     it.in = it.i < r.hi[0] && it.j < r.hi[1] && it.k < r.hi[2];
-    V B;
+    V<R> B;
     const int cur = D.state[s].cur;
-    B.U = DB.U[cur];
-    B.Un = DB.U[cur ^ 1];
+    B.U = (R *)DB.U[cur];
+    B.Un = (R *)DB.U[cur ^ 1];
     B.M = DB.M;
     B.total = DB.total;
     B.si = DB.si;
@@ -140,24 +161,26 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
   }
 }
 
+template <class R>
 struct Num {
-  double nH, nNa, ne_eff, chiH, chiNa, wH, wNa;
+  R nH, nNa, ne_eff, chiH, chiNa, wH, wNa;
 };
 
 // Hall_Num_Limiter (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:111-157)
-__device__ __forceinline__ Num num_limiter(const Consts &c, double rhoH, double rhoNa) {
-  Num d;
-  const double rH = dmax(rhoH, 0.0), rN = dmax(rhoNa, 0.0);
+template <class R>
+__device__ __forceinline__ Num<R> num_limiter(const ConstsT<R> &c, R rhoH, R rhoNa) {
+  Num<R> d;
+  const R rH = dmax(rhoH, R(0.0)), rN = dmax(rhoNa, R(0.0));
   d.nH = rH / c.M_H * c.M_ref;
   d.nNa = rN / c.M_Na * c.M_ref;
-  const double ne_true = d.nH + d.nNa;
+  const R ne_true = d.nH + d.nNa;
   d.ne_eff = sqrt(ne_true * ne_true + c.ne_hall_floor * c.ne_hall_floor);
-  if (ne_true > 1.0e-300) {
+  if ((double)ne_true > 1.0e-300) {
     d.chiH = d.nH / ne_true;
     d.chiNa = d.nNa / ne_true;
   } else {
-    d.chiH = 1.0;
-    d.chiNa = 0.0;
+    d.chiH = R(1.0);
+    d.chiNa = R(0.0);
   }
   d.wH = d.nH / d.ne_eff;
   d.wNa = d.nNa / d.ne_eff;
@@ -173,37 +196,43 @@ __device__ __forceinline__ void shift1(int axis, int &i, int &j, int &k, int s) 
 // ------------------------------------------------------------------ ideal EMF
 __device__ __forceinline__ int bcomp(int axis) { return axis == 0 ? cBX : axis == 1 ? cBY : cBZ; }
 __device__ __forceinline__ int bacomp(int axis) { return axis == 0 ? cBAX : axis == 1 ? cBAY : cBAZ; }
-__device__ __forceinline__ double face_tot(const V &B, int axis, int i, int j, int k) {
+template <class R>
+__device__ __forceinline__ R face_tot(const V<R> &B, int axis, int i, int j, int k) {
   return AT(bcomp(axis), i, j, k) + AT(bacomp(axis), i, j, k);
 }
-__device__ __forceinline__ double cell_beta_ind(const V &B, int axis, int i, int j, int k) {
+template <class R>
+__device__ __forceinline__ R cell_beta_ind(const V<R> &B, int axis, int i, int j, int k) {
   int ip = i, jp = j, kp = k;
   shift1(axis, ip, jp, kp, 1);
-  return 0.5 * (AT(bcomp(axis), i, j, k) + AT(bcomp(axis), ip, jp, kp));
+  return R(0.5) * (AT(bcomp(axis), i, j, k) + AT(bcomp(axis), ip, jp, kp));
 }
-__device__ __forceinline__ double cell_beta_tot(const V &B, int axis, int i, int j, int k) {
+template <class R>
+__device__ __forceinline__ R cell_beta_tot(const V<R> &B, int axis, int i, int j, int k) {
   int ip = i, jp = j, kp = k;
   shift1(axis, ip, jp, kp, 1);
-  return 0.5 * (face_tot(B, axis, i, j, k) + face_tot(B, axis, ip, jp, kp));
+  return R(0.5) * (face_tot(B, axis, i, j, k) + face_tot(B, axis, ip, jp, kp));
 }
-__device__ __forceinline__ double ucon(const V &B, int axis, int i, int j, int k) { return AT(cUC + axis, i, j, k); }
+template <class R>
+__device__ __forceinline__ R ucon(const V<R> &B, int axis, int i, int j, int k) { return AT(cUC + axis, i, j, k); }
 
 // flux() of AssembleOneDirectionEMF_ (Ideal.cpp:517-536)
-__device__ __forceinline__ double emf_flux(const V &B, int ba, int fa, int iL, int jL, int kL, int iR, int jR, int kR,
-                                           double bff) {
-  const double btL = cell_beta_tot(B, ba, iL, jL, kL), btR = cell_beta_tot(B, ba, iR, jR, kR);
-  const double biL = cell_beta_ind(B, ba, iL, jL, kL), biR = cell_beta_ind(B, ba, iR, jR, kR);
-  const double ufL = ucon(B, fa, iL, jL, kL), ufR = ucon(B, fa, iR, jR, kR);
-  const double ubL = ucon(B, ba, iL, jL, kL), ubR = ucon(B, ba, iR, jR, kR);
-  const double GL = ufL * btL - ubL * bff, GR = ufR * btR - ubR * bff;
-  const double r = dmax(fabs(ufL), fabs(ufR));
-  return 0.5 * (GL + GR) - 0.5 * r * (biR - biL);
+template <class R>
+__device__ __forceinline__ R emf_flux(const V<R> &B, int ba, int fa, int iL, int jL, int kL, int iR, int jR, int kR,
+                                           R bff) {
+  const R btL = cell_beta_tot(B, ba, iL, jL, kL), btR = cell_beta_tot(B, ba, iR, jR, kR);
+  const R biL = cell_beta_ind(B, ba, iL, jL, kL), biR = cell_beta_ind(B, ba, iR, jR, kR);
+  const R ufL = ucon(B, fa, iL, jL, kL), ufR = ucon(B, fa, iR, jR, kR);
+  const R ubL = ucon(B, ba, iL, jL, kL), ubR = ucon(B, ba, iR, jR, kR);
+  const R GL = ufL * btL - ubL * bff, GR = ufR * btR - ubR * bff;
+  const R r = dmax(fabs(ufL), fabs(ufR));
+  return R(0.5) * (GL + GR) - R(0.5) * r * (biR - biL);
 }
 
 // AssembleOneDirectionEMF_ (Ideal.cpp:433-594) for all three face families on
 // [-1, inner_hi + 1) (the one locally evaluated ghost layer, Ideal.cpp:548-555).
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
-  for_items<kExt>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kExt>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
     const int q[3] = {i, j, k}, n[3] = {B.n0, B.n1, B.n2};
@@ -214,21 +243,21 @@ __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
       if (!in) continue;
       int iL = i, jL = j, kL = k;
       shift1(fa, iL, jL, kL, -1);
-      const double bff = face_tot(B, fa, i, j, k);
-      double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+      const R bff = face_tot(B, fa, i, j, k);
+      R e0 = R(0.0), e1 = R(0.0), e2 = R(0.0);
       if (fa == 0) {
-        const double Ge = emf_flux(B, 1, 0, iL, jL, kL, i, j, k, bff);
-        const double Gz = emf_flux(B, 2, 0, iL, jL, kL, i, j, k, bff);
+        const R Ge = emf_flux(B, 1, 0, iL, jL, kL, i, j, k, bff);
+        const R Gz = emf_flux(B, 2, 0, iL, jL, kL, i, j, k, bff);
         e1 = Gz;
         e2 = -Ge;
       } else if (fa == 1) {
-        const double Gx = emf_flux(B, 0, 1, iL, jL, kL, i, j, k, bff);
-        const double Gz = emf_flux(B, 2, 1, iL, jL, kL, i, j, k, bff);
+        const R Gx = emf_flux(B, 0, 1, iL, jL, kL, i, j, k, bff);
+        const R Gz = emf_flux(B, 2, 1, iL, jL, kL, i, j, k, bff);
         e0 = -Gz;
         e2 = Gx;
       } else {
-        const double Gx = emf_flux(B, 0, 2, iL, jL, kL, i, j, k, bff);
-        const double Ge = emf_flux(B, 1, 2, iL, jL, kL, i, j, k, bff);
+        const R Gx = emf_flux(B, 0, 2, iL, jL, kL, i, j, k, bff);
+        const R Ge = emf_flux(B, 1, 2, iL, jL, kL, i, j, k, bff);
         e0 = Ge;
         e1 = -Gx;
       }
@@ -241,89 +270,92 @@ __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
   });
 }
 
-__device__ __forceinline__ double max_abs_u4(const V &B, int axis, int i0, int j0, int k0, int i1, int j1, int k1,
+template <class R>
+__device__ __forceinline__ R max_abs_u4(const V<R> &B, int axis, int i0, int j0, int k0, int i1, int j1, int k1,
                                              int i2, int j2, int k2, int i3, int j3, int k3) {
-  double a = 0.0;
+  R a = R(0.0);
   a = dmax(a, fabs(ucon(B, axis, i0, j0, k0)));
   a = dmax(a, fabs(ucon(B, axis, i1, j1, k1)));
   a = dmax(a, fabs(ucon(B, axis, i2, j2, k2)));
   a = dmax(a, fabs(ucon(B, axis, i3, j3, k3)));
   return a;
 }
-__device__ __forceinline__ double pe_node(const V &B, int i, int j, int k) {
-  double sum = 0.0;
+template <class R>
+__device__ __forceinline__ R pe_node(const V<R> &B, int i, int j, int k) {
+  R sum = R(0.0);
   for (int di = -1; di <= 0; ++di)
     for (int dj = -1; dj <= 0; ++dj)
       for (int dk = -1; dk <= 0; ++dk)
         sum += AT(cPVH + 3, i + di, j + dj, k + dk) + AT(cPVN + 3, i + di, j + dj, k + dk);
-  return 0.125 * sum;
+  return R(0.125) * sum;
 }
 
 // AssembleEdgeEMF_FromFaceE_Ideal_ (Ideal.cpp:138-372) + AddAmbipolarEdgeEMF_
 // (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Ambipo.cpp:3-143) on the owned edges.
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
-  for_items<kBox>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const Consts &c = S.c;
+    const ConstsT<R> &c = consts_of<R>(S);
     const int i = it.i, j = it.j, k = it.k;
-    const double Cuct = 0.5;
-    const double pc = (c.rho_ref * c.U_ref) / (c.q_e * c.L_ref * c.B_ref * c.n_ref);
+    const R Cuct = R(0.5);
+    const R pc = (c.rho_ref * c.U_ref) / (c.q_e * c.L_ref * c.B_ref * c.n_ref);
     if (i < B.n0) {
-      const double Ec = 0.25 * (AT(cEFY, i, j, k) + AT(cEFY, i, j, k - 1) + AT(cEFZ, i, j, k) + AT(cEFZ, i, j - 1, k));
-      const double ae = max_abs_u4(B, 1, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
-      const double az = max_abs_u4(B, 2, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
-      const double d1 = AT(cBZ, i, j, k) - AT(cBZ, i, j - 1, k);
-      const double d2 = AT(cBY, i, j, k) - AT(cBY, i, j, k - 1);
-      double e = Ec + Cuct * (0.5 * ae * d1 - 0.5 * az * d2);
+      const R Ec = R(0.25) * (AT(cEFY, i, j, k) + AT(cEFY, i, j, k - 1) + AT(cEFZ, i, j, k) + AT(cEFZ, i, j - 1, k));
+      const R ae = max_abs_u4(B, 1, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
+      const R az = max_abs_u4(B, 2, i, j, k, i, j - 1, k, i, j, k - 1, i, j - 1, k - 1);
+      const R d1 = AT(cBZ, i, j, k) - AT(cBZ, i, j - 1, k);
+      const R d2 = AT(cBY, i, j, k) - AT(cBY, i, j, k - 1);
+      R e = Ec + Cuct * (R(0.5) * ae * d1 - R(0.5) * az * d2);
       if (c.ambipolar) {
-        const double p0 = pe_node(B, i, j, k), p1 = pe_node(B, i + 1, j, k);
-        double rH = 0.0, rN = 0.0;
+        const R p0 = pe_node(B, i, j, k), p1 = pe_node(B, i + 1, j, k);
+        R rH = R(0.0), rN = R(0.0);
         for (int dj = -1; dj <= 0; ++dj)
           for (int dk = -1; dk <= 0; ++dk) {
             rH += AT(cUH, i, j + dj, k + dk);
             rN += AT(cUN, i, j + dj, k + dk);
           }
-        e -= pc * (p1 - p0) / num_limiter(c, 0.25 * rH, 0.25 * rN).ne_eff;
+        e -= pc * (p1 - p0) / num_limiter(c, R(0.25) * rH, R(0.25) * rN).ne_eff;
       }
       AT(cEX, i, j, k) = e;
     }
     if (j < B.n1) {
-      const double Ec = 0.25 * (AT(cEFX + 1, i, j, k) + AT(cEFX + 1, i, j, k - 1) + AT(cEFZ + 1, i, j, k) +
+      const R Ec = R(0.25) * (AT(cEFX + 1, i, j, k) + AT(cEFX + 1, i, j, k - 1) + AT(cEFZ + 1, i, j, k) +
                                 AT(cEFZ + 1, i - 1, j, k));
-      const double az = max_abs_u4(B, 2, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
-      const double ax = max_abs_u4(B, 0, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
-      const double d1 = AT(cBX, i, j, k) - AT(cBX, i, j, k - 1);
-      const double d2 = AT(cBZ, i, j, k) - AT(cBZ, i - 1, j, k);
-      double e = Ec + Cuct * (0.5 * az * d1 - 0.5 * ax * d2);
+      const R az = max_abs_u4(B, 2, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
+      const R ax = max_abs_u4(B, 0, i, j, k, i - 1, j, k, i, j, k - 1, i - 1, j, k - 1);
+      const R d1 = AT(cBX, i, j, k) - AT(cBX, i, j, k - 1);
+      const R d2 = AT(cBZ, i, j, k) - AT(cBZ, i - 1, j, k);
+      R e = Ec + Cuct * (R(0.5) * az * d1 - R(0.5) * ax * d2);
       if (c.ambipolar) {
-        const double p0 = pe_node(B, i, j, k), p1 = pe_node(B, i, j + 1, k);
-        double rH = 0.0, rN = 0.0;
+        const R p0 = pe_node(B, i, j, k), p1 = pe_node(B, i, j + 1, k);
+        R rH = R(0.0), rN = R(0.0);
         for (int di = -1; di <= 0; ++di)
           for (int dk = -1; dk <= 0; ++dk) {
             rH += AT(cUH, i + di, j, k + dk);
             rN += AT(cUN, i + di, j, k + dk);
           }
-        e -= pc * (p1 - p0) / num_limiter(c, 0.25 * rH, 0.25 * rN).ne_eff;
+        e -= pc * (p1 - p0) / num_limiter(c, R(0.25) * rH, R(0.25) * rN).ne_eff;
       }
       AT(cEY, i, j, k) = e;
     }
     if (k < B.n2) {
-      const double Ec = 0.25 * (AT(cEFX + 2, i, j, k) + AT(cEFX + 2, i, j - 1, k) + AT(cEFY + 2, i, j, k) +
+      const R Ec = R(0.25) * (AT(cEFX + 2, i, j, k) + AT(cEFX + 2, i, j - 1, k) + AT(cEFY + 2, i, j, k) +
                                 AT(cEFY + 2, i - 1, j, k));
-      const double ax = max_abs_u4(B, 0, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
-      const double ae = max_abs_u4(B, 1, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
-      const double d1 = AT(cBY, i, j, k) - AT(cBY, i - 1, j, k);
-      const double d2 = AT(cBX, i, j, k) - AT(cBX, i, j - 1, k);
-      double e = Ec + Cuct * (0.5 * ax * d1 - 0.5 * ae * d2);
+      const R ax = max_abs_u4(B, 0, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
+      const R ae = max_abs_u4(B, 1, i, j, k, i - 1, j, k, i, j - 1, k, i - 1, j - 1, k);
+      const R d1 = AT(cBY, i, j, k) - AT(cBY, i - 1, j, k);
+      const R d2 = AT(cBX, i, j, k) - AT(cBX, i, j - 1, k);
+      R e = Ec + Cuct * (R(0.5) * ax * d1 - R(0.5) * ae * d2);
       if (c.ambipolar) {
-        const double p0 = pe_node(B, i, j, k), p1 = pe_node(B, i, j, k + 1);
-        double rH = 0.0, rN = 0.0;
+        const R p0 = pe_node(B, i, j, k), p1 = pe_node(B, i, j, k + 1);
+        R rH = R(0.0), rN = R(0.0);
         for (int di = -1; di <= 0; ++di)
           for (int dj = -1; dj <= 0; ++dj) {
             rH += AT(cUH, i + di, j + dj, k);
             rN += AT(cUN, i + di, j + dj, k);
           }
-        e -= pc * (p1 - p0) / num_limiter(c, 0.25 * rH, 0.25 * rN).ne_eff;
+        e -= pc * (p1 - p0) / num_limiter(c, R(0.25) * rH, R(0.25) * rN).ne_eff;
       }
       AT(cEZ, i, j, k) = e;
     }
@@ -332,15 +364,16 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
 
 // ------------------------------------------------------------------ Hall EMF
 // BuildHallFaceEMF_Rusanov_diff_ step 1 (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:110-146).
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_hall_cell(Dir D) {
-  for_items<kAlloc>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
     const int64_t o = B.off(i, j, k);
-    const Num d = num_limiter(S.c, B.c(cUH)[o], B.c(cUN)[o]);
-    const double alpha = S.c.hall_coef / d.ne_eff;
-    const double Jx = B.c(cJC)[o], Jy = B.c(cJC + 1)[o], Jz = B.c(cJC + 2)[o];
-    const double Bx = B.c(cBC)[o], By = B.c(cBC + 1)[o], Bz = B.c(cBC + 2)[o];
+    const Num<R> d = num_limiter(consts_of<R>(S), B.c(cUH)[o], B.c(cUN)[o]);
+    const R alpha = consts_of<R>(S).hall_coef / d.ne_eff;
+    const R Jx = B.c(cJC)[o], Jy = B.c(cJC + 1)[o], Jz = B.c(cJC + 2)[o];
+    const R Bx = B.c(cBC)[o], By = B.c(cBC + 1)[o], Bz = B.c(cBC + 2)[o];
     B.c(cEHC)[o] = alpha * (Jy * Bz - Jz * By);
     B.c(cEHC + 1)[o] = alpha * (Jz * Bx - Jx * Bz);
     B.c(cEHC + 2)[o] = alpha * (Jx * By - Jy * Bx);
@@ -349,74 +382,76 @@ __global__ void __launch_bounds__(kTileThreads) k_hall_cell(Dir D) {
 }
 
 // BuildHallFaceEMF_Rusanov_diff_ steps 2-4 (Hall.cpp:148-400).
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_hall_edge(Dir D) {
-  for_items<kBox>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
-    const double eps = 1e-14, Cwh = 0.1;
+    const R eps = R(1e-14), Cwh = R(0.1);
     if (i < B.n0) {
-      double Ec[3];
+      R Ec[3];
       for (int q = 0; q < 3; ++q)
-        Ec[q] = 0.25 * (AT(cEHC + q, i, j - 1, k - 1) + AT(cEHC + q, i, j - 1, k) + AT(cEHC + q, i, j, k - 1) +
+        Ec[q] = R(0.25) * (AT(cEHC + q, i, j - 1, k - 1) + AT(cEHC + q, i, j - 1, k) + AT(cEHC + q, i, j, k - 1) +
                         AT(cEHC + q, i, j, k));
-      const double Ecen = Ec[0] * AT(cDRX, i, j, k) + Ec[1] * AT(cDRX + 1, i, j, k) + Ec[2] * AT(cDRX + 2, i, j, k);
-      const double be =
+      const R Ecen = Ec[0] * AT(cDRX, i, j, k) + Ec[1] * AT(cDRX + 1, i, j, k) + Ec[2] * AT(cDRX + 2, i, j, k);
+      const R be =
           dmax(dmax(AT(cHB, i, j - 1, k - 1), AT(cHB, i, j - 1, k)), dmax(AT(cHB, i, j, k - 1), AT(cHB, i, j, k)));
-      const double L = dmax(AT(cDLX, i, j, k), eps);
-      const double Abz = 0.5 * (AT(cAZ, i, j, k) + AT(cAZ, i, j - 1, k));
-      const double ihe = L / dmax(Abz, eps);
-      const double mue = Cwh * be * ihe * ihe;
-      const double Abe = 0.5 * (AT(cAY, i, j, k) + AT(cAY, i, j, k - 1));
-      const double ihz = L / dmax(Abe, eps);
-      const double muz = Cwh * be * ihz * ihz;
-      const double d1 = AT(cBZ, i, j, k) - AT(cBZ, i, j - 1, k);
-      const double d2 = AT(cBY, i, j, k) - AT(cBY, i, j, k - 1);
-      AT(cHX, i, j, k) = AT(cTPX, i, j, k) * (Ecen + 0.5 * mue * d1 - 0.5 * muz * d2);
+      const R L = dmax(AT(cDLX, i, j, k), eps);
+      const R Abz = R(0.5) * (AT(cAZ, i, j, k) + AT(cAZ, i, j - 1, k));
+      const R ihe = L / dmax(Abz, eps);
+      const R mue = Cwh * be * ihe * ihe;
+      const R Abe = R(0.5) * (AT(cAY, i, j, k) + AT(cAY, i, j, k - 1));
+      const R ihz = L / dmax(Abe, eps);
+      const R muz = Cwh * be * ihz * ihz;
+      const R d1 = AT(cBZ, i, j, k) - AT(cBZ, i, j - 1, k);
+      const R d2 = AT(cBY, i, j, k) - AT(cBY, i, j, k - 1);
+      AT(cHX, i, j, k) = AT(cTPX, i, j, k) * (Ecen + R(0.5) * mue * d1 - R(0.5) * muz * d2);
     }
     if (j < B.n1) {
-      double Ec[3];
+      R Ec[3];
       for (int q = 0; q < 3; ++q)
-        Ec[q] = 0.25 * (AT(cEHC + q, i - 1, j, k - 1) + AT(cEHC + q, i - 1, j, k) + AT(cEHC + q, i, j, k - 1) +
+        Ec[q] = R(0.25) * (AT(cEHC + q, i - 1, j, k - 1) + AT(cEHC + q, i - 1, j, k) + AT(cEHC + q, i, j, k - 1) +
                         AT(cEHC + q, i, j, k));
-      const double Ecen = Ec[0] * AT(cDRY, i, j, k) + Ec[1] * AT(cDRY + 1, i, j, k) + Ec[2] * AT(cDRY + 2, i, j, k);
-      const double be =
+      const R Ecen = Ec[0] * AT(cDRY, i, j, k) + Ec[1] * AT(cDRY + 1, i, j, k) + Ec[2] * AT(cDRY + 2, i, j, k);
+      const R be =
           dmax(dmax(AT(cHB, i - 1, j, k - 1), AT(cHB, i - 1, j, k)), dmax(AT(cHB, i, j, k - 1), AT(cHB, i, j, k)));
-      const double L = dmax(AT(cDLY, i, j, k), eps);
-      const double Abx = 0.5 * (AT(cAX, i, j, k) + AT(cAX, i, j, k - 1));
-      const double ihz = L / dmax(Abx, eps);
-      const double muz = Cwh * be * ihz * ihz;
-      const double Abz = 0.5 * (AT(cAZ, i, j, k) + AT(cAZ, i - 1, j, k));
-      const double ihx = L / dmax(Abz, eps);
-      const double mux = Cwh * be * ihx * ihx;
-      const double d1 = AT(cBX, i, j, k) - AT(cBX, i, j, k - 1);
-      const double d2 = AT(cBZ, i, j, k) - AT(cBZ, i - 1, j, k);
-      AT(cHY, i, j, k) = AT(cTPY, i, j, k) * (Ecen + 0.5 * muz * d1 - 0.5 * mux * d2);
+      const R L = dmax(AT(cDLY, i, j, k), eps);
+      const R Abx = R(0.5) * (AT(cAX, i, j, k) + AT(cAX, i, j, k - 1));
+      const R ihz = L / dmax(Abx, eps);
+      const R muz = Cwh * be * ihz * ihz;
+      const R Abz = R(0.5) * (AT(cAZ, i, j, k) + AT(cAZ, i - 1, j, k));
+      const R ihx = L / dmax(Abz, eps);
+      const R mux = Cwh * be * ihx * ihx;
+      const R d1 = AT(cBX, i, j, k) - AT(cBX, i, j, k - 1);
+      const R d2 = AT(cBZ, i, j, k) - AT(cBZ, i - 1, j, k);
+      AT(cHY, i, j, k) = AT(cTPY, i, j, k) * (Ecen + R(0.5) * muz * d1 - R(0.5) * mux * d2);
     }
     if (k < B.n2) {
-      double Ec[3];
+      R Ec[3];
       for (int q = 0; q < 3; ++q)
-        Ec[q] = 0.25 * (AT(cEHC + q, i - 1, j - 1, k) + AT(cEHC + q, i - 1, j, k) + AT(cEHC + q, i, j - 1, k) +
+        Ec[q] = R(0.25) * (AT(cEHC + q, i - 1, j - 1, k) + AT(cEHC + q, i - 1, j, k) + AT(cEHC + q, i, j - 1, k) +
                         AT(cEHC + q, i, j, k));
-      const double Ecen = Ec[0] * AT(cDRZ, i, j, k) + Ec[1] * AT(cDRZ + 1, i, j, k) + Ec[2] * AT(cDRZ + 2, i, j, k);
-      const double be =
+      const R Ecen = Ec[0] * AT(cDRZ, i, j, k) + Ec[1] * AT(cDRZ + 1, i, j, k) + Ec[2] * AT(cDRZ + 2, i, j, k);
+      const R be =
           dmax(dmax(AT(cHB, i - 1, j - 1, k), AT(cHB, i - 1, j, k)), dmax(AT(cHB, i, j - 1, k), AT(cHB, i, j, k)));
-      const double L = dmax(AT(cDLZ, i, j, k), eps);
-      const double Abe = 0.5 * (AT(cAY, i, j, k) + AT(cAY, i - 1, j, k));
-      const double ihx = L / dmax(Abe, eps);
-      const double mux = Cwh * be * ihx * ihx;
-      const double Abx = 0.5 * (AT(cAX, i, j, k) + AT(cAX, i, j - 1, k));
-      const double ihe = L / dmax(Abx, eps);
-      const double mue = Cwh * be * ihe * ihe;
-      const double d1 = AT(cBY, i, j, k) - AT(cBY, i - 1, j, k);
-      const double d2 = AT(cBX, i, j, k) - AT(cBX, i, j - 1, k);
-      AT(cHZ, i, j, k) = AT(cTPZ, i, j, k) * (Ecen + 0.5 * mux * d1 - 0.5 * mue * d2);
+      const R L = dmax(AT(cDLZ, i, j, k), eps);
+      const R Abe = R(0.5) * (AT(cAY, i, j, k) + AT(cAY, i - 1, j, k));
+      const R ihx = L / dmax(Abe, eps);
+      const R mux = Cwh * be * ihx * ihx;
+      const R Abx = R(0.5) * (AT(cAX, i, j, k) + AT(cAX, i, j - 1, k));
+      const R ihe = L / dmax(Abx, eps);
+      const R mue = Cwh * be * ihe * ihe;
+      const R d1 = AT(cBY, i, j, k) - AT(cBY, i - 1, j, k);
+      const R d2 = AT(cBX, i, j, k) - AT(cBX, i, j - 1, k);
+      AT(cHZ, i, j, k) = AT(cTPZ, i, j, k) * (Ecen + R(0.5) * mux * d1 - R(0.5) * mue * d2);
     }
   });
 }
 
 // E += Ehall on owned edges (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:135-147).
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_add_hall(Dir D) {
-  for_items<kBox>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int64_t o = B.off(it.i, it.j, it.k);
     if (it.i < B.n0) B.c(cEX)[o] += B.c(cHX)[o];
@@ -427,104 +462,137 @@ __global__ void __launch_bounds__(kTileThreads) k_add_hall(Dir D) {
 
 // ------------------------------------------------------------------ fluid update
 // Rusanov face flux of Scheme_U_ (Z4_Mercury/src/physics/MercurySolver_FluidRHS.cpp:36-104).
-__device__ __forceinline__ void rusanov(const V &B, double g, int u0, int pv0, double k1, double k2, double k3, int iL,
-                                        int jL, int kL, int i, int j, int k, double out[5]) {
-  const double rhoL = AT(u0, iL, jL, kL), uL = AT(pv0, iL, jL, kL), vL = AT(pv0 + 1, iL, jL, kL),
+template <class R>
+__device__ __forceinline__ void rusanov(const V<R> &B, R g, int u0, int pv0, R k1, R k2, R k3,
+                                        R sk, int iL, int jL, int kL, int i, int j, int k, R out[5]) {
+  const R rhoL = AT(u0, iL, jL, kL), uL = AT(pv0, iL, jL, kL), vL = AT(pv0 + 1, iL, jL, kL),
                wL = AT(pv0 + 2, iL, jL, kL), pL = AT(pv0 + 3, iL, jL, kL);
-  const double rhoR = AT(u0, i, j, k), uR = AT(pv0, i, j, k), vR = AT(pv0 + 1, i, j, k), wR = AT(pv0 + 2, i, j, k),
+  const R rhoR = AT(u0, i, j, k), uR = AT(pv0, i, j, k), vR = AT(pv0 + 1, i, j, k), wR = AT(pv0 + 2, i, j, k),
                pR = AT(pv0 + 3, i, j, k);
-  const double reL = pL / (g - 1.0) + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL);
-  const double reR = pR / (g - 1.0) + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR);
-  const double kk = k1 * k1 + k2 * k2 + k3 * k3;
-  const double uvwL = k1 * uL + k2 * vL + k3 * wL, uvwR = k1 * uR + k2 * vR + k3 * wR;
-  const double cL = sqrt(dmax(0.0, g * pL / dmax(rhoL, 1e-30))), cR = sqrt(dmax(0.0, g * pR / dmax(rhoR, 1e-30)));
-  const double rad = dmax(fabs(uvwL) + cL * sqrt(kk), fabs(uvwR) + cR * sqrt(kk));
-  out[0] = 0.5 * (rhoL * uvwL + rhoR * uvwR) - 0.5 * rad * (rhoR - rhoL);
-  out[1] = 0.5 * ((rhoL * uvwL * uL + k1 * pL) + (rhoR * uvwR * uR + k1 * pR)) - 0.5 * rad * (rhoR * uR - rhoL * uL);
-  out[2] = 0.5 * ((rhoL * uvwL * vL + k2 * pL) + (rhoR * uvwR * vR + k2 * pR)) - 0.5 * rad * (rhoR * vR - rhoL * vL);
-  out[3] = 0.5 * ((rhoL * uvwL * wL + k3 * pL) + (rhoR * uvwR * wR + k3 * pR)) - 0.5 * rad * (rhoR * wR - rhoL * wL);
-  out[4] = 0.5 * (uvwL * (reL + pL) + uvwR * (reR + pR)) - 0.5 * rad * (reR - reL);
+  const R reL = pL / (g - R(1.0)) + R(0.5) * rhoL * (uL * uL + vL * vL + wL * wL);
+  const R reR = pR / (g - R(1.0)) + R(0.5) * rhoR * (uR * uR + vR * vR + wR * wR);
+  // sk = sqrt(k1 * k1 + k2 * k2 + k3 * k3), the face's |JD| (FNORM component 3)
+  const R uvwL = k1 * uL + k2 * vL + k3 * wL, uvwR = k1 * uR + k2 * vR + k3 * wR;
+  const R cL = sqrt(dmax(R(0.0), g * pL / dmax(rhoL, R(1e-30)))), cR = sqrt(dmax(R(0.0), g * pR / dmax(rhoR, R(1e-30))));
+  const R rad = dmax(fabs(uvwL) + cL * sk, fabs(uvwR) + cR * sk);
+  out[0] = R(0.5) * (rhoL * uvwL + rhoR * uvwR) - R(0.5) * rad * (rhoR - rhoL);
+  out[1] = R(0.5) * ((rhoL * uvwL * uL + k1 * pL) + (rhoR * uvwR * uR + k1 * pR)) - R(0.5) * rad * (rhoR * uR - rhoL * uL);
+  out[2] = R(0.5) * ((rhoL * uvwL * vL + k2 * pL) + (rhoR * uvwR * vR + k2 * pR)) - R(0.5) * rad * (rhoR * vR - rhoL * vL);
+  out[3] = R(0.5) * ((rhoL * uvwL * wL + k3 * pL) + (rhoR * uvwR * wR + k3 * pR)) - R(0.5) * rad * (rhoR * wR - rhoL * wL);
+  out[4] = R(0.5) * (uvwL * (reL + pL) + uvwR * (reR + pR)) - R(0.5) * rad * (reR - reL);
 }
 
 // ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid (FluidRHS.cpp:206-527) +
 // ApplyUpdate_Euler_ (Z4_Mercury/src/physics/MercurySolver_Advance.cpp:73-147)
-// for one owned cell and one ion species; the state goes to the other buffer.
-__global__ void __launch_bounds__(kTileThreads, 2) k_fluid(Dir D) {
-  for_items<kCells2>(D, [&](const DevSolve &S, const V &B, const Item &it) {
-    if (!it.in) return;
-    const Consts &c = S.c;
-    const double dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
-    if (!(dt >= 1e-7) || !isfinite(dt)) return;  // the reference aborts; k_flip records the status
+// for one tile of owned cells and one ion species; the state goes to the
+// other buffer.  Per direction, the tile's face fluxes are computed once into
+// shared memory (a face's flux has the same inputs and operation order for
+// both cells that share it), then every cell accumulates
+// r[m] -= (F+ - F-) / J, the per-component order of Scheme_U_'s divergence.
+constexpr int kMaxFaces = (kTileI + 1) * kTileJ * kTileK;
+// Minimum resident CTAs per SM asked of the compiler for the two
+// register-heavy kernels (caps registers at 65536 / (256 * n)).
+#ifndef MHD_MIN_CTAS_FLUID
+#define MHD_MIN_CTAS_FLUID 3
+#endif
+#ifndef MHD_MIN_CTAS_PV
+#define MHD_MIN_CTAS_PV 3
+#endif  // largest per-direction face count of a tile
+template <class R>
+__global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir D) {
+  __shared__ R F[5][kMaxFaces];
+  for_items<R, kCells2>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    const ConstsT<R> &c = consts_of<R>(S);
+    const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
+    const bool dt_ok = (dt >= R(1e-7)) && isfinite(dt);  // the reference aborts; k_flip records the status
     const int i = it.i, j = it.j, k = it.k, s = it.species;
     const int u0 = s ? cUN : cUH, pv0 = s ? cPVN : cPVH;
-    const double g = c.gamma;
-    const double invJ = 1.0 / AT(cJAC, i, j, k);
-    // r[m] = ((0 - dx[m]/J) - dy[m]/J) - dz[m]/J, accumulated direction by
-    // direction (the per-component operation sequence of Scheme_U_'s divergence)
-    double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const R g = c.gamma;
+    const int tid = threadIdx.x;
+    const int li = tid / (kTileK * kTileJ), lj = (tid / kTileK) % kTileJ, lk = tid % kTileK;
+    R r[5] = {R(0.0), R(0.0), R(0.0), R(0.0), R(0.0)};
 #pragma unroll 1
     for (int dir = 0; dir < 3; ++dir) {
       const int cm = dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
-      int ip = i, jp = j, kp = k, im = i, jm = j, km = k;
-      shift1(dir, ip, jp, kp, 1);
-      shift1(dir, im, jm, km, -1);
-      double Fm[5], Fp[5];
-      rusanov(B, g, u0, pv0, AT(cm, i, j, k), AT(cm + 1, i, j, k), AT(cm + 2, i, j, k), im, jm, km, i, j, k, Fm);
-      rusanov(B, g, u0, pv0, AT(cm, ip, jp, kp), AT(cm + 1, ip, jp, kp), AT(cm + 2, ip, jp, kp), i, j, k, ip, jp, kp,
-              Fp);
+      const int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
+      const int ei = kTileI + (dir == 0), ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
+      const int nf = ei * ej * ek;
+      for (int f = tid; f < nf; f += kTileThreads) {
+        const int fk = f % ek, fj = (f / ek) % ej, fi = f / (ek * ej);
+        const int x[3] = {it.o[0] + fi, it.o[1] + fj, it.o[2] + fk};
+        bool need = dt_ok;
+        for (int a = 0; a < 3; ++a) need = need && x[a] >= it.lo[a] && x[a] < it.hi[a] + (a == dir);
+        if (need) {
+          int im = x[0], jm = x[1], km = x[2];
+          shift1(dir, im, jm, km, -1);
+          R Fl[5];
+          rusanov(B, g, u0, pv0, R(ATM(cm, x[0], x[1], x[2])), R(ATM(cm + 1, x[0], x[1], x[2])), R(ATM(cm + 2, x[0], x[1], x[2])),
+                  AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
 #pragma unroll
-      for (int m = 0; m < 5; ++m) r[m] -= (Fp[m] - Fm[m]) * invJ;
-    }
-    // sources (FluidRHS.cpp:206-527)
-    const double Tn0 = 1000.0, sk1 = 5.0e-5, sk2 = 1.0e-5;
-    const double a4 = (c.L_ref / c.U_ref);
-    const double a5 = (3.0 * c.L_ref * c.k_Boltz * c.n_ref) / (c.rho_ref * c.U_ref * c.U_ref * c.U_ref);
-    const double upx = AT(cUP, i, j, k), upy = AT(cUP + 1, i, j, k), upz = AT(cUP + 2, i, j, k);
-    const double Bx = AT(cBC, i, j, k), By = AT(cBC + 1, i, j, k), Bz = AT(cBC + 2, i, j, k);
-    const double Jx = AT(cJC, i, j, k), Jy = AT(cJC + 1, i, j, k), Jz = AT(cJC + 2, i, j, k);
-    const double sjbx = Jy * Bz - Jz * By, sjby = Jz * Bx - Jx * Bz, sjbz = Jx * By - Jy * Bx;
-    const Num num = num_limiter(c, AT(cUH, i, j, k), AT(cUN, i, j, k));
-    double dpex = 0.0, dpey = 0.0, dpez = 0.0;
-    if (c.ambipolar) {
-      const double Vol = fabs(AT(cJAC, i, j, k));
-      double ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0, cxm = 0, cym = 0, czm = 0;
-      if (Vol > 0.0) {
-        ax = 0.5 * (AT(cJDX, i - 1, j, k) + AT(cJDX, i, j, k)) / Vol;
-        ay = 0.5 * (AT(cJDX + 1, i - 1, j, k) + AT(cJDX + 1, i, j, k)) / Vol;
-        az = 0.5 * (AT(cJDX + 2, i - 1, j, k) + AT(cJDX + 2, i, j, k)) / Vol;
-        bx = 0.5 * (AT(cJDY, i, j - 1, k) + AT(cJDY, i, j, k)) / Vol;
-        by = 0.5 * (AT(cJDY + 1, i, j - 1, k) + AT(cJDY + 1, i, j, k)) / Vol;
-        bz = 0.5 * (AT(cJDY + 2, i, j - 1, k) + AT(cJDY + 2, i, j, k)) / Vol;
-        cxm = 0.5 * (AT(cJDZ, i, j, k - 1) + AT(cJDZ, i, j, k)) / Vol;
-        cym = 0.5 * (AT(cJDZ + 1, i, j, k - 1) + AT(cJDZ + 1, i, j, k)) / Vol;
-        czm = 0.5 * (AT(cJDZ + 2, i, j, k - 1) + AT(cJDZ + 2, i, j, k)) / Vol;
+          for (int m = 0; m < 5; ++m) F[m][f] = Fl[m];
+        }
       }
-      const double pip = AT(cPVH + 3, i + 1, j, k) + AT(cPVN + 3, i + 1, j, k);
-      const double pim = AT(cPVH + 3, i - 1, j, k) + AT(cPVN + 3, i - 1, j, k);
-      const double pjp = AT(cPVH + 3, i, j + 1, k) + AT(cPVN + 3, i, j + 1, k);
-      const double pjm = AT(cPVH + 3, i, j - 1, k) + AT(cPVN + 3, i, j - 1, k);
-      const double pkp = AT(cPVH + 3, i, j, k + 1) + AT(cPVN + 3, i, j, k + 1);
-      const double pkm = AT(cPVH + 3, i, j, k - 1) + AT(cPVN + 3, i, j, k - 1);
-      dpex = 0.5 * (ax * (pip - pim) + bx * (pjp - pjm) + cxm * (pkp - pkm));
-      dpey = 0.5 * (ay * (pip - pim) + by * (pjp - pjm) + cym * (pkp - pkm));
-      dpez = 0.5 * (az * (pip - pim) + bz * (pjp - pjm) + czm * (pkp - pkm));
+      __syncthreads();
+      if (it.in && dt_ok) {
+        const R invJ = R(1.0) / R(ATM(cJAC, i, j, k));
+        const int fm = (li * ej + lj) * ek + lk;
+        const int fp = fm + (dir == 0 ? ej * ek : dir == 1 ? ek : 1);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) r[m] -= (F[m][fp] - F[m][fm]) * invJ;
+      }
+      __syncthreads();
     }
-    const double x = AT(cCX, i, j, k), y = AT(cCY, i, j, k), z = AT(cCZ, i, j, k);
-    const double rho_cyl = sqrt(y * y + z * z);
-    const double vst = (x < 0.0 && rho_cyl < 1.0) ? sk2 : sk1;
-    const double nS = s ? num.nNa : num.nH;
-    const double chi = s ? num.wNa : num.wH;
-    const double rho = dmax(AT(u0, i, j, k), 0.0);
-    const double u = AT(pv0, i, j, k), v = AT(pv0 + 1, i, j, k), w = AT(pv0 + 2, i, j, k);
-    const double u2 = u * u + v * v + w * w;
-    const double subx = (v - upy) * Bz - (w - upz) * By;
-    const double suby = (w - upz) * Bx - (u - upx) * Bz;
-    const double subz = (u - upx) * By - (v - upy) * Bx;
-    const double subu = subx * u + suby * v + subz * w;
-    const double sjbu = sjbx * u + sjby * v + sjbz * w;
-    const double dpeu = dpex * u + dpey * v + dpez * w;
-    const double Ts0 = AT(pv0 + 4, i, j, k) * c.T_ref;
-    double b1, b2;
+    if (!it.in || !dt_ok) return;
+    // sources (FluidRHS.cpp:206-527)
+    const R Tn0 = R(1000.0), sk1 = R(5.0e-5), sk2 = R(1.0e-5);
+    const R a4 = (c.L_ref / c.U_ref);
+    const R a5 = (R(3.0) * c.L_ref * c.k_Boltz * c.n_ref) / (c.rho_ref * c.U_ref * c.U_ref * c.U_ref);
+    const R upx = AT(cUP, i, j, k), upy = AT(cUP + 1, i, j, k), upz = AT(cUP + 2, i, j, k);
+    const R Bx = AT(cBC, i, j, k), By = AT(cBC + 1, i, j, k), Bz = AT(cBC + 2, i, j, k);
+    const R Jx = AT(cJC, i, j, k), Jy = AT(cJC + 1, i, j, k), Jz = AT(cJC + 2, i, j, k);
+    const R sjbx = Jy * Bz - Jz * By, sjby = Jz * Bx - Jx * Bz, sjbz = Jx * By - Jy * Bx;
+    const Num<R> num = num_limiter(c, AT(cUH, i, j, k), AT(cUN, i, j, k));
+    R dpex = R(0.0), dpey = R(0.0), dpez = R(0.0);
+    if (c.ambipolar) {
+      const R Vol = fabs(R(ATM(cJAC, i, j, k)));
+      R ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0, cxm = 0, cym = 0, czm = 0;
+      if (Vol > R(0.0)) {
+        ax = R(0.5) * (R(ATM(cJDX, i - 1, j, k)) + R(ATM(cJDX, i, j, k))) / Vol;
+        ay = R(0.5) * (R(ATM(cJDX + 1, i - 1, j, k)) + R(ATM(cJDX + 1, i, j, k))) / Vol;
+        az = R(0.5) * (R(ATM(cJDX + 2, i - 1, j, k)) + R(ATM(cJDX + 2, i, j, k))) / Vol;
+        bx = R(0.5) * (R(ATM(cJDY, i, j - 1, k)) + R(ATM(cJDY, i, j, k))) / Vol;
+        by = R(0.5) * (R(ATM(cJDY + 1, i, j - 1, k)) + R(ATM(cJDY + 1, i, j, k))) / Vol;
+        bz = R(0.5) * (R(ATM(cJDY + 2, i, j - 1, k)) + R(ATM(cJDY + 2, i, j, k))) / Vol;
+        cxm = R(0.5) * (R(ATM(cJDZ, i, j, k - 1)) + R(ATM(cJDZ, i, j, k))) / Vol;
+        cym = R(0.5) * (R(ATM(cJDZ + 1, i, j, k - 1)) + R(ATM(cJDZ + 1, i, j, k))) / Vol;
+        czm = R(0.5) * (R(ATM(cJDZ + 2, i, j, k - 1)) + R(ATM(cJDZ + 2, i, j, k))) / Vol;
+      }
+      const R pip = AT(cPVH + 3, i + 1, j, k) + AT(cPVN + 3, i + 1, j, k);
+      const R pim = AT(cPVH + 3, i - 1, j, k) + AT(cPVN + 3, i - 1, j, k);
+      const R pjp = AT(cPVH + 3, i, j + 1, k) + AT(cPVN + 3, i, j + 1, k);
+      const R pjm = AT(cPVH + 3, i, j - 1, k) + AT(cPVN + 3, i, j - 1, k);
+      const R pkp = AT(cPVH + 3, i, j, k + 1) + AT(cPVN + 3, i, j, k + 1);
+      const R pkm = AT(cPVH + 3, i, j, k - 1) + AT(cPVN + 3, i, j, k - 1);
+      dpex = R(0.5) * (ax * (pip - pim) + bx * (pjp - pjm) + cxm * (pkp - pkm));
+      dpey = R(0.5) * (ay * (pip - pim) + by * (pjp - pjm) + cym * (pkp - pkm));
+      dpez = R(0.5) * (az * (pip - pim) + bz * (pjp - pjm) + czm * (pkp - pkm));
+    }
+    const R x = AT(cCX, i, j, k), y = AT(cCY, i, j, k), z = AT(cCZ, i, j, k);
+    const R rho_cyl = sqrt(y * y + z * z);
+    const R vst = (x < R(0.0) && rho_cyl < R(1.0)) ? sk2 : sk1;
+    const R nS = s ? num.nNa : num.nH;
+    const R chi = s ? num.wNa : num.wH;
+    const R rho = dmax(AT(u0, i, j, k), R(0.0));
+    const R u = AT(pv0, i, j, k), v = AT(pv0 + 1, i, j, k), w = AT(pv0 + 2, i, j, k);
+    const R u2 = u * u + v * v + w * w;
+    const R subx = (v - upy) * Bz - (w - upz) * By;
+    const R suby = (w - upz) * Bx - (u - upx) * Bz;
+    const R subz = (u - upx) * By - (v - upy) * Bx;
+    const R subu = subx * u + suby * v + subz * w;
+    const R sjbu = sjbx * u + sjby * v + sjbz * w;
+    const R dpeu = dpex * u + dpey * v + dpez * w;
+    const R Ts0 = AT(pv0 + 4, i, j, k) * c.T_ref;
+    R b1, b2;
     if (!s) {
       b1 = vst * (Tn0 - Ts0) * (c.M_H / (c.M_H + c.M_Na));
       b2 = (c.M_Na / (c.M_H + c.M_Na)) * vst;
@@ -543,9 +611,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_fluid(Dir D) {
       r[4] -= chi * dpeu;
     }
     if (s) {
-      const double a1_Na = (c.L_ref / c.U_ref) * (c.m_Na / c.rho_ref) * 1e6;
-      const double a6 = (1.0e6 * c.L_ref * c.k_Boltz) / (c.rho_ref * c.U_ref * c.U_ref * c.U_ref * (c.gamma - 1.0));
-      const double sss = AT(cPHOTO, i, j, k);
+      const R a1_Na = (c.L_ref / c.U_ref) * (c.m_Na / c.rho_ref) * R(1e6);
+      const R a6 = (R(1.0e6) * c.L_ref * c.k_Boltz) / (c.rho_ref * c.U_ref * c.U_ref * c.U_ref * (c.gamma - R(1.0)));
+      const R sss = AT(cPHOTO, i, j, k);
       r[0] += a1_Na * sss;
       r[4] += a6 * sss * Tn0;
     }
@@ -562,22 +630,23 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_fluid(Dir D) {
 }
 
 // B_face += dt * (-curl E) on the owned faces (CTOperators.cpp:6-56 with multiplier -1).
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_bface(Dir D) {
-  for_items<kBox>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const double dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
-    if (!(dt >= 1e-7) || !isfinite(dt)) return;
+    const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
+    if (!(dt >= R(1e-7)) || !isfinite(dt)) return;
     const int i = it.i, j = it.j, k = it.k;
     if (j < B.n1 && k < B.n2) {
-      const double rb = -1.0 * ((AT(cEY, i, j, k) - AT(cEY, i, j, k + 1)) + (AT(cEZ, i, j + 1, k) - AT(cEZ, i, j, k)));
+      const R rb = -R(1.0) * ((AT(cEY, i, j, k) - AT(cEY, i, j, k + 1)) + (AT(cEZ, i, j + 1, k) - AT(cEZ, i, j, k)));
       AT(cBX, i, j, k) += dt * rb;
     }
     if (i < B.n0 && k < B.n2) {
-      const double rb = -1.0 * ((AT(cEX, i, j, k + 1) - AT(cEX, i, j, k)) + (AT(cEZ, i, j, k) - AT(cEZ, i + 1, j, k)));
+      const R rb = -R(1.0) * ((AT(cEX, i, j, k + 1) - AT(cEX, i, j, k)) + (AT(cEZ, i, j, k) - AT(cEZ, i + 1, j, k)));
       AT(cBY, i, j, k) += dt * rb;
     }
     if (i < B.n0 && j < B.n1) {
-      const double rb = -1.0 * ((AT(cEX, i, j, k) - AT(cEX, i, j + 1, k)) + (AT(cEY, i + 1, j, k) - AT(cEY, i, j, k)));
+      const R rb = -R(1.0) * ((AT(cEX, i, j, k) - AT(cEX, i, j + 1, k)) + (AT(cEY, i + 1, j, k) - AT(cEY, i, j, k)));
       AT(cBZ, i, j, k) += dt * rb;
     }
   });
@@ -587,20 +656,21 @@ __global__ void __launch_bounds__(kTileThreads) k_bface(Dir D) {
 // calc_Bcell (Z4_Mercury/src/physics/MercurySolver_MagneticCell.cpp:3-90) on owned cells and
 // CurlAdjFaceToEdge + alpha scaling of Calc_J_Edge (CTOperators.cpp:59-110,
 // Z4_Mercury/src/physics/MercurySolver_Current.cpp:140-190) on owned edges.
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_bcell_jedge(Dir D) {
-  for_items<kBox>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
     if (i < B.n0 && j < B.n1 && k < B.n2) {
-      const double pt[6] = {-AT(cBX, i, j, k) - AT(cBAX, i, j, k), AT(cBX, i + 1, j, k) + AT(cBAX, i + 1, j, k),
+      const R pt[6] = {-AT(cBX, i, j, k) - AT(cBAX, i, j, k), AT(cBX, i + 1, j, k) + AT(cBAX, i + 1, j, k),
                             -AT(cBY, i, j, k) - AT(cBAY, i, j, k), AT(cBY, i, j + 1, k) + AT(cBAY, i, j + 1, k),
                             -AT(cBZ, i, j, k) - AT(cBAZ, i, j, k), AT(cBZ, i, j, k + 1) + AT(cBAZ, i, j, k + 1)};
-      const double pi_[6] = {-AT(cBX, i, j, k), AT(cBX, i + 1, j, k), -AT(cBY, i, j, k),
+      const R pi_[6] = {-AT(cBX, i, j, k), AT(cBX, i + 1, j, k), -AT(cBY, i, j, k),
                              AT(cBY, i, j + 1, k), -AT(cBZ, i, j, k), AT(cBZ, i, j, k + 1)};
-      double bxt = 0, byt = 0, bzt = 0, bxi = 0, byi = 0, bzi = 0;
+      R bxt = 0, byt = 0, bzt = 0, bxi = 0, byi = 0, bzi = 0;
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const double wx = AT(cWB + q, i, j, k), wy = AT(cWB + 6 + q, i, j, k), wz = AT(cWB + 12 + q, i, j, k);
+        const R wx = AT(cWB + q, i, j, k), wy = AT(cWB + 6 + q, i, j, k), wz = AT(cWB + 12 + q, i, j, k);
         bxt += wx * pt[q];
         byt += wy * pt[q];
         bzt += wz * pt[q];
@@ -617,33 +687,34 @@ __global__ void __launch_bounds__(kTileThreads) k_bcell_jedge(Dir D) {
       B.c(cBIC + 2)[o] = bzi;
     }
     if (i < B.n0) {
-      const double v = ((AT(cBFY, i, j, k - 1) * AT(cBY, i, j, k - 1) - AT(cBFY, i, j, k) * AT(cBY, i, j, k)) +
-                        (AT(cBFZ, i, j, k) * AT(cBZ, i, j, k) - AT(cBFZ, i, j - 1, k) * AT(cBZ, i, j - 1, k))) * 1.0;
+      const R v = ((AT(cBFY, i, j, k - 1) * AT(cBY, i, j, k - 1) - AT(cBFY, i, j, k) * AT(cBY, i, j, k)) +
+                        (AT(cBFZ, i, j, k) * AT(cBZ, i, j, k) - AT(cBFZ, i, j - 1, k) * AT(cBZ, i, j - 1, k))) * R(1.0);
       AT(cJX, i, j, k) = v * AT(cALX, i, j, k);
     }
     if (j < B.n1) {
-      const double v = ((AT(cBFX, i, j, k) * AT(cBX, i, j, k) - AT(cBFX, i, j, k - 1) * AT(cBX, i, j, k - 1)) +
-                        (AT(cBFZ, i - 1, j, k) * AT(cBZ, i - 1, j, k) - AT(cBFZ, i, j, k) * AT(cBZ, i, j, k))) * 1.0;
+      const R v = ((AT(cBFX, i, j, k) * AT(cBX, i, j, k) - AT(cBFX, i, j, k - 1) * AT(cBX, i, j, k - 1)) +
+                        (AT(cBFZ, i - 1, j, k) * AT(cBZ, i - 1, j, k) - AT(cBFZ, i, j, k) * AT(cBZ, i, j, k))) * R(1.0);
       AT(cJY, i, j, k) = v * AT(cALY, i, j, k);
     }
     if (k < B.n2) {
-      const double v = ((AT(cBFX, i, j - 1, k) * AT(cBX, i, j - 1, k) - AT(cBFX, i, j, k) * AT(cBX, i, j, k)) +
-                        (AT(cBFY, i, j, k) * AT(cBY, i, j, k) - AT(cBFY, i - 1, j, k) * AT(cBY, i - 1, j, k))) * 1.0;
+      const R v = ((AT(cBFX, i, j - 1, k) * AT(cBX, i, j - 1, k) - AT(cBFX, i, j, k) * AT(cBX, i, j, k)) +
+                        (AT(cBFY, i, j, k) * AT(cBY, i, j, k) - AT(cBFY, i - 1, j, k) * AT(cBY, i - 1, j, k))) * R(1.0);
       AT(cJZ, i, j, k) = v * AT(cALZ, i, j, k);
     }
   });
 }
 
 // calc_Jcell (Current.cpp:203-243), owned cells.
+template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_jcell(Dir D) {
-  for_items<kCells>(D, [&](const DevSolve &S, const V &B, const Item &it) {
+  for_items<R, kCells>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
-    const double s[12] = {AT(cJX, i, j, k),         AT(cJX, i, j + 1, k),     AT(cJX, i, j, k + 1),
+    const R s[12] = {AT(cJX, i, j, k),         AT(cJX, i, j + 1, k),     AT(cJX, i, j, k + 1),
                           AT(cJX, i, j + 1, k + 1), AT(cJY, i, j, k),         AT(cJY, i + 1, j, k),
                           AT(cJY, i, j, k + 1),     AT(cJY, i + 1, j, k + 1), AT(cJZ, i, j, k),
                           AT(cJZ, i + 1, j, k),     AT(cJZ, i, j + 1, k),     AT(cJZ, i + 1, j + 1, k)};
-    double jx = 0, jy = 0, jz = 0;
+    R jx = 0, jy = 0, jz = 0;
 #pragma unroll
     for (int q = 0; q < 12; ++q) {
       jx += AT(cWJ + q, i, j, k) * s[q];
@@ -659,85 +730,114 @@ __global__ void __launch_bounds__(kTileThreads) k_jcell(Dir D) {
 
 // CFL time step of one cell and both species (Compute_Timestep,
 // Z4_Mercury/src/physics/MercurySolver_Timestep.cpp:8-141).
-__device__ __forceinline__ double fast_cf(double cs2, double vA2, double vAn2) {
-  const double term = cs2 + vA2;
-  double disc = term * term - 4.0 * cs2 * vAn2;
-  if (disc < 0.0) disc = 0.0;
-  return sqrt(0.5 * (term + sqrt(disc)));
+template <class R>
+__device__ __forceinline__ R fast_cf(R cs2, R vA2, R vAn2) {
+  const R term = cs2 + vA2;
+  R disc = term * term - R(4.0) * cs2 * vAn2;
+  if (disc < R(0.0)) disc = R(0.0);
+  return sqrt(R(0.5) * (term + sqrt(disc)));
 }
-__device__ __forceinline__ double face_term(const Consts &c, double ax, double ay, double az, bool outward_plus, double ux,
-                                            double uy, double uz, double Bx, double By, double Bz, double B2, double rho,
-                                            double cs2) {
-  const double An = sqrt(ax * ax + ay * ay + az * az);
-  if (An <= 0.0) return 0.0;
-  double nx = ax / An, ny = ay / An, nz = az / An;
+// One face's term of the CFL denominator.  (nx, ny, nz, An) are the face's
+// precomputed a / |a| and |a| (k_face_normals: the same operations as the
+// reference evaluates per face); vA2 = inver_MA2 * B2 / rho is the same for
+// all faces of a cell and species.
+template <class R>
+__device__ __forceinline__ R face_term(const ConstsT<R> &c, R nx, R ny, R nz, R An,
+                                            bool outward_plus, R ux, R uy, R uz, R Bx, R By,
+                                            R Bz, R vA2, R rho, R cs2) {
+  if (An <= R(0.0)) return R(0.0);
   if (!outward_plus) {
     nx = -nx;
     ny = -ny;
     nz = -nz;
   }
-  const double un = ux * nx + uy * ny + uz * nz;
-  const double Bn = Bx * nx + By * ny + Bz * nz;
-  const double vA2 = c.inver_MA2 * B2 / rho;
-  const double vAn2 = c.inver_MA2 * (Bn * Bn) / rho;
+  const R un = ux * nx + uy * ny + uz * nz;
+  const R Bn = Bx * nx + By * ny + Bz * nz;
+  const R vAn2 = c.inver_MA2 * (Bn * Bn) / rho;
   return (fabs(un) + fast_cf(cs2, vA2, vAn2)) * An;
 }
-__device__ __forceinline__ double cell_dt(const V &B, const Consts &c, int i, int j, int k) {
-  double dtl = 1e100;
-  const double Vol = fabs(AT(cJAC, i, j, k));
-  if (!(Vol > 0.0)) return dtl;
-  const double Bx = AT(cBC, i, j, k), By = AT(cBC + 1, i, j, k), Bz = AT(cBC + 2, i, j, k);
-  const double B2 = Bx * Bx + By * By + Bz * Bz;
+template <class R>
+__device__ __forceinline__ R cell_dt(const V<R> &B, const ConstsT<R> &c, int i, int j, int k) {
+  R dtl = R(1e100);
+  const R Vol = fabs(R(ATM(cJAC, i, j, k)));
+  if (!(Vol > R(0.0))) return dtl;
+  const R Bx = AT(cBC, i, j, k), By = AT(cBC + 1, i, j, k), Bz = AT(cBC + 2, i, j, k);
+  const R B2 = Bx * Bx + By * By + Bz * Bz;
+#pragma unroll 1
   for (int s = 0; s < 2; ++s) {
     const int u0 = s ? cUN : cUH;
-    const double rho = dmax(AT(u0, i, j, k), 1e-2);
-    const double ux = AT(u0 + 1, i, j, k) / rho, uy = AT(u0 + 2, i, j, k) / rho, uz = AT(u0 + 3, i, j, k) / rho;
-    const double E = AT(u0 + 4, i, j, k);
-    const double ke = 0.5 * rho * (ux * ux + uy * uy + uz * uz);
-    const double pr = (c.gamma - 1.0) * (E - ke);
-    const double cs2 = c.gamma * pr / rho;
-    double den = 0.0;
-    den += face_term(c, AT(cJDX, i, j, k), AT(cJDX + 1, i, j, k), AT(cJDX + 2, i, j, k), false, ux, uy, uz, Bx, By, Bz,
-                     B2, rho, cs2);
-    den += face_term(c, AT(cJDX, i + 1, j, k), AT(cJDX + 1, i + 1, j, k), AT(cJDX + 2, i + 1, j, k), true, ux, uy, uz, Bx,
-                     By, Bz, B2, rho, cs2);
-    den += face_term(c, AT(cJDY, i, j, k), AT(cJDY + 1, i, j, k), AT(cJDY + 2, i, j, k), false, ux, uy, uz, Bx, By, Bz,
-                     B2, rho, cs2);
-    den += face_term(c, AT(cJDY, i, j + 1, k), AT(cJDY + 1, i, j + 1, k), AT(cJDY + 2, i, j + 1, k), true, ux, uy, uz, Bx,
-                     By, Bz, B2, rho, cs2);
-    den += face_term(c, AT(cJDZ, i, j, k), AT(cJDZ + 1, i, j, k), AT(cJDZ + 2, i, j, k), false, ux, uy, uz, Bx, By, Bz,
-                     B2, rho, cs2);
-    den += face_term(c, AT(cJDZ, i, j, k + 1), AT(cJDZ + 1, i, j, k + 1), AT(cJDZ + 2, i, j, k + 1), true, ux, uy, uz, Bx,
-                     By, Bz, B2, rho, cs2);
-    if (den > 0.0) dtl = dmin(dtl, c.CFL * Vol / den);
+    const R rho = dmax(AT(u0, i, j, k), R(1e-2));
+    const R ux = AT(u0 + 1, i, j, k) / rho, uy = AT(u0 + 2, i, j, k) / rho, uz = AT(u0 + 3, i, j, k) / rho;
+    const R E = AT(u0 + 4, i, j, k);
+    const R ke = R(0.5) * rho * (ux * ux + uy * uy + uz * uz);
+    const R pr = (c.gamma - R(1.0)) * (E - ke);
+    const R cs2 = c.gamma * pr / rho;
+    const R vA2 = c.inver_MA2 * B2 / rho;
+    R den = R(0.0);
+    // faces xi-, xi+, eta-, eta+, zeta-, zeta+ (the reference's summation order)
+#pragma unroll 1
+    for (int f = 0; f < 6; ++f) {
+      const int a = f >> 1, up = f & 1;
+      const int cn = a == 0 ? cFNX : a == 1 ? cFNY : cFNZ;
+      int fi = i, fj = j, fk = k;
+      shift1(a, fi, fj, fk, up);
+      den += face_term(c, AT(cn, fi, fj, fk), AT(cn + 1, fi, fj, fk), AT(cn + 2, fi, fj, fk), AT(cn + 3, fi, fj, fk),
+                       up != 0, ux, uy, uz, Bx, By, Bz, vA2, rho, cs2);
+    }
+    if (den > R(0.0)) dtl = dmin(dtl, c.CFL * Vol / den);
   }
   return dtl;
+}
+
+// Static per-face terms of the CFL time step and the Rusanov wave speed, once
+// per solve (run by mhd_prepare): |a| = sqrt(ax ax + ay ay + az az) and
+// a / |a| of the face area vectors JD, the operations and order
+// Compute_Timestep (Timestep.cpp:15-16,78-93) and calc_Jac_radius_GCL (FluidRHS.cpp:5-14)
+// apply to the same static inputs every step.  Owned faces and one more layer.
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) {
+      const int cm = a == 0 ? cJDX : a == 1 ? cJDY : cJDZ;
+      const int cn = a == 0 ? cFNX : a == 1 ? cFNY : cFNZ;
+      const int64_t o = B.off(it.i, it.j, it.k);
+      const double ax = B.m(cm)[o], ay = B.m(cm + 1)[o], az = B.m(cm + 2)[o];
+      const double An = sqrt(ax * ax + ay * ay + az * az);
+      B.c(cn)[o] = R(ax / An);
+      B.c(cn + 1)[o] = R(ay / An);
+      B.c(cn + 2)[o] = R(az / An);
+      B.c(cn + 3)[o] = R(An);
+    }
+  });
 }
 
 // calc_PV + calc_Uplus (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:159-301) on the allocated
 // cell range, the contravariant velocities UCON where the Jacobian exists
 // ([-(g-1), n + g - 1)), and the next step's CFL dt on owned cells (CTA min,
-// one atomicMin per tile on the positive-double bit pattern).
-__global__ void __launch_bounds__(kTileThreads, 2) k_pv_uplus(Dir D) {
-  __shared__ double red[kTileThreads / 32];
-  for_items<kAlloc>(D, [&](const DevSolve &S, const V &B, const Item &it) {
-    const Consts &c = S.c;
+// one atomicMin per tile on the bit pattern of the positive double).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir D) {
+  __shared__ R red[kTileThreads / 32];
+  for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    const ConstsT<R> &c = consts_of<R>(S);
     const int i = it.i, j = it.j, k = it.k;
-    double dtl = 1e100;
+    R dtl = R(1e100);
     if (it.in) {
-      double vel[2][3];
+      R vel[2][3];
       for (int s = 0; s < 2; ++s) {
         const int u0 = s ? cUN : cUH, pv0 = s ? cPVN : cPVH;
-        const double coeff = s ? c.state_coeff_Na : c.state_coeff_H;
-        const double rho = dmax(AT(u0, i, j, k), 1e-12);
-        const double u = AT(u0 + 1, i, j, k) / rho, v = AT(u0 + 2, i, j, k) / rho, w = AT(u0 + 3, i, j, k) / rho;
-        const double E = AT(u0 + 4, i, j, k);
-        const double ke = 0.5 * rho * (u * u + v * v + w * w);
-        double eint = E - ke;
-        if (eint < 0.0) eint = 0.0;
-        double pr = (c.gamma - 1.0) * eint;
-        pr = dmax(pr, 1e-12);
-        const double T = pr / (rho * coeff);
+        const R coeff = s ? c.state_coeff_Na : c.state_coeff_H;
+        const R rho = dmax(AT(u0, i, j, k), R(1e-12));
+        const R u = AT(u0 + 1, i, j, k) / rho, v = AT(u0 + 2, i, j, k) / rho, w = AT(u0 + 3, i, j, k) / rho;
+        const R E = AT(u0 + 4, i, j, k);
+        const R ke = R(0.5) * rho * (u * u + v * v + w * w);
+        R eint = E - ke;
+        if (eint < R(0.0)) eint = R(0.0);
+        R pr = (c.gamma - R(1.0)) * eint;
+        pr = dmax(pr, R(1e-12));
+        const R T = pr / (rho * coeff);
         const int64_t o = B.off(i, j, k);
         B.c(pv0)[o] = u;
         B.c(pv0 + 1)[o] = v;
@@ -748,25 +848,25 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_pv_uplus(Dir D) {
         vel[s][1] = v;
         vel[s][2] = w;
       }
-      const double rH = dmax(AT(cUH, i, j, k), 0.0), rN = dmax(AT(cUN, i, j, k), 0.0);
-      const Num d = num_limiter(c, rH, rN);
-      double up[3];
+      const R rH = dmax(AT(cUH, i, j, k), R(0.0)), rN = dmax(AT(cUN, i, j, k), R(0.0));
+      const Num<R> d = num_limiter(c, rH, rN);
+      R up[3];
       for (int q = 0; q < 3; ++q) {
-        const double uH = rH > 1e-20 ? vel[0][q] : 0.0;
-        const double uN = rN > 1e-20 ? vel[1][q] : 0.0;
+        const R uH = rH > R(1e-20) ? vel[0][q] : R(0.0);
+        const R uN = rN > R(1e-20) ? vel[1][q] : R(0.0);
         up[q] = d.chiH * uH + d.chiNa * uN;
         AT(cUP + q, i, j, k) = up[q];
       }
       const int gm = c.nghost - 1;
       if (i >= -gm && i < B.n0 + gm && j >= -gm && j < B.n1 + gm && k >= -gm && k < B.n2 + gm) {
-        const double inv_jac = 1.0 / (fabs(AT(cJAC, i, j, k)) + 1.0e-30);
+        const R inv_jac = R(1.0) / (fabs(R(ATM(cJAC, i, j, k))) + R(1.0e-30));
         for (int axis = 0; axis < 3; ++axis) {
           int ip = i, jp = j, kp = k;
           shift1(axis, ip, jp, kp, 1);
           const int cm = axis == 0 ? cJDX : axis == 1 ? cJDY : cJDZ;
-          const double kx = 0.5 * (AT(cm, i, j, k) + AT(cm, ip, jp, kp));
-          const double ky = 0.5 * (AT(cm + 1, i, j, k) + AT(cm + 1, ip, jp, kp));
-          const double kz = 0.5 * (AT(cm + 2, i, j, k) + AT(cm + 2, ip, jp, kp));
+          const R kx = R(0.5) * (R(ATM(cm, i, j, k)) + R(ATM(cm, ip, jp, kp)));
+          const R ky = R(0.5) * (R(ATM(cm + 1, i, j, k)) + R(ATM(cm + 1, ip, jp, kp)));
+          const R kz = R(0.5) * (R(ATM(cm + 2, i, j, k)) + R(ATM(cm + 2, ip, jp, kp)));
           AT(cUC + axis, i, j, k) = (kx * up[0] + ky * up[1] + kz * up[2]) * inv_jac;
         }
       }
@@ -776,9 +876,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_pv_uplus(Dir D) {
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dtl;
     __syncthreads();
     if (threadIdx.x < 32) {
-      double v = threadIdx.x < kTileThreads / 32 ? red[threadIdx.x] : 1e100;
+      R v = threadIdx.x < kTileThreads / 32 ? red[threadIdx.x] : R(1e100);
       for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if (threadIdx.x == 0 && v < 1e100)
+      if (threadIdx.x == 0 && v < R(1e100))
         atomicMin(&D.state[it.s].dt_bits, (unsigned long long)__double_as_longlong(v));
     }
     __syncthreads();
@@ -796,46 +896,57 @@ __device__ __forceinline__ int find_solve(const int *prefix, int nsolves, int e)
   }
   return lo;
 }
-__device__ __forceinline__ double *decode(const DevSolve &S, int cur, int64_t code) {
-  const int blk = (int)(code >> 48);
-  const int comp = (int)((code >> 40) & 0xff);
-  const int64_t off = code & ((int64_t(1) << 40) - 1);
-  const DevBlock &DB = S.blocks[blk];
-  return comp < kNumUComps ? DB.U[cur] + (int64_t)comp * DB.total + off
-                           : DB.M + (int64_t)(comp - kNumUComps) * DB.total + off;
+template <class R>
+__device__ __forceinline__ R *at_code(const DevSolve &S, int cur, int64_t code) {
+  return (R *)(S.arena + (code & kCodeOffMask) + ((code & kCodeUFlag) ? (int64_t)cur * S.ubuf : int64_t(0)));
+}
+__device__ __forceinline__ const int *op_prefix(const Dir &D, const SyncOp &op) {
+  if (op.kind == SYNC_COPY) return D.copy_prefix[op.arg][op.phase];
+  return op.arg ? D.aliasJ_prefix : D.aliasE_prefix;
 }
 
-// One sync phase (halo or owner copies) of group g for every active solve:
-// dst <- sign * src (MercuryBoundary::Sync_, Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110).
-__global__ void k_copy(Dir D, int g, int phase) {
-  const int *pre = D.copy_prefix[g][phase];
-  const int total = pre[D.nsolves];
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+// MercuryBoundary::Sync_ stages (Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110) and
+// ReduceEdgeAliasCandidatesToOwners_ (Z4_Mercury/src/physics/MercurySolver_Current.cpp:3-57)
+// for every active solve, up to two independent operations per launch.
+// Work unit: a group of 8 lanes.  A copy phase gives each group one segment
+// (dst <- sign * src on up to 8 consecutive elements); an alias reduction
+// gives each lane one class, whose members are summed in stored order from
+// 0.0 and written to the owner as owner_sign * sum / count.
+template <class R>
+__global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
+  const int lane = threadIdx.x & 7;
+  const int stride = (gridDim.x * blockDim.x) >> 3;
+  const int *pre0 = op_prefix(D, ops.op[0]);
+  const int *pre1 = ops.n > 1 ? op_prefix(D, ops.op[1]) : nullptr;
+  const int t0 = pre0[D.nsolves];
+  const int total = t0 + (pre1 ? pre1[D.nsolves] : 0);
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; g < total; g += stride) {
+    const bool second = g >= t0;
+    const SyncOp &op = second ? ops.op[1] : ops.op[0];
+    const int *pre = second ? pre1 : pre0;
+    const int e = second ? g - t0 : g;
     const int s = find_solve(pre, D.nsolves, e);
     if (!solve_active(D, s)) continue;
     const DevSolve &S = D.solves[s];
-    const DevTable &T = phase ? S.owner[g] : S.halo[g];
     const int q = e - pre[s];
     const int cur = D.state[s].cur;
-    *decode(S, cur, T.dst[q]) = T.sign[q] * *decode(S, cur, T.src[q]);
-  }
-}
-
-// ReduceEdgeAliasCandidatesToOwners_ (Z4_Mercury/src/physics/MercurySolver_Current.cpp:3-57):
-// one thread per class, members summed in stored order from 0.0.  which = 0: E, 1: J.
-__global__ void k_alias(Dir D, int which) {
-  const int *pre = which ? D.aliasJ_prefix : D.aliasE_prefix;
-  const int total = pre[D.nsolves];
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
-    const int s = find_solve(pre, D.nsolves, e);
-    if (!solve_active(D, s)) continue;
-    const DevSolve &S = D.solves[s];
-    const DevAlias &A = which ? S.aliasJ : S.aliasE;
-    const int q = e - pre[s];
-    const int cur = D.state[s].cur;
-    double sum = 0.0;
-    for (int m = A.offset[q]; m < A.offset[q + 1]; ++m) sum += A.msign[m] * *decode(S, cur, A.member[m]);
-    *decode(S, cur, A.owner[q]) = A.osign[q] * sum / (double)(A.offset[q + 1] - A.offset[q]);
+    if (op.kind == SYNC_COPY) {
+      const DevTable &T = op.phase ? S.owner[op.arg] : S.halo[op.arg];
+      const int64_t dcode = T.seg[2 * q], scode = T.seg[2 * q + 1];
+      const int len = (int)((dcode >> kSegLenShift) & 7) + 1;
+      if (lane < len) {
+        const R v = at_code<R>(S, cur, scode)[lane];
+        at_code<R>(S, cur, dcode)[lane] = ((dcode >> kSegNegBit) & 1) ? -v : v;
+      }
+    } else {
+      const DevAlias &A = op.arg ? S.aliasJ : S.aliasE;
+      const int c = q * 8 + lane;
+      if (c < A.n) {
+        R sum = R(0.0);
+        for (int m = A.offset[c]; m < A.offset[c + 1]; ++m) sum += R(A.msign[m]) * *at_code<R>(S, cur, A.member[m]);
+        *at_code<R>(S, cur, A.owner[c]) = R(A.osign[c]) * sum / (R)(A.offset[c + 1] - A.offset[c]);
+      }
+    }
   }
 }
 
@@ -881,31 +992,39 @@ static void grids() {
   g_grid_copy = sms * 8;
 }
 
-void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, int arg0, int arg1) {
-  grids();
+template <class R>
+static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops) {
   switch (k) {
-    case SK_FACE_EMF: k_face_emf<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_EDGE_EMF: k_edge_emf<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_HALL_CELL: k_hall_cell<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_HALL_EDGE: k_hall_edge<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_ADD_HALL: k_add_hall<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_FLUID: k_fluid<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_BFACE: k_bface<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_BCELL_JEDGE: k_bcell_jedge<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_JCELL: k_jcell<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_PV_UPLUS: k_pv_uplus<<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_COPY: k_copy<<<g_grid_copy, 256, 0, st>>>(D, arg0, arg1); break;
-    case SK_ALIAS: k_alias<<<g_grid_copy, 128, 0, st>>>(D, arg0); break;
+    case SK_FACE_EMF: k_face_emf<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_EDGE_EMF: k_edge_emf<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_HALL_CELL: k_hall_cell<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_HALL_EDGE: k_hall_edge<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_ADD_HALL: k_add_hall<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_FLUID: k_fluid<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_BFACE: k_bface<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_BCELL_JEDGE: k_bcell_jedge<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_JCELL: k_jcell<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_PV_UPLUS: k_pv_uplus<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_SYNC: k_sync<R><<<g_grid_copy, 256, 0, st>>>(D, *ops); break;
+    case SK_FACE_NORMALS: k_face_normals<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
     default: break;
   }
 }
 
+void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision) {
+  grids();
+  if (precision == kMixed)
+    launch_as<float>(k, D, st, ops);
+  else
+    launch_as<double>(k, D, st, ops);
+}
+
 const char *step_kernel_name(StepKernel k) {
   static const char *names[] = {"k_face_emf", "k_edge_emf", "k_hall_cell", "k_hall_edge", "k_add_hall",
                                 "k_fluid",    "k_bface",    "k_bcell_jedge", "k_jcell",   "k_pv_uplus",
-                                "k_copy",     "k_alias",    "k_flip",        "k_retire"};
+                                "k_sync",     "k_flip",     "k_retire",      "k_face_normals"};
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }
 

@@ -9,9 +9,9 @@ from mpcns_mercury_b200.capi import REF_FIELD
 NGHOST = 4
 
 
-def context_from_dump(dump, n, tag="step0:", cfl=0.4):
+def context_from_dump(dump, n, tag="step0:", cfl=0.4, precision=0):
     """Upload the reference's step-0 state and static inputs into a new context."""
-    ctx = Context([(n, n, n)], NGHOST, reference_constants(cfl=cfl))
+    ctx = Context([(n, n, n)], NGHOST, reference_constants(cfl=cfl), precision=precision)
     for name in mo.STATE_FIELDS:
         r = dump[(tag + name, 0)]
         ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
@@ -43,3 +43,19 @@ def compare(ctx, dump, tag, names, tol):
         worst[name] = mo.rel_l2(dev[sl], r.data[sl])
     bad = {k: v for k, v in worst.items() if not v <= tol}
     return worst, bad
+
+
+def div_b(ctx, n):
+    """max |sum of outward face fluxes| / max |B face| over the owned cells."""
+    g = NGHOST
+    lo = (-g, -g, -g)
+    B = []
+    for ax, name in enumerate(("B_XI", "B_ETA", "B_ZETA")):
+        hi = [n + g] * 3
+        hi[ax] += 1
+        B.append(ctx.download(name, lo, tuple(hi))[..., 0])
+    o = slice(g, g + n)
+    p = slice(g + 1, g + n + 1)
+    d = (B[0][p, o, o] - B[0][o, o, o]) + (B[1][o, p, o] - B[1][o, o, o]) + (B[2][o, o, p] - B[2][o, o, o])
+    scale = max(float(np.abs(b[o, o, o]).max()) for b in B)
+    return float(np.abs(d).max()) / scale
