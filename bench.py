@@ -2,26 +2,34 @@
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-Workloads (synthetic inputs generated here):
-  cube32   config 1: one periodic curvilinear 32^3 block, Orszag-Tang vortex on
+Workloads (synthetic inputs generated here, seeded):
+  ensemble (default)  64 independent periodic curvilinear boxes, cells per axis
+           log-uniform (x, y in [24, 64], z in [24, 128]), Orszag-Tang vortex on
            two ion fluids (H+, Na+ mass 1:23), Hall + electron pressure on,
-           resistivity off, CFL 0.4, FP64.
+           resistivity off, CFL 0.4.  ``value``: one mixed-precision batch (one
+           CUDA graph launch advances every solve by a step), K timed steps with
+           the state resident in HBM (inputs larger than L2).  Beside it: the
+           same solves one by one through the plain FP64 single-solve path, the
+           FP64 batch, and the mixed batch's relative L2 error against FP64.
+  serve    a seeded Poisson stream of requests (sizes from a pool of shapes of
+           the ensemble's distribution, 50-500 steps each) served by the
+           continuous-batching request loop (mixed precision) and one by one
+           through the plain FP64 path: throughput and p50/p99 latency.
+  cube32   one periodic curvilinear 32^3 block (the same physics), FP64 — the
+           reference's own single-block test case; cubeN: N^3.
 
 Metric: Mcell-updates/s = owned cells x steps / time (ghost cells are never
-counted; "per fluid" is the same count with n_fluids = 2).  ``value`` times K
-steps with the state resident in HBM (CUDA events on the solve's stream, L2
-flushed between steps because the 32^3 working set fits in L2); ``e2e`` is a
-full solve through the C ABI with host buffers: pinned-host uploads of every
-input field, mhd_prepare, K synchronous mhd_step calls each returning dt to the
-host, and the download of the final state.
+counted; "per fluid" is the same count with n_fluids = 2).  ``e2e`` is the
+same metric through the C ABI from host buffers, uploads and downloads
+included.
 
 With --gpus N > 1 (torchrun), each rank runs an independent replica of the
-workload (the single-block step has no data-path exchange); ``value`` is the
-sum of all replicas' cell updates over the max-over-ranks device time.
+workload (solves have no data-path exchange); ``value`` is the sum of all
+replicas' cell updates over the max-over-ranks device time.
 
 ``--impl reference`` times the reference's own CPU implementation (the
 reference solver compiled from its sources, oracle/_ref/mercury_ref) on a
-bounded sample of the same workload on this host; rank 0 only.
+bounded sample of the same workload on this host's cores; rank 0 only.
 """
 from __future__ import annotations
 
@@ -44,23 +52,30 @@ METRIC = "Mcell-updates/s batched vs plain on 1 B200 at stated error; p50/p99 la
 UNIT = "Mcell-updates/s"
 L2_BYTES = 126 * 1024 * 1024
 
-# Algorithmic HBM bytes per owned cell of each FP64 kernel: the distinct field
-# components it must read and write once per DOF (8 B each), as listed in
-# mpcns_mercury_b200/csrc/mhd_kernels.cu.  Kernels over the allocated cell
-# range count the allocated cells.
-KERNEL_BYTES_PER_CELL = {
-    "k_face_emf": 8 * (3 + 3 + 3 + 9),                      # B, Badd, UCON -> Eface
-    "k_edge_emf": 8 * (9 + 3 + 3 + 2 + 2 + 3),              # Eface, UCON, B, p_e x2, rho x2 -> E
-    "k_hall_cell": 8 * (2 + 3 + 3 + 3 + 1),                 # rho x2, J_cell, B_cell -> EHC, beta
-    "k_hall_edge": 8 * (3 + 1 + 9 + 3 + 3 + 3 + 3 + 3),     # EHC, beta, dr, dl, Area, B, taper -> Ehall
-    "k_add_hall": 8 * (3 + 3 + 3),                          # E += Ehall
-    "k_fluid": 8 * (10 + 10 + 9 + 1 + 3 + 3 + 3 + 1 + 3 + 10),  # U, PV, JD, Jac, U+, B_cell, J_cell, Photo, xyz -> U'
-    "k_bface": 8 * (3 + 3 + 3),                             # B += dt curl E
-    "k_bcell_jedge": 8 * (3 + 3 + 18 + 3 + 3 + 3 + 3 + 3),  # B, Badd, W_B, beta, alpha -> B_cell, Bind, J edges
-    "k_jcell": 8 * (3 + 36 + 3),                            # J edges, W_J -> J_cell
-    "k_pv_uplus": 8 * (10 + 1 + 9 + 3 + 10 + 3 + 3),        # U, Jac, JD, B_cell -> PV, U+, UCON (+ dt)
+# Algorithmic HBM traffic per owned cell of each step kernel: the distinct
+# field components it must read and write once per DOF, as (real-valued
+# components, metric components) — mpcns_mercury_b200/csrc/mhd_kernels.cu.
+# A real component is 8 B in FP64 and 4 B in mixed precision; the metric
+# (Jac, JD) is 8 B in both.  Kernels over the allocated cell range count the
+# allocated cells.
+KERNEL_COMPS = {
+    "k_face_emf": (3 + 3 + 3 + 9, 0),                        # B, Badd, UCON -> Eface
+    "k_edge_emf": (9 + 3 + 3 + 2 + 2 + 3, 0),                # Eface, UCON, B, p_e x2, rho x2 -> E
+    "k_hall_cell": (2 + 3 + 3 + 3 + 1, 0),                   # rho x2, J_cell, B_cell -> EHC, beta
+    "k_hall_edge": (3 + 1 + 9 + 3 + 3 + 3 + 3 + 3, 0),       # EHC, beta, dr, dl, Area, B, taper -> Ehall
+    "k_add_hall": (3 + 3 + 3, 0),                            # E += Ehall
+    "k_fluid": (10 + 10 + 3 + 3 + 3 + 3 + 1 + 3 + 10, 10),   # U, PV, |JD|, U+, B_cell, J_cell, Photo, xyz -> U'; Jac, JD
+    "k_bface": (3 + 3 + 3, 0),                               # B += dt curl E
+    "k_bcell_jedge": (3 + 3 + 18 + 3 + 3 + 3 + 3 + 3, 0),    # B, Badd, W_B, beta, alpha -> B_cell, Bind, J edges
+    "k_jcell": (3 + 36 + 3, 0),                              # J edges, W_J -> J_cell
+    "k_pv_uplus": (10 + 3 + 12 + 10 + 3 + 3, 10),            # U, B_cell, face normals -> PV, U+, UCON (+ dt); Jac, JD
 }
 ALLOCATED_RANGE_KERNELS = {"k_hall_cell", "k_pv_uplus"}
+
+
+def kernel_bytes_per_cell(name, precision):
+    real, metric = KERNEL_COMPS[name]
+    return real * (4 if precision == 1 else 8) + metric * 8
 
 
 def load_peaks():
@@ -127,13 +142,11 @@ def build_workload(name: str):
     """(cells per block, static+state fields {ref name: Arr}, topology kind)"""
     from mpcns_mercury_b200 import setup as S
 
-    if name == "cube32":
-        geom, f = S.cube_case(32)
-        return [(32, 32, 32)], [f], "config 1: periodic curvilinear 32^3 cube, Orszag-Tang, 2 ion fluids, Hall+p_e, FP64"
     if name.startswith("cube"):
         n = int(name[4:])
         geom, f = S.cube_case(n)
-        return [(n, n, n)], [f], f"config-1 physics on a periodic curvilinear {n}^3 cube (size study), FP64"
+        return [(n, n, n)], [f], (f"periodic curvilinear {n}^3 cube, Orszag-Tang on 2 ion fluids, Hall + p_e, "
+                                  "CFL 0.4, FP64")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -246,18 +259,18 @@ def profile_kernels(ctx, nsteps):
     return out
 
 
-def roofline(prof, cells, peak, peak_kind):
-    kernels = {k: v for k, v in prof.items() if k in KERNEL_BYTES_PER_CELL}
+def roofline(prof, cells, peak, peak_kind, precision=0, traffic_key=None):
+    kernels = {k: v for k, v in prof.items() if k in KERNEL_COMPS}
     if not kernels:
         return None
     top = max(kernels, key=kernels.get)
     g = 4
     ncell = sum((a + 2 * g) * (b + 2 * g) * (c + 2 * g) if top in ALLOCATED_RANGE_KERNELS else a * b * c
                 for a, b, c in cells)
-    algo_bytes = KERNEL_BYTES_PER_CELL[top] * ncell
+    algo_bytes = kernel_bytes_per_cell(top, precision) * ncell
     ms = kernels[top]
     achieved = algo_bytes / (ms * 1e-3) / 1e9
-    traffic = load_traffic(top)
+    traffic = load_traffic(traffic_key or top)
     return {"kernel": top, "bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_kind,
             "algo_bytes_per_launch": int(algo_bytes), "launch_ms": round(ms, 5),
@@ -309,43 +322,302 @@ def run_e2e(args, cells, fields, device):
             "wall_s": round(t1 - t0, 4)}
 
 
+# ------------------------------------------------------------------ ensemble (batched vs plain)
+def _owned_state(get, fields):
+    """Owned DOFs of the state fields, from get(name, lo, hi)."""
+    from mpcns_mercury_b200.workloads import STATE_FIELDS
+
+    out = {}
+    for name in STATE_FIELDS:
+        a = fields[name]
+        d = get(name, a.lo, a.hi)
+        g = [-v for v in a.lo]
+        out[name] = d[g[0]:a.hi[0], g[1]:a.hi[1], g[2]:a.hi[2]].copy()
+    return out
+
+
+def _rel_l2(a, b):
+    den = float(np.sqrt(np.sum(b * b)))
+    return float(np.sqrt(np.sum((a - b) ** 2))) / (den if den > 0 else 1.0)
+
+
+def _batch_step_profile(batch, nsteps):
+    import ctypes
+    from mpcns_mercury_b200.capi import check, lib
+
+    ms = (ctypes.c_float * 256)()
+    names = (ctypes.c_char_p * 256)()
+    n = ctypes.c_int()
+    check(lib().mhd_batch_step_profiled(batch.b, nsteps, 256, ms, names, ctypes.byref(n)), "mhd_batch_step_profiled")
+    out = {}
+    for q in range(n.value):
+        key = names[q].decode()
+        out[key] = out.get(key, 0.0) + ms[q]
+    return out
+
+
+def _timed_batch_steps(batch, steps, device):
+    """Device time (ms) of ``steps`` graph launches on the batch's stream."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(batch.stream(), device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_ensemble(args, rank, world, device):
+    """64 independent periodic-box solves of uneven sizes, advanced together by
+    one batch in mixed precision, against the same solves run one by one through
+    the plain FP64 single-solve path."""
+    import torch
+    from mpcns_mercury_b200 import Context, reference_constants
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.capi import Batch, SolveDesc
+
+    nsol = args.solves
+    sizes = W.ensemble_sizes(nsol)
+    base_id = rank * nsol
+    cells = [tuple(c) for c in sizes]
+    ncell = owned_cells(cells)
+    W_, K = args.warmup, args.steps
+    total_steps = W_ + K
+    k0 = reference_constants(cfl=0.4)
+    batches = {1: Batch(nsol, 1), 0: Batch(nsol, 0)}
+    slots = {1: [], 0: []}
+    t_api = {1: 0.0, 0: 0.0}   # host wall time of the batch's add/upload/sync/prepare calls
+    plain_ms = 0.0
+    plain_state = []
+    h2d_bytes = 0
+    for sid, fields in enumerate(W.generate_cases([(c, base_id + s) for s, c in enumerate(cells)])):
+        n = cells[sid]
+        for prec, b in batches.items():
+            t0 = time.perf_counter()
+            d = SolveDesc([n], 4, k0, precision=prec)
+            slot = b.add(d)
+            nb = W.upload_case(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk), fields)
+            b.sync(slot, "UCELL")
+            b.sync(slot, "BFACE")
+            b.prepare(slot)
+            b.request(slot, total_steps)
+            t_api[prec] += time.perf_counter() - t0
+            slots[prec].append(slot)
+            d.close()
+            if prec == 1:
+                h2d_bytes += nb
+        # plain FP64, this solve alone
+        ctx = Context([n], 4, k0)
+        W.upload_case(lambda f, a, lo, hi, blk: ctx.upload(f, a, lo, hi, block=blk), fields)
+        ctx.sync("UCELL")
+        ctx.sync("BFACE")
+        ctx.prepare()
+        ctx.step(W_)
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.step_async(K)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        ctx.synchronize()
+        plain_state.append((fields, _owned_state(lambda nm, lo, hi: ctx.download(W.capi_field(nm), lo, hi), fields)))
+        ctx.close()
+        del fields
+
+    # batched runs: W untimed launches, then K timed (inputs >> L2)
+    for prec, b in batches.items():
+        b.run(W_)
+        b.poll()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    if rank == 0:
+        sampler.start()
+    t_run0 = time.perf_counter()
+    mixed_ms = _timed_batch_steps(batches[1], K, device)
+    t_run_mixed = time.perf_counter() - t_run0
+    clocks = sampler.stop() if rank == 0 else None
+    fp64_ms = _timed_batch_steps(batches[0], K, device)
+    infos = {p: b.poll() for p, b in batches.items()}
+    for p in batches:
+        for s in slots[p]:
+            if infos[p][s].status != 0 or infos[p][s].step != total_steps:
+                raise RuntimeError(f"batch precision {p} slot {s}: status {infos[p][s].status} step {infos[p][s].step}")
+    if world > 1:
+        t = torch.tensor([mixed_ms, fp64_ms, plain_ms], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        mixed_ms, fp64_ms, plain_ms = (float(v) for v in t.tolist())
+
+    # errors: mixed batch vs plain FP64 (the FP64 path equals the reference bitwise),
+    # and FP64 batch vs plain FP64 (must be identical)
+    t_dl0 = time.perf_counter()
+    worst = {}
+    fp64_identical = True
+    d2h_bytes = 0
+    for sid, (fields, ref) in enumerate(plain_state):
+        got = _owned_state(lambda nm, lo, hi: batches[1].download(slots[1][sid], W.capi_field(nm), lo, hi), fields)
+        d2h_bytes += sum(v.nbytes for v in got.values())
+        for name in ref:
+            worst[name] = max(worst.get(name, 0.0), _rel_l2(got[name], ref[name]))
+        if sid < 8:  # the FP64 batch on a sample of solves
+            got64 = _owned_state(lambda nm, lo, hi: batches[0].download(slots[0][sid], W.capi_field(nm), lo, hi),
+                                 fields)
+            fp64_identical = fp64_identical and all(np.array_equal(got64[k], ref[k]) for k in ref)
+    t_dl = (time.perf_counter() - t_dl0) / 2
+
+    value = world * ncell * K / (mixed_ms * 1e-3) / 1e6
+    plain = world * ncell * K / (plain_ms * 1e-3) / 1e6
+    batched64 = world * ncell * K / (fp64_ms * 1e-3) / 1e6
+    for s_ in slots[1]:
+        batches[1].request(s_, 3)  # every solve active for the profiled steps
+    prof = _batch_step_profile(batches[1], 3)
+    peak, peak_kind = load_peaks()
+    roof = roofline(prof, cells, peak, peak_kind, precision=1, traffic_key="k_fluid_mixed_ensemble")
+    launches = batches[1].kernels_per_step()
+    # e2e: the mixed batch through the C ABI from host buffers: add + upload of
+    # every solve, prepare, W + K steps, download of every final state
+    e2e_s = t_api[1] + t_run_mixed * (W_ + K) / K + t_dl
+    for b in batches.values():
+        b.close()
+    cpu = cpu_baseline_sample(args, cells) if (rank == 0 and not args.no_cpu_baseline) else None
+    return {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W_,
+        "ms_per_step": round(mixed_ms / K, 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (metric f64)", "data": "synthetic",
+        "config": {"workload": "ensemble", "solves": nsol, "description":
+                   f"{nsol} independent periodic curvilinear boxes (Orszag-Tang, 2 ion fluids, Hall + p_e), "
+                   "cells per axis log-uniform x,y in [24,64], z in [24,128], one block each, seeded noise per "
+                   "solve; one batch, one CUDA graph launch per step advancing every solve",
+                   "cells_per_replica": ncell, "precision": "mixed: FP32 state/work/flux/EMF/update, FP64 Jac/JD",
+                   "l2": "inputs larger than L2 (not flushed)", "parallelism": f"replicas x{world}",
+                   "plain_fp64_one_by_one_mcells": round(plain, 3),
+                   "batched_fp64_mcells": round(batched64, 3),
+                   "batched_mixed_vs_plain_fp64": round(value / plain, 3),
+                   "batched_fp64_vs_plain_fp64": round(batched64 / plain, 3),
+                   "error_vs_fp64_rel_l2_max_over_solves": {k: float(f"{v:.3e}") for k, v in worst.items()},
+                   "error_steps": total_steps, "fp64_batch_bitwise_equal_plain": bool(fp64_identical)},
+        "roofline": roof, "cpu_baseline": cpu,
+        "e2e": {"value": round(world * ncell * (W_ + K) / e2e_s / 1e6, 3), "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d_bytes / (W_ + K)), "d2h_bytes_per_step": int(d2h_bytes / (W_ + K)),
+                "wall_s": round(e2e_s, 3),
+                "what": "mixed batch via the C ABI from pageable host arrays: add+upload+prepare of every solve, "
+                        "W+K steps, download of every final state"},
+        "gpu_launches": launches * K, "clocks": clocks,
+        "kernel_ms": {k: round(v, 5) for k, v in prof.items()},
+    }
+
+
+# ------------------------------------------------------------------ serving
+def run_serving(args, rank, world, device):
+    """Poisson request stream served by the continuous-batching server
+    (mixed precision) and, for comparison, one by one through the plain FP64
+    path."""
+    from mpcns_mercury_b200 import serving as SV
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.setup import Uniform
+
+    nreq = args.requests
+    shapes = W.ensemble_sizes(args.shapes, stream=200000 + rank)
+    pool = list(W.generate_cases([(c, 300000 + rank * 1000 + i) for i, c in enumerate(shapes)]))
+    u = Uniform(400000 + rank).sym(0.5, 3 * nreq) + 0.5
+    t = 0.0
+    reqs = []
+    for q in range(nreq):
+        t += -np.log(1.0 - u[3 * q]) / args.rate           # exponential inter-arrival times
+        shape = min(int(u[3 * q + 1] * args.shapes), args.shapes - 1)
+        steps = 50 + min(int(u[3 * q + 2] * 451), 450)      # 50 .. 500
+        reqs.append(SV.Request(rid=q, arrival_s=t, cells=tuple(shapes[shape]), steps=steps, fields=pool[shape]))
+    srv = SV.Server(capacity=args.capacity, precision=1, hbm_budget=args.hbm_budget)
+    batched = srv.serve(reqs)
+    srv.close()
+    for r in reqs:
+        r.done_s = float("nan")
+    plain = SV.serve_one_by_one(reqs, precision=0)
+    line = {
+        "metric": METRIC, "value": round(batched["mcell_updates_per_s"] * world, 3), "unit": UNIT, "n_gpus": world,
+        "steps": int(sum(r.steps for r in reqs)), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (metric f64)", "data": "synthetic",
+        "config": {"workload": "serve", "requests": nreq, "arrival_rate_per_s": args.rate, "shapes": args.shapes,
+                   "capacity": args.capacity, "hbm_budget_bytes": args.hbm_budget,
+                   "batched_mixed": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in batched.items()},
+                   "plain_fp64_one_by_one": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in plain.items()},
+                   "latency_p50_s": round(batched["latency_p50_s"], 4),
+                   "latency_p99_s": round(batched["latency_p99_s"], 4)},
+        "roofline": None, "cpu_baseline": None,
+        "e2e": {"value": round(batched["mcell_updates_per_s"] * world, 3), "unit": UNIT,
+                "what": "wall clock of the whole request loop, uploads and downloads included"},
+    }
+    return line
+
+
 # ------------------------------------------------------------------ reference arm
-def reference_workload_job(workload):
+def reference_cubes(args):
+    """Cubes (cells per axis) the reference build runs for a bounded sample of
+    ``args.workload``: the workload's own cube, or, for the ensemble and the
+    request stream, the cube of the same cell count for each of the first
+    members (the reference's test case generator builds cubes; its cost per
+    cell-step does not depend on the aspect ratio)."""
+    from mpcns_mercury_b200 import workloads as W
+
+    if args.workload == "cube32":
+        return [32]
+    if args.workload.startswith("cube"):
+        return [int(args.workload[4:])]
+    if args.workload == "ensemble":
+        sizes = W.ensemble_sizes(args.solves)
+    elif args.workload == "serve":
+        sizes = W.ensemble_sizes(args.shapes, stream=200000)
+    else:
+        raise SystemExit(f"unknown workload {args.workload}")
+    return [max(8, int(round((a * b * c) ** (1.0 / 3.0)))) for a, b, c in sizes]
+
+
+def run_reference_steps(n, steps):
+    """Run the reference build on the n^3 cube for ``steps`` steps; returns
+    (seconds spent in StepOnce, cells)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mercury_oracle as mo
 
-    if workload == "cube32":
-        job = dict(mo.CUBE_JOB)
-        job.update(n=32)
-        return job, 32 ** 3
-    raise SystemExit(f"unknown workload {workload}")
-
-
-def run_reference_steps(workload, steps):
-    """Run the reference build for ``steps`` steps; returns (seconds in StepOnce, cells)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import mercury_oracle as mo
-
-    job, cells = reference_workload_job(workload)
-    job.update(steps=steps, dump_fields="U_H", dump_at=str(steps))
+    job = dict(mo.CUBE_JOB)
+    job.update(n=n, steps=steps, dump_fields="U_H", dump_at=str(steps))
     d = mo.run_job(job, timeout=1800)
     secs, nsteps, ncell = d[("timing", -1)].data.ravel()
     return float(secs), int(ncell)
 
 
-def cpu_baseline_sample(args):
+def reference_sample(args, steps):
+    """The reference on the host cores: one single-rank process per core, each
+    on one member cube of the workload, run concurrently.  Returns (aggregate
+    Mcell-updates/s = sum of the processes' own rates, processes, description)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    cubes = reference_cubes(args)
+    procs = min(len(cubes), max(1, os.cpu_count() or 1))
+    cubes = cubes[:procs]
+    with ThreadPoolExecutor(max_workers=procs) as ex:
+        res = list(ex.map(lambda n: run_reference_steps(n, steps), cubes))
+    rate = sum(c * steps / secs for secs, c in res) / 1e6
+    desc = (f"{args.workload}: {procs} concurrent single-rank reference processes (oracle/_ref, built from the "
+            f"reference sources), cubes {cubes}, {steps} StepOnce calls each, setup excluded")
+    return rate, procs, desc
+
+
+def cpu_baseline_sample(args, cells=None):
     """The reference (built from its sources) on the host: a bounded sample of
-    the same workload, single core (the reference has one thread per rank)."""
+    the same workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mercury_oracle as mo
 
     if not mo.available():
         return None
-    steps = args.cpu_sample_steps
-    secs, ncell = run_reference_steps(args.workload, steps)
-    return {"value": round(ncell * steps / secs / 1e6, 4), "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"{args.workload}: {steps} StepOnce calls of the reference build (oracle/_ref), "
-                      f"setup excluded, 1 core"}
+    rate, procs, desc = reference_sample(args, args.cpu_sample_steps)
+    return {"value": round(rate, 4), "unit": UNIT, "cores": procs, "kind": "reference", "sample": desc}
 
 
 def run_reference(args, rank, world):
@@ -356,24 +628,26 @@ def run_reference(args, rank, world):
         return None
     if not mo.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/mercury_ref is not built on this host"}
-    total, cells = 0.0, 0
     steps = args.cpu_sample_steps
-    for _ in range(max(1, args.warmup // 3)):
-        run_reference_steps(args.workload, 1)
-    times = []
-    for _ in range(args.steps):
-        secs, cells = run_reference_steps(args.workload, steps)
-        times.append(secs)
-        total += secs
-    value = cells * steps * args.steps / total / 1e6
-    desc = {"workload": args.workload, "steps_per_sample": steps,
-            "implementation": "reference solver compiled from its own sources, single rank, 1 thread"}
+    run_reference_steps(8, 1)  # warm the binary and the file cache
+    # each sample restarts the reference (its setup is not timed); a few
+    # samples keep the whole run within minutes
+    samples = max(1, min(args.steps, 3))
+    rates = []
+    t0 = time.perf_counter()
+    for _ in range(samples):
+        rate, procs, desc = reference_sample(args, steps)
+        rates.append(rate)
+    wall = time.perf_counter() - t0
+    value = float(np.mean(rates))
     return {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * total / (args.steps * steps), 4),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / samples, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": desc,
-            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": 1, "kind": "reference",
-                             "sample": f"{args.steps} x {steps} StepOnce calls"},
+            "config": {"workload": args.workload, "steps_per_sample": steps, "samples": samples,
+                       "implementation": "reference solver compiled from its own sources, single rank per process, "
+                                         f"{procs} processes"},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": procs, "kind": "reference",
+                             "sample": desc},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -381,10 +655,16 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="cube32")
+    ap.add_argument("--workload", default="ensemble", help="ensemble (default), serve, cube32, cubeN")
+    ap.add_argument("--solves", type=int, default=64, help="ensemble: solves per GPU")
+    ap.add_argument("--requests", type=int, default=400, help="serve: requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: mean arrivals per second")
+    ap.add_argument("--shapes", type=int, default=16, help="serve: distinct request shapes")
+    ap.add_argument("--capacity", type=int, default=64, help="serve: batch slots")
+    ap.add_argument("--hbm-budget", type=float, default=100e9, help="serve: device bytes for admitted solves")
     ap.add_argument("--cpu-sample-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -411,7 +691,12 @@ def main():
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        line = run_ours(args, rank, world, device)
+        if args.workload == "ensemble":
+            line = run_ensemble(args, rank, world, device)
+        elif args.workload == "serve":
+            line = run_serving(args, rank, world, device)
+        else:
+            line = run_ours(args, rank, world, device)
     finally:
         if world > 1:
             torch.distributed.destroy_process_group()

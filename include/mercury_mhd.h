@@ -41,7 +41,8 @@ enum mhd_status {
   MHD_ERR_DT = 4,       /* dt non-finite or below 1e-7 (reference aborts) */
   MHD_ERR_NONFINITE = 5,/* non-finite state detected */
   MHD_ERR_SOLVE = 6,    /* implicit solve did not converge */
-  MHD_ERR_STATE = 7     /* call out of order (e.g. step before prepare) */
+  MHD_ERR_STATE = 7,    /* call out of order (e.g. step before prepare) */
+  MHD_ERR_TIMEOUT = 8   /* a device-side wait exceeded its iteration limit */
 };
 
 /* Field identifiers: the reference's catalog names

@@ -99,8 +99,8 @@ struct Solve {
   DevBlock *dblocks = nullptr;
   int *dtile_prefix[kNumRanges] = {};
   int tiles[kNumRanges] = {};
-  int64_t *tab_seg[kMaxGroups][2] = {};
-  int tab_n[kMaxGroups][2] = {};  // segments
+  int64_t *tab_seg[kMaxGroups][3] = {};
+  int tab_n[kMaxGroups][3] = {};  // segments; phase 0 halo (step depth), 1 owner, 2 halo (all)
   int32_t *al_off = nullptr;
   int64_t *al_memE = nullptr, *al_ownE = nullptr, *al_memJ = nullptr, *al_ownJ = nullptr;
   double *al_msign = nullptr, *al_osign = nullptr;
@@ -145,7 +145,7 @@ struct mhd_batch {
   DevSolve *dsolves = nullptr;
   SolveState *dstate = nullptr;
   int *dprefix_tiles[kNumRanges] = {};
-  int *dprefix_copy[kMaxGroups][2] = {};
+  int *dprefix_copy[kMaxGroups][3] = {};
   int *dprefix_aliasE = nullptr, *dprefix_aliasJ = nullptr;
   cudaGraphExec_t graph = nullptr;
   int kernels_per_step = 0;
@@ -167,7 +167,7 @@ struct mhd_batch {
     d.mode = mode;
     for (int r = 0; r < kNumRanges; ++r) d.solve_tile_prefix[r] = dprefix_tiles[r];
     for (int g = 0; g < kMaxGroups; ++g)
-      for (int p = 0; p < 2; ++p) d.copy_prefix[g][p] = dprefix_copy[g][p];
+      for (int p = 0; p < 3; ++p) d.copy_prefix[g][p] = dprefix_copy[g][p];
     d.aliasE_prefix = dprefix_aliasE;
     d.aliasJ_prefix = dprefix_aliasJ;
     return d;
@@ -212,9 +212,10 @@ void sync2(mhd_batch *b, int mode, SyncOp a, SyncOp c, int *nk) {
 }
 
 // MercuryBoundary::Sync(group) (Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110):
-// the group's halo copies, then its owner copies.
-void enqueue_sync(mhd_batch *b, int mode, int g, int *nk) {
-  sync1(b, mode, copy_op(g, 0), nk);
+// the group's halo copies, then its owner copies.  full: every ghost layer
+// (mhd_sync); otherwise the layers the step reads (kHaloDepth).
+void enqueue_sync(mhd_batch *b, int mode, int g, int *nk, bool full = false) {
+  sync1(b, mode, copy_op(g, full ? 2 : 0), nk);
   sync1(b, mode, copy_op(g, 1), nk);
 }
 
@@ -282,7 +283,7 @@ int publish(mhd_batch *b) {
   for (int r = 0; r < kNumRanges; ++r)
     if ((rc = put(b->dprefix_tiles[r], [&](const Solve *S) { return S->tiles[r]; }))) return rc;
   for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 3; ++p)
       if ((rc = put(b->dprefix_copy[g][p], [&](const Solve *S) { return S->tab_n[g][p]; }))) return rc;
   if ((rc = put(b->dprefix_aliasE, [](const Solve *S) { return (S->al_n + 7) / 8; }))) return rc;
   if ((rc = put(b->dprefix_aliasJ, [](const Solve *S) { return (S->al_n + 7) / 8; }))) return rc;
@@ -302,6 +303,7 @@ int publish(mhd_batch *b) {
     for (int g = 0; g < kMaxGroups; ++g) {
       d.halo[g] = DevTable{S->tab_seg[g][0], S->tab_n[g][0]};
       d.owner[g] = DevTable{S->tab_seg[g][1], S->tab_n[g][1]};
+      d.halo_full[g] = DevTable{S->tab_seg[g][2], S->tab_n[g][2]};
     }
     d.aliasE = DevAlias{S->al_off, S->al_memE, S->al_msign, S->al_ownE, S->al_osign, S->al_n};
     d.aliasJ = DevAlias{S->al_off, S->al_memJ, S->al_msign, S->al_ownJ, S->al_osign, S->al_n};
@@ -317,21 +319,52 @@ int publish(mhd_batch *b) {
 // Destinations of one phase are distinct and no copy of a phase reads a
 // value the phase writes, so the order of application does not change the
 // result.  Signs must be +1 or -1 (orientation flips).
-int upload_copies(Solve *S, const mhd_copy *tab, int n, int g, int phase, cudaStream_t st) {
+// Ghost depth each group's halo is filled to inside the step: the farthest
+// ghost layer any kernel of the step reads it at (U and the face fluxes: the
+// face EMF candidates and contravariant velocities two layers out; B_cell and
+// J_cell: the Hall cell field one layer out; E, E_Hall and J edges are read
+// only at owned and alias positions).  Explicit syncs (mhd_sync) fill every
+// layer.
+constexpr int kHaloDepth[MHD_NUM_GROUPS] = {2, 2, 0, 0, 1, 0, 1};
+
+// Ghost depth of a DOF: how far outside its owned range [0, n + stagger) it lies.
+int dof_depth(const Solve *S, const mhd_dof &d) {
+  const Box &bx = S->boxes[d.block];
+  const int *st = kStagger[kFieldSpec[d.field].loc];
+  const int q[3] = {d.i, d.j, d.k};
+  int depth = 0;
+  for (int a = 0; a < 3; ++a) {
+    const int hi = bx.n[a] + st[a];
+    const int da = q[a] < 0 ? -q[a] : (q[a] >= hi ? q[a] - hi + 1 : 0);
+    depth = da > depth ? da : depth;
+  }
+  return depth;
+}
+
+// max_depth < 0: every entry; otherwise only entries whose destination lies
+// at most max_depth ghost layers out.
+int upload_copies(Solve *S, const mhd_copy *tab, int n, int g, int phase, cudaStream_t st, int max_depth = -1) {
   if (n < 0 || (n > 0 && !tab)) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, phase);
-  std::vector<int64_t> dst(n), src(n);
-  std::vector<int> order(n);
-  std::vector<char> neg(n);
+  std::vector<int64_t> dst, src;
+  std::vector<char> neg;
+  dst.reserve(n);
+  src.reserve(n);
+  neg.reserve(n);
   for (int t = 0; t < n; ++t) {
     bool o1, o2;
-    dst[t] = S->code(tab[t].dst, &o1);
-    src[t] = S->code(tab[t].src, &o2);
+    const int64_t dc = S->code(tab[t].dst, &o1);
+    const int64_t sc = S->code(tab[t].src, &o2);
     if (!o1 || !o2) return fail(MHD_ERR_ARG, "group %d phase %d: entry %d out of range", g, phase, t);
     if (tab[t].sign != 1.0 && tab[t].sign != -1.0)
       return fail(MHD_ERR_ARG, "group %d phase %d: entry %d has sign %g (must be +1 or -1)", g, phase, t, tab[t].sign);
-    neg[t] = tab[t].sign < 0.0;
-    order[t] = t;
+    if (max_depth >= 0 && dof_depth(S, tab[t].dst) > max_depth) continue;
+    dst.push_back(dc);
+    src.push_back(sc);
+    neg.push_back(tab[t].sign < 0.0);
   }
+  n = (int)dst.size();
+  std::vector<int> order(n);
+  for (int t = 0; t < n; ++t) order[t] = t;
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return dst[a] < dst[c]; });
   std::vector<int64_t> seg;
   seg.reserve(2 * (size_t)n);
@@ -410,7 +443,7 @@ void free_solve(Solve *S, cudaStream_t st) {
   f(S->dblocks);
   for (int r = 0; r < kNumRanges; ++r) f(S->dtile_prefix[r]);
   for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 2; ++p) {
+    for (int p = 0; p < 3; ++p) {
       f(S->tab_seg[g][p]);
     }
   for (void *p : {(void *)S->al_off, (void *)S->al_memE, (void *)S->al_ownE, (void *)S->al_memJ, (void *)S->al_ownJ,
@@ -518,7 +551,7 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
   for (int r = 0; r < kNumRanges; ++r)
     if (cudaMalloc(&b->dprefix_tiles[r], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
   for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 3; ++p)
       if (cudaMalloc(&b->dprefix_copy[g][p], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
   if (cudaMalloc(&b->dprefix_aliasE, sizeof(int) * C1) != cudaSuccess ||
       cudaMalloc(&b->dprefix_aliasJ, sizeof(int) * C1) != cudaSuccess)
@@ -545,7 +578,7 @@ int mhd_batch_destroy(mhd_batch *b) {
   if (b->hstate) cudaFreeHost(b->hstate);
   for (int r = 0; r < kNumRanges; ++r) cudaFree(b->dprefix_tiles[r]);
   for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 2; ++p) cudaFree(b->dprefix_copy[g][p]);
+    for (int p = 0; p < 3; ++p) cudaFree(b->dprefix_copy[g][p]);
   cudaFree(b->dprefix_aliasE);
   cudaFree(b->dprefix_aliasJ);
   for (auto e : b->prof_events) cudaEventDestroy(e);
@@ -573,8 +606,8 @@ int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
 }
 
 int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
-  if (!b || !desc || !slot_out || desc->n_blocks < 1 || !desc->cells || desc->nghost < 1)
-    return fail(MHD_ERR_ARG, "mhd_batch_add: bad descriptor");
+  if (!b || !desc || !slot_out || desc->n_blocks < 1 || !desc->cells) return fail(MHD_ERR_ARG, "mhd_batch_add: bad descriptor");
+  if (desc->nghost < 2) return fail(MHD_ERR_ARG, "mhd_batch_add: nghost %d (the step's stencils need >= 2)", desc->nghost);
   if (desc->precision != b->precision)
     return fail(MHD_ERR_ARG, "solve precision %d differs from the batch's (%d)", desc->precision, b->precision);
   if (desc->n_blocks >= (1 << 15)) return fail(MHD_ERR_ARG, "too many blocks (%d)", desc->n_blocks);
@@ -648,8 +681,9 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
     if ((rc = dev_upload(prefix[r], &S->dtile_prefix[r], st))) return bail(rc);
   }
   for (int g = 0; g < MHD_NUM_GROUPS; ++g) {
-    if ((rc = upload_copies(S, desc->groups[g].halo, desc->groups[g].n_halo, g, 0, st))) return bail(rc);
+    if ((rc = upload_copies(S, desc->groups[g].halo, desc->groups[g].n_halo, g, 0, st, kHaloDepth[g]))) return bail(rc);
     if ((rc = upload_copies(S, desc->groups[g].owner, desc->groups[g].n_owner, g, 1, st))) return bail(rc);
+    if ((rc = upload_copies(S, desc->groups[g].halo, desc->groups[g].n_halo, g, 2, st))) return bail(rc);
   }
   if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
   SolveState s0{};
@@ -731,7 +765,7 @@ int mhd_batch_sync(mhd_batch *b, int slot, int group) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
   if (group < 0 || group >= MHD_NUM_GROUPS) return fail(MHD_ERR_ARG, "mhd_sync: bad group %d", group);
-  rc = targeted(b, slot, [&](int *nk) { enqueue_sync(b, 1, group, nk); });
+  rc = targeted(b, slot, [&](int *nk) { enqueue_sync(b, 1, group, nk, true); });
   if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(b->stream));
   return MHD_OK;

@@ -20,12 +20,19 @@ enum RangeKind : int {
   kCells = 0,    // owned cells [0, n)
   kBox = 1,      // [0, n + 1): owned faces and edges of all families
   kExt = 2,      // [-1, n + 2): face EMF candidates incl. one ghost layer
-  kAlloc = 3,    // [-g, n + g): allocated cell range
+  kAlloc = 3,    // [-gs, n + gs), gs = min(nghost, kStepGhost): the ghost cells the step maintains
   kCells2 = 4,   // owned cells, two work items per tile (one per ion species)
   kNumRanges = 5
 };
 
 constexpr int kTileK = 32, kTileJ = 4, kTileI = 2, kTileThreads = kTileK * kTileJ * kTileI;
+
+// Ghost depth the step keeps valid between its passes: the widest stencil
+// reach of its kernels (face EMF candidates on [-1, n + 2) read contravariant
+// velocities and face fluxes two layers out).  The step's halo copies stop at
+// the depth each group's readers need (kHaloDepth); explicit syncs fill all
+// ghost layers.
+constexpr int kStepGhost = 2;
 
 // Precision of a batch: every component array holds `real` values (double
 // or float) except the metric (Jac and the face area vectors JD), which is
@@ -120,7 +127,7 @@ struct DevSolve {
   int64_t ubuf;                       // bytes per U buffer
   int nblocks;
   const int *tile_prefix[kNumRanges]; // per range: nblocks + 1 prefix sums of tile counts
-  DevTable halo[kMaxGroups], owner[kMaxGroups];
+  DevTable halo[kMaxGroups], owner[kMaxGroups], halo_full[kMaxGroups];
   DevAlias aliasE, aliasJ;
 };
 
@@ -131,9 +138,10 @@ struct Dir {
   int nsolves;
   int mode;  // 0: solves with remaining steps (the step); 1: solves with mask set (prepare, sync)
   const int *solve_tile_prefix[kNumRanges];  // nsolves + 1 per range
-  // sync tables: per group and phase (0 halo, 1 owner) prefix sums over the
-  // solves of their segment counts; alias tables: of their 8-class groups
-  const int *copy_prefix[kMaxGroups][2];
+  // sync tables: per group and phase (0 halo to the step's depth, 1 owner,
+  // 2 every halo copy) prefix sums over the solves of their segment counts;
+  // alias tables: of their 8-class groups
+  const int *copy_prefix[kMaxGroups][3];
   const int *aliasE_prefix, *aliasJ_prefix;
 };
 
@@ -160,7 +168,12 @@ __host__ __device__ inline RangeBox range_of(int kind, const int n[3], int g) {
       case kCells2: r.lo[a] = 0; r.hi[a] = n[a]; break;
       case kBox: r.lo[a] = 0; r.hi[a] = n[a] + 1; break;
       case kExt: r.lo[a] = -1; r.hi[a] = n[a] + 2; break;
-      default: r.lo[a] = -g; r.hi[a] = n[a] + g; break;
+      default: {
+        const int gs = g < kStepGhost ? g : kStepGhost;
+        r.lo[a] = -gs;
+        r.hi[a] = n[a] + gs;
+        break;
+      }
     }
   }
   return r;

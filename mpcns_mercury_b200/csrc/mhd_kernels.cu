@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
         up[q] = d.chiH * uH + d.chiNa * uN;
         AT(cUP + q, i, j, k) = up[q];
       }
-      const int gm = c.nghost - 1;
+      const int gm = min(c.nghost - 1, kStepGhost);
       if (i >= -gm && i < B.n0 + gm && j >= -gm && j < B.n1 + gm && k >= -gm && k < B.n2 + gm) {
         const R inv_jac = R(1.0) / (fabs(R(ATM(cJAC, i, j, k))) + R(1.0e-30));
         for (int axis = 0; axis < 3; ++axis) {
@@ -931,7 +931,7 @@ __global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
     const int q = e - pre[s];
     const int cur = D.state[s].cur;
     if (op.kind == SYNC_COPY) {
-      const DevTable &T = op.phase ? S.owner[op.arg] : S.halo[op.arg];
+      const DevTable &T = op.phase == 1 ? S.owner[op.arg] : op.phase == 2 ? S.halo_full[op.arg] : S.halo[op.arg];
       const int64_t dcode = T.seg[2 * q], scode = T.seg[2 * q + 1];
       const int len = (int)((dcode >> kSegLenShift) & 7) + 1;
       if (lane < len) {

@@ -17,7 +17,7 @@ enum SyncKind { SYNC_COPY = 0, SYNC_ALIAS = 1 };
 struct SyncOp {
   int kind;   // SyncKind
   int arg;    // SYNC_COPY: group; SYNC_ALIAS: 0 = E, 1 = J
-  int phase;  // SYNC_COPY: 0 halo, 1 owner
+  int phase;  // SYNC_COPY: 0 halo copies to the step's depth, 1 owner copies, 2 every halo copy
 };
 struct SyncOps {
   SyncOp op[2];

@@ -1,0 +1,166 @@
+"""Request loop over a batch (mhd_batch): independent solves arrive over time,
+are admitted while a slot and device memory are free, run together on one
+CUDA graph per step (continuous batching: a solve joins or leaves between
+graph launches while the others keep running), and leave when their steps
+are done.  The reference runs one solve per MPI job and has no counterpart;
+this is the serving layer around the step.
+
+    server = Server(capacity=64, precision=1, hbm_budget=100e9)
+    stats = server.serve(requests)      # requests: arrival times, sizes, steps
+    stats["latency_p50_s"], stats["latency_p99_s"], stats["mcell_updates_per_s"]
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+from .constants import reference_constants
+from .workloads import NGHOST, STATE_FIELDS, capi_field, upload_case
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival_s: float          # seconds after the start of serving
+    cells: tuple              # cells per axis of the (single, periodic) block
+    steps: int
+    fields: dict              # {reference field name: Arr} inputs (static + initial state)
+    keep_result: bool = False
+    # filled in by the server
+    admitted_s: float = float("nan")
+    done_s: float = float("nan")
+    result: dict = field(default_factory=dict)
+    slot: int = -1
+
+
+def percentile(values, q):
+    return float(np.percentile(np.asarray(values, dtype=np.float64), q)) if len(values) else float("nan")
+
+
+class Server:
+    """Continuous-batching server of independent solves on one GPU."""
+
+    def __init__(self, capacity: int = 64, precision: int = 1, hbm_budget: float = 100e9, chunk_steps: int = 8,
+                 cfl: float = 0.4):
+        self.batch = capi.Batch(capacity, precision)
+        self.capacity = capacity
+        self.precision = precision
+        self.hbm_budget = float(hbm_budget)
+        self.chunk = int(chunk_steps)
+        self.constants = reference_constants(cfl=cfl)
+
+    def close(self):
+        self.batch.close()
+
+    # ------------------------------------------------------------------ one solve
+    def _admit(self, req: Request) -> int:
+        d = capi.SolveDesc([req.cells], NGHOST, self.constants, precision=self.precision)
+        slot = self.batch.add(d)
+        upload_case(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b), req.fields)
+        self.batch.sync(slot, "UCELL")
+        self.batch.sync(slot, "BFACE")
+        self.batch.prepare(slot)
+        self.batch.request(slot, req.steps)
+        req.slot = slot
+        d.close()
+        return slot
+
+    def _retire(self, req: Request):
+        if req.keep_result:
+            req.result = {name: self.batch.download(req.slot, capi_field(name), req.fields[name].lo,
+                                                    req.fields[name].hi) for name in STATE_FIELDS}
+        self.batch.remove(req.slot)
+
+    @staticmethod
+    def _bytes(req: Request, precision: int) -> int:
+        d = capi.SolveDesc([req.cells], NGHOST, reference_constants(), precision=precision)
+        b = d.device_bytes()
+        d.close()
+        return b
+
+    # ------------------------------------------------------------------ the loop
+    def serve(self, requests, clock=time.perf_counter):
+        """Serve ``requests`` (sorted by arrival) in real time; returns statistics."""
+        pending = sorted(requests, key=lambda r: r.arrival_s)
+        need = {r.rid: self._bytes(r, self.precision) for r in pending}
+        running: dict[int, Request] = {}
+        remaining: dict[int, int] = {}
+        used = 0
+        t0 = clock()
+        nxt = 0
+        graph_steps = 0
+        while nxt < len(pending) or running:
+            now = clock() - t0
+            # admission: arrived requests, in arrival order, while a slot and memory are free
+            while (nxt < len(pending) and pending[nxt].arrival_s <= now and len(running) < self.capacity
+                   and used + need[pending[nxt].rid] <= self.hbm_budget):
+                r = pending[nxt]
+                r.admitted_s = clock() - t0
+                self._admit(r)
+                running[r.slot] = r
+                remaining[r.slot] = r.steps
+                used += need[r.rid]
+                nxt += 1
+            if not running:
+                # idle until the next arrival
+                wait = pending[nxt].arrival_s - (clock() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.05))
+                continue
+            # advance every running solve by up to `chunk` steps, stopping at the
+            # first completion (graph launches are asynchronous; the poll synchronises)
+            n = max(1, min(self.chunk, min(remaining.values())))
+            self.batch.run(n)
+            graph_steps += n
+            infos = self.batch.poll()
+            now = clock() - t0
+            for slot in list(running):
+                inf = infos[slot]
+                if inf.status != 0:
+                    raise capi.MhdError(inf.status, f"request {running[slot].rid} (slot {slot})")
+                remaining[slot] = int(inf.remaining)
+                if inf.remaining == 0:
+                    r = running.pop(slot)
+                    del remaining[slot]
+                    r.done_s = now
+                    self._retire(r)
+                    used -= need[r.rid]
+        makespan = clock() - t0
+        lat = [r.done_s - r.arrival_s for r in pending]
+        work = sum(int(np.prod(r.cells)) * r.steps for r in pending)
+        return {"requests": len(pending), "makespan_s": makespan, "graph_steps": graph_steps,
+                "cell_updates": work, "mcell_updates_per_s": work / makespan / 1e6,
+                "latency_p50_s": percentile(lat, 50), "latency_p99_s": percentile(lat, 99),
+                "latency_mean_s": float(np.mean(lat)) if lat else float("nan")}
+
+
+def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl: float = 0.4):
+    """The same requests served first-come first-served through the plain
+    single-solve path (mhd_ctx, one solve on the GPU at a time)."""
+    pending = sorted(requests, key=lambda r: r.arrival_s)
+    t0 = clock()
+    for r in pending:
+        now = clock() - t0
+        if r.arrival_s > now:
+            time.sleep(r.arrival_s - now)
+        r.admitted_s = clock() - t0
+        ctx = capi.Context([r.cells], NGHOST, reference_constants(cfl=cfl), precision=precision)
+        upload_case(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), r.fields)
+        ctx.sync("UCELL")
+        ctx.sync("BFACE")
+        ctx.prepare()
+        ctx.step(r.steps)
+        if r.keep_result:
+            r.result = {name: ctx.download(capi_field(name), r.fields[name].lo, r.fields[name].hi)
+                        for name in STATE_FIELDS}
+        ctx.close()
+        r.done_s = clock() - t0
+    makespan = clock() - t0
+    lat = [r.done_s - r.arrival_s for r in pending]
+    work = sum(int(np.prod(r.cells)) * r.steps for r in pending)
+    return {"requests": len(pending), "makespan_s": makespan, "cell_updates": work,
+            "mcell_updates_per_s": work / makespan / 1e6, "latency_p50_s": percentile(lat, 50),
+            "latency_p99_s": percentile(lat, 99), "latency_mean_s": float(np.mean(lat)) if lat else float("nan")}

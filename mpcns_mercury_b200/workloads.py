@@ -67,3 +67,26 @@ def ensemble_sizes(nsolves: int, stream: int = 100000):
         sizes.append((int(round(math.exp(lo + a * (hx - lo)))), int(round(math.exp(lo + b * (hx - lo)))),
                       int(round(math.exp(lo + c * (hz - lo))))))
     return sizes
+
+
+def _case_worker(spec):
+    cells, solve_id = spec
+    return case_fields(cells, solve_id=solve_id)
+
+
+def generate_cases(specs, workers: int | None = None):
+    """Yields case_fields(cells, solve_id) for every (cells, solve_id) in
+    ``specs``, in order, computed by a pool of spawned host processes (safe to
+    start after CUDA is initialised in this process)."""
+    import multiprocessing as mp
+    import os
+    from concurrent.futures import ProcessPoolExecutor
+
+    specs = list(specs)
+    workers = workers or min(len(specs), max(1, (os.cpu_count() or 2) - 1), 32)
+    if workers <= 1 or len(specs) <= 1:
+        for sp in specs:
+            yield _case_worker(sp)
+        return
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        yield from ex.map(_case_worker, specs)

@@ -114,7 +114,7 @@ STATIC_FIELDS = ["Jac", "JDxi", "JDet", "JDze", "Area_xi", "Area_eta", "Area_zet
 
 
 def cube_run(n=32, steps=100, dump_at=None, extra=None, workdir=None):
-    """Run config 1 (or a smaller cube) on the reference build.
+    """Run the periodic curvilinear Orszag-Tang cube (32^3, or another n) on the reference build.
 
     Returns the dump: ``static:<name>`` (block 0) for the static inputs and the
     Hall taper, grid arrays, and ``step<k>:<name>`` for state + derived + work

@@ -1,7 +1,7 @@
 """Generates tests/golden/cube6_ot_5steps.npz from the reference built from
 its own sources (oracle/_ref): the static inputs, grid cell centres, the
 step-0 state and derived fields, and the state after 5 steps of a periodic
-6^3 curvilinear cube (the config-1 case at a small size).
+6^3 curvilinear cube (the periodic Orszag-Tang cube at a small size).
 
     python tests/golden/make_golden.py
 """

@@ -1,6 +1,6 @@
 """Mixed precision (FP32 state, work fields and flux/EMF/update arithmetic;
-FP64 metric Jac/JD) against the reference's FP64 step, on the config-1 case
-(periodic curvilinear 32^3 cube, Orszag-Tang, 100 steps).
+FP64 metric Jac/JD) against the reference's FP64 step, on the periodic
+curvilinear Orszag-Tang cube (32^3, 100 steps).
 
 Tolerance: per-field relative L2 <= 1e-5 over the owned DOFs of the state
 (U_H, U_Na, B faces) after 100 steps; div B (max |sum of face fluxes| over

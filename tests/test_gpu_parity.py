@@ -1,5 +1,5 @@
 """FP64 GPU step vs the reference built from its own sources (oracle/_ref),
-on the config-1 case (periodic curvilinear cube, Orszag-Tang, two ion
+on the periodic curvilinear Orszag-Tang cube (32^3, two ion
 fluids, Hall + electron pressure), through the C ABI.
 
 Tolerance: the FP64 path must match to <= 1e-12 relative L2 per field after
@@ -49,8 +49,8 @@ def test_step_matches_reference(cube16, steps):
     assert info.step == steps
 
 
-def test_config1_100_steps(ref_oracle):
-    """Config 1 in full: 32^3, 100 steps."""
+def test_cube32_100_steps(ref_oracle):
+    """The full 32^3 cube, 100 steps."""
     if not has_gpu():
         pytest.skip("no GPU")
     import mercury_oracle as mo
