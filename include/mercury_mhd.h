@@ -258,6 +258,15 @@ int mhd_batch_destroy(mhd_batch *batch);
 int64_t mhd_desc_device_bytes(const mhd_desc *desc);
 /* Adds a solve (allocates its arena, uploads its tables) into a free slot. */
 int mhd_batch_add(mhd_batch *batch, const mhd_desc *desc, int *slot);
+/* Adds a solve with the blocks and topology of the solve in src_slot, sharing
+ * its device sync and alias tables (no descriptor processing): the way a
+ * server admits a request whose grid it already holds.  constants: the new
+ * solve's constants (NULL = the template's).  copy_static = 1 copies the
+ * template's fields (static geometry, sources, and its current state) on
+ * the device; 0 zeroes them.  The caller then uploads what differs (normally
+ * the state) and calls mhd_batch_sync / mhd_batch_prepare as after
+ * mhd_batch_add. */
+int mhd_batch_add_like(mhd_batch *batch, int src_slot, const mhd_constants *constants, int copy_static, int *slot);
 /* Frees a slot; the solve's memory is released in stream order. */
 int mhd_batch_remove(mhd_batch *batch, int slot);
 int mhd_batch_upload_field(mhd_batch *batch, int slot, int field, int block, const double *data,
@@ -273,6 +282,15 @@ int mhd_batch_request(mhd_batch *batch, int slot, int64_t nsteps);
 int mhd_batch_run(mhd_batch *batch, int nsteps);
 /* Synchronises and fills infos[0 .. capacity) (empty slots read zero). */
 int mhd_batch_poll(mhd_batch *batch, mhd_info *infos);
+/* Asynchronous form: mhd_batch_poll_async enqueues a snapshot of every slot's
+ * state after the work queued so far and returns a ticket (two snapshots can
+ * be outstanding); mhd_batch_poll_wait waits for that snapshot only, so the
+ * host can act on step k while step k + 1 runs.  Uploads from pageable host
+ * memory, mhd_batch_add_like, mhd_batch_sync, mhd_batch_prepare,
+ * mhd_batch_request and mhd_batch_remove are asynchronous too (stream-ordered
+ * with the steps). */
+int mhd_batch_poll_async(mhd_batch *batch, int *ticket);
+int mhd_batch_poll_wait(mhd_batch *batch, int ticket, mhd_info *infos);
 void *mhd_batch_stream(mhd_batch *batch);
 int mhd_batch_kernels_per_step(mhd_batch *batch);
 int mhd_batch_step_profiled(mhd_batch *batch, int nsteps, int max_kernels, float *kernel_ms,

@@ -103,9 +103,9 @@ EXPORTS = [
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy",
-    "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_remove", "mhd_batch_upload_field",
+    "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
-    "mhd_batch_poll", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
+    "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view",
 ]
 
@@ -156,6 +156,8 @@ def lib() -> ctypes.CDLL:
     L.mhd_desc_device_bytes.argtypes = [ctypes.POINTER(MhdDesc)]
     L.mhd_desc_device_bytes.restype = ctypes.c_int64
     L.mhd_batch_add.argtypes = [P, ctypes.POINTER(MhdDesc), ctypes.POINTER(ctypes.c_int)]
+    L.mhd_batch_add_like.argtypes = [P, ctypes.c_int, ctypes.POINTER(MhdConstants), ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_int)]
     L.mhd_batch_remove.argtypes = [P, ctypes.c_int]
     L.mhd_batch_upload_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p,
                                          ctypes.c_int]
@@ -165,6 +167,8 @@ def lib() -> ctypes.CDLL:
     L.mhd_batch_request.argtypes = [P, ctypes.c_int, ctypes.c_int64]
     L.mhd_batch_run.argtypes = [P, ctypes.c_int]
     L.mhd_batch_poll.argtypes = [P, ctypes.POINTER(MhdInfo)]
+    L.mhd_batch_poll_async.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
+    L.mhd_batch_poll_wait.argtypes = [P, ctypes.c_int, ctypes.POINTER(MhdInfo)]
     L.mhd_batch_stream.argtypes = [P]
     L.mhd_batch_stream.restype = ctypes.c_void_p
     L.mhd_batch_kernels_per_step.argtypes = [P]
@@ -314,6 +318,13 @@ class Batch:
         check(lib().mhd_batch_add(self.b, ctypes.byref(desc.desc), ctypes.byref(slot)), "mhd_batch_add")
         return slot.value
 
+    def add_like(self, src_slot: int, constants=None, copy_static: bool = True) -> int:
+        slot = ctypes.c_int()
+        cp = ctypes.byref(constants) if constants is not None else None
+        check(lib().mhd_batch_add_like(self.b, src_slot, cp, int(copy_static), ctypes.byref(slot)),
+              "mhd_batch_add_like")
+        return slot.value
+
     def remove(self, slot: int):
         check(lib().mhd_batch_remove(self.b, slot), "mhd_batch_remove")
 
@@ -345,6 +356,16 @@ class Batch:
     def poll(self):
         infos = (MhdInfo * self.capacity)()
         check(lib().mhd_batch_poll(self.b, infos), "mhd_batch_poll")
+        return list(infos)
+
+    def poll_async(self) -> int:
+        t = ctypes.c_int()
+        check(lib().mhd_batch_poll_async(self.b, ctypes.byref(t)), "mhd_batch_poll_async")
+        return t.value
+
+    def poll_wait(self, ticket: int):
+        infos = (MhdInfo * self.capacity)()
+        check(lib().mhd_batch_poll_wait(self.b, ticket, infos), "mhd_batch_poll_wait")
         return list(infos)
 
     def stream(self) -> int:

@@ -89,14 +89,11 @@ int dev_upload(const std::vector<T> &h, T **d, cudaStream_t st) {
 // One solve: its arena, tables and its directory entry's pointees.  Arena
 // bytes: [U buffer 0 | U buffer 1 | M of every block], per block U = 10 real
 // arrays, M = 10 metric double arrays then kNumRComps real arrays.
-struct Solve {
-  int nblocks = 0, nghost = 0, es = 8;  // es: bytes per real
-  bool prepared = false;
-  std::vector<Box> boxes;
-  std::vector<int64_t> ubase, mbase;  // bytes
-  int64_t ubuf = 0, main_off = 0, arena_bytes = 0, table_bytes = 0;
-  char *arena = nullptr;
-  DevBlock *dblocks = nullptr;
+// Device tables of a solve's topology (tile prefix sums, sync segments, alias
+// classes).  Solves added with mhd_batch_add_like share their template's
+// tables; the last user frees them.
+struct Tables {
+  int users = 0;
   int *dtile_prefix[kNumRanges] = {};
   int tiles[kNumRanges] = {};
   int64_t *tab_seg[kMaxGroups][3] = {};
@@ -105,6 +102,18 @@ struct Solve {
   int64_t *al_memE = nullptr, *al_ownE = nullptr, *al_memJ = nullptr, *al_ownJ = nullptr;
   double *al_msign = nullptr, *al_osign = nullptr;
   int al_n = 0;
+  int64_t table_bytes = 0;
+};
+
+struct Solve {
+  int nblocks = 0, nghost = 0, es = 8;  // es: bytes per real
+  bool prepared = false;
+  std::vector<Box> boxes;
+  std::vector<int64_t> ubase, mbase;  // bytes
+  int64_t ubuf = 0, main_off = 0, arena_bytes = 0;
+  char *arena = nullptr;
+  DevBlock *dblocks = nullptr;
+  Tables *T = nullptr;
   Consts consts{};
 
   int comp_bytes(int c) const { return is_metric(c) ? 8 : es; }
@@ -153,6 +162,9 @@ struct mhd_batch {
   size_t staging_elems = 0;
   void **comp_ptrs = nullptr;
   SolveState *hstate = nullptr;  // pinned mirror of dstate
+  SolveState *hsnap[2] = {};     // pinned snapshots for mhd_batch_poll_async
+  cudaEvent_t snap_ev[2] = {};
+  int snap_next = 0;
   // eager profiling
   bool profiling = false;
   std::vector<cudaEvent_t> prof_events;
@@ -281,12 +293,12 @@ int publish(mhd_batch *b) {
   };
   int rc;
   for (int r = 0; r < kNumRanges; ++r)
-    if ((rc = put(b->dprefix_tiles[r], [&](const Solve *S) { return S->tiles[r]; }))) return rc;
+    if ((rc = put(b->dprefix_tiles[r], [&](const Solve *S) { return S->T->tiles[r]; }))) return rc;
   for (int g = 0; g < kMaxGroups; ++g)
     for (int p = 0; p < 3; ++p)
-      if ((rc = put(b->dprefix_copy[g][p], [&](const Solve *S) { return S->tab_n[g][p]; }))) return rc;
-  if ((rc = put(b->dprefix_aliasE, [](const Solve *S) { return (S->al_n + 7) / 8; }))) return rc;
-  if ((rc = put(b->dprefix_aliasJ, [](const Solve *S) { return (S->al_n + 7) / 8; }))) return rc;
+      if ((rc = put(b->dprefix_copy[g][p], [&](const Solve *S) { return S->T->tab_n[g][p]; }))) return rc;
+  if ((rc = put(b->dprefix_aliasE, [](const Solve *S) { return (S->T->al_n + 7) / 8; }))) return rc;
+  if ((rc = put(b->dprefix_aliasJ, [](const Solve *S) { return (S->T->al_n + 7) / 8; }))) return rc;
   std::vector<DevSolve> ds((size_t)C);
   for (int s = 0; s < C; ++s) {
     DevSolve &d = ds[s];
@@ -299,14 +311,14 @@ int publish(mhd_batch *b) {
     d.arena = S->arena;
     d.ubuf = S->ubuf;
     d.nblocks = S->nblocks;
-    for (int r = 0; r < kNumRanges; ++r) d.tile_prefix[r] = S->dtile_prefix[r];
+    for (int r = 0; r < kNumRanges; ++r) d.tile_prefix[r] = S->T->dtile_prefix[r];
     for (int g = 0; g < kMaxGroups; ++g) {
-      d.halo[g] = DevTable{S->tab_seg[g][0], S->tab_n[g][0]};
-      d.owner[g] = DevTable{S->tab_seg[g][1], S->tab_n[g][1]};
-      d.halo_full[g] = DevTable{S->tab_seg[g][2], S->tab_n[g][2]};
+      d.halo[g] = DevTable{S->T->tab_seg[g][0], S->T->tab_n[g][0]};
+      d.owner[g] = DevTable{S->T->tab_seg[g][1], S->T->tab_n[g][1]};
+      d.halo_full[g] = DevTable{S->T->tab_seg[g][2], S->T->tab_n[g][2]};
     }
-    d.aliasE = DevAlias{S->al_off, S->al_memE, S->al_msign, S->al_ownE, S->al_osign, S->al_n};
-    d.aliasJ = DevAlias{S->al_off, S->al_memJ, S->al_msign, S->al_ownJ, S->al_osign, S->al_n};
+    d.aliasE = DevAlias{S->T->al_off, S->T->al_memE, S->T->al_msign, S->T->al_ownE, S->T->al_osign, S->T->al_n};
+    d.aliasJ = DevAlias{S->T->al_off, S->T->al_memJ, S->T->al_msign, S->T->al_ownJ, S->T->al_osign, S->T->al_n};
   }
   CUDA_TRY(cudaMemcpyAsync(b->dsolves, ds.data(), sizeof(DevSolve) * C, cudaMemcpyHostToDevice, b->stream));
   return MHD_OK;
@@ -392,15 +404,15 @@ int upload_copies(Solve *S, const mhd_copy *tab, int n, int g, int phase, cudaSt
     len = 1;
   }
   flush();
-  S->tab_n[g][phase] = (int)(seg.size() / 2);
-  S->table_bytes += (int64_t)seg.size() * 8;
-  return dev_upload(seg, &S->tab_seg[g][phase], st);
+  S->T->tab_n[g][phase] = (int)(seg.size() / 2);
+  S->T->table_bytes += (int64_t)seg.size() * 8;
+  return dev_upload(seg, &S->T->tab_seg[g][phase], st);
 }
 
 int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
-  S->al_n = a.n_classes;
+  S->T->al_n = a.n_classes;
   if (a.n_classes <= 0) {
-    S->al_n = 0;
+    S->T->al_n = 0;
     return MHD_OK;
   }
   if (!a.offset || !a.member || !a.member_sign || !a.owner || !a.owner_sign)
@@ -424,12 +436,12 @@ int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
     if (!both(a.owner[c], &oE[c], &oJ[c])) return fail(MHD_ERR_ARG, "alias owner %d out of range", c);
   std::vector<int32_t> off(a.offset, a.offset + a.n_classes + 1);
   std::vector<double> ms(a.member_sign, a.member_sign + nm), os(a.owner_sign, a.owner_sign + a.n_classes);
-  S->table_bytes += (int64_t)nm * 24 + (int64_t)a.n_classes * 28;
+  S->T->table_bytes += (int64_t)nm * 24 + (int64_t)a.n_classes * 28;
   int rc;
-  if ((rc = dev_upload(off, &S->al_off, st)) || (rc = dev_upload(mE, &S->al_memE, st)) ||
-      (rc = dev_upload(mJ, &S->al_memJ, st)) || (rc = dev_upload(oE, &S->al_ownE, st)) ||
-      (rc = dev_upload(oJ, &S->al_ownJ, st)) || (rc = dev_upload(ms, &S->al_msign, st)) ||
-      (rc = dev_upload(os, &S->al_osign, st)))
+  if ((rc = dev_upload(off, &S->T->al_off, st)) || (rc = dev_upload(mE, &S->T->al_memE, st)) ||
+      (rc = dev_upload(mJ, &S->T->al_memJ, st)) || (rc = dev_upload(oE, &S->T->al_ownE, st)) ||
+      (rc = dev_upload(oJ, &S->T->al_ownJ, st)) || (rc = dev_upload(ms, &S->T->al_msign, st)) ||
+      (rc = dev_upload(os, &S->T->al_osign, st)))
     return rc;
   return MHD_OK;
 }
@@ -441,14 +453,16 @@ void free_solve(Solve *S, cudaStream_t st) {
   };
   f(S->arena);
   f(S->dblocks);
-  for (int r = 0; r < kNumRanges; ++r) f(S->dtile_prefix[r]);
-  for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 3; ++p) {
-      f(S->tab_seg[g][p]);
-    }
-  for (void *p : {(void *)S->al_off, (void *)S->al_memE, (void *)S->al_ownE, (void *)S->al_memJ, (void *)S->al_ownJ,
-                  (void *)S->al_msign, (void *)S->al_osign})
-    f(p);
+  Tables *T = S->T;
+  if (T && --T->users == 0) {
+    for (int r = 0; r < kNumRanges; ++r) f(T->dtile_prefix[r]);
+    for (int g = 0; g < kMaxGroups; ++g)
+      for (int p = 0; p < 3; ++p) f(T->tab_seg[g][p]);
+    for (void *p : {(void *)T->al_off, (void *)T->al_memE, (void *)T->al_ownE, (void *)T->al_memJ, (void *)T->al_ownJ,
+                    (void *)T->al_msign, (void *)T->al_osign})
+      f(p);
+    delete T;
+  }
   delete S;
 }
 
@@ -546,7 +560,11 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
   if (cudaMalloc(&b->dsolves, sizeof(DevSolve) * capacity) != cudaSuccess ||
       cudaMalloc(&b->dstate, sizeof(SolveState) * capacity) != cudaSuccess ||
       cudaMalloc(&b->comp_ptrs, sizeof(void *) * 72) != cudaSuccess ||
-      cudaMallocHost(&b->hstate, sizeof(SolveState) * capacity) != cudaSuccess)
+      cudaMallocHost(&b->hstate, sizeof(SolveState) * capacity) != cudaSuccess ||
+      cudaMallocHost(&b->hsnap[0], sizeof(SolveState) * capacity) != cudaSuccess ||
+      cudaMallocHost(&b->hsnap[1], sizeof(SolveState) * capacity) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->snap_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->snap_ev[1], cudaEventDisableTiming) != cudaSuccess)
     return bail(fail(MHD_ERR_OOM, "directory of %d slots", capacity));
   for (int r = 0; r < kNumRanges; ++r)
     if (cudaMalloc(&b->dprefix_tiles[r], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
@@ -576,6 +594,10 @@ int mhd_batch_destroy(mhd_batch *b) {
   cudaFree(b->dstate);
   cudaFree(b->comp_ptrs);
   if (b->hstate) cudaFreeHost(b->hstate);
+  for (int q = 0; q < 2; ++q) {
+    if (b->hsnap[q]) cudaFreeHost(b->hsnap[q]);
+    if (b->snap_ev[q]) cudaEventDestroy(b->snap_ev[q]);
+  }
   for (int r = 0; r < kNumRanges; ++r) cudaFree(b->dprefix_tiles[r]);
   for (int g = 0; g < kMaxGroups; ++g)
     for (int p = 0; p < 3; ++p) cudaFree(b->dprefix_copy[g][p]);
@@ -620,6 +642,12 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   if (slot < 0) return fail(MHD_ERR_OOM, "mhd_batch_add: all %d slots in use", b->capacity);
   auto *S = new (std::nothrow) Solve();
   if (!S) return fail(MHD_ERR_OOM, "host allocation");
+  S->T = new (std::nothrow) Tables();
+  if (!S->T) {
+    delete S;
+    return fail(MHD_ERR_OOM, "host allocation");
+  }
+  S->T->users = 1;
   cudaStream_t st = b->stream;
   auto bail = [&](int rc) {
     free_solve(S, st);
@@ -677,8 +705,8 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   int rc;
   if ((rc = dev_upload(blocks, &S->dblocks, st))) return bail(rc);
   for (int r = 0; r < kNumRanges; ++r) {
-    S->tiles[r] = prefix[r].back();
-    if ((rc = dev_upload(prefix[r], &S->dtile_prefix[r], st))) return bail(rc);
+    S->T->tiles[r] = prefix[r].back();
+    if ((rc = dev_upload(prefix[r], &S->T->dtile_prefix[r], st))) return bail(rc);
   }
   for (int g = 0; g < MHD_NUM_GROUPS; ++g) {
     if ((rc = upload_copies(S, desc->groups[g].halo, desc->groups[g].n_halo, g, 0, st, kHaloDepth[g]))) return bail(rc);
@@ -693,6 +721,79 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   if ((rc = publish(b))) return rc;
   CUDA_TRY(cudaStreamSynchronize(st));
   *slot_out = slot;
+  return MHD_OK;
+}
+
+int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constants, int copy_static, int *slot_out) {
+  int rc = slot_check(b, src_slot);
+  if (rc) return rc;
+  if (!slot_out) return fail(MHD_ERR_ARG, "mhd_batch_add_like: null slot");
+  int slot = -1;
+  for (int s = 0; s < b->capacity; ++s)
+    if (!b->slots[s]) {
+      slot = s;
+      break;
+    }
+  if (slot < 0) return fail(MHD_ERR_OOM, "mhd_batch_add_like: all %d slots in use", b->capacity);
+  const Solve *src = b->slots[src_slot];
+  auto *S = new (std::nothrow) Solve();
+  if (!S) return fail(MHD_ERR_OOM, "host allocation");
+  cudaStream_t st = b->stream;
+  S->nblocks = src->nblocks;
+  S->nghost = src->nghost;
+  S->es = src->es;
+  S->boxes = src->boxes;
+  S->ubase = src->ubase;
+  S->mbase = src->mbase;
+  S->ubuf = src->ubuf;
+  S->main_off = src->main_off;
+  S->arena_bytes = src->arena_bytes;
+  S->T = src->T;
+  S->T->users += 1;
+  S->consts = src->consts;
+  if (constants) {
+    const mhd_constants &k = *constants;
+    S->consts = Consts{k.gamma,         k.M_H,       k.M_Na,        k.M_ref,
+                       k.T_ref,         k.L_ref,     k.U_ref,       k.B_ref,
+                       k.n_ref,         k.rho_ref,   k.m_Na,        k.k_Boltz,
+                       k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
+                       k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
+                       k.inver_MA2,     k.ne_hall_floor, k.ambipolar, S->nghost};
+  }
+  auto bail = [&](int code) {
+    free_solve(S, st);
+    return code;
+  };
+  if (cudaMallocAsync((void **)&S->arena, S->arena_bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
+  }
+  // the template's fields (static geometry and sources, and its current
+  // state, which the caller normally overwrites) or zeros
+  const cudaError_t e = copy_static ? cudaMemcpyAsync(S->arena, src->arena, S->arena_bytes, cudaMemcpyDeviceToDevice, st)
+                                    : cudaMemsetAsync(S->arena, 0, S->arena_bytes, st);
+  if (e != cudaSuccess) return bail(fail(MHD_ERR_CUDA, "arena init: %s", cudaGetErrorString(e)));
+  std::vector<DevBlock> blocks(S->nblocks);
+  for (int bi = 0; bi < S->nblocks; ++bi) {
+    const Box &bx = S->boxes[bi];
+    DevBlock &d = blocks[bi];
+    d.U[0] = S->arena + S->ubase[bi];
+    d.U[1] = S->arena + S->ubuf + S->ubase[bi];
+    d.M = S->arena + S->main_off + S->mbase[bi];
+    d.total = bx.total;
+    d.si = bx.si;
+    d.sj = bx.sj;
+    d.G = bx.G;
+    for (int a = 0; a < 3; ++a) d.n[a] = bx.n[a];
+    d.solve = slot;
+  }
+  if ((rc = dev_upload(blocks, &S->dblocks, st))) return bail(rc);
+  SolveState s0{};
+  s0.dt_bits = kDtUnset;
+  if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
+  b->slots[slot] = S;
+  if ((rc = publish(b))) return rc;
+  *slot_out = slot;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
 }
 
@@ -731,7 +832,15 @@ int mhd_batch_upload_field(mhd_batch *b, int slot, int field, int block, const d
                                                                        ncomp, b->comp_ptrs, ndst, bx.si, bx.sj, bx.G,
                                                                        S->comp_bytes(c0) == 4);
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  // A copy from pageable memory is staged by the driver before
+  // cudaMemcpyAsync returns; page-locked memory is read by the DMA later, so
+  // wait for it before the caller may reuse the buffer.
+  cudaPointerAttributes pa{};
+  if (cudaPointerGetAttributes(&pa, data) != cudaSuccess) {
+    cudaGetLastError();
+    pa.type = cudaMemoryTypeHost;
+  }
+  if (pa.type != cudaMemoryTypeUnregistered) CUDA_TRY(cudaStreamSynchronize(b->stream));
   S->prepared = false;
   return MHD_OK;
 }
@@ -765,10 +874,7 @@ int mhd_batch_sync(mhd_batch *b, int slot, int group) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
   if (group < 0 || group >= MHD_NUM_GROUPS) return fail(MHD_ERR_ARG, "mhd_sync: bad group %d", group);
-  rc = targeted(b, slot, [&](int *nk) { enqueue_sync(b, 1, group, nk, true); });
-  if (rc) return rc;
-  CUDA_TRY(cudaStreamSynchronize(b->stream));
-  return MHD_OK;
+  return targeted(b, slot, [&](int *nk) { enqueue_sync(b, 1, group, nk, true); });  // asynchronous
 }
 
 int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
@@ -778,17 +884,14 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   s0.dt_bits = kDtUnset;
   s0.time = time;
   s0.step = step;
-  // keep the current buffer index
-  if ((rc = read_state(b))) return rc;
-  s0.cur = b->hstate[slot].cur;
-  if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return rc;
+  // reset everything before the buffer index (dt, time, step, remaining, status); keep cur
+  if ((rc = set_state_field(b, slot, 0, &s0, offsetof(SolveState, cur)))) return rc;
   rc = targeted(b, slot, [&](int *nk) {
     launch(b, 1, SK_FACE_NORMALS, nk);
     enqueue_derived(b, 1, nk);
   });
   if (rc) return rc;
-  CUDA_TRY(cudaStreamSynchronize(b->stream));
-  b->slots[slot]->prepared = true;
+  b->slots[slot]->prepared = true;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
 }
 
@@ -822,8 +925,40 @@ int mhd_batch_poll(mhd_batch *b, mhd_info *infos) {
     infos[s].status = st.status;
     infos[s].remaining = st.remaining;
     const Solve *S = b->slots[s];
-    infos[s].device_bytes = S ? S->arena_bytes + S->table_bytes : 0;
+    infos[s].device_bytes = S ? S->arena_bytes + S->T->table_bytes : 0;
   }
+  return MHD_OK;
+}
+
+static void fill_infos(mhd_batch *b, const SolveState *hs, mhd_info *infos) {
+  for (int s = 0; s < b->capacity; ++s) {
+    const SolveState &st = hs[s];
+    std::memset(&infos[s], 0, sizeof(mhd_info));
+    infos[s].time = st.time;
+    infos[s].dt = st.dt;
+    infos[s].step = st.step;
+    infos[s].status = st.status;
+    infos[s].remaining = st.remaining;
+    const Solve *S = b->slots[s];
+    infos[s].device_bytes = S ? S->arena_bytes + S->T->table_bytes : 0;
+  }
+}
+
+int mhd_batch_poll_async(mhd_batch *b, int *ticket) {
+  if (!b || !ticket) return fail(MHD_ERR_ARG, "mhd_batch_poll_async: bad arguments");
+  const int t = b->snap_next;
+  b->snap_next ^= 1;
+  CUDA_TRY(cudaMemcpyAsync(b->hsnap[t], b->dstate, sizeof(SolveState) * b->capacity, cudaMemcpyDeviceToHost,
+                           b->stream));
+  CUDA_TRY(cudaEventRecord(b->snap_ev[t], b->stream));
+  *ticket = t;
+  return MHD_OK;
+}
+
+int mhd_batch_poll_wait(mhd_batch *b, int ticket, mhd_info *infos) {
+  if (!b || !infos || ticket < 0 || ticket > 1) return fail(MHD_ERR_ARG, "mhd_batch_poll_wait: bad arguments");
+  CUDA_TRY(cudaEventSynchronize(b->snap_ev[ticket]));
+  fill_infos(b, b->hsnap[ticket], infos);
   return MHD_OK;
 }
 

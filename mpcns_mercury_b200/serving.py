@@ -29,6 +29,7 @@ class Request:
     steps: int
     fields: dict              # {reference field name: Arr} inputs (static + initial state)
     keep_result: bool = False
+    geometry: object = None   # requests with equal keys share their grid and static fields (default: cells)
     # filled in by the server
     admitted_s: float = float("nan")
     done_s: float = float("nan")
@@ -40,32 +41,60 @@ def percentile(values, q):
     return float(np.percentile(np.asarray(values, dtype=np.float64), q)) if len(values) else float("nan")
 
 
+def _geometry_key(req: Request):
+    return req.geometry if req.geometry is not None else tuple(req.cells)
+
+
+def _upload_state(upload, fields):
+    for name in STATE_FIELDS:
+        a = fields[name]
+        upload(capi_field(name), a.data, a.lo, a.hi, 0)
+
+
 class Server:
-    """Continuous-batching server of independent solves on one GPU."""
+    """Continuous-batching server of independent solves on one GPU.
+
+    The first request of a grid makes a template solve holding the grid's
+    topology tables and static fields (never stepped); every request is then
+    admitted with mhd_batch_add_like from its grid's template (shared tables,
+    static fields copied on the device) and uploads only its state."""
 
     def __init__(self, capacity: int = 64, precision: int = 1, hbm_budget: float = 100e9, chunk_steps: int = 8,
-                 cfl: float = 0.4):
-        self.batch = capi.Batch(capacity, precision)
+                 cfl: float = 0.4, max_grids: int = 16):
+        self.batch = capi.Batch(capacity + max_grids, precision)
         self.capacity = capacity
+        self.max_grids = max_grids
         self.precision = precision
         self.hbm_budget = float(hbm_budget)
         self.chunk = int(chunk_steps)
         self.constants = reference_constants(cfl=cfl)
+        self.templates = {}     # geometry key -> template slot
+        self.grid_bytes = {}    # geometry key -> device bytes of one solve
 
     def close(self):
         self.batch.close()
 
     # ------------------------------------------------------------------ one solve
+    def _template(self, req: Request) -> int:
+        key = _geometry_key(req)
+        if key not in self.templates:
+            if len(self.templates) >= self.max_grids:
+                raise RuntimeError(f"more than {self.max_grids} distinct grids")
+            d = capi.SolveDesc([req.cells], NGHOST, self.constants, precision=self.precision)
+            slot = self.batch.add(d)
+            d.close()
+            upload_case(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b), req.fields)
+            self.templates[key] = slot
+        return self.templates[key]
+
     def _admit(self, req: Request) -> int:
-        d = capi.SolveDesc([req.cells], NGHOST, self.constants, precision=self.precision)
-        slot = self.batch.add(d)
-        upload_case(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b), req.fields)
+        slot = self.batch.add_like(self._template(req), copy_static=True)
+        _upload_state(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b), req.fields)
         self.batch.sync(slot, "UCELL")
         self.batch.sync(slot, "BFACE")
         self.batch.prepare(slot)
         self.batch.request(slot, req.steps)
         req.slot = slot
-        d.close()
         return slot
 
     def _retire(self, req: Request):
@@ -81,53 +110,78 @@ class Server:
         d.close()
         return b
 
+    def _need(self, req: Request) -> int:
+        key = _geometry_key(req)
+        if key not in self.grid_bytes:
+            self.grid_bytes[key] = self._bytes(req, self.precision)
+        return self.grid_bytes[key]
+
     # ------------------------------------------------------------------ the loop
     def serve(self, requests, clock=time.perf_counter):
-        """Serve ``requests`` (sorted by arrival) in real time; returns statistics."""
+        """Serve ``requests`` (sorted by arrival) in real time; returns statistics.
+
+        Each pass admits the requests that have arrived (asynchronous calls,
+        ordered on the batch's stream), enqueues `chunk` graph launches and a
+        state snapshot, then waits for the previous pass's snapshot only: the
+        host retires finished solves and admits new ones while the GPU runs
+        the next chunk.  A solve that finishes inside a chunk idles for the
+        rest of it."""
         pending = sorted(requests, key=lambda r: r.arrival_s)
-        need = {r.rid: self._bytes(r, self.precision) for r in pending}
+        need = {r.rid: self._need(r) for r in pending}
         running: dict[int, Request] = {}
-        remaining: dict[int, int] = {}
+        epoch: dict[int, int] = {}   # slot -> snapshots enqueued before its request
         used = 0
         t0 = clock()
         nxt = 0
         graph_steps = 0
+        snaps = 0
+        ticket = None                # (ticket, snapshot number) of the last enqueued snapshot
         while nxt < len(pending) or running:
             now = clock() - t0
-            # admission: arrived requests, in arrival order, while a slot and memory are free
+            # admission: arrived requests, in arrival order, while a slot and memory are
+            # free (a grid's template, made on first use, is charged once)
             while (nxt < len(pending) and pending[nxt].arrival_s <= now and len(running) < self.capacity
-                   and used + need[pending[nxt].rid] <= self.hbm_budget):
+                   and used + need[pending[nxt].rid] * (1 if _geometry_key(pending[nxt]) in self.templates else 2)
+                   <= self.hbm_budget):
                 r = pending[nxt]
+                if _geometry_key(r) not in self.templates:
+                    used += need[r.rid]
                 r.admitted_s = clock() - t0
                 self._admit(r)
                 running[r.slot] = r
-                remaining[r.slot] = r.steps
+                epoch[r.slot] = snaps
                 used += need[r.rid]
                 nxt += 1
             if not running:
+                if pending[nxt].arrival_s <= clock() - t0:
+                    raise RuntimeError(f"request {pending[nxt].rid} does not fit the device budget "
+                                       f"({need[pending[nxt].rid]} bytes, {used} held by grid templates)")
                 # idle until the next arrival
                 wait = pending[nxt].arrival_s - (clock() - t0)
                 if wait > 0:
                     time.sleep(min(wait, 0.05))
                 continue
-            # advance every running solve by up to `chunk` steps, stopping at the
-            # first completion (graph launches are asynchronous; the poll synchronises)
-            n = max(1, min(self.chunk, min(remaining.values())))
-            self.batch.run(n)
-            graph_steps += n
-            infos = self.batch.poll()
-            now = clock() - t0
-            for slot in list(running):
-                inf = infos[slot]
-                if inf.status != 0:
-                    raise capi.MhdError(inf.status, f"request {running[slot].rid} (slot {slot})")
-                remaining[slot] = int(inf.remaining)
-                if inf.remaining == 0:
-                    r = running.pop(slot)
-                    del remaining[slot]
-                    r.done_s = now
-                    self._retire(r)
-                    used -= need[r.rid]
+            self.batch.run(self.chunk)
+            graph_steps += self.chunk
+            new = (self.batch.poll_async(), snaps + 1)
+            snaps += 1
+            if ticket is not None:
+                infos = self.batch.poll_wait(ticket[0])
+                now = clock() - t0
+                for slot in list(running):
+                    if epoch[slot] >= ticket[1]:
+                        continue  # admitted after that snapshot was taken
+                    inf = infos[slot]
+                    if inf.status != 0:
+                        raise capi.MhdError(inf.status, f"request {running[slot].rid} (slot {slot})")
+                    if inf.remaining == 0:
+                        r = running.pop(slot)
+                        del epoch[slot]
+                        r.done_s = now
+                        self._retire(r)
+                        used -= need[r.rid]
+            ticket = new
+        self.batch.poll()
         makespan = clock() - t0
         lat = [r.done_s - r.arrival_s for r in pending]
         work = sum(int(np.prod(r.cells)) * r.steps for r in pending)
@@ -139,16 +193,25 @@ class Server:
 
 def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl: float = 0.4):
     """The same requests served first-come first-served through the plain
-    single-solve path (mhd_ctx, one solve on the GPU at a time)."""
+    single-solve path (mhd_ctx, one solve on the GPU at a time).  Like the
+    server, it keeps one context per grid (tables and static fields uploaded
+    once) and uploads each request's state."""
     pending = sorted(requests, key=lambda r: r.arrival_s)
+    ctxs = {}
     t0 = clock()
     for r in pending:
         now = clock() - t0
         if r.arrival_s > now:
             time.sleep(r.arrival_s - now)
         r.admitted_s = clock() - t0
-        ctx = capi.Context([r.cells], NGHOST, reference_constants(cfl=cfl), precision=precision)
-        upload_case(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), r.fields)
+        key = _geometry_key(r)
+        ctx = ctxs.get(key)
+        if ctx is None:
+            ctx = capi.Context([r.cells], NGHOST, reference_constants(cfl=cfl), precision=precision)
+            upload_case(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), r.fields)
+            ctxs[key] = ctx
+        else:
+            _upload_state(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), r.fields)
         ctx.sync("UCELL")
         ctx.sync("BFACE")
         ctx.prepare()
@@ -156,9 +219,10 @@ def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl:
         if r.keep_result:
             r.result = {name: ctx.download(capi_field(name), r.fields[name].lo, r.fields[name].hi)
                         for name in STATE_FIELDS}
-        ctx.close()
         r.done_s = clock() - t0
     makespan = clock() - t0
+    for ctx in ctxs.values():
+        ctx.close()
     lat = [r.done_s - r.arrival_s for r in pending]
     work = sum(int(np.prod(r.cells)) * r.steps for r in pending)
     return {"requests": len(pending), "makespan_s": makespan, "cell_updates": work,
