@@ -393,6 +393,10 @@ def run_ensemble(args, rank, world, device):
     plain_ms = 0.0
     plain_state = []
     h2d_bytes = 0
+    only = getattr(args, "batched_only", False)
+    if only:
+        batches[0].close()
+        del batches[0]
     for sid, fields in enumerate(W.generate_cases([(c, base_id + s) for s, c in enumerate(cells)])):
         n = cells[sid]
         for prec, b in batches.items():
@@ -409,6 +413,8 @@ def run_ensemble(args, rank, world, device):
             d.close()
             if prec == 1:
                 h2d_bytes += nb
+        if only:
+            continue
         # plain FP64, this solve alone
         ctx = Context([n], 4, k0)
         W.upload_case(lambda f, a, lo, hi, blk: ctx.upload(f, a, lo, hi, block=blk), fields)
@@ -443,6 +449,12 @@ def run_ensemble(args, rank, world, device):
     mixed_ms = _timed_batch_steps(batches[1], K, device)
     t_run_mixed = time.perf_counter() - t_run0
     clocks = sampler.stop() if rank == 0 else None
+    if only:
+        ms = mixed_ms
+        batches[1].close()
+        return {"metric": METRIC, "value": round(world * ncell * K / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
+                "n_gpus": world, "steps": K, "warmup": W_, "ms_per_step": round(ms / K, 5),
+                "config": {"workload": "ensemble", "solves": nsol, "batched_only": True}}
     fp64_ms = _timed_batch_steps(batches[0], K, device)
     infos = {p: b.poll() for p, b in batches.items()}
     for p in batches:
@@ -660,6 +672,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="ensemble", help="ensemble (default), serve, cube32, cubeN")
     ap.add_argument("--solves", type=int, default=64, help="ensemble: solves per GPU")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="ensemble: run only the mixed batch (profiling; no plain/FP64 legs, no error check)")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: mean arrivals per second")
     ap.add_argument("--shapes", type=int, default=16, help="serve: distinct request shapes")

@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 #include "mhd_engine.cuh"
 #include "mhd_kernels.cuh"
@@ -46,8 +47,7 @@ constexpr int cALX = kComp.first[MHD_HODGE_EDGE_XI], cALY = kComp.first[MHD_HODG
               cALZ = kComp.first[MHD_HODGE_EDGE_ZETA];
 constexpr int cWB = kComp.first[MHD_BCELL_W], cWJ = kComp.first[MHD_JCELL_W];
 constexpr int cBAX = kComp.first[MHD_BADD_XI], cBAY = kComp.first[MHD_BADD_ETA], cBAZ = kComp.first[MHD_BADD_ZETA];
-constexpr int cPHOTO = kComp.first[MHD_PHOTO], cCX = kComp.first[MHD_CELL_X], cCY = kComp.first[MHD_CELL_Y],
-              cCZ = kComp.first[MHD_CELL_Z];
+constexpr int cPHOTO = kComp.first[MHD_PHOTO], cCX = kComp.first[MHD_CELL_X];  // CELL_Y, CELL_Z follow
 constexpr int cTPX = kComp.first[MHD_TAPER_XI], cTPY = kComp.first[MHD_TAPER_ETA], cTPZ = kComp.first[MHD_TAPER_ZETA];
 
 // std::max / std::min semantics (first argument wins ties, incl. signed zeros).
@@ -511,47 +511,83 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
     const int tid = threadIdx.x;
     const int li = tid / (kTileK * kTileJ), lj = (tid / kTileK) % kTileJ, lk = tid % kTileK;
     R r[5] = {R(0.0), R(0.0), R(0.0), R(0.0), R(0.0)};
+    // The cell values the source terms and the update read: cen(q) loads
+    // value q; in FP32 all of them are loaded before the flux passes into
+    // registers (their latency hides behind the passes), in FP64 at their use.
+    auto cen = [&](int q) -> R {
+      switch (q) {
+        case 0: case 1: case 2: return AT(cUP + q, i, j, k);
+        case 3: case 4: case 5: return AT(cBC + (q - 3), i, j, k);
+        case 6: case 7: case 8: return AT(cJC + (q - 6), i, j, k);
+        case 9: return AT(cUH, i, j, k);
+        case 10: return AT(cUN, i, j, k);
+        case 11: return AT(pv0 + 4, i, j, k);
+        case 12: case 13: case 14: case 15: case 16: return AT(u0 + (q - 12), i, j, k);
+        case 17: return AT(cPHOTO, i, j, k);
+        case 18: case 19: case 20: return AT(cCX + (q - 18), i, j, k);
+        default: return AT(pv0 + (q - 21), i, j, k);  // 21..23: u, v, w
+      }
+    };
+    constexpr int kCen = sizeof(R) == 4 ? 24 : 1;
+    R cvals[kCen];
+    if constexpr (sizeof(R) == 4) {
+      if (it.in && dt_ok) {
+#pragma unroll
+        for (int q = 0; q < 24; ++q) cvals[q] = cen(q);
+      }
+    }
+    auto CV = [&](int q) -> R {
+      if constexpr (sizeof(R) == 4) return cvals[q];
+      else return cen(q);
+    };
+    // 1/J of this cell, once (the same value every direction divides by)
+    const R invJ = (it.in && dt_ok) ? R(1.0) / R(ATM(cJAC, i, j, k)) : R(0.0);
+    // one pass per direction (unrolled: the face grid's extents are constants)
+    auto face_pass = [&](auto dirc) {
+      constexpr int dir = decltype(dirc)::value;
+      constexpr int cm = dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
+      constexpr int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
+      constexpr int ei = kTileI + (dir == 0), ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
+      constexpr int nf = ei * ej * ek;
 #pragma unroll 1
-    for (int dir = 0; dir < 3; ++dir) {
-      const int cm = dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
-      const int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
-      const int ei = kTileI + (dir == 0), ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
-      const int nf = ei * ej * ek;
       for (int f = tid; f < nf; f += kTileThreads) {
         const int fk = f % ek, fj = (f / ek) % ej, fi = f / (ek * ej);
         const int x[3] = {it.o[0] + fi, it.o[1] + fj, it.o[2] + fk};
         bool need = dt_ok;
+#pragma unroll
         for (int a = 0; a < 3; ++a) need = need && x[a] >= it.lo[a] && x[a] < it.hi[a] + (a == dir);
         if (need) {
           int im = x[0], jm = x[1], km = x[2];
           shift1(dir, im, jm, km, -1);
           R Fl[5];
-          rusanov(B, g, u0, pv0, R(ATM(cm, x[0], x[1], x[2])), R(ATM(cm + 1, x[0], x[1], x[2])), R(ATM(cm + 2, x[0], x[1], x[2])),
-                  AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
+          rusanov(B, g, u0, pv0, R(ATM(cm, x[0], x[1], x[2])), R(ATM(cm + 1, x[0], x[1], x[2])),
+                  R(ATM(cm + 2, x[0], x[1], x[2])), AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
 #pragma unroll
           for (int m = 0; m < 5; ++m) F[m][f] = Fl[m];
         }
       }
       __syncthreads();
       if (it.in && dt_ok) {
-        const R invJ = R(1.0) / R(ATM(cJAC, i, j, k));
         const int fm = (li * ej + lj) * ek + lk;
         const int fp = fm + (dir == 0 ? ej * ek : dir == 1 ? ek : 1);
 #pragma unroll
         for (int m = 0; m < 5; ++m) r[m] -= (F[m][fp] - F[m][fm]) * invJ;
       }
       __syncthreads();
-    }
+    };
+    face_pass(std::integral_constant<int, 0>{});
+    face_pass(std::integral_constant<int, 1>{});
+    face_pass(std::integral_constant<int, 2>{});
     if (!it.in || !dt_ok) return;
     // sources (FluidRHS.cpp:206-527)
     const R Tn0 = R(1000.0), sk1 = R(5.0e-5), sk2 = R(1.0e-5);
     const R a4 = (c.L_ref / c.U_ref);
     const R a5 = (R(3.0) * c.L_ref * c.k_Boltz * c.n_ref) / (c.rho_ref * c.U_ref * c.U_ref * c.U_ref);
-    const R upx = AT(cUP, i, j, k), upy = AT(cUP + 1, i, j, k), upz = AT(cUP + 2, i, j, k);
-    const R Bx = AT(cBC, i, j, k), By = AT(cBC + 1, i, j, k), Bz = AT(cBC + 2, i, j, k);
-    const R Jx = AT(cJC, i, j, k), Jy = AT(cJC + 1, i, j, k), Jz = AT(cJC + 2, i, j, k);
+    const R upx = CV(0), upy = CV(1), upz = CV(2);
+    const R Bx = CV(3), By = CV(4), Bz = CV(5);
+    const R Jx = CV(6), Jy = CV(7), Jz = CV(8);
     const R sjbx = Jy * Bz - Jz * By, sjby = Jz * Bx - Jx * Bz, sjbz = Jx * By - Jy * Bx;
-    const Num<R> num = num_limiter(c, AT(cUH, i, j, k), AT(cUN, i, j, k));
+    const Num<R> num = num_limiter(c, CV(9), CV(10));
     R dpex = R(0.0), dpey = R(0.0), dpez = R(0.0);
     if (c.ambipolar) {
       const R Vol = fabs(R(ATM(cJAC, i, j, k)));
@@ -577,13 +613,13 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
       dpey = R(0.5) * (ay * (pip - pim) + by * (pjp - pjm) + cym * (pkp - pkm));
       dpez = R(0.5) * (az * (pip - pim) + bz * (pjp - pjm) + czm * (pkp - pkm));
     }
-    const R x = AT(cCX, i, j, k), y = AT(cCY, i, j, k), z = AT(cCZ, i, j, k);
+    const R x = CV(18), y = CV(19), z = CV(20);
     const R rho_cyl = sqrt(y * y + z * z);
     const R vst = (x < R(0.0) && rho_cyl < R(1.0)) ? sk2 : sk1;
     const R nS = s ? num.nNa : num.nH;
     const R chi = s ? num.wNa : num.wH;
-    const R rho = dmax(AT(u0, i, j, k), R(0.0));
-    const R u = AT(pv0, i, j, k), v = AT(pv0 + 1, i, j, k), w = AT(pv0 + 2, i, j, k);
+    const R rho = dmax(CV(12), R(0.0));
+    const R u = CV(21), v = CV(22), w = CV(23);
     const R u2 = u * u + v * v + w * w;
     const R subx = (v - upy) * Bz - (w - upz) * By;
     const R suby = (w - upz) * Bx - (u - upx) * Bz;
@@ -591,7 +627,7 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
     const R subu = subx * u + suby * v + subz * w;
     const R sjbu = sjbx * u + sjby * v + sjbz * w;
     const R dpeu = dpex * u + dpey * v + dpez * w;
-    const R Ts0 = AT(pv0 + 4, i, j, k) * c.T_ref;
+    const R Ts0 = CV(11) * c.T_ref;
     R b1, b2;
     if (!s) {
       b1 = vst * (Tn0 - Ts0) * (c.M_H / (c.M_H + c.M_Na));
@@ -613,7 +649,7 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
     if (s) {
       const R a1_Na = (c.L_ref / c.U_ref) * (c.m_Na / c.rho_ref) * R(1e6);
       const R a6 = (R(1.0e6) * c.L_ref * c.k_Boltz) / (c.rho_ref * c.U_ref * c.U_ref * c.U_ref * (c.gamma - R(1.0)));
-      const R sss = AT(cPHOTO, i, j, k);
+      const R sss = CV(17);
       r[0] += a1_Na * sss;
       r[4] += a6 * sss * Tn0;
     }
@@ -625,7 +661,7 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
     r[4] += a4 * rho * u2 * b2;
     const int64_t o = B.off(i, j, k);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) B.Un[(int64_t)(u0 + m) * B.total + o] = B.U[(int64_t)(u0 + m) * B.total + o] + dt * r[m];
+    for (int m = 0; m < 5; ++m) B.Un[(int64_t)(u0 + m) * B.total + o] = CV(12 + m) + dt * r[m];
   });
 }
 
@@ -763,28 +799,64 @@ __device__ __forceinline__ R cell_dt(const V<R> &B, const ConstsT<R> &c, int i, 
   if (!(Vol > R(0.0))) return dtl;
   const R Bx = AT(cBC, i, j, k), By = AT(cBC + 1, i, j, k), Bz = AT(cBC + 2, i, j, k);
   const R B2 = Bx * Bx + By * By + Bz * Bz;
-#pragma unroll 1
-  for (int s = 0; s < 2; ++s) {
-    const int u0 = s ? cUN : cUH;
-    const R rho = dmax(AT(u0, i, j, k), R(1e-2));
-    const R ux = AT(u0 + 1, i, j, k) / rho, uy = AT(u0 + 2, i, j, k) / rho, uz = AT(u0 + 3, i, j, k) / rho;
-    const R E = AT(u0 + 4, i, j, k);
-    const R ke = R(0.5) * rho * (ux * ux + uy * uy + uz * uz);
-    const R pr = (c.gamma - R(1.0)) * (E - ke);
-    const R cs2 = c.gamma * pr / rho;
-    const R vA2 = c.inver_MA2 * B2 / rho;
-    R den = R(0.0);
-    // faces xi-, xi+, eta-, eta+, zeta-, zeta+ (the reference's summation order)
-#pragma unroll 1
+  if constexpr (sizeof(R) == 4) {
+    // FP32: the six faces' unit normals and |a| and both species' states are
+    // loaded once, up front (xi-, xi+, eta-, eta+, zeta-, zeta+: the
+    // reference's summation order)
+    R fn[6][4];
+#pragma unroll
     for (int f = 0; f < 6; ++f) {
       const int a = f >> 1, up = f & 1;
       const int cn = a == 0 ? cFNX : a == 1 ? cFNY : cFNZ;
       int fi = i, fj = j, fk = k;
       shift1(a, fi, fj, fk, up);
-      den += face_term(c, AT(cn, fi, fj, fk), AT(cn + 1, fi, fj, fk), AT(cn + 2, fi, fj, fk), AT(cn + 3, fi, fj, fk),
-                       up != 0, ux, uy, uz, Bx, By, Bz, vA2, rho, cs2);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) fn[f][q] = AT(cn + q, fi, fj, fk);
     }
-    if (den > R(0.0)) dtl = dmin(dtl, c.CFL * Vol / den);
+    R Us[2][5];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) Us[s][q] = AT((s ? cUN : cUH) + q, i, j, k);
+#pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+      const R rho = dmax(Us[s][0], R(1e-2));
+      const R ux = Us[s][1] / rho, uy = Us[s][2] / rho, uz = Us[s][3] / rho;
+      const R E = Us[s][4];
+      const R ke = R(0.5) * rho * (ux * ux + uy * uy + uz * uz);
+      const R pr = (c.gamma - R(1.0)) * (E - ke);
+      const R cs2 = c.gamma * pr / rho;
+      const R vA2 = c.inver_MA2 * B2 / rho;
+      R den = R(0.0);
+#pragma unroll
+      for (int f = 0; f < 6; ++f)
+        den += face_term(c, fn[f][0], fn[f][1], fn[f][2], fn[f][3], (f & 1) != 0, ux, uy, uz, Bx, By, Bz, vA2, rho, cs2);
+      if (den > R(0.0)) dtl = dmin(dtl, c.CFL * Vol / den);
+    }
+  } else {
+#pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+      const int u0 = s ? cUN : cUH;
+      const R rho = dmax(AT(u0, i, j, k), R(1e-2));
+      const R ux = AT(u0 + 1, i, j, k) / rho, uy = AT(u0 + 2, i, j, k) / rho, uz = AT(u0 + 3, i, j, k) / rho;
+      const R E = AT(u0 + 4, i, j, k);
+      const R ke = R(0.5) * rho * (ux * ux + uy * uy + uz * uz);
+      const R pr = (c.gamma - R(1.0)) * (E - ke);
+      const R cs2 = c.gamma * pr / rho;
+      const R vA2 = c.inver_MA2 * B2 / rho;
+      R den = R(0.0);
+      // faces xi-, xi+, eta-, eta+, zeta-, zeta+ (the reference's summation order)
+#pragma unroll 1
+      for (int f = 0; f < 6; ++f) {
+        const int a = f >> 1, up = f & 1;
+        const int cn = a == 0 ? cFNX : a == 1 ? cFNY : cFNZ;
+        int fi = i, fj = j, fk = k;
+        shift1(a, fi, fj, fk, up);
+        den += face_term(c, AT(cn, fi, fj, fk), AT(cn + 1, fi, fj, fk), AT(cn + 2, fi, fj, fk), AT(cn + 3, fi, fj, fk),
+                         up != 0, ux, uy, uz, Bx, By, Bz, vA2, rho, cs2);
+      }
+      if (den > R(0.0)) dtl = dmin(dtl, c.CFL * Vol / den);
+    }
   }
   return dtl;
 }
@@ -814,12 +886,11 @@ __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
 }
 
 // calc_PV + calc_Uplus (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:159-301) on the allocated
-// cell range, the contravariant velocities UCON where the Jacobian exists
-// ([-(g-1), n + g - 1)), and the next step's CFL dt on owned cells (CTA min,
-// one atomicMin per tile on the bit pattern of the positive double).
+// cell range the step keeps, the contravariant velocities UCON there, and
+// the next step's CFL dt on owned cells (warp min, one atomicMin per warp on
+// the bit pattern of the positive double).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir D) {
-  __shared__ R red[kTileThreads / 32];
   for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     const ConstsT<R> &c = consts_of<R>(S);
     const int i = it.i, j = it.j, k = it.k;
@@ -872,16 +943,10 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
       }
       if (i >= 0 && i < B.n0 && j >= 0 && j < B.n1 && k >= 0 && k < B.n2) dtl = cell_dt(B, c, i, j, k);
     }
+    // warp minimum, one atomicMin per warp (min is exact in any order)
     for (int o = 16; o > 0; o >>= 1) dtl = dmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dtl;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      R v = threadIdx.x < kTileThreads / 32 ? red[threadIdx.x] : R(1e100);
-      for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if (threadIdx.x == 0 && v < R(1e100))
-        atomicMin(&D.state[it.s].dt_bits, (unsigned long long)__double_as_longlong(v));
-    }
-    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && dtl < R(1e100))
+      atomicMin(&D.state[it.s].dt_bits, (unsigned long long)__double_as_longlong(dtl));
   });
 }
 
