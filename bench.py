@@ -137,6 +137,24 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------------ ranks
+def max_over_ranks(vals, device=None):
+    """Element-wise maximum of ``vals`` over all ranks (identity on one rank)."""
+    import torch
+
+    dist = torch.distributed
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in vals]
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replicas_value(world, cells_per_replica, steps, max_ms):
+    """Whole-job Mcell-updates/s of `world` replicas timed by the slowest rank."""
+    return world * cells_per_replica * steps / (max_ms * 1e-3) / 1e6
+
+
 # ------------------------------------------------------------------ workloads
 def build_workload(name: str):
     """(cells per block, static+state fields {ref name: Arr}, topology kind)"""
@@ -207,12 +225,10 @@ def run_ours(args, rank, world, device):
     torch.cuda.synchronize()
     clocks = sampler.stop() if rank == 0 else None
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+        (total_ms,) = max_over_ranks([total_ms], device)
         torch.distributed.barrier()
     info = ctx.info()
-    value = world * ncell * args.steps / (total_ms * 1e-3) / 1e6
+    value = replicas_value(world, ncell, args.steps, total_ms)
 
     # per-kernel profile (eager, events between kernels) for the roofline
     nprof = max(3, min(20, args.steps))
@@ -462,9 +478,7 @@ def run_ensemble(args, rank, world, device):
             if infos[p][s].status != 0 or infos[p][s].step != total_steps:
                 raise RuntimeError(f"batch precision {p} slot {s}: status {infos[p][s].status} step {infos[p][s].step}")
     if world > 1:
-        t = torch.tensor([mixed_ms, fp64_ms, plain_ms], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        mixed_ms, fp64_ms, plain_ms = (float(v) for v in t.tolist())
+        mixed_ms, fp64_ms, plain_ms = max_over_ranks([mixed_ms, fp64_ms, plain_ms], device)
 
     # errors: mixed batch vs plain FP64 (the FP64 path equals the reference bitwise),
     # and FP64 batch vs plain FP64 (must be identical)
@@ -483,9 +497,9 @@ def run_ensemble(args, rank, world, device):
             fp64_identical = fp64_identical and all(np.array_equal(got64[k], ref[k]) for k in ref)
     t_dl = (time.perf_counter() - t_dl0) / 2
 
-    value = world * ncell * K / (mixed_ms * 1e-3) / 1e6
-    plain = world * ncell * K / (plain_ms * 1e-3) / 1e6
-    batched64 = world * ncell * K / (fp64_ms * 1e-3) / 1e6
+    value = replicas_value(world, ncell, K, mixed_ms)
+    plain = replicas_value(world, ncell, K, plain_ms)
+    batched64 = replicas_value(world, ncell, K, fp64_ms)
     for s_ in slots[1]:
         batches[1].request(s_, 3)  # every solve active for the profiled steps
     prof = _batch_step_profile(batches[1], 3)
