@@ -58,6 +58,7 @@ enum mhd_field {
   MHD_E_XI, MHD_E_ETA, MHD_E_ZETA, MHD_EHALL_XI, MHD_EHALL_ETA, MHD_EHALL_ZETA,
   MHD_EFACE_XI, MHD_EFACE_ETA, MHD_EFACE_ZETA, MHD_EHC, MHD_HALL_BETA,
   MHD_UCON,                                   /* contravariant U_plus components along xi, eta, zeta */
+  MHD_DIVB,                                   /* div B per cell (mhd_div_b) */
   MHD_FNORM_XI, MHD_FNORM_ETA, MHD_FNORM_ZETA, /* unit normal (3) and |JD| of the faces, set by mhd_prepare */
   /* static geometry and sources (uploaded once) */
   MHD_JAC, MHD_JDXI, MHD_JDET, MHD_JDZE, MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA,
@@ -67,6 +68,7 @@ enum mhd_field {
   MHD_BCELL_W, MHD_JCELL_W, MHD_BADD_XI, MHD_BADD_ETA, MHD_BADD_ZETA, MHD_PHOTO,
   MHD_CELL_X, MHD_CELL_Y, MHD_CELL_Z,                              /* cell centres */
   MHD_TAPER_XI, MHD_TAPER_ETA, MHD_TAPER_ZETA,                     /* Hall radial taper per edge */
+  MHD_LOCAL_ETA_XI, MHD_LOCAL_ETA_ETA, MHD_LOCAL_ETA_ZETA,         /* local artificial resistivity per edge */
   MHD_NUM_FIELDS
 };
 
@@ -81,8 +83,13 @@ typedef struct mhd_constants {
   double gamma, M_H, M_Na, M_ref, T_ref, L_ref, U_ref, B_ref, n_ref, rho_ref, m_Na, k_Boltz, q_e, mu0;
   double state_coeff_H, state_coeff_Na, CFL, hall_coef, momentum_induce_coeff, momentum_hall_coeff;
   double inver_MA2, ne_hall_floor;
-  int32_t ambipolar; /* is_Ambipolar_Efield */
-  int32_t pad_;
+  /* artificial resistivity (AddArtificialResistivityToEdgeEMF_,
+   * Z4_Mercury/src/physics/MercurySolver_MagExplicit_Resis.cpp:6-64):
+   * E += eta_art(|J|/|dr|) J with eta_art rising smoothly from 0 at
+   * arti_J_start to arti_eta_max at arti_J_on; off when arti_eta_max <= 0 */
+  double arti_eta_max, arti_J_start, arti_J_on;
+  int32_t ambipolar;  /* is_Ambipolar_Efield */
+  int32_t local_arti; /* E += MHD_LOCAL_ETA * J (AddLocalArtificialResistivityToEdgeEMF_, same file :66-185) */
 } mhd_constants;
 
 /* One DOF reference in the FieldBlock index space. */
@@ -127,6 +134,7 @@ typedef struct mhd_desc {
 } mhd_desc;
 
 typedef struct mhd_ctx mhd_ctx;
+typedef struct mhd_batch mhd_batch; /* many solves on one GPU: see "batched solves" below */
 
 /* Replaces the MercurySolver constructor's device-side duties: allocates the
  * device field arena (SoA, one array per component), uploads the sync and
@@ -175,6 +183,14 @@ typedef struct mhd_info {
   int64_t remaining;   /* steps of the current request not yet taken */
 } mhd_info;
 int mhd_get_info(mhd_ctx *ctx, mhd_info *info);
+
+/* calc_divB (Z4_Mercury/src/physics/MercurySolver_MagneticCell.cpp:151-241) on
+ * the current state: MHD_DIVB = (sum of the cell's outward face fluxes) / Jac
+ * on the owned cells, and *max_abs = max |div B| over them.  (The reference
+ * zeroes the first shell next to "Pole" patches; blocks built from
+ * mhd_topology_periodic_block have none.) */
+int mhd_div_b(mhd_ctx *ctx, double *max_abs);
+int mhd_batch_div_b(mhd_batch *batch, int slot, double *max_abs);
 
 /* Static description of a field id: ncomp and mhd_location. */
 int mhd_field_info(int field, int32_t *ncomp, int32_t *location);
@@ -245,7 +261,6 @@ int mhd_hall_emf_static_scratch(const mhd_hall_block *in, double *out_xi, double
  * is active while it has steps left in its request; slots with different
  * block shapes, sync tables and constants share a batch.  mhd_ctx is a batch
  * of capacity 1.  Calls on one batch are serialised by the caller. */
-typedef struct mhd_batch mhd_batch;
 /* precision: 0 = FP64 (every field double); 1 = mixed (state, work and
  * static fields float, fluxes / EMFs / updates computed in float; the metric
  * MHD_JAC and MHD_JD* stays double).  Every solve of a batch has the batch's

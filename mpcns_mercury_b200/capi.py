@@ -20,13 +20,14 @@ FIELDS = [
     "U_H", "U_NA", "B_XI", "B_ETA", "B_ZETA",
     "PV_H", "PV_NA", "U_PLUS", "B_CELL", "BIND_CELL", "J_CELL", "J_XI", "J_ETA", "J_ZETA",
     "E_XI", "E_ETA", "E_ZETA", "EHALL_XI", "EHALL_ETA", "EHALL_ZETA",
-    "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA", "UCON", "FNORM_XI", "FNORM_ETA", "FNORM_ZETA",
+    "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA", "UCON", "DIVB", "FNORM_XI", "FNORM_ETA", "FNORM_ZETA",
     "JAC", "JDXI", "JDET", "JDZE", "AREA_XI", "AREA_ETA", "AREA_ZETA",
     "DL_XI", "DL_ETA", "DL_ZETA", "DR_XI", "DR_ETA", "DR_ZETA",
     "HODGE_FACE_XI", "HODGE_FACE_ETA", "HODGE_FACE_ZETA",
     "HODGE_EDGE_XI", "HODGE_EDGE_ETA", "HODGE_EDGE_ZETA",
     "BCELL_W", "JCELL_W", "BADD_XI", "BADD_ETA", "BADD_ZETA", "PHOTO",
     "CELL_X", "CELL_Y", "CELL_Z", "TAPER_XI", "TAPER_ETA", "TAPER_ZETA",
+    "LOCAL_ETA_XI", "LOCAL_ETA_ETA", "LOCAL_ETA_ZETA",
 ]
 FIELD_ID = {name: i for i, name in enumerate(FIELDS)}
 
@@ -51,7 +52,8 @@ REF_FIELD = {
     "Hodge_star_inverse_2form_to_1form_edge_zeta_lumped": "HODGE_EDGE_ZETA",
     "Bcell_from_Bface_w": "BCELL_W", "Jcell_from_Jedge_w": "JCELL_W",
     "Badd_xi": "BADD_XI", "Badd_eta": "BADD_ETA", "Badd_zeta": "BADD_ZETA", "Photo_rate": "PHOTO",
-    "taper_xi": "TAPER_XI", "taper_eta": "TAPER_ETA", "taper_zeta": "TAPER_ZETA",
+    "divB": "DIVB", "taper_xi": "TAPER_XI", "taper_eta": "TAPER_ETA", "taper_zeta": "TAPER_ZETA",
+    "local_arti_eta_xi": "LOCAL_ETA_XI", "local_arti_eta_eta": "LOCAL_ETA_ETA", "local_arti_eta_zeta": "LOCAL_ETA_ZETA",
 }
 
 GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL"]
@@ -63,8 +65,9 @@ class MhdConstants(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "gamma", "M_H", "M_Na", "M_ref", "T_ref", "L_ref", "U_ref", "B_ref", "n_ref", "rho_ref", "m_Na",
         "k_Boltz", "q_e", "mu0", "state_coeff_H", "state_coeff_Na", "CFL", "hall_coef",
-        "momentum_induce_coeff", "momentum_hall_coeff", "inver_MA2", "ne_hall_floor")] + [
-        ("ambipolar", ctypes.c_int32), ("pad_", ctypes.c_int32)]
+        "momentum_induce_coeff", "momentum_hall_coeff", "inver_MA2", "ne_hall_floor",
+        "arti_eta_max", "arti_J_start", "arti_J_on")] + [
+        ("ambipolar", ctypes.c_int32), ("local_arti", ctypes.c_int32)]
 
 
 class MhdDof(ctypes.Structure):
@@ -103,7 +106,7 @@ EXPORTS = [
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy",
-    "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
+    "mhd_div_b", "mhd_batch_div_b", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view",
@@ -152,6 +155,8 @@ def lib() -> ctypes.CDLL:
     L.mhd_topology_fill_desc.argtypes = [P, ctypes.POINTER(MhdDesc)]
     L.mhd_topology_destroy.argtypes = [P]
     L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
+    L.mhd_div_b.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+    L.mhd_batch_div_b.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.mhd_batch_destroy.argtypes = [P]
     L.mhd_desc_device_bytes.argtypes = [ctypes.POINTER(MhdDesc)]
     L.mhd_desc_device_bytes.restype = ctypes.c_int64
@@ -252,6 +257,12 @@ class Context:
 
     def kernels_per_step(self) -> int:
         return lib().mhd_kernels_per_step(self.ctx)
+
+    def div_b(self) -> float:
+        """max |div B| over the owned cells (MHD_DIVB holds the field)."""
+        v = ctypes.c_double()
+        check(lib().mhd_div_b(self.ctx, ctypes.byref(v)), "mhd_div_b")
+        return v.value
 
     def stream(self) -> int:
         return lib().mhd_stream(self.ctx)

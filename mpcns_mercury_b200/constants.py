@@ -12,7 +12,9 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
                         R_uni: float = 8.314, mu_mag: float = 1.256637061e-6, q_e: float = 1.602e-19,
                         U_ref: float = 4.031e5, T_ref: float = 1.7407e5, n_ref: float = 4e7,
                         M_ref: float = 0.001, B_ref: float = 1e-9, L_ref: float = 2.44e6,
-                        M_H: float = 0.001, M_Na: float = 0.023) -> MhdConstants:
+                        M_H: float = 0.001, M_Na: float = 0.023, arti_eta_max: float = 0.0,
+                        arti_J_start: float = 800.0, arti_J_on: float = 3000.0,
+                        local_arti: bool = False) -> MhdConstants:
     c = MhdConstants()
     c.gamma = gamma
     c.q_e = q_e
@@ -37,4 +39,10 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
     c.inver_MA2 = B_ref * B_ref / (U_ref * U_ref * mu_mag * c.rho_ref)
     c.ne_hall_floor = 0.01
     c.ambipolar = 1 if ambipolar else 0
+    # artificial resistivity (arti_eta_max, J_range_start, J_range_on,
+    # is_local_artificial_resistivity of the MHD control file)
+    c.arti_eta_max = arti_eta_max
+    c.arti_J_start = arti_J_start
+    c.arti_J_on = arti_J_on
+    c.local_arti = 1 if local_arti else 0
     return c

@@ -681,7 +681,8 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
                      k.n_ref,         k.rho_ref,   k.m_Na,        k.k_Boltz,
                      k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
                      k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
-                     k.inver_MA2,     k.ne_hall_floor, k.ambipolar, desc->nghost};
+                     k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
+                     k.ambipolar,     k.local_arti, desc->nghost};
   if (cudaMallocAsync((void **)&S->arena, S->arena_bytes, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
@@ -758,7 +759,8 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
                        k.n_ref,         k.rho_ref,   k.m_Na,        k.k_Boltz,
                        k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
                        k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
-                       k.inver_MA2,     k.ne_hall_floor, k.ambipolar, S->nghost};
+                       k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
+                       k.ambipolar,     k.local_arti, S->nghost};
   }
   auto bail = [&](int code) {
     free_solve(S, st);
@@ -892,6 +894,21 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   });
   if (rc) return rc;
   b->slots[slot]->prepared = true;  // asynchronous: stream-ordered with the batch's other work
+  return MHD_OK;
+}
+
+int mhd_batch_div_b(mhd_batch *b, int slot, double *max_abs) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  const unsigned long long zero = 0;
+  if ((rc = set_state_field(b, slot, offsetof(SolveState, divb_bits), &zero, sizeof zero))) return rc;
+  rc = targeted(b, slot, [&](int *nk) { launch(b, 1, SK_DIVB, nk); });
+  if (rc) return rc;
+  if ((rc = read_state(b))) return rc;
+  unsigned long long bits = b->hstate[slot].divb_bits;
+  double v;
+  std::memcpy(&v, &bits, sizeof v);
+  if (max_abs) *max_abs = v;
   return MHD_OK;
 }
 
@@ -1100,6 +1117,11 @@ int mhd_step_profiled(mhd_ctx *ctx, int nsteps, int max_kernels, float *kernel_m
   rc = mhd_batch_step_profiled(ctx->batch, nsteps, max_kernels, kernel_ms, kernel_names, n_kernels);
   if (rc) return rc;
   return mhd_synchronize(ctx);
+}
+
+int mhd_div_b(mhd_ctx *ctx, double *max_abs) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_div_b(ctx->batch, 0, max_abs);
 }
 
 int mhd_sync(mhd_ctx *ctx, int group) {

@@ -65,7 +65,9 @@ struct ConstsT {
   T gamma, M_H, M_Na, M_ref, T_ref, L_ref, U_ref, B_ref, n_ref, rho_ref, m_Na, k_Boltz, q_e, mu0;
   T state_coeff_H, state_coeff_Na, CFL, hall_coef, momentum_induce_coeff, momentum_hall_coeff;
   T inver_MA2, ne_hall_floor;
+  T arti_eta_max, arti_J_start, arti_J_on;
   int ambipolar;
+  int local_arti;
   int nghost;
 };
 using Consts = ConstsT<double>;
@@ -74,8 +76,9 @@ inline ConstsT<float> to_float(const Consts &c) {
                         (float)c.L_ref, (float)c.U_ref, (float)c.B_ref, (float)c.n_ref, (float)c.rho_ref,
                         (float)c.m_Na, (float)c.k_Boltz, (float)c.q_e, (float)c.mu0, (float)c.state_coeff_H,
                         (float)c.state_coeff_Na, (float)c.CFL, (float)c.hall_coef, (float)c.momentum_induce_coeff,
-                        (float)c.momentum_hall_coeff, (float)c.inver_MA2, (float)c.ne_hall_floor, c.ambipolar,
-                        c.nghost};
+                        (float)c.momentum_hall_coeff, (float)c.inver_MA2, (float)c.ne_hall_floor,
+                        (float)c.arti_eta_max, (float)c.arti_J_start, (float)c.arti_J_on, c.ambipolar,
+                        c.local_arti, c.nghost};
 }
 
 // Per-solve device state.
@@ -88,6 +91,7 @@ struct SolveState {
   int cur;                     // which U buffer holds the current state
   int mask;                    // selected for a targeted pass (Dir::mode == 1)
   int pad_;
+  unsigned long long divb_bits;  // max |div B| of the last mhd_div_b (non-negative double bits)
 };
 
 // Sync tables of one solve address DOFs by "codes": the byte offset from the

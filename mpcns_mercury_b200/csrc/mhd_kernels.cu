@@ -35,6 +35,7 @@ constexpr int cEX = kComp.first[MHD_E_XI], cEY = kComp.first[MHD_E_ETA], cEZ = k
 constexpr int cHX = kComp.first[MHD_EHALL_XI], cHY = kComp.first[MHD_EHALL_ETA], cHZ = kComp.first[MHD_EHALL_ZETA];
 constexpr int cEFX = kComp.first[MHD_EFACE_XI], cEFY = kComp.first[MHD_EFACE_ETA], cEFZ = kComp.first[MHD_EFACE_ZETA];
 constexpr int cEHC = kComp.first[MHD_EHC], cHB = kComp.first[MHD_HALL_BETA], cUC = kComp.first[MHD_UCON];
+constexpr int cDIVB = kComp.first[MHD_DIVB];
 constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA], cFNZ = kComp.first[MHD_FNORM_ZETA];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
@@ -49,6 +50,7 @@ constexpr int cWB = kComp.first[MHD_BCELL_W], cWJ = kComp.first[MHD_JCELL_W];
 constexpr int cBAX = kComp.first[MHD_BADD_XI], cBAY = kComp.first[MHD_BADD_ETA], cBAZ = kComp.first[MHD_BADD_ZETA];
 constexpr int cPHOTO = kComp.first[MHD_PHOTO], cCX = kComp.first[MHD_CELL_X];  // CELL_Y, CELL_Z follow
 constexpr int cTPX = kComp.first[MHD_TAPER_XI], cTPY = kComp.first[MHD_TAPER_ETA], cTPZ = kComp.first[MHD_TAPER_ZETA];
+constexpr int cLEX = kComp.first[MHD_LOCAL_ETA_XI];  // LOCAL_ETA_ETA, LOCAL_ETA_ZETA follow
 
 // std::max / std::min semantics (first argument wins ties, incl. signed zeros).
 template <class R>
@@ -290,6 +292,33 @@ __device__ __forceinline__ R pe_node(const V<R> &B, int i, int j, int k) {
   return R(0.125) * sum;
 }
 
+// AddArtificialResistivityToEdgeEMF_ and AddLocalArtificialResistivityToEdgeEMF_
+// (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Resis.cpp:6-64, 66-185) on one owned edge of
+// family `axis`: E += eta_art(|J| / |dr|) J, then E += eta_local J.
+template <class R>
+__device__ __forceinline__ R add_artificial(const V<R> &B, const ConstsT<R> &c, int axis, int i, int j, int k, R e) {
+  const int cj = axis == 0 ? cJX : axis == 1 ? cJY : cJZ;
+  if (c.arti_eta_max > R(0.0)) {
+    const int cd = axis == 0 ? cDRX : axis == 1 ? cDRY : cDRZ;
+    const R J1 = AT(cj, i, j, k);
+    const R dx = AT(cd, i, j, k), dy = AT(cd + 1, i, j, k), dz = AT(cd + 2, i, j, k);
+    const R dr_len = sqrt(dx * dx + dy * dy + dz * dz);
+    const R Jmag = fabs(J1) / dmax(dr_len, R(1.0e-30));
+    R eta;
+    if (c.arti_J_on <= c.arti_J_start) {
+      eta = (Jmag > c.arti_J_start) ? c.arti_eta_max : R(0.0);
+    } else {
+      R q = (Jmag - c.arti_J_start) / (c.arti_J_on - c.arti_J_start);
+      q = dmax(R(0.0), dmin(R(1.0), q));
+      const R S = q * q * (R(3.0) - R(2.0) * q);
+      eta = c.arti_eta_max * S;
+    }
+    e += eta * J1;
+  }
+  if (c.local_arti) e += AT(cLEX + axis, i, j, k) * AT(cj, i, j, k);
+  return e;
+}
+
 // AssembleEdgeEMF_FromFaceE_Ideal_ (Ideal.cpp:138-372) + AddAmbipolarEdgeEMF_
 // (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Ambipo.cpp:3-143) on the owned edges.
 template <class R>
@@ -317,7 +346,7 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
           }
         e -= pc * (p1 - p0) / num_limiter(c, R(0.25) * rH, R(0.25) * rN).ne_eff;
       }
-      AT(cEX, i, j, k) = e;
+      AT(cEX, i, j, k) = add_artificial(B, c, 0, i, j, k, e);
     }
     if (j < B.n1) {
       const R Ec = R(0.25) * (AT(cEFX + 1, i, j, k) + AT(cEFX + 1, i, j, k - 1) + AT(cEFZ + 1, i, j, k) +
@@ -337,7 +366,7 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
           }
         e -= pc * (p1 - p0) / num_limiter(c, R(0.25) * rH, R(0.25) * rN).ne_eff;
       }
-      AT(cEY, i, j, k) = e;
+      AT(cEY, i, j, k) = add_artificial(B, c, 1, i, j, k, e);
     }
     if (k < B.n2) {
       const R Ec = R(0.25) * (AT(cEFX + 2, i, j, k) + AT(cEFX + 2, i, j - 1, k) + AT(cEFY + 2, i, j, k) +
@@ -357,7 +386,7 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
           }
         e -= pc * (p1 - p0) / num_limiter(c, R(0.25) * rH, R(0.25) * rN).ne_eff;
       }
-      AT(cEZ, i, j, k) = e;
+      AT(cEZ, i, j, k) = add_artificial(B, c, 2, i, j, k, e);
     }
   });
 }
@@ -861,6 +890,26 @@ __device__ __forceinline__ R cell_dt(const V<R> &B, const ConstsT<R> &c, int i, 
   return dtl;
 }
 
+// calc_divB (Z4_Mercury/src/physics/MercurySolver_MagneticCell.cpp:186-193) on the owned cells,
+// and max |div B| per solve (atomicMax on the bits of the non-negative double).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_div_b(Dir D) {
+  for_items<R, kCells>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    R v = R(0.0);
+    if (it.in) {
+      const int i = it.i, j = it.j, k = it.k;
+      v = (AT(cBX, i + 1, j, k) - AT(cBX, i, j, k) + AT(cBY, i, j + 1, k) - AT(cBY, i, j, k) + AT(cBZ, i, j, k + 1) -
+           AT(cBZ, i, j, k)) /
+          R(ATM(cJAC, i, j, k));
+      AT(cDIVB, i, j, k) = v;
+    }
+    double a = fabs((double)v);
+    if (!(a == a)) a = __longlong_as_double(0x7ff0000000000000LL);  // NaN counts as infinite
+    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&D.state[it.s].divb_bits, (unsigned long long)__double_as_longlong(a));
+  });
+}
+
 // Static per-face terms of the CFL time step and the Rusanov wave speed, once
 // per solve (run by mhd_prepare): |a| = sqrt(ax ax + ay ay + az az) and
 // a / |a| of the face area vectors JD, the operations and order
@@ -1072,6 +1121,7 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_PV_UPLUS: k_pv_uplus<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
     case SK_SYNC: k_sync<R><<<g_grid_copy, 256, 0, st>>>(D, *ops); break;
     case SK_FACE_NORMALS: k_face_normals<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_DIVB: k_div_b<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
     default: break;
@@ -1089,7 +1139,7 @@ void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncO
 const char *step_kernel_name(StepKernel k) {
   static const char *names[] = {"k_face_emf", "k_edge_emf", "k_hall_cell", "k_hall_edge", "k_add_hall",
                                 "k_fluid",    "k_bface",    "k_bcell_jedge", "k_jcell",   "k_pv_uplus",
-                                "k_sync",     "k_flip",     "k_retire",      "k_face_normals"};
+                                "k_sync",     "k_flip",     "k_retire",      "k_face_normals", "k_div_b"};
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }
 

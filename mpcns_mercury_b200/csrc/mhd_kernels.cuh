@@ -8,7 +8,7 @@ namespace mhd {
 
 enum StepKernel {
   SK_FACE_EMF = 0, SK_EDGE_EMF, SK_HALL_CELL, SK_HALL_EDGE, SK_ADD_HALL, SK_FLUID, SK_BFACE, SK_BCELL_JEDGE,
-  SK_JCELL, SK_PV_UPLUS, SK_SYNC, SK_FLIP, SK_RETIRE, SK_FACE_NORMALS, SK_COUNT
+  SK_JCELL, SK_PV_UPLUS, SK_SYNC, SK_FLIP, SK_RETIRE, SK_FACE_NORMALS, SK_DIVB, SK_COUNT
 };
 
 // One launch of k_sync runs up to two independent sync operations: a copy

@@ -37,14 +37,14 @@ constexpr FieldSpec kFieldSpec[MHD_NUM_FIELDS] = {
     {3, MHD_CELL},      {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA}, {1, MHD_EDGE_XI},
     {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA},
     {3, MHD_FACE_XI},   {3, MHD_FACE_ETA},  {3, MHD_FACE_ZETA}, {3, MHD_CELL},      {1, MHD_CELL},
-    {3, MHD_CELL} /* UCON */,
+    {3, MHD_CELL} /* UCON */, {1, MHD_CELL} /* DIVB */,
     {4, MHD_FACE_XI},   {4, MHD_FACE_ETA},  {4, MHD_FACE_ZETA} /* FNORM */, {1, MHD_CELL},      {3, MHD_FACE_XI},   {3, MHD_FACE_ETA},  {3, MHD_FACE_ZETA}, {1, MHD_FACE_XI},
     {1, MHD_FACE_ETA},  {1, MHD_FACE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA},
     {3, MHD_EDGE_XI},   {3, MHD_EDGE_ETA},  {3, MHD_EDGE_ZETA}, {1, MHD_FACE_XI},   {1, MHD_FACE_ETA},
     {1, MHD_FACE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA}, {18, MHD_CELL},
     {36, MHD_CELL},     {1, MHD_FACE_XI},   {1, MHD_FACE_ETA},  {1, MHD_FACE_ZETA}, {1, MHD_CELL},
     {1, MHD_CELL},      {1, MHD_CELL},      {1, MHD_CELL},      {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},
-    {1, MHD_EDGE_ZETA}};
+    {1, MHD_EDGE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA} /* LOCAL_ETA */};
 
 // Stagger: 1 where the location is node-like (n + 1 owned DOFs) along an axis.
 constexpr int kStagger[7][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 0}};

@@ -171,16 +171,16 @@ std::string setup_mhd() {
   o << "bool    is_Ambipolar_Efield " << job_int("ambipolar", 1) << "\n";
   o << "double  r_min " << job_dbl("hall_r_min", 0.0) << "\n";
   o << "double  r_max " << job_dbl("hall_r_max", 0.0) << "\n";
-  o << "double  arti_eta_max 0.00\n";
-  o << "double  J_range_start 800.0\n";
-  o << "double  J_range_on 3000.0\n";
-  o << "bool    is_local_artificial_resistivity 0\n";
-  o << "double  local_arti_eta_max 0.1\n";
-  o << "double  local_arti_x0 1.53\n";
-  o << "double  local_arti_y0 0.0\n";
-  o << "double  local_arti_z0 0.25\n";
-  o << "double  local_arti_r_decay 0.05\n";
-  o << "double  local_arti_r_cutoff 0.05\n";
+  o << "double  arti_eta_max " << job_dbl("arti_eta_max", 0.0) << "\n";
+  o << "double  J_range_start " << job_dbl("arti_J_start", 800.0) << "\n";
+  o << "double  J_range_on " << job_dbl("arti_J_on", 3000.0) << "\n";
+  o << "bool    is_local_artificial_resistivity " << job_int("local_arti", 0) << "\n";
+  o << "double  local_arti_eta_max " << job_dbl("local_arti_eta_max", 0.1) << "\n";
+  o << "double  local_arti_x0 " << job_dbl("local_arti_x0", 1.53) << "\n";
+  o << "double  local_arti_y0 " << job_dbl("local_arti_y0", 0.0) << "\n";
+  o << "double  local_arti_z0 " << job_dbl("local_arti_z0", 0.25) << "\n";
+  o << "double  local_arti_r_decay " << job_dbl("local_arti_r_decay", 0.05) << "\n";
+  o << "double  local_arti_r_cutoff " << job_dbl("local_arti_r_cutoff", 0.05) << "\n";
   o << "END_OF_FILE\n";
   return o.str();
 }
@@ -657,6 +657,31 @@ void dump_taper(MercurySolver &S, Dumper &d) {
     }
 }
 
+// Local artificial resistivity per edge as the reference fills it on its first
+// use (AddLocalArtificialResistivityToEdgeEMF_,
+// Z4_Mercury/src/physics/MercurySolver_MagExplicit_Resis.cpp:117-158): the harness triggers that fill
+// once before stepping (the E field is zeroed at the start of every step, so
+// the extra contribution is discarded) and dumps the arrays over the E box.
+void dump_local_eta(MercurySolver &S, Dumper &d) {
+  S.AddLocalArtificialResistivityToEdgeEMF_();
+  Field *fld = S.fld_;
+  const int fids[3] = {S.fid_.fid_E.xi, S.fid_.fid_E.eta, S.fid_.fid_E.zeta};
+  const char *names[3] = {"local_arti_eta_xi", "local_arti_eta_eta", "local_arti_eta_zeta"};
+  for (int a = 0; a < 3; ++a)
+    for (int ib = 0; ib < fld->num_blocks(); ++ib) {
+      FieldBlock &E = fld->field(fids[a], ib);
+      auto &eta = a == 0 ? S.local_arti_eta_xi_[ib] : a == 1 ? S.local_arti_eta_eta_[ib] : S.local_arti_eta_ze_[ib];
+      const Int3 lo = E.get_lo(), hi = E.get_hi();
+      const int ni = hi.i - lo.i, nj = hi.j - lo.j, nk = hi.k - lo.k;
+      std::vector<double> t((size_t)ni * nj * nk, 0.0);
+      for (int i = lo.i; i < hi.i; ++i)
+        for (int j = lo.j; j < hi.j; ++j)
+          for (int k = lo.k; k < hi.k; ++k) t[((size_t)(i - lo.i) * nj + (j - lo.j)) * nk + (k - lo.k)] = eta(i, j, k);
+      const int l[3] = {lo.i, lo.j, lo.k}, h[3] = {hi.i, hi.j, hi.k};
+      d.rec(std::string("static:") + names[a], ib, l, h, 1, t.data());
+    }
+}
+
 // Edge alias classes exactly as ReduceEdgeAliasCandidatesToOwners_ consumes
 // them (Z4_Mercury/src/physics/MercurySolver_Current.cpp:8-35): classes with a
 // global id and more than one member, sorted by global id; per class the owner
@@ -759,6 +784,7 @@ int main(int argc, char **argv) {
       for (auto &name : static_fields) dump_field(d, fld, name, "static:");
       if (job_int("dump_grid", 0)) dump_grid(d, grd);
       if (job_int("dump_taper", 0)) dump_taper(S, d);
+      if (job_int("local_arti", 0)) dump_local_eta(S, d);
       const auto state_fields = split_ws(job_str("dump_fields", "U_H U_Na B_xi B_eta B_zeta"));
       const long steps = job_int("steps", 1);
       std::vector<long> at;
@@ -767,6 +793,7 @@ int main(int argc, char **argv) {
         for (long a : at)
           if (a == step) {
             const std::string tag = "step" + std::to_string(step) + ":";
+            if (job_int("calc_divb", 0)) S.calc_divB();  // the reference's output-step diagnostic
             for (auto &name : state_fields) dump_field(d, fld, name, tag);
             const double meta[2] = {S.dt, S.run_data_->time};
             const int l[3] = {0, 0, 0}, h[3] = {1, 1, 2};
