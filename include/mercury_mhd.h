@@ -69,6 +69,10 @@ enum mhd_field {
   MHD_CELL_X, MHD_CELL_Y, MHD_CELL_Z,                              /* cell centres */
   MHD_TAPER_XI, MHD_TAPER_ETA, MHD_TAPER_ZETA,                     /* Hall radial taper per edge */
   MHD_LOCAL_ETA_XI, MHD_LOCAL_ETA_ETA, MHD_LOCAL_ETA_ZETA,         /* local artificial resistivity per edge */
+  MHD_ETA_RES_XI, MHD_ETA_RES_ETA, MHD_ETA_RES_ZETA,               /* implicit resistivity per owned edge */
+  /* work of the implicit resistive solve (3 components: xi, eta, zeta edges;
+   * BSTAR: xi, eta, zeta faces) */
+  MHD_RES_W, MHD_RES_X, MHD_RES_R, MHD_RES_P, MHD_RES_Q, MHD_RES_BSTAR,
   MHD_NUM_FIELDS
 };
 
@@ -90,6 +94,15 @@ typedef struct mhd_constants {
   double arti_eta_max, arti_J_start, arti_J_on;
   int32_t ambipolar;  /* is_Ambipolar_Efield */
   int32_t local_arti; /* E += MHD_LOCAL_ETA * J (AddLocalArtificialResistivityToEdgeEMF_, same file :66-185) */
+  /* implicit resistive substep (SolveImplicitResistiveDiffusion_,
+   * Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:475-555): after the
+   * explicit update, solve (I + dt eta alpha C^T beta C) E = eta J(B*) on the
+   * owned edges with eta > 0 (eta: MHD_ETA_RES_*), then B = B* - dt curl E.
+   * Solved by preconditioned CG to ||A E - b|| <= res_rtol ||b|| (at most
+   * res_max_it iterations, else MHD_ERR_SOLVE).  FP64 solves only. */
+  double res_rtol;
+  int32_t resistive;  /* is_Mercury_resistance */
+  int32_t res_max_it;
 } mhd_constants;
 
 /* One DOF reference in the FieldBlock index space. */

@@ -27,7 +27,8 @@ FIELDS = [
     "HODGE_EDGE_XI", "HODGE_EDGE_ETA", "HODGE_EDGE_ZETA",
     "BCELL_W", "JCELL_W", "BADD_XI", "BADD_ETA", "BADD_ZETA", "PHOTO",
     "CELL_X", "CELL_Y", "CELL_Z", "TAPER_XI", "TAPER_ETA", "TAPER_ZETA",
-    "LOCAL_ETA_XI", "LOCAL_ETA_ETA", "LOCAL_ETA_ZETA",
+    "LOCAL_ETA_XI", "LOCAL_ETA_ETA", "LOCAL_ETA_ZETA", "ETA_RES_XI", "ETA_RES_ETA", "ETA_RES_ZETA",
+    "RES_W", "RES_X", "RES_R", "RES_P", "RES_Q", "RES_BSTAR",
 ]
 FIELD_ID = {name: i for i, name in enumerate(FIELDS)}
 
@@ -53,6 +54,7 @@ REF_FIELD = {
     "Bcell_from_Bface_w": "BCELL_W", "Jcell_from_Jedge_w": "JCELL_W",
     "Badd_xi": "BADD_XI", "Badd_eta": "BADD_ETA", "Badd_zeta": "BADD_ZETA", "Photo_rate": "PHOTO",
     "divB": "DIVB", "taper_xi": "TAPER_XI", "taper_eta": "TAPER_ETA", "taper_zeta": "TAPER_ZETA",
+    "eta_res_xi": "ETA_RES_XI", "eta_res_eta": "ETA_RES_ETA", "eta_res_zeta": "ETA_RES_ZETA",
     "local_arti_eta_xi": "LOCAL_ETA_XI", "local_arti_eta_eta": "LOCAL_ETA_ETA", "local_arti_eta_zeta": "LOCAL_ETA_ZETA",
 }
 
@@ -67,7 +69,8 @@ class MhdConstants(ctypes.Structure):
         "k_Boltz", "q_e", "mu0", "state_coeff_H", "state_coeff_Na", "CFL", "hall_coef",
         "momentum_induce_coeff", "momentum_hall_coeff", "inver_MA2", "ne_hall_floor",
         "arti_eta_max", "arti_J_start", "arti_J_on")] + [
-        ("ambipolar", ctypes.c_int32), ("local_arti", ctypes.c_int32)]
+        ("ambipolar", ctypes.c_int32), ("local_arti", ctypes.c_int32), ("res_rtol", ctypes.c_double),
+        ("resistive", ctypes.c_int32), ("res_max_it", ctypes.c_int32)]
 
 
 class MhdDof(ctypes.Structure):

@@ -14,7 +14,8 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
                         M_ref: float = 0.001, B_ref: float = 1e-9, L_ref: float = 2.44e6,
                         M_H: float = 0.001, M_Na: float = 0.023, arti_eta_max: float = 0.0,
                         arti_J_start: float = 800.0, arti_J_on: float = 3000.0,
-                        local_arti: bool = False) -> MhdConstants:
+                        local_arti: bool = False, resistive: bool = False, res_rtol: float = 1e-13,
+                        res_max_it: int = 500) -> MhdConstants:
     c = MhdConstants()
     c.gamma = gamma
     c.q_e = q_e
@@ -45,4 +46,8 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
     c.arti_J_start = arti_J_start
     c.arti_J_on = arti_J_on
     c.local_arti = 1 if local_arti else 0
+    # implicit resistive substep (is_Mercury_resistance; the per-edge eta is a field)
+    c.resistive = 1 if resistive else 0
+    c.res_rtol = res_rtol
+    c.res_max_it = res_max_it
     return c

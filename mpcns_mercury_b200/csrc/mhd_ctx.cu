@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstddef>
 #include <cstdio>
@@ -114,6 +115,8 @@ struct Solve {
   char *arena = nullptr;
   DevBlock *dblocks = nullptr;
   Tables *T = nullptr;
+  double res_rtol = 0.0;
+  int res_max_it = 0;
   Consts consts{};
 
   int comp_bytes(int c) const { return is_metric(c) ? 8 : es; }
@@ -157,6 +160,10 @@ struct mhd_batch {
   int *dprefix_copy[kMaxGroups][3] = {};
   int *dprefix_aliasE = nullptr, *dprefix_aliasJ = nullptr;
   cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph_a = nullptr, graph_b = nullptr;  // the step split around implicit resistive solves
+  int n_res = 0;                                        // slots whose solve has the implicit resistive substep
+  ResScratch res{nullptr, nullptr};
+  double *hres = nullptr;                               // pinned copy of res.result
   int kernels_per_step = 0;
   double *staging = nullptr;
   size_t staging_elems = 0;
@@ -204,8 +211,9 @@ void mark(mhd_batch *b, const char *name) {
   cudaEventRecord(b->prof_events[b->prof_used++], b->stream);
 }
 
-void launch(mhd_batch *b, int mode, StepKernel k, int *nk, const SyncOps *ops = nullptr) {
-  launch_step_kernel(k, b->dir(mode), b->stream, ops, b->precision);
+void launch(mhd_batch *b, int mode, StepKernel k, int *nk, const SyncOps *ops = nullptr, int iarg = 0,
+            double darg = 0.0) {
+  launch_step_kernel(k, b->dir(mode), b->stream, ops, b->precision, iarg, darg, b->res);
   ++*nk;
   mark(b, step_kernel_name(k));
 }
@@ -245,8 +253,11 @@ void enqueue_derived(mhd_batch *b, int mode, int *nk) {
   launch(b, mode, SK_PV_UPLUS, nk);
 }
 
-// StepOnce (Z4_Mercury/src/MercurySolver_Driver.cpp:21-61) for every active slot.
-void enqueue_step(mhd_batch *b, int *nk) {
+// StepOnce (Z4_Mercury/src/MercurySolver_Driver.cpp:21-61) for every active slot, in two
+// parts: A up to the Euler update and Sync(U), Sync(B faces); B the derived
+// refresh.  With implicit resistive solves, their substep
+// (Driver.cpp:33-38) runs between A and B and B starts with Sync(B faces).
+void enqueue_step_a(mhd_batch *b, int *nk) {
   const int m = 0;
   // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171);
   // the E alias reduction (ideal EMF) and Sync(Ehall) touch different fields
@@ -265,8 +276,16 @@ void enqueue_step(mhd_batch *b, int *nk) {
   launch(b, m, SK_FLIP, nk);
   sync2(b, m, copy_op(MHD_SYNC_UCELL, 0), copy_op(MHD_SYNC_BFACE, 0), nk);
   sync2(b, m, copy_op(MHD_SYNC_UCELL, 1), copy_op(MHD_SYNC_BFACE, 1), nk);
+}
+void enqueue_step_b(mhd_batch *b, int *nk, bool resync_b) {
+  const int m = 0;
+  if (resync_b) enqueue_sync(b, m, MHD_SYNC_BFACE, nk);
   enqueue_derived(b, m, nk);
   launch(b, m, SK_RETIRE, nk);
+}
+void enqueue_step(mhd_batch *b, int *nk) {
+  enqueue_step_a(b, nk);
+  enqueue_step_b(b, nk, false);
 }
 
 int ensure_staging(mhd_batch *b, size_t elems) {  // elems doubles
@@ -495,19 +514,100 @@ int targeted(mhd_batch *b, int slot, F &&enqueue) {
   return set_state_field(b, slot, offsetof(SolveState, mask), &zero, sizeof zero);
 }
 
-int build_graph(mhd_batch *b) {
-  if (b->graph) return MHD_OK;
+template <class F>
+int capture(mhd_batch *b, cudaGraphExec_t *out, int *nk_out, F &&enqueue) {
+  if (*out) return MHD_OK;
   cudaGraph_t g = nullptr;
   CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   int nk = 0;
-  enqueue_step(b, &nk);
+  enqueue(&nk);
   cudaError_t e = cudaStreamEndCapture(b->stream, &g);
   if (e != cudaSuccess) return fail(MHD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&b->graph, g, 0);
+  e = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(MHD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-  b->kernels_per_step = nk;
+  if (nk_out) *nk_out = nk;
   return MHD_OK;
+}
+
+int build_graph(mhd_batch *b) {
+  return capture(b, &b->graph, &b->kernels_per_step, [&](int *nk) { enqueue_step(b, nk); });
+}
+
+// Dot product of the CG (2 values) into b->hres.
+int res_dot(mhd_batch *b, int op) {
+  int nk = 0;
+  launch(b, 1, SK_RES_DOT, &nk, nullptr, op);
+  launch(b, 1, SK_RES_SUM, &nk);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(b->hres, b->res.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return MHD_OK;
+}
+
+// q = A p (MatMultImplicitResistive_, Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:420-472):
+// E_res from p, its owner copies, dB = -dt curl E_res, Sync(dB), dJ, its
+// alias reduction and owner copies, q = E_res - eta dJ.
+void res_apply(mhd_batch *b, int *nk) {
+  launch(b, 1, SK_RES_VEC, nk, nullptr, RES_E_FROM_P);
+  sync1(b, 1, copy_op(MHD_SYNC_EEDGE, 1), nk);
+  launch(b, 1, SK_RES_DB, nk);
+  enqueue_sync(b, 1, MHD_SYNC_BFACE, nk);
+  launch(b, 1, SK_RES_DJ, nk);
+  sync1(b, 1, alias_op(1), nk);
+  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, 1), nk);
+  launch(b, 1, SK_RES_Q, nk);
+}
+
+// The implicit resistive substep of one solve (SolveImplicitResistiveDiffusion_,
+// Mercury_ImplicitResistive.cpp:475-555), after the explicit update and its
+// Sync(B faces): B* snapshot, J(B*), b = eta J(B*), CG in the inner product
+// weighted by 1 / (eta alpha) (A is self-adjoint in it), then B = B* - dt
+// curl E_res.  The reference solves with GMRES; the solution is the same to
+// the solvers' tolerance.
+int res_solve(mhd_batch *b, int slot) {
+  Solve *S = b->slots[slot];
+  const int one = 1, zero = 0;
+  int rc = set_state_field(b, slot, offsetof(SolveState, mask), &one, sizeof one);
+  if (rc) return rc;
+  int nk = 0;
+  launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_SNAPSHOT);
+  launch(b, 1, SK_BCELL_JEDGE, &nk);  // Calc_J_Edge on B* (B_cell is refreshed again after the substep)
+  sync1(b, 1, alias_op(1), &nk);
+  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, 1), &nk);
+  launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_INIT);
+  if ((rc = res_dot(b, RES_DOT_RR))) return rc;
+  double rho = b->hres[0];
+  const double bnorm = std::sqrt(b->hres[1]);
+  const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-13;
+  bool converged = bnorm == 0.0;
+  for (int it = 0; it < S->res_max_it && !converged; ++it) {
+    res_apply(b, &nk);
+    if ((rc = res_dot(b, RES_DOT_PQ))) return rc;
+    const double pq = b->hres[0];
+    if (!(pq > 0.0)) break;  // breakdown: not positive definite on these unknowns
+    const double alpha = rho / pq;
+    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_AXPY, alpha);
+    if ((rc = res_dot(b, RES_DOT_RR))) return rc;
+    const double rho_new = b->hres[0];
+    if (std::sqrt(b->hres[1]) <= rtol * bnorm) {
+      converged = true;
+      break;
+    }
+    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_PUPD, rho_new / rho);
+    rho = rho_new;
+  }
+  if (!converged) {
+    const int st = MHD_ERR_SOLVE;
+    if ((rc = set_state_field(b, slot, offsetof(SolveState, status), &st, sizeof st))) return rc;
+  }
+  // E_res = x, its owner copies; B = B* + dt (-curl E_res) on the owned faces
+  launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_E_FROM_X);
+  sync1(b, 1, copy_op(MHD_SYNC_EEDGE, 1), &nk);
+  launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_RESTORE);
+  launch(b, 1, SK_RES_BUPDATE, &nk);
+  CUDA_TRY(cudaGetLastError());
+  return set_state_field(b, slot, offsetof(SolveState, mask), &zero, sizeof zero);
 }
 
 int xfer(mhd_batch *b, int slot, int field, int block, const int32_t lo[3], const int32_t hi[3], int ncomp,
@@ -574,6 +674,10 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
   if (cudaMalloc(&b->dprefix_aliasE, sizeof(int) * C1) != cudaSuccess ||
       cudaMalloc(&b->dprefix_aliasJ, sizeof(int) * C1) != cudaSuccess)
     return bail(fail(MHD_ERR_OOM, "prefix"));
+  if (cudaMalloc(&b->res.partial, sizeof(double) * 2 * res_dot_grid()) != cudaSuccess ||
+      cudaMalloc(&b->res.result, sizeof(double) * 2) != cudaSuccess ||
+      cudaMallocHost(&b->hres, sizeof(double) * 2) != cudaSuccess)
+    return bail(fail(MHD_ERR_OOM, "solver scratch"));
   if (cudaMemsetAsync(b->dstate, 0, sizeof(SolveState) * capacity, b->stream) != cudaSuccess)
     return bail(fail(MHD_ERR_CUDA, "state init"));
   int rc = publish(b);
@@ -587,6 +691,11 @@ int mhd_batch_destroy(mhd_batch *b) {
   if (!b) return MHD_OK;
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->graph_a) cudaGraphExecDestroy(b->graph_a);
+  if (b->graph_b) cudaGraphExecDestroy(b->graph_b);
+  cudaFree(b->res.partial);
+  cudaFree(b->res.result);
+  if (b->hres) cudaFreeHost(b->hres);
   for (auto *S : b->slots) free_solve(S, b->stream);
   if (b->staging) cudaFreeAsync(b->staging, b->stream);
   if (b->stream) cudaStreamSynchronize(b->stream);
@@ -632,6 +741,8 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   if (desc->nghost < 2) return fail(MHD_ERR_ARG, "mhd_batch_add: nghost %d (the step's stencils need >= 2)", desc->nghost);
   if (desc->precision != b->precision)
     return fail(MHD_ERR_ARG, "solve precision %d differs from the batch's (%d)", desc->precision, b->precision);
+  if (desc->constants.resistive && b->precision != kFP64)
+    return fail(MHD_ERR_ARG, "the implicit resistive substep is available in FP64 only");
   if (desc->n_blocks >= (1 << 15)) return fail(MHD_ERR_ARG, "too many blocks (%d)", desc->n_blocks);
   int slot = -1;
   for (int s = 0; s < b->capacity; ++s)
@@ -682,7 +793,7 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
                      k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
                      k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
                      k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
-                     k.ambipolar,     k.local_arti, desc->nghost};
+                     k.ambipolar,     k.local_arti, desc->nghost, k.resistive};
   if (cudaMallocAsync((void **)&S->arena, S->arena_bytes, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
@@ -718,7 +829,10 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   SolveState s0{};
   s0.dt_bits = kDtUnset;
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
+  S->res_rtol = k.res_rtol;
+  S->res_max_it = k.res_max_it;
   b->slots[slot] = S;
+  if (S->consts.resistive) ++b->n_res;
   if ((rc = publish(b))) return rc;
   CUDA_TRY(cudaStreamSynchronize(st));
   *slot_out = slot;
@@ -729,6 +843,8 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   int rc = slot_check(b, src_slot);
   if (rc) return rc;
   if (!slot_out) return fail(MHD_ERR_ARG, "mhd_batch_add_like: null slot");
+  if (constants && constants->resistive && b->precision != kFP64)
+    return fail(MHD_ERR_ARG, "the implicit resistive substep is available in FP64 only");
   int slot = -1;
   for (int s = 0; s < b->capacity; ++s)
     if (!b->slots[s]) {
@@ -760,7 +876,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
                        k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
                        k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
                        k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
-                       k.ambipolar,     k.local_arti, S->nghost};
+                       k.ambipolar,     k.local_arti, S->nghost, k.resistive};
   }
   auto bail = [&](int code) {
     free_solve(S, st);
@@ -793,7 +909,10 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   SolveState s0{};
   s0.dt_bits = kDtUnset;
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
+  S->res_rtol = constants ? constants->res_rtol : src->res_rtol;
+  S->res_max_it = constants ? constants->res_max_it : src->res_max_it;
   b->slots[slot] = S;
+  if (S->consts.resistive) ++b->n_res;
   if ((rc = publish(b))) return rc;
   *slot_out = slot;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
@@ -804,6 +923,7 @@ int mhd_batch_remove(mhd_batch *b, int slot) {
   if (rc) return rc;
   Solve *S = b->slots[slot];
   b->slots[slot] = nullptr;
+  if (S->consts.resistive) --b->n_res;
   SolveState s0{};
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return rc;
   if ((rc = publish(b))) return rc;
@@ -888,8 +1008,14 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   s0.step = step;
   // reset everything before the buffer index (dt, time, step, remaining, status); keep cur
   if ((rc = set_state_field(b, slot, 0, &s0, offsetof(SolveState, cur)))) return rc;
+  const bool res = b->slots[slot]->consts.resistive != 0;
   rc = targeted(b, slot, [&](int *nk) {
     launch(b, 1, SK_FACE_NORMALS, nk);
+    if (res) {  // unknowns of the implicit resistive substep: W = 1 / (eta alpha) on them
+      launch(b, 1, SK_RES_SEED, nk);
+      sync1(b, 1, copy_op(MHD_SYNC_EEDGE, 1), nk);
+      launch(b, 1, SK_RES_W, nk);
+    }
     enqueue_derived(b, 1, nk);
   });
   if (rc) return rc;
@@ -923,9 +1049,25 @@ int mhd_batch_request(mhd_batch *b, int slot, int64_t nsteps) {
 
 int mhd_batch_run(mhd_batch *b, int nsteps) {
   if (!b || nsteps < 0) return fail(MHD_ERR_ARG, "mhd_batch_run: bad arguments");
-  int rc = build_graph(b);
-  if (rc) return rc;
-  for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+  int rc;
+  if (b->n_res == 0) {
+    if ((rc = build_graph(b))) return rc;
+    for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+    return MHD_OK;
+  }
+  // with implicit resistive solves: part A, each such solve's substep (host-driven CG), part B
+  if ((rc = capture(b, &b->graph_a, nullptr, [&](int *nk) { enqueue_step_a(b, nk); }))) return rc;
+  if ((rc = capture(b, &b->graph_b, nullptr, [&](int *nk) { enqueue_step_b(b, nk, true); }))) return rc;
+  for (int s = 0; s < nsteps; ++s) {
+    CUDA_TRY(cudaGraphLaunch(b->graph_a, b->stream));
+    if ((rc = read_state(b))) return rc;
+    for (int q = 0; q < b->capacity; ++q) {
+      const Solve *S = b->slots[q];
+      if (S && S->consts.resistive && b->hstate[q].remaining > 0 && b->hstate[q].status == 0)
+        if ((rc = res_solve(b, q))) return rc;
+    }
+    CUDA_TRY(cudaGraphLaunch(b->graph_b, b->stream));
+  }
   return MHD_OK;
 }
 

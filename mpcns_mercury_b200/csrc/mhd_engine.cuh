@@ -22,7 +22,8 @@ enum RangeKind : int {
   kExt = 2,      // [-1, n + 2): face EMF candidates incl. one ghost layer
   kAlloc = 3,    // [-gs, n + gs), gs = min(nghost, kStepGhost): the ghost cells the step maintains
   kCells2 = 4,   // owned cells, two work items per tile (one per ion species)
-  kNumRanges = 5
+  kFull = 5,     // [-(g + 1), n + g + 2): the whole box
+  kNumRanges = 6
 };
 
 constexpr int kTileK = 32, kTileJ = 4, kTileI = 2, kTileThreads = kTileK * kTileJ * kTileI;
@@ -69,6 +70,7 @@ struct ConstsT {
   int ambipolar;
   int local_arti;
   int nghost;
+  int resistive;
 };
 using Consts = ConstsT<double>;
 inline ConstsT<float> to_float(const Consts &c) {
@@ -78,7 +80,7 @@ inline ConstsT<float> to_float(const Consts &c) {
                         (float)c.state_coeff_Na, (float)c.CFL, (float)c.hall_coef, (float)c.momentum_induce_coeff,
                         (float)c.momentum_hall_coeff, (float)c.inver_MA2, (float)c.ne_hall_floor,
                         (float)c.arti_eta_max, (float)c.arti_J_start, (float)c.arti_J_on, c.ambipolar,
-                        c.local_arti, c.nghost};
+                        c.local_arti, c.nghost, c.resistive};
 }
 
 // Per-solve device state.
@@ -172,6 +174,7 @@ __host__ __device__ inline RangeBox range_of(int kind, const int n[3], int g) {
       case kCells2: r.lo[a] = 0; r.hi[a] = n[a]; break;
       case kBox: r.lo[a] = 0; r.hi[a] = n[a] + 1; break;
       case kExt: r.lo[a] = -1; r.hi[a] = n[a] + 2; break;
+      case kFull: r.lo[a] = -(g + 1); r.hi[a] = n[a] + g + 2; break;
       default: {
         const int gs = g < kStepGhost ? g : kStepGhost;
         r.lo[a] = -gs;

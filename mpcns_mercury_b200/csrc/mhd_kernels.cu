@@ -36,6 +36,9 @@ constexpr int cHX = kComp.first[MHD_EHALL_XI], cHY = kComp.first[MHD_EHALL_ETA],
 constexpr int cEFX = kComp.first[MHD_EFACE_XI], cEFY = kComp.first[MHD_EFACE_ETA], cEFZ = kComp.first[MHD_EFACE_ZETA];
 constexpr int cEHC = kComp.first[MHD_EHC], cHB = kComp.first[MHD_HALL_BETA], cUC = kComp.first[MHD_UCON];
 constexpr int cDIVB = kComp.first[MHD_DIVB];
+constexpr int cETAR = kComp.first[MHD_ETA_RES_XI];  // ETA_RES_ETA, ETA_RES_ZETA follow
+constexpr int cRW = kComp.first[MHD_RES_W], cRX = kComp.first[MHD_RES_X], cRR = kComp.first[MHD_RES_R],
+              cRP = kComp.first[MHD_RES_P], cRQ = kComp.first[MHD_RES_Q], cRBS = kComp.first[MHD_RES_BSTAR];
 constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA], cFNZ = kComp.first[MHD_FNORM_ZETA];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
@@ -910,6 +913,226 @@ __global__ void __launch_bounds__(kTileThreads) k_div_b(Dir D) {
   });
 }
 
+// ------------------------------------------------------------------ implicit resistive substep
+// SolveImplicitResistiveDiffusion_ (Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:475-575):
+// (I + dt eta alpha C^T beta C) E = eta J(B*) on the owned edges with eta > 0.
+// The operator is self-adjoint in the inner product weighted by
+// W = 1 / (eta alpha), so CG runs in that inner product; the edge, face and J
+// fields of the explicit step are the operator's scratch (E: E_res, B: dB,
+// J: dJ), with the step's own E / B / J sync and alias tables.
+
+// Owned-range test of an edge of family a at (i, j, k).
+__device__ __forceinline__ bool edge_owned(int a, int i, int j, int k, int n0, int n1, int n2) {
+  return a == 0 ? (i < n0 && j <= n1 && k <= n2) : a == 1 ? (i <= n0 && j < n1 && k <= n2) : (i <= n0 && j <= n1 && k < n2);
+}
+
+// E = the element offset of each edge (owned range and alias layer): after
+// the owner copies, an edge still holding its own offset is not a
+// non-owner alias (its own unknown).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_seed(Dir D) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int64_t o = B.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) B.c(cEX + a)[o] = R((double)o);
+  });
+}
+
+// W = 1 / (eta alpha) on the unknowns (owned, not a non-owner alias, eta > 0,
+// alpha > 0: BuildImplicitResistiveEdgeDofMap_, Mercury_ImplicitResistive.cpp:168-226), 0 elsewhere.
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_w(Dir D) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int64_t o = B.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) {
+      R w = R(0.0);
+      if (edge_owned(a, it.i, it.j, it.k, B.n0, B.n1, B.n2) && B.c(cEX + a)[o] == R((double)o)) {
+        const R eta = B.c(cETAR + a)[o], alpha = B.c(cALX + a)[o];
+        if (eta > R(0.0) && alpha > R(0.0)) w = R(1.0) / (eta * alpha);
+      }
+      B.c(cRW + a)[o] = w;
+    }
+  });
+}
+
+// Vector operations of the CG on the unknowns (W > 0); other entries stay 0.
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op, double s) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int64_t o = B.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) {
+      const bool dof = B.c(cRW + a)[o] > R(0.0);
+      R *x = B.c(cRX + a) + o, *r = B.c(cRR + a) + o, *p = B.c(cRP + a) + o;
+      switch (op) {
+        case RES_INIT: {  // b = eta J (PackImplicitJedgeToVec_, :395-418); x = 0, r = p = b
+          const R bv = dof ? R(0.0) + B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
+          *x = R(0.0);
+          *r = bv;
+          *p = bv;
+          break;
+        }
+        case RES_E_FROM_P: B.c(cEX + a)[o] = dof ? *p : R(0.0); break;  // UnpackVecToImplicitEres_ (:294-312)
+        case RES_E_FROM_X: B.c(cEX + a)[o] = dof ? *x : R(0.0); break;
+        case RES_AXPY:
+          if (dof) {
+            *x += R(s) * *p;
+            *r -= R(s) * B.c(cRQ + a)[o];
+          }
+          break;
+        default:  // RES_PUPD
+          if (dof) *p = *r + R(s) * *p;
+          break;
+      }
+    }
+  });
+}
+
+// dB = -dt curl E on the owned faces (CurlEdgeToFace with multiplier -dt,
+// Z4_Mercury/src/operators/CTOperators.cpp:6-56; MatMultImplicitResistive_, :420-445).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_db(Dir D) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const R m = R(-D.state[it.s].dt);
+    const int i = it.i, j = it.j, k = it.k;
+    if (j < B.n1 && k < B.n2)
+      AT(cBX, i, j, k) = m * ((AT(cEY, i, j, k) - AT(cEY, i, j, k + 1)) + (AT(cEZ, i, j + 1, k) - AT(cEZ, i, j, k)));
+    if (i < B.n0 && k < B.n2)
+      AT(cBY, i, j, k) = m * ((AT(cEX, i, j, k + 1) - AT(cEX, i, j, k)) + (AT(cEZ, i, j, k) - AT(cEZ, i + 1, j, k)));
+    if (i < B.n0 && j < B.n1)
+      AT(cBZ, i, j, k) = m * ((AT(cEX, i, j, k) - AT(cEX, i, j + 1, k)) + (AT(cEY, i + 1, j, k) - AT(cEY, i, j, k)));
+  });
+}
+
+// dJ = alpha CurlAdjFaceToEdge(beta dB) on the owned edges (CalcImplicitDeltaJedgeFromDeltaB_,
+// Mercury_ImplicitResistive.cpp:314-393; CTOperators.cpp:59-110).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_dj(Dir D) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int i = it.i, j = it.j, k = it.k;
+    if (i < B.n0) {
+      const R v = ((AT(cBFY, i, j, k - 1) * AT(cBY, i, j, k - 1) - AT(cBFY, i, j, k) * AT(cBY, i, j, k)) +
+                   (AT(cBFZ, i, j, k) * AT(cBZ, i, j, k) - AT(cBFZ, i, j - 1, k) * AT(cBZ, i, j - 1, k))) * R(1.0);
+      AT(cJX, i, j, k) = v * AT(cALX, i, j, k);
+    }
+    if (j < B.n1) {
+      const R v = ((AT(cBFX, i, j, k) * AT(cBX, i, j, k) - AT(cBFX, i, j, k - 1) * AT(cBX, i, j, k - 1)) +
+                   (AT(cBFZ, i - 1, j, k) * AT(cBZ, i - 1, j, k) - AT(cBFZ, i, j, k) * AT(cBZ, i, j, k))) * R(1.0);
+      AT(cJY, i, j, k) = v * AT(cALY, i, j, k);
+    }
+    if (k < B.n2) {
+      const R v = ((AT(cBFX, i, j - 1, k) * AT(cBX, i, j - 1, k) - AT(cBFX, i, j, k) * AT(cBX, i, j, k)) +
+                   (AT(cBFY, i, j, k) * AT(cBY, i, j, k) - AT(cBFY, i - 1, j, k) * AT(cBY, i - 1, j, k))) * R(1.0);
+      AT(cJZ, i, j, k) = v * AT(cALZ, i, j, k);
+    }
+  });
+}
+
+// q = A p = E_res - eta dJ on the unknowns (MatMultImplicitResistive_, :446-468).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_q(Dir D) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int64_t o = B.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) {
+      const bool dof = B.c(cRW + a)[o] > R(0.0);
+      B.c(cRQ + a)[o] = dof ? B.c(cEX + a)[o] - B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
+    }
+  });
+}
+
+// Dot products on the unknowns: op RES_DOT_PQ: (sum W p q, 0); RES_DOT_RR:
+// (sum W r r, sum r r).  Per-CTA partial sums in a fixed order (deterministic).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_dot(Dir D, int op, double *partial) {
+  __shared__ double sh[2][kTileThreads / 32];
+  double acc0 = 0.0, acc1 = 0.0;
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int64_t o = B.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) {
+      const double w = (double)B.c(cRW + a)[o];
+      if (!(w > 0.0)) continue;
+      if (op == RES_DOT_PQ) {
+        acc0 += w * (double)B.c(cRP + a)[o] * (double)B.c(cRQ + a)[o];
+      } else {
+        const double r = (double)B.c(cRR + a)[o];
+        acc0 += w * r * r;
+        acc1 += r * r;
+      }
+    }
+  });
+  for (int of = 16; of > 0; of >>= 1) {
+    acc0 += __shfl_xor_sync(0xffffffffu, acc0, of);
+    acc1 += __shfl_xor_sync(0xffffffffu, acc1, of);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = acc0;
+    sh[1][threadIdx.x >> 5] = acc1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < kTileThreads / 32; ++w) {
+      s0 += sh[0][w];
+      s1 += sh[1][w];
+    }
+    partial[2 * blockIdx.x] = s0;
+    partial[2 * blockIdx.x + 1] = s1;
+  }
+}
+__global__ void k_res_sum(const double *partial, int n, double *result) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int q = 0; q < n; ++q) {
+      s0 += partial[2 * q];
+      s1 += partial[2 * q + 1];
+    }
+    result[0] = s0;
+    result[1] = s1;
+  }
+}
+
+// B* snapshot / restore over the whole box (SnapshotImplicitResistiveBstar_,
+// RestoreImplicitResistiveBstar_, :260-292).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_copyb(Dir D, int op) {
+  for_items<R, kFull>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int64_t o = B.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) {
+      if (op == RES_SNAPSHOT) B.c(cRBS + a)[o] = B.c(cBX + a)[o];
+      else B.c(cBX + a)[o] = B.c(cRBS + a)[o];
+    }
+  });
+}
+
+// B += dt (-curl E_res) on the owned faces (ApplyImplicitResistiveUpdate_, :557-575;
+// ApplyUpdate_Euler_BfaceOnly_, Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:435-473).
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_bupdate(Dir D) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const R dt = R(D.state[it.s].dt);
+    const int i = it.i, j = it.j, k = it.k;
+    if (j < B.n1 && k < B.n2) {
+      const R rb = R(-1.0) * ((AT(cEY, i, j, k) - AT(cEY, i, j, k + 1)) + (AT(cEZ, i, j + 1, k) - AT(cEZ, i, j, k)));
+      AT(cBX, i, j, k) += dt * rb;
+    }
+    if (i < B.n0 && k < B.n2) {
+      const R rb = R(-1.0) * ((AT(cEX, i, j, k + 1) - AT(cEX, i, j, k)) + (AT(cEZ, i, j, k) - AT(cEZ, i + 1, j, k)));
+      AT(cBY, i, j, k) += dt * rb;
+    }
+    if (i < B.n0 && j < B.n1) {
+      const R rb = R(-1.0) * ((AT(cEX, i, j, k) - AT(cEX, i, j + 1, k)) + (AT(cEY, i + 1, j, k) - AT(cEY, i, j, k)));
+      AT(cBZ, i, j, k) += dt * rb;
+    }
+  });
+}
+
 // Static per-face terms of the CFL time step and the Rusanov wave speed, once
 // per solve (run by mhd_prepare): |a| = sqrt(ax ax + ay ay + az az) and
 // a / |a| of the face area vectors JD, the operations and order
@@ -1107,7 +1330,8 @@ static void grids() {
 }
 
 template <class R>
-static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops) {
+static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
+                      ResScratch rs) {
   switch (k) {
     case SK_FACE_EMF: k_face_emf<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
     case SK_EDGE_EMF: k_edge_emf<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
@@ -1122,24 +1346,42 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_SYNC: k_sync<R><<<g_grid_copy, 256, 0, st>>>(D, *ops); break;
     case SK_FACE_NORMALS: k_face_normals<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
     case SK_DIVB: k_div_b<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_SEED: k_res_seed<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_W: k_res_w<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_VEC: k_res_vec<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, darg); break;
+    case SK_RES_DB: k_res_db<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_DJ: k_res_dj<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_Q: k_res_q<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_DOT: k_res_dot<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.partial); break;
+    case SK_RES_SUM: k_res_sum<<<1, 32, 0, st>>>(rs.partial, g_grid_tiles, rs.result); break;
+    case SK_RES_COPYB: k_res_copyb<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg); break;
+    case SK_RES_BUPDATE: k_res_bupdate<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
     default: break;
   }
 }
 
-void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision) {
+void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision, int iarg,
+                        double darg, ResScratch rs) {
   grids();
   if (precision == kMixed)
-    launch_as<float>(k, D, st, ops);
+    launch_as<float>(k, D, st, ops, iarg, darg, rs);
   else
-    launch_as<double>(k, D, st, ops);
+    launch_as<double>(k, D, st, ops, iarg, darg, rs);
+}
+
+int res_dot_grid() {
+  grids();
+  return g_grid_tiles;
 }
 
 const char *step_kernel_name(StepKernel k) {
   static const char *names[] = {"k_face_emf", "k_edge_emf", "k_hall_cell", "k_hall_edge", "k_add_hall",
                                 "k_fluid",    "k_bface",    "k_bcell_jedge", "k_jcell",   "k_pv_uplus",
-                                "k_sync",     "k_flip",     "k_retire",      "k_face_normals", "k_div_b"};
+                                "k_sync",     "k_flip",     "k_retire",      "k_face_normals", "k_div_b",
+                                "k_res_seed", "k_res_w",    "k_res_vec",     "k_res_db",   "k_res_dj",
+                                "k_res_q",    "k_res_dot",  "k_res_sum",     "k_res_copyb", "k_res_bupdate"};
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }
 

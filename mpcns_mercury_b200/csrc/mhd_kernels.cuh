@@ -8,7 +8,10 @@ namespace mhd {
 
 enum StepKernel {
   SK_FACE_EMF = 0, SK_EDGE_EMF, SK_HALL_CELL, SK_HALL_EDGE, SK_ADD_HALL, SK_FLUID, SK_BFACE, SK_BCELL_JEDGE,
-  SK_JCELL, SK_PV_UPLUS, SK_SYNC, SK_FLIP, SK_RETIRE, SK_FACE_NORMALS, SK_DIVB, SK_COUNT
+  SK_JCELL, SK_PV_UPLUS, SK_SYNC, SK_FLIP, SK_RETIRE, SK_FACE_NORMALS, SK_DIVB,
+  // implicit resistive substep
+  SK_RES_SEED, SK_RES_W, SK_RES_VEC, SK_RES_DB, SK_RES_DJ, SK_RES_Q, SK_RES_DOT, SK_RES_SUM, SK_RES_COPYB,
+  SK_RES_BUPDATE, SK_COUNT
 };
 
 // One launch of k_sync runs up to two independent sync operations: a copy
@@ -24,9 +27,23 @@ struct SyncOps {
   int n;
 };
 
+// Operations of SK_RES_VEC / SK_RES_DOT / SK_RES_COPYB (the arg of the launch).
+enum ResVecOp { RES_INIT = 0, RES_E_FROM_P, RES_E_FROM_X, RES_AXPY, RES_PUPD };
+enum ResDotOp { RES_DOT_PQ = 0, RES_DOT_RR };
+enum ResCopyOp { RES_SNAPSHOT = 0, RES_RESTORE };
+
+// Scratch of the CG dot products: per-CTA partial sums and the two results.
+struct ResScratch {
+  double *partial;  // 2 * grid
+  double *result;   // 2
+};
+
 // Launch one engine kernel over the directory D (ops: SK_SYNC only) in the
-// batch's precision (Precision).
-void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision);
+// batch's precision (Precision); iarg / darg: the operation and scalar of the
+// implicit resistive kernels.
+void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision, int iarg = 0,
+                        double darg = 0.0, ResScratch rs = ResScratch{nullptr, nullptr});
+int res_dot_grid();
 const char *step_kernel_name(StepKernel k);
 
 }  // namespace mhd

@@ -682,6 +682,31 @@ void dump_local_eta(MercurySolver &S, Dumper &d) {
     }
 }
 
+// Implicit-resistivity coefficient per edge as the reference evaluates it for
+// its unknowns (ImplicitResistiveEtaAtEdge_,
+// Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:228-258) on every edge of the owned
+// range, zero elsewhere.
+void dump_eta_res(MercurySolver &S, Dumper &d) {
+  Field *fld = S.fld_;
+  const int fids[3] = {S.fid_.fid_Eres.xi, S.fid_.fid_Eres.eta, S.fid_.fid_Eres.zeta};
+  const TOPO::EntityAxis axes[3] = {TOPO::EntityAxis::Xi, TOPO::EntityAxis::Eta, TOPO::EntityAxis::Zeta};
+  const char *names[3] = {"eta_res_xi", "eta_res_eta", "eta_res_zeta"};
+  for (int a = 0; a < 3; ++a)
+    for (int ib = 0; ib < fld->num_blocks(); ++ib) {
+      FieldBlock &E = fld->field(fids[a], ib);
+      const Int3 lo = E.get_lo(), hi = E.get_hi(), ilo = E.inner_lo(), ihi = E.inner_hi();
+      const int ni = hi.i - lo.i, nj = hi.j - lo.j, nk = hi.k - lo.k;
+      std::vector<double> t((size_t)ni * nj * nk, 0.0);
+      for (int i = ilo.i; i < ihi.i; ++i)
+        for (int j = ilo.j; j < ihi.j; ++j)
+          for (int k = ilo.k; k < ihi.k; ++k)
+            t[((size_t)(i - lo.i) * nj + (j - lo.j)) * nk + (k - lo.k)] =
+                S.ImplicitResistiveEtaAtEdge_(TOPO::make_edge(0, ib, i, j, k, axes[a]));
+      const int l[3] = {lo.i, lo.j, lo.k}, h[3] = {hi.i, hi.j, hi.k};
+      d.rec(std::string("static:") + names[a], ib, l, h, 1, t.data());
+    }
+}
+
 // Edge alias classes exactly as ReduceEdgeAliasCandidatesToOwners_ consumes
 // them (Z4_Mercury/src/physics/MercurySolver_Current.cpp:8-35): classes with a
 // global id and more than one member, sorted by global id; per class the owner
@@ -785,6 +810,7 @@ int main(int argc, char **argv) {
       if (job_int("dump_grid", 0)) dump_grid(d, grd);
       if (job_int("dump_taper", 0)) dump_taper(S, d);
       if (job_int("local_arti", 0)) dump_local_eta(S, d);
+      if (job_int("resistive", 0)) dump_eta_res(S, d);
       const auto state_fields = split_ws(job_str("dump_fields", "U_H U_Na B_xi B_eta B_zeta"));
       const long steps = job_int("steps", 1);
       std::vector<long> at;

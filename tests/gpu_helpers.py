@@ -18,7 +18,8 @@ def context_from_dump(dump, n, tag="step0:", cfl=0.4, precision=0, constants=Non
     for name in mo.STATIC_FIELDS + ["taper_xi", "taper_eta", "taper_zeta"]:
         r = dump[("static:" + name, 0)]
         ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
-    for name in ("local_arti_eta_xi", "local_arti_eta_eta", "local_arti_eta_zeta"):
+    for name in ("local_arti_eta_xi", "local_arti_eta_eta", "local_arti_eta_zeta", "eta_res_xi", "eta_res_eta",
+                 "eta_res_zeta"):
         if ("static:" + name, 0) in dump:
             r = dump[("static:" + name, 0)]
             ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
