@@ -619,6 +619,8 @@ int xfer(mhd_batch *b, int slot, int field, int block, const int32_t lo[3], cons
     return fail(MHD_ERR_ARG, "transfer: bad arguments");
   if (ncomp != kFieldSpec[field].ncomp)
     return fail(MHD_ERR_ARG, "field %d has %d components, got %d", field, kFieldSpec[field].ncomp, ncomp);
+  if (kComp.first[field] >= kFirstResComp && !S->consts.resistive)
+    return fail(MHD_ERR_ARG, "field %d exists only in solves with the implicit resistive substep", field);
   const Box &bx = S->boxes[block];
   for (int a = 0; a < 3; ++a)
     if (lo[a] < -bx.G || hi[a] > bx.n[a] + 1 + bx.G || hi[a] <= lo[a])
@@ -726,7 +728,8 @@ int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
     if (n[0] < 2 || n[1] < 2 || n[2] < 2) return -1;
     const Box bx = make_box(n, desc->nghost);
     const int64_t es = desc->precision == kMixed ? 4 : 8;
-    bytes += ((int64_t)kNumMetric * 8 + (int64_t)(kNumRComps + 2 * kNumUComps) * es) * bx.total;
+    const int64_t nr = kNumRComps - (desc->constants.resistive ? 0 : kNumResComps);
+    bytes += ((int64_t)kNumMetric * 8 + (nr + 2 * kNumUComps) * es) * bx.total;
   }
   for (int g = 0; g < MHD_NUM_GROUPS; ++g)
     bytes += (int64_t)(desc->groups[g].n_halo + desc->groups[g].n_owner) * 24;
@@ -779,7 +782,8 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
     S->ubase.push_back(u);
     S->mbase.push_back(m);
     u += (int64_t)kNumUComps * bx.total * S->es;
-    m += ((int64_t)kNumMetric * 8 + (int64_t)kNumRComps * S->es) * bx.total;
+    m += ((int64_t)kNumMetric * 8 + (int64_t)(kNumRComps - (desc->constants.resistive ? 0 : kNumResComps)) * S->es) *
+         bx.total;
     for (int r = 0; r < kNumRanges; ++r)
       prefix[r].push_back(prefix[r].back() + tiles_of(range_of(r, n, desc->nghost), r));
   }
@@ -845,6 +849,8 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   if (!slot_out) return fail(MHD_ERR_ARG, "mhd_batch_add_like: null slot");
   if (constants && constants->resistive && b->precision != kFP64)
     return fail(MHD_ERR_ARG, "the implicit resistive substep is available in FP64 only");
+  if (constants && (constants->resistive != 0) != (b->slots[src_slot]->consts.resistive != 0))
+    return fail(MHD_ERR_ARG, "mhd_batch_add_like: the implicit resistive substep must match the template's");
   int slot = -1;
   for (int s = 0; s < b->capacity; ++s)
     if (!b->slots[s]) {

@@ -43,6 +43,11 @@ constexpr int kMetricFirst = kComp.first[MHD_JAC];  // JAC, JDXI, JDET, JDZE are
 constexpr int kNumMetric = kComp.first[MHD_JDZE] + 3 - kMetricFirst;
 constexpr int kNumRComps = kNumComps - kNumUComps - kNumMetric;  // real-valued comps outside U
 static_assert(kNumMetric == 10, "metric components");
+// The work arrays of the implicit resistive substep are the last components;
+// solves without the substep do not allocate them.
+constexpr int kFirstResComp = kComp.first[MHD_RES_W];
+constexpr int kNumResComps = kNumComps - kFirstResComp;
+static_assert(MHD_RES_BSTAR == MHD_NUM_FIELDS - 1, "resistive work fields last");
 __host__ __device__ constexpr bool is_metric(int comp) { return comp >= kMetricFirst && comp < kMetricFirst + kNumMetric; }
 // Index of a non-U, non-metric component among the real-valued M arrays.
 __host__ __device__ constexpr int rslot(int comp) {
