@@ -777,7 +777,10 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
     const int n[3] = {desc->cells[3 * bi], desc->cells[3 * bi + 1], desc->cells[3 * bi + 2]};
     if (n[0] < 2 || n[1] < 2 || n[2] < 2) return bail(fail(MHD_ERR_ARG, "block %d: cells %d %d %d", bi, n[0], n[1], n[2]));
     Box bx = make_box(n, desc->nghost);
-    if (bx.total >= (int64_t(1) << 40)) return bail(fail(MHD_ERR_ARG, "block %d too large", bi));
+    // kernels address a block's arrays with 32-bit element offsets
+    if ((int64_t)(kNumComps + kNumUComps) * bx.total >= (int64_t(1) << 31))
+      return bail(fail(MHD_ERR_ARG, "block %d too large (%lld cells with ghosts); split it into smaller blocks", bi,
+                       (long long)bx.total));
     S->boxes.push_back(bx);
     S->ubase.push_back(u);
     S->mbase.push_back(m);

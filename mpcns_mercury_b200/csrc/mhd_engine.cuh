@@ -102,16 +102,16 @@ struct SolveState {
 };
 
 // Sync tables of one solve address DOFs by "codes": the byte offset from the
-// solve's arena base (bits 0..55); bit 60 marks a U component, whose offset
+// solve's arena base (bits 0..54); bit 60 marks a U component, whose offset
 // is taken in U buffer 0 and shifted by cur * ubuf bytes at run time.  All
 // synced components are real-valued.
-constexpr int64_t kCodeOffMask = (int64_t(1) << 56) - 1;
+constexpr int64_t kCodeOffMask = (int64_t(1) << 55) - 1;
 constexpr int64_t kCodeUFlag = int64_t(1) << 60;
-// Copy segments: `len` (1..8) consecutive destinations dst.. <- sign * src..
+// Copy segments: `len` (1..32) consecutive destinations dst.. <- sign * src..
 // (consecutive sources), stored as two int64: dst code with (len - 1) in bits
-// 56..58 and a negative sign in bit 59, and the src code.
-constexpr int kSegMax = 8;
-constexpr int kSegLenShift = 56, kSegNegBit = 59;
+// 55..59 and a negative sign in bit 61, and the src code.
+constexpr int kSegMax = 32;
+constexpr int kSegLenShift = 55, kSegNegBit = 61;
 struct DevTable {
   const int64_t *seg = nullptr;  // 2 * n
   int n = 0;                     // segments

@@ -63,22 +63,21 @@ __device__ __forceinline__ R dmin(R a, R b) { return (b < a) ? b : a; }
 
 // One block's fields for the current step: U = current buffer, M = metric
 // (double) then the other real-valued components (mhd_engine.cuh).
+// Element offsets inside a block are 32-bit (mhd_batch_add keeps every
+// block's component arrays below 2^31 elements in total).
 template <class R>
 struct V {
   R *U, *Un;
   char *M;
-  int64_t total, si, sj;
+  int total, si, sj;
   int G, n0, n1, n2;
   // real-valued component (U or M)
   __device__ __forceinline__ R *c(int comp) const {
-    return comp < kNumUComps ? U + (int64_t)comp * total
-                             : (R *)(M + (int64_t)kNumMetric * total * 8) + (int64_t)rslot(comp) * total;
+    return comp < kNumUComps ? U + comp * total : (R *)(M + (int64_t)kNumMetric * total * 8) + rslot(comp) * total;
   }
   // metric component (JAC, JD*), double in every precision
-  __device__ __forceinline__ double *m(int comp) const { return (double *)M + (int64_t)(comp - kMetricFirst) * total; }
-  __device__ __forceinline__ int64_t off(int i, int j, int k) const {
-    return (int64_t)(i + G) * si + (int64_t)(j + G) * sj + (k + G);
-  }
+  __device__ __forceinline__ double *m(int comp) const { return (double *)M + (comp - kMetricFirst) * total; }
+  __device__ __forceinline__ int off(int i, int j, int k) const { return (i + G) * si + (j + G) * sj + (k + G); }
 };
 #define AT(cc, i, j, k) (B.c(cc)[B.off((i), (j), (k))])
 #define ATM(cc, i, j, k) (B.m(cc)[B.off((i), (j), (k))])
@@ -155,9 +154,9 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
     B.U = (R *)DB.U[cur];
     B.Un = (R *)DB.U[cur ^ 1];
     B.M = DB.M;
-    B.total = DB.total;
-    B.si = DB.si;
-    B.sj = DB.sj;
+    B.total = (int)DB.total;
+    B.si = (int)DB.si;
+    B.sj = (int)DB.sj;
     B.G = DB.G;
     B.n0 = DB.n[0];
     B.n1 = DB.n[1];
@@ -267,7 +266,7 @@ __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
         e1 = -Gx;
       }
       const int ce = fa == 0 ? cEFX : fa == 1 ? cEFY : cEFZ;
-      const int64_t o = B.off(i, j, k);
+      const int o = B.off(i, j, k);
       B.c(ce)[o] = e0;
       B.c(ce + 1)[o] = e1;
       B.c(ce + 2)[o] = e2;
@@ -401,7 +400,7 @@ __global__ void __launch_bounds__(kTileThreads) k_hall_cell(Dir D) {
   for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
-    const int64_t o = B.off(i, j, k);
+    const int o = B.off(i, j, k);
     const Num<R> d = num_limiter(consts_of<R>(S), B.c(cUH)[o], B.c(cUN)[o]);
     const R alpha = consts_of<R>(S).hall_coef / d.ne_eff;
     const R Jx = B.c(cJC)[o], Jy = B.c(cJC + 1)[o], Jz = B.c(cJC + 2)[o];
@@ -485,7 +484,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_add_hall(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const int64_t o = B.off(it.i, it.j, it.k);
+    const int o = B.off(it.i, it.j, it.k);
     if (it.i < B.n0) B.c(cEX)[o] += B.c(cHX)[o];
     if (it.j < B.n1) B.c(cEY)[o] += B.c(cHY)[o];
     if (it.k < B.n2) B.c(cEZ)[o] += B.c(cHZ)[o];
@@ -691,9 +690,9 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
     r[4] -= a4 * rho * u2 * vst;
     r[4] += a5 * nS * b1;
     r[4] += a4 * rho * u2 * b2;
-    const int64_t o = B.off(i, j, k);
+    const int o = B.off(i, j, k);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) B.Un[(int64_t)(u0 + m) * B.total + o] = CV(12 + m) + dt * r[m];
+    for (int m = 0; m < 5; ++m) B.Un[(u0 + m) * B.total + o] = CV(12 + m) + dt * r[m];
   });
 }
 
@@ -746,7 +745,7 @@ __global__ void __launch_bounds__(kTileThreads) k_bcell_jedge(Dir D) {
         byi += wy * pi_[q];
         bzi += wz * pi_[q];
       }
-      const int64_t o = B.off(i, j, k);
+      const int o = B.off(i, j, k);
       B.c(cBC)[o] = bxt;
       B.c(cBC + 1)[o] = byt;
       B.c(cBC + 2)[o] = bzt;
@@ -789,7 +788,7 @@ __global__ void __launch_bounds__(kTileThreads) k_jcell(Dir D) {
       jy += AT(cWJ + 12 + q, i, j, k) * s[q];
       jz += AT(cWJ + 24 + q, i, j, k) * s[q];
     }
-    const int64_t o = B.off(i, j, k);
+    const int o = B.off(i, j, k);
     B.c(cJC)[o] = jx;
     B.c(cJC + 1)[o] = jy;
     B.c(cJC + 2)[o] = jz;
@@ -933,7 +932,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_seed(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const int64_t o = B.off(it.i, it.j, it.k);
+    const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) B.c(cEX + a)[o] = R((double)o);
   });
 }
@@ -944,7 +943,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_w(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const int64_t o = B.off(it.i, it.j, it.k);
+    const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       R w = R(0.0);
       if (edge_owned(a, it.i, it.j, it.k, B.n0, B.n1, B.n2) && B.c(cEX + a)[o] == R((double)o)) {
@@ -961,7 +960,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op, double s) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const int64_t o = B.off(it.i, it.j, it.k);
+    const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       const bool dof = B.c(cRW + a)[o] > R(0.0);
       R *x = B.c(cRX + a) + o, *r = B.c(cRR + a) + o, *p = B.c(cRP + a) + o;
@@ -1036,7 +1035,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_q(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const int64_t o = B.off(it.i, it.j, it.k);
+    const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       const bool dof = B.c(cRW + a)[o] > R(0.0);
       B.c(cRQ + a)[o] = dof ? B.c(cEX + a)[o] - B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
@@ -1052,7 +1051,7 @@ __global__ void __launch_bounds__(kTileThreads) k_res_dot(Dir D, int op, double 
   double acc0 = 0.0, acc1 = 0.0;
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const int64_t o = B.off(it.i, it.j, it.k);
+    const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       const double w = (double)B.c(cRW + a)[o];
       if (!(w > 0.0)) continue;
@@ -1102,7 +1101,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_copyb(Dir D, int op) {
   for_items<R, kFull>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
-    const int64_t o = B.off(it.i, it.j, it.k);
+    const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       if (op == RES_SNAPSHOT) B.c(cRBS + a)[o] = B.c(cBX + a)[o];
       else B.c(cBX + a)[o] = B.c(cRBS + a)[o];
@@ -1146,7 +1145,7 @@ __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
     for (int a = 0; a < 3; ++a) {
       const int cm = a == 0 ? cJDX : a == 1 ? cJDY : cJDZ;
       const int cn = a == 0 ? cFNX : a == 1 ? cFNY : cFNZ;
-      const int64_t o = B.off(it.i, it.j, it.k);
+      const int o = B.off(it.i, it.j, it.k);
       const double ax = B.m(cm)[o], ay = B.m(cm + 1)[o], az = B.m(cm + 2)[o];
       const double An = sqrt(ax * ax + ay * ay + az * az);
       B.c(cn)[o] = R(ax / An);
@@ -1181,7 +1180,7 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
         R pr = (c.gamma - R(1.0)) * eint;
         pr = dmax(pr, R(1e-12));
         const R T = pr / (rho * coeff);
-        const int64_t o = B.off(i, j, k);
+        const int o = B.off(i, j, k);
         B.c(pv0)[o] = u;
         B.c(pv0 + 1)[o] = v;
         B.c(pv0 + 2)[o] = w;
@@ -1270,11 +1269,17 @@ __global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
     if (op.kind == SYNC_COPY) {
       const DevTable &T = op.phase == 1 ? S.owner[op.arg] : op.phase == 2 ? S.halo_full[op.arg] : S.halo[op.arg];
       const int64_t dcode = T.seg[2 * q], scode = T.seg[2 * q + 1];
-      const int len = (int)((dcode >> kSegLenShift) & 7) + 1;
-      if (lane < len) {
-        const R v = at_code<R>(S, cur, scode)[lane];
-        at_code<R>(S, cur, dcode)[lane] = ((dcode >> kSegNegBit) & 1) ? -v : v;
-      }
+      const int len = (int)((dcode >> kSegLenShift) & 31) + 1;
+      const bool neg = (dcode >> kSegNegBit) & 1;
+      const R *src = at_code<R>(S, cur, scode);
+      R *dst = at_code<R>(S, cur, dcode);
+      R v[kSegMax / 8];
+#pragma unroll
+      for (int u = 0; u < kSegMax / 8; ++u)
+        if (lane + 8 * u < len) v[u] = src[lane + 8 * u];
+#pragma unroll
+      for (int u = 0; u < kSegMax / 8; ++u)
+        if (lane + 8 * u < len) dst[lane + 8 * u] = neg ? -v[u] : v[u];
     } else {
       const DevAlias &A = op.arg ? S.aliasJ : S.aliasE;
       const int c = q * 8 + lane;
