@@ -1367,13 +1367,28 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
   }
 }
 
+// The FP32 instantiations are compiled in their own translation unit (this
+// file built with MHD_KERNELS_F32 and FP32 fast-math flags: FMA contraction,
+// approximate division and square root); the FP64 one keeps the bit-exact
+// flags.
+#if MHD_KERNELS_F32
+void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
+                            ResScratch rs) {
+  grids();
+  launch_as<float>(k, D, st, ops, iarg, darg, rs);
+}
+#else
+void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
+                            ResScratch rs);
+
 void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision, int iarg,
                         double darg, ResScratch rs) {
-  grids();
-  if (precision == kMixed)
-    launch_as<float>(k, D, st, ops, iarg, darg, rs);
-  else
+  if (precision == kMixed) {
+    launch_step_kernel_f32(k, D, st, ops, iarg, darg, rs);
+  } else {
+    grids();
     launch_as<double>(k, D, st, ops, iarg, darg, rs);
+  }
 }
 
 int res_dot_grid() {
@@ -1389,5 +1404,6 @@ const char *step_kernel_name(StepKernel k) {
                                 "k_res_q",    "k_res_dot",  "k_res_sum",     "k_res_copyb", "k_res_bupdate"};
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }
+#endif  // MHD_KERNELS_F32
 
 }  // namespace mhd
