@@ -190,11 +190,19 @@ __host__ __device__ inline RangeBox range_of(int kind, const int n[3], int g) {
   }
   return r;
 }
+// Work items of a block: kCells2 (the fluid kernel) uses 3-D tiles of
+// 32 k x 4 j x 2 i cells (two per tile, one per species); every other range is
+// cut into runs of kTileThreads consecutive positions of its box (k fastest),
+// so no lane idles at the end of short k rows.
 __host__ __device__ inline int tiles_of(const RangeBox &r, int kind) {
-  const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
-  const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
-  const int ti = (r.hi[0] - r.lo[0] + kTileI - 1) / kTileI;
-  return tk * tj * ti * (kind == kCells2 ? 2 : 1);
+  if (kind == kCells2) {
+    const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
+    const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
+    const int ti = (r.hi[0] - r.lo[0] + kTileI - 1) / kTileI;
+    return tk * tj * ti * 2;
+  }
+  const int64_t vol = (int64_t)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
+  return (int)((vol + kTileThreads - 1) / kTileThreads);
 }
 
 }  // namespace mhd

@@ -131,24 +131,33 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
     Item it;
     it.s = s;
     it.species = 0;
-    if (KIND == kCells2) {
-      it.species = t & 1;
-      t >>= 1;
-    }
-    const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
-    const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
-    const int bk = t % tk, bj = (t / tk) % tj, bi = t / (tk * tj);
-    it.o[0] = r.lo[0] + bi * kTileI;
-    it.o[1] = r.lo[1] + bj * kTileJ;
-    it.o[2] = r.lo[2] + bk * kTileK;
     for (int a = 0; a < 3; ++a) {
       it.hi[a] = r.hi[a];
       it.lo[a] = r.lo[a];
     }
-    it.k = it.o[2] + (tid % kTileK);
-    it.j = it.o[1] + ((tid / kTileK) % kTileJ);
-    it.i = it.o[0] + (tid / (kTileK * kTileJ));
-    it.in = it.i < r.hi[0] && it.j < r.hi[1] && it.k < r.hi[2];
+    if (KIND == kCells2) {  // 32 k x 4 j x 2 i tile, one species
+      it.species = t & 1;
+      t >>= 1;
+      const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
+      const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
+      const int bk = t % tk, bj = (t / tk) % tj, bi = t / (tk * tj);
+      it.o[0] = r.lo[0] + bi * kTileI;
+      it.o[1] = r.lo[1] + bj * kTileJ;
+      it.o[2] = r.lo[2] + bk * kTileK;
+      it.k = it.o[2] + (tid % kTileK);
+      it.j = it.o[1] + ((tid / kTileK) % kTileJ);
+      it.i = it.o[0] + (tid / (kTileK * kTileJ));
+      it.in = it.i < r.hi[0] && it.j < r.hi[1] && it.k < r.hi[2];
+    } else {  // a run of kTileThreads consecutive positions of the range box (k fastest)
+      const int ek = r.hi[2] - r.lo[2], ej = r.hi[1] - r.lo[1];
+      const int L = t * kTileThreads + tid;
+      const int rest = L / ek;
+      it.k = r.lo[2] + (L - rest * ek);
+      it.j = r.lo[1] + rest % ej;
+      it.i = r.lo[0] + rest / ej;
+      it.in = L < ek * ej * (r.hi[0] - r.lo[0]);
+      it.o[0] = it.o[1] = it.o[2] = 0;
+    }
     V<R> B;
     const int cur = D.state[s].cur;
     B.U = (R *)DB.U[cur];
