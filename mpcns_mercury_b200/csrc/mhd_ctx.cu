@@ -23,6 +23,7 @@
 #include "mercury_mhd.h"
 #include "mhd_engine.cuh"
 #include "mhd_kernels.cuh"
+#include "mhd_parallel.h"
 
 using namespace mhd;
 
@@ -372,31 +373,52 @@ int dof_depth(const Solve *S, const mhd_dof &d) {
   return depth;
 }
 
-// max_depth < 0: every entry; otherwise only entries whose destination lies
-// at most max_depth ghost layers out.
-int upload_copies(Solve *S, const mhd_copy *tab, int n, int g, int phase, cudaStream_t st, int max_depth = -1) {
-  if (n < 0 || (n > 0 && !tab)) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, phase);
+// A copy table encoded as arena codes (validated once, shared by the phases
+// built from it).
+struct Encoded {
   std::vector<int64_t> dst, src;
-  std::vector<char> neg;
-  dst.reserve(n);
-  src.reserve(n);
-  neg.reserve(n);
-  for (int t = 0; t < n; ++t) {
+  std::vector<uint8_t> neg, depth;
+  bool ascending = true;  // destinations strictly increasing in table order
+};
+
+constexpr int kEncodeChunk = 1 << 13;
+
+// Encodes entries [t0, t1) of a table; records the first invalid entry of
+// the chunk and whether its destinations ascend.
+void encode_chunk(const Solve *S, const mhd_copy *tab, int t0, int t1, Encoded *e, int *bad, int *kind, char *asc) {
+  *bad = -1;
+  *asc = 1;
+  for (int t = t0; t < t1; ++t) {
     bool o1, o2;
     const int64_t dc = S->code(tab[t].dst, &o1);
     const int64_t sc = S->code(tab[t].src, &o2);
-    if (!o1 || !o2) return fail(MHD_ERR_ARG, "group %d phase %d: entry %d out of range", g, phase, t);
-    if (tab[t].sign != 1.0 && tab[t].sign != -1.0)
-      return fail(MHD_ERR_ARG, "group %d phase %d: entry %d has sign %g (must be +1 or -1)", g, phase, t, tab[t].sign);
-    if (max_depth >= 0 && dof_depth(S, tab[t].dst) > max_depth) continue;
-    dst.push_back(dc);
-    src.push_back(sc);
-    neg.push_back(tab[t].sign < 0.0);
+    if (!o1 || !o2 || (tab[t].sign != 1.0 && tab[t].sign != -1.0)) {
+      *bad = t;
+      *kind = (!o1 || !o2) ? 1 : 2;
+      return;
+    }
+    e->dst[t] = dc;
+    e->src[t] = sc;
+    e->neg[t] = tab[t].sign < 0.0;
+    const int d = dof_depth(S, tab[t].dst);
+    e->depth[t] = (uint8_t)(d > 255 ? 255 : d);
+    if (t > t0 && dc <= e->dst[t - 1]) *asc = 0;
   }
-  n = (int)dst.size();
-  std::vector<int> order(n);
-  for (int t = 0; t < n; ++t) order[t] = t;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return dst[a] < dst[c]; });
+}
+
+// One phase's segments from an encoded table.  max_depth < 0: every entry;
+// otherwise only entries whose destination lies at most max_depth ghost
+// layers out.  A table already in ascending destination order (the periodic
+// builder's) is segmented without a sort.
+std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth) {
+  const int n0 = (int)e.dst.size();
+  std::vector<int> order;
+  order.reserve(n0);
+  for (int t = 0; t < n0; ++t)
+    if (max_depth < 0 || e.depth[t] <= max_depth) order.push_back(t);
+  const int n = (int)order.size();
+  if (!e.ascending)
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return e.dst[a] < e.dst[c]; });
   std::vector<int64_t> seg;
   seg.reserve(2 * (size_t)n);
   int64_t sd = 0, ss = 0;
@@ -410,22 +432,81 @@ int upload_copies(Solve *S, const mhd_copy *tab, int n, int g, int phase, cudaSt
   };
   for (int u = 0; u < n; ++u) {
     const int t = order[u];
-    if (u + 1 < n && dst[order[u + 1]] == dst[t]) continue;  // a later entry overwrites this destination
-    if (len && len < kSegMax && dst[t] == sd + (int64_t)len * S->es && src[t] == ss + (int64_t)len * S->es &&
-        (bool)neg[t] == sneg) {
+    if (u + 1 < n && e.dst[order[u + 1]] == e.dst[t]) continue;  // a later entry overwrites this destination
+    if (len && len < kSegMax && e.dst[t] == sd + (int64_t)len * es && e.src[t] == ss + (int64_t)len * es &&
+        (bool)e.neg[t] == sneg) {
       ++len;
       continue;
     }
     flush();
-    sd = dst[t];
-    ss = src[t];
-    sneg = neg[t];
+    sd = e.dst[t];
+    ss = e.src[t];
+    sneg = e.neg[t];
     len = 1;
   }
   flush();
-  S->T->tab_n[g][phase] = (int)(seg.size() / 2);
-  S->T->table_bytes += (int64_t)seg.size() * 8;
-  return dev_upload(seg, &S->T->tab_seg[g][phase], st);
+  return seg;
+}
+
+// Every group's three phases (pruned halo, owner, full halo) compiled on the
+// host threads and uploaded.
+int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
+  // every table's chunks on one pool of host threads
+  constexpr int NT = 2 * MHD_NUM_GROUPS;
+  std::vector<Encoded> enc(NT);
+  const mhd_copy *tabs[NT];
+  int ntab[NT], first_chunk[NT + 1];
+  first_chunk[0] = 0;
+  for (int q = 0; q < NT; ++q) {
+    const int g = q / 2, p = q % 2;
+    tabs[q] = p ? groups[g].owner : groups[g].halo;
+    ntab[q] = p ? groups[g].n_owner : groups[g].n_halo;
+    if (ntab[q] < 0 || (ntab[q] > 0 && !tabs[q])) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, p);
+    Encoded &e = enc[q];
+    e.dst.resize(ntab[q]);
+    e.src.resize(ntab[q]);
+    e.neg.resize(ntab[q]);
+    e.depth.resize(ntab[q]);
+    first_chunk[q + 1] = first_chunk[q] + (ntab[q] + kEncodeChunk - 1) / kEncodeChunk;
+  }
+  const int nch = first_chunk[NT];
+  std::vector<int> bad(nch), kind(nch, 0);
+  std::vector<char> asc(nch);
+  std::vector<int> chunk_table(nch);
+  for (int q = 0; q < NT; ++q)
+    for (int c = first_chunk[q]; c < first_chunk[q + 1]; ++c) chunk_table[c] = q;
+  mhd::parallel_for(nch, [&](int c) {
+    const int q = chunk_table[c];
+    const int t0 = (c - first_chunk[q]) * kEncodeChunk, t1 = std::min(ntab[q], t0 + kEncodeChunk);
+    encode_chunk(S, tabs[q], t0, t1, &enc[q], &bad[c], &kind[c], &asc[c]);
+  });
+  for (int q = 0; q < NT; ++q) {
+    const int g = q / 2, p = q % 2;
+    Encoded &e = enc[q];
+    e.ascending = true;
+    for (int c = first_chunk[q]; c < first_chunk[q + 1]; ++c) {
+      if (bad[c] >= 0) {
+        if (kind[c] == 1) return fail(MHD_ERR_ARG, "group %d phase %d: entry %d out of range", g, p, bad[c]);
+        return fail(MHD_ERR_ARG, "group %d phase %d: entry %d has sign %g (must be +1 or -1)", g, p, bad[c],
+                    tabs[q][bad[c]].sign);
+      }
+      const int t0 = (c - first_chunk[q]) * kEncodeChunk;
+      if (!asc[c] || (t0 && e.dst[t0] <= e.dst[t0 - 1])) e.ascending = false;
+    }
+  }
+  std::vector<std::vector<int64_t>> seg(3 * MHD_NUM_GROUPS);
+  mhd::parallel_for(3 * MHD_NUM_GROUPS, [&](int q) {
+    const int g = q / 3, phase = q % 3;
+    seg[q] = build_segments(enc[2 * g + (phase == 1)], S->es, phase == 0 ? kHaloDepth[g] : -1);
+  });
+  for (int q = 0; q < 3 * MHD_NUM_GROUPS; ++q) {
+    const int g = q / 3, phase = q % 3;
+    S->T->tab_n[g][phase] = (int)(seg[q].size() / 2);
+    S->T->table_bytes += (int64_t)seg[q].size() * 8;
+    const int rc = dev_upload(seg[q], &S->T->tab_seg[g][phase], st);
+    if (rc) return rc;
+  }
+  return MHD_OK;
 }
 
 int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
@@ -827,10 +908,10 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
     S->T->tiles[r] = prefix[r].back();
     if ((rc = dev_upload(prefix[r], &S->T->dtile_prefix[r], st))) return bail(rc);
   }
-  for (int g = 0; g < MHD_NUM_GROUPS; ++g) {
-    if ((rc = upload_copies(S, desc->groups[g].halo, desc->groups[g].n_halo, g, 0, st, kHaloDepth[g]))) return bail(rc);
-    if ((rc = upload_copies(S, desc->groups[g].owner, desc->groups[g].n_owner, g, 1, st))) return bail(rc);
-    if ((rc = upload_copies(S, desc->groups[g].halo, desc->groups[g].n_halo, g, 2, st))) return bail(rc);
+  try {
+    if ((rc = upload_groups(S, desc->groups, st))) return bail(rc);
+  } catch (...) {  // host allocation or thread creation failed
+    return bail(fail(MHD_ERR_OOM, "host memory for the copy tables"));
   }
   if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
   SolveState s0{};

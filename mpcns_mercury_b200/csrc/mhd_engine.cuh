@@ -26,7 +26,16 @@ enum RangeKind : int {
   kNumRanges = 6
 };
 
-constexpr int kTileK = 32, kTileJ = 4, kTileI = 2, kTileThreads = kTileK * kTileJ * kTileI;
+// Fluid-kernel tile (cells along k, j, i); 256 threads per CTA everywhere.
+// 16 x 4 x 4 wastes fewer lanes than 32 x 4 x 2 on blocks whose k extent is
+// not a multiple of 32 and needs 6% fewer face fluxes per tile (912 vs 968).
+#ifndef MHD_TILE_K
+#define MHD_TILE_K 16
+#define MHD_TILE_J 4
+#define MHD_TILE_I 4
+#endif
+constexpr int kTileK = MHD_TILE_K, kTileJ = MHD_TILE_J, kTileI = MHD_TILE_I, kTileThreads = 256;
+static_assert(kTileK * kTileJ * kTileI == kTileThreads, "fluid tile of 256 cells");
 
 // Ghost depth the step keeps valid between its passes: the widest stencil
 // reach of its kernels (face EMF candidates on [-1, n + 2) read contravariant

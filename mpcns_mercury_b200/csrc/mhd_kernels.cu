@@ -529,7 +529,9 @@ __device__ __forceinline__ void rusanov(const V<R> &B, R g, int u0, int pv0, R k
 // shared memory (a face's flux has the same inputs and operation order for
 // both cells that share it), then every cell accumulates
 // r[m] -= (F+ - F-) / J, the per-component order of Scheme_U_'s divergence.
-constexpr int kMaxFaces = (kTileI + 1) * kTileJ * kTileK;
+constexpr int cmax3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b > c ? b : c); }
+constexpr int kMaxFaces = cmax3((kTileI + 1) * kTileJ * kTileK, kTileI * (kTileJ + 1) * kTileK,
+                                kTileI * kTileJ * (kTileK + 1));
 // Minimum resident CTAs per SM asked of the compiler for the two
 // register-heavy kernels (caps registers at 65536 / (256 * n)).
 #ifndef MHD_MIN_CTAS_FLUID

@@ -19,14 +19,29 @@
 // node-like indices in [0, n) and members are listed in lexicographic (i, j, k)
 // order, the order the reference's topology stores them in.
 #include <cstdint>
+#include <memory>
 #include <new>
 #include <vector>
 
 #include "mercury_mhd.h"
 #include "mhd_layout.cuh"
+#include "mhd_parallel.h"
+
+// A copy table whose entries are written once, by the building threads (no
+// zero-fill of a freshly allocated table).
+struct CopyTable {
+  std::unique_ptr<mhd_copy[]> p;
+  size_t n = 0;
+  void allocate(size_t count) {
+    p.reset(count ? new mhd_copy[count] : nullptr);
+    n = count;
+  }
+  mhd_copy *data() const { return p.get(); }
+  size_t size() const { return n; }
+};
 
 struct mhd_topology {
-  std::vector<mhd_copy> halo[MHD_NUM_GROUPS], owner[MHD_NUM_GROUPS];
+  CopyTable halo[MHD_NUM_GROUPS], owner[MHD_NUM_GROUPS];
   std::vector<int32_t> alias_offset;
   std::vector<mhd_dof> alias_member, alias_owner;
   std::vector<double> alias_msign, alias_osign;
@@ -50,50 +65,89 @@ const GroupSpec kGroups[] = {
     {MHD_SYNC_J_CELL, 0, {MHD_J_CELL}},
 };
 
-void build_group(mhd_topology *t, const GroupSpec &gs, const int n[3], int g) {
-  for (int field : gs.fields) {
-    const int loc = mhd::kFieldSpec[field].loc;
-    const int nc = mhd::kFieldSpec[field].ncomp;
-    const int *st = mhd::kStagger[loc];
-    for (int i = -g; i < n[0] + st[0] + g; ++i)
-      for (int j = -g; j < n[1] + st[1] + g; ++j)
-        for (int k = -g; k < n[2] + st[2] + g; ++k) {
-          const int idx[3] = {i, j, k};
-          int src[3];
-          int nout = 0;
-          for (int a = 0; a < 3; ++a) nout += !(idx[a] >= 0 && idx[a] < n[a] + st[a]);
-          bool is_owner_copy = false;
-          if (nout == 0) {
-            bool alias = false;
-            for (int a = 0; a < 3; ++a) {
-              const bool al = st[a] && idx[a] == n[a];
-              src[a] = al ? 0 : idx[a];
-              alias = alias || al;
-            }
-            if (!alias) continue;
-            is_owner_copy = true;
-          } else {
-            if (gs.corner1d && nout > 1) continue;
-            for (int a = 0; a < 3; ++a) {
-              int v = idx[a];
-              if (st[a]) {
-                if (v < 0) v += n[a];
-                else if (v > n[a]) v -= n[a];
-              } else {
-                v = ((v % n[a]) + n[a]) % n[a];
-              }
-              src[a] = v;
-            }
+// One field component of a group: its halo and owner copies are emitted in
+// (i, j, k) order, the order of the engine's arena, so the compiled tables
+// need no sort.  emit(copy, is_owner) receives every entry.
+template <class Emit>
+void walk_unit(const GroupSpec &gs, int field, int m, const int n[3], int g, Emit &&emit) {
+  const int *st = mhd::kStagger[mhd::kFieldSpec[field].loc];
+  for (int i = -g; i < n[0] + st[0] + g; ++i)
+    for (int j = -g; j < n[1] + st[1] + g; ++j) {
+      // (i, j) owned and not an alias index: positions k in [0, n) copy nothing
+      const bool ij_in = i >= 0 && i < n[0] + st[0] && j >= 0 && j < n[1] + st[1];
+      const bool ij_alias = (st[0] && i == n[0]) || (st[1] && j == n[1]);
+      const bool skip_interior = ij_in && !ij_alias;
+      for (int k = -g; k < n[2] + st[2] + g; ++k) {
+        if (skip_interior && k == 0) k = n[2];
+        const int idx[3] = {i, j, k};
+        int src[3];
+        int nout = 0;
+        for (int a = 0; a < 3; ++a) nout += !(idx[a] >= 0 && idx[a] < n[a] + st[a]);
+        bool is_owner_copy = false;
+        if (nout == 0) {
+          bool alias = false;
+          for (int a = 0; a < 3; ++a) {
+            const bool al = st[a] && idx[a] == n[a];
+            src[a] = al ? 0 : idx[a];
+            alias = alias || al;
           }
-          for (int m = 0; m < nc; ++m) {
-            mhd_copy c;
-            c.dst = {field, 0, i, j, k, m};
-            c.src = {field, 0, src[0], src[1], src[2], m};
-            c.sign = 1.0;
-            (is_owner_copy ? t->owner : t->halo)[gs.group].push_back(c);
+          if (!alias) continue;
+          is_owner_copy = true;
+        } else {
+          if (gs.corner1d && nout > 1) continue;
+          for (int a = 0; a < 3; ++a) {
+            int v = idx[a];
+            if (st[a]) {
+              if (v < 0) v += n[a];
+              else if (v > n[a]) v -= n[a];
+            } else {
+              v = ((v % n[a]) + n[a]) % n[a];
+            }
+            src[a] = v;
           }
         }
+        mhd_copy c;
+        c.dst = {field, 0, i, j, k, m};
+        c.src = {field, 0, src[0], src[1], src[2], m};
+        c.sign = 1.0;
+        emit(c, is_owner_copy);
+      }
+    }
+}
+
+// Every group's tables, one field component per task: a counting pass sizes
+// the tables, a second pass writes each component's entries at its offset.
+void build_groups(mhd_topology *t, const int n[3], int g) {
+  struct Unit {
+    const GroupSpec *gs;
+    int field, m;
+    size_t nh, no, oh, oo;  // counts and offsets in the group's tables
+  };
+  std::vector<Unit> units;
+  for (const auto &gs : kGroups)
+    for (int field : gs.fields)
+      for (int m = 0; m < mhd::kFieldSpec[field].ncomp; ++m) units.push_back({&gs, field, m, 0, 0, 0, 0});
+  const int nu = (int)units.size();
+  mhd::parallel_for(nu, [&](int u) {
+    Unit &U = units[u];
+    walk_unit(*U.gs, U.field, U.m, n, g, [&](const mhd_copy &, bool own) { ++(own ? U.no : U.nh); });
+  });
+  size_t nh[MHD_NUM_GROUPS] = {}, no[MHD_NUM_GROUPS] = {};
+  for (Unit &U : units) {
+    U.oh = nh[U.gs->group];
+    U.oo = no[U.gs->group];
+    nh[U.gs->group] += U.nh;
+    no[U.gs->group] += U.no;
   }
+  for (int q = 0; q < MHD_NUM_GROUPS; ++q) {
+    t->halo[q].allocate(nh[q]);
+    t->owner[q].allocate(no[q]);
+  }
+  mhd::parallel_for(nu, [&](int u) {
+    const Unit &U = units[u];
+    mhd_copy *h = t->halo[U.gs->group].data() + U.oh, *o = t->owner[U.gs->group].data() + U.oo;
+    walk_unit(*U.gs, U.field, U.m, n, g, [&](const mhd_copy &c, bool own) { *(own ? o++ : h++) = c; });
+  });
 }
 
 void build_alias(mhd_topology *t, const int n[3]) {
@@ -138,8 +192,13 @@ extern "C" int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghos
   auto *t = new (std::nothrow) mhd_topology();
   if (!t) return MHD_ERR_OOM;
   const int n[3] = {cells[0], cells[1], cells[2]};
-  for (const auto &gs : kGroups) build_group(t, gs, n, nghost);
-  build_alias(t, n);
+  try {
+    build_groups(t, n, nghost);
+    build_alias(t, n);
+  } catch (...) {  // allocation or thread creation failed
+    delete t;
+    return MHD_ERR_OOM;
+  }
   *out = t;
   return MHD_OK;
 }
