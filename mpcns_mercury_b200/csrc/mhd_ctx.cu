@@ -728,6 +728,7 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
   if (!out || capacity < 1 || capacity > 65536) return fail(MHD_ERR_ARG, "mhd_batch_create: capacity %d", capacity);
   if (precision != kFP64 && precision != kMixed) return fail(MHD_ERR_ARG, "mhd_batch_create: precision %d", precision);
   *out = nullptr;
+  init_launch_grids();
   auto *b = new (std::nothrow) mhd_batch();
   if (!b) return fail(MHD_ERR_OOM, "host allocation");
   b->capacity = capacity;

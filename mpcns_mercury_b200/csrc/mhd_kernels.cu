@@ -13,6 +13,7 @@
 //   * B_cell/Bind_cell and J_edge share one pass over the face fluxes;
 //   * the next step's CFL dt is reduced in the same pass that refreshes the
 //     primitive variables (both read U and B_cell after their syncs).
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -1335,43 +1336,94 @@ __global__ void k_retire(Dir D) {
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
-static int g_grid_tiles = 0, g_grid_copy = 0;
-static void grids() {
-  if (g_grid_tiles) return;
+// Every range kernel is persistent (grid-stride over tiles): its grid is the
+// SM count times the CTAs of it that fit on one SM (at most 8), so all CTAs
+// are resident at once and none starts in a late partial wave.  The
+// residual-dot kernel keeps a fixed grid: its partial sums are indexed by CTA.
+static int g_grid_tiles = 0;
+static int g_grid_kernel[SK_COUNT];
+
+template <class R>
+static const void *kernel_fn(StepKernel k) {
+  switch (k) {
+    case SK_FACE_EMF: return (const void *)k_face_emf<R>;
+    case SK_EDGE_EMF: return (const void *)k_edge_emf<R>;
+    case SK_HALL_CELL: return (const void *)k_hall_cell<R>;
+    case SK_HALL_EDGE: return (const void *)k_hall_edge<R>;
+    case SK_ADD_HALL: return (const void *)k_add_hall<R>;
+    case SK_FLUID: return (const void *)k_fluid<R>;
+    case SK_BFACE: return (const void *)k_bface<R>;
+    case SK_BCELL_JEDGE: return (const void *)k_bcell_jedge<R>;
+    case SK_JCELL: return (const void *)k_jcell<R>;
+    case SK_PV_UPLUS: return (const void *)k_pv_uplus<R>;
+    case SK_SYNC: return (const void *)k_sync<R>;
+    case SK_FACE_NORMALS: return (const void *)k_face_normals<R>;
+    case SK_DIVB: return (const void *)k_div_b<R>;
+    case SK_RES_SEED: return (const void *)k_res_seed<R>;
+    case SK_RES_W: return (const void *)k_res_w<R>;
+    case SK_RES_VEC: return (const void *)k_res_vec<R>;
+    case SK_RES_DB: return (const void *)k_res_db<R>;
+    case SK_RES_DJ: return (const void *)k_res_dj<R>;
+    case SK_RES_Q: return (const void *)k_res_q<R>;
+    case SK_RES_COPYB: return (const void *)k_res_copyb<R>;
+    case SK_RES_BUPDATE: return (const void *)k_res_bupdate<R>;
+    default: return nullptr;
+  }
+}
+
+static std::once_flag g_grids_once;
+
+template <class R>
+static void grids_init() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  g_grid_tiles = sms * 8;  // persistent: up to 8 resident 256-thread CTAs per SM
-  g_grid_copy = sms * 8;
+  for (int k = 0; k < SK_COUNT; ++k) {
+    int per_sm = 8;
+    const void *fn = kernel_fn<R>((StepKernel)k);
+    if (fn && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTileThreads, 0) != cudaSuccess ||
+               per_sm < 1)) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    g_grid_kernel[k] = sms * (per_sm < 8 ? per_sm : 8);
+  }
+  g_grid_tiles = sms * 8;
+}
+
+template <class R>
+static void grids() {
+  std::call_once(g_grids_once, grids_init<R>);
 }
 
 template <class R>
 static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
                       ResScratch rs) {
+  const int G = g_grid_kernel[k];
   switch (k) {
-    case SK_FACE_EMF: k_face_emf<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_EDGE_EMF: k_edge_emf<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_HALL_CELL: k_hall_cell<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_HALL_EDGE: k_hall_edge<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_ADD_HALL: k_add_hall<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_FLUID: k_fluid<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_BFACE: k_bface<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_BCELL_JEDGE: k_bcell_jedge<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_JCELL: k_jcell<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_PV_UPLUS: k_pv_uplus<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_SYNC: k_sync<R><<<g_grid_copy, 256, 0, st>>>(D, *ops); break;
-    case SK_FACE_NORMALS: k_face_normals<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_DIVB: k_div_b<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_SEED: k_res_seed<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_W: k_res_w<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_VEC: k_res_vec<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, darg); break;
-    case SK_RES_DB: k_res_db<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_DJ: k_res_dj<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_Q: k_res_q<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_FACE_EMF: k_face_emf<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_EDGE_EMF: k_edge_emf<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_HALL_CELL: k_hall_cell<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_HALL_EDGE: k_hall_edge<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_ADD_HALL: k_add_hall<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_FLUID: k_fluid<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_BFACE: k_bface<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_BCELL_JEDGE: k_bcell_jedge<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_JCELL: k_jcell<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_PV_UPLUS: k_pv_uplus<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_SYNC: k_sync<R><<<G, kTileThreads, 0, st>>>(D, *ops); break;
+    case SK_FACE_NORMALS: k_face_normals<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_DIVB: k_div_b<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_SEED: k_res_seed<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_W: k_res_w<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_VEC: k_res_vec<R><<<G, kTileThreads, 0, st>>>(D, iarg, darg); break;
+    case SK_RES_DB: k_res_db<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_DJ: k_res_dj<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_Q: k_res_q<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_RES_DOT: k_res_dot<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.partial); break;
     case SK_RES_SUM: k_res_sum<<<1, 32, 0, st>>>(rs.partial, g_grid_tiles, rs.result); break;
-    case SK_RES_COPYB: k_res_copyb<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg); break;
-    case SK_RES_BUPDATE: k_res_bupdate<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_COPYB: k_res_copyb<R><<<G, kTileThreads, 0, st>>>(D, iarg); break;
+    case SK_RES_BUPDATE: k_res_bupdate<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
     default: break;
@@ -1385,9 +1437,11 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
 #if MHD_KERNELS_F32
 void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
                             ResScratch rs) {
-  grids();
+  grids<float>();
   launch_as<float>(k, D, st, ops, iarg, darg, rs);
 }
+
+void init_launch_grids_f32() { grids<float>(); }
 #else
 void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
                             ResScratch rs);
@@ -1397,13 +1451,20 @@ void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncO
   if (precision == kMixed) {
     launch_step_kernel_f32(k, D, st, ops, iarg, darg, rs);
   } else {
-    grids();
+    grids<double>();
     launch_as<double>(k, D, st, ops, iarg, darg, rs);
   }
 }
 
+void init_launch_grids_f32();
+
+void init_launch_grids() {
+  grids<double>();
+  init_launch_grids_f32();
+}
+
 int res_dot_grid() {
-  grids();
+  grids<double>();
   return g_grid_tiles;
 }
 

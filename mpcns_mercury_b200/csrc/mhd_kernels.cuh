@@ -44,6 +44,8 @@ struct ResScratch {
 void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision, int iarg = 0,
                         double darg = 0.0, ResScratch rs = ResScratch{nullptr, nullptr});
 int res_dot_grid();
+// Queries every kernel's resident CTAs per SM once (call before any stream capture).
+void init_launch_grids();
 const char *step_kernel_name(StepKernel k);
 
 }  // namespace mhd
