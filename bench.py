@@ -59,8 +59,8 @@ L2_BYTES = 126 * 1024 * 1024
 # (Jac, JD) is 8 B in both.  Kernels over the allocated cell range count the
 # allocated cells.
 KERNEL_COMPS = {
-    "k_face_emf": (3 + 3 + 3 + 9, 0),                        # B, Badd, UCON -> Eface
-    "k_edge_emf": (9 + 3 + 3 + 2 + 2 + 3, 0),                # Eface, UCON, B, p_e x2, rho x2 -> E
+    "k_face_emf": (3 + 3 + 3 + 9 + 2 + 1, 0),                # B, Badd, UCON, p x2 -> Eface, node p_e
+    "k_edge_emf": (9 + 3 + 3 + 1 + 2 + 3, 0),                # Eface, UCON, B, node p_e, rho x2 -> E
     "k_hall_cell": (2 + 3 + 3 + 3 + 1, 0),                   # rho x2, J_cell, B_cell -> EHC, beta
     "k_hall_edge": (3 + 1 + 9 + 3 + 3 + 3 + 3 + 3, 0),       # EHC, beta, dr, dl, Area, B, taper -> Ehall
     "k_add_hall": (3 + 3 + 3, 0),                            # E += Ehall

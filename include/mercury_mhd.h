@@ -60,6 +60,7 @@ enum mhd_field {
   MHD_UCON,                                   /* contravariant U_plus components along xi, eta, zeta */
   MHD_DIVB,                                   /* div B per cell (mhd_div_b) */
   MHD_FNORM_XI, MHD_FNORM_ETA, MHD_FNORM_ZETA, /* unit normal (3) and |JD| of the faces, set by mhd_prepare */
+  MHD_PE_NODE,                                /* electron pressure at the nodes: 8-cell mean of p_H + p_Na (ambipolar) */
   /* static geometry and sources (uploaded once) */
   MHD_JAC, MHD_JDXI, MHD_JDET, MHD_JDZE, MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA,
   MHD_DL_XI, MHD_DL_ETA, MHD_DL_ZETA, MHD_DR_XI, MHD_DR_ETA, MHD_DR_ZETA,
@@ -76,7 +77,8 @@ enum mhd_field {
   MHD_NUM_FIELDS
 };
 
-enum mhd_location { MHD_CELL = 0, MHD_FACE_XI, MHD_FACE_ETA, MHD_FACE_ZETA, MHD_EDGE_XI, MHD_EDGE_ETA, MHD_EDGE_ZETA };
+enum mhd_location { MHD_CELL = 0, MHD_FACE_XI, MHD_FACE_ETA, MHD_FACE_ZETA, MHD_EDGE_XI, MHD_EDGE_ETA, MHD_EDGE_ZETA,
+                    MHD_NODE };
 
 /* Sync groups: MercuryBoundary::Sync names (Z4_Mercury/src/boundary/Boundary_Build.cpp:564-703). */
 enum mhd_group { MHD_SYNC_UCELL = 0, MHD_SYNC_BFACE, MHD_SYNC_EHALL, MHD_SYNC_EEDGE, MHD_SYNC_B_CELL,

@@ -344,13 +344,6 @@ int publish(mhd_batch *b) {
   return MHD_OK;
 }
 
-// One group phase's copy table as segments: sorted by destination (a
-// destination written twice keeps the later entry, as sequential
-// application would), then runs of consecutive destinations with
-// consecutive sources and the same sign merged, up to kSegMax elements.
-// Destinations of one phase are distinct and no copy of a phase reads a
-// value the phase writes, so the order of application does not change the
-// result.  Signs must be +1 or -1 (orientation flips).
 // Ghost depth each group's halo is filled to inside the step: the farthest
 // ghost layer any kernel of the step reads it at (U and the face fluxes: the
 // face EMF candidates and contravariant velocities two layers out; B_cell and
@@ -409,7 +402,16 @@ void encode_chunk(const Solve *S, const mhd_copy *tab, int t0, int t1, Encoded *
 // One phase's segments from an encoded table.  max_depth < 0: every entry;
 // otherwise only entries whose destination lies at most max_depth ghost
 // layers out.  A table already in ascending destination order (the periodic
-// builder's) is segmented without a sort.
+// builder's) is segmented without a sort.  Entries sorted by destination (a
+// destination written twice keeps the later entry, as sequential application
+// would) form runs of up to kSegMax consecutive destinations with
+// consecutive sources and one sign; runs of equal length, sign and
+// source - destination offset whose destinations step by one stride are then
+// merged into strided segments of up to kSegElems elements (the k ghosts of
+// successive grid lines, the alias layer of a staggered axis).  Destinations
+// of one phase are distinct and no copy of a phase reads a value the phase
+// writes, so the order of application does not change the result.  Signs
+// must be +1 or -1 (orientation flips).
 std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth) {
   const int n0 = (int)e.dst.size();
   std::vector<int> order;
@@ -419,32 +421,58 @@ std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth) {
   const int n = (int)order.size();
   if (!e.ascending)
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return e.dst[a] < e.dst[c]; });
-  std::vector<int64_t> seg;
-  seg.reserve(2 * (size_t)n);
-  int64_t sd = 0, ss = 0;
-  int len = 0;
-  bool sneg = false;
-  auto flush = [&]() {
-    if (!len) return;
-    seg.push_back(sd | ((int64_t)(len - 1) << kSegLenShift) | ((int64_t)sneg << kSegNegBit));
-    seg.push_back(ss);
-    len = 0;
+  struct Run {
+    int64_t dst, src;
+    int len;
+    bool neg;
   };
+  std::vector<Run> runs;
+  runs.reserve(n / 2 + 1);
   for (int u = 0; u < n; ++u) {
     const int t = order[u];
     if (u + 1 < n && e.dst[order[u + 1]] == e.dst[t]) continue;  // a later entry overwrites this destination
-    if (len && len < kSegMax && e.dst[t] == sd + (int64_t)len * es && e.src[t] == ss + (int64_t)len * es &&
-        (bool)e.neg[t] == sneg) {
-      ++len;
-      continue;
+    if (!runs.empty()) {
+      Run &r = runs.back();
+      if (r.len < kSegMax && e.dst[t] == r.dst + (int64_t)r.len * es && e.src[t] == r.src + (int64_t)r.len * es &&
+          (bool)e.neg[t] == r.neg) {
+        ++r.len;
+        continue;
+      }
     }
-    flush();
-    sd = e.dst[t];
-    ss = e.src[t];
-    sneg = e.neg[t];
-    len = 1;
+    runs.push_back(Run{e.dst[t], e.src[t], 1, (bool)e.neg[t]});
   }
-  flush();
+  // runs of one (len, sign, src - dst) class, each class in destination order
+  std::vector<int> ro(runs.size());
+  for (size_t q = 0; q < runs.size(); ++q) ro[q] = (int)q;
+  std::stable_sort(ro.begin(), ro.end(), [&](int a, int c) {
+    const Run &x = runs[a], &y = runs[c];
+    if (x.len != y.len) return x.len < y.len;
+    if (x.neg != y.neg) return x.neg < y.neg;
+    return x.src - x.dst < y.src - y.dst;
+  });
+  std::vector<int64_t> seg;
+  seg.reserve(kSegWords * runs.size());
+  for (size_t u = 0; u < ro.size();) {
+    const Run &r0 = runs[ro[u]];
+    int reps = 1;
+    int64_t stride = 0;
+    while (u + reps < ro.size() && (reps + 1) * r0.len <= kSegElems && reps < 65536) {
+      const Run &rn = runs[ro[u + reps]];
+      if (rn.len != r0.len || rn.neg != r0.neg || rn.src - rn.dst != r0.src - r0.dst) break;
+      const int64_t step = rn.dst - runs[ro[u + reps - 1]].dst;
+      if (reps == 1) {
+        if (step <= 0 || step >= (int64_t(1) << (63 - kSegStrideShift))) break;
+        stride = step;
+      } else if (step != stride) {
+        break;
+      }
+      ++reps;
+    }
+    seg.push_back(r0.dst | ((int64_t)(r0.len - 1) << kSegLenShift) | ((int64_t)r0.neg << kSegNegBit));
+    seg.push_back(r0.src);
+    seg.push_back((int64_t)(reps - 1) | (stride << kSegStrideShift));
+    u += reps;
+  }
   return seg;
 }
 
@@ -501,7 +529,7 @@ int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
   });
   for (int q = 0; q < 3 * MHD_NUM_GROUPS; ++q) {
     const int g = q / 3, phase = q % 3;
-    S->T->tab_n[g][phase] = (int)(seg[q].size() / 2);
+    S->T->tab_n[g][phase] = (int)(seg[q].size() / kSegWords);
     S->T->table_bytes += (int64_t)seg[q].size() * 8;
     const int rc = dev_upload(seg[q], &S->T->tab_seg[g][phase], st);
     if (rc) return rc;

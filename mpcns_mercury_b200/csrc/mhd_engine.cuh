@@ -116,13 +116,21 @@ struct SolveState {
 // synced components are real-valued.
 constexpr int64_t kCodeOffMask = (int64_t(1) << 55) - 1;
 constexpr int64_t kCodeUFlag = int64_t(1) << 60;
-// Copy segments: `len` (1..32) consecutive destinations dst.. <- sign * src..
-// (consecutive sources), stored as two int64: dst code with (len - 1) in bits
-// 55..59 and a negative sign in bit 61, and the src code.
-constexpr int kSegMax = 32;
-constexpr int kSegLenShift = 55, kSegNegBit = 61;
+// Copy segments: `reps` runs of `len` (1..32) consecutive destinations
+// dst + r * stride .. <- sign * (src + r * stride) .. (consecutive sources),
+// len * reps <= kSegElems, stored as three int64: the dst code with
+// (len - 1) in bits 55..59 and a negative sign in bit 61; the src code;
+// (reps - 1) in bits 0..15 and the byte stride in bits 16..63.
+constexpr int kSegMax = 32;     // elements of one run
+#ifndef MHD_SEG_ELEMS
+#define MHD_SEG_ELEMS 32
+#endif
+constexpr int kSegElems = MHD_SEG_ELEMS;  // elements of one segment (a multiple of 8, at most 64)
+static_assert(kSegElems % 8 == 0 && kSegElems <= 64, "segment size");
+constexpr int kSegWords = 3;
+constexpr int kSegLenShift = 55, kSegNegBit = 61, kSegStrideShift = 16;
 struct DevTable {
-  const int64_t *seg = nullptr;  // 2 * n
+  const int64_t *seg = nullptr;  // kSegWords * n
   int n = 0;                     // segments
 };
 // Edge alias classes: members member[offset[c] .. offset[c+1]) (codes and

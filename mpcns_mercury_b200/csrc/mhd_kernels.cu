@@ -41,6 +41,7 @@ constexpr int cETAR = kComp.first[MHD_ETA_RES_XI];  // ETA_RES_ETA, ETA_RES_ZETA
 constexpr int cRW = kComp.first[MHD_RES_W], cRX = kComp.first[MHD_RES_X], cRR = kComp.first[MHD_RES_R],
               cRP = kComp.first[MHD_RES_P], cRQ = kComp.first[MHD_RES_Q], cRBS = kComp.first[MHD_RES_BSTAR];
 constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA], cFNZ = kComp.first[MHD_FNORM_ZETA];
+constexpr int cPEN = kComp.first[MHD_PE_NODE];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
 constexpr int cAX = kComp.first[MHD_AREA_XI], cAY = kComp.first[MHD_AREA_ETA], cAZ = kComp.first[MHD_AREA_ZETA];
@@ -242,14 +243,32 @@ __device__ __forceinline__ R emf_flux(const V<R> &B, int ba, int fa, int iL, int
   return R(0.5) * (GL + GR) - R(0.5) * r * (biR - biL);
 }
 
+// Electron pressure at node (i, j, k): the mean of p_H + p_Na over the 8
+// cells around it, summed in the order of AddAmbipolarEdgeEMF_
+// (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Ambipo.cpp:3-143).
+template <class R>
+__device__ __forceinline__ R pe_node(const V<R> &B, int i, int j, int k) {
+  R sum = R(0.0);
+  for (int di = -1; di <= 0; ++di)
+    for (int dj = -1; dj <= 0; ++dj)
+      for (int dk = -1; dk <= 0; ++dk)
+        sum += AT(cPVH + 3, i + di, j + dj, k + dk) + AT(cPVN + 3, i + di, j + dj, k + dk);
+  return R(0.125) * sum;
+}
+
 // AssembleOneDirectionEMF_ (Ideal.cpp:433-594) for all three face families on
-// [-1, inner_hi + 1) (the one locally evaluated ghost layer, Ideal.cpp:548-555).
+// [-1, inner_hi + 1) (the one locally evaluated ghost layer, Ideal.cpp:548-555),
+// and, with the ambipolar term on, the node electron pressure on [0, n + 1)
+// that the edge EMFs of the owned edges read (each node is shared by six
+// edges).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
   for_items<R, kExt>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
     const int q[3] = {i, j, k}, n[3] = {B.n0, B.n1, B.n2};
+    if (consts_of<R>(S).ambipolar && i >= 0 && j >= 0 && k >= 0 && i <= n[0] && j <= n[1] && k <= n[2])
+      AT(cPEN, i, j, k) = pe_node(B, i, j, k);
 #pragma unroll 1
     for (int fa = 0; fa < 3; ++fa) {
       bool in = true;
@@ -293,15 +312,6 @@ __device__ __forceinline__ R max_abs_u4(const V<R> &B, int axis, int i0, int j0,
   a = dmax(a, fabs(ucon(B, axis, i2, j2, k2)));
   a = dmax(a, fabs(ucon(B, axis, i3, j3, k3)));
   return a;
-}
-template <class R>
-__device__ __forceinline__ R pe_node(const V<R> &B, int i, int j, int k) {
-  R sum = R(0.0);
-  for (int di = -1; di <= 0; ++di)
-    for (int dj = -1; dj <= 0; ++dj)
-      for (int dk = -1; dk <= 0; ++dk)
-        sum += AT(cPVH + 3, i + di, j + dj, k + dk) + AT(cPVN + 3, i + di, j + dj, k + dk);
-  return R(0.125) * sum;
 }
 
 // AddArtificialResistivityToEdgeEMF_ and AddLocalArtificialResistivityToEdgeEMF_
@@ -349,7 +359,7 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
       const R d2 = AT(cBY, i, j, k) - AT(cBY, i, j, k - 1);
       R e = Ec + Cuct * (R(0.5) * ae * d1 - R(0.5) * az * d2);
       if (c.ambipolar) {
-        const R p0 = pe_node(B, i, j, k), p1 = pe_node(B, i + 1, j, k);
+        const R p0 = AT(cPEN, i, j, k), p1 = AT(cPEN, i + 1, j, k);
         R rH = R(0.0), rN = R(0.0);
         for (int dj = -1; dj <= 0; ++dj)
           for (int dk = -1; dk <= 0; ++dk) {
@@ -369,7 +379,7 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
       const R d2 = AT(cBZ, i, j, k) - AT(cBZ, i - 1, j, k);
       R e = Ec + Cuct * (R(0.5) * az * d1 - R(0.5) * ax * d2);
       if (c.ambipolar) {
-        const R p0 = pe_node(B, i, j, k), p1 = pe_node(B, i, j + 1, k);
+        const R p0 = AT(cPEN, i, j, k), p1 = AT(cPEN, i, j + 1, k);
         R rH = R(0.0), rN = R(0.0);
         for (int di = -1; di <= 0; ++di)
           for (int dk = -1; dk <= 0; ++dk) {
@@ -389,7 +399,7 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
       const R d2 = AT(cBX, i, j, k) - AT(cBX, i, j - 1, k);
       R e = Ec + Cuct * (R(0.5) * ax * d1 - R(0.5) * ae * d2);
       if (c.ambipolar) {
-        const R p0 = pe_node(B, i, j, k), p1 = pe_node(B, i, j, k + 1);
+        const R p0 = AT(cPEN, i, j, k), p1 = AT(cPEN, i, j, k + 1);
         R rH = R(0.0), rN = R(0.0);
         for (int di = -1; di <= 0; ++di)
           for (int dj = -1; dj <= 0; ++dj) {
@@ -539,7 +549,7 @@ constexpr int kMaxFaces = cmax3((kTileI + 1) * kTileJ * kTileK, kTileI * (kTileJ
 #define MHD_MIN_CTAS_FLUID 3
 #endif
 #ifndef MHD_MIN_CTAS_PV
-#define MHD_MIN_CTAS_PV 3
+#define MHD_MIN_CTAS_PV 4
 #endif  // largest per-direction face count of a tile
 template <class R>
 __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir D) {
@@ -1257,9 +1267,10 @@ __device__ __forceinline__ const int *op_prefix(const Dir &D, const SyncOp &op) 
 // ReduceEdgeAliasCandidatesToOwners_ (Z4_Mercury/src/physics/MercurySolver_Current.cpp:3-57)
 // for every active solve, up to two independent operations per launch.
 // Work unit: a group of 8 lanes.  A copy phase gives each group one segment
-// (dst <- sign * src on up to 8 consecutive elements); an alias reduction
-// gives each lane one class, whose members are summed in stored order from
-// 0.0 and written to the owner as owner_sign * sum / count.
+// (dst <- sign * src on up to kSegElems elements: reps strided runs of len
+// consecutive elements); an alias reduction gives each lane one class, whose
+// members are summed in stored order from 0.0 and written to the owner as
+// owner_sign * sum / count.
 template <class R>
 __global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
   const int lane = threadIdx.x & 7;
@@ -1280,18 +1291,29 @@ __global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
     const int cur = D.state[s].cur;
     if (op.kind == SYNC_COPY) {
       const DevTable &T = op.phase == 1 ? S.owner[op.arg] : op.phase == 2 ? S.halo_full[op.arg] : S.halo[op.arg];
-      const int64_t dcode = T.seg[2 * q], scode = T.seg[2 * q + 1];
+      const int64_t *w = T.seg + kSegWords * (int64_t)q;
+      const int64_t dcode = w[0], scode = w[1], rw = w[2];
       const int len = (int)((dcode >> kSegLenShift) & 31) + 1;
+      const int n = len * ((int)(rw & 0xffff) + 1);
+      const int64_t stride = rw >> kSegStrideShift;  // bytes between runs
       const bool neg = (dcode >> kSegNegBit) & 1;
-      const R *src = at_code<R>(S, cur, scode);
-      R *dst = at_code<R>(S, cur, dcode);
-      R v[kSegMax / 8];
+      const char *src = (const char *)at_code<R>(S, cur, scode);
+      char *dst = (char *)at_code<R>(S, cur, dcode);
+      // element e of the segment: run e / len, offset e % len (e < 64, so
+      // e * ceil(2^16 / len) >> 16 is the exact quotient)
+      const int inv = (65536 + len - 1) / len;
+      R v[kSegElems / 8];
+      int64_t off[kSegElems / 8];
 #pragma unroll
-      for (int u = 0; u < kSegMax / 8; ++u)
-        if (lane + 8 * u < len) v[u] = src[lane + 8 * u];
+      for (int u = 0; u < kSegElems / 8; ++u) {
+        const int e = lane + 8 * u;
+        const int r = (e * inv) >> 16;
+        off[u] = r * stride + (int64_t)(e - r * len) * (int64_t)sizeof(R);
+        if (e < n) v[u] = *(const R *)(src + off[u]);
+      }
 #pragma unroll
-      for (int u = 0; u < kSegMax / 8; ++u)
-        if (lane + 8 * u < len) dst[lane + 8 * u] = neg ? -v[u] : v[u];
+      for (int u = 0; u < kSegElems / 8; ++u)
+        if (lane + 8 * u < n) *(R *)(dst + off[u]) = neg ? -v[u] : v[u];
     } else {
       const DevAlias &A = op.arg ? S.aliasJ : S.aliasE;
       const int c = q * 8 + lane;

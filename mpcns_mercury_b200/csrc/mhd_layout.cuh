@@ -38,7 +38,8 @@ constexpr FieldSpec kFieldSpec[MHD_NUM_FIELDS] = {
     {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA},
     {3, MHD_FACE_XI},   {3, MHD_FACE_ETA},  {3, MHD_FACE_ZETA}, {3, MHD_CELL},      {1, MHD_CELL},
     {3, MHD_CELL} /* UCON */, {1, MHD_CELL} /* DIVB */,
-    {4, MHD_FACE_XI},   {4, MHD_FACE_ETA},  {4, MHD_FACE_ZETA} /* FNORM */, {1, MHD_CELL},      {3, MHD_FACE_XI},   {3, MHD_FACE_ETA},  {3, MHD_FACE_ZETA}, {1, MHD_FACE_XI},
+    {4, MHD_FACE_XI},   {4, MHD_FACE_ETA},  {4, MHD_FACE_ZETA} /* FNORM */, {1, MHD_NODE} /* PE_NODE */,
+    {1, MHD_CELL},      {3, MHD_FACE_XI},   {3, MHD_FACE_ETA},  {3, MHD_FACE_ZETA}, {1, MHD_FACE_XI},
     {1, MHD_FACE_ETA},  {1, MHD_FACE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA},
     {3, MHD_EDGE_XI},   {3, MHD_EDGE_ETA},  {3, MHD_EDGE_ZETA}, {1, MHD_FACE_XI},   {1, MHD_FACE_ETA},
     {1, MHD_FACE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA}, {18, MHD_CELL},
@@ -50,7 +51,7 @@ constexpr FieldSpec kFieldSpec[MHD_NUM_FIELDS] = {
     {3, MHD_FACE_XI} /* RES_W, RES_X, RES_R, RES_P, RES_Q, RES_BSTAR */};
 
 // Stagger: 1 where the location is node-like (n + 1 owned DOFs) along an axis.
-constexpr int kStagger[7][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 0}};
+constexpr int kStagger[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 1, 1}};
 
 // First component index of each field in the component numbering
 // (U_H, U_Na occupy 0..9; everything else follows).
