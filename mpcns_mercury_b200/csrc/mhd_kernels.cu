@@ -230,17 +230,20 @@ __device__ __forceinline__ R cell_beta_tot(const V<R> &B, int axis, int i, int j
 template <class R>
 __device__ __forceinline__ R ucon(const V<R> &B, int axis, int i, int j, int k) { return AT(cUC + axis, i, j, k); }
 
-// flux() of AssembleOneDirectionEMF_ (Ideal.cpp:517-536)
+// flux() of AssembleOneDirectionEMF_ (Ideal.cpp:517-536).  The right cell's
+// cell-averaged total and induced B (btR[ba], biR[ba]) and contravariant
+// velocities (uR[a]) are evaluated once per cell by the caller: every face
+// family of the cell shares that cell.
 template <class R>
-__device__ __forceinline__ R emf_flux(const V<R> &B, int ba, int fa, int iL, int jL, int kL, int iR, int jR, int kR,
-                                           R bff) {
-  const R btL = cell_beta_tot(B, ba, iL, jL, kL), btR = cell_beta_tot(B, ba, iR, jR, kR);
-  const R biL = cell_beta_ind(B, ba, iL, jL, kL), biR = cell_beta_ind(B, ba, iR, jR, kR);
-  const R ufL = ucon(B, fa, iL, jL, kL), ufR = ucon(B, fa, iR, jR, kR);
-  const R ubL = ucon(B, ba, iL, jL, kL), ubR = ucon(B, ba, iR, jR, kR);
-  const R GL = ufL * btL - ubL * bff, GR = ufR * btR - ubR * bff;
+__device__ __forceinline__ R emf_flux(const V<R> &B, int ba, int fa, int iL, int jL, int kL, const R btR[3],
+                                      const R biR[3], const R uR[3], R bff) {
+  const R btL = cell_beta_tot(B, ba, iL, jL, kL);
+  const R biL = cell_beta_ind(B, ba, iL, jL, kL);
+  const R ufL = ucon(B, fa, iL, jL, kL), ufR = uR[fa];
+  const R ubL = ucon(B, ba, iL, jL, kL), ubR = uR[ba];
+  const R GL = ufL * btL - ubL * bff, GR = ufR * btR[ba] - ubR * bff;
   const R r = dmax(fabs(ufL), fabs(ufR));
-  return R(0.5) * (GL + GR) - R(0.5) * r * (biR - biL);
+  return R(0.5) * (GL + GR) - R(0.5) * r * (biR[ba] - biL);
 }
 
 // Electron pressure at node (i, j, k): the mean of p_H + p_Na over the 8
@@ -269,6 +272,14 @@ __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
     const int q[3] = {i, j, k}, n[3] = {B.n0, B.n1, B.n2};
     if (consts_of<R>(S).ambipolar && i >= 0 && j >= 0 && k >= 0 && i <= n[0] && j <= n[1] && k <= n[2])
       AT(cPEN, i, j, k) = pe_node(B, i, j, k);
+    // this cell is the right cell of its three faces
+    R btR[3], biR[3], uR[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      btR[a] = cell_beta_tot(B, a, i, j, k);
+      biR[a] = cell_beta_ind(B, a, i, j, k);
+      uR[a] = ucon(B, a, i, j, k);
+    }
 #pragma unroll 1
     for (int fa = 0; fa < 3; ++fa) {
       bool in = true;
@@ -279,18 +290,18 @@ __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
       const R bff = face_tot(B, fa, i, j, k);
       R e0 = R(0.0), e1 = R(0.0), e2 = R(0.0);
       if (fa == 0) {
-        const R Ge = emf_flux(B, 1, 0, iL, jL, kL, i, j, k, bff);
-        const R Gz = emf_flux(B, 2, 0, iL, jL, kL, i, j, k, bff);
+        const R Ge = emf_flux(B, 1, 0, iL, jL, kL, btR, biR, uR, bff);
+        const R Gz = emf_flux(B, 2, 0, iL, jL, kL, btR, biR, uR, bff);
         e1 = Gz;
         e2 = -Ge;
       } else if (fa == 1) {
-        const R Gx = emf_flux(B, 0, 1, iL, jL, kL, i, j, k, bff);
-        const R Gz = emf_flux(B, 2, 1, iL, jL, kL, i, j, k, bff);
+        const R Gx = emf_flux(B, 0, 1, iL, jL, kL, btR, biR, uR, bff);
+        const R Gz = emf_flux(B, 2, 1, iL, jL, kL, btR, biR, uR, bff);
         e0 = -Gz;
         e2 = Gx;
       } else {
-        const R Gx = emf_flux(B, 0, 2, iL, jL, kL, i, j, k, bff);
-        const R Ge = emf_flux(B, 1, 2, iL, jL, kL, i, j, k, bff);
+        const R Gx = emf_flux(B, 0, 2, iL, jL, kL, btR, biR, uR, bff);
+        const R Ge = emf_flux(B, 1, 2, iL, jL, kL, btR, biR, uR, bff);
         e0 = Ge;
         e1 = -Gx;
       }
