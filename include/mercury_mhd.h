@@ -61,6 +61,8 @@ enum mhd_field {
   MHD_DIVB,                                   /* div B per cell (mhd_div_b) */
   MHD_FNORM_XI, MHD_FNORM_ETA, MHD_FNORM_ZETA, /* unit normal (3) and |JD| of the faces, set by mhd_prepare */
   MHD_PE_NODE,                                /* electron pressure at the nodes: 8-cell mean of p_H + p_Na (ambipolar) */
+  MHD_AMBI_COEF,                              /* 9 cell-averaged JD / Jac coefficients of grad p_e, set by mhd_prepare */
+  MHD_DPE,                                    /* grad p_e term of the ion momentum sources per cell (ambipolar) */
   /* static geometry and sources (uploaded once) */
   MHD_JAC, MHD_JDXI, MHD_JDET, MHD_JDZE, MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA,
   MHD_DL_XI, MHD_DL_ETA, MHD_DL_ZETA, MHD_DR_XI, MHD_DR_ETA, MHD_DR_ZETA,

@@ -41,7 +41,7 @@ constexpr int cETAR = kComp.first[MHD_ETA_RES_XI];  // ETA_RES_ETA, ETA_RES_ZETA
 constexpr int cRW = kComp.first[MHD_RES_W], cRX = kComp.first[MHD_RES_X], cRR = kComp.first[MHD_RES_R],
               cRP = kComp.first[MHD_RES_P], cRQ = kComp.first[MHD_RES_Q], cRBS = kComp.first[MHD_RES_BSTAR];
 constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA], cFNZ = kComp.first[MHD_FNORM_ZETA];
-constexpr int cPEN = kComp.first[MHD_PE_NODE];
+constexpr int cPEN = kComp.first[MHD_PE_NODE], cAMB = kComp.first[MHD_AMBI_COEF], cDPE = kComp.first[MHD_DPE];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
 constexpr int cAX = kComp.first[MHD_AREA_XI], cAY = kComp.first[MHD_AREA_ETA], cAZ = kComp.first[MHD_AREA_ZETA];
@@ -263,15 +263,33 @@ __device__ __forceinline__ R pe_node(const V<R> &B, int i, int j, int k) {
 // [-1, inner_hi + 1) (the one locally evaluated ghost layer, Ideal.cpp:548-555),
 // and, with the ambipolar term on, the node electron pressure on [0, n + 1)
 // that the edge EMFs of the owned edges read (each node is shared by six
-// edges).
+// edges) and the grad p_e source term of the owned cells that the fluid
+// update of both species reads.
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_face_emf(Dir D) {
   for_items<R, kExt>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
     const int q[3] = {i, j, k}, n[3] = {B.n0, B.n1, B.n2};
-    if (consts_of<R>(S).ambipolar && i >= 0 && j >= 0 && k >= 0 && i <= n[0] && j <= n[1] && k <= n[2])
+    if (consts_of<R>(S).ambipolar && i >= 0 && j >= 0 && k >= 0 && i <= n[0] && j <= n[1] && k <= n[2]) {
       AT(cPEN, i, j, k) = pe_node(B, i, j, k);
+      if (i < n[0] && j < n[1] && k < n[2]) {
+        // grad p_e term of the ion momentum sources of an owned cell, the
+        // same for both species (AddSourceToRHS_Fluid, FluidRHS.cpp:206-527)
+        const R pip = AT(cPVH + 3, i + 1, j, k) + AT(cPVN + 3, i + 1, j, k);
+        const R pim = AT(cPVH + 3, i - 1, j, k) + AT(cPVN + 3, i - 1, j, k);
+        const R pjp = AT(cPVH + 3, i, j + 1, k) + AT(cPVN + 3, i, j + 1, k);
+        const R pjm = AT(cPVH + 3, i, j - 1, k) + AT(cPVN + 3, i, j - 1, k);
+        const R pkp = AT(cPVH + 3, i, j, k + 1) + AT(cPVN + 3, i, j, k + 1);
+        const R pkm = AT(cPVH + 3, i, j, k - 1) + AT(cPVN + 3, i, j, k - 1);
+        const R ax = AT(cAMB, i, j, k), ay = AT(cAMB + 1, i, j, k), az = AT(cAMB + 2, i, j, k);
+        const R bx = AT(cAMB + 3, i, j, k), by = AT(cAMB + 4, i, j, k), bz = AT(cAMB + 5, i, j, k);
+        const R cxm = AT(cAMB + 6, i, j, k), cym = AT(cAMB + 7, i, j, k), czm = AT(cAMB + 8, i, j, k);
+        AT(cDPE, i, j, k) = R(0.5) * (ax * (pip - pim) + bx * (pjp - pjm) + cxm * (pkp - pkm));
+        AT(cDPE + 1, i, j, k) = R(0.5) * (ay * (pip - pim) + by * (pjp - pjm) + cym * (pkp - pkm));
+        AT(cDPE + 2, i, j, k) = R(0.5) * (az * (pip - pim) + bz * (pjp - pjm) + czm * (pkp - pkm));
+      }
+    }
     // this cell is the right cell of its three faces
     R btR[3], biR[3], uR[3];
 #pragma unroll
@@ -653,29 +671,10 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
     const R sjbx = Jy * Bz - Jz * By, sjby = Jz * Bx - Jx * Bz, sjbz = Jx * By - Jy * Bx;
     const Num<R> num = num_limiter(c, CV(9), CV(10));
     R dpex = R(0.0), dpey = R(0.0), dpez = R(0.0);
-    if (c.ambipolar) {
-      const R Vol = fabs(R(ATM(cJAC, i, j, k)));
-      R ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0, cxm = 0, cym = 0, czm = 0;
-      if (Vol > R(0.0)) {
-        ax = R(0.5) * (R(ATM(cJDX, i - 1, j, k)) + R(ATM(cJDX, i, j, k))) / Vol;
-        ay = R(0.5) * (R(ATM(cJDX + 1, i - 1, j, k)) + R(ATM(cJDX + 1, i, j, k))) / Vol;
-        az = R(0.5) * (R(ATM(cJDX + 2, i - 1, j, k)) + R(ATM(cJDX + 2, i, j, k))) / Vol;
-        bx = R(0.5) * (R(ATM(cJDY, i, j - 1, k)) + R(ATM(cJDY, i, j, k))) / Vol;
-        by = R(0.5) * (R(ATM(cJDY + 1, i, j - 1, k)) + R(ATM(cJDY + 1, i, j, k))) / Vol;
-        bz = R(0.5) * (R(ATM(cJDY + 2, i, j - 1, k)) + R(ATM(cJDY + 2, i, j, k))) / Vol;
-        cxm = R(0.5) * (R(ATM(cJDZ, i, j, k - 1)) + R(ATM(cJDZ, i, j, k))) / Vol;
-        cym = R(0.5) * (R(ATM(cJDZ + 1, i, j, k - 1)) + R(ATM(cJDZ + 1, i, j, k))) / Vol;
-        czm = R(0.5) * (R(ATM(cJDZ + 2, i, j, k - 1)) + R(ATM(cJDZ + 2, i, j, k))) / Vol;
-      }
-      const R pip = AT(cPVH + 3, i + 1, j, k) + AT(cPVN + 3, i + 1, j, k);
-      const R pim = AT(cPVH + 3, i - 1, j, k) + AT(cPVN + 3, i - 1, j, k);
-      const R pjp = AT(cPVH + 3, i, j + 1, k) + AT(cPVN + 3, i, j + 1, k);
-      const R pjm = AT(cPVH + 3, i, j - 1, k) + AT(cPVN + 3, i, j - 1, k);
-      const R pkp = AT(cPVH + 3, i, j, k + 1) + AT(cPVN + 3, i, j, k + 1);
-      const R pkm = AT(cPVH + 3, i, j, k - 1) + AT(cPVN + 3, i, j, k - 1);
-      dpex = R(0.5) * (ax * (pip - pim) + bx * (pjp - pjm) + cxm * (pkp - pkm));
-      dpey = R(0.5) * (ay * (pip - pim) + by * (pjp - pjm) + cym * (pkp - pkm));
-      dpez = R(0.5) * (az * (pip - pim) + bz * (pjp - pjm) + czm * (pkp - pkm));
+    if (c.ambipolar) {  // grad p_e term, once per cell (k_face_emf)
+      dpex = AT(cDPE, i, j, k);
+      dpey = AT(cDPE + 1, i, j, k);
+      dpez = AT(cDPE + 2, i, j, k);
     }
     const R x = CV(18), y = CV(19), z = CV(20);
     const R rho_cyl = sqrt(y * y + z * z);
@@ -1174,6 +1173,29 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
+    {
+      // Ambipolar pressure-gradient coefficients of an owned cell
+      // (AddSourceToRHS_Fluid, FluidRHS.cpp:206-527): face JD averaged to the
+      // cell and divided by |Jac| (zero where |Jac| is not positive).
+      const int i = it.i, j = it.j, k = it.k;
+      if (consts_of<R>(S).ambipolar && i < B.n0 && j < B.n1 && k < B.n2) {
+        const R Vol = fabs(R(ATM(cJAC, i, j, k)));
+        R a[9] = {R(0.0), R(0.0), R(0.0), R(0.0), R(0.0), R(0.0), R(0.0), R(0.0), R(0.0)};
+        if (Vol > R(0.0)) {
+          a[0] = R(0.5) * (R(ATM(cJDX, i - 1, j, k)) + R(ATM(cJDX, i, j, k))) / Vol;
+          a[1] = R(0.5) * (R(ATM(cJDX + 1, i - 1, j, k)) + R(ATM(cJDX + 1, i, j, k))) / Vol;
+          a[2] = R(0.5) * (R(ATM(cJDX + 2, i - 1, j, k)) + R(ATM(cJDX + 2, i, j, k))) / Vol;
+          a[3] = R(0.5) * (R(ATM(cJDY, i, j - 1, k)) + R(ATM(cJDY, i, j, k))) / Vol;
+          a[4] = R(0.5) * (R(ATM(cJDY + 1, i, j - 1, k)) + R(ATM(cJDY + 1, i, j, k))) / Vol;
+          a[5] = R(0.5) * (R(ATM(cJDY + 2, i, j - 1, k)) + R(ATM(cJDY + 2, i, j, k))) / Vol;
+          a[6] = R(0.5) * (R(ATM(cJDZ, i, j, k - 1)) + R(ATM(cJDZ, i, j, k))) / Vol;
+          a[7] = R(0.5) * (R(ATM(cJDZ + 1, i, j, k - 1)) + R(ATM(cJDZ + 1, i, j, k))) / Vol;
+          a[8] = R(0.5) * (R(ATM(cJDZ + 2, i, j, k - 1)) + R(ATM(cJDZ + 2, i, j, k))) / Vol;
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) AT(cAMB + q, i, j, k) = a[q];
+      }
+    }
 #pragma unroll 1
     for (int a = 0; a < 3; ++a) {
       const int cm = a == 0 ? cJDX : a == 1 ? cJDY : cJDZ;
