@@ -68,7 +68,7 @@ KERNEL_COMPS = {
     "k_bface": (3 + 3 + 3, 0),                               # B += dt curl E
     "k_bcell_jedge": (3 + 3 + 18 + 3 + 3 + 3 + 3 + 3, 0),    # B, Badd, W_B, beta, alpha -> B_cell, Bind, J edges
     "k_jcell": (3 + 36 + 3, 0),                              # J edges, W_J -> J_cell
-    "k_pv_uplus": (10 + 3 + 12 + 10 + 3 + 3, 10),            # U, B_cell, face normals -> PV, U+, UCON (+ dt); Jac, JD
+    "k_pv_uplus": (10 + 3 + 12 + 10 + 10 + 3 + 3, 1),        # U, B_cell, face normals, UCON coef -> PV, U+, UCON (+ dt); Jac
 }
 ALLOCATED_RANGE_KERNELS = {"k_hall_cell", "k_pv_uplus"}
 

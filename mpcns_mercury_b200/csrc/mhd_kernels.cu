@@ -42,6 +42,7 @@ constexpr int cRW = kComp.first[MHD_RES_W], cRX = kComp.first[MHD_RES_X], cRR = 
               cRP = kComp.first[MHD_RES_P], cRQ = kComp.first[MHD_RES_Q], cRBS = kComp.first[MHD_RES_BSTAR];
 constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA], cFNZ = kComp.first[MHD_FNORM_ZETA];
 constexpr int cPEN = kComp.first[MHD_PE_NODE], cAMB = kComp.first[MHD_AMBI_COEF], cDPE = kComp.first[MHD_DPE];
+constexpr int cUCK = kComp.first[MHD_UCON_COEF];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
 constexpr int cAX = kComp.first[MHD_AREA_XI], cAY = kComp.first[MHD_AREA_ETA], cAZ = kComp.first[MHD_AREA_ZETA];
@@ -1167,12 +1168,36 @@ __global__ void __launch_bounds__(kTileThreads) k_res_bupdate(Dir D) {
 // Static per-face terms of the CFL time step and the Rusanov wave speed, once
 // per solve (run by mhd_prepare): |a| = sqrt(ax ax + ay ay + az az) and
 // a / |a| of the face area vectors JD, the operations and order
-// Compute_Timestep (Timestep.cpp:15-16,78-93) and calc_Jac_radius_GCL (FluidRHS.cpp:5-14)
-// apply to the same static inputs every step.  Owned faces and one more layer.
+// Per-solve static terms, evaluated once at prepare with the reference's
+// expressions: the face normals and |JD| that Compute_Timestep
+// (Timestep.cpp:15-16,78-93) and calc_Jac_radius_GCL (FluidRHS.cpp:5-14) apply
+// every step (owned faces and one more layer), the ambipolar gradient
+// coefficients (owned cells) and the contravariant-velocity coefficients
+// (the cells k_pv_uplus refreshes).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
+    {
+      // Coefficients of the contravariant velocities (calc_Uplus,
+      // Tools.cpp:159-301) on the cells k_pv_uplus refreshes them on: the
+      // face JD of each axis averaged to the cell, and 1 / (|Jac| + 1e-30).
+      const int i = it.i, j = it.j, k = it.k;
+      const int gm = min(consts_of<R>(S).nghost - 1, kStepGhost);
+      if (i >= -gm && i < B.n0 + gm && j >= -gm && j < B.n1 + gm && k >= -gm && k < B.n2 + gm) {
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+          int ip = i, jp = j, kp = k;
+          shift1(axis, ip, jp, kp, 1);
+          const int cm = axis == 0 ? cJDX : axis == 1 ? cJDY : cJDZ;
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+            AT(cUCK + 3 * axis + q, i, j, k) = R(0.5) * (R(ATM(cm + q, i, j, k)) + R(ATM(cm + q, ip, jp, kp)));
+        }
+        AT(cUCK + 9, i, j, k) = R(1.0) / (fabs(R(ATM(cJAC, i, j, k))) + R(1.0e-30));
+      }
+    }
+    if (it.i < 0 || it.j < 0 || it.k < 0 || it.i > B.n0 || it.j > B.n1 || it.k > B.n2) return;  // [0, n + 1) below
     {
       // Ambipolar pressure-gradient coefficients of an owned cell
       // (AddSourceToRHS_Fluid, FluidRHS.cpp:206-527): face JD averaged to the
@@ -1256,14 +1281,12 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
       }
       const int gm = min(c.nghost - 1, kStepGhost);
       if (i >= -gm && i < B.n0 + gm && j >= -gm && j < B.n1 + gm && k >= -gm && k < B.n2 + gm) {
-        const R inv_jac = R(1.0) / (fabs(R(ATM(cJAC, i, j, k))) + R(1.0e-30));
+        // coefficients (cell-averaged JD, 1 / (|Jac| + 1e-30)) from k_face_normals
+        const R inv_jac = AT(cUCK + 9, i, j, k);
+#pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
-          int ip = i, jp = j, kp = k;
-          shift1(axis, ip, jp, kp, 1);
-          const int cm = axis == 0 ? cJDX : axis == 1 ? cJDY : cJDZ;
-          const R kx = R(0.5) * (R(ATM(cm, i, j, k)) + R(ATM(cm, ip, jp, kp)));
-          const R ky = R(0.5) * (R(ATM(cm + 1, i, j, k)) + R(ATM(cm + 1, ip, jp, kp)));
-          const R kz = R(0.5) * (R(ATM(cm + 2, i, j, k)) + R(ATM(cm + 2, ip, jp, kp)));
+          const R kx = AT(cUCK + 3 * axis, i, j, k), ky = AT(cUCK + 3 * axis + 1, i, j, k),
+                  kz = AT(cUCK + 3 * axis + 2, i, j, k);
           AT(cUC + axis, i, j, k) = (kx * up[0] + ky * up[1] + kz * up[2]) * inv_jac;
         }
       }
