@@ -286,19 +286,23 @@ def roofline(prof, cells, peak, peak_kind, precision=0, traffic_key=None):
     algo_bytes = kernel_bytes_per_cell(top, precision) * ncell
     ms = kernels[top]
     achieved = algo_bytes / (ms * 1e-3) / 1e9
-    traffic = load_traffic(traffic_key or top)
+    per_cell = load_traffic(traffic_key) if traffic_key and traffic_key.startswith(top + "_") else None
+    traffic = int(per_cell * sum(a * b * c for a, b, c in cells)) if per_cell else None
     return {"kernel": top, "bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_kind,
             "algo_bytes_per_launch": int(algo_bytes), "launch_ms": round(ms, 5),
-            "traffic": traffic, "share_of_step": round(ms / sum(prof.values()), 4)}
+            "traffic": traffic, "traffic_note": ("ncu DRAM bytes per owned cell of a captured launch (8-solve "
+                                                 "ensemble) x this launch's owned cells") if per_cell else None,
+            "share_of_step": round(ms / sum(prof.values()), 4)}
 
 
-def load_traffic(kernel):
-    """dram bytes per launch of ``kernel`` from the committed ncu summary, if any."""
+def load_traffic(key):
+    """DRAM bytes per owned cell of a kernel from the committed ncu summary
+    (profiles/dram_bytes.json), if any."""
     p = os.path.join(ROOT, "profiles", "dram_bytes.json")
     try:
         with open(p) as f:
-            return json.load(f).get(kernel)
+            return float(json.load(f)[key]["bytes_per_owned_cell"])
     except Exception:
         return None
 
