@@ -62,7 +62,7 @@ KERNEL_COMPS = {
     "k_face_emf": (3 + 3 + 3 + 9 + 2 + 1 + 9 + 3, 0),        # B, Badd, UCON, p x2, grad coef -> Eface, node p_e, grad p_e
     "k_edge_emf": (9 + 3 + 3 + 1 + 2 + 3, 0),                # Eface, UCON, B, node p_e, rho x2 -> E
     "k_hall_cell": (2 + 3 + 3 + 3 + 1, 0),                   # rho x2, J_cell, B_cell -> EHC, beta
-    "k_hall_edge": (3 + 1 + 9 + 3 + 3 + 3 + 3 + 3, 0),       # EHC, beta, dr, dl, Area, B, taper -> Ehall
+    "k_hall_edge": (3 + 1 + 9 + 6 + 3 + 3 + 3, 0),           # EHC, beta, dr, Hall ratios, B, taper -> Ehall
     "k_add_hall": (3 + 3 + 3, 0),                            # E += Ehall
     "k_fluid": (10 + 10 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 10, 10),  # U, PV, |JD|, grad p_e, U+, B_cell, J_cell, Photo, xyz -> U'; Jac, JD
     "k_bface": (3 + 3 + 3, 0),                               # B += dt curl E

@@ -162,6 +162,9 @@ struct mhd_batch {
   int *dprefix_aliasE = nullptr, *dprefix_aliasJ = nullptr;
   cudaGraphExec_t graph = nullptr;
   cudaGraphExec_t graph_a = nullptr, graph_b = nullptr;  // the step split around implicit resistive solves
+  // solves whose pruned-halo (0) / owner (1) table of a group has entries:
+  // sync phases empty in every solve get no launch in the step
+  int live_tables[kMaxGroups][2] = {};
   int n_res = 0;                                        // slots whose solve has the implicit resistive substep
   ResScratch res{nullptr, nullptr};
   double *hres = nullptr;                               // pinned copy of res.result
@@ -222,15 +225,32 @@ void launch(mhd_batch *b, int mode, StepKernel k, int *nk, const SyncOps *ops = 
 SyncOp copy_op(int g, int phase) { return SyncOp{SYNC_COPY, g, phase}; }
 SyncOp alias_op(int which) { return SyncOp{SYNC_ALIAS, which, 0}; }
 
+// A sync operation some solve of the batch has work for (a copy phase whose
+// table is empty in every solve is left out: the depth-0 halos of E, E_Hall
+// and the J edges, and the owner phases of cell fields, which have no alias
+// DOFs).
+bool op_live(const mhd_batch *b, const SyncOp &o) {
+  return o.kind != SYNC_COPY || o.phase == 2 || b->live_tables[o.arg][o.phase] > 0;
+}
+
 // One k_sync launch running one or two independent sync operations.
 void sync1(mhd_batch *b, int mode, SyncOp a, int *nk) {
+  if (!op_live(b, a)) return;
   SyncOps ops{{a, a}, 1};
   launch(b, mode, SK_SYNC, nk, &ops);
 }
 void sync2(mhd_batch *b, int mode, SyncOp a, SyncOp c, int *nk) {
+  if (!op_live(b, a)) return sync1(b, mode, c, nk);
+  if (!op_live(b, c)) return sync1(b, mode, a, nk);
   SyncOps ops{{a, c}, 2};
   launch(b, mode, SK_SYNC, nk, &ops);
 }
+
+// Adds (d = +1) or removes (d = -1) a solve's step tables from the batch's
+// counts; true when a phase that no solve had entries for gains some (the
+// step graphs, which leave that phase out, must be captured anew).
+bool count_tables(mhd_batch *b, const Solve *S, int d);
+void drop_graphs(mhd_batch *b);
 
 // MercuryBoundary::Sync(group) (Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110):
 // the group's halo copies, then its owner copies.  full: every ghost layer
@@ -643,6 +663,27 @@ int build_graph(mhd_batch *b) {
   return capture(b, &b->graph, &b->kernels_per_step, [&](int *nk) { enqueue_step(b, nk); });
 }
 
+bool count_tables(mhd_batch *b, const Solve *S, int d) {
+  bool grew = false;
+  for (int g = 0; g < MHD_NUM_GROUPS; ++g)
+    for (int p = 0; p < 2; ++p)
+      if (S->T->tab_n[g][p] > 0) {
+        grew = grew || (d > 0 && b->live_tables[g][p] == 0);
+        b->live_tables[g][p] += d;
+      }
+  return grew;
+}
+
+// The step graphs are captured again at the next run (call with no graph
+// launch in flight).
+void drop_graphs(mhd_batch *b) {
+  for (cudaGraphExec_t *g : {&b->graph, &b->graph_a, &b->graph_b})
+    if (*g) {
+      cudaGraphExecDestroy(*g);
+      *g = nullptr;
+    }
+}
+
 // Dot product of the CG (2 values) into b->hres.
 int res_dot(mhd_batch *b, int op) {
   int nk = 0;
@@ -950,8 +991,10 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   S->res_max_it = k.res_max_it;
   b->slots[slot] = S;
   if (S->consts.resistive) ++b->n_res;
+  const bool grew = count_tables(b, S, +1);
   if ((rc = publish(b))) return rc;
   CUDA_TRY(cudaStreamSynchronize(st));
+  if (grew) drop_graphs(b);
   *slot_out = slot;
   return MHD_OK;
 }
@@ -1032,6 +1075,10 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   S->res_max_it = constants ? constants->res_max_it : src->res_max_it;
   b->slots[slot] = S;
   if (S->consts.resistive) ++b->n_res;
+  if (count_tables(b, S, +1)) {  // not reached while the template itself is in the batch
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    drop_graphs(b);
+  }
   if ((rc = publish(b))) return rc;
   *slot_out = slot;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
@@ -1043,6 +1090,7 @@ int mhd_batch_remove(mhd_batch *b, int slot) {
   Solve *S = b->slots[slot];
   b->slots[slot] = nullptr;
   if (S->consts.resistive) --b->n_res;
+  count_tables(b, S, -1);
   SolveState s0{};
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return rc;
   if ((rc = publish(b))) return rc;

@@ -43,6 +43,7 @@ constexpr int cRW = kComp.first[MHD_RES_W], cRX = kComp.first[MHD_RES_X], cRR = 
 constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA], cFNZ = kComp.first[MHD_FNORM_ZETA];
 constexpr int cPEN = kComp.first[MHD_PE_NODE], cAMB = kComp.first[MHD_AMBI_COEF], cDPE = kComp.first[MHD_DPE];
 constexpr int cUCK = kComp.first[MHD_UCON_COEF];
+constexpr int cIHX = kComp.first[MHD_HALL_IH_XI], cIHY = kComp.first[MHD_HALL_IH_ETA], cIHZ = kComp.first[MHD_HALL_IH_ZETA];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
 constexpr int cAX = kComp.first[MHD_AREA_XI], cAY = kComp.first[MHD_AREA_ETA], cAZ = kComp.first[MHD_AREA_ZETA];
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(kTileThreads) k_hall_edge(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
-    const R eps = R(1e-14), Cwh = R(0.1);
+    const R Cwh = R(0.1);
     if (i < B.n0) {
       R Ec[3];
       for (int q = 0; q < 3; ++q)
@@ -477,12 +478,8 @@ __global__ void __launch_bounds__(kTileThreads) k_hall_edge(Dir D) {
       const R Ecen = Ec[0] * AT(cDRX, i, j, k) + Ec[1] * AT(cDRX + 1, i, j, k) + Ec[2] * AT(cDRX + 2, i, j, k);
       const R be =
           dmax(dmax(AT(cHB, i, j - 1, k - 1), AT(cHB, i, j - 1, k)), dmax(AT(cHB, i, j, k - 1), AT(cHB, i, j, k)));
-      const R L = dmax(AT(cDLX, i, j, k), eps);
-      const R Abz = R(0.5) * (AT(cAZ, i, j, k) + AT(cAZ, i, j - 1, k));
-      const R ihe = L / dmax(Abz, eps);
+      const R ihe = AT(cIHX, i, j, k), ihz = AT(cIHX + 1, i, j, k);
       const R mue = Cwh * be * ihe * ihe;
-      const R Abe = R(0.5) * (AT(cAY, i, j, k) + AT(cAY, i, j, k - 1));
-      const R ihz = L / dmax(Abe, eps);
       const R muz = Cwh * be * ihz * ihz;
       const R d1 = AT(cBZ, i, j, k) - AT(cBZ, i, j - 1, k);
       const R d2 = AT(cBY, i, j, k) - AT(cBY, i, j, k - 1);
@@ -496,12 +493,8 @@ __global__ void __launch_bounds__(kTileThreads) k_hall_edge(Dir D) {
       const R Ecen = Ec[0] * AT(cDRY, i, j, k) + Ec[1] * AT(cDRY + 1, i, j, k) + Ec[2] * AT(cDRY + 2, i, j, k);
       const R be =
           dmax(dmax(AT(cHB, i - 1, j, k - 1), AT(cHB, i - 1, j, k)), dmax(AT(cHB, i, j, k - 1), AT(cHB, i, j, k)));
-      const R L = dmax(AT(cDLY, i, j, k), eps);
-      const R Abx = R(0.5) * (AT(cAX, i, j, k) + AT(cAX, i, j, k - 1));
-      const R ihz = L / dmax(Abx, eps);
+      const R ihz = AT(cIHY, i, j, k), ihx = AT(cIHY + 1, i, j, k);
       const R muz = Cwh * be * ihz * ihz;
-      const R Abz = R(0.5) * (AT(cAZ, i, j, k) + AT(cAZ, i - 1, j, k));
-      const R ihx = L / dmax(Abz, eps);
       const R mux = Cwh * be * ihx * ihx;
       const R d1 = AT(cBX, i, j, k) - AT(cBX, i, j, k - 1);
       const R d2 = AT(cBZ, i, j, k) - AT(cBZ, i - 1, j, k);
@@ -515,12 +508,8 @@ __global__ void __launch_bounds__(kTileThreads) k_hall_edge(Dir D) {
       const R Ecen = Ec[0] * AT(cDRZ, i, j, k) + Ec[1] * AT(cDRZ + 1, i, j, k) + Ec[2] * AT(cDRZ + 2, i, j, k);
       const R be =
           dmax(dmax(AT(cHB, i - 1, j - 1, k), AT(cHB, i - 1, j, k)), dmax(AT(cHB, i, j - 1, k), AT(cHB, i, j, k)));
-      const R L = dmax(AT(cDLZ, i, j, k), eps);
-      const R Abe = R(0.5) * (AT(cAY, i, j, k) + AT(cAY, i - 1, j, k));
-      const R ihx = L / dmax(Abe, eps);
+      const R ihx = AT(cIHZ, i, j, k), ihe = AT(cIHZ + 1, i, j, k);
       const R mux = Cwh * be * ihx * ihx;
-      const R Abx = R(0.5) * (AT(cAX, i, j, k) + AT(cAX, i, j - 1, k));
-      const R ihe = L / dmax(Abx, eps);
       const R mue = Cwh * be * ihe * ihe;
       const R d1 = AT(cBY, i, j, k) - AT(cBY, i - 1, j, k);
       const R d2 = AT(cBX, i, j, k) - AT(cBX, i, j - 1, k);
@@ -1172,8 +1161,8 @@ __global__ void __launch_bounds__(kTileThreads) k_res_bupdate(Dir D) {
 // expressions: the face normals and |JD| that Compute_Timestep
 // (Timestep.cpp:15-16,78-93) and calc_Jac_radius_GCL (FluidRHS.cpp:5-14) apply
 // every step (owned faces and one more layer), the ambipolar gradient
-// coefficients (owned cells) and the contravariant-velocity coefficients
-// (the cells k_pv_uplus refreshes).
+// coefficients (owned cells), the contravariant-velocity coefficients (the
+// cells k_pv_uplus refreshes) and the Hall diffusion ratios (owned edges).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
   for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
@@ -1198,6 +1187,34 @@ __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
       }
     }
     if (it.i < 0 || it.j < 0 || it.k < 0 || it.i > B.n0 || it.j > B.n1 || it.k > B.n2) return;  // [0, n + 1) below
+    {
+      // Hall diffusion ratios of the owned edges (BuildHallFaceEMF_Rusanov_diff_
+      // step 3, Hall.cpp:148-400): edge length over the face area averaged
+      // to the edge, both floored at 1e-14, per transverse direction.
+      const int i = it.i, j = it.j, k = it.k;
+      const R eps = R(1e-14);
+      if (i < B.n0) {
+        const R L = dmax(AT(cDLX, i, j, k), eps);
+        const R Abz = R(0.5) * (AT(cAZ, i, j, k) + AT(cAZ, i, j - 1, k));
+        const R Abe = R(0.5) * (AT(cAY, i, j, k) + AT(cAY, i, j, k - 1));
+        AT(cIHX, i, j, k) = L / dmax(Abz, eps);
+        AT(cIHX + 1, i, j, k) = L / dmax(Abe, eps);
+      }
+      if (j < B.n1) {
+        const R L = dmax(AT(cDLY, i, j, k), eps);
+        const R Abx = R(0.5) * (AT(cAX, i, j, k) + AT(cAX, i, j, k - 1));
+        const R Abz = R(0.5) * (AT(cAZ, i, j, k) + AT(cAZ, i - 1, j, k));
+        AT(cIHY, i, j, k) = L / dmax(Abx, eps);
+        AT(cIHY + 1, i, j, k) = L / dmax(Abz, eps);
+      }
+      if (k < B.n2) {
+        const R L = dmax(AT(cDLZ, i, j, k), eps);
+        const R Abe = R(0.5) * (AT(cAY, i, j, k) + AT(cAY, i - 1, j, k));
+        const R Abx = R(0.5) * (AT(cAX, i, j, k) + AT(cAX, i, j - 1, k));
+        AT(cIHZ, i, j, k) = L / dmax(Abe, eps);
+        AT(cIHZ + 1, i, j, k) = L / dmax(Abx, eps);
+      }
+    }
     {
       // Ambipolar pressure-gradient coefficients of an owned cell
       // (AddSourceToRHS_Fluid, FluidRHS.cpp:206-527): face JD averaged to the
