@@ -80,10 +80,10 @@ __global__ void k_gather_aos(double *__restrict__ aos, int lo0, int lo1, int lo2
 }
 
 template <class T>
-int dev_upload(const std::vector<T> &h, T **d, cudaStream_t st) {
+int dev_upload(cudaMemPool_t pool, const std::vector<T> &h, T **d, cudaStream_t st) {
   *d = nullptr;
   if (h.empty()) return MHD_OK;
-  CUDA_TRY(cudaMallocAsync((void **)d, sizeof(T) * h.size(), st));
+  CUDA_TRY(cudaMallocFromPoolAsync((void **)d, sizeof(T) * h.size(), pool, st));
   CUDA_TRY(cudaMemcpyAsync(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st));
   return MHD_OK;
 }
@@ -109,6 +109,7 @@ struct Tables {
 
 struct Solve {
   int nblocks = 0, nghost = 0, es = 8;  // es: bytes per real
+  cudaMemPool_t pool = nullptr;         // the batch's device memory pool
   bool prepared = false;
   std::vector<Box> boxes;
   std::vector<int64_t> ubase, mbase;  // bytes
@@ -153,6 +154,10 @@ struct mhd_batch {
   int capacity = 0;
   int precision = kFP64;
   cudaStream_t stream = nullptr;
+  // Device memory of solves, tables and staging: the batch's own pool, which
+  // keeps freed memory for the next solve instead of returning it to the
+  // driver at every synchronisation (admitting a solve then maps no memory).
+  cudaMemPool_t pool = nullptr;
   std::vector<Solve *> slots;
   // device directory (fixed addresses for the lifetime of the batch)
   DevSolve *dsolves = nullptr;
@@ -314,7 +319,7 @@ int ensure_staging(mhd_batch *b, size_t elems) {  // elems doubles
   if (b->staging) cudaFreeAsync(b->staging, b->stream);
   b->staging = nullptr;
   b->staging_elems = 0;
-  if (cudaMallocAsync((void **)&b->staging, sizeof(double) * elems, b->stream) != cudaSuccess)
+  if (cudaMallocFromPoolAsync((void **)&b->staging, sizeof(double) * elems, b->pool, b->stream) != cudaSuccess)
     return fail(MHD_ERR_OOM, "staging of %zu doubles", elems);
   b->staging_elems = elems;
   return MHD_OK;
@@ -551,7 +556,7 @@ int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
     const int g = q / 3, phase = q % 3;
     S->T->tab_n[g][phase] = (int)(seg[q].size() / kSegWords);
     S->T->table_bytes += (int64_t)seg[q].size() * 8;
-    const int rc = dev_upload(seg[q], &S->T->tab_seg[g][phase], st);
+    const int rc = dev_upload(S->pool, seg[q], &S->T->tab_seg[g][phase], st);
     if (rc) return rc;
   }
   return MHD_OK;
@@ -586,10 +591,10 @@ int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
   std::vector<double> ms(a.member_sign, a.member_sign + nm), os(a.owner_sign, a.owner_sign + a.n_classes);
   S->T->table_bytes += (int64_t)nm * 24 + (int64_t)a.n_classes * 28;
   int rc;
-  if ((rc = dev_upload(off, &S->T->al_off, st)) || (rc = dev_upload(mE, &S->T->al_memE, st)) ||
-      (rc = dev_upload(mJ, &S->T->al_memJ, st)) || (rc = dev_upload(oE, &S->T->al_ownE, st)) ||
-      (rc = dev_upload(oJ, &S->T->al_ownJ, st)) || (rc = dev_upload(ms, &S->T->al_msign, st)) ||
-      (rc = dev_upload(os, &S->T->al_osign, st)))
+  if ((rc = dev_upload(S->pool, off, &S->T->al_off, st)) || (rc = dev_upload(S->pool, mE, &S->T->al_memE, st)) ||
+      (rc = dev_upload(S->pool, mJ, &S->T->al_memJ, st)) || (rc = dev_upload(S->pool, oE, &S->T->al_ownE, st)) ||
+      (rc = dev_upload(S->pool, oJ, &S->T->al_ownJ, st)) || (rc = dev_upload(S->pool, ms, &S->T->al_msign, st)) ||
+      (rc = dev_upload(S->pool, os, &S->T->al_osign, st)))
     return rc;
   return MHD_OK;
 }
@@ -809,6 +814,20 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
   };
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(MHD_ERR_CUDA, "stream create"));
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    uint64_t keep = UINT64_MAX;
+    if (cudaMemPoolCreate(&b->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+      b->pool = nullptr;
+      return bail(fail(MHD_ERR_CUDA, "memory pool create"));
+    }
+  }
   const size_t C1 = (size_t)capacity + 1;
   if (cudaMalloc(&b->dsolves, sizeof(DevSolve) * capacity) != cudaSuccess ||
       cudaMalloc(&b->dstate, sizeof(SolveState) * capacity) != cudaSuccess ||
@@ -867,6 +886,7 @@ int mhd_batch_destroy(mhd_batch *b) {
   cudaFree(b->dprefix_aliasJ);
   for (auto e : b->prof_events) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->pool) cudaMemPoolDestroy(b->pool);  // every allocation from it was freed and the stream drained
   delete b;
   return MHD_OK;
 }
@@ -907,6 +927,7 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   if (slot < 0) return fail(MHD_ERR_OOM, "mhd_batch_add: all %d slots in use", b->capacity);
   auto *S = new (std::nothrow) Solve();
   if (!S) return fail(MHD_ERR_OOM, "host allocation");
+  S->pool = b->pool;
   S->T = new (std::nothrow) Tables();
   if (!S->T) {
     delete S;
@@ -952,7 +973,7 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
                      k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
                      k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
                      k.ambipolar,     k.local_arti, desc->nghost, k.resistive};
-  if (cudaMallocAsync((void **)&S->arena, S->arena_bytes, st) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync((void **)&S->arena, S->arena_bytes, b->pool, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
   }
@@ -973,10 +994,10 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
     d.solve = slot;
   }
   int rc;
-  if ((rc = dev_upload(blocks, &S->dblocks, st))) return bail(rc);
+  if ((rc = dev_upload(S->pool, blocks, &S->dblocks, st))) return bail(rc);
   for (int r = 0; r < kNumRanges; ++r) {
     S->T->tiles[r] = prefix[r].back();
-    if ((rc = dev_upload(prefix[r], &S->T->dtile_prefix[r], st))) return bail(rc);
+    if ((rc = dev_upload(S->pool, prefix[r], &S->T->dtile_prefix[r], st))) return bail(rc);
   }
   try {
     if ((rc = upload_groups(S, desc->groups, st))) return bail(rc);
@@ -1017,6 +1038,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   const Solve *src = b->slots[src_slot];
   auto *S = new (std::nothrow) Solve();
   if (!S) return fail(MHD_ERR_OOM, "host allocation");
+  S->pool = b->pool;
   cudaStream_t st = b->stream;
   S->nblocks = src->nblocks;
   S->nghost = src->nghost;
@@ -1044,7 +1066,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
     free_solve(S, st);
     return code;
   };
-  if (cudaMallocAsync((void **)&S->arena, S->arena_bytes, st) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync((void **)&S->arena, S->arena_bytes, b->pool, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
   }
@@ -1067,7 +1089,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
     for (int a = 0; a < 3; ++a) d.n[a] = bx.n[a];
     d.solve = slot;
   }
-  if ((rc = dev_upload(blocks, &S->dblocks, st))) return bail(rc);
+  if ((rc = dev_upload(S->pool, blocks, &S->dblocks, st))) return bail(rc);
   SolveState s0{};
   s0.dt_bits = kDtUnset;
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
