@@ -61,16 +61,15 @@ L2_BYTES = 126 * 1024 * 1024
 KERNEL_COMPS = {
     "k_face_emf": (3 + 3 + 3 + 9 + 2 + 1 + 9 + 3, 0),        # B, Badd, UCON, p x2, grad coef -> Eface, node p_e, grad p_e
     "k_edge_emf": (9 + 3 + 3 + 1 + 2 + 3, 0),                # Eface, UCON, B, node p_e, rho x2 -> E
-    "k_hall_cell": (2 + 3 + 3 + 3 + 1, 0),                   # rho x2, J_cell, B_cell -> EHC, beta
     "k_hall_edge": (3 + 1 + 9 + 6 + 3 + 3 + 3, 0),           # EHC, beta, dr, Hall ratios, B, taper -> Ehall
     "k_add_hall": (3 + 3 + 3, 0),                            # E += Ehall
     "k_fluid": (10 + 10 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 10, 10),  # U, PV, |JD|, grad p_e, U+, B_cell, J_cell, Photo, xyz -> U'; Jac, JD
     "k_bface": (3 + 3 + 3, 0),                               # B += dt curl E
     "k_bcell_jedge": (3 + 3 + 18 + 3 + 3 + 3 + 3 + 3, 0),    # B, Badd, W_B, beta, alpha -> B_cell, Bind, J edges
     "k_jcell": (3 + 36 + 3, 0),                              # J edges, W_J -> J_cell
-    "k_pv_uplus": (10 + 3 + 12 + 10 + 10 + 3 + 3, 1),        # U, B_cell, face normals, UCON coef -> PV, U+, UCON (+ dt); Jac
+    "k_pv_uplus": (10 + 3 + 3 + 12 + 10 + 10 + 3 + 3 + 3 + 1, 1),  # U, B_cell, J_cell, face normals, UCON coef -> PV, U+, UCON, Hall EHC, beta (+ dt); Jac
 }
-ALLOCATED_RANGE_KERNELS = {"k_hall_cell", "k_pv_uplus"}
+ALLOCATED_RANGE_KERNELS = {"k_pv_uplus"}
 
 
 def kernel_bytes_per_cell(name, precision):

@@ -289,7 +289,6 @@ void enqueue_step_a(mhd_batch *b, int *nk) {
   // the E alias reduction (ideal EMF) and Sync(Ehall) touch different fields
   launch(b, m, SK_FACE_EMF, nk);
   launch(b, m, SK_EDGE_EMF, nk);
-  launch(b, m, SK_HALL_CELL, nk);
   launch(b, m, SK_HALL_EDGE, nk);
   sync2(b, m, alias_op(0), copy_op(MHD_SYNC_EHALL, 0), nk);
   sync1(b, m, copy_op(MHD_SYNC_EHALL, 1), nk);

@@ -445,24 +445,6 @@ __global__ void __launch_bounds__(kTileThreads) k_edge_emf(Dir D) {
 }
 
 // ------------------------------------------------------------------ Hall EMF
-// BuildHallFaceEMF_Rusanov_diff_ step 1 (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:110-146).
-template <class R>
-__global__ void __launch_bounds__(kTileThreads) k_hall_cell(Dir D) {
-  for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
-    if (!it.in) return;
-    const int i = it.i, j = it.j, k = it.k;
-    const int o = B.off(i, j, k);
-    const Num<R> d = num_limiter(consts_of<R>(S), B.c(cUH)[o], B.c(cUN)[o]);
-    const R alpha = consts_of<R>(S).hall_coef / d.ne_eff;
-    const R Jx = B.c(cJC)[o], Jy = B.c(cJC + 1)[o], Jz = B.c(cJC + 2)[o];
-    const R Bx = B.c(cBC)[o], By = B.c(cBC + 1)[o], Bz = B.c(cBC + 2)[o];
-    B.c(cEHC)[o] = alpha * (Jy * Bz - Jz * By);
-    B.c(cEHC + 1)[o] = alpha * (Jz * Bx - Jx * Bz);
-    B.c(cEHC + 2)[o] = alpha * (Jx * By - Jy * Bx);
-    B.c(cHB)[o] = fabs(alpha) * sqrt(Bx * Bx + By * By + Bz * Bz);
-  });
-}
-
 // BuildHallFaceEMF_Rusanov_diff_ steps 2-4 (Hall.cpp:148-400).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_hall_edge(Dir D) {
@@ -1254,8 +1236,8 @@ __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
 }
 
 // calc_PV + calc_Uplus (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:159-301) on the allocated
-// cell range the step keeps, the contravariant velocities UCON there, and
-// the next step's CFL dt on owned cells (warp min, one atomicMin per warp on
+// cell range the step keeps, the contravariant velocities UCON and the next
+// step's Hall cell field there, and the next step's CFL dt on owned cells (warp min, one atomicMin per warp on
 // the bit pattern of the positive double).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir D) {
@@ -1289,6 +1271,19 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
       }
       const R rH = dmax(AT(cUH, i, j, k), R(0.0)), rN = dmax(AT(cUN, i, j, k), R(0.0));
       const Num<R> d = num_limiter(c, rH, rN);
+      {
+        // the next step's Hall cell field, BuildHallFaceEMF_Rusanov_diff_ step 1
+        // (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:110-146): its inputs (J_cell,
+        // B_cell, the densities) are final here (num_limiter clamps the
+        // densities at zero itself, so d is the limiter of the raw densities)
+        const R alpha = c.hall_coef / d.ne_eff;
+        const R Jx = AT(cJC, i, j, k), Jy = AT(cJC + 1, i, j, k), Jz = AT(cJC + 2, i, j, k);
+        const R Bx = AT(cBC, i, j, k), By = AT(cBC + 1, i, j, k), Bz = AT(cBC + 2, i, j, k);
+        AT(cEHC, i, j, k) = alpha * (Jy * Bz - Jz * By);
+        AT(cEHC + 1, i, j, k) = alpha * (Jz * Bx - Jx * Bz);
+        AT(cEHC + 2, i, j, k) = alpha * (Jx * By - Jy * Bx);
+        AT(cHB, i, j, k) = fabs(alpha) * sqrt(Bx * Bx + By * By + Bz * Bz);
+      }
       R up[3];
       for (int q = 0; q < 3; ++q) {
         const R uH = rH > R(1e-20) ? vel[0][q] : R(0.0);
@@ -1443,7 +1438,6 @@ static const void *kernel_fn(StepKernel k) {
   switch (k) {
     case SK_FACE_EMF: return (const void *)k_face_emf<R>;
     case SK_EDGE_EMF: return (const void *)k_edge_emf<R>;
-    case SK_HALL_CELL: return (const void *)k_hall_cell<R>;
     case SK_HALL_EDGE: return (const void *)k_hall_edge<R>;
     case SK_ADD_HALL: return (const void *)k_add_hall<R>;
     case SK_FLUID: return (const void *)k_fluid<R>;
@@ -1498,7 +1492,6 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
   switch (k) {
     case SK_FACE_EMF: k_face_emf<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_EDGE_EMF: k_edge_emf<R><<<G, kTileThreads, 0, st>>>(D); break;
-    case SK_HALL_CELL: k_hall_cell<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_HALL_EDGE: k_hall_edge<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_ADD_HALL: k_add_hall<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_FLUID: k_fluid<R><<<G, kTileThreads, 0, st>>>(D); break;
@@ -1564,7 +1557,7 @@ int res_dot_grid() {
 }
 
 const char *step_kernel_name(StepKernel k) {
-  static const char *names[] = {"k_face_emf", "k_edge_emf", "k_hall_cell", "k_hall_edge", "k_add_hall",
+  static const char *names[] = {"k_face_emf", "k_edge_emf", "k_hall_edge", "k_add_hall",
                                 "k_fluid",    "k_bface",    "k_bcell_jedge", "k_jcell",   "k_pv_uplus",
                                 "k_sync",     "k_flip",     "k_retire",      "k_face_normals", "k_div_b",
                                 "k_res_seed", "k_res_w",    "k_res_vec",     "k_res_db",   "k_res_dj",

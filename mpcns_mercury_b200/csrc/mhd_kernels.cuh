@@ -7,7 +7,7 @@
 namespace mhd {
 
 enum StepKernel {
-  SK_FACE_EMF = 0, SK_EDGE_EMF, SK_HALL_CELL, SK_HALL_EDGE, SK_ADD_HALL, SK_FLUID, SK_BFACE, SK_BCELL_JEDGE,
+  SK_FACE_EMF = 0, SK_EDGE_EMF, SK_HALL_EDGE, SK_ADD_HALL, SK_FLUID, SK_BFACE, SK_BCELL_JEDGE,
   SK_JCELL, SK_PV_UPLUS, SK_SYNC, SK_FLIP, SK_RETIRE, SK_FACE_NORMALS, SK_DIVB,
   // implicit resistive substep
   SK_RES_SEED, SK_RES_W, SK_RES_VEC, SK_RES_DB, SK_RES_DJ, SK_RES_Q, SK_RES_DOT, SK_RES_SUM, SK_RES_COPYB,

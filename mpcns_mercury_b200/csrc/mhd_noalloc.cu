@@ -13,8 +13,8 @@
 // range, lives in a file-scope __device__ array of fixed size instead of
 // being allocated.
 //
-// The arithmetic is the same as the context path (k_hall_cell / k_hall_edge
-// in mhd_kernels.cu, i.e. BuildHallFaceEMF_Rusanov_diff_ of the reference,
+// The arithmetic is the same as the context path (the Hall cell field of
+// k_pv_uplus and k_hall_edge in mhd_kernels.cu, i.e. BuildHallFaceEMF_Rusanov_diff_ of the reference,
 // Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:58-400), in the
 // same operation order, so the two agree bitwise on the edges both write.
 #include <cuda_runtime.h>
