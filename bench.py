@@ -63,7 +63,7 @@ KERNEL_COMPS = {
     "k_edge_emf": (9 + 3 + 3 + 1 + 2 + 3, 0),                # Eface, UCON, B, node p_e, rho x2 -> E
     "k_hall_edge": (3 + 1 + 9 + 6 + 3 + 3 + 3, 0),           # EHC, beta, dr, Hall ratios, B, taper -> Ehall
     "k_add_hall": (3 + 3 + 3, 0),                            # E += Ehall
-    "k_fluid": (10 + 10 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 10, 10),  # U, PV, |JD|, grad p_e, U+, B_cell, J_cell, Photo, xyz -> U'; Jac, JD
+    "k_fluid": (10 + 10 + 3 + 10 + 3 + 3 + 3 + 3 + 1 + 3 + 10, 0),  # U, PV, |JD|, JD + 1/Jac, grad p_e, U+, B_cell, J_cell, Photo, xyz -> U'
     "k_bface": (3 + 3 + 3, 0),                               # B += dt curl E
     "k_bcell_jedge": (3 + 3 + 18 + 3 + 3 + 3 + 3 + 3, 0),    # B, Badd, W_B, beta, alpha -> B_cell, Bind, J edges
     "k_jcell": (3 + 36 + 3, 0),                              # J edges, W_J -> J_cell

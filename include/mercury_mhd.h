@@ -65,6 +65,7 @@ enum mhd_field {
   MHD_DPE,                                    /* grad p_e term of the ion momentum sources per cell (ambipolar) */
   MHD_UCON_COEF,                              /* cell-averaged JD (3 x 3) and 1 / (|Jac| + 1e-30) of UCON, set by mhd_prepare */
   MHD_HALL_IH_XI, MHD_HALL_IH_ETA, MHD_HALL_IH_ZETA, /* Hall diffusion length / area ratios (2 per edge), set by mhd_prepare */
+  MHD_FLUX_METRIC,                            /* JD of the xi, eta, zeta faces (3 x 3) and 1 / Jac in the step's real type, set by mhd_prepare */
   /* static geometry and sources (uploaded once) */
   MHD_JAC, MHD_JDXI, MHD_JDET, MHD_JDZE, MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA,
   MHD_DL_XI, MHD_DL_ETA, MHD_DL_ZETA, MHD_DR_XI, MHD_DR_ETA, MHD_DR_ZETA,

@@ -21,7 +21,7 @@ FIELDS = [
     "PV_H", "PV_NA", "U_PLUS", "B_CELL", "BIND_CELL", "J_CELL", "J_XI", "J_ETA", "J_ZETA",
     "E_XI", "E_ETA", "E_ZETA", "EHALL_XI", "EHALL_ETA", "EHALL_ZETA",
     "EFACE_XI", "EFACE_ETA", "EFACE_ZETA", "EHC", "HALL_BETA", "UCON", "DIVB", "FNORM_XI", "FNORM_ETA", "FNORM_ZETA", "PE_NODE", "AMBI_COEF",
-    "DPE", "UCON_COEF", "HALL_IH_XI", "HALL_IH_ETA", "HALL_IH_ZETA",
+    "DPE", "UCON_COEF", "HALL_IH_XI", "HALL_IH_ETA", "HALL_IH_ZETA", "FLUX_METRIC",
     "JAC", "JDXI", "JDET", "JDZE", "AREA_XI", "AREA_ETA", "AREA_ZETA",
     "DL_XI", "DL_ETA", "DL_ZETA", "DR_XI", "DR_ETA", "DR_ZETA",
     "HODGE_FACE_XI", "HODGE_FACE_ETA", "HODGE_FACE_ZETA",

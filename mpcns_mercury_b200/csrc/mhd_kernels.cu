@@ -44,6 +44,7 @@ constexpr int cFNX = kComp.first[MHD_FNORM_XI], cFNY = kComp.first[MHD_FNORM_ETA
 constexpr int cPEN = kComp.first[MHD_PE_NODE], cAMB = kComp.first[MHD_AMBI_COEF], cDPE = kComp.first[MHD_DPE];
 constexpr int cUCK = kComp.first[MHD_UCON_COEF];
 constexpr int cIHX = kComp.first[MHD_HALL_IH_XI], cIHY = kComp.first[MHD_HALL_IH_ETA], cIHZ = kComp.first[MHD_HALL_IH_ZETA];
+constexpr int cFM = kComp.first[MHD_FLUX_METRIC];
 constexpr int cJAC = kComp.first[MHD_JAC], cJDX = kComp.first[MHD_JDXI], cJDY = kComp.first[MHD_JDET],
               cJDZ = kComp.first[MHD_JDZE];
 constexpr int cAX = kComp.first[MHD_AREA_XI], cAY = kComp.first[MHD_AREA_ETA], cAZ = kComp.first[MHD_AREA_ZETA];
@@ -594,12 +595,18 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
       if constexpr (sizeof(R) == 4) return cvals[q];
       else return cen(q);
     };
-    // 1/J of this cell, once (the same value every direction divides by)
-    const R invJ = (it.in && dt_ok) ? R(1.0) / R(ATM(cJAC, i, j, k)) : R(0.0);
+    // 1/J of this cell (the same value every direction divides by)
+    R invJ = R(0.0);
+    if (it.in && dt_ok) {
+      if constexpr (sizeof(R) == 4) invJ = AT(cFM + 9, i, j, k);  // R(1) / R(Jac), from k_face_normals
+      else invJ = R(1.0) / R(ATM(cJAC, i, j, k));
+    }
     // one pass per direction (unrolled: the face grid's extents are constants)
     auto face_pass = [&](auto dirc) {
       constexpr int dir = decltype(dirc)::value;
-      constexpr int cm = dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
+      // the face's JD: FP32 reads the real-typed copy (k_face_normals), FP64
+      // the metric itself (the same values; faster there)
+      constexpr int cm = sizeof(R) == 4 ? cFM + 3 * dir : dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
       constexpr int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
       constexpr int ei = kTileI + (dir == 0), ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
       constexpr int nf = ei * ej * ek;
@@ -614,8 +621,17 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
           int im = x[0], jm = x[1], km = x[2];
           shift1(dir, im, jm, km, -1);
           R Fl[5];
-          rusanov(B, g, u0, pv0, R(ATM(cm, x[0], x[1], x[2])), R(ATM(cm + 1, x[0], x[1], x[2])),
-                  R(ATM(cm + 2, x[0], x[1], x[2])), AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
+          R k1, k2, k3;
+          if constexpr (sizeof(R) == 4) {
+            k1 = AT(cm, x[0], x[1], x[2]);
+            k2 = AT(cm + 1, x[0], x[1], x[2]);
+            k3 = AT(cm + 2, x[0], x[1], x[2]);
+          } else {
+            k1 = ATM(cm, x[0], x[1], x[2]);
+            k2 = ATM(cm + 1, x[0], x[1], x[2]);
+            k3 = ATM(cm + 2, x[0], x[1], x[2]);
+          }
+          rusanov(B, g, u0, pv0, k1, k2, k3, AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
 #pragma unroll
           for (int m = 0; m < 5; ++m) F[m][f] = Fl[m];
         }
@@ -1144,7 +1160,8 @@ __global__ void __launch_bounds__(kTileThreads) k_res_bupdate(Dir D) {
 // (Timestep.cpp:15-16,78-93) and calc_Jac_radius_GCL (FluidRHS.cpp:5-14) apply
 // every step (owned faces and one more layer), the ambipolar gradient
 // coefficients (owned cells), the contravariant-velocity coefficients (the
-// cells k_pv_uplus refreshes) and the Hall diffusion ratios (owned edges).
+// cells k_pv_uplus refreshes), the Hall diffusion ratios (owned edges) and
+// the fluid fluxes' face JD and 1 / Jac in the real type.
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
   for_items<R, kAlloc>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
@@ -1169,6 +1186,18 @@ __global__ void __launch_bounds__(kTileThreads) k_face_normals(Dir D) {
       }
     }
     if (it.i < 0 || it.j < 0 || it.k < 0 || it.i > B.n0 || it.j > B.n1 || it.k > B.n2) return;  // [0, n + 1) below
+    {
+      // the face JD the fluid fluxes read and the cell's 1 / Jac, converted
+      // to the real type once (the values the fluid kernel would form)
+      const int i = it.i, j = it.j, k = it.k;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        AT(cFM + q, i, j, k) = R(ATM(cJDX + q, i, j, k));
+        AT(cFM + 3 + q, i, j, k) = R(ATM(cJDY + q, i, j, k));
+        AT(cFM + 6 + q, i, j, k) = R(ATM(cJDZ + q, i, j, k));
+      }
+      AT(cFM + 9, i, j, k) = R(1.0) / R(ATM(cJAC, i, j, k));
+    }
     {
       // Hall diffusion ratios of the owned edges (BuildHallFaceEMF_Rusanov_diff_
       // step 3, Hall.cpp:148-400): edge length over the face area averaged

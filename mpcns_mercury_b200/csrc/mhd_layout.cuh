@@ -40,7 +40,7 @@ constexpr FieldSpec kFieldSpec[MHD_NUM_FIELDS] = {
     {3, MHD_CELL} /* UCON */, {1, MHD_CELL} /* DIVB */,
     {4, MHD_FACE_XI},   {4, MHD_FACE_ETA},  {4, MHD_FACE_ZETA} /* FNORM */, {1, MHD_NODE} /* PE_NODE */, {9, MHD_CELL} /* AMBI_COEF */,
     {3, MHD_CELL} /* DPE */, {10, MHD_CELL} /* UCON_COEF */,
-    {2, MHD_EDGE_XI},   {2, MHD_EDGE_ETA},  {2, MHD_EDGE_ZETA} /* HALL_IH */,
+    {2, MHD_EDGE_XI},   {2, MHD_EDGE_ETA},  {2, MHD_EDGE_ZETA} /* HALL_IH */, {10, MHD_CELL} /* FLUX_METRIC */,
     {1, MHD_CELL},      {3, MHD_FACE_XI},   {3, MHD_FACE_ETA},  {3, MHD_FACE_ZETA}, {1, MHD_FACE_XI},
     {1, MHD_FACE_ETA},  {1, MHD_FACE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA},
     {3, MHD_EDGE_XI},   {3, MHD_EDGE_ETA},  {3, MHD_EDGE_ZETA}, {1, MHD_FACE_XI},   {1, MHD_FACE_ETA},
