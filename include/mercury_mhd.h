@@ -288,6 +288,12 @@ int mhd_hall_emf_static_scratch(const mhd_hall_block *in, double *out_xi, double
  * doubles; mhd_batch_device_view returns a float array for float fields. */
 int mhd_batch_create(int capacity, int precision, mhd_batch **out);
 int mhd_batch_destroy(mhd_batch *batch);
+/* Grows the batch's device memory pool by `bytes` ahead of the solves that
+ * will use it (the pool keeps memory that solves free, and memory reserved
+ * here, until mhd_batch_destroy): solves added later take their arenas and
+ * tables from it without mapping new memory.  No reference counterpart (its
+ * solver allocates at setup).  Synchronous. */
+int mhd_batch_reserve(mhd_batch *batch, int64_t bytes);
 /* Device bytes a solve of this descriptor occupies (arena and tables); -1 on
  * a bad descriptor.  Lets a server admit requests against free HBM. */
 int64_t mhd_desc_device_bytes(const mhd_desc *desc);

@@ -109,7 +109,7 @@ EXPORTS = [
     "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
-    "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy",
+    "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
@@ -162,6 +162,7 @@ def lib() -> ctypes.CDLL:
     L.mhd_div_b.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
     L.mhd_batch_div_b.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.mhd_batch_destroy.argtypes = [P]
+    L.mhd_batch_reserve.argtypes = [P, ctypes.c_int64]
     L.mhd_desc_device_bytes.argtypes = [ctypes.POINTER(MhdDesc)]
     L.mhd_desc_device_bytes.restype = ctypes.c_int64
     L.mhd_batch_add.argtypes = [P, ctypes.POINTER(MhdDesc), ctypes.POINTER(ctypes.c_int)]
@@ -388,6 +389,10 @@ class Batch:
 
     def kernels_per_step(self) -> int:
         return lib().mhd_batch_kernels_per_step(self.b)
+
+    def reserve(self, nbytes: int):
+        """Grow the batch's device memory pool ahead of the solves (mhd_batch_reserve)."""
+        check(lib().mhd_batch_reserve(self.b, int(nbytes)), "mhd_batch_reserve")
 
     def close(self):
         if getattr(self, "b", None):

@@ -18,6 +18,8 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include "mercury_mhd.h"
@@ -466,14 +468,29 @@ std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth) {
     runs.push_back(Run{e.dst[t], e.src[t], 1, (bool)e.neg[t]});
   }
   // runs of one (len, sign, src - dst) class, each class in destination order
-  std::vector<int> ro(runs.size());
-  for (size_t q = 0; q < runs.size(); ++q) ro[q] = (int)q;
-  std::stable_sort(ro.begin(), ro.end(), [&](int a, int c) {
-    const Run &x = runs[a], &y = runs[c];
-    if (x.len != y.len) return x.len < y.len;
-    if (x.neg != y.neg) return x.neg < y.neg;
-    return x.src - x.dst < y.src - y.dst;
-  });
+  // (classes are few: a hash of the key buckets the runs in one pass)
+  std::vector<int> ro;
+  ro.reserve(runs.size());
+  {
+    struct KeyHash {
+      size_t operator()(const std::pair<int64_t, int> &k) const {
+        return std::hash<int64_t>()(k.first) ^ (std::hash<int>()(k.second) * 0x9e3779b97f4a7c15ull);
+      }
+    };
+    std::unordered_map<std::pair<int64_t, int>, int, KeyHash> cls;  // key -> class index
+    std::vector<std::vector<int>> members;
+    for (size_t q = 0; q < runs.size(); ++q) {
+      const Run &r = runs[q];
+      const std::pair<int64_t, int> key(r.src - r.dst, r.len * 2 + (r.neg ? 1 : 0));
+      auto it = cls.find(key);
+      if (it == cls.end()) {
+        it = cls.emplace(key, (int)members.size()).first;
+        members.emplace_back();
+      }
+      members[it->second].push_back((int)q);
+    }
+    for (auto &m : members) ro.insert(ro.end(), m.begin(), m.end());
+  }
   std::vector<int64_t> seg;
   seg.reserve(kSegWords * runs.size());
   for (size_t u = 0; u < ro.size();) {
@@ -887,6 +904,19 @@ int mhd_batch_destroy(mhd_batch *b) {
   if (b->stream) cudaStreamDestroy(b->stream);
   if (b->pool) cudaMemPoolDestroy(b->pool);  // every allocation from it was freed and the stream drained
   delete b;
+  return MHD_OK;
+}
+
+int mhd_batch_reserve(mhd_batch *b, int64_t bytes) {
+  if (!b || bytes < 0) return fail(MHD_ERR_ARG, "mhd_batch_reserve: bad arguments");
+  if (bytes == 0) return MHD_OK;
+  void *p = nullptr;
+  if (cudaMallocFromPoolAsync(&p, (size_t)bytes, b->pool, b->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MHD_ERR_OOM, "mhd_batch_reserve: %lld bytes", (long long)bytes);
+  }
+  CUDA_TRY(cudaFreeAsync(p, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
   return MHD_OK;
 }
 
