@@ -123,3 +123,37 @@ def test_batch_request_before_prepare_is_refused(cases):
     with pytest.raises(MhdError):
         b.add(d)  # capacity 1 is full
     b.close()
+
+
+def test_reserved_pool_equals_single(cases):
+    """Solves added after mhd_batch_reserve take their memory from the grown
+    pool; a solve removed and another added in its place reuse it.  Results
+    stay bitwise equal to the single-solve path."""
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.capi import Batch, MhdError, SolveDesc
+
+    ref = {sid: _single(cases[sid], SIZES[sid], 3) for sid in (0, 3)}
+    b = Batch(2)
+    need = 0
+    for sid in (0, 3):
+        d = SolveDesc([SIZES[sid]], W.NGHOST, reference_constants(cfl=0.4))
+        need += d.device_bytes()
+        d.close()
+    b.reserve(need)
+    with pytest.raises(MhdError):
+        b.reserve(-1)
+    slot, d = _add(b, cases[3], SIZES[3])
+    b.request(slot, 1)
+    b.run(1)
+    b.remove(slot)  # its memory goes back to the pool
+    d.close()
+    for sid in (0, 3):
+        slot, d = _add(b, cases[sid], SIZES[sid])
+        b.request(slot, 3)
+        b.run(3)
+        assert b.poll()[slot].step == 3
+        assert _same(_state(b, slot, cases[sid]), ref[sid][0])
+        b.remove(slot)
+        d.close()
+    b.close()
