@@ -352,6 +352,46 @@ int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghost, mhd_topo
 int mhd_topology_fill_desc(const mhd_topology *topo, mhd_desc *desc);
 int mhd_topology_destroy(mhd_topology *topo);
 
+/* ---- Restart files ----
+ * The reference's checkpoint format, MPCNSRST version 1
+ * (IOModule::WriteRestartBinFile / ReadRestartBinFile,
+ * src/6_io/IOModule_Bin.cpp:168-420), with the fields its Mercury solver
+ * checkpoints: U_H, U_Na, B_xi, B_eta, B_zeta
+ * (Z4_Mercury/src/MercurySolver.cpp:33-35).  Files written here resume in the
+ * reference and the reference's files resume here. */
+#define MHD_RESTART_FIELDS 5 /* U_H, U_Na, B_xi, B_eta, B_zeta, in this order */
+typedef struct mhd_restart_image {
+  int32_t step;          /* steps taken */
+  double time;           /* physical time */
+  int32_t n_blocks;
+  const int32_t *cells;  /* 3 per block */
+  int32_t nghost;
+  /* per state field: the blocks' arrays one after another, each over the
+   * FieldBlock range [-nghost, n + stagger + nghost) in (i, j, k, comp)
+   * order (mhd_restart_values doubles in all) */
+  double *data[MHD_RESTART_FIELDS];
+  uint32_t loaded;       /* mhd_restart_read: bit f set when the file held field f */
+} mhd_restart_image;
+/* Doubles of state field `state_field` over all blocks; -1 on bad arguments. */
+int64_t mhd_restart_values(const mhd_restart_image *img, int32_t state_field);
+/* Host-only file I/O of an image.  The reader checks the header, block count,
+ * and for the state fields their location, components, nghost and ranges
+ * against img (cells, nghost) as the reference's reader does; fields it does
+ * not restore are skipped; fields missing from the file are left as they
+ * are (see `loaded`).  No device work. */
+int mhd_restart_write(const char *path, const mhd_restart_image *img);
+int mhd_restart_read(const char *path, mhd_restart_image *img);
+/* Writes a solve's current state: the state fields' ghost layers are filled
+ * first (mhd_sync of U and B faces), as the reference's checkpoint holds
+ * them.  Synchronous. */
+int mhd_batch_save_restart(mhd_batch *batch, int slot, const char *path);
+/* Loads the state fields the file holds, fills their ghost layers and
+ * prepares the solve at the file's time and step (*step, *time, may be
+ * NULL), ready to step.  Synchronous. */
+int mhd_batch_load_restart(mhd_batch *batch, int slot, const char *path, int32_t *step, double *time);
+int mhd_save_restart(mhd_ctx *ctx, const char *path);
+int mhd_load_restart(mhd_ctx *ctx, const char *path, int32_t *step, double *time);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ UNITS = [
     ("mhd_topology.cpp", "mhd_topology.o", EXACT),
     ("mhd_noalloc.cu", "mhd_noalloc.o", EXACT),
     ("mhd_host_setup.cpp", "mhd_host_setup.o", EXACT),
+    ("mhd_restart.cpp", "mhd_restart.o", EXACT),
 ]
 SOURCES = sorted({u[0] for u in UNITS})
 

@@ -105,12 +105,23 @@ class MhdInfo(ctypes.Structure):
                 ("remaining", ctypes.c_int64)]
 
 
+RESTART_FIELDS = ["U_H", "U_Na", "B_xi", "B_eta", "B_zeta"]  # MPCNSRST field list, in file order
+RESTART_CAPI = ["U_H", "U_NA", "B_XI", "B_ETA", "B_ZETA"]
+
+
+class MhdRestartImage(ctypes.Structure):
+    _fields_ = [("step", ctypes.c_int32), ("time", ctypes.c_double), ("n_blocks", ctypes.c_int32),
+                ("cells", ctypes.POINTER(ctypes.c_int32)), ("nghost", ctypes.c_int32),
+                ("data", ctypes.POINTER(ctypes.c_double) * 5), ("loaded", ctypes.c_uint32)]
+
+
 EXPORTS = [
     "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
-    "mhd_div_b", "mhd_batch_div_b", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
+    "mhd_div_b", "mhd_batch_div_b", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
+    "mhd_save_restart", "mhd_load_restart", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view",
@@ -160,6 +171,16 @@ def lib() -> ctypes.CDLL:
     L.mhd_topology_destroy.argtypes = [P]
     L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
     L.mhd_div_b.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+    RI = ctypes.POINTER(MhdRestartImage)
+    L.mhd_restart_values.argtypes = [RI, ctypes.c_int32]
+    L.mhd_restart_values.restype = ctypes.c_int64
+    L.mhd_restart_write.argtypes = [ctypes.c_char_p, RI]
+    L.mhd_restart_read.argtypes = [ctypes.c_char_p, RI]
+    L.mhd_save_restart.argtypes = [P, ctypes.c_char_p]
+    L.mhd_load_restart.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]
+    L.mhd_batch_save_restart.argtypes = [P, ctypes.c_int, ctypes.c_char_p]
+    L.mhd_batch_load_restart.argtypes = [P, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32),
+                                         ctypes.POINTER(ctypes.c_double)]
     L.mhd_batch_div_b.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.mhd_batch_destroy.argtypes = [P]
     L.mhd_batch_reserve.argtypes = [P, ctypes.c_int64]
@@ -204,6 +225,56 @@ def field_info(field: str):
 
 def _i3(v):
     return (ctypes.c_int32 * 3)(*[int(x) for x in v])
+
+
+def _restart_shapes(cells, nghost):
+    """Per state field, per block: the (ni, nj, nk, ncomp) FieldBlock shape."""
+    stag = {"U_H": (0, 0, 0, 5), "U_Na": (0, 0, 0, 5), "B_xi": (1, 0, 0, 1), "B_eta": (0, 1, 0, 1),
+            "B_zeta": (0, 0, 1, 1)}
+    return {f: [tuple(n[a] + stag[f][a] + 2 * nghost for a in range(3)) + (stag[f][3],) for n in cells]
+            for f in RESTART_FIELDS}
+
+
+def restart_read(path, cells, nghost: int):
+    """Read an MPCNSRST restart file (mhd_restart_read) for blocks of `cells`
+    with `nghost` ghost layers: returns (step, time, {field: [array per block]})
+    with only the fields the file holds; arrays are (ni, nj, nk, ncomp) over
+    the FieldBlock range [-nghost, n + stagger + nghost)."""
+    import numpy as np
+    shapes = _restart_shapes(cells, nghost)
+    bufs = {f: np.zeros(sum(int(np.prod(sh)) for sh in shapes[f])) for f in RESTART_FIELDS}
+    cc = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
+    img = MhdRestartImage(0, 0.0, len(cells), cc, nghost)
+    for q, f in enumerate(RESTART_FIELDS):
+        img.data[q] = bufs[f].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    check(lib().mhd_restart_read(os.fsencode(path), ctypes.byref(img)), "mhd_restart_read")
+    out = {}
+    for q, f in enumerate(RESTART_FIELDS):
+        if img.loaded & (1 << q):
+            arrs, off = [], 0
+            for sh in shapes[f]:
+                n = int(np.prod(sh))
+                arrs.append(bufs[f][off:off + n].reshape(sh).copy())
+                off += n
+            out[f] = arrs
+    return img.step, img.time, out
+
+
+def restart_write(path, step: int, time: float, cells, nghost: int, fields):
+    """Write an MPCNSRST restart file (mhd_restart_write); `fields` maps each
+    of RESTART_FIELDS to a list of per-block arrays shaped as restart_read
+    returns them."""
+    import numpy as np
+    shapes = _restart_shapes(cells, nghost)
+    bufs = {}
+    for f in RESTART_FIELDS:
+        parts = [np.ascontiguousarray(np.asarray(a, dtype=np.float64)).reshape(sh) for a, sh in zip(fields[f], shapes[f])]
+        bufs[f] = np.concatenate([a.ravel() for a in parts])
+    cc = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
+    img = MhdRestartImage(int(step), float(time), len(cells), cc, nghost)
+    for q, f in enumerate(RESTART_FIELDS):
+        img.data[q] = bufs[f].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    check(lib().mhd_restart_write(os.fsencode(path), ctypes.byref(img)), "mhd_restart_write")
 
 
 class Context:
@@ -268,6 +339,18 @@ class Context:
         v = ctypes.c_double()
         check(lib().mhd_div_b(self.ctx, ctypes.byref(v)), "mhd_div_b")
         return v.value
+
+    def save_restart(self, path):
+        """Write the state as an MPCNSRST restart file (mhd_save_restart)."""
+        check(lib().mhd_save_restart(self.ctx, os.fsencode(path)), "mhd_save_restart")
+
+    def load_restart(self, path):
+        """Load an MPCNSRST restart file and prepare the solve at its step and
+        time (mhd_load_restart); returns (step, time)."""
+        st, t = ctypes.c_int32(), ctypes.c_double()
+        check(lib().mhd_load_restart(self.ctx, os.fsencode(path), ctypes.byref(st), ctypes.byref(t)),
+              "mhd_load_restart")
+        return st.value, t.value
 
     def stream(self) -> int:
         return lib().mhd_stream(self.ctx)
@@ -393,6 +476,18 @@ class Batch:
     def reserve(self, nbytes: int):
         """Grow the batch's device memory pool ahead of the solves (mhd_batch_reserve)."""
         check(lib().mhd_batch_reserve(self.b, int(nbytes)), "mhd_batch_reserve")
+
+    def save_restart(self, slot: int, path):
+        """Write a solve's state as an MPCNSRST restart file (mhd_batch_save_restart)."""
+        check(lib().mhd_batch_save_restart(self.b, slot, os.fsencode(path)), "mhd_batch_save_restart")
+
+    def load_restart(self, slot: int, path):
+        """Load an MPCNSRST restart file into a solve and prepare it
+        (mhd_batch_load_restart); returns (step, time)."""
+        st, t = ctypes.c_int32(), ctypes.c_double()
+        check(lib().mhd_batch_load_restart(self.b, slot, os.fsencode(path), ctypes.byref(st), ctypes.byref(t)),
+              "mhd_batch_load_restart")
+        return st.value, t.value
 
     def close(self):
         if getattr(self, "b", None):

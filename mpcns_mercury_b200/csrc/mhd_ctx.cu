@@ -26,6 +26,7 @@
 #include "mhd_engine.cuh"
 #include "mhd_kernels.cuh"
 #include "mhd_parallel.h"
+#include "mhd_error.h"
 
 using namespace mhd;
 
@@ -42,6 +43,20 @@ int fail(int code, const char *fmt, ...) {
   g_last_error = buf;
   return code;
 }
+
+}  // namespace
+
+int mhd::set_error(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+namespace {
 
 #define CUDA_TRY(expr)                                                                        \
   do {                                                                                        \
@@ -1241,6 +1256,93 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   return MHD_OK;
 }
 
+int mhd_batch_save_restart(mhd_batch *b, int slot, const char *path) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  if (!path) return fail(MHD_ERR_ARG, "mhd_batch_save_restart: null path");
+  const Solve *S = b->slots[slot];
+  // every ghost layer of the state fields, as the reference's checkpoint holds them
+  if ((rc = mhd_batch_sync(b, slot, MHD_SYNC_UCELL)) || (rc = mhd_batch_sync(b, slot, MHD_SYNC_BFACE))) return rc;
+  if ((rc = read_state(b))) return rc;
+  std::vector<int32_t> cells;
+  for (const Box &bx : S->boxes)
+    for (int a = 0; a < 3; ++a) cells.push_back(bx.n[a]);
+  mhd_restart_image img{};
+  img.step = (int32_t)b->hstate[slot].step;
+  img.time = b->hstate[slot].time;
+  img.n_blocks = S->nblocks;
+  img.cells = cells.data();
+  img.nghost = S->nghost;
+  const int fields[MHD_RESTART_FIELDS] = {MHD_U_H, MHD_U_NA, MHD_B_XI, MHD_B_ETA, MHD_B_ZETA};
+  std::vector<double> buf[MHD_RESTART_FIELDS];
+  for (int f = 0; f < MHD_RESTART_FIELDS; ++f) {
+    buf[f].resize((size_t)mhd_restart_values(&img, f));
+    img.data[f] = buf[f].data();
+    double *d = buf[f].data();
+    const int *st = kStagger[kFieldSpec[fields[f]].loc];
+    const int nc = kFieldSpec[fields[f]].ncomp;
+    for (int blk = 0; blk < S->nblocks; ++blk) {
+      int32_t lo[3], hi[3];
+      int64_t n = nc;
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = -S->nghost;
+        hi[a] = S->boxes[blk].n[a] + st[a] + S->nghost;
+        n *= hi[a] - lo[a];
+      }
+      if ((rc = mhd_batch_download_field(b, slot, fields[f], blk, d, lo, hi, nc))) return rc;
+      d += n;
+    }
+  }
+  return mhd_restart_write(path, &img);
+}
+
+int mhd_batch_load_restart(mhd_batch *b, int slot, const char *path, int32_t *step, double *time) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  if (!path) return fail(MHD_ERR_ARG, "mhd_batch_load_restart: null path");
+  const Solve *S = b->slots[slot];
+  std::vector<int32_t> cells;
+  for (const Box &bx : S->boxes)
+    for (int a = 0; a < 3; ++a) cells.push_back(bx.n[a]);
+  mhd_restart_image img{};
+  img.n_blocks = S->nblocks;
+  img.cells = cells.data();
+  img.nghost = S->nghost;
+  std::vector<double> buf[MHD_RESTART_FIELDS];
+  for (int f = 0; f < MHD_RESTART_FIELDS; ++f) {
+    buf[f].resize((size_t)mhd_restart_values(&img, f));
+    img.data[f] = buf[f].data();
+  }
+  if ((rc = mhd_restart_read(path, &img))) return rc;
+  const int fields[MHD_RESTART_FIELDS] = {MHD_U_H, MHD_U_NA, MHD_B_XI, MHD_B_ETA, MHD_B_ZETA};
+  for (int f = 0; f < MHD_RESTART_FIELDS; ++f) {
+    if (!(img.loaded & (1u << f))) continue;  // not in the file: the solve keeps its values
+    const double *d = buf[f].data();
+    const int *st = kStagger[kFieldSpec[fields[f]].loc];
+    const int nc = kFieldSpec[fields[f]].ncomp;
+    for (int blk = 0; blk < S->nblocks; ++blk) {
+      int32_t lo[3], hi[3];
+      int64_t n = nc;
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = -S->nghost;
+        hi[a] = S->boxes[blk].n[a] + st[a] + S->nghost;
+        n *= hi[a] - lo[a];
+      }
+      if ((rc = mhd_batch_upload_field(b, slot, fields[f], blk, d, lo, hi, nc))) return rc;
+      d += n;
+    }
+  }
+  // the reference synchronises the restored fields before its first derived
+  // refresh (Z4_Mercury/src/MercurySolver.cpp:133-145)
+  if ((rc = mhd_batch_sync(b, slot, MHD_SYNC_UCELL)) || (rc = mhd_batch_sync(b, slot, MHD_SYNC_BFACE)) ||
+      (rc = mhd_batch_prepare(b, slot, img.time, img.step)))
+    return rc;
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  if (step) *step = img.step;
+  if (time) *time = img.time;
+  return MHD_OK;
+}
+
 int mhd_batch_div_b(mhd_batch *b, int slot, double *max_abs) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
@@ -1482,6 +1584,16 @@ int mhd_step_profiled(mhd_ctx *ctx, int nsteps, int max_kernels, float *kernel_m
 int mhd_div_b(mhd_ctx *ctx, double *max_abs) {
   if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
   return mhd_batch_div_b(ctx->batch, 0, max_abs);
+}
+
+int mhd_save_restart(mhd_ctx *ctx, const char *path) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_save_restart(ctx->batch, 0, path);
+}
+
+int mhd_load_restart(mhd_ctx *ctx, const char *path, int32_t *step, double *time) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_load_restart(ctx->batch, 0, path, step, time);
 }
 
 int mhd_sync(mhd_ctx *ctx, int group) {

@@ -799,6 +799,12 @@ int main(int argc, char **argv) {
       const std::string init = job_str("init", "ot");
       if (init == "ot") set_orszag_tang(S);
       if (init == "na_fraction") set_na_fraction(S);
+      if (!job_str("read_restart").empty()) {
+        // resume the state from a restart file through the reference's own
+        // reader (IOModule::ReadRestartBinFile, src/6_io/IOModule_Bin.cpp:234-420)
+        S.io_.Change_RestartPath(job_str("read_restart"));
+        S.io_.ReadRestartBinFile();
+      }
       S.mercury_bound_.Sync("Ucell");
       S.mercury_bound_.Sync("Bface");
       // Advance() begins with UpdateDerivedFields_ and the step-0 control
@@ -833,6 +839,13 @@ int main(int argc, char **argv) {
         S.StepOnce();
         stepping += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         dump_state(s);
+      }
+      if (!job_str("write_restart").empty()) {
+        // the reference's own restart writer (IOModule::WriteRestartBinFile,
+        // src/6_io/IOModule_Bin.cpp:168-232), with the step count and time of
+        // this run
+        S.io_.Change_RestartPath(job_str("write_restart"));
+        S.io_.WriteRestartBinFile((int)(job_int("restart_step0", 0) + steps), S.run_data_->time);
       }
       {
         // wall time of the StepOnce calls alone (setup and dumps excluded)

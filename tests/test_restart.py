@@ -1,0 +1,123 @@
+"""Restart files in the reference's MPCNSRST version 1 format
+(src/6_io/IOModule_Bin.cpp:168-420), host side: the library's reader
+(mhd_restart_read) against a file the reference's own writer produced after
+a few steps (its state is also dumped, so every value is checked, ghosts
+included), and the library's writer (mhd_restart_write) against the same
+file byte for byte.  Malformed files are rejected with MHD_ERR_ARG."""
+import struct
+
+import numpy as np
+import pytest
+
+N = 6
+NGHOST = 4
+STEPS = 3
+
+
+@pytest.fixture(scope="module")
+def ref_restart(ref_oracle, tmp_path_factory):
+    d = tmp_path_factory.mktemp("restart")
+    path = str(d / "ref.bin")
+    job = dict(ref_oracle.CUBE_JOB)
+    job.update(n=N, steps=STEPS, dump_at=str(STEPS), write_restart=path,
+               dump_fields=" ".join(ref_oracle.STATE_FIELDS))
+    dump = ref_oracle.run_job(job, workdir=str(d / "job"))
+    return path, dump
+
+
+def test_reader_matches_reference_state(ref_restart):
+    from mpcns_mercury_b200 import capi
+
+    path, dump = ref_restart
+    step, time, fields = capi.restart_read(path, [(N, N, N)], NGHOST)
+    assert step == STEPS
+    assert time == dump[(f"step{STEPS}:dt_time", -1)].data.ravel()[1]
+    assert sorted(fields) == sorted(capi.RESTART_FIELDS)
+    for name in capi.RESTART_FIELDS:
+        ref = dump[(f"step{STEPS}:{name}", 0)]
+        assert tuple(ref.lo) == (-NGHOST,) * 3
+        got = fields[name][0]
+        assert got.shape == ref.data.shape, name
+        assert np.array_equal(got, ref.data), name
+
+
+def test_writer_reproduces_reference_file(ref_restart, tmp_path):
+    from mpcns_mercury_b200 import capi
+
+    path, _ = ref_restart
+    step, time, fields = capi.restart_read(path, [(N, N, N)], NGHOST)
+    out = str(tmp_path / "ours.bin")
+    capi.restart_write(out, step, time, [(N, N, N)], NGHOST, fields)
+    with open(path, "rb") as a, open(out, "rb") as b:
+        assert a.read() == b.read()
+
+
+def _fields_of(path):
+    """(header bytes, [(name, field bytes)]) of a one-block restart file."""
+    raw = open(path, "rb").read()
+    head = raw[:8 + 4 + 4 + 8 + 4 + 4]
+    nfield = struct.unpack_from("<i", raw, 28)[0]
+    pos, out = len(head), []
+    for _ in range(nfield):
+        start = pos
+        ln = struct.unpack_from("<i", raw, pos)[0]
+        name = raw[pos + 4:pos + 4 + ln].decode()
+        pos += 4 + ln
+        _, ncomp, _ = struct.unpack_from("<iii", raw, pos)
+        pos += 12
+        lo = struct.unpack_from("<3i", raw, pos)
+        hi = struct.unpack_from("<3i", raw, pos + 12)
+        pos += 28
+        pos += 8 * int(np.prod(np.subtract(hi, lo))) * ncomp
+        out.append((name, raw[start:pos]))
+    return head, out
+
+
+def _assemble(head, parts):
+    return head[:28] + struct.pack("<i", len(parts)) + b"".join(p for _, p in parts)
+
+
+def test_reader_skips_unknown_and_reports_missing(ref_restart, tmp_path):
+    """Fields the library does not restore are skipped; fields the file lacks
+    are reported absent (the reference keeps their current values)."""
+    from mpcns_mercury_b200 import capi
+
+    path, dump = ref_restart
+    head, parts = _fields_of(path)
+    extra = bytearray(parts[2][1])             # B_xi's record renamed: an unknown field
+    extra[4:8] = b"X_xi"
+    mixed = [parts[0], ("X_xi", bytes(extra)), parts[1], parts[2], parts[3]]  # no B_zeta
+    p = str(tmp_path / "mixed.bin")
+    open(p, "wb").write(_assemble(head, mixed))
+    _, _, fields = capi.restart_read(p, [(N, N, N)], NGHOST)
+    assert sorted(fields) == sorted(["U_H", "U_Na", "B_xi", "B_eta"])
+    assert np.array_equal(fields["U_Na"][0], dump[(f"step{STEPS}:U_Na", 0)].data)
+
+
+@pytest.mark.parametrize("case", ["magic", "version", "blocks", "nghost", "range", "truncated", "location"])
+def test_reader_rejects_malformed(ref_restart, tmp_path, case):
+    from mpcns_mercury_b200 import capi
+
+    path, _ = ref_restart
+    raw = bytearray(open(path, "rb").read())
+    cells, nghost = [(N, N, N)], NGHOST
+    if case == "magic":
+        raw[0:8] = b"MPCNSRSX"
+    elif case == "version":
+        raw[8:12] = struct.pack("<i", 2)
+    elif case == "blocks":
+        cells = [(N, N, N), (N, N, N)]
+    elif case == "nghost":
+        nghost = NGHOST - 1
+    elif case == "range":
+        cells = [(N, N, N + 1)]
+    elif case == "truncated":
+        raw = raw[:len(raw) - 100]
+    elif case == "location":
+        ln = struct.unpack_from("<i", raw, 32)[0]
+        raw[36 + ln:40 + ln] = struct.pack("<i", 1)  # U_H claimed face-centred
+    p = str(tmp_path / f"{case}.bin")
+    open(p, "wb").write(bytes(raw))
+    with pytest.raises(capi.MhdError) as e:
+        capi.restart_read(p, cells, nghost)
+    assert "ERR_ARG" in str(e.value) and "mhd_restart_read:" in str(e.value)
