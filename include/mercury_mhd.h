@@ -352,6 +352,22 @@ int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghost, mhd_topo
 int mhd_topology_fill_desc(const mhd_topology *topo, mhd_desc *desc);
 int mhd_topology_destroy(mhd_topology *topo);
 
+/* ---- Per-solve setup on the device ----
+ * Computes every static field the step reads for one block from its node
+ * coordinates, with the reference's formulas (compute_metric_fields,
+ * src/7_metric/Metric.cpp:108-669,1261-1328; SetupCellReconstructionWeights_,
+ * Z4_Mercury/src/MercurySolver_ReconstructionSetup.cpp:29-193;
+ * Initial_Na_And_PhotoRate_, Z4_Mercury/include/2_Initial.h:227-440): JAC,
+ * JD*, AREA_*, DL_*, DR_*, HODGE_FACE_*, HODGE_EDGE_*, BCELL_W, JCELL_W,
+ * PHOTO, CELL_X/Y/Z; BADD_* zero (no dipole, no IMF) and TAPER_* 1 on the
+ * owned edges (Hall radial taper off).  nodes: x, y, z interleaved, (i, j, k)
+ * over [-(nghost + 1), n + nghost + 2) per axis, i slowest (AoS, like
+ * mhd_upload_field with 3 components).  L_ref: the length unit of the photo
+ * rate.  Replaces uploading those fields; the state is uploaded as before.
+ * Synchronous; mhd_prepare must follow. */
+int mhd_batch_setup_geometry(mhd_batch *batch, int slot, int block, const double *nodes, double L_ref);
+int mhd_setup_geometry(mhd_ctx *ctx, int block, const double *nodes, double L_ref);
+
 /* ---- Restart files ----
  * The reference's checkpoint format, MPCNSRST version 1
  * (IOModule::WriteRestartBinFile / ReadRestartBinFile,

@@ -120,7 +120,7 @@ EXPORTS = [
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
-    "mhd_div_b", "mhd_batch_div_b", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
+    "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
     "mhd_save_restart", "mhd_load_restart", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
@@ -171,6 +171,8 @@ def lib() -> ctypes.CDLL:
     L.mhd_topology_destroy.argtypes = [P]
     L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
     L.mhd_div_b.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+    L.mhd_setup_geometry.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_double]
+    L.mhd_batch_setup_geometry.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_double]
     RI = ctypes.POINTER(MhdRestartImage)
     L.mhd_restart_values.argtypes = [RI, ctypes.c_int32]
     L.mhd_restart_values.restype = ctypes.c_int64
@@ -340,6 +342,13 @@ class Context:
         check(lib().mhd_div_b(self.ctx, ctypes.byref(v)), "mhd_div_b")
         return v.value
 
+    def setup_geometry(self, nodes, block: int = 0, L_ref: float = 2.44e6):
+        """Compute the block's static fields on the device from its nodes
+        (mhd_setup_geometry); nodes: (ni, nj, nk, 3) over the node range."""
+        import numpy as np
+        a = np.ascontiguousarray(nodes, dtype=np.float64)
+        check(lib().mhd_setup_geometry(self.ctx, block, a.ctypes.data, float(L_ref)), "mhd_setup_geometry")
+
     def save_restart(self, path):
         """Write the state as an MPCNSRST restart file (mhd_save_restart)."""
         check(lib().mhd_save_restart(self.ctx, os.fsencode(path)), "mhd_save_restart")
@@ -476,6 +485,14 @@ class Batch:
     def reserve(self, nbytes: int):
         """Grow the batch's device memory pool ahead of the solves (mhd_batch_reserve)."""
         check(lib().mhd_batch_reserve(self.b, int(nbytes)), "mhd_batch_reserve")
+
+    def setup_geometry(self, slot: int, nodes, block: int = 0, L_ref: float = 2.44e6):
+        """Compute a solve's static fields on the device from a block's nodes
+        (mhd_batch_setup_geometry)."""
+        import numpy as np
+        a = np.ascontiguousarray(nodes, dtype=np.float64)
+        check(lib().mhd_batch_setup_geometry(self.b, slot, block, a.ctypes.data, float(L_ref)),
+              "mhd_batch_setup_geometry")
 
     def save_restart(self, slot: int, path):
         """Write a solve's state as an MPCNSRST restart file (mhd_batch_save_restart)."""

@@ -27,6 +27,7 @@
 #include "mhd_kernels.cuh"
 #include "mhd_parallel.h"
 #include "mhd_error.h"
+#include "mhd_geometry.cuh"
 
 using namespace mhd;
 
@@ -1343,6 +1344,83 @@ int mhd_batch_load_restart(mhd_batch *b, int slot, const char *path, int32_t *st
   return MHD_OK;
 }
 
+int mhd_batch_setup_geometry(mhd_batch *b, int slot, int block, const double *nodes, double L_ref) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  Solve *S = b->slots[slot];
+  if (block < 0 || block >= S->nblocks || !nodes) return fail(MHD_ERR_ARG, "mhd_batch_setup_geometry: bad arguments");
+  const Box &bx = S->boxes[block];
+  cudaStream_t st = b->stream;
+  // the nodes (x, y, z over the whole box) into a temporary device array
+  const int e[3] = {bx.n[0] + 1 + 2 * bx.G, bx.n[1] + 1 + 2 * bx.G, bx.n[2] + 1 + 2 * bx.G};
+  const size_t npts = (size_t)e[0] * e[1] * e[2];
+  double *dn = nullptr;
+  void **dtab = nullptr;
+  auto release = [&]() {
+    if (dn) cudaFreeAsync(dn, st);
+    if (dtab) cudaFreeAsync(dtab, st);
+  };
+  if (cudaMallocFromPoolAsync((void **)&dn, sizeof(double) * 3 * (size_t)bx.total, b->pool, st) != cudaSuccess ||
+      cudaMallocFromPoolAsync((void **)&dtab, sizeof(void *) * GEO_COUNT, b->pool, st) != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return fail(MHD_ERR_OOM, "mhd_batch_setup_geometry: temporary arrays");
+  }
+  if ((rc = ensure_staging(b, npts * 3))) {
+    release();
+    return rc;
+  }
+  void *node_ptrs[3] = {dn, dn + bx.total, dn + 2 * bx.total};
+  // every output component of the block, in GeoOut order
+  std::vector<void *> tab;
+  auto add = [&](int field, int ncomp) {
+    for (int m = 0; m < ncomp; ++m) tab.push_back(S->comp_ptr(block, kComp.first[field] + m, 0));
+  };
+  add(MHD_JAC, 1);
+  add(MHD_JDXI, 3);
+  add(MHD_JDET, 3);
+  add(MHD_JDZE, 3);
+  for (int f : {MHD_AREA_XI, MHD_AREA_ETA, MHD_AREA_ZETA, MHD_HODGE_FACE_XI, MHD_HODGE_FACE_ETA, MHD_HODGE_FACE_ZETA,
+                MHD_DL_XI, MHD_DL_ETA, MHD_DL_ZETA})
+    add(f, 1);
+  for (int f : {MHD_DR_XI, MHD_DR_ETA, MHD_DR_ZETA}) add(f, 3);
+  for (int f : {MHD_HODGE_EDGE_XI, MHD_HODGE_EDGE_ETA, MHD_HODGE_EDGE_ZETA}) add(f, 1);
+  add(MHD_BCELL_W, 18);
+  add(MHD_JCELL_W, 36);
+  for (int f : {MHD_BADD_XI, MHD_BADD_ETA, MHD_BADD_ZETA, MHD_PHOTO, MHD_CELL_X, MHD_CELL_Y, MHD_CELL_Z, MHD_TAPER_XI,
+                MHD_TAPER_ETA, MHD_TAPER_ZETA})
+    add(f, 1);
+  if ((int)tab.size() != GEO_COUNT) {
+    release();
+    return fail(MHD_ERR_ARG, "mhd_batch_setup_geometry: output table of %d components", (int)tab.size());
+  }
+  GeoBox gb;
+  for (int a = 0; a < 3; ++a) gb.n[a] = bx.n[a];
+  gb.G = bx.G;
+  gb.nghost = S->nghost;
+  gb.si = bx.si;
+  gb.sj = bx.sj;
+  gb.total = bx.total;
+  cudaError_t ce;
+  if ((ce = cudaMemcpyAsync(b->staging, nodes, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (ce = cudaMemcpyAsync(b->comp_ptrs, node_ptrs, sizeof node_ptrs, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (ce = cudaMemcpyAsync(dtab, tab.data(), sizeof(void *) * GEO_COUNT, cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+    release();
+    return fail(MHD_ERR_CUDA, "mhd_batch_setup_geometry: %s", cudaGetErrorString(ce));
+  }
+  k_scatter_aos<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(b->staging, -bx.G, -bx.G, -bx.G, e[0], e[1], e[2], 3,
+                                                                 b->comp_ptrs, 1, bx.si, bx.sj, bx.G, 0);
+  if ((ce = cudaGetLastError()) != cudaSuccess ||
+      (ce = launch_geometry(dn, gb, dtab, S->es == 4, L_ref, st)) != cudaSuccess) {
+    release();
+    return fail(MHD_ERR_CUDA, "mhd_batch_setup_geometry: %s", cudaGetErrorString(ce));
+  }
+  release();
+  CUDA_TRY(cudaStreamSynchronize(st));  // the caller may reuse `nodes`
+  S->prepared = false;
+  return MHD_OK;
+}
+
 int mhd_batch_div_b(mhd_batch *b, int slot, double *max_abs) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
@@ -1584,6 +1662,11 @@ int mhd_step_profiled(mhd_ctx *ctx, int nsteps, int max_kernels, float *kernel_m
 int mhd_div_b(mhd_ctx *ctx, double *max_abs) {
   if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
   return mhd_batch_div_b(ctx->batch, 0, max_abs);
+}
+
+int mhd_setup_geometry(mhd_ctx *ctx, int block, const double *nodes, double L_ref) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_setup_geometry(ctx->batch, 0, block, nodes, L_ref);
 }
 
 int mhd_save_restart(mhd_ctx *ctx, const char *path) {

@@ -63,8 +63,9 @@ def cube_nodes(n, amp: float = 0.05):
     return (-G, -G, -G), x, y, z
 
 
-class Geometry:
-    """Static fields of one block from its node coordinates (with ghosts)."""
+class Nodes:
+    """Node coordinates of one block (with ghosts) and its dual points (cell
+    centres): what the initial state needs, without the static fields."""
 
     def __init__(self, cells, node_lo, x, y, z, nghost: int = NGHOST):
         self.n = tuple(int(v) for v in cells)
@@ -73,11 +74,6 @@ class Geometry:
         self.x, self.y, self.z = x, y, z
         self.fields: dict[str, Arr] = {}
         self._dual()
-        self._faces()
-        self._jac()
-        self._face_hodge()
-        self._edges()
-        self._weights()
 
     # helpers -------------------------------------------------------------
     def N(self, lo, hi, di=0, dj=0, dk=0):
@@ -105,6 +101,23 @@ class Geometry:
         chi = tuple(self.n[a] + g for a in range(3))
         for name, d in zip(("cell_x", "cell_y", "cell_z"), out):
             self.fields[name] = Arr(clo, chi, d[..., None].copy())
+
+    def aos(self):
+        """The nodes as one (ni, nj, nk, 3) array over the node range (the
+        layout mhd_setup_geometry takes)."""
+        return np.ascontiguousarray(np.stack([self.x, self.y, self.z], axis=-1))
+
+
+class Geometry(Nodes):
+    """Static fields of one block from its node coordinates (with ghosts)."""
+
+    def __init__(self, cells, node_lo, x, y, z, nghost: int = NGHOST):
+        super().__init__(cells, node_lo, x, y, z, nghost)
+        self._faces()
+        self._jac()
+        self._face_hodge()
+        self._edges()
+        self._weights()
 
     def _faces(self):
         g = self.g
@@ -492,7 +505,7 @@ class _MT19937_64:
         return x & 0xFFFFFFFFFFFFFFFF
 
 
-def orszag_tang_state(geom: Geometry, gamma: float = 1.6667, noise: float = 1e-3, solve_id: int = 0):
+def orszag_tang_state(geom: Nodes, gamma: float = 1.6667, noise: float = 1e-3, solve_id: int = 0):
     """Config-1 initial state on a periodic cube: both ion fluids carry the
     Orszag-Tang vortex (rho = 1, p = 0.6, v = (-sin 2 pi y, sin 2 pi x, 0)) with
     multiplicative noise (1 + U[-noise, noise]) on every conserved component;
@@ -590,3 +603,12 @@ def cube_case(n=32, amp: float = 0.05, solve_id: int = 0):
         f[name] = Arr((-g,) * 3, tuple(hi_), t)
     f.update(orszag_tang_state(geom, solve_id=solve_id))
     return geom, f
+
+
+def cube_state(n=32, amp: float = 0.05, solve_id: int = 0):
+    """The periodic cube's nodes (AoS, for mhd_setup_geometry) and initial
+    state only: the static fields are then computed on the device."""
+    ns = (n, n, n) if np.isscalar(n) else tuple(int(v) for v in n)
+    lo, x, y, z = cube_nodes(ns, amp)
+    nodes = Nodes(ns, lo, x, y, z)
+    return nodes.aos(), orszag_tang_state(nodes, solve_id=solve_id)

@@ -54,6 +54,20 @@ def upload_case(upload, fields: dict, block: int = 0) -> int:
     return nbytes
 
 
+def setup_case_on_device(setup_geometry, upload, cells, solve_id: int = 0) -> int:
+    """One periodic box set up with its static fields computed on the device:
+    setup_geometry(nodes) (mhd_setup_geometry) then upload(capi name, array,
+    lo, hi, block) of the initial state only; returns the bytes uploaded."""
+    nodes, state = S.cube_state(tuple(int(v) for v in cells), solve_id=solve_id)
+    setup_geometry(nodes)
+    nbytes = nodes.nbytes
+    for name in STATE_FIELDS:
+        a = state[name]
+        upload(capi_field(name), a.data, a.lo, a.hi, 0)
+        nbytes += a.data.nbytes
+    return nbytes
+
+
 def ensemble_sizes(nsolves: int, stream: int = 100000):
     """Per-solve block sizes of the ensemble: cells per axis log-uniform,
     x and y in [24, 64], z in [24, 128] (the per-block range 24^3 .. 64x64x128),
