@@ -591,7 +591,9 @@ def run_serving(args, rank, world, device):
 
     nreq = args.requests
     shapes = W.ensemble_sizes(args.shapes, stream=200000 + rank)
-    pool = list(W.generate_cases([(c, 300000 + rank * 1000 + i) for i, c in enumerate(shapes)]))
+    # each shape's request carries its nodes and initial state; the server
+    # computes the static fields on the device when the shape first arrives
+    pool = W.state_cases([(c, 300000 + rank * 1000 + i) for i, c in enumerate(shapes)])
     u = Uniform(400000 + rank).sym(0.5, 3 * nreq) + 0.5
     t = 0.0
     reqs = []

@@ -18,7 +18,7 @@ import numpy as np
 
 from . import capi
 from .constants import reference_constants
-from .workloads import NGHOST, STATE_FIELDS, capi_field, upload_case
+from .workloads import NGHOST, STATE_FIELDS, capi_field, upload_request
 
 
 @dataclass
@@ -27,7 +27,8 @@ class Request:
     arrival_s: float          # seconds after the start of serving
     cells: tuple              # cells per axis of the (single, periodic) block
     steps: int
-    fields: dict              # {reference field name: Arr} inputs (static + initial state)
+    fields: dict              # {reference field name: Arr} inputs: static + initial state, or the
+                              # block's "nodes" (statics computed on the device) + initial state
     keep_result: bool = False
     geometry: object = None   # requests with equal keys share their grid and static fields (default: cells)
     # filled in by the server
@@ -83,7 +84,8 @@ class Server:
             d = capi.SolveDesc([req.cells], NGHOST, self.constants, precision=self.precision)
             slot = self.batch.add(d)
             d.close()
-            upload_case(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b), req.fields)
+            upload_request(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b),
+                           lambda nodes: self.batch.setup_geometry(slot, nodes), req.fields)
             self.templates[key] = slot
         return self.templates[key]
 
@@ -208,7 +210,7 @@ def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl:
         ctx = ctxs.get(key)
         if ctx is None:
             ctx = capi.Context([r.cells], NGHOST, reference_constants(cfl=cfl), precision=precision)
-            upload_case(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), r.fields)
+            upload_request(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), ctx.setup_geometry, r.fields)
             ctxs[key] = ctx
         else:
             _upload_state(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), r.fields)

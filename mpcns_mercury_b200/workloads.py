@@ -54,6 +54,32 @@ def upload_case(upload, fields: dict, block: int = 0) -> int:
     return nbytes
 
 
+def upload_request(upload, setup_geometry, fields: dict, block: int = 0) -> int:
+    """Inputs of one solve: with a "nodes" entry (the block's node
+    coordinates, AoS) the static fields are computed on the device
+    (setup_geometry(nodes)) and only the state is uploaded; otherwise every
+    input field is uploaded.  Returns the bytes sent to the device."""
+    if "nodes" not in fields:
+        return upload_case(upload, fields, block)
+    setup_geometry(fields["nodes"])
+    nbytes = fields["nodes"].nbytes
+    for name in STATE_FIELDS:
+        a = fields[name]
+        upload(capi_field(name), a.data, a.lo, a.hi, block)
+        nbytes += a.data.nbytes
+    return nbytes
+
+
+def state_cases(cases):
+    """[(cells, solve_id)] -> [{"nodes": ..., state fields}]: the requests of
+    device-side setup (host work: nodes and the seeded initial state only)."""
+    out = []
+    for cells, sid in cases:
+        nodes, state = S.cube_state(tuple(int(v) for v in cells), solve_id=sid)
+        out.append({"nodes": nodes, **state})
+    return out
+
+
 def setup_case_on_device(setup_geometry, upload, cells, solve_id: int = 0) -> int:
     """One periodic box set up with its static fields computed on the device:
     setup_geometry(nodes) (mhd_setup_geometry) then upload(capi name, array,
