@@ -348,22 +348,25 @@ class _PinnedInputs:
     def __init__(self):
         self.buf = None
 
-    def copy(self, fields):
+    def copy(self, fields, names=UPLOAD_FIELDS):
+        """Page-locked copies of fields[name] for `names` (Arr, or a plain
+        array such as "nodes")."""
         import torch
         from mpcns_mercury_b200.setup import Arr
 
-        need = sum(fields[n].data.nbytes for n in UPLOAD_FIELDS)
+        arr = {n: (fields[n].data if isinstance(fields[n], Arr) else fields[n]) for n in names}
+        need = sum(a.nbytes for a in arr.values())
         if self.buf is None or self.buf.numel() < need:
             self.buf = None
             self.buf = torch.empty(need, dtype=torch.uint8, pin_memory=True)
         raw = self.buf.numpy()
         out, off = {}, 0
-        for n in UPLOAD_FIELDS:
-            a = fields[n]
-            v = raw[off:off + a.data.nbytes].view(np.float64).reshape(a.data.shape)
-            v[...] = a.data
-            out[n] = Arr(a.lo, a.hi, v)
-            off += a.data.nbytes
+        for n in names:
+            a = arr[n]
+            v = raw[off:off + a.nbytes].view(np.float64).reshape(a.shape)
+            v[...] = a
+            out[n] = Arr(fields[n].lo, fields[n].hi, v) if isinstance(fields[n], Arr) else v
+            off += a.nbytes
         return out
 
 
@@ -420,6 +423,7 @@ def run_ensemble(args, rank, world, device):
     the plain FP64 single-solve path."""
     import torch
     from mpcns_mercury_b200 import Context, reference_constants
+    from mpcns_mercury_b200 import setup as S
     from mpcns_mercury_b200 import workloads as W
     from mpcns_mercury_b200.capi import Batch, SolveDesc
 
@@ -450,15 +454,26 @@ def run_ensemble(args, rank, world, device):
             need += d.device_bytes()
             d.close()
         b.reserve(need)
-    pin = _PinnedInputs()
+    pin, pin_nodes = _PinnedInputs(), _PinnedInputs()
     for sid, fields in enumerate(W.generate_cases([(c, base_id + s) for s, c in enumerate(cells)])):
         n = cells[sid]
-        pinned = pin.copy(fields)  # the inputs in page-locked host memory (not timed)
+        # the inputs in page-locked host memory (not timed): every field for
+        # the FP64 batch (bitwise against the plain path); the block's nodes
+        # and the state for the mixed batch, whose static fields are computed
+        # on the device (mhd_batch_setup_geometry) inside the timed region
+        pinned = pin.copy(fields)
+        _, nx, ny, nz = S.cube_nodes(n)
+        node_inputs = pin_nodes.copy({"nodes": np.stack([nx, ny, nz], axis=-1), **{k: fields[k] for k in W.STATE_FIELDS}},
+                                     names=["nodes"] + W.STATE_FIELDS)
         for prec, b in batches.items():
             d = SolveDesc([n], 4, k0, precision=prec)  # host topology (setup, not timed)
             t0 = time.perf_counter()
             slot = b.add(d)
-            nb = W.upload_case(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk), pinned)
+            if prec == 1:
+                nb = W.upload_request(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk),
+                                      lambda nodes: b.setup_geometry(slot, nodes), node_inputs)
+            else:
+                nb = W.upload_case(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk), pinned)
             b.sync(slot, "UCELL")
             b.sync(slot, "BFACE")
             b.prepare(slot)
@@ -572,9 +587,11 @@ def run_ensemble(args, rank, world, device):
                 "h2d_bytes_per_step": int(h2d_bytes / (W_ + K)), "d2h_bytes_per_step": int(d2h_bytes / (W_ + K)),
                 "wall_s": round(e2e_s, 3),
                 "what": "mixed batch via the C ABI from page-locked host arrays: add (copy-table compile and "
-                        "upload) + upload of every input field + prepare of every solve, W+K steps, download of "
-                        "every final state; host topology construction and the device memory reservation are "
-                        "setup, outside the timed region, as the reference arm times StepOnce only"},
+                        "upload), upload of the block's nodes with the static fields computed from them on the "
+                        "device (mhd_batch_setup_geometry), upload of the initial state, prepare of every solve, "
+                        "W+K steps, download of every final state; host topology construction and the device "
+                        "memory reservation are setup, outside the timed region, as the reference arm times "
+                        "StepOnce only"},
         "gpu_launches": launches * K, "clocks": clocks,
         "kernel_ms": {k: round(v, 5) for k, v in prof.items()},
     }
