@@ -466,9 +466,11 @@ def run_ensemble(args, rank, world, device):
         node_inputs = pin_nodes.copy({"nodes": np.stack([nx, ny, nz], axis=-1), **{k: fields[k] for k in W.STATE_FIELDS}},
                                      names=["nodes"] + W.STATE_FIELDS)
         for prec, b in batches.items():
-            d = SolveDesc([n], 4, k0, precision=prec)  # host topology (setup, not timed)
+            # FP64: host topology as explicit copy lists (setup, not timed), the
+            # reference-format path; mixed: the periodic tables compiled directly
+            d = SolveDesc([n], 4, k0, precision=prec) if prec == 0 else None
             t0 = time.perf_counter()
-            slot = b.add(d)
+            slot = b.add(d) if prec == 0 else b.add_periodic(n, 4, k0)
             if prec == 1:
                 nb = W.upload_request(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk),
                                       lambda nodes: b.setup_geometry(slot, nodes), node_inputs)
@@ -480,7 +482,8 @@ def run_ensemble(args, rank, world, device):
             b.request(slot, total_steps)
             t_api[prec] += time.perf_counter() - t0
             slots[prec].append(slot)
-            d.close()
+            if d is not None:
+                d.close()
             if prec == 1:
                 h2d_bytes += nb
         if only:
@@ -586,12 +589,11 @@ def run_ensemble(args, rank, world, device):
         "e2e": {"value": round(world * ncell * (W_ + K) / e2e_s / 1e6, 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d_bytes / (W_ + K)), "d2h_bytes_per_step": int(d2h_bytes / (W_ + K)),
                 "wall_s": round(e2e_s, 3),
-                "what": "mixed batch via the C ABI from page-locked host arrays: add (copy-table compile and "
-                        "upload), upload of the block's nodes with the static fields computed from them on the "
+                "what": "mixed batch via the C ABI from page-locked host arrays: add (mhd_batch_add_periodic: "
+                        "sync tables compiled from the periodic connectivity, uploaded), upload of the block's nodes with the static fields computed from them on the "
                         "device (mhd_batch_setup_geometry), upload of the initial state, prepare of every solve, "
-                        "W+K steps, download of every final state; host topology construction and the device "
-                        "memory reservation are setup, outside the timed region, as the reference arm times "
-                        "StepOnce only"},
+                        "W+K steps, download of every final state; the device memory reservation is setup, "
+                        "outside the timed region, as the reference arm times StepOnce only"},
         "gpu_launches": launches * K, "clocks": clocks,
         "kernel_ms": {k: round(v, 5) for k, v in prof.items()},
     }

@@ -299,6 +299,14 @@ int mhd_batch_reserve(mhd_batch *batch, int64_t bytes);
 int64_t mhd_desc_device_bytes(const mhd_desc *desc);
 /* Adds a solve (allocates its arena, uploads its tables) into a free slot. */
 int mhd_batch_add(mhd_batch *batch, const mhd_desc *desc, int *slot);
+/* Adds a one-block solve periodic in every direction (cells, nghost and the
+ * constants as in mhd_desc; the batch's precision) with its sync tables and
+ * edge alias classes compiled directly from the periodic connectivity, the
+ * same copies mhd_topology_periodic_block lists (no explicit copy lists:
+ * the fast way to admit such a solve).  No reference counterpart (its
+ * topology builder, src/2_topology/TopologyBuilder.cpp:436, makes the lists). */
+int mhd_batch_add_periodic(mhd_batch *batch, const int32_t cells[3], int32_t nghost, const mhd_constants *constants,
+                           int *slot);
 /* Adds a solve with the blocks and topology of the solve in src_slot, sharing
  * its device sync and alias tables (no descriptor processing): the way a
  * server admits a request whose grid it already holds.  constants: the new

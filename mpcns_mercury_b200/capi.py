@@ -121,7 +121,7 @@ EXPORTS = [
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
-    "mhd_save_restart", "mhd_load_restart", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
+    "mhd_save_restart", "mhd_load_restart", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view",
@@ -186,6 +186,7 @@ def lib() -> ctypes.CDLL:
     L.mhd_batch_div_b.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.mhd_batch_destroy.argtypes = [P]
     L.mhd_batch_reserve.argtypes = [P, ctypes.c_int64]
+    L.mhd_batch_add_periodic.argtypes = [P, i32p, ctypes.c_int32, ctypes.POINTER(MhdConstants), ctypes.POINTER(ctypes.c_int)]
     L.mhd_desc_device_bytes.argtypes = [ctypes.POINTER(MhdDesc)]
     L.mhd_desc_device_bytes.restype = ctypes.c_int64
     L.mhd_batch_add.argtypes = [P, ctypes.POINTER(MhdDesc), ctypes.POINTER(ctypes.c_int)]
@@ -505,6 +506,14 @@ class Batch:
         check(lib().mhd_batch_load_restart(self.b, slot, os.fsencode(path), ctypes.byref(st), ctypes.byref(t)),
               "mhd_batch_load_restart")
         return st.value, t.value
+
+    def add_periodic(self, cells, nghost: int, constants) -> int:
+        """Add a one-block periodic solve with its tables compiled directly
+        (mhd_batch_add_periodic); returns its slot."""
+        slot = ctypes.c_int()
+        check(lib().mhd_batch_add_periodic(self.b, _i3(cells), nghost, ctypes.byref(constants), ctypes.byref(slot)),
+              "mhd_batch_add_periodic")
+        return slot.value
 
     def close(self):
         if getattr(self, "b", None):

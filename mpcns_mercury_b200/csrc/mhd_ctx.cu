@@ -28,6 +28,7 @@
 #include "mhd_parallel.h"
 #include "mhd_error.h"
 #include "mhd_geometry.cuh"
+#include "mhd_periodic.h"
 
 using namespace mhd;
 
@@ -533,8 +534,122 @@ std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth) {
   return seg;
 }
 
-// Every group's three phases (pruned halo, owner, full halo) compiled on the
-// host threads and uploaded.
+// The three phases of every group (pruned halo, owner, full halo) segmented
+// on the host threads from the encoded halo (2 g) and owner (2 g + 1)
+// tables, and uploaded.
+int upload_encoded(Solve *S, const std::vector<Encoded> &enc, cudaStream_t st) {
+  std::vector<std::vector<int64_t>> seg(3 * MHD_NUM_GROUPS);
+  mhd::parallel_for(3 * MHD_NUM_GROUPS, [&](int q) {
+    const int g = q / 3, phase = q % 3;
+    seg[q] = build_segments(enc[2 * g + (phase == 1)], S->es, phase == 0 ? kHaloDepth[g] : -1);
+  });
+  for (int q = 0; q < 3 * MHD_NUM_GROUPS; ++q) {
+    const int g = q / 3, phase = q % 3;
+    S->T->tab_n[g][phase] = (int)(seg[q].size() / kSegWords);
+    S->T->table_bytes += (int64_t)seg[q].size() * 8;
+    const int rc = dev_upload(S->pool, seg[q], &S->T->tab_seg[g][phase], st);
+    if (rc) return rc;
+  }
+  return MHD_OK;
+}
+
+// The encoded tables of a block periodic in every direction, straight from
+// the periodic walks (mhd_periodic.h), without the explicit copy lists: one
+// field component per host thread, a counting pass then a writing pass.
+int upload_groups_periodic(Solve *S, cudaStream_t st) {
+  using namespace mhd::periodic;
+  const Box &bx = S->boxes[0];
+  const int n[3] = {bx.n[0], bx.n[1], bx.n[2]}, g = S->nghost;
+  struct Unit {
+    const GroupSpec *gs;
+    int field, m;
+    size_t nh, no, oh, oo;
+  };
+  std::vector<Unit> units;
+  for (const auto &gs : kGroups)
+    for (int field : gs.fields)
+      for (int m = 0; m < kFieldSpec[field].ncomp; ++m) units.push_back({&gs, field, m, 0, 0, 0, 0});
+  const int nu = (int)units.size();
+  mhd::parallel_for(nu, [&](int u) {
+    Unit &U = units[u];
+    walk_unit(*U.gs, U.field, U.m, n, g, [&](const mhd_copy &, bool own) { ++(own ? U.no : U.nh); });
+  });
+  std::vector<Encoded> enc(2 * MHD_NUM_GROUPS);
+  size_t nh[MHD_NUM_GROUPS] = {}, no[MHD_NUM_GROUPS] = {};
+  for (Unit &U : units) {
+    U.oh = nh[U.gs->group];
+    U.oo = no[U.gs->group];
+    nh[U.gs->group] += U.nh;
+    no[U.gs->group] += U.no;
+  }
+  for (int q = 0; q < MHD_NUM_GROUPS; ++q)
+    for (int p = 0; p < 2; ++p) {
+      Encoded &e = enc[2 * q + p];
+      const size_t cnt = p ? no[q] : nh[q];
+      e.dst.resize(cnt);
+      e.src.resize(cnt);
+      e.neg.assign(cnt, 0);
+      e.depth.resize(cnt);
+    }
+  mhd::parallel_for(nu, [&](int u) {
+    Unit &U = units[u];
+    size_t ih = U.oh, io = U.oo;
+    Encoded &eh = enc[2 * U.gs->group], &eo = enc[2 * U.gs->group + 1];
+    // the arena code of (i, j, k) of this component: its array's base plus
+    // the box offset (Solve::code for one block, without the lookups)
+    const int c = kComp.first[U.field] + U.m;
+    const int64_t base = S->comp_base(0, c, 0) | (c < kNumUComps ? kCodeUFlag : 0);
+    const int64_t es = S->es, G = bx.G;
+    const int *stg = kStagger[kFieldSpec[U.field].loc];
+    auto code = [&](const mhd_dof &q) { return base + ((q.i + G) * bx.si + (q.j + G) * bx.sj + (q.k + G)) * es; };
+    walk_unit(*U.gs, U.field, U.m, n, g, [&](const mhd_copy &cp, bool own) {
+      Encoded &e = own ? eo : eh;
+      const size_t t = own ? io++ : ih++;
+      e.dst[t] = code(cp.dst);
+      e.src[t] = code(cp.src);
+      const int q[3] = {cp.dst.i, cp.dst.j, cp.dst.k};
+      int depth = 0;
+      for (int a = 0; a < 3; ++a) {
+        const int hi = n[a] + stg[a];
+        const int da = q[a] < 0 ? -q[a] : (q[a] >= hi ? q[a] - hi + 1 : 0);
+        depth = da > depth ? da : depth;
+      }
+      e.depth[t] = (uint8_t)depth;
+    });
+  });
+  for (Encoded &e : enc) {
+    e.ascending = true;
+    for (size_t t = 1; t < e.dst.size(); ++t)
+      if (e.dst[t] <= e.dst[t - 1]) {
+        e.ascending = false;
+        break;
+      }
+  }
+  return upload_encoded(S, enc, st);
+}
+
+int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st);
+
+// Edge alias classes of a periodic block (mhd_periodic.h).
+int upload_aliases_periodic(Solve *S, cudaStream_t st) {
+  const Box &bx = S->boxes[0];
+  const int n[3] = {bx.n[0], bx.n[1], bx.n[2]};
+  std::vector<int32_t> off;
+  std::vector<mhd_dof> mem, own;
+  std::vector<double> ms, os;
+  mhd::periodic::alias_classes(n, off, mem, ms, own, os);
+  mhd_alias_classes a{};
+  a.n_classes = (int32_t)own.size();
+  a.offset = off.data();
+  a.member = mem.data();
+  a.member_sign = ms.data();
+  a.owner = own.data();
+  a.owner_sign = os.data();
+  return upload_aliases(S, a, st);
+}
+
+// Every group's explicit copy tables (the descriptor's) encoded on the host
+// threads, then segmented and uploaded.
 int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
   // every table's chunks on one pool of host threads
   constexpr int NT = 2 * MHD_NUM_GROUPS;
@@ -579,19 +694,7 @@ int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
       if (!asc[c] || (t0 && e.dst[t0] <= e.dst[t0 - 1])) e.ascending = false;
     }
   }
-  std::vector<std::vector<int64_t>> seg(3 * MHD_NUM_GROUPS);
-  mhd::parallel_for(3 * MHD_NUM_GROUPS, [&](int q) {
-    const int g = q / 3, phase = q % 3;
-    seg[q] = build_segments(enc[2 * g + (phase == 1)], S->es, phase == 0 ? kHaloDepth[g] : -1);
-  });
-  for (int q = 0; q < 3 * MHD_NUM_GROUPS; ++q) {
-    const int g = q / 3, phase = q % 3;
-    S->T->tab_n[g][phase] = (int)(seg[q].size() / kSegWords);
-    S->T->table_bytes += (int64_t)seg[q].size() * 8;
-    const int rc = dev_upload(S->pool, seg[q], &S->T->tab_seg[g][phase], st);
-    if (rc) return rc;
-  }
-  return MHD_OK;
+  return upload_encoded(S, enc, st);
 }
 
 int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
@@ -955,8 +1058,9 @@ int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
   return bytes;
 }
 
-int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
+static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slot_out) {
   if (!b || !desc || !slot_out || desc->n_blocks < 1 || !desc->cells) return fail(MHD_ERR_ARG, "mhd_batch_add: bad descriptor");
+  if (periodic && desc->n_blocks != 1) return fail(MHD_ERR_ARG, "mhd_batch_add_periodic: one block");
   if (desc->nghost < 2) return fail(MHD_ERR_ARG, "mhd_batch_add: nghost %d (the step's stencils need >= 2)", desc->nghost);
   if (desc->precision != b->precision)
     return fail(MHD_ERR_ARG, "solve precision %d differs from the batch's (%d)", desc->precision, b->precision);
@@ -1045,11 +1149,15 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
     if ((rc = dev_upload(S->pool, prefix[r], &S->T->dtile_prefix[r], st))) return bail(rc);
   }
   try {
-    if ((rc = upload_groups(S, desc->groups, st))) return bail(rc);
+    if (periodic) {
+      if ((rc = upload_groups_periodic(S, st)) || (rc = upload_aliases_periodic(S, st))) return bail(rc);
+    } else {
+      if ((rc = upload_groups(S, desc->groups, st))) return bail(rc);
+      if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
+    }
   } catch (...) {  // host allocation or thread creation failed
     return bail(fail(MHD_ERR_OOM, "host memory for the copy tables"));
   }
-  if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
   SolveState s0{};
   s0.dt_bits = kDtUnset;
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
@@ -1063,6 +1171,20 @@ int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) {
   if (grew) drop_graphs(b);
   *slot_out = slot;
   return MHD_OK;
+}
+
+int mhd_batch_add(mhd_batch *b, const mhd_desc *desc, int *slot_out) { return add_solve(b, desc, false, slot_out); }
+
+int mhd_batch_add_periodic(mhd_batch *b, const int32_t cells[3], int32_t nghost, const mhd_constants *constants,
+                           int *slot_out) {
+  if (!b || !cells || !constants) return fail(MHD_ERR_ARG, "mhd_batch_add_periodic: bad arguments");
+  mhd_desc d{};
+  d.n_blocks = 1;
+  d.cells = cells;
+  d.nghost = nghost;
+  d.precision = b->precision;
+  d.constants = *constants;
+  return add_solve(b, &d, true, slot_out);
 }
 
 int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constants, int copy_static, int *slot_out) {

@@ -81,9 +81,7 @@ class Server:
         if key not in self.templates:
             if len(self.templates) >= self.max_grids:
                 raise RuntimeError(f"more than {self.max_grids} distinct grids")
-            d = capi.SolveDesc([req.cells], NGHOST, self.constants, precision=self.precision)
-            slot = self.batch.add(d)
-            d.close()
+            slot = self.batch.add_periodic(req.cells, NGHOST, self.constants)
             upload_request(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b),
                            lambda nodes: self.batch.setup_geometry(slot, nodes), req.fields)
             self.templates[key] = slot

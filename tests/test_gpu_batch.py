@@ -157,3 +157,30 @@ def test_reserved_pool_equals_single(cases):
         b.remove(slot)
         d.close()
     b.close()
+
+
+def test_add_periodic_equals_explicit_tables(cases):
+    """A solve added with mhd_batch_add_periodic (tables compiled straight from
+    the periodic connectivity) steps bit for bit like the same solve added
+    from the explicit copy lists of mhd_topology_periodic_block, in both
+    precisions."""
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.capi import Batch, SolveDesc
+
+    k0 = reference_constants(cfl=0.4)
+    n, fields = SIZES[1], cases[1]
+    for precision in (0, 1):
+        b = Batch(2, precision)
+        d = SolveDesc([n], W.NGHOST, k0, precision=precision)
+        slots = [b.add(d), b.add_periodic(n, W.NGHOST, k0)]
+        for slot in slots:
+            W.upload_case(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk), fields)
+            b.sync(slot, "UCELL")
+            b.sync(slot, "BFACE")
+            b.prepare(slot)
+            b.request(slot, 5)
+        b.run(5)
+        assert _same(_state(b, slots[1], fields), _state(b, slots[0], fields)), precision
+        b.close()
+        d.close()
