@@ -297,7 +297,8 @@ int mhd_batch_reserve(mhd_batch *batch, int64_t bytes);
 /* Device bytes a solve of this descriptor occupies (arena and tables); -1 on
  * a bad descriptor.  Lets a server admit requests against free HBM. */
 int64_t mhd_desc_device_bytes(const mhd_desc *desc);
-/* Adds a solve (allocates its arena, uploads its tables) into a free slot. */
+/* Adds a solve (allocates its arena, uploads its tables) into a free slot;
+ * stream-ordered with the batch's other work. */
 int mhd_batch_add(mhd_batch *batch, const mhd_desc *desc, int *slot);
 /* Adds a one-block solve periodic in every direction (cells, nghost and the
  * constants as in mhd_desc; the batch's precision) with its sync tables and
@@ -372,7 +373,8 @@ int mhd_topology_destroy(mhd_topology *topo);
  * over [-(nghost + 1), n + nghost + 2) per axis, i slowest (AoS, like
  * mhd_upload_field with 3 components).  L_ref: the length unit of the photo
  * rate.  Replaces uploading those fields; the state is uploaded as before.
- * Synchronous; mhd_prepare must follow. */
+ * Asynchronous like mhd_batch_upload_field (it waits only for page-locked
+ * nodes); mhd_prepare must follow. */
 int mhd_batch_setup_geometry(mhd_batch *batch, int slot, int block, const double *nodes, double L_ref);
 int mhd_setup_geometry(mhd_ctx *ctx, int block, const double *nodes, double L_ref);
 

@@ -1167,8 +1167,13 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
   if (S->consts.resistive) ++b->n_res;
   const bool grew = count_tables(b, S, +1);
   if ((rc = publish(b))) return rc;
-  CUDA_TRY(cudaStreamSynchronize(st));
-  if (grew) drop_graphs(b);
+  // asynchronous: the host data went to the device through pageable copies,
+  // staged before they returned; a step graph to capture anew waits for the
+  // graphs in flight first
+  if (grew) {
+    CUDA_TRY(cudaStreamSynchronize(st));
+    drop_graphs(b);
+  }
   *slot_out = slot;
   return MHD_OK;
 }
@@ -1538,7 +1543,14 @@ int mhd_batch_setup_geometry(mhd_batch *b, int slot, int block, const double *no
     return fail(MHD_ERR_CUDA, "mhd_batch_setup_geometry: %s", cudaGetErrorString(ce));
   }
   release();
-  CUDA_TRY(cudaStreamSynchronize(st));  // the caller may reuse `nodes`
+  // page-locked nodes are read by the DMA later: wait before the caller may
+  // reuse them (pageable ones were staged before the copy returned)
+  cudaPointerAttributes pa{};
+  if (cudaPointerGetAttributes(&pa, nodes) != cudaSuccess) {
+    cudaGetLastError();
+    pa.type = cudaMemoryTypeHost;
+  }
+  if (pa.type != cudaMemoryTypeUnregistered) CUDA_TRY(cudaStreamSynchronize(st));
   S->prepared = false;
   return MHD_OK;
 }
