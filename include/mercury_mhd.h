@@ -105,8 +105,12 @@ typedef struct mhd_constants {
    * Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:475-555): after the
    * explicit update, solve (I + dt eta alpha C^T beta C) E = eta J(B*) on the
    * owned edges with eta > 0 (eta: MHD_ETA_RES_*), then B = B* - dt curl E.
-   * Solved by preconditioned CG to ||A E - b|| <= res_rtol ||b|| (at most
-   * res_max_it iterations, else MHD_ERR_SOLVE).  FP64 solves only. */
+   * Solved to ||A E - b|| <= res_rtol ||b||, else MHD_ERR_SOLVE.  FP64
+   * solves: preconditioned CG (at most res_max_it iterations; res_rtol 0 =
+   * 1e-13).  Mixed-precision solves: iterative refinement with the residual
+   * A E - b and its norms in FP64 and each correction solved by FP32 CG (on
+   * the solve's own FP32 edge fields) to 1e-4 of its right-hand side (at most
+   * res_max_it iterations each, at most 30 refinements; res_rtol 0 = 1e-10). */
   double res_rtol;
   int32_t resistive;  /* is_Mercury_resistance */
   int32_t res_max_it;
@@ -201,6 +205,12 @@ typedef struct mhd_info {
   int32_t pad_;
   int64_t device_bytes;
   int64_t remaining;   /* steps of the current request not yet taken */
+  /* last implicit resistive substep of the solve (zeros without one):
+   * residual norm / ||b|| at exit (FP64 solves: CG's recursive residual;
+   * mixed precision: the refinement's FP64 residual ||A E - b||), CG
+   * iterations (over all refinements) and refinements (0 in FP64 solves) */
+  double res_relres;
+  int32_t res_iters, res_refinements;
 } mhd_info;
 int mhd_get_info(mhd_ctx *ctx, mhd_info *info);
 
@@ -294,8 +304,10 @@ int mhd_batch_destroy(mhd_batch *batch);
  * tables from it without mapping new memory.  No reference counterpart (its
  * solver allocates at setup).  Synchronous. */
 int mhd_batch_reserve(mhd_batch *batch, int64_t bytes);
-/* Device bytes a solve of this descriptor occupies (arena and tables); -1 on
- * a bad descriptor.  Lets a server admit requests against free HBM. */
+/* Device bytes a solve of this descriptor occupies (arena and tables, and
+ * for a mixed-precision solve with the implicit resistive substep its FP64
+ * companion, which holds the refinement's residual); -1 on a bad descriptor.
+ * Lets a server admit requests against free HBM. */
 int64_t mhd_desc_device_bytes(const mhd_desc *desc);
 /* Adds a solve (allocates its arena, uploads its tables) into a free slot;
  * stream-ordered with the batch's other work. */

@@ -102,7 +102,8 @@ class MhdDesc(ctypes.Structure):
 class MhdInfo(ctypes.Structure):
     _fields_ = [("time", ctypes.c_double), ("dt", ctypes.c_double), ("step", ctypes.c_int64),
                 ("status", ctypes.c_int32), ("pad_", ctypes.c_int32), ("device_bytes", ctypes.c_int64),
-                ("remaining", ctypes.c_int64)]
+                ("remaining", ctypes.c_int64), ("res_relres", ctypes.c_double), ("res_iters", ctypes.c_int32),
+                ("res_refinements", ctypes.c_int32)]
 
 
 RESTART_FIELDS = ["U_H", "U_Na", "B_xi", "B_eta", "B_zeta"]  # MPCNSRST field list, in file order

@@ -138,6 +138,12 @@ struct Solve {
   Tables *T = nullptr;
   double res_rtol = 0.0;
   int res_max_it = 0;
+  // mixed precision with the implicit resistive substep: slot of the FP64
+  // companion solve (same blocks and tables) in the batch's companion batch
+  int shadow_slot = -1;
+  // the last implicit resistive substep (mhd_info)
+  double res_relres = 0.0;
+  int res_iters = 0, res_refinements = 0;
   Consts consts{};
 
   int comp_bytes(int c) const { return is_metric(c) ? 8 : es; }
@@ -190,6 +196,10 @@ struct mhd_batch {
   // sync phases empty in every solve get no launch in the step
   int live_tables[kMaxGroups][2] = {};
   int n_res = 0;                                        // slots whose solve has the implicit resistive substep
+  // FP64 batch of the companions of mixed-precision resistive solves, which
+  // runs on this batch's stream and pool (borrowed = true in the companion)
+  mhd_batch *shadow = nullptr;
+  bool borrowed = false;
   ResScratch res{nullptr, nullptr};
   double *hres = nullptr;                               // pinned copy of res.result
   int kernels_per_step = 0;
@@ -849,12 +859,101 @@ void res_apply(mhd_batch *b, int *nk) {
   launch(b, 1, SK_RES_Q, nk);
 }
 
+// CG iterations on the masked solve of b from x = 0 and r = p = the
+// right-hand side (rho = its W-weighted r.r), until ||r|| <= tol or max_it
+// iterations; *rnorm: the last ||r||, *iters: iterations taken.
+int res_cg(mhd_batch *b, double rho, double tol, int max_it, double *rnorm, int *iters, bool *converged) {
+  int rc, nk = 0;
+  *converged = *rnorm <= tol;
+  *iters = 0;
+  for (int it = 0; it < max_it && !*converged; ++it) {
+    res_apply(b, &nk);
+    if ((rc = res_dot(b, RES_DOT_PQ))) return rc;
+    const double pq = b->hres[0];
+    if (!(pq > 0.0)) break;  // breakdown: not positive definite on these unknowns
+    const double alpha = rho / pq;
+    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_AXPY, alpha);
+    ++*iters;
+    if ((rc = res_dot(b, RES_DOT_RR))) return rc;
+    const double rho_new = b->hres[0];
+    *rnorm = std::sqrt(b->hres[1]);
+    if (*rnorm <= tol) {
+      *converged = true;
+      break;
+    }
+    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_PUPD, rho_new / rho);
+    rho = rho_new;
+  }
+  return MHD_OK;
+}
+
+// The mixed-precision solve of (I + dt eta alpha C^T beta C) E = b by
+// iterative refinement: the residual r = b - A x and its norms in FP64 on
+// the solve's FP64 companion (widened alpha, beta, eta, W; its own copies of
+// the E / B / J syncs), each correction A d = r solved by FP32 CG on the
+// solve's own arrays to 1e-4 of ||r||, x += d in FP64.  b = eta J(B*) is the
+// FP32 step's current (the state is FP32).  On return the solve's x holds
+// the solution rounded to FP32.
+int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
+  mhd_batch *sh = b->shadow;
+  const int cs = S->shadow_slot;
+  const Solve *C = sh->slots[cs];
+  const Dir Dm = b->dir(1);
+  cudaStream_t st = b->stream;
+  constexpr int kMaxRefinements = 30;
+  constexpr double kInnerRtol = 1e-4;
+  const int one = 1, zero = 0;
+  int rc, nk = 0;
+  // the companion's dt, coefficients, b and x = 0
+  CUDA_TRY(cudaMemcpyAsync((char *)(sh->dstate + cs) + offsetof(SolveState, dt),
+                           (const char *)(b->dstate + slot) + offsetof(SolveState, dt), sizeof(double),
+                           cudaMemcpyDeviceToDevice, st));
+  launch_res_cross(Dm, C->dblocks, RES_X_SETUP, st);
+  CUDA_TRY(cudaGetLastError());
+  if ((rc = set_state_field(sh, cs, offsetof(SolveState, mask), &one, sizeof one))) return rc;
+  if ((rc = res_dot(sh, RES_DOT_RR))) return rc;
+  const double bnorm = std::sqrt(sh->hres[1]);
+  const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-10;
+  double rn = bnorm;
+  S->res_iters = 0;
+  S->res_refinements = 0;
+  for (;;) {
+    if (S->res_refinements > 0) {  // r = b - A x in FP64
+      launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_P_FROM_X);
+      res_apply(sh, &nk);
+      launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_RESID);
+      if ((rc = res_dot(sh, RES_DOT_RR))) return rc;
+      rn = std::sqrt(sh->hres[1]);
+    }
+    if (rn <= rtol * bnorm) {
+      *converged = true;
+      break;
+    }
+    if (S->res_refinements == kMaxRefinements || !(rn == rn)) break;
+    // the correction: FP32 CG on r rounded to FP32, x += d in FP64
+    launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_R, st);
+    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
+    if ((rc = res_dot(b, RES_DOT_RR))) return rc;
+    double r32 = std::sqrt(b->hres[1]);
+    int iters = 0;
+    bool inner = false;
+    if ((rc = res_cg(b, b->hres[0], kInnerRtol * r32, S->res_max_it, &r32, &iters, &inner))) return rc;
+    launch_res_cross(Dm, C->dblocks, RES_X_ADD_X, st);
+    S->res_iters += iters;
+    ++S->res_refinements;
+  }
+  S->res_relres = bnorm > 0.0 ? rn / bnorm : 0.0;
+  launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_X, st);
+  CUDA_TRY(cudaGetLastError());
+  return set_state_field(sh, cs, offsetof(SolveState, mask), &zero, sizeof zero);
+}
+
 // The implicit resistive substep of one solve (SolveImplicitResistiveDiffusion_,
 // Mercury_ImplicitResistive.cpp:475-555), after the explicit update and its
-// Sync(B faces): B* snapshot, J(B*), b = eta J(B*), CG in the inner product
-// weighted by 1 / (eta alpha) (A is self-adjoint in it), then B = B* - dt
-// curl E_res.  The reference solves with GMRES; the solution is the same to
-// the solvers' tolerance.
+// Sync(B faces): B* snapshot, J(B*), b = eta J(B*), the solve (FP64: CG in
+// the inner product weighted by 1 / (eta alpha), in which A is self-adjoint;
+// mixed precision: res_refine), then B = B* - dt curl E_res.  The reference
+// solves with GMRES; the solution is the same to the solvers' tolerance.
 int res_solve(mhd_batch *b, int slot) {
   Solve *S = b->slots[slot];
   const int one = 1, zero = 0;
@@ -866,26 +965,17 @@ int res_solve(mhd_batch *b, int slot) {
   sync1(b, 1, alias_op(1), &nk);
   sync1(b, 1, copy_op(MHD_SYNC_JEDGE, 1), &nk);
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_INIT);
-  if ((rc = res_dot(b, RES_DOT_RR))) return rc;
-  double rho = b->hres[0];
-  const double bnorm = std::sqrt(b->hres[1]);
-  const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-13;
-  bool converged = bnorm == 0.0;
-  for (int it = 0; it < S->res_max_it && !converged; ++it) {
-    res_apply(b, &nk);
-    if ((rc = res_dot(b, RES_DOT_PQ))) return rc;
-    const double pq = b->hres[0];
-    if (!(pq > 0.0)) break;  // breakdown: not positive definite on these unknowns
-    const double alpha = rho / pq;
-    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_AXPY, alpha);
+  bool converged = false;
+  if (S->shadow_slot >= 0) {
+    if ((rc = res_refine(b, slot, S, &converged))) return rc;
+  } else {
     if ((rc = res_dot(b, RES_DOT_RR))) return rc;
-    const double rho_new = b->hres[0];
-    if (std::sqrt(b->hres[1]) <= rtol * bnorm) {
-      converged = true;
-      break;
-    }
-    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_PUPD, rho_new / rho);
-    rho = rho_new;
+    const double bnorm = std::sqrt(b->hres[1]);
+    const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-13;
+    double rn = bnorm;
+    if ((rc = res_cg(b, b->hres[0], rtol * bnorm, S->res_max_it, &rn, &S->res_iters, &converged))) return rc;
+    S->res_relres = bnorm > 0.0 ? rn / bnorm : 0.0;
+    S->res_refinements = 0;
   }
   if (!converged) {
     const int st = MHD_ERR_SOLVE;
@@ -997,6 +1087,7 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
 int mhd_batch_destroy(mhd_batch *b) {
   if (!b) return MHD_OK;
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->shadow) mhd_batch_destroy(b->shadow);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->graph_a) cudaGraphExecDestroy(b->graph_a);
   if (b->graph_b) cudaGraphExecDestroy(b->graph_b);
@@ -1020,8 +1111,8 @@ int mhd_batch_destroy(mhd_batch *b) {
   cudaFree(b->dprefix_aliasE);
   cudaFree(b->dprefix_aliasJ);
   for (auto e : b->prof_events) cudaEventDestroy(e);
-  if (b->stream) cudaStreamDestroy(b->stream);
-  if (b->pool) cudaMemPoolDestroy(b->pool);  // every allocation from it was freed and the stream drained
+  if (b->stream && !b->borrowed) cudaStreamDestroy(b->stream);
+  if (b->pool && !b->borrowed) cudaMemPoolDestroy(b->pool);  // every allocation from it was freed and the stream drained
   delete b;
   return MHD_OK;
 }
@@ -1055,7 +1146,29 @@ int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
   if (desc->edge_aliases.n_classes > 0 && desc->edge_aliases.offset)
     bytes += (int64_t)desc->edge_aliases.offset[desc->edge_aliases.n_classes] * 24 +
              (int64_t)desc->edge_aliases.n_classes * 28;
+  if (desc->precision == kMixed && desc->constants.resistive) {  // the FP64 companion of the implicit substep
+    mhd_desc d64 = *desc;
+    d64.precision = kFP64;
+    bytes += mhd_desc_device_bytes(&d64);
+  }
   return bytes;
+}
+
+// The FP64 companion batch of a mixed-precision batch, made at its first
+// resistive solve: same capacity, on the batch's own stream and pool.
+static int ensure_shadow(mhd_batch *b) {
+  if (b->shadow) return MHD_OK;
+  mhd_batch *sh = nullptr;
+  int rc = mhd_batch_create(b->capacity, kFP64, &sh);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(sh->stream));  // idle: its own stream and pool are replaced
+  cudaStreamDestroy(sh->stream);
+  cudaMemPoolDestroy(sh->pool);
+  sh->stream = b->stream;
+  sh->pool = b->pool;
+  sh->borrowed = true;
+  b->shadow = sh;
+  return MHD_OK;
 }
 
 static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slot_out) {
@@ -1064,8 +1177,6 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
   if (desc->nghost < 2) return fail(MHD_ERR_ARG, "mhd_batch_add: nghost %d (the step's stencils need >= 2)", desc->nghost);
   if (desc->precision != b->precision)
     return fail(MHD_ERR_ARG, "solve precision %d differs from the batch's (%d)", desc->precision, b->precision);
-  if (desc->constants.resistive && b->precision != kFP64)
-    return fail(MHD_ERR_ARG, "the implicit resistive substep is available in FP64 only");
   if (desc->n_blocks >= (1 << 15)) return fail(MHD_ERR_ARG, "too many blocks (%d)", desc->n_blocks);
   int slot = -1;
   for (int s = 0; s < b->capacity; ++s)
@@ -1102,6 +1213,10 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
     if ((int64_t)(kNumComps + kNumUComps) * bx.total >= (int64_t(1) << 31))
       return bail(fail(MHD_ERR_ARG, "block %d too large (%lld cells with ghosts); split it into smaller blocks", bi,
                        (long long)bx.total));
+    // the substep marks its unknowns by element offsets held in the real type
+    if (desc->constants.resistive && S->es == 4 && bx.total > (int64_t(1) << 24))
+      return bail(fail(MHD_ERR_ARG, "block %d: %lld cells with ghosts exceed 2^24 (mixed-precision implicit substep)",
+                       bi, (long long)bx.total));
     S->boxes.push_back(bx);
     S->ubase.push_back(u);
     S->mbase.push_back(m);
@@ -1174,6 +1289,16 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
     CUDA_TRY(cudaStreamSynchronize(st));
     drop_graphs(b);
   }
+  if (b->precision == kMixed && S->consts.resistive) {
+    mhd_desc d64 = *desc;
+    d64.precision = kFP64;
+    int cs = -1;
+    if ((rc = ensure_shadow(b)) || (rc = add_solve(b->shadow, &d64, periodic, &cs))) {
+      mhd_batch_remove(b, slot);
+      return rc;
+    }
+    S->shadow_slot = cs;
+  }
   *slot_out = slot;
   return MHD_OK;
 }
@@ -1196,8 +1321,6 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   int rc = slot_check(b, src_slot);
   if (rc) return rc;
   if (!slot_out) return fail(MHD_ERR_ARG, "mhd_batch_add_like: null slot");
-  if (constants && constants->resistive && b->precision != kFP64)
-    return fail(MHD_ERR_ARG, "the implicit resistive substep is available in FP64 only");
   if (constants && (constants->resistive != 0) != (b->slots[src_slot]->consts.resistive != 0))
     return fail(MHD_ERR_ARG, "mhd_batch_add_like: the implicit resistive substep must match the template's");
   int slot = -1;
@@ -1274,6 +1397,14 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
     drop_graphs(b);
   }
   if ((rc = publish(b))) return rc;
+  if (src->shadow_slot >= 0) {
+    int cs = -1;
+    if ((rc = mhd_batch_add_like(b->shadow, src->shadow_slot, nullptr, 0, &cs))) {
+      mhd_batch_remove(b, slot);
+      return rc;
+    }
+    S->shadow_slot = cs;
+  }
   *slot_out = slot;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
 }
@@ -1282,6 +1413,7 @@ int mhd_batch_remove(mhd_batch *b, int slot) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
   Solve *S = b->slots[slot];
+  if (S->shadow_slot >= 0 && (rc = mhd_batch_remove(b->shadow, S->shadow_slot))) return rc;
   b->slots[slot] = nullptr;
   if (S->consts.resistive) --b->n_res;
   count_tables(b, S, -1);
@@ -1603,6 +1735,21 @@ int mhd_batch_run(mhd_batch *b, int nsteps) {
   return MHD_OK;
 }
 
+// Host-side fields of a slot's mhd_info: device bytes (with an FP64
+// companion's) and the last implicit substep's figures.
+static void fill_solve_info(const mhd_batch *b, int s, mhd_info *info) {
+  const Solve *S = b->slots[s];
+  if (!S) return;
+  info->device_bytes = S->arena_bytes + S->T->table_bytes;
+  if (S->shadow_slot >= 0) {
+    const Solve *C = b->shadow->slots[S->shadow_slot];
+    info->device_bytes += C->arena_bytes + C->T->table_bytes;
+  }
+  info->res_relres = S->res_relres;
+  info->res_iters = S->res_iters;
+  info->res_refinements = S->res_refinements;
+}
+
 int mhd_batch_poll(mhd_batch *b, mhd_info *infos) {
   if (!b || !infos) return fail(MHD_ERR_ARG, "mhd_batch_poll: bad arguments");
   int rc = read_state(b);
@@ -1615,8 +1762,7 @@ int mhd_batch_poll(mhd_batch *b, mhd_info *infos) {
     infos[s].step = st.step;
     infos[s].status = st.status;
     infos[s].remaining = st.remaining;
-    const Solve *S = b->slots[s];
-    infos[s].device_bytes = S ? S->arena_bytes + S->T->table_bytes : 0;
+    fill_solve_info(b, s, &infos[s]);
   }
   return MHD_OK;
 }
@@ -1630,8 +1776,7 @@ static void fill_infos(mhd_batch *b, const SolveState *hs, mhd_info *infos) {
     infos[s].step = st.step;
     infos[s].status = st.status;
     infos[s].remaining = st.remaining;
-    const Solve *S = b->slots[s];
-    infos[s].device_bytes = S ? S->arena_bytes + S->T->table_bytes : 0;
+    fill_solve_info(b, s, &infos[s]);
   }
 }
 

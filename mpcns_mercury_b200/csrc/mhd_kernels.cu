@@ -55,6 +55,7 @@ constexpr int cBFX = kComp.first[MHD_HODGE_FACE_XI], cBFY = kComp.first[MHD_HODG
 constexpr int cALX = kComp.first[MHD_HODGE_EDGE_XI], cALY = kComp.first[MHD_HODGE_EDGE_ETA],
               cALZ = kComp.first[MHD_HODGE_EDGE_ZETA];
 constexpr int cWB = kComp.first[MHD_BCELL_W], cWJ = kComp.first[MHD_JCELL_W];
+static_assert(cBFY == cBFX + 1 && cBFZ == cBFX + 2 && cALY == cALX + 1 && cALZ == cALX + 2, "xi, eta, zeta consecutive");
 constexpr int cBAX = kComp.first[MHD_BADD_XI], cBAY = kComp.first[MHD_BADD_ETA], cBAZ = kComp.first[MHD_BADD_ZETA];
 constexpr int cPHOTO = kComp.first[MHD_PHOTO], cCX = kComp.first[MHD_CELL_X];  // CELL_Y, CELL_Z follow
 constexpr int cTPX = kComp.first[MHD_TAPER_XI], cTPY = kComp.first[MHD_TAPER_ETA], cTPZ = kComp.first[MHD_TAPER_ZETA];
@@ -95,6 +96,7 @@ struct V {
 
 struct Item {
   int s;       // solve
+  int blk;     // block of the solve
   int species; // kCells2 only
   int i, j, k;
   bool in;     // inside the kernel's range
@@ -141,6 +143,7 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
     const RangeBox r = range_of(KIND, DB.n, S.c.nghost);
     Item it;
     it.s = s;
+    it.blk = b;
     it.species = 0;
     for (int a = 0; a < 3; ++a) {
       it.hi[a] = r.hi[a];
@@ -1000,6 +1003,14 @@ __global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op, double 
         }
         case RES_E_FROM_P: B.c(cEX + a)[o] = dof ? *p : R(0.0); break;  // UnpackVecToImplicitEres_ (:294-312)
         case RES_E_FROM_X: B.c(cEX + a)[o] = dof ? *x : R(0.0); break;
+        case RES_RESTART:  // CG on the right-hand side already in r: x = 0, p = r
+          *x = R(0.0);
+          *p = dof ? *r : R(0.0);
+          break;
+        case RES_P_FROM_X: *p = dof ? *x : R(0.0); break;
+        case RES_RESID:  // r = b - q, b kept in the B* snapshot arrays (FP64 companion of a mixed solve)
+          *r = dof ? B.c(cRBS + a)[o] - B.c(cRQ + a)[o] : R(0.0);
+          break;
         case RES_AXPY:
           if (dof) {
             *x += R(s) * *p;
@@ -1560,6 +1571,50 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
 // approximate division and square root); the FP64 one keeps the bit-exact
 // flags.
 #if MHD_KERNELS_F32
+// Vectors of the mixed-precision implicit substep between a solve's FP32
+// arena (the masked solve of D) and its FP64 companion (cblocks: the
+// companion's blocks, the same boxes), over the whole box:
+// RES_X_SETUP: companion alpha, beta, eta, W = the solve's (widened); the
+//   companion's b (B* snapshot arrays) and r = the solve's r (the FP32
+//   right-hand side eta J(B*)); companion x = 0.
+// RES_X_DEMOTE_R: r = (float) companion r (the next correction's right-hand side).
+// RES_X_ADD_X: companion x += x (the correction).
+// RES_X_DEMOTE_X: x = (float) companion x (the solution).
+__global__ void __launch_bounds__(kTileThreads) k_res_cross(Dir D, const DevBlock *cblocks, int op) {
+  for_items<float, kFull>(D, [&](const DevSolve &S, const V<float> &B, const Item &it) {
+    if (!it.in) return;
+    const DevBlock &CB = cblocks[it.blk];
+    V<double> C;
+    C.U = C.Un = nullptr;
+    C.M = CB.M;
+    C.total = (int)CB.total;
+    C.si = (int)CB.si;
+    C.sj = (int)CB.sj;
+    C.G = CB.G;
+    C.n0 = CB.n[0];
+    C.n1 = CB.n[1];
+    C.n2 = CB.n[2];
+    const int o = B.off(it.i, it.j, it.k), oc = C.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) {
+      switch (op) {
+        case RES_X_SETUP:
+          for (int c : {cALX, cBFX, cETAR, cRW}) C.c(c + a)[oc] = (double)B.c(c + a)[o];
+          C.c(cRBS + a)[oc] = C.c(cRR + a)[oc] = (double)B.c(cRR + a)[o];
+          C.c(cRX + a)[oc] = 0.0;
+          break;
+        case RES_X_DEMOTE_R: B.c(cRR + a)[o] = (float)C.c(cRR + a)[oc]; break;
+        case RES_X_ADD_X: C.c(cRX + a)[oc] += (double)B.c(cRX + a)[o]; break;
+        default: B.c(cRX + a)[o] = (float)C.c(cRX + a)[oc]; break;  // RES_X_DEMOTE_X
+      }
+    }
+  });
+}
+
+void launch_res_cross(const Dir &D, const DevBlock *cblocks, int op, cudaStream_t st) {
+  grids<float>();
+  k_res_cross<<<g_grid_tiles, kTileThreads, 0, st>>>(D, cblocks, op);
+}
+
 void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
                             ResScratch rs) {
   grids<float>();

@@ -28,7 +28,7 @@ struct SyncOps {
 };
 
 // Operations of SK_RES_VEC / SK_RES_DOT / SK_RES_COPYB (the arg of the launch).
-enum ResVecOp { RES_INIT = 0, RES_E_FROM_P, RES_E_FROM_X, RES_AXPY, RES_PUPD };
+enum ResVecOp { RES_INIT = 0, RES_E_FROM_P, RES_E_FROM_X, RES_AXPY, RES_PUPD, RES_RESTART, RES_P_FROM_X, RES_RESID };
 enum ResDotOp { RES_DOT_PQ = 0, RES_DOT_RR };
 enum ResCopyOp { RES_SNAPSHOT = 0, RES_RESTORE };
 
@@ -44,6 +44,11 @@ struct ResScratch {
 void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision, int iarg = 0,
                         double darg = 0.0, ResScratch rs = ResScratch{nullptr, nullptr});
 int res_dot_grid();
+// Mixed-precision implicit substep: moves its vectors between the masked
+// solve of the FP32 directory D and the solve's FP64 companion, whose blocks
+// are cblocks (k_res_cross, FP32 translation unit).
+enum ResCrossOp { RES_X_SETUP = 0, RES_X_DEMOTE_R, RES_X_ADD_X, RES_X_DEMOTE_X };
+void launch_res_cross(const Dir &D, const DevBlock *cblocks, int op, cudaStream_t st);
 // Queries every kernel's resident CTAs per SM once (call before any stream capture).
 void init_launch_grids();
 const char *step_kernel_name(StepKernel k);

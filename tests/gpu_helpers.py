@@ -9,26 +9,31 @@ from mpcns_mercury_b200.capi import REF_FIELD
 NGHOST = 4
 
 
-def context_from_dump(dump, n, tag="step0:", cfl=0.4, precision=0, constants=None):
-    """Upload the reference's step-0 state and static inputs into a new context."""
-    ctx = Context([(n, n, n)], NGHOST, constants or reference_constants(cfl=cfl), precision=precision)
+def upload_from_dump(upload, dump, tag="step0:"):
+    """upload(field, data, lo, hi) of the reference's state at ``tag`` and its static inputs."""
     for name in mo.STATE_FIELDS:
         r = dump[(tag + name, 0)]
-        ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
+        upload(REF_FIELD[name], r.data, r.lo, r.hi)
     for name in mo.STATIC_FIELDS + ["taper_xi", "taper_eta", "taper_zeta"]:
         r = dump[("static:" + name, 0)]
-        ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
+        upload(REF_FIELD[name], r.data, r.lo, r.hi)
     for name in ("local_arti_eta_xi", "local_arti_eta_eta", "local_arti_eta_zeta", "eta_res_xi", "eta_res_eta",
                  "eta_res_zeta"):
         if ("static:" + name, 0) in dump:
             r = dump[("static:" + name, 0)]
-            ctx.upload(REF_FIELD[name], r.data, r.lo, r.hi)
+            upload(REF_FIELD[name], r.data, r.lo, r.hi)
     # cell centres: the reference reads dual_x(i+1, j+1, k+1) for cell (i, j, k)
     for ax, fld in zip("xyz", ("CELL_X", "CELL_Y", "CELL_Z")):
         r = dump[("dual_" + ax, 0)]
         lo = tuple(v - 1 for v in r.lo)
         hi = tuple(v - 1 for v in r.hi)
-        ctx.upload(fld, r.data, lo, hi)
+        upload(fld, r.data, lo, hi)
+
+
+def context_from_dump(dump, n, tag="step0:", cfl=0.4, precision=0, constants=None):
+    """Upload the reference's step-0 state and static inputs into a new context."""
+    ctx = Context([(n, n, n)], NGHOST, constants or reference_constants(cfl=cfl), precision=precision)
+    upload_from_dump(ctx.upload, dump, tag)
     return ctx
 
 

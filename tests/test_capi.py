@@ -66,3 +66,22 @@ def test_struct_layouts_match_header():
     want = [ctypes.sizeof(capi.MhdDesc), ctypes.sizeof(capi.MhdConstants), ctypes.sizeof(capi.MhdCopy),
             ctypes.sizeof(capi.MhdInfo), ctypes.sizeof(capi.MhdAliasClasses)]
     assert got == want
+
+
+def test_mixed_resistive_solve_counts_its_fp64_companion():
+    """mhd_desc_device_bytes of a mixed-precision solve with the implicit
+    substep includes the FP64 companion that holds the refinement's residual."""
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200.capi import SolveDesc
+
+    cells = [(16, 16, 16)]
+    res, plain = reference_constants(cfl=0.4, resistive=True), reference_constants(cfl=0.4)
+    by = {}
+    for key, k, prec in (("mixed_res", res, 1), ("mixed", plain, 1), ("fp64_res", res, 0), ("fp64", plain, 0)):
+        d = SolveDesc(cells, 3, k, precision=prec)
+        by[key] = d.device_bytes()
+        d.close()
+    # the substep's 18 work arrays: 8 bytes each in FP64, 4 in mixed
+    res_arrays_fp64 = by["fp64_res"] - by["fp64"]
+    assert res_arrays_fp64 > 0
+    assert by["mixed_res"] == by["mixed"] + res_arrays_fp64 // 2 + by["fp64_res"]
