@@ -644,6 +644,101 @@ def run_serving(args, rank, world, device):
     return line
 
 
+# ------------------------------------------------------------------ implicit substep
+# Algorithmic bytes of one CG iteration per unknown: about 21 words touched
+# per edge unknown (the operator's E from p, dB = -dt curl E, dJ = alpha
+# C^T beta dB, q = E - eta dJ, and the vector updates and dot products), in
+# the substep's real type.
+RES_WORDS_PER_DOF_ITER = 21
+
+
+def run_implicit(args, rank, world, device):
+    """The implicit resistive substep on the periodic curvilinear n^3 cube
+    (Orszag-Tang, eta from the reference's radial window 0.84 < r < 1.04 with
+    eta_max_mercury 1.25e7), FP64 (CG) and mixed precision (FP32 CG inside
+    FP64 refinement), both to a relative residual of 1e-10.  The substep's
+    time is the step's time with it minus the step's time without it (same
+    inputs); value: CG unknown-iterations per second of the FP64 solve."""
+    import numpy as np
+    import torch
+
+    from mpcns_mercury_b200 import Context, reference_constants
+    from mpcns_mercury_b200 import setup as S
+
+    n = args.implicit_n
+    geom, f = S.cube_case(n)
+    eta = S.resistivity_eta(geom, reference_constants())
+    peak, peak_kind = load_peaks()
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+
+    def timed(precision, resistive):
+        k = reference_constants(cfl=0.4, resistive=resistive, res_rtol=1e-10, res_max_it=2000)
+        ctx = Context([(n, n, n)], 4, k, precision=precision)
+        for name in UPLOAD_FIELDS:
+            a = f[name]
+            ctx.upload(capi_field(name), a.data, a.lo, a.hi)
+        if resistive:
+            for name, a in eta.items():
+                ctx.upload(name.upper(), a.data, a.lo, a.hi)
+        ctx.sync("UCELL")
+        ctx.sync("BFACE")
+        ctx.prepare()
+        dofs = 0
+        if resistive:
+            w = ctx.download("RES_W", (0, 0, 0), (n + 1, n + 1, n + 1))
+            dofs = int(np.count_nonzero(w > 0.0))
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+        for _ in range(args.warmup):
+            ctx.step(1)
+        torch.cuda.synchronize()
+        ms, iters, refinements, relres = 0.0, 0, 0, 0.0
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.step(1)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            info = ctx.info()
+            iters += info.res_iters
+            refinements += info.res_refinements
+            relres = max(relres, info.res_relres)
+            assert info.status == 0, info.status
+        ctx.close()
+        return ms / args.steps, dofs, iters / args.steps, refinements / args.steps, relres
+
+    out = {}
+    if rank == 0:
+        sampler.start()
+    for prec, label in ((0, "fp64"), (1, "mixed")):
+        ms_res, dofs, it, ref, relres = timed(prec, True)
+        ms_plain, _, _, _, _ = timed(prec, False)
+        sub_ms = ms_res - ms_plain
+        dof_iters = dofs * it
+        word = 8 if prec == 0 else 4
+        gbs = RES_WORDS_PER_DOF_ITER * word * dof_iters / (sub_ms * 1e-3) / 1e9
+        out[label] = {"step_ms_with_substep": round(ms_res, 4), "step_ms_without": round(ms_plain, 4),
+                      "substep_ms": round(sub_ms, 4), "unknowns": dofs, "cg_iterations_per_step": round(it, 2),
+                      "refinements_per_step": round(ref, 2), "max_relres": relres,
+                      "us_per_cg_iteration": round(1e3 * sub_ms / max(it, 1e-9), 3),
+                      "dof_iterations_per_s": round(dof_iters / (sub_ms * 1e-3), 1),
+                      "achieved_gbs": round(gbs, 2), "frac_of_peak": round(gbs / peak, 4)}
+    clocks = sampler.stop() if rank == 0 else None
+    f64 = out["fp64"]
+    return {
+        "metric": "implicit resistive CG unknown-iterations/s", "value": f64["dof_iterations_per_s"],
+        "unit": "dof-iterations/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": f64["step_ms_with_substep"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "implicit", "cells": [n, n, n], "nghost": 4, "res_rtol": 1e-10,
+                   "eta": "reference window 0.84 < r < 1.04, eta_max_mercury 1.25e7", "l2": "not flushed",
+                   "bytes_per_dof_iteration": f"{RES_WORDS_PER_DOF_ITER} words of the real type",
+                   "peak_gbs": peak, "peak_source": peak_kind, **out},
+        "clocks": clocks,
+    }
+
+
 # ------------------------------------------------------------------ reference arm
 def reference_cubes(args):
     """Cubes (cells per axis) the reference build runs for a bounded sample of
@@ -746,7 +841,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="ensemble", help="ensemble (default), serve, cube32, cubeN")
+    ap.add_argument("--workload", default="ensemble", help="ensemble (default), serve, implicit, cube32, cubeN")
     ap.add_argument("--solves", type=int, default=64, help="ensemble: solves per GPU")
     ap.add_argument("--batched-only", action="store_true",
                     help="ensemble: run only the mixed batch (profiling; no plain/FP64 legs, no error check)")
@@ -755,6 +850,7 @@ def main():
     ap.add_argument("--shapes", type=int, default=16, help="serve: distinct request shapes")
     ap.add_argument("--capacity", type=int, default=64, help="serve: batch slots")
     ap.add_argument("--hbm-budget", type=float, default=100e9, help="serve: device bytes for admitted solves")
+    ap.add_argument("--implicit-n", type=int, default=64, help="implicit: cells per axis of the cube")
     ap.add_argument("--cpu-sample-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -785,6 +881,8 @@ def main():
             line = run_ensemble(args, rank, world, device)
         elif args.workload == "serve":
             line = run_serving(args, rank, world, device)
+        elif args.workload == "implicit":
+            line = run_implicit(args, rank, world, device)
         else:
             line = run_ours(args, rank, world, device)
     finally:

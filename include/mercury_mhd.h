@@ -106,8 +106,9 @@ typedef struct mhd_constants {
    * explicit update, solve (I + dt eta alpha C^T beta C) E = eta J(B*) on the
    * owned edges with eta > 0 (eta: MHD_ETA_RES_*), then B = B* - dt curl E.
    * Solved to ||A E - b|| <= res_rtol ||b||, else MHD_ERR_SOLVE.  FP64
-   * solves: preconditioned CG (at most res_max_it iterations; res_rtol 0 =
-   * 1e-13).  Mixed-precision solves: iterative refinement with the residual
+   * solves: preconditioned CG (at most res_max_it iterations, capped at
+   * 100000; res_rtol 0 = 1e-13), its iteration loop run on the device as a
+   * CUDA graph with a conditional loop node.  Mixed-precision solves: iterative refinement with the residual
    * A E - b and its norms in FP64 and each correction solved by FP32 CG (on
    * the solve's own FP32 edge fields) to 1e-4 of its right-hand side (at most
    * res_max_it iterations each, at most 30 refinements; res_rtol 0 = 1e-10). */

@@ -192,6 +192,7 @@ struct mhd_batch {
   int *dprefix_aliasE = nullptr, *dprefix_aliasJ = nullptr;
   cudaGraphExec_t graph = nullptr;
   cudaGraphExec_t graph_a = nullptr, graph_b = nullptr;  // the step split around implicit resistive solves
+  cudaGraphExec_t graph_cg = nullptr;                   // the CG iteration loop of the masked solve
   // solves whose pruned-halo (0) / owner (1) table of a group has entries:
   // sync phases empty in every solve get no launch in the step
   int live_tables[kMaxGroups][2] = {};
@@ -202,6 +203,7 @@ struct mhd_batch {
   bool borrowed = false;
   ResScratch res{nullptr, nullptr};
   double *hres = nullptr;                               // pinned copy of res.result
+  ResCG *hcg = nullptr;                                 // pinned copy of res.cg
   int kernels_per_step = 0;
   double *staging = nullptr;
   size_t staging_elems = 0;
@@ -827,7 +829,7 @@ bool count_tables(mhd_batch *b, const Solve *S, int d) {
 // The step graphs are captured again at the next run (call with no graph
 // launch in flight).
 void drop_graphs(mhd_batch *b) {
-  for (cudaGraphExec_t *g : {&b->graph, &b->graph_a, &b->graph_b})
+  for (cudaGraphExec_t *g : {&b->graph, &b->graph_a, &b->graph_b, &b->graph_cg})
     if (*g) {
       cudaGraphExecDestroy(*g);
       *g = nullptr;
@@ -848,42 +850,94 @@ int res_dot(mhd_batch *b, int op) {
 // q = A p (MatMultImplicitResistive_, Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:420-472):
 // E_res from p, its owner copies, dB = -dt curl E_res, Sync(dB), dJ, its
 // alias reduction and owner copies, q = E_res - eta dJ.
-void res_apply(mhd_batch *b, int *nk) {
-  launch(b, 1, SK_RES_VEC, nk, nullptr, RES_E_FROM_P);
+void res_apply_core(mhd_batch *b, int *nk) {  // from E_res (set) to dJ (synced)
   sync1(b, 1, copy_op(MHD_SYNC_EEDGE, 1), nk);
   launch(b, 1, SK_RES_DB, nk);
   enqueue_sync(b, 1, MHD_SYNC_BFACE, nk);
   launch(b, 1, SK_RES_DJ, nk);
   sync1(b, 1, alias_op(1), nk);
   sync1(b, 1, copy_op(MHD_SYNC_JEDGE, 1), nk);
+}
+void res_apply(mhd_batch *b, int *nk) {
+  launch(b, 1, SK_RES_VEC, nk, nullptr, RES_E_FROM_P);
+  res_apply_core(b, nk);
   launch(b, 1, SK_RES_Q, nk);
 }
 
-// CG iterations on the masked solve of b from x = 0 and r = p = the
-// right-hand side (rho = its W-weighted r.r), until ||r|| <= tol or max_it
-// iterations; *rnorm: the last ||r||, *iters: iterations taken.
-int res_cg(mhd_batch *b, double rho, double tol, int max_it, double *rnorm, int *iters, bool *converged) {
-  int rc, nk = 0;
-  *converged = *rnorm <= tol;
-  *iters = 0;
-  for (int it = 0; it < max_it && !*converged; ++it) {
-    res_apply(b, &nk);
-    if ((rc = res_dot(b, RES_DOT_PQ))) return rc;
-    const double pq = b->hres[0];
-    if (!(pq > 0.0)) break;  // breakdown: not positive definite on these unknowns
-    const double alpha = rho / pq;
-    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_AXPY, alpha);
-    ++*iters;
-    if ((rc = res_dot(b, RES_DOT_RR))) return rc;
-    const double rho_new = b->hres[0];
-    *rnorm = std::sqrt(b->hres[1]);
-    if (*rnorm <= tol) {
-      *converged = true;
-      break;
-    }
-    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_PUPD, rho_new / rho);
-    rho = rho_new;
+// The CG iteration loop of the masked solve as one CUDA graph: k_res_cg
+// (CG_INIT) sets the loop condition, then a conditional WHILE node repeats
+// the iteration (operator, q and (p.q)_W, the x / r update and the stop
+// test, the direction update) until the device CG state says it is over.
+// Captured once per batch (again after the tables change).
+int build_cg_graph(mhd_batch *b) {
+  if (b->graph_cg) return MHD_OK;
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaGraphCreate(&g, 0));
+  const bool prof = b->profiling;
+  b->profiling = false;  // no event records inside the graph
+  auto fin = [&](cudaError_t e, const char *what) {
+    b->profiling = prof;
+    cudaGraphDestroy(g);
+    return fail(MHD_ERR_CUDA, "CG graph, %s: %s", what, cudaGetErrorString(e));
+  };
+  cudaGraphConditionalHandle h = 0;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return fin(e, "condition");
+  b->res.handle = h;
+  int nk = 0;
+  if ((e = cudaStreamBeginCaptureToGraph(b->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return fin(e, "capture");
+  launch(b, 1, SK_RES_CG, &nk, nullptr, CG_INIT);
+  if ((e = cudaStreamEndCapture(b->stream, &g)) != cudaSuccess) return fin(e, "capture");
+  cudaGraphNode_t init = nullptr;
+  size_t n = 1;
+  if ((e = cudaGraphGetNodes(g, &init, &n)) != cudaSuccess || n != 1)
+    return fin(e != cudaSuccess ? e : cudaErrorUnknown, "init node");
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t loop = nullptr;
+  if ((e = cudaGraphAddNode(&loop, g, &init, 1, &p)) != cudaSuccess) return fin(e, "loop node");
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return fin(e, "body capture");
+  res_apply_core(b, &nk);
+  launch(b, 1, SK_RES_CG, &nk, nullptr, CG_PQ);
+  launch(b, 1, SK_RES_CG, &nk, nullptr, CG_RR);
+  launch(b, 1, SK_RES_PUPD_E, &nk);
+  if ((e = cudaStreamEndCapture(b->stream, &body)) != cudaSuccess) return fin(e, "body capture");
+  e = cudaGraphInstantiate(&b->graph_cg, g, 0);
+  b->profiling = prof;
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    b->graph_cg = nullptr;
+    return fail(MHD_ERR_CUDA, "CG graph instantiate: %s", cudaGetErrorString(e));
   }
+  return MHD_OK;
+}
+
+// CG on the masked solve from x = 0 and r = p = the right-hand side
+// (already set) until ||r|| <= tol_factor ||r_0|| or max_it iterations, the
+// loop on the device (build_cg_graph); one host round trip at the end.
+int res_cg(mhd_batch *b, double tol_factor, int max_it, double *r0, double *rnorm, int *iters, bool *converged) {
+  int rc = build_cg_graph(b);
+  if (rc) return rc;
+  ResCG *h = b->hcg;
+  *h = ResCG{};
+  h->tol_factor = tol_factor;
+  h->max_it = std::max(0, std::min(max_it, 100000));  // the loop runs on the device: a hard bound
+  CUDA_TRY(cudaMemcpyAsync(b->res.cg, h, sizeof(ResCG), cudaMemcpyHostToDevice, b->stream));
+  CUDA_TRY(cudaGraphLaunch(b->graph_cg, b->stream));
+  CUDA_TRY(cudaMemcpyAsync(h, b->res.cg, sizeof(ResCG), cudaMemcpyDeviceToHost, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  *r0 = h->r0;
+  *rnorm = h->rnorm;
+  *iters = h->it;
+  *converged = h->converged != 0;
   return MHD_OK;
 }
 
@@ -933,11 +987,10 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
     // the correction: FP32 CG on r rounded to FP32, x += d in FP64
     launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_R, st);
     launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
-    if ((rc = res_dot(b, RES_DOT_RR))) return rc;
-    double r32 = std::sqrt(b->hres[1]);
+    double r32_0 = 0.0, r32 = 0.0;
     int iters = 0;
     bool inner = false;
-    if ((rc = res_cg(b, b->hres[0], kInnerRtol * r32, S->res_max_it, &r32, &iters, &inner))) return rc;
+    if ((rc = res_cg(b, kInnerRtol, S->res_max_it, &r32_0, &r32, &iters, &inner))) return rc;
     launch_res_cross(Dm, C->dblocks, RES_X_ADD_X, st);
     S->res_iters += iters;
     ++S->res_refinements;
@@ -969,11 +1022,9 @@ int res_solve(mhd_batch *b, int slot) {
   if (S->shadow_slot >= 0) {
     if ((rc = res_refine(b, slot, S, &converged))) return rc;
   } else {
-    if ((rc = res_dot(b, RES_DOT_RR))) return rc;
-    const double bnorm = std::sqrt(b->hres[1]);
     const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-13;
-    double rn = bnorm;
-    if ((rc = res_cg(b, b->hres[0], rtol * bnorm, S->res_max_it, &rn, &S->res_iters, &converged))) return rc;
+    double bnorm = 0.0, rn = 0.0;
+    if ((rc = res_cg(b, rtol, S->res_max_it, &bnorm, &rn, &S->res_iters, &converged))) return rc;
     S->res_relres = bnorm > 0.0 ? rn / bnorm : 0.0;
     S->res_refinements = 0;
   }
@@ -1073,7 +1124,9 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
     return bail(fail(MHD_ERR_OOM, "prefix"));
   if (cudaMalloc(&b->res.partial, sizeof(double) * 2 * res_dot_grid()) != cudaSuccess ||
       cudaMalloc(&b->res.result, sizeof(double) * 2) != cudaSuccess ||
-      cudaMallocHost(&b->hres, sizeof(double) * 2) != cudaSuccess)
+      cudaMalloc(&b->res.cg, sizeof(ResCG)) != cudaSuccess ||
+      cudaMallocHost(&b->hres, sizeof(double) * 2) != cudaSuccess ||
+      cudaMallocHost(&b->hcg, sizeof(ResCG)) != cudaSuccess)
     return bail(fail(MHD_ERR_OOM, "solver scratch"));
   if (cudaMemsetAsync(b->dstate, 0, sizeof(SolveState) * capacity, b->stream) != cudaSuccess)
     return bail(fail(MHD_ERR_CUDA, "state init"));
@@ -1091,9 +1144,12 @@ int mhd_batch_destroy(mhd_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->graph_a) cudaGraphExecDestroy(b->graph_a);
   if (b->graph_b) cudaGraphExecDestroy(b->graph_b);
+  if (b->graph_cg) cudaGraphExecDestroy(b->graph_cg);
   cudaFree(b->res.partial);
   cudaFree(b->res.result);
+  cudaFree(b->res.cg);
   if (b->hres) cudaFreeHost(b->hres);
+  if (b->hcg) cudaFreeHost(b->hcg);
   for (auto *S : b->slots) free_solve(S, b->stream);
   if (b->staging) cudaFreeAsync(b->staging, b->stream);
   if (b->stream) cudaStreamSynchronize(b->stream);

@@ -1132,6 +1132,148 @@ __global__ void k_res_sum(const double *partial, int n, double *result) {
   }
 }
 
+// One step of the CG iteration with its dot product, the scalar update done
+// by the last CTA to finish (no host round trip).  The last CTA sums the
+// per-CTA partials with all its threads in a fixed order (thread t takes
+// CTAs t, t + 256, ...; then a fixed tree), so the sums are deterministic,
+// then sets the loop condition of the graph (CG_INIT, CG_RR); CG_PQ clears
+// it first, so a loop whose stop test did not run ends.
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_cg(Dir D, int op, double *partial, ResCG *cg,
+                                                         cudaGraphConditionalHandle handle) {
+  __shared__ double sh[2][kTileThreads / 32];
+  __shared__ unsigned int ticket;
+  __shared__ double tot[2];
+  if (op == CG_PQ && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
+  const bool skip = op == CG_RR && cg->done != 0;  // breakdown in CG_PQ
+  const R alpha = R(cg->alpha);
+  double acc0 = 0.0, acc1 = 0.0;
+  if (!skip)
+    for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+      if (!it.in) return;
+      const int o = B.off(it.i, it.j, it.k);
+      for (int a = 0; a < 3; ++a) {
+        const R wr = B.c(cRW + a)[o];
+        const bool dof = wr > R(0.0);
+        const double w = (double)wr;
+        R *x = B.c(cRX + a) + o, *r = B.c(cRR + a) + o, *p = B.c(cRP + a) + o, *q = B.c(cRQ + a) + o;
+        if (op == CG_INIT) {
+          B.c(cEX + a)[o] = dof ? *p : R(0.0);
+          if (w > 0.0) {
+            const double rv = (double)*r;
+            acc0 += w * rv * rv;
+            acc1 += rv * rv;
+          }
+        } else if (op == CG_PQ) {
+          const R qv = dof ? B.c(cEX + a)[o] - B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
+          *q = qv;
+          if (w > 0.0) acc0 += w * (double)*p * (double)qv;
+        } else {
+          if (dof) {
+            *x += alpha * *p;
+            *r -= alpha * *q;
+          }
+          if (w > 0.0) {
+            const double rv = (double)*r;
+            acc0 += w * rv * rv;
+            acc1 += rv * rv;
+          }
+        }
+      }
+    });
+  for (int of = 16; of > 0; of >>= 1) {
+    acc0 += __shfl_xor_sync(0xffffffffu, acc0, of);
+    acc1 += __shfl_xor_sync(0xffffffffu, acc1, of);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = acc0;
+    sh[1][threadIdx.x >> 5] = acc1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < kTileThreads / 32; ++w) {
+      s0 += sh[0][w];
+      s1 += sh[1][w];
+    }
+    partial[2 * blockIdx.x] = s0;
+    partial[2 * blockIdx.x + 1] = s1;
+    __threadfence();
+    ticket = atomicAdd(&cg->arrivals, 1u);
+  }
+  __syncthreads();
+  if (ticket != gridDim.x - 1) return;  // the whole CTA agrees
+  __threadfence();
+  double u0 = 0.0, u1 = 0.0;
+  for (unsigned q = threadIdx.x; q < gridDim.x; q += kTileThreads) {
+    u0 += __ldcg(partial + 2 * q);
+    u1 += __ldcg(partial + 2 * q + 1);
+  }
+  for (int of = 16; of > 0; of >>= 1) {
+    u0 += __shfl_xor_sync(0xffffffffu, u0, of);
+    u1 += __shfl_xor_sync(0xffffffffu, u1, of);
+  }
+  __syncthreads();  // sh is reused
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = u0;
+    sh[1][threadIdx.x >> 5] = u1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v0 = 0.0, v1 = 0.0;
+    for (int w = 0; w < kTileThreads / 32; ++w) {
+      v0 += sh[0][w];
+      v1 += sh[1][w];
+    }
+    tot[0] = v0;
+    tot[1] = v1;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double t0 = tot[0], t1 = tot[1];
+  cg->arrivals = 0;
+  if (op == CG_INIT) {
+    cg->rho = t0;
+    cg->r0 = cg->rnorm = sqrt(t1);
+    cg->tol = cg->tol_factor * cg->r0;
+    cg->it = 0;
+    cg->converged = cg->rnorm <= cg->tol;
+    cg->done = cg->converged || cg->max_it <= 0;
+    cudaGraphSetConditional(handle, cg->done ? 0u : 1u);
+  } else if (op == CG_PQ) {
+    if (!(t0 > 0.0)) cg->done = 1;  // breakdown: not positive definite on these unknowns
+    else cg->alpha = cg->rho / t0;
+  } else {
+    if (!skip) {
+      cg->it += 1;
+      cg->rnorm = sqrt(t1);
+      if (cg->rnorm <= cg->tol) cg->converged = cg->done = 1;
+      else if (cg->it >= cg->max_it) cg->done = 1;
+      cg->beta = t0 / cg->rho;
+      cg->rho = t0;
+    }
+    cudaGraphSetConditional(handle, cg->done ? 0u : 1u);
+  }
+}
+
+// p = r + beta p and E_res = p on the unknowns (the next iteration's
+// operator input), unless the loop is over.
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_pupd_e(Dir D, const ResCG *cg) {
+  if (cg->done) return;
+  const R beta = R(cg->beta);
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int o = B.off(it.i, it.j, it.k);
+    for (int a = 0; a < 3; ++a) {
+      const bool dof = B.c(cRW + a)[o] > R(0.0);
+      R *p = B.c(cRP + a) + o;
+      if (dof) *p = B.c(cRR + a)[o] + beta * *p;
+      B.c(cEX + a)[o] = dof ? *p : R(0.0);
+    }
+  });
+}
+
 // B* snapshot / restore over the whole box (SnapshotImplicitResistiveBstar_,
 // RestoreImplicitResistiveBstar_, :260-292).
 template <class R>
@@ -1504,6 +1646,8 @@ static const void *kernel_fn(StepKernel k) {
     case SK_RES_Q: return (const void *)k_res_q<R>;
     case SK_RES_COPYB: return (const void *)k_res_copyb<R>;
     case SK_RES_BUPDATE: return (const void *)k_res_bupdate<R>;
+    case SK_RES_CG: return (const void *)k_res_cg<R>;
+    case SK_RES_PUPD_E: return (const void *)k_res_pupd_e<R>;
     default: return nullptr;
   }
 }
@@ -1560,6 +1704,8 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_RES_SUM: k_res_sum<<<1, 32, 0, st>>>(rs.partial, g_grid_tiles, rs.result); break;
     case SK_RES_COPYB: k_res_copyb<R><<<G, kTileThreads, 0, st>>>(D, iarg); break;
     case SK_RES_BUPDATE: k_res_bupdate<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_RES_CG: k_res_cg<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.partial, rs.cg, rs.handle); break;
+    case SK_RES_PUPD_E: k_res_pupd_e<R><<<G, kTileThreads, 0, st>>>(D, rs.cg); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
     default: break;
@@ -1653,7 +1799,9 @@ const char *step_kernel_name(StepKernel k) {
                                 "k_fluid",    "k_bface",    "k_bcell_jedge", "k_jcell",   "k_pv_uplus",
                                 "k_sync",     "k_flip",     "k_retire",      "k_face_normals", "k_div_b",
                                 "k_res_seed", "k_res_w",    "k_res_vec",     "k_res_db",   "k_res_dj",
-                                "k_res_q",    "k_res_dot",  "k_res_sum",     "k_res_copyb", "k_res_bupdate"};
+                                "k_res_q",    "k_res_dot",  "k_res_sum",     "k_res_copyb", "k_res_bupdate",
+                                "k_res_cg",   "k_res_pupd_e"};
+  static_assert(sizeof(names) / sizeof(names[0]) == SK_COUNT, "a name per kernel");
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }
 #endif  // MHD_KERNELS_F32

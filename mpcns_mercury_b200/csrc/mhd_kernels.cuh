@@ -11,7 +11,7 @@ enum StepKernel {
   SK_JCELL, SK_PV_UPLUS, SK_SYNC, SK_FLIP, SK_RETIRE, SK_FACE_NORMALS, SK_DIVB,
   // implicit resistive substep
   SK_RES_SEED, SK_RES_W, SK_RES_VEC, SK_RES_DB, SK_RES_DJ, SK_RES_Q, SK_RES_DOT, SK_RES_SUM, SK_RES_COPYB,
-  SK_RES_BUPDATE, SK_COUNT
+  SK_RES_BUPDATE, SK_RES_CG, SK_RES_PUPD_E, SK_COUNT
 };
 
 // One launch of k_sync runs up to two independent sync operations: a copy
@@ -32,10 +32,30 @@ enum ResVecOp { RES_INIT = 0, RES_E_FROM_P, RES_E_FROM_X, RES_AXPY, RES_PUPD, RE
 enum ResDotOp { RES_DOT_PQ = 0, RES_DOT_RR };
 enum ResCopyOp { RES_SNAPSHOT = 0, RES_RESTORE };
 
-// Scratch of the CG dot products: per-CTA partial sums and the two results.
+// CG state of the masked solve on the device, for the iteration loop run as
+// a CUDA graph (k_res_cg, k_res_pupd_e): the host sets tol_factor and max_it
+// (and zeros the rest) before the graph and reads it back after.
+struct ResCG {
+  double rho, alpha, beta;  // W-weighted r.r, step length, direction update
+  double r0, rnorm, tol;    // ||r|| at the start and now, stop when rnorm <= tol = tol_factor * r0
+  double tol_factor;
+  int it, max_it;           // iterations taken, at most max_it
+  int done, converged;      // loop over (converged, max_it reached, or breakdown)
+  unsigned int arrivals;    // CTAs finished with the current dot product
+  int pad_;
+};
+// Steps of k_res_cg: CG_INIT: E = p, (r.r)_W and r.r, sets rho, r0, tol;
+// CG_PQ: q = A p (its last part, E - eta dJ) and (p.q)_W, sets alpha;
+// CG_RR: x += alpha p, r -= alpha q, (r.r)_W and r.r, the stop test and beta.
+enum ResCgOp { CG_INIT = 0, CG_PQ, CG_RR };
+
+// Scratch of the CG dot products: per-CTA partial sums and the two results;
+// the device CG state and the graph's loop condition.
 struct ResScratch {
   double *partial;  // 2 * grid
   double *result;   // 2
+  ResCG *cg = nullptr;
+  unsigned long long handle = 0;  // cudaGraphConditionalHandle of the loop
 };
 
 // Launch one engine kernel over the directory D (ops: SK_SYNC only) in the

@@ -375,6 +375,37 @@ def _pinv_sym3(M: np.ndarray) -> np.ndarray:
 
 
 # ------------------------------------------------------------------ sources
+def resistivity_eta(geom: Geometry, constants, eta_max: float = 1.25e7, r_inner: float = 0.84,
+                    r_outer: float = 1.04, width: float = 0.02) -> dict:
+    """Per-edge eta of the implicit resistive substep (ImplicitResistiveEtaAtEdge_,
+    Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:222-258) on the owned
+    edges, zero elsewhere: inver_Rem * window(r), r = |midpoint| of the edge,
+    window = min(1, 0.5 (tanh((r - r_inner) / width) - tanh((r - r_outer) / width)))
+    and 0 at or below 1e-10 (MercuryResistivityShape_,
+    Z4_Mercury/src/physics/MercurySolver_Tools.cpp:50-69), inver_Rem = eta_max /
+    (mu0 U_ref L_ref) (Tools.cpp:44); 0 on collapsed edges (|dl| <= 1e-12).
+    Returns {"eta_res_xi" | "eta_res_eta" | "eta_res_zeta": Arr}."""
+    inv_rem = eta_max / (constants.mu0 * constants.U_ref * constants.L_ref)
+    out = {}
+    for axis, name in enumerate(("eta_res_xi", "eta_res_eta", "eta_res_zeta")):
+        stag = tuple(0 if a == axis else 1 for a in range(3))
+        eo = tuple(1 if a == axis else 0 for a in range(3))
+        lo, hi = geom.alloc_range(stag, geom.g)
+        ilo, ihi = (0, 0, 0), tuple(geom.n[a] + stag[a] for a in range(3))
+        p0, p1 = geom.N(ilo, ihi), geom.N(ilo, ihi, *eo)
+        xm, ym, zm = (0.5 * (p0[a] + p1[a]) for a in range(3))
+        r = np.sqrt(xm * xm + ym * ym + zm * zm)
+        shape = 0.5 * (np.tanh((r - r_inner) / width) - np.tanh((r - r_outer) / width))
+        shape = np.where(np.isfinite(shape) & (shape > 1e-10), np.minimum(1.0, shape), 0.0)
+        dl = geom.fields[("dl_xi", "dl_eta", "dl_zeta")[axis]]
+        dlv = dl.data[dl.sl(ilo, ihi)][..., 0]
+        data = np.zeros(tuple(hi[a] - lo[a] for a in range(3)) + (1,))
+        arr = Arr(lo, hi, data)
+        data[arr.sl(ilo, ihi)] = np.where(np.abs(dlv) <= 1e-12, 0.0, inv_rem * shape)[..., None]
+        out[name] = arr
+    return out
+
+
 def photo_rate(geom: Geometry, L_ref: float = 2.44e6):
     """Neutral Na [cm^-3] and Na+ production rate [cm^-3 s^-1] on the cell range
     [-g, n + g), Initial_Na_And_PhotoRate_ (Z4_Mercury/include/2_Initial.h:227-440)."""

@@ -53,3 +53,24 @@ def test_seeded_initial_state_matches(both, name):
     r = d[("step0:" + name, 0)]
     a = f[name]
     assert np.array_equal(_owned(a.data, a.lo, a.hi), _owned(r.data, r.lo, r.hi))
+
+
+def test_resistivity_eta_matches_reference(ref_oracle):
+    """Edge eta of the implicit substep against the reference's own
+    ImplicitResistiveEtaAtEdge_ (eta_max_mercury 1.25e7, window 0.84..1.04)."""
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200 import setup as S
+
+    n = 6
+    d = ref_oracle.cube_run(n=n, steps=0, dump_at=[0], extra=dict(resistive=1))
+    geom, _ = S.cube_case(n)
+    eta = S.resistivity_eta(geom, reference_constants())
+    nonzero = 0
+    for name, a in eta.items():
+        r = d[("static:" + name, 0)]
+        x, y = _owned(a.data, a.lo, a.hi), _owned(r.data, r.lo, r.hi)
+        assert x.shape == y.shape
+        assert np.array_equal(x == 0.0, y == 0.0), name
+        assert np.max(np.abs(x - y)) <= 1e-14 * np.max(np.abs(y)), name
+        nonzero += int(np.count_nonzero(y))
+    assert nonzero > 0
