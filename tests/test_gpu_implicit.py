@@ -125,3 +125,27 @@ def test_mixed_precision_implicit_in_a_batch(res_dump):
     b.remove(s0)
     b.close()
     d.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_unconverged_substep_reports_solve_status(res_dump, precision):
+    """A solve capped below convergence ends its device loop at res_max_it
+    and the step returns MHD_ERR_SOLVE (the reference throws there)."""
+    from gpu_helpers import context_from_dump
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200.capi import MhdError
+
+    # one CG iteration per solve: the operator needs about 200 to reach 1e-10
+    k = reference_constants(cfl=0.4, resistive=True, res_rtol=1e-14, res_max_it=1)
+    ctx = context_from_dump(res_dump, 16, precision=precision, constants=k)
+    ctx.prepare()
+    with pytest.raises(MhdError):
+        ctx.step(1)
+    info = ctx.info()
+    assert info.status == 6  # MHD_ERR_SOLVE
+    if precision == 0:
+        assert info.res_iters == 1 and info.res_refinements == 0
+    else:  # 30 refinements of one FP32 iteration each
+        assert info.res_refinements == 30 and info.res_iters == 30
+    assert info.res_relres > 1e-14
+    ctx.close()
