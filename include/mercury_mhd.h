@@ -371,6 +371,17 @@ const char *mhd_last_error(void);
  * owned by the returned handle. */
 typedef struct mhd_topology mhd_topology;
 int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghost, mhd_topology **out);
+/* A box periodic in every direction cut into blocks[0] x blocks[1] x
+ * blocks[2] aligned blocks of cells[3] cells each, joined face to face
+ * (block id (p * blocks[1] + q) * blocks[2] + r for lattice position
+ * (p, q, r)): the sync tables and edge alias classes the reference builds
+ * for such inner patches (Grid::Read_Inner_Boundary,
+ * src/1_grid/1_MPCNS_Grid.cpp:400-517; TopologyBuilder.cpp:436;
+ * HaloBuild.cpp:382-540).  A block needs at least nghost cells along every
+ * axis.  The descriptor it fills has blocks[0] * blocks[1] * blocks[2]
+ * blocks. */
+int mhd_topology_periodic_lattice(const int32_t cells[3], const int32_t blocks[3], int32_t nghost,
+                                  mhd_topology **out);
 int mhd_topology_fill_desc(const mhd_topology *topo, mhd_desc *desc);
 int mhd_topology_destroy(mhd_topology *topo);
 

@@ -119,7 +119,7 @@ class MhdRestartImage(ctypes.Structure):
 EXPORTS = [
     "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
-    "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block",
+    "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block", "mhd_topology_periodic_lattice",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
     "mhd_save_restart", "mhd_load_restart", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
@@ -168,6 +168,7 @@ def lib() -> ctypes.CDLL:
                                   i32p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), i32p]
     L.mhd_last_error.restype = ctypes.c_char_p
     L.mhd_topology_periodic_block.argtypes = [i32p, ctypes.c_int32, ctypes.POINTER(P)]
+    L.mhd_topology_periodic_lattice.argtypes = [i32p, i32p, ctypes.c_int32, ctypes.POINTER(P)]
     L.mhd_topology_fill_desc.argtypes = [P, ctypes.POINTER(MhdDesc)]
     L.mhd_topology_destroy.argtypes = [P]
     L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
@@ -384,7 +385,10 @@ class Context:
 class SolveDesc:
     """A solve descriptor (mhd_desc) with the storage it points to kept alive."""
 
-    def __init__(self, cells, nghost: int, constants: MhdConstants, precision: int = 0):
+    def __init__(self, cells, nghost: int, constants: MhdConstants, precision: int = 0, lattice=None):
+        """cells: cells per block.  One block: periodic in every direction.
+        lattice=(bx, by, bz): the blocks (bx * by * bz equal ones, in the
+        order of mhd_topology_periodic_lattice) tile a periodic box."""
         L = lib()
         self._cells = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
         self.desc = MhdDesc()
@@ -394,7 +398,13 @@ class SolveDesc:
         self.desc.precision = precision
         self.desc.constants = constants
         self._topo = ctypes.c_void_p()
-        if len(cells) == 1:
+        if lattice is not None:
+            if len(cells) != lattice[0] * lattice[1] * lattice[2] or any(tuple(c) != tuple(cells[0]) for c in cells):
+                raise ValueError("a lattice has bx * by * bz blocks of equal cells")
+            check(L.mhd_topology_periodic_lattice(_i3(cells[0]), _i3(lattice), nghost, ctypes.byref(self._topo)),
+                  "mhd_topology_periodic_lattice")
+            check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
+        elif len(cells) == 1:
             check(L.mhd_topology_periodic_block(_i3(cells[0]), nghost, ctypes.byref(self._topo)),
                   "mhd_topology_periodic_block")
             check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")

@@ -1,6 +1,7 @@
 // Host-side topology builder: flattened sync tables (explicit copy lists,
 // the reference's format) and edge alias classes for one block that is
-// periodic in every direction, from the walks of mhd_periodic.h.
+// periodic in every direction, or for a periodic box cut into a lattice of
+// aligned blocks, from the walks of mhd_periodic.h.
 #include <cstdint>
 #include <memory>
 #include <new>
@@ -74,6 +75,42 @@ void build_alias(mhd_topology *t, const int n[3]) {
   mhd::periodic::alias_classes(n, t->alias_offset, t->alias_member, t->alias_msign, t->alias_owner, t->alias_osign);
 }
 
+// The lattice's tables: one task per (block, field component), counted and
+// then written in place, as build_groups.
+void build_lattice_groups(mhd_topology *t, const int n[3], const Lattice &L, int g) {
+  struct Unit {
+    const GroupSpec *gs;
+    int field, m, blk;
+    size_t nh, no, oh, oo;
+  };
+  std::vector<Unit> units;
+  for (int blk = 0; blk < L.blocks(); ++blk)
+    for (const auto &gs : kGroups)
+      for (int field : gs.fields)
+        for (int m = 0; m < mhd::kFieldSpec[field].ncomp; ++m) units.push_back({&gs, field, m, blk, 0, 0, 0, 0});
+  const int nu = (int)units.size();
+  mhd::parallel_for(nu, [&](int u) {
+    Unit &U = units[u];
+    walk_lattice(*U.gs, U.field, U.m, n, L, U.blk, g, [&](const mhd_copy &, bool own) { ++(own ? U.no : U.nh); });
+  });
+  size_t nh[MHD_NUM_GROUPS] = {}, no[MHD_NUM_GROUPS] = {};
+  for (Unit &U : units) {
+    U.oh = nh[U.gs->group];
+    U.oo = no[U.gs->group];
+    nh[U.gs->group] += U.nh;
+    no[U.gs->group] += U.no;
+  }
+  for (int q = 0; q < MHD_NUM_GROUPS; ++q) {
+    t->halo[q].allocate(nh[q]);
+    t->owner[q].allocate(no[q]);
+  }
+  mhd::parallel_for(nu, [&](int u) {
+    const Unit &U = units[u];
+    mhd_copy *h = t->halo[U.gs->group].data() + U.oh, *o = t->owner[U.gs->group].data() + U.oo;
+    walk_lattice(*U.gs, U.field, U.m, n, L, U.blk, g, [&](const mhd_copy &c, bool own) { *(own ? o++ : h++) = c; });
+  });
+}
+
 }  // namespace
 
 extern "C" int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghost, mhd_topology **out) {
@@ -87,6 +124,30 @@ extern "C" int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghos
     build_groups(t, n, nghost);
     build_alias(t, n);
   } catch (...) {  // allocation or thread creation failed
+    delete t;
+    return MHD_ERR_OOM;
+  }
+  *out = t;
+  return MHD_OK;
+}
+
+extern "C" int mhd_topology_periodic_lattice(const int32_t cells[3], const int32_t blocks[3], int32_t nghost,
+                                             mhd_topology **out) {
+  if (!cells || !blocks || !out || nghost < 1) return MHD_ERR_ARG;
+  for (int a = 0; a < 3; ++a)
+    if (cells[a] < 2 || blocks[a] < 1) return MHD_ERR_ARG;
+  // a block's ghost layers come from its neighbours' owned DOFs, one block away
+  for (int a = 0; a < 3; ++a)
+    if (cells[a] < nghost) return MHD_ERR_ARG;
+  if ((int64_t)blocks[0] * blocks[1] * blocks[2] >= (1 << 15)) return MHD_ERR_ARG;
+  auto *t = new (std::nothrow) mhd_topology();
+  if (!t) return MHD_ERR_OOM;
+  const int n[3] = {cells[0], cells[1], cells[2]};
+  const Lattice L{{blocks[0], blocks[1], blocks[2]}};
+  try {
+    build_lattice_groups(t, n, L, nghost);
+    alias_classes_lattice(n, L, t->alias_offset, t->alias_member, t->alias_msign, t->alias_owner, t->alias_osign);
+  } catch (...) {
     delete t;
     return MHD_ERR_OOM;
   }

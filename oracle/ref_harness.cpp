@@ -262,6 +262,88 @@ void write_cube_case(const fs::path &geo) {
   write_text(geo / "boundary_condition" / "inner   0.txt", in.str());
 }
 
+// Case "lattice": the periodic curvilinear unit cube of the "cube" case cut
+// into bx x by x bz aligned blocks of n^3 cells each (block id
+// (p * by + q) * bz + r for lattice position (p, q, r)).  Every block face is
+// an inner patch joined to the neighbouring block's opposite face, listed
+// from both sides with the "cube" case's orientation marks; a patch that
+// wraps around the box carries negative block ids (periodic,
+// src/1_grid/1_MPCNS_Grid.cpp:455-464).  No physical or parallel patches.
+void write_lattice_case(const fs::path &geo) {
+  const int n = (int)job_int("n", 4);
+  int nb[3] = {2, 2, 2};
+  std::istringstream(job_str("nb", "2 2 2")) >> nb[0] >> nb[1] >> nb[2];
+  const double amp = job_dbl("amp", 0.05);
+  const int np = n + 1;
+  const double two_pi = 2.0 * std::acos(-1.0);
+  const int nblock = nb[0] * nb[1] * nb[2];
+  auto bid = [&](int p, int q, int r) { return (p * nb[1] + q) * nb[2] + r; };
+  std::vector<std::string> names(nblock, "Fluid");
+  std::vector<std::array<int, 3>> dims(nblock, {np, np, np});
+  std::vector<std::vector<double>> xyz(nblock);
+  for (int p = 0; p < nb[0]; ++p)
+    for (int q = 0; q < nb[1]; ++q)
+      for (int r = 0; r < nb[2]; ++r) {
+        const size_t m = (size_t)np * np * np;
+        std::vector<double> blk(3 * m);
+        for (int k = 0; k < np; ++k)
+          for (int j = 0; j < np; ++j)
+            for (int i = 0; i < np; ++i) {
+              const double a = (double)(p * n + i) / (nb[0] * n), b = (double)(q * n + j) / (nb[1] * n),
+                           c = (double)(r * n + k) / (nb[2] * n);
+              const size_t o = ((size_t)k * np + j) * np + i;
+              blk[o] = a + amp * std::sin(two_pi * b) * std::sin(two_pi * c);
+              blk[m + o] = b + amp * std::sin(two_pi * c) * std::sin(two_pi * a);
+              blk[2 * m + o] = c + amp * std::sin(two_pi * a) * std::sin(two_pi * b);
+            }
+        xyz[bid(p, q, r)] = std::move(blk);
+      }
+  write_grid_binary(geo / "grid   0.grd", names, dims, xyz);
+
+  fs::create_directories(geo / "boundary_condition");
+  std::string bnd, par = "\t" + std::to_string(nblock) + "\t0\n";
+  for (int b = 0; b < nblock; ++b) {
+    bnd += "\t0\n";
+    par += "\t0";
+  }
+  par += "\nimin\timax\tjmin\tjmax\tkmin\tkmax\ts_r_id\ts_flag\tr_flag\tPhysic_Name\n";
+  write_text(geo / "boundary_condition" / "boundary   0.txt", bnd);
+  write_text(geo / "boundary_condition" / "boundary_name.fvbnd", kFvbnd);
+  write_text(geo / "boundary_condition" / "parallel   0.txt", par);
+  const std::string N = std::to_string(np);
+  auto face = [&](int axis, bool hi) {
+    std::string rg[3];
+    for (int a = 0; a < 3; ++a) {
+      if (a == axis)
+        rg[a] = (hi ? N : "1") + std::string("\t") + (hi ? N : "1");
+      else if (a == (axis + 2) % 3)
+        rg[a] = "-1\t-" + N;
+      else
+        rg[a] = "1\t" + N;
+    }
+    return rg[0] + "\t" + rg[1] + "\t" + rg[2];
+  };
+  std::ostringstream in;
+  in << "\t" << 6 * nblock << "\n";
+  for (int b = 0; b < nblock; ++b) in << "\t6";
+  in << "\nimin\timax\tjmin\tjmax\tkmin\tkmax\tid\tPhysic_Name\n";
+  for (int p = 0; p < nb[0]; ++p)
+    for (int q = 0; q < nb[1]; ++q)
+      for (int r = 0; r < nb[2]; ++r) {
+        const int pos[3] = {p, q, r};
+        for (int axis = 0; axis < 3; ++axis)
+          for (int hi = 0; hi < 2; ++hi) {
+            int t[3] = {p, q, r};
+            const bool wrap = hi ? pos[axis] == nb[axis] - 1 : pos[axis] == 0;
+            t[axis] = (pos[axis] + (hi ? 1 : nb[axis] - 1)) % nb[axis];
+            const int sgn = wrap ? -1 : 1;
+            in << face(axis, hi) << "\t" << sgn * (bid(p, q, r) + 1) << "\tFluid\n"
+               << face(axis, !hi) << "\t" << sgn * (bid(t[0], t[1], t[2]) + 1) << "\tFluid\n";
+          }
+      }
+  write_text(geo / "boundary_condition" / "inner   0.txt", in.str());
+}
+
 // Config "shell": 6-panel gnomonic (equiangular) cubed-sphere shell,
 // r in [1, r_out] with r_k = r_out^(k/nr); panel p has local axes
 // (i: xi angle, j: eta angle, k: radius), right-handed.  Shared panel-edge
@@ -414,6 +496,8 @@ void write_case(const fs::path &work) {
   const std::string kind = job_str("case", "cube");
   if (kind == "cube")
     write_cube_case(work / "CASE" / "geometry");
+  else if (kind == "lattice")
+    write_lattice_case(work / "CASE" / "geometry");
   else if (kind == "shell")
     write_shell_case(work / "CASE" / "geometry");
   else {
