@@ -285,7 +285,11 @@ def restart_write(path, step: int, time: float, cells, nghost: int, fields):
 class Context:
     """One device-resident solve behind the C ABI (mhd_ctx)."""
 
-    def __init__(self, cells, nghost: int, constants: MhdConstants, topology=None, precision: int = 0):
+    def __init__(self, cells, nghost: int, constants: MhdConstants, topology=None, precision: int = 0,
+                 lattice=None):
+        """cells: cells per block; one block is periodic in every direction,
+        lattice=(bx, by, bz) makes bx * by * bz equal blocks tile a periodic
+        box (mhd_topology_periodic_lattice)."""
         L = lib()
         self._cells = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
         self.desc = MhdDesc()
@@ -295,7 +299,13 @@ class Context:
         self.desc.precision = precision
         self.desc.constants = constants
         self._topo = ctypes.c_void_p()
-        if topology is None and len(cells) == 1:
+        if topology is None and lattice is not None:
+            if len(cells) != lattice[0] * lattice[1] * lattice[2] or any(tuple(c) != tuple(cells[0]) for c in cells):
+                raise ValueError("a lattice has bx * by * bz blocks of equal cells")
+            check(L.mhd_topology_periodic_lattice(_i3(cells[0]), _i3(lattice), nghost, ctypes.byref(self._topo)),
+                  "mhd_topology_periodic_lattice")
+            check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
+        elif topology is None and len(cells) == 1:
             check(L.mhd_topology_periodic_block(_i3(cells[0]), nghost, ctypes.byref(self._topo)),
                   "mhd_topology_periodic_block")
             check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
