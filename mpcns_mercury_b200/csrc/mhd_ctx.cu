@@ -987,7 +987,7 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
     // the correction: FP32 CG on r rounded to FP32, x += d in FP64
     launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_R, st);
     launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
-    double r32_0 = 0.0, r32 = 0.0;
+    double r32_0 = 0.0, r32 = 0.0;  // the correction's own residuals: not used (r is checked in FP64)
     int iters = 0;
     bool inner = false;
     if ((rc = res_cg(b, kInnerRtol, S->res_max_it, &r32_0, &r32, &iters, &inner))) return rc;

@@ -143,10 +143,11 @@ inline void alias_classes(const int n[3], std::vector<int32_t> &offset, std::vec
 //           that axis, an index past the owned range reads index - n of the
 //           block after it; a node-like index n is kept (the same block's
 //           alias DOF); corner ghosts read the diagonal neighbour.
-//   owner : an owned alias DOF (node-like index n) takes index 0 of the
-//           block after it along each such axis.
-//   edge alias classes: an edge on a block's lower node-like planes owns
-//   the class of its images at index n of the blocks before it.
+//   owner : an owned DOF on a block boundary plane (node-like index 0 or n)
+//           takes the value of its owner among its images in the blocks it
+//           touches, the image with the smallest (block, i, j, k).
+//   edge alias classes: the same images and owner, members in (block, i, j,
+//   k) order.
 struct Lattice {
   int nb[3];
   int id(const int pos[3]) const { return (pos[0] * nb[1] + pos[1]) * nb[2] + pos[2]; }
@@ -205,8 +206,11 @@ struct Lattice {
   }
 };
 
-// walk_unit for block blk of a lattice: the same entries in the same order
-// for a 1 x 1 x 1 lattice.
+// walk_unit for block blk of a lattice (the same entries for a 1 x 1 x 1
+// lattice).  An owned DOF shared with other block positions takes the value
+// of its owner, the image with the smallest (block, i, j, k): across a
+// periodic wrap that is index 0 (as on one block), across an inner patch the
+// block with the smaller id, which is what the reference's probe shows.
 template <class Emit>
 inline void walk_lattice(const GroupSpec &gs, int field, int m, const int n[3], const Lattice &L, int blk, int g,
                          Emit &&emit) {
@@ -226,13 +230,10 @@ inline void walk_lattice(const GroupSpec &gs, int field, int m, const int n[3], 
         int src[3], d[3] = {0, 0, 0};
         int nout = 0;
         for (int a = 0; a < 3; ++a) nout += !(idx[a] >= 0 && idx[a] < n[a] + st[a]);
-        bool is_owner_copy = false;
         if (nout == 0) {
           // an owned DOF on a block's boundary planes: its owner among its images
           int ob = blk;
           if (!L.owner_of(blk, idx, st, n, &ob, src)) continue;
-          d[0] = d[1] = d[2] = 0;
-          is_owner_copy = true;
           mhd_copy c;
           c.dst = {field, blk, i, j, k, m};
           c.src = {field, ob, src[0], src[1], src[2], m};
@@ -257,7 +258,7 @@ inline void walk_lattice(const GroupSpec &gs, int field, int m, const int n[3], 
         c.dst = {field, blk, i, j, k, m};
         c.src = {field, L.step(blk, d), src[0], src[1], src[2], m};
         c.sign = 1.0;
-        emit(c, is_owner_copy);
+        emit(c, false);
       }
     }
 }
