@@ -212,3 +212,15 @@ def test_one_block_lattice_is_the_periodic_block():
     finally:
         L.mhd_topology_destroy(t1)
         L.mhd_topology_destroy(t2)
+
+
+@pytest.mark.parametrize("cells,blocks,nghost", [((3, 4, 4), (2, 2, 2), 4), ((4, 4, 4), (0, 2, 2), 4),
+                                                 ((4, 4, 4), (2, 2, 2), 0), ((1, 4, 4), (1, 1, 1), 1)])
+def test_lattice_rejects_bad_arguments(cells, blocks, nghost):
+    """Blocks thinner than the ghost depth, empty lattices, no ghosts: MHD_ERR_ARG."""
+    from mpcns_mercury_b200 import capi
+
+    t = ctypes.c_void_p()
+    rc = capi.lib().mhd_topology_periodic_lattice(capi._i3(list(cells)), capi._i3(list(blocks)), nghost,
+                                                  ctypes.byref(t))
+    assert rc == 1 and not t.value  # MHD_ERR_ARG, nothing allocated
