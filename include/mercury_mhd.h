@@ -214,6 +214,12 @@ typedef struct mhd_info {
   int32_t res_iters, res_refinements;
 } mhd_info;
 int mhd_get_info(mhd_ctx *ctx, mhd_info *info);
+/* The solve's sticky device status (an mhd_status: MHD_OK, or the first
+ * failure a step met, e.g. MHD_ERR_DT where the reference exits,
+ * Z4_Mercury/src/physics/MercurySolver_Timestep.cpp:139, or MHD_ERR_SOLVE
+ * where it throws, Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:520),
+ * after the work queued so far.  Returns MHD_OK when the status was read. */
+int mhd_get_status(mhd_ctx *ctx, int32_t *status);
 
 /* calc_divB (Z4_Mercury/src/physics/MercurySolver_MagneticCell.cpp:151-241) on
  * the current state: MHD_DIVB = (sum of the cell's outward face fluxes) / Jac

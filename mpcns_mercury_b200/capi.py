@@ -118,7 +118,7 @@ class MhdRestartImage(ctypes.Structure):
 
 EXPORTS = [
     "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
-    "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_field_info", "mhd_stream",
+    "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_get_status", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block", "mhd_topology_periodic_lattice",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
@@ -160,6 +160,7 @@ def lib() -> ctypes.CDLL:
     L.mhd_synchronize.argtypes = [P]
     L.mhd_sync.argtypes = [P, ctypes.c_int]
     L.mhd_get_info.argtypes = [P, ctypes.POINTER(MhdInfo)]
+    L.mhd_get_status.argtypes = [P, ctypes.POINTER(ctypes.c_int32)]
     L.mhd_field_info.argtypes = [ctypes.c_int, i32p, i32p]
     L.mhd_stream.argtypes = [P]
     L.mhd_stream.restype = ctypes.c_void_p
@@ -345,6 +346,12 @@ class Context:
         inf = MhdInfo()
         check(lib().mhd_get_info(self.ctx, ctypes.byref(inf)), "mhd_get_info")
         return inf
+
+    def status(self) -> int:
+        """The sticky device status (0 = MHD_OK) after the queued work."""
+        st = ctypes.c_int32()
+        check(lib().mhd_get_status(self.ctx, ctypes.byref(st)), "mhd_get_status")
+        return st.value
 
     def kernels_per_step(self) -> int:
         return lib().mhd_kernels_per_step(self.ctx)

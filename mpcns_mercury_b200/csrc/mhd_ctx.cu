@@ -2024,6 +2024,14 @@ int mhd_get_info(mhd_ctx *ctx, mhd_info *info) {
   return mhd_batch_poll(ctx->batch, info);
 }
 
+int mhd_get_status(mhd_ctx *ctx, int32_t *status) {
+  if (!ctx || !status) return fail(MHD_ERR_ARG, "mhd_get_status: bad arguments");
+  const int rc = read_state(ctx->batch);
+  if (rc) return rc;
+  *status = ctx->batch->hstate[0].status;
+  return MHD_OK;
+}
+
 void *mhd_stream(mhd_ctx *ctx) { return ctx ? mhd_batch_stream(ctx->batch) : nullptr; }
 
 int mhd_kernels_per_step(mhd_ctx *ctx) { return ctx ? mhd_batch_kernels_per_step(ctx->batch) : -1; }
