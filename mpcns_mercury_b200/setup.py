@@ -537,7 +537,7 @@ class _MT19937_64:
 
 
 def orszag_tang_state(geom: Nodes, gamma: float = 1.6667, noise: float = 1e-3, solve_id: int = 0):
-    """Config-1 initial state on a periodic cube: both ion fluids carry the
+    """The cube case's initial state on a periodic cube: both ion fluids carry the
     Orszag-Tang vortex (rho = 1, p = 0.6, v = (-sin 2 pi y, sin 2 pi x, 0)) with
     multiplicative noise (1 + U[-noise, noise]) on every conserved component;
     B = curl A on the faces with A_z = (cos 4 pi x / (4 pi) + cos 2 pi y / (2 pi)) / sqrt(4 pi)
@@ -604,7 +604,7 @@ def orszag_tang_state(geom: Nodes, gamma: float = 1.6667, noise: float = 1e-3, s
 
 
 def cube_case(n=32, amp: float = 0.05, solve_id: int = 0):
-    """Config 1: geometry, sources and initial state of the periodic cube
+    """The periodic curvilinear cube case: geometry, sources and initial state of the cube
     (n cells per axis, or three per-axis counts for a periodic box).
     Returns (Geometry, {field name: Arr}) with every static input the step
     reads (reference names) and the initial state."""

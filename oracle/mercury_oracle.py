@@ -80,7 +80,7 @@ def run_job(job: dict, timeout: float = 3600.0, workdir: str | None = None) -> d
     return read_dump(lines["out"])
 
 
-# Config-1 case: periodic curvilinear unit cube, Orszag-Tang vortex, two ion
+# The cube case: periodic curvilinear unit cube, Orszag-Tang vortex, two ion
 # fluids, Hall + electron pressure on, resistivity off, CFL 0.4.  The IMF is
 # zero so the background field Badd vanishes and B is the vortex field alone.
 CUBE_JOB = {
@@ -158,7 +158,7 @@ def rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
 
 
-# Config-2 case: 6-panel cubed-sphere shell r in [1, 8], 48x48x96 cells per
+# The shell case: 6-panel cubed-sphere shell r in [1, 8], 48x48x96 cells per
 # panel (r_k = 8^(k/96)), inner wall (the reference's Coupled-Solid handlers),
 # outer Farfield; upstream v = (-4, 0, 0), n = 1, p = 0.1, IMF (0, 0, -0.2);
 # centred dipole, tilt 0, |B| = 1 at the surface equator (moment in A m^2 with
