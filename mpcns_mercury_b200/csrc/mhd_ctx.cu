@@ -1503,7 +1503,7 @@ int mhd_batch_upload_field(mhd_batch *b, int slot, int field, int block, const d
                                                                        ncomp, b->comp_ptrs, ndst, bx.si, bx.sj, bx.G,
                                                                        S->comp_bytes(c0) == 4);
   CUDA_TRY(cudaGetLastError());
-  // A copy from pageable memory is staged by the driver before
+  // A copy from pageable memory is staged by CUDA before
   // cudaMemcpyAsync returns; page-locked memory is read by the DMA later, so
   // wait for it before the caller may reuse the buffer.
   cudaPointerAttributes pa{};

@@ -2,7 +2,7 @@
  * (MercurySolver::StepOnce, Z4_Mercury/src/MercurySolver_Driver.cpp:21-61)
  * for ONE periodic block.  THIS IS TEST INFRASTRUCTURE (the oracle): only the
  * parity tests, the smoke check and the CPU-baseline leg of the benchmark call
- * it, as the checker.  The product never links it.
+ * it, to check results against it.  The product never links it.
  *
  * Every routine follows the reference function named in its comment, in the
  * reference's loop and operation order, in FP64, so that the restatement is
