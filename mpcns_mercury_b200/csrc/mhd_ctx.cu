@@ -377,7 +377,7 @@ int publish(mhd_batch *b) {
   std::vector<DevSolve> ds((size_t)C);
   for (int s = 0; s < C; ++s) {
     DevSolve &d = ds[s];
-    std::memset(&d, 0, sizeof d);
+    d = DevSolve{};
     const Solve *S = b->slots[s];
     if (!S) continue;
     d.c = S->consts;
