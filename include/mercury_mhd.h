@@ -448,6 +448,32 @@ int mhd_batch_load_restart(mhd_batch *batch, int slot, const char *path, int32_t
 int mhd_save_restart(mhd_ctx *ctx, const char *path);
 int mhd_load_restart(mhd_ctx *ctx, const char *path, int32_t *step, double *time);
 
+/* ---- Checkpoint plot file ----
+ * The Tecplot binary file (#!TDV112) the reference writes beside each
+ * restart file (IOModule::WriteTecplotBinFile,
+ * src/6_io/IOModule_Tecplot.cpp:749-1017) in the AllNode mode its Mercury
+ * solver selects (Z4_Mercury/src/MercurySolver.cpp:49-86): per block one
+ * ordered zone "Zone<b>_<name>" of (n + 1)^3 nodes; variables x, y, z and the
+ * cell fields below averaged to the nodes, each node the |Jac|-weighted mean
+ * of its eight cells (ghost cells included,
+ * IOModule::EvalValue_CellToNode_), written as float after the per-variable
+ * minimum and maximum.  Blocks without singular nodes (no averaging across
+ * singular edges).  Host-only: the arrays are the ones mhd_download_field
+ * returns (FieldBlock layout, (i, j, k, comp) order). */
+#define MHD_TECPLOT_FIELDS 6 /* PV_H (5), PV_Na (5), B_cell (3), Bind_cell (3), Na (1), J_cell (3) */
+typedef struct mhd_tecplot_image {
+  int32_t n_blocks;
+  const int32_t *cells;            /* 3 per block */
+  const char *const *block_names;  /* per block */
+  double time;                     /* solution time of the zones */
+  const double *const *nodes;      /* per block: node x, y, z (3 components) over [0, n + 1) per axis */
+  const double *const *jac;        /* per block: Jac over [-jac_ghost, n + jac_ghost) */
+  int32_t jac_ghost;               /* >= 1 */
+  const double *const *cell[MHD_TECPLOT_FIELDS]; /* per field, per block: over [-cell_ghost, n + cell_ghost) */
+  int32_t cell_ghost;              /* >= 1 */
+} mhd_tecplot_image;
+int mhd_tecplot_write(const char *path, const mhd_tecplot_image *img);
+
 #ifdef __cplusplus
 }
 #endif

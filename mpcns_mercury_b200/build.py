@@ -28,6 +28,7 @@ UNITS = [
     ("mhd_noalloc.cu", "mhd_noalloc.o", EXACT),
     ("mhd_host_setup.cpp", "mhd_host_setup.o", EXACT),
     ("mhd_restart.cpp", "mhd_restart.o", EXACT),
+    ("mhd_tecplot.cpp", "mhd_tecplot.o", EXACT),
     ("mhd_geometry.cu", "mhd_geometry.o", EXACT),
 ]
 SOURCES = sorted({u[0] for u in UNITS})

@@ -116,13 +116,24 @@ class MhdRestartImage(ctypes.Structure):
                 ("data", ctypes.POINTER(ctypes.c_double) * 5), ("loaded", ctypes.c_uint32)]
 
 
+TECPLOT_FIELDS = ["PV_H", "PV_Na", "B_cell", "Bind_cell", "Na", "J_cell"]  # mhd_tecplot_image.cell order
+_DPP = ctypes.POINTER(ctypes.POINTER(ctypes.c_double))
+
+
+class MhdTecplotImage(ctypes.Structure):
+    _fields_ = [("n_blocks", ctypes.c_int32), ("cells", ctypes.POINTER(ctypes.c_int32)),
+                ("block_names", ctypes.POINTER(ctypes.c_char_p)), ("time", ctypes.c_double),
+                ("nodes", _DPP), ("jac", _DPP), ("jac_ghost", ctypes.c_int32),
+                ("cell", _DPP * 6), ("cell_ghost", ctypes.c_int32)]
+
+
 EXPORTS = [
     "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_get_status", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block", "mhd_topology_periodic_lattice",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
-    "mhd_save_restart", "mhd_load_restart", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
+    "mhd_save_restart", "mhd_load_restart", "mhd_tecplot_write", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view",
@@ -180,6 +191,7 @@ def lib() -> ctypes.CDLL:
     L.mhd_restart_values.argtypes = [RI, ctypes.c_int32]
     L.mhd_restart_values.restype = ctypes.c_int64
     L.mhd_restart_write.argtypes = [ctypes.c_char_p, RI]
+    L.mhd_tecplot_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(MhdTecplotImage)]
     L.mhd_restart_read.argtypes = [ctypes.c_char_p, RI]
     L.mhd_save_restart.argtypes = [P, ctypes.c_char_p]
     L.mhd_load_restart.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]
@@ -281,6 +293,39 @@ def restart_write(path, step: int, time: float, cells, nghost: int, fields):
     for q, f in enumerate(RESTART_FIELDS):
         img.data[q] = bufs[f].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     check(lib().mhd_restart_write(os.fsencode(path), ctypes.byref(img)), "mhd_restart_write")
+
+
+def tecplot_write(path, cells, block_names, time: float, nodes, jac, jac_ghost: int, fields, cell_ghost: int):
+    """Write the checkpoint plot file (mhd_tecplot_write).  nodes: per block
+    an array (n+1, n+1, n+1, 3) of node x, y, z; jac: per block Jac over
+    [-jac_ghost, n + jac_ghost); fields: each of TECPLOT_FIELDS mapped to per
+    block arrays over [-cell_ghost, n + cell_ghost) (FieldBlock layout)."""
+    import numpy as np
+
+    nb = len(cells)
+    keep = []
+
+    def ptrs(arrays):
+        arr = [np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in arrays]
+        keep.append(arr)
+        return (ctypes.POINTER(ctypes.c_double) * nb)(*[a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for a in arr])
+
+    cc = (ctypes.c_int32 * (3 * nb))(*[int(x) for b in cells for x in b])
+    names = (ctypes.c_char_p * nb)(*[str(n).encode() for n in block_names])
+    img = MhdTecplotImage()
+    img.n_blocks = nb
+    img.cells = cc
+    img.block_names = names
+    img.time = float(time)
+    pn, pj = ptrs(nodes), ptrs(jac)
+    img.nodes = ctypes.cast(pn, _DPP)
+    img.jac = ctypes.cast(pj, _DPP)
+    img.jac_ghost = int(jac_ghost)
+    pf = [ptrs(fields[f]) for f in TECPLOT_FIELDS]
+    for q in range(6):
+        img.cell[q] = ctypes.cast(pf[q], _DPP)
+    img.cell_ghost = int(cell_ghost)
+    check(lib().mhd_tecplot_write(os.fsencode(path), ctypes.byref(img)), "mhd_tecplot_write")
 
 
 class Context:

@@ -64,7 +64,11 @@ def run_job(job: dict, timeout: float = 3600.0, workdir: str | None = None) -> d
     """Run the reference harness with ``job`` (key -> value) and return its dump."""
     if not available():
         raise FileNotFoundError(f"{REF_BIN} is not built (make -C oracle)")
-    tmp = workdir or tempfile.mkdtemp(prefix="mhd_oracle_")
+    if workdir is None:  # a fresh folder under the oracle's own (git-ignored) build directory
+        jobs = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "jobs")
+        os.makedirs(jobs, exist_ok=True)
+        workdir = tempfile.mkdtemp(prefix="job_", dir=jobs)
+    tmp = workdir
     os.makedirs(tmp, exist_ok=True)
     dump = os.path.join(tmp, "dump.bin")
     jobfile = os.path.join(tmp, "job.txt")

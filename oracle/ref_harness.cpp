@@ -931,6 +931,17 @@ int main(int argc, char **argv) {
         S.io_.Change_RestartPath(job_str("write_restart"));
         S.io_.WriteRestartBinFile((int)(job_int("restart_step0", 0) + steps), S.run_data_->time);
       }
+      if (!job_str("write_tecplot").empty()) {
+        // the reference's own checkpoint plot file (IOModule::WriteTecplotBinFile,
+        // src/6_io/IOModule_Tecplot.cpp:749-1017, in the AllNode mode and with
+        // the variables MercurySolver's constructor selects), written to its
+        // default ./DATA/ path and copied to the requested one
+        fs::create_directories("DATA");
+        S.io_.WriteTecplotBinFile((int)steps, S.run_data_->time);
+        for (const auto &e : fs::directory_iterator("DATA"))
+          if (e.path().extension() == ".plt")
+            fs::copy_file(e.path(), job_str("write_tecplot"), fs::copy_options::overwrite_existing);
+      }
       {
         // wall time of the StepOnce calls alone (setup and dumps excluded)
         long cells = 0;

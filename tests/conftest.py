@@ -11,6 +11,9 @@ for p in (ROOT, os.path.join(ROOT, "oracle")):
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+    # temporary files of the tests stay inside the repository (git-ignored)
+    if config.option.basetemp is None:
+        config.option.basetemp = os.path.join(ROOT, "tests", ".tmp")
 
 
 def has_gpu() -> bool:

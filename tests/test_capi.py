@@ -48,23 +48,23 @@ def test_bad_arguments_return_status():
     assert L.mhd_topology_periodic_block(capi._i3([1, 4, 4]), 4, ctypes.byref(t)) == 1
 
 
-def test_struct_layouts_match_header():
+def test_struct_layouts_match_header(tmp_path):
     """ctypes mirrors of the header structs have the C sizes."""
     import subprocess
-    import tempfile
 
     from mpcns_mercury_b200 import capi
 
-    src = ('#include <stdio.h>\n#include "mercury_mhd.h"\nint main(){printf("%zu %zu %zu %zu %zu",'
-           'sizeof(mhd_desc),sizeof(mhd_constants),sizeof(mhd_copy),sizeof(mhd_info),sizeof(mhd_alias_classes));}')
-    with tempfile.TemporaryDirectory() as d:
-        c = os.path.join(d, "s.c")
-        open(c, "w").write(src)
-        exe = os.path.join(d, "s")
-        subprocess.check_call(["gcc", "-I" + os.path.join(ROOT, "include"), c, "-o", exe])
-        got = [int(x) for x in subprocess.check_output([exe]).split()]
+    src = ('#include <stdio.h>\n#include "mercury_mhd.h"\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu",'
+           'sizeof(mhd_desc),sizeof(mhd_constants),sizeof(mhd_copy),sizeof(mhd_info),sizeof(mhd_alias_classes),'
+           'sizeof(mhd_restart_image),sizeof(mhd_tecplot_image));}')
+    c = str(tmp_path / "s.c")
+    open(c, "w").write(src)
+    exe = str(tmp_path / "s")
+    subprocess.check_call(["gcc", "-I" + os.path.join(ROOT, "include"), c, "-o", exe])
+    got = [int(x) for x in subprocess.check_output([exe]).split()]
     want = [ctypes.sizeof(capi.MhdDesc), ctypes.sizeof(capi.MhdConstants), ctypes.sizeof(capi.MhdCopy),
-            ctypes.sizeof(capi.MhdInfo), ctypes.sizeof(capi.MhdAliasClasses)]
+            ctypes.sizeof(capi.MhdInfo), ctypes.sizeof(capi.MhdAliasClasses), ctypes.sizeof(capi.MhdRestartImage),
+            ctypes.sizeof(capi.MhdTecplotImage)]
     assert got == want
 
 
