@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import os
 import struct
+import shutil
 import subprocess
 import tempfile
 from dataclasses import dataclass
@@ -64,7 +65,8 @@ def run_job(job: dict, timeout: float = 3600.0, workdir: str | None = None) -> d
     """Run the reference harness with ``job`` (key -> value) and return its dump."""
     if not available():
         raise FileNotFoundError(f"{REF_BIN} is not built (make -C oracle)")
-    if workdir is None:  # a fresh folder under the oracle's own (git-ignored) build directory
+    own = workdir is None
+    if own:  # a fresh folder under the oracle's own (git-ignored) build directory, removed afterwards
         jobs = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "jobs")
         os.makedirs(jobs, exist_ok=True)
         workdir = tempfile.mkdtemp(prefix="job_", dir=jobs)
@@ -78,10 +80,14 @@ def run_job(job: dict, timeout: float = 3600.0, workdir: str | None = None) -> d
     with open(jobfile, "w") as f:
         for k, v in lines.items():
             f.write(f"{k} {v}\n")
-    proc = subprocess.run([REF_BIN, jobfile], capture_output=True, text=True, timeout=timeout)
-    if proc.returncode != 0:
-        raise RuntimeError(f"oracle failed ({proc.returncode}):\n{proc.stdout[-4000:]}\n{proc.stderr[-4000:]}")
-    return read_dump(lines["out"])
+    try:
+        proc = subprocess.run([REF_BIN, jobfile], capture_output=True, text=True, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"oracle failed ({proc.returncode}):\n{proc.stdout[-4000:]}\n{proc.stderr[-4000:]}")
+        return read_dump(lines["out"])
+    finally:
+        if own:
+            shutil.rmtree(tmp, ignore_errors=True)
 
 
 # The cube case: periodic curvilinear unit cube, Orszag-Tang vortex, two ion
