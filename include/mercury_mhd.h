@@ -447,6 +447,19 @@ int mhd_batch_save_restart(mhd_batch *batch, int slot, const char *path);
 int mhd_batch_load_restart(mhd_batch *batch, int slot, const char *path, int32_t *step, double *time);
 int mhd_save_restart(mhd_ctx *ctx, const char *path);
 int mhd_load_restart(mhd_ctx *ctx, const char *path, int32_t *step, double *time);
+/* The run-data file the reference writes beside each checkpoint
+ * (IOModule::WriteRunDataFile -> RunData::WriteBinary,
+ * include/6_io/RunData.h:96-149): step, time, the last step's dt, the
+ * residual references (the Mercury solver: 13 values of 1.0,
+ * Z4_Mercury/src/MercurySolver.cpp:29-30, src/6_io/IOModele_Basic.cpp:55),
+ * residual_max (0) and the monitors (double and int32 values by key, written
+ * in key order; the Mercury solver's are the run's performance figures,
+ * src/6_io/RuntimeMonitor.cpp:28-55).  mhd_info gives step, time and dt.  The
+ * reader returns step, time and dt.  Host-only. */
+int mhd_rundata_write(const char *path, int32_t step, double time, double dt, int32_t nref,
+                      const double *residual_ref, double residual_max, int32_t n_dmon, const char *const *dkeys,
+                      const double *dvals, int32_t n_imon, const char *const *ikeys, const int32_t *ivals);
+int mhd_rundata_read(const char *path, int32_t *step, double *time, double *dt);
 
 /* ---- Checkpoint plot file ----
  * The Tecplot binary file (#!TDV112) the reference writes beside each

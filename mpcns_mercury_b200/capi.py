@@ -133,7 +133,7 @@ EXPORTS = [
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block", "mhd_topology_periodic_lattice",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
-    "mhd_save_restart", "mhd_load_restart", "mhd_tecplot_write", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
+    "mhd_save_restart", "mhd_load_restart", "mhd_tecplot_write", "mhd_rundata_write", "mhd_rundata_read", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view",
@@ -192,6 +192,12 @@ def lib() -> ctypes.CDLL:
     L.mhd_restart_values.restype = ctypes.c_int64
     L.mhd_restart_write.argtypes = [ctypes.c_char_p, RI]
     L.mhd_tecplot_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(MhdTecplotImage)]
+    L.mhd_rundata_write.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double), ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int32)]
+    L.mhd_rundata_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
     L.mhd_restart_read.argtypes = [ctypes.c_char_p, RI]
     L.mhd_save_restart.argtypes = [P, ctypes.c_char_p]
     L.mhd_load_restart.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]
@@ -326,6 +332,31 @@ def tecplot_write(path, cells, block_names, time: float, nodes, jac, jac_ghost: 
         img.cell[q] = ctypes.cast(pf[q], _DPP)
     img.cell_ghost = int(cell_ghost)
     check(lib().mhd_tecplot_write(os.fsencode(path), ctypes.byref(img)), "mhd_tecplot_write")
+
+
+MERCURY_NRES = 13  # residual references of the Mercury solver's run-data file
+
+
+def rundata_write(path, step: int, time: float, dt: float, residual_ref=(1.0,) * MERCURY_NRES,
+                  residual_max: float = 0.0, monitors_d=None, monitors_i=None):
+    """Write the run-data file (mhd_rundata_write); monitors_d / monitors_i:
+    {key: value} of double / int32 monitors."""
+    ref = (ctypes.c_double * len(residual_ref))(*[float(v) for v in residual_ref])
+    md, mi = dict(monitors_d or {}), dict(monitors_i or {})
+    dk = (ctypes.c_char_p * max(1, len(md)))(*[k.encode() for k in md])
+    dv = (ctypes.c_double * max(1, len(md)))(*[float(v) for v in md.values()])
+    ik = (ctypes.c_char_p * max(1, len(mi)))(*[k.encode() for k in mi])
+    iv = (ctypes.c_int32 * max(1, len(mi)))(*[int(v) for v in mi.values()])
+    check(lib().mhd_rundata_write(os.fsencode(path), int(step), float(time), float(dt), len(residual_ref), ref,
+                                  float(residual_max), len(md), dk, dv, len(mi), ik, iv), "mhd_rundata_write")
+
+
+def rundata_read(path):
+    """(step, time, dt) of a run-data file (mhd_rundata_read)."""
+    st, t, dt = ctypes.c_int32(), ctypes.c_double(), ctypes.c_double()
+    check(lib().mhd_rundata_read(os.fsencode(path), ctypes.byref(st), ctypes.byref(t), ctypes.byref(dt)),
+          "mhd_rundata_read")
+    return st.value, t.value, dt.value
 
 
 class Context:

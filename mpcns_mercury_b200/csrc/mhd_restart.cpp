@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 
 #include "mercury_mhd.h"
@@ -186,6 +187,82 @@ int mhd_restart_read(const char *path, mhd_restart_image *img) {
   img->step = step;
   img->time = time;
   img->loaded = loaded;
+  return MHD_OK;
+}
+
+// The run-data file written beside each checkpoint (RunData::WriteBinary,
+// include/6_io/RunData.h:96-149, through IOModule::WriteRunDataFile):
+// "MPCNSRUN", int32 version = 1, int32 step, double time, double dt,
+// int32 nref + nref doubles, double residual_max, then the double and the
+// int32 monitor maps, each an int32 count and per entry (in key order, as a
+// std::map holds them) int32 key length, key bytes and the value.  The
+// Mercury solver's monitors are RuntimeMonitor's (src/6_io/RuntimeMonitor.cpp:
+// 28-55): "Perf/CPUInterval_s", "Perf/s_per_MCells_step" and "Perf/Cells".
+int mhd_rundata_write(const char *path, int32_t step, double time, double dt, int32_t nref,
+                      const double *residual_ref, double residual_max, int32_t n_dmon, const char *const *dkeys,
+                      const double *dvals, int32_t n_imon, const char *const *ikeys, const int32_t *ivals) {
+  if (!path || nref < 0 || (nref > 0 && !residual_ref) || n_dmon < 0 || n_imon < 0 ||
+      (n_dmon > 0 && (!dkeys || !dvals)) || (n_imon > 0 && (!ikeys || !ivals)))
+    return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_write: bad arguments");
+  std::map<std::string, double> dm;
+  std::map<std::string, int32_t> im;
+  for (int q = 0; q < n_dmon; ++q) {
+    if (!dkeys[q]) return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_write: null key");
+    dm[dkeys[q]] = dvals[q];
+  }
+  for (int q = 0; q < n_imon; ++q) {
+    if (!ikeys[q]) return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_write: null key");
+    im[ikeys[q]] = ivals[q];
+  }
+  std::string out("MPCNSRUN");
+  auto put = [&](const void *p, size_t n) { out.append((const char *)p, n); };
+  auto key = [&](const std::string &k) {
+    const int32_t n = (int32_t)k.size();
+    put(&n, 4);
+    out += k;
+  };
+  const int32_t version = 1, nd = (int32_t)dm.size(), ni = (int32_t)im.size();
+  put(&version, 4);
+  put(&step, 4);
+  put(&time, 8);
+  put(&dt, 8);
+  put(&nref, 4);
+  if (nref > 0) put(residual_ref, 8 * (size_t)nref);
+  put(&residual_max, 8);
+  put(&nd, 4);
+  for (const auto &e : dm) {
+    key(e.first);
+    put(&e.second, 8);
+  }
+  put(&ni, 4);
+  for (const auto &e : im) {
+    key(e.first);
+    put(&e.second, 4);
+  }
+  File f;
+  f.fp = std::fopen(path, "wb");
+  if (!f.fp) return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_write: cannot open %s", path);
+  bool ok = std::fwrite(out.data(), 1, out.size(), f.fp) == out.size();
+  ok = std::fclose(f.fp) == 0 && ok;
+  f.fp = nullptr;
+  return ok ? MHD_OK : mhd::set_error(MHD_ERR_ARG, "mhd_rundata_write: write failed");
+}
+
+// RunData::ReadBinary (include/6_io/RunData.h:151-200): step, time and dt of
+// a run-data file (its residuals and monitors are not needed to resume).
+int mhd_rundata_read(const char *path, int32_t *step, double *time, double *dt) {
+  if (!path || !step || !time || !dt) return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_read: bad arguments");
+  File f;
+  f.fp = std::fopen(path, "rb");
+  if (!f.fp) return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_read: cannot open %s", path);
+  char magic[8];
+  int32_t version = 0;
+  if (std::fread(magic, 1, 8, f.fp) != 8 || std::memcmp(magic, "MPCNSRUN", 8) != 0)
+    return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_read: %s is not a run-data file", path);
+  if (std::fread(&version, 4, 1, f.fp) != 1 || version != 1)
+    return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_read: %s: unsupported version", path);
+  if (std::fread(step, 4, 1, f.fp) != 1 || std::fread(time, 8, 1, f.fp) != 1 || std::fread(dt, 8, 1, f.fp) != 1)
+    return mhd::set_error(MHD_ERR_ARG, "mhd_rundata_read: %s: truncated", path);
   return MHD_OK;
 }
 

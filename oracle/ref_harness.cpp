@@ -931,6 +931,13 @@ int main(int argc, char **argv) {
         S.io_.Change_RestartPath(job_str("write_restart"));
         S.io_.WriteRestartBinFile((int)(job_int("restart_step0", 0) + steps), S.run_data_->time);
       }
+      if (!job_str("write_rundata").empty()) {
+        // the reference's run-data file (IOModule::WriteRunDataFile), from its
+        // default ./DATA/RunData.bin
+        fs::create_directories("DATA");
+        S.io_.WriteRunDataFile();
+        fs::copy_file("DATA/RunData.bin", job_str("write_rundata"), fs::copy_options::overwrite_existing);
+      }
       if (!job_str("write_tecplot").empty()) {
         // the reference's own checkpoint plot file (IOModule::WriteTecplotBinFile,
         // src/6_io/IOModule_Tecplot.cpp:749-1017, in the AllNode mode and with

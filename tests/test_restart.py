@@ -152,3 +152,42 @@ def test_multi_block_restart_matches_reference(ref_lattice_restart, tmp_path):
     capi.restart_write(out, step, time, cells, NGHOST, fields)
     with open(path, "rb") as a, open(out, "rb") as c:
         assert a.read() == c.read()
+
+
+def test_rundata_file_matches_reference(ref_oracle, tmp_path):
+    """The run-data file beside a checkpoint (RunData::WriteBinary) from the
+    run's step, time and last dt, byte for byte against the reference's, and
+    read back."""
+    from mpcns_mercury_b200 import capi
+
+    ref = str(tmp_path / "ref.bin")
+    job = dict(ref_oracle.CUBE_JOB)
+    job.update(n=N, steps=STEPS, dump_at=str(STEPS), write_rundata=ref, dump_fields="U_H")
+    dump = ref_oracle.run_job(job, workdir=str(tmp_path / "job"))
+    dt, time = dump[(f"step{STEPS}:dt_time", -1)].data.ravel()
+    # the monitors are the run's wall-clock performance figures: taken from
+    # the reference's file (the format is what is checked)
+    raw = open(ref, "rb").read()
+    p = 8 + 4 + 4 + 8 + 8
+    nref = struct.unpack_from("<i", raw, p)[0]
+    p += 4 + 8 * nref + 8
+    mons = []
+    for fmt, size in (("<d", 8), ("<i", 4)):
+        n = struct.unpack_from("<i", raw, p)[0]
+        p += 4
+        m = {}
+        for _ in range(n):
+            ln = struct.unpack_from("<i", raw, p)[0]
+            key = raw[p + 4:p + 4 + ln].decode()
+            m[key] = struct.unpack_from(fmt, raw, p + 4 + ln)[0]
+            p += 4 + ln + size
+        mons.append(m)
+    assert sorted(mons[0]) == ["Perf/CPUInterval_s", "Perf/s_per_MCells_step"] and list(mons[1]) == ["Perf/Cells"]
+    assert mons[1]["Perf/Cells"] == N ** 3
+    ours = str(tmp_path / "ours.bin")
+    # keys given out of order: the writer orders them as the reference's map does
+    capi.rundata_write(ours, STEPS, time, dt, monitors_d=dict(reversed(list(mons[0].items()))),
+                       monitors_i={"Perf/Cells": N ** 3})
+    with open(ref, "rb") as a, open(ours, "rb") as b:
+        assert a.read() == b.read()
+    assert capi.rundata_read(ref) == (STEPS, time, dt)
