@@ -434,13 +434,12 @@ def run_ensemble(args, rank, world, device):
     ncell = owned_cells(cells)
     W_, K = args.warmup, args.steps
     total_steps = W_ + K
+    err_steps = max(total_steps, args.error_steps)  # the mixed error is stated after this many steps
     k0 = reference_constants(cfl=0.4)
     batches = {1: Batch(nsol, 1), 0: Batch(nsol, 0)}
     slots = {1: [], 0: []}
-    t_api = {1: 0.0, 0: 0.0}   # wall time of the batch's add/upload/sync/prepare calls
     plain_ms = 0.0
     plain_state = []
-    h2d_bytes = 0
     only = getattr(args, "batched_only", False)
     if only:
         batches[0].close()
@@ -469,7 +468,6 @@ def run_ensemble(args, rank, world, device):
             # FP64: host topology as explicit copy lists (setup, not timed), the
             # reference-format path; mixed: the periodic tables compiled directly
             d = SolveDesc([n], 4, k0, precision=prec) if prec == 0 else None
-            t0 = time.perf_counter()
             slot = b.add(d) if prec == 0 else b.add_periodic(n, 4, k0)
             if prec == 1:
                 nb = W.upload_request(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk),
@@ -479,13 +477,10 @@ def run_ensemble(args, rank, world, device):
             b.sync(slot, "UCELL")
             b.sync(slot, "BFACE")
             b.prepare(slot)
-            b.request(slot, total_steps)
-            t_api[prec] += time.perf_counter() - t0
+            b.request(slot, err_steps)
             slots[prec].append(slot)
             if d is not None:
                 d.close()
-            if prec == 1:
-                h2d_bytes += nb
         if only:
             continue
         # plain FP64, this solve alone
@@ -503,6 +498,8 @@ def run_ensemble(args, rank, world, device):
         e1.record(stream)
         e1.synchronize()
         plain_ms += e0.elapsed_time(e1)
+        if err_steps > total_steps:
+            ctx.step_async(err_steps - total_steps)  # untimed: on to the error check's step count
         ctx.synchronize()
         plain_state.append((fields, _owned_state(lambda nm, lo, hi: ctx.download(W.capi_field(nm), lo, hi), fields)))
         ctx.close()
@@ -518,9 +515,7 @@ def run_ensemble(args, rank, world, device):
     sampler = ClockSampler(device.index if device.index is not None else 0)
     if rank == 0:
         sampler.start()
-    t_run0 = time.perf_counter()
     mixed_ms = _timed_batch_steps(batches[1], K, device)
-    t_run_mixed = time.perf_counter() - t_run0
     clocks = sampler.stop() if rank == 0 else None
     if only:
         ms = mixed_ms
@@ -529,30 +524,29 @@ def run_ensemble(args, rank, world, device):
                 "n_gpus": world, "steps": K, "warmup": W_, "ms_per_step": round(ms / K, 5),
                 "config": {"workload": "ensemble", "solves": nsol, "batched_only": True}}
     fp64_ms = _timed_batch_steps(batches[0], K, device)
+    for b in batches.values():  # untimed: on to the error check's step count
+        if err_steps > total_steps:
+            b.run(err_steps - total_steps)
     infos = {p: b.poll() for p, b in batches.items()}
     for p in batches:
         for s in slots[p]:
-            if infos[p][s].status != 0 or infos[p][s].step != total_steps:
+            if infos[p][s].status != 0 or infos[p][s].step != err_steps:
                 raise RuntimeError(f"batch precision {p} slot {s}: status {infos[p][s].status} step {infos[p][s].step}")
     if world > 1:
         mixed_ms, fp64_ms, plain_ms = max_over_ranks([mixed_ms, fp64_ms, plain_ms], device)
 
     # errors: mixed batch vs plain FP64 (the FP64 path equals the reference bitwise),
     # and FP64 batch vs plain FP64 (must be identical)
-    t_dl0 = time.perf_counter()
     worst = {}
     fp64_identical = True
-    d2h_bytes = 0
     for sid, (fields, ref) in enumerate(plain_state):
         got = _owned_state(lambda nm, lo, hi: batches[1].download(slots[1][sid], W.capi_field(nm), lo, hi), fields)
-        d2h_bytes += sum(v.nbytes for v in got.values())
         for name in ref:
             worst[name] = max(worst.get(name, 0.0), _rel_l2(got[name], ref[name]))
         if sid < 8:  # the FP64 batch on a sample of solves
             got64 = _owned_state(lambda nm, lo, hi: batches[0].download(slots[0][sid], W.capi_field(nm), lo, hi),
                                  fields)
             fp64_identical = fp64_identical and all(np.array_equal(got64[k], ref[k]) for k in ref)
-    t_dl = (time.perf_counter() - t_dl0) / 2
 
     value = replicas_value(world, ncell, K, mixed_ms)
     plain = replicas_value(world, ncell, K, plain_ms)
@@ -563,11 +557,9 @@ def run_ensemble(args, rank, world, device):
     peak, peak_kind = load_peaks()
     roof = roofline(prof, cells, peak, peak_kind, precision=1, traffic_key="k_fluid_mixed_ensemble")
     launches = batches[1].kernels_per_step()
-    # e2e: the mixed batch through the C ABI from host buffers: add + upload of
-    # every solve, prepare, W + K steps, download of every final state
-    e2e_s = t_api[1] + t_run_mixed * (W_ + K) / K + t_dl
     for b in batches.values():
         b.close()
+    e2e = run_e2e_batch(cells, base_id, W_, K, world)
     cpu = cpu_baseline_sample(args, cells) if (rank == 0 and not args.no_cpu_baseline) else None
     return {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W_,
@@ -584,19 +576,78 @@ def run_ensemble(args, rank, world, device):
                    "batched_mixed_vs_plain_fp64": round(value / plain, 3),
                    "batched_fp64_vs_plain_fp64": round(batched64 / plain, 3),
                    "error_vs_fp64_rel_l2_max_over_solves": {k: float(f"{v:.3e}") for k, v in worst.items()},
-                   "error_steps": total_steps, "fp64_batch_bitwise_equal_plain": bool(fp64_identical)},
+                   "error_steps": err_steps, "fp64_batch_bitwise_equal_plain": bool(fp64_identical)},
         "roofline": roof, "cpu_baseline": cpu,
-        "e2e": {"value": round(world * ncell * (W_ + K) / e2e_s / 1e6, 3), "unit": UNIT,
-                "h2d_bytes_per_step": int(h2d_bytes / (W_ + K)), "d2h_bytes_per_step": int(d2h_bytes / (W_ + K)),
-                "wall_s": round(e2e_s, 3),
-                "what": "mixed batch via the C ABI from page-locked host arrays: add (mhd_batch_add_periodic: "
-                        "sync tables compiled from the periodic connectivity, uploaded), upload of the block's nodes with the static fields computed from them on the "
-                        "device (mhd_batch_setup_geometry), upload of the initial state, prepare of every solve, "
-                        "W+K steps, download of every final state; the device memory reservation is setup, "
-                        "outside the timed region, as the reference arm times StepOnce only"},
+        "e2e": e2e,
         "gpu_launches": launches * K, "clocks": clocks,
         "kernel_ms": {k: round(v, 5) for k, v in prof.items()},
     }
+
+
+def run_e2e_batch(cells, base_id, W_, K, world):
+    """The mixed batch end to end through the C ABI, timed as one wall-clock
+    region: from page-locked host inputs (each solve's block nodes and initial
+    state), add every solve (sync tables compiled from the periodic
+    connectivity), compute its static fields on the device from the nodes,
+    upload the state, prepare, run W + K steps, and download every solve's
+    final state to host memory.  The device memory reservation of the batch
+    happens before the timed region (the reference arm times StepOnce only)."""
+    import torch
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.capi import Batch, SolveDesc
+
+    k0 = reference_constants(cfl=0.4)
+    inputs = W.state_cases([(c, base_id + s) for s, c in enumerate(cells)])
+    pinned = []
+    for inp in inputs:  # page-locked copies of the host inputs (not timed)
+        pf = {}
+        for name, a in inp.items():
+            arr = a.data if hasattr(a, "data") and not isinstance(a, np.ndarray) else a
+            t = torch.empty(arr.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = arr
+            pf[name] = t.numpy() if isinstance(a, np.ndarray) else type(a)(a.lo, a.hi, t.numpy())
+        pinned.append(pf)
+    del inputs
+    batch = Batch(len(cells), 1)
+    need = 0
+    for n in cells:
+        d = SolveDesc([n], 4, k0, precision=1)
+        need += d.device_bytes()
+        d.close()
+    batch.reserve(need)
+    torch.cuda.synchronize()
+    h2d = d2h = 0
+    t0 = time.perf_counter()
+    slots = []
+    for n, pf in zip(cells, pinned):
+        slot = batch.add_periodic(n, 4, k0)
+        h2d += W.upload_request(lambda f, a, lo, hi, blk: batch.upload(slot, f, a, lo, hi, block=blk),
+                                lambda nodes: batch.setup_geometry(slot, nodes), pf)
+        batch.sync(slot, "UCELL")
+        batch.sync(slot, "BFACE")
+        batch.prepare(slot)
+        batch.request(slot, W_ + K)
+        slots.append(slot)
+    batch.run(W_ + K)
+    info = batch.poll()
+    for slot, pf in zip(slots, pinned):
+        for name in W.STATE_FIELDS:
+            a = pf[name]
+            d2h += batch.download(slot, W.capi_field(name), a.lo, a.hi).nbytes
+    t1 = time.perf_counter()
+    ok = all(info[s].status == 0 and info[s].step == W_ + K for s in slots)
+    batch.close()
+    if not ok:
+        raise RuntimeError("e2e batch: a solve did not finish its steps")
+    ncell = owned_cells(cells)
+    return {"value": round(world * ncell * (W_ + K) / (t1 - t0) / 1e6, 3), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / (W_ + K)), "d2h_bytes_per_step": int(d2h / (W_ + K)),
+            "wall_s": round(t1 - t0, 4), "steps": W_ + K,
+            "what": "one wall-clock region: add of every solve (mhd_batch_add_periodic), its static fields "
+                    "computed on the device from the uploaded nodes (mhd_batch_setup_geometry), upload of the "
+                    "initial state, prepare, W+K steps, download of every final state, all through the C ABI "
+                    "from page-locked host arrays"}
 
 
 # ------------------------------------------------------------------ serving
@@ -740,67 +791,85 @@ def run_implicit(args, rank, world, device):
 
 
 # ------------------------------------------------------------------ reference arm
-def reference_cubes(args):
-    """Cubes (cells per axis) the reference build runs for a bounded sample of
-    ``args.workload``: the workload's own cube, or, for the ensemble and the
-    request stream, the cube of the same cell count for each of the first
-    members (the reference's test case generator builds cubes; its cost per
-    cell-step does not depend on the aspect ratio)."""
+def reference_members(args):
+    """Cells per axis of every member of ``args.workload``, exactly as our arm
+    runs them (sizes drawn without loading the CUDA library)."""
     from mpcns_mercury_b200 import workloads as W
 
-    if args.workload == "cube32":
-        return [32]
     if args.workload.startswith("cube"):
-        return [int(args.workload[4:])]
+        n = int(args.workload[4:])
+        return [(n, n, n)]
     if args.workload == "ensemble":
-        sizes = W.ensemble_sizes(args.solves)
-    elif args.workload == "serve":
-        sizes = W.ensemble_sizes(args.shapes, stream=200000)
-    else:
-        raise SystemExit(f"unknown workload {args.workload}")
-    return [max(8, int(round((a * b * c) ** (1.0 / 3.0)))) for a, b, c in sizes]
+        return [tuple(c) for c in W.ensemble_sizes(args.solves)]
+    if args.workload == "serve":
+        return [tuple(c) for c in W.ensemble_sizes(args.shapes, stream=200000)]
+    raise SystemExit(f"unknown workload {args.workload}")
 
 
-def run_reference_steps(n, steps):
-    """Run the reference build on the n^3 cube for ``steps`` steps; returns
-    (seconds spent in StepOnce, cells)."""
+def run_reference_member(cells, warm, steps, solve_id=0):
+    """One member on the reference build (one single-rank process): ``warm``
+    untimed StepOnce calls, then ``steps`` timed ones.  Returns (seconds per
+    timed step, owned cells)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mercury_oracle as mo
 
     job = dict(mo.CUBE_JOB)
-    job.update(n=n, steps=steps, dump_fields="U_H", dump_at=str(steps))
-    d = mo.run_job(job, timeout=1800)
+    job.update(n=" ".join(str(int(v)) for v in cells), steps=warm + steps, time_from=warm, dump_fields="U_H",
+               dump_at=str(warm + steps), solve_id=solve_id)
+    d = mo.run_job(job, timeout=3600)
     secs, nsteps, ncell = d[("timing", -1)].data.ravel()
-    return float(secs), int(ncell)
+    return float(secs) / max(1.0, float(nsteps)), int(ncell)
 
 
-def reference_sample(args, steps):
-    """The reference on the host cores: one single-rank process per core, each
-    on one member cube of the workload, run concurrently.  Returns (aggregate
-    Mcell-updates/s = sum of the processes' own rates, processes, description)."""
+def reference_sample(members, warm, steps, procs):
+    """Every member on the reference build, the members partitioned over
+    ``procs`` host cores (longest first onto the least loaded core), each core
+    running its members one after another as single-rank processes.  A step
+    of the whole workload advances every member once, so it takes as long as
+    the busiest core's members take per step.  Returns (Mcell-updates/s,
+    seconds per workload step, cores used)."""
     from concurrent.futures import ThreadPoolExecutor
 
-    cubes = reference_cubes(args)
-    procs = min(len(cubes), max(1, os.cpu_count() or 1))
-    cubes = cubes[:procs]
+    procs = max(1, min(procs, len(members)))
+    load = [0] * procs
+    parts = [[] for _ in range(procs)]
+    for sid in sorted(range(len(members)), key=lambda q: -(members[q][0] * members[q][1] * members[q][2])):
+        w = load.index(min(load))
+        parts[w].append(sid)
+        load[w] += members[sid][0] * members[sid][1] * members[sid][2]
+
+    def core(part):
+        return sum(run_reference_member(members[sid], warm, steps, solve_id=sid)[0] for sid in part)
+
     with ThreadPoolExecutor(max_workers=procs) as ex:
-        res = list(ex.map(lambda n: run_reference_steps(n, steps), cubes))
-    rate = sum(c * steps / secs for secs, c in res) / 1e6
-    desc = (f"{args.workload}: {procs} concurrent single-rank reference processes (oracle/_ref, built from the "
-            f"reference sources), cubes {cubes}, {steps} StepOnce calls each, setup excluded")
-    return rate, procs, desc
+        per_core = list(ex.map(core, parts))
+    step_s = max(per_core)
+    cells = sum(a * b * c for a, b, c in members)
+    return cells / step_s / 1e6, step_s, procs
 
 
 def cpu_baseline_sample(args, cells=None):
-    """The reference (built from its sources) on the host: a bounded sample of
-    the same workload."""
+    """The reference (built from its sources) on this host: a bounded sample
+    of the same workload (its first members, a few steps each, on every
+    core), and the 32^3 cube on one core (the single-block case, one solve)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mercury_oracle as mo
 
     if not mo.available():
         return None
-    rate, procs, desc = reference_sample(args, args.cpu_sample_steps)
-    return {"value": round(rate, 4), "unit": UNIT, "cores": procs, "kind": "reference", "sample": desc}
+    members = reference_members(args)
+    cores = os.cpu_count() or 1
+    sample = members[:min(len(members), cores)]
+    rate, step_s, procs = reference_sample(sample, 1, 2, cores)
+    one_step_s, one_cells = run_reference_member((32, 32, 32), 1, 5)
+    return {"value": round(rate, 4), "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"{args.workload}: the first {len(sample)} members at their own shapes, one single-rank "
+                      f"reference process per member (oracle/_ref, built from the reference sources) spread over "
+                      f"{procs} cores, 1 untimed + 2 timed StepOnce calls each, setup excluded",
+            "one_core_cube32": {"value": round(one_cells / one_step_s / 1e6, 4), "unit": UNIT, "cores": 1,
+                                "ms_per_step": round(1e3 * one_step_s, 3),
+                                "sample": "periodic curvilinear 32^3 cube (Orszag-Tang, 2 ion fluids, Hall + p_e), "
+                                          "one process on one core, 1 untimed + 5 timed StepOnce calls"}}
 
 
 def run_reference(args, rank, world):
@@ -811,26 +880,27 @@ def run_reference(args, rank, world):
         return None
     if not mo.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/mercury_ref is not built on this host"}
-    steps = args.cpu_sample_steps
-    run_reference_steps(8, 1)  # warm the binary and the file cache
-    # each sample restarts the reference (its setup is not timed); a few
-    # samples keep the whole run within minutes
-    samples = max(1, min(args.steps, 3))
-    rates = []
+    members = reference_members(args)
+    cores = os.cpu_count() or 1
+    # every member once: one untimed step, then a bounded number of timed
+    # steps (the reference's per-member setup takes seconds, so the whole
+    # run stays within minutes)
+    steps = max(1, min(args.steps, args.ref_steps))
     t0 = time.perf_counter()
-    for _ in range(samples):
-        rate, procs, desc = reference_sample(args, steps)
-        rates.append(rate)
+    value, step_s, procs = reference_sample(members, 1, steps, cores)
     wall = time.perf_counter() - t0
-    value = float(np.mean(rates))
+    cells = sum(a * b * c for a, b, c in members)
     return {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / samples, 3),
+            "steps": steps, "warmup": 1, "ms_per_step": round(1e3 * step_s, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "steps_per_sample": steps, "samples": samples,
-                       "implementation": "reference solver compiled from its own sources, single rank per process, "
-                                         f"{procs} processes"},
+            "config": {"workload": args.workload, "members": len(members), "cells_per_replica": cells,
+                       "blocks": [list(c) for c in members], "wall_s": round(wall, 2),
+                       "implementation": "reference solver compiled from its own sources (oracle/_ref), one "
+                                         f"single-rank process per member, members spread over {procs} cores",
+                       "timing": "per member: 1 untimed StepOnce, then the timed ones (setup excluded); a workload "
+                                 "step takes as long as the busiest core's members take per step"},
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": procs, "kind": "reference",
-                             "sample": desc},
+                             "sample": f"all {len(members)} members at their own shapes, {steps} timed steps each"},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -851,7 +921,9 @@ def main():
     ap.add_argument("--capacity", type=int, default=64, help="serve: batch slots")
     ap.add_argument("--hbm-budget", type=float, default=100e9, help="serve: device bytes for admitted solves")
     ap.add_argument("--implicit-n", type=int, default=64, help="implicit: cells per axis of the cube")
-    ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    ap.add_argument("--error-steps", type=int, default=100,
+                    help="ensemble: steps after which the mixed batch's error against FP64 is stated")
+    ap.add_argument("--ref-steps", type=int, default=5, help="reference arm: timed steps per member (at most --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -39,10 +39,10 @@ enum mhd_status {
   MHD_ERR_CUDA = 2,     /* CUDA runtime error (see mhd_last_error) */
   MHD_ERR_OOM = 3,      /* device allocation failed */
   MHD_ERR_DT = 4,       /* dt non-finite or below 1e-7 (reference aborts) */
-  MHD_ERR_NONFINITE = 5,/* non-finite state detected */
+  MHD_ERR_NONFINITE = 5,/* a NaN/Inf in an owned cell's state: the solve is retired
+                           at its next step, the batch's other solves go on */
   MHD_ERR_SOLVE = 6,    /* implicit solve did not converge */
-  MHD_ERR_STATE = 7,    /* call out of order (e.g. step before prepare) */
-  MHD_ERR_TIMEOUT = 8   /* a device-side wait exceeded its iteration limit */
+  MHD_ERR_STATE = 7     /* call out of order (e.g. step before prepare) */
 };
 
 /* Field identifiers: the reference's catalog names
@@ -258,11 +258,13 @@ int mhd_seeded_uniform(uint64_t seed, int64_t count, double a, double *out);
  * memory through its own pool, or a request loop that must not allocate per
  * call).  The caller passes device pointers to its inputs and outputs in the
  * box layout of mhd_device_view (element (i,j,k) at p[(i+G)*si + (j+G)*sj +
- * (k+G)], G >= nghost + 1); the only intermediate — alpha (J x B) and
- * |alpha||B| on the cells [-nghost, n + nghost)^3 — lives in a library-owned
- * static device array of MHD_HALL_SCRATCH_MAX_CELLS cells x 4 doubles
- * (32 MiB), held by every GPU that loads the library until the process exits.
- * Blocks with more cells than that return MHD_ERR_ARG.  The first call on a
+ * (k+G)], G >= nghost + 1, sj >= n[2] + 1 + 2G, si >= sj (n[1] + 1 + 2G));
+ * the only intermediate — alpha (J x B) and |alpha||B| on the cells
+ * [-1, n]^3 around the owned edges — lives in a library-owned static device
+ * array of MHD_HALL_SCRATCH_MAX_CELLS cells x 4 doubles (32 MiB), held by
+ * every GPU that loads the library until the process exits.  Blocks with
+ * (n[0] + 2)(n[1] + 2)(n[2] + 2) above that, and strides smaller than the
+ * box, return MHD_ERR_ARG with a message (mhd_last_error).  The first call on a
  * device looks up the array's device address (once per device, with that
  * device current); make that first call before any stream capture.  All calls
  * share the one array and nothing in it needs to start at zero (every cell is

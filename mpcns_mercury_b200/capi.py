@@ -61,7 +61,7 @@ REF_FIELD = {
 
 GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL"]
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_DT", 5: "ERR_NONFINITE", 6: "ERR_SOLVE",
-          7: "ERR_STATE", 8: "ERR_TIMEOUT"}
+          7: "ERR_STATE"}
 
 
 class MhdConstants(ctypes.Structure):

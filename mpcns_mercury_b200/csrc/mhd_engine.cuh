@@ -104,9 +104,9 @@ struct SolveState {
   long long step;              // steps taken
   long long remaining;         // steps still to take in the current request (0 = idle)
   int status;                  // sticky mhd_status
+  int nonfinite;               // set when an owned cell's CFL dt came out non-finite (NaN/Inf state)
   int cur;                     // which U buffer holds the current state
   int mask;                    // selected for a targeted pass (Dir::mode == 1)
-  int pad_;
   unsigned long long divb_bits;  // max |div B| of the last mhd_div_b (non-negative double bits)
 };
 

@@ -568,7 +568,9 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
   for_items<R, kCells2>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     const ConstsT<R> &c = consts_of<R>(S);
     const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
-    const bool dt_ok = (dt >= R(1e-7)) && isfinite(dt);  // the reference aborts; k_flip records the status
+    // the reference aborts; k_flip records the status (and a solve with a
+    // non-finite cell is not advanced)
+    const bool dt_ok = (dt >= R(1e-7)) && isfinite(dt) && !D.state[it.s].nonfinite;
     const int i = it.i, j = it.j, k = it.k, s = it.species;
     const int u0 = s ? cUN : cUH, pv0 = s ? cPVN : cPVH;
     const R g = c.gamma;
@@ -731,7 +733,7 @@ __global__ void __launch_bounds__(kTileThreads) k_bface(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
-    if (!(dt >= R(1e-7)) || !isfinite(dt)) return;
+    if (!(dt >= R(1e-7)) || !isfinite(dt) || D.state[it.s].nonfinite) return;  // k_flip records the status
     const int i = it.i, j = it.j, k = it.k;
     if (j < B.n1 && k < B.n2) {
       const R rb = -R(1.0) * ((AT(cEY, i, j, k) - AT(cEY, i, j, k + 1)) + (AT(cEZ, i, j + 1, k) - AT(cEZ, i, j, k)));
@@ -1433,6 +1435,7 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
     const ConstsT<R> &c = consts_of<R>(S);
     const int i = it.i, j = it.j, k = it.k;
     R dtl = R(1e100);
+    bool bad = false;
     if (it.in) {
       R vel[2][3];
       for (int s = 0; s < 2; ++s) {
@@ -1490,12 +1493,16 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
           AT(cUC + axis, i, j, k) = (kx * up[0] + ky * up[1] + kz * up[2]) * inv_jac;
         }
       }
-      if (i >= 0 && i < B.n0 && j >= 0 && j < B.n1 && k >= 0 && k < B.n2) dtl = cell_dt(B, c, i, j, k);
+      if (i >= 0 && i < B.n0 && j >= 0 && j < B.n1 && k >= 0 && k < B.n2) {
+        dtl = cell_dt(B, c, i, j, k);
+        bad = !isfinite(dtl);  // a NaN drops out of the minimum below: record it instead
+      }
     }
     // warp minimum, one atomicMin per warp (min is exact in any order)
     for (int o = 16; o > 0; o >>= 1) dtl = dmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
     if ((threadIdx.x & 31) == 0 && dtl < R(1e100))
       atomicMin(&D.state[it.s].dt_bits, (unsigned long long)__double_as_longlong(dtl));
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(&D.state[it.s].nonfinite, 1);
   });
 }
 
@@ -1591,6 +1598,11 @@ __global__ void k_flip(Dir D) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < D.nsolves; s += gridDim.x * blockDim.x) {
     SolveState &st = D.state[s];
     if (!st.remaining) continue;
+    if (st.nonfinite) {  // a NaN/Inf cell: retire the solve, the others go on
+      st.status = MHD_ERR_NONFINITE;
+      st.remaining = 0;
+      continue;
+    }
     const double dt = __longlong_as_double((long long)st.dt_bits);
     if (!(dt >= 1e-7) || !isfinite(dt)) {
       st.status = MHD_ERR_DT;

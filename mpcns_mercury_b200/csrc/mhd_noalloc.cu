@@ -9,9 +9,9 @@
 // fragmented.  Such a caller owns its input and output buffers (any device
 // pointers it can obtain) and calls mhd_hall_emf_static_scratch; the only
 // intermediate the computation needs, the cell-centred Hall field
-// alpha (J x B) and the diffusivity scale |alpha||B| over the allocated cell
-// range, lives in a file-scope __device__ array of fixed size instead of
-// being allocated.
+// alpha (J x B) and the diffusivity scale |alpha||B| on the cells around the
+// owned edges, lives in a file-scope __device__ array of fixed size instead
+// of being allocated.
 //
 // The arithmetic is the same as the context path (the Hall cell field of
 // k_pv_uplus and k_hall_edge in mhd_kernels.cu, i.e. BuildHallFaceEMF_Rusanov_diff_ of the reference,
@@ -24,11 +24,13 @@
 #include <mutex>
 
 #include "mercury_mhd.h"
+#include "mhd_error.h"
 
 namespace {
 
-// Scratch: 4 doubles (Ehc x, y, z and beta) per cell of the allocated cell
-// range [-g, n + g)^3, at most MHD_HALL_SCRATCH_MAX_CELLS cells (32 MiB).
+// Scratch: 4 doubles (Ehc x, y, z and beta) per cell of the range the edge
+// pass reads, [-1, n]^3 (n + 2 cells per axis), at most
+// MHD_HALL_SCRATCH_MAX_CELLS cells (32 MiB).
 // Every GPU that loads the library holds this array until the process exits.
 __device__ __align__(256) double g_hall_scratch[4 * (size_t)MHD_HALL_SCRATCH_MAX_CELLS];
 
@@ -39,24 +41,25 @@ std::mutex g_scratch_mu;
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
 
 struct View {
-  int n0, n1, n2, G, g;
+  int n0, n1, n2, G;
   int64_t si, sj;
-  int e1, e2;  // extents of the allocated cell range along j and k (scratch layout)
+  int e1, e2;  // extents of the scratch cell range [-1, n] along j and k
   __device__ __forceinline__ int64_t off(int i, int j, int k) const {
     return (int64_t)(i + G) * si + (int64_t)(j + G) * sj + (k + G);
   }
-  // compact scratch index of cell (i, j, k) in [-g, n + g)
+  // compact scratch index of cell (i, j, k) in [-1, n]^3
   __device__ __forceinline__ int64_t soff(int i, int j, int k) const {
-    return ((int64_t)(i + g) * e1 + (j + g)) * e2 + (k + g);
+    return ((int64_t)(i + 1) * e1 + (j + 1)) * e2 + (k + 1);
   }
 };
 
-// Pass 1: alpha (J x B) and |alpha||B| on every cell of [-g, n + g).
+// Pass 1: alpha (J x B) and |alpha||B| on every cell of [-1, n]^3, the cells
+// around the owned edges.
 __global__ void k_hall_cell_static(mhd_hall_block in, View v, double *scratch, int64_t ncell) {
-  const int k = -v.g + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = -v.g + (int)(blockIdx.y * blockDim.y + threadIdx.y);
-  const int i = -v.g + (int)(blockIdx.z * blockDim.z + threadIdx.z);
-  if (i >= v.n0 + v.g || j >= v.n1 + v.g || k >= v.n2 + v.g) return;
+  const int k = -1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = -1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int i = -1 + (int)(blockIdx.z * blockDim.z + threadIdx.z);
+  if (i > v.n0 || j > v.n1 || k > v.n2) return;
   const int64_t o = v.off(i, j, k);
   // Hall_Num_Limiter (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:111-157): only ne_eff is needed
   const double rH = dmax(in.rho_H[o], 0.0), rN = dmax(in.rho_Na[o], 0.0);
@@ -162,36 +165,59 @@ int scratch_for_current_device(double **out) {
 
 extern "C" int mhd_hall_emf_static_scratch(const mhd_hall_block *in, double *out_xi, double *out_eta,
                                            double *out_zeta, void *stream) {
-  if (!in || !out_xi || !out_eta || !out_zeta) return MHD_ERR_ARG;
-  if (in->n[0] < 1 || in->n[1] < 1 || in->n[2] < 1 || in->nghost < 1 || in->G < in->nghost + 1) return MHD_ERR_ARG;
-  if (!in->rho_H || !in->rho_Na) return MHD_ERR_ARG;
+  using mhd::set_error;
+  if (!in || !out_xi || !out_eta || !out_zeta)
+    return set_error(MHD_ERR_ARG, "mhd_hall_emf_static_scratch: null block description or output pointer");
+  if (in->n[0] < 1 || in->n[1] < 1 || in->n[2] < 1 || in->nghost < 1 || in->G < in->nghost + 1)
+    return set_error(MHD_ERR_ARG, "mhd_hall_emf_static_scratch: need n >= 1 per axis, nghost >= 1, G >= nghost + 1");
+  // the box layout of mhd_device_view: [-G, n + 1 + G) per axis, k contiguous
+  const int64_t bj = (int64_t)in->n[2] + 1 + 2 * (int64_t)in->G, bi = (int64_t)in->n[1] + 1 + 2 * (int64_t)in->G;
+  if (in->sj < bj || in->si < in->sj * bi)
+    return set_error(MHD_ERR_ARG,
+                     "mhd_hall_emf_static_scratch: strides sj=%lld si=%lld smaller than the box (need sj >= %lld, "
+                     "si >= sj * %lld)", (long long)in->sj, (long long)in->si, (long long)bj, (long long)bi);
+  if (!in->rho_H || !in->rho_Na)
+    return set_error(MHD_ERR_ARG, "mhd_hall_emf_static_scratch: null density pointer");
   for (int a = 0; a < 3; ++a)
     if (!in->J_cell[a] || !in->B_cell[a] || !in->B_face[a] || !in->area[a] || !in->dl[a] || !in->taper[a] ||
         !in->dr_xi[a] || !in->dr_eta[a] || !in->dr_zeta[a])
-      return MHD_ERR_ARG;
-  const int g = in->nghost;
-  const int64_t e0 = (int64_t)in->n[0] + 2 * g, e1 = (int64_t)in->n[1] + 2 * g, e2 = (int64_t)in->n[2] + 2 * g;
+      return set_error(MHD_ERR_ARG, "mhd_hall_emf_static_scratch: null input pointer (component %d)", a);
+  const int64_t e0 = (int64_t)in->n[0] + 2, e1 = (int64_t)in->n[1] + 2, e2 = (int64_t)in->n[2] + 2;
   const int64_t ncell = e0 * e1 * e2;
-  if (ncell > (int64_t)MHD_HALL_SCRATCH_MAX_CELLS) return MHD_ERR_ARG;  // block exceeds the static scratch
+  if (ncell > (int64_t)MHD_HALL_SCRATCH_MAX_CELLS)
+    return set_error(MHD_ERR_ARG,
+                     "mhd_hall_emf_static_scratch: block of %dx%dx%d cells needs %lld scratch cells ((n + 2) per "
+                     "axis), more than the static array's %d", in->n[0], in->n[1], in->n[2], (long long)ncell,
+                     MHD_HALL_SCRATCH_MAX_CELLS);
   double *scratch = nullptr;
-  int rc = scratch_for_current_device(&scratch);
-  if (rc != MHD_OK) return rc;
+  if (scratch_for_current_device(&scratch) != MHD_OK)
+    return set_error(MHD_ERR_CUDA, "mhd_hall_emf_static_scratch: device address of the static scratch not found "
+                                   "(cudaGetDevice / cudaGetSymbolAddress failed)");
   View v;
   v.n0 = in->n[0];
   v.n1 = in->n[1];
   v.n2 = in->n[2];
   v.G = in->G;
-  v.g = g;
   v.si = in->si;
   v.sj = in->sj;
   v.e1 = (int)e1;
   v.e2 = (int)e2;
   cudaStream_t st = (cudaStream_t)stream;
-  const dim3 blk(32, 4, 2);
+  mhd_hall_block blk = *in;
+  const dim3 b3(32, 4, 2);
+  // each launch's own status (an earlier, unrelated launch error of the
+  // caller is neither reported nor cleared here)
   const dim3 gc((unsigned)((e2 + 31) / 32), (unsigned)((e1 + 3) / 4), (unsigned)((e0 + 1) / 2));
-  k_hall_cell_static<<<gc, blk, 0, st>>>(*in, v, scratch, ncell);
+  void *cell_args[] = {&blk, &v, &scratch, (void *)&ncell};
+  cudaError_t err = cudaLaunchKernel((const void *)k_hall_cell_static, gc, b3, cell_args, 0, st);
+  if (err != cudaSuccess)
+    return set_error(MHD_ERR_CUDA, "mhd_hall_emf_static_scratch: cell pass launch: %s", cudaGetErrorString(err));
   const dim3 ge((unsigned)((in->n[2] + 1 + 31) / 32), (unsigned)((in->n[1] + 1 + 3) / 4),
                 (unsigned)((in->n[0] + 1 + 1) / 2));
-  k_hall_edge_static<<<ge, blk, 0, st>>>(*in, v, scratch, ncell, out_xi, out_eta, out_zeta);
-  return cudaGetLastError() == cudaSuccess ? MHD_OK : MHD_ERR_CUDA;
+  const double *cscratch = scratch;
+  void *edge_args[] = {&blk, &v, (void *)&cscratch, (void *)&ncell, &out_xi, &out_eta, &out_zeta};
+  err = cudaLaunchKernel((const void *)k_hall_edge_static, ge, b3, edge_args, 0, st);
+  if (err != cudaSuccess)
+    return set_error(MHD_ERR_CUDA, "mhd_hall_emf_static_scratch: edge pass launch: %s", cudaGetErrorString(err));
+  return MHD_OK;
 }

@@ -536,6 +536,17 @@ class _MT19937_64:
         return x & 0xFFFFFFFFFFFFFFFF
 
 
+def host_uniform_sym(solve_id: int, a: float, count: int) -> np.ndarray:
+    """The first ``count`` draws of Uniform(solve_id).sym(a, count), computed
+    in Python with the engine above (no library call): for the few draws that
+    size a workload, in processes that must not load the CUDA library."""
+    g = _MT19937_64(20261203 + solve_id)
+    out = np.empty(count)
+    for q in range(count):
+        out[q] = -a + 2.0 * a * ((g.next() >> 11) * 2.0 ** -53)
+    return out
+
+
 def orszag_tang_state(geom: Nodes, gamma: float = 1.6667, noise: float = 1e-3, solve_id: int = 0):
     """The cube case's initial state on a periodic cube: both ion fluids carry the
     Orszag-Tang vortex (rho = 1, p = 0.6, v = (-sin 2 pi y, sin 2 pi x, 0)) with

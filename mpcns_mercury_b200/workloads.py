@@ -98,8 +98,9 @@ def ensemble_sizes(nsolves: int, stream: int = 100000):
     """Per-solve block sizes of the ensemble: cells per axis log-uniform,
     x and y in [24, 64], z in [24, 128] (the per-block range 24^3 .. 64x64x128),
     drawn from the seeded generator with solve_id = ``stream`` (a stream no
-    solve's own noise uses)."""
-    u = S.Uniform(stream).sym(0.5, 3 * nsolves) + 0.5
+    solve's own noise uses).  Computed without the CUDA library, so that the
+    CPU reference arm can size the same workload."""
+    u = S.host_uniform_sym(stream, 0.5, 3 * nsolves) + 0.5
     lo, hx, hz = math.log(24.0), math.log(64.0), math.log(128.0)
     sizes = []
     for s in range(nsolves):

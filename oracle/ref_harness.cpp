@@ -209,21 +209,29 @@ void write_grid_binary(const fs::path &p, const std::vector<std::string> &names,
   for (auto &b : xyz) f.write((const char *)b.data(), (std::streamsize)(b.size() * sizeof(double)));
 }
 
-// Config "cube": one block of n^3 cells on the unit cube, periodic in every
-// direction, nodes x_a = xi_a + amp*sin(2 pi xi_b)*sin(2 pi xi_c) for cyclic
-// (a, b, c).  Periodic connectivity uses negative block ids
-// (src/1_grid/1_MPCNS_Grid.cpp:455-464).
+// Config "cube": one periodic block of n0 x n1 x n2 cells on the unit box
+// ("n" holds one count for a cube or three per-axis counts), periodic in
+// every direction, nodes x_a = xi_a + amp*sin(2 pi xi_b)*sin(2 pi xi_c) for
+// cyclic (a, b, c), xi_a = index / n_a.  Periodic connectivity uses negative
+// block ids (src/1_grid/1_MPCNS_Grid.cpp:455-464).
+void cube_counts(int nc[3]) {
+  std::istringstream is(job_str("n", "32"));
+  is >> nc[0];
+  if (!(is >> nc[1] >> nc[2])) nc[1] = nc[2] = nc[0];
+}
+
 void write_cube_case(const fs::path &geo) {
-  const int n = (int)job_int("n", 32);
+  int nc[3];
+  cube_counts(nc);
   const double amp = job_dbl("amp", 0.05);
-  const int np = n + 1;
+  const int np0 = nc[0] + 1, np1 = nc[1] + 1, np2 = nc[2] + 1;
   const double two_pi = 2.0 * std::acos(-1.0);
-  std::vector<double> x((size_t)np * np * np), y(x.size()), z(x.size());
-  for (int k = 0; k < np; ++k)
-    for (int j = 0; j < np; ++j)
-      for (int i = 0; i < np; ++i) {
-        const double a = (double)i / n, b = (double)j / n, c = (double)k / n;
-        const size_t o = ((size_t)k * np + j) * np + i;
+  std::vector<double> x((size_t)np0 * np1 * np2), y(x.size()), z(x.size());
+  for (int k = 0; k < np2; ++k)
+    for (int j = 0; j < np1; ++j)
+      for (int i = 0; i < np0; ++i) {
+        const double a = (double)i / nc[0], b = (double)j / nc[1], c = (double)k / nc[2];
+        const size_t o = ((size_t)k * np1 + j) * np0 + i;
         x[o] = a + amp * std::sin(two_pi * b) * std::sin(two_pi * c);
         y[o] = b + amp * std::sin(two_pi * c) * std::sin(two_pi * a);
         z[o] = c + amp * std::sin(two_pi * a) * std::sin(two_pi * b);
@@ -232,7 +240,7 @@ void write_cube_case(const fs::path &geo) {
   blk.insert(blk.end(), x.begin(), x.end());
   blk.insert(blk.end(), y.begin(), y.end());
   blk.insert(blk.end(), z.begin(), z.end());
-  write_grid_binary(geo / "grid   0.grd", {"Fluid"}, {{np, np, np}}, {blk});
+  write_grid_binary(geo / "grid   0.grd", {"Fluid"}, {{np0, np1, np2}}, {blk});
 
   fs::create_directories(geo / "boundary_condition");
   write_text(geo / "boundary_condition" / "boundary   0.txt", "\t0\n");
@@ -241,16 +249,16 @@ void write_cube_case(const fs::path &geo) {
   // Six periodic face pairs, both directions listed as in the reference's own
   // geometry fixtures (Z0_NULL/CASE/geometry.tar.gz).
   std::ostringstream in;
-  const std::string N = std::to_string(np);
+  const std::string N[3] = {std::to_string(np0), std::to_string(np1), std::to_string(np2)};
   auto face = [&](int axis, bool hi) {
     std::string r[3];
     for (int a = 0; a < 3; ++a) {
       if (a == axis)
-        r[a] = (hi ? N : "1") + std::string("\t") + (hi ? N : "1");
+        r[a] = (hi ? N[a] : "1") + std::string("\t") + (hi ? N[a] : "1");
       else if (a == (axis + 2) % 3)
-        r[a] = "-1\t-" + N;  // second tangential direction carries the sign mark
+        r[a] = "-1\t-" + N[a];  // second tangential direction carries the sign mark
       else
-        r[a] = "1\t" + N;
+        r[a] = "1\t" + N[a];
     }
     return r[0] + "\t" + r[1] + "\t" + r[2];
   };
@@ -581,7 +589,7 @@ std::vector<std::string> split_ws(const std::string &s) {
 }
 
 // ---------------------------------------------------------------- initial state
-// Orszag-Tang vortex on both ion fluids: rho = 1, p = 0.6,
+// Orszag-Tang vortex on both ion fluids (every block of the periodic box): rho = 1, p = 0.6,
 // v = (-sin 2 pi y, sin 2 pi x, 0), B = curl A with
 // A_z = (cos 4 pi x / (4 pi) + cos 2 pi y / (2 pi)) / sqrt(4 pi), i.e.
 // B = (-sin 2 pi y, sin 4 pi x, 0) / sqrt(4 pi).  Multiplicative noise
@@ -596,66 +604,89 @@ void set_orszag_tang(MercurySolver &S) {
   const double gamma = S.gamma_;
   const double noise = job_dbl("noise", 1e-3);
   Uniform rng(20261203ull + (uint64_t)job_int("solve_id", 0));
-  const int ib = 0;
-  FieldBlock &UH = fld->field(S.fid_.fid_U_H, ib);
-  FieldBlock &UN = fld->field(S.fid_.fid_U_Na, ib);
-  Block &blk = grd->grids(ib);
-  const int n = blk.mx;  // cells per direction
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j)
-      for (int k = 0; k < n; ++k) {
-        const double x = blk.dual_x(i + 1, j + 1, k + 1);
-        const double y = blk.dual_y(i + 1, j + 1, k + 1);
-        const double rho = 1.0, p = 0.6;
-        const double u = -std::sin(2.0 * pi * y), v = std::sin(2.0 * pi * x), w = 0.0;
-        const double q[5] = {rho, rho * u, rho * v, rho * w,
-                             p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)};
-        for (FieldBlock *U : {&UH, &UN})
-          for (int m = 0; m < 5; ++m) (*U)(i, j, k, m) = q[m] * (1.0 + rng.sym(noise));
+  // cells per block and blocks per axis: one periodic block ("cube"), or the
+  // "lattice" case's bx x by x bz blocks of equal size tiling the periodic box
+  int nc[3], nb[3] = {1, 1, 1};
+  cube_counts(nc);
+  if (job_str("case", "cube") == "lattice") std::istringstream(job_str("nb", "2 2 2")) >> nb[0] >> nb[1] >> nb[2];
+  const int n0 = nc[0], n1 = nc[1], n2 = nc[2];  // cells per direction of a block
+  const int N0 = n0 * nb[0], N1 = n1 * nb[1], N2 = n2 * nb[2];
+  auto bid = [&](int p, int q, int r) { return (p * nb[1] + q) * nb[2] + r; };
+  for (int p = 0; p < nb[0]; ++p)
+    for (int q = 0; q < nb[1]; ++q)
+      for (int r = 0; r < nb[2]; ++r) {
+        const int ib = bid(p, q, r);
+        FieldBlock &UH = fld->field(S.fid_.fid_U_H, ib);
+        FieldBlock &UN = fld->field(S.fid_.fid_U_Na, ib);
+        Block &blk = grd->grids(ib);
+        for (int i = 0; i < n0; ++i)
+          for (int j = 0; j < n1; ++j)
+            for (int k = 0; k < n2; ++k) {
+              const double x = blk.dual_x(i + 1, j + 1, k + 1);
+              const double y = blk.dual_y(i + 1, j + 1, k + 1);
+              const double rho = 1.0, pr = 0.6;
+              const double u = -std::sin(2.0 * pi * y), v = std::sin(2.0 * pi * x), w = 0.0;
+              const double qv[5] = {rho, rho * u, rho * v, rho * w,
+                                    pr / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)};
+              for (FieldBlock *U : {&UH, &UN})
+                for (int m = 0; m < 5; ++m) (*U)(i, j, k, m) = qv[m] * (1.0 + rng.sym(noise));
+            }
       }
-  // Edge potentials A_z * dz on the periodic edge set.
+  // Edge potentials A_z * dz on the periodic edge set of the whole box
+  // (global indices I = p * n0 + i, ...), each evaluated on the block that
+  // holds the edge's lower node.
   auto Az = [&](double x, double y) {
     return (std::cos(4.0 * pi * x) / (4.0 * pi) + std::cos(2.0 * pi * y) / (2.0 * pi)) /
            std::sqrt(4.0 * pi);
   };
-  std::vector<double> ax((size_t)n * n * n), ay(ax.size()), az(ax.size());
-  auto idx = [&](int i, int j, int k) { return ((size_t)i * n + j) * n + k; };
-  auto edge_val = [&](int i0, int j0, int k0, int i1, int j1, int k1) {
+  std::vector<double> ax((size_t)N0 * N1 * N2), ay(ax.size()), az(ax.size());
+  auto idx = [&](int i, int j, int k) { return ((size_t)i * N1 + j) * N2 + k; };
+  auto edge_val = [&](int I, int J, int K, int di, int dj, int dk) {
+    Block &blk = grd->grids(bid(I / n0, J / n1, K / n2));
+    const int i0 = I % n0, j0 = J % n1, k0 = K % n2, i1 = i0 + di, j1 = j0 + dj, k1 = k0 + dk;
     const double xa = blk.x(i0, j0, k0), ya = blk.y(i0, j0, k0), za = blk.z(i0, j0, k0);
     const double xb = blk.x(i1, j1, k1), yb = blk.y(i1, j1, k1), zb = blk.z(i1, j1, k1);
     return Az(0.5 * (xa + xb), 0.5 * (ya + yb)) * (zb - za);
   };
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j)
-      for (int k = 0; k < n; ++k) ax[idx(i, j, k)] = edge_val(i, j, k, i + 1, j, k) * (1.0 + rng.sym(noise));
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j)
-      for (int k = 0; k < n; ++k) ay[idx(i, j, k)] = edge_val(i, j, k, i, j + 1, k) * (1.0 + rng.sym(noise));
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j)
-      for (int k = 0; k < n; ++k) az[idx(i, j, k)] = edge_val(i, j, k, i, j, k + 1) * (1.0 + rng.sym(noise));
-  auto w = [&](int a) { return ((a % n) + n) % n; };
-  auto EX = [&](int i, int j, int k) { return ax[idx(w(i), w(j), w(k))]; };
-  auto EY = [&](int i, int j, int k) { return ay[idx(w(i), w(j), w(k))]; };
-  auto EZ = [&](int i, int j, int k) { return az[idx(w(i), w(j), w(k))]; };
+  for (int i = 0; i < N0; ++i)
+    for (int j = 0; j < N1; ++j)
+      for (int k = 0; k < N2; ++k) ax[idx(i, j, k)] = edge_val(i, j, k, 1, 0, 0) * (1.0 + rng.sym(noise));
+  for (int i = 0; i < N0; ++i)
+    for (int j = 0; j < N1; ++j)
+      for (int k = 0; k < N2; ++k) ay[idx(i, j, k)] = edge_val(i, j, k, 0, 1, 0) * (1.0 + rng.sym(noise));
+  for (int i = 0; i < N0; ++i)
+    for (int j = 0; j < N1; ++j)
+      for (int k = 0; k < N2; ++k) az[idx(i, j, k)] = edge_val(i, j, k, 0, 0, 1) * (1.0 + rng.sym(noise));
+  auto wi = [&](int a) { return ((a % N0) + N0) % N0; };
+  auto wj = [&](int a) { return ((a % N1) + N1) % N1; };
+  auto wk = [&](int a) { return ((a % N2) + N2) % N2; };
   // Face fluxes = discrete curl of the edge potential, same stencil as the
   // reference's CurlEdgeToFace (Z4_Mercury/src/operators/CTOperators.cpp:6-56)
-  // with multiplier +1.
-  FieldBlock &Bx = fld->field(S.fid_.fid_B.xi, ib);
-  FieldBlock &By = fld->field(S.fid_.fid_B.eta, ib);
-  FieldBlock &Bz = fld->field(S.fid_.fid_B.zeta, ib);
-  for (int i = 0; i <= n; ++i)
-    for (int j = 0; j < n; ++j)
-      for (int k = 0; k < n; ++k)
-        Bx(i, j, k, 0) = (EY(i, j, k) - EY(i, j, k + 1)) + (EZ(i, j + 1, k) - EZ(i, j, k));
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j <= n; ++j)
-      for (int k = 0; k < n; ++k)
-        By(i, j, k, 0) = (EX(i, j, k + 1) - EX(i, j, k)) + (EZ(i, j, k) - EZ(i + 1, j, k));
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j)
-      for (int k = 0; k <= n; ++k)
-        Bz(i, j, k, 0) = (EX(i, j, k) - EX(i, j + 1, k)) + (EY(i + 1, j, k) - EY(i, j, k));
+  // with multiplier +1; block faces on a shared boundary get identical values.
+  for (int p = 0; p < nb[0]; ++p)
+    for (int q = 0; q < nb[1]; ++q)
+      for (int r = 0; r < nb[2]; ++r) {
+        const int ib = bid(p, q, r);
+        const int I0 = p * n0, J0 = q * n1, K0 = r * n2;
+        auto EX = [&](int i, int j, int k) { return ax[idx(wi(I0 + i), wj(J0 + j), wk(K0 + k))]; };
+        auto EY = [&](int i, int j, int k) { return ay[idx(wi(I0 + i), wj(J0 + j), wk(K0 + k))]; };
+        auto EZ = [&](int i, int j, int k) { return az[idx(wi(I0 + i), wj(J0 + j), wk(K0 + k))]; };
+        FieldBlock &Bx = fld->field(S.fid_.fid_B.xi, ib);
+        FieldBlock &By = fld->field(S.fid_.fid_B.eta, ib);
+        FieldBlock &Bz = fld->field(S.fid_.fid_B.zeta, ib);
+        for (int i = 0; i <= n0; ++i)
+          for (int j = 0; j < n1; ++j)
+            for (int k = 0; k < n2; ++k)
+              Bx(i, j, k, 0) = (EY(i, j, k) - EY(i, j, k + 1)) + (EZ(i, j + 1, k) - EZ(i, j, k));
+        for (int i = 0; i < n0; ++i)
+          for (int j = 0; j <= n1; ++j)
+            for (int k = 0; k < n2; ++k)
+              By(i, j, k, 0) = (EX(i, j, k + 1) - EX(i, j, k)) + (EZ(i, j, k) - EZ(i + 1, j, k));
+        for (int i = 0; i < n0; ++i)
+          for (int j = 0; j < n1; ++j)
+            for (int k = 0; k <= n2; ++k)
+              Bz(i, j, k, 0) = (EX(i, j, k) - EX(i, j + 1, k)) + (EY(i + 1, j, k) - EY(i, j, k));
+      }
 }
 
 // Magnetosphere start: the reference's uniform solar wind (Common_Initial,
@@ -917,11 +948,13 @@ int main(int argc, char **argv) {
           }
       };
       dump_state(0);
+      // wall time of the StepOnce calls after the first time_from (warm-up) steps
+      const long time_from = job_int("time_from", 0);
       double stepping = 0.0;
       for (long s = 1; s <= steps; ++s) {
         const auto t0 = std::chrono::steady_clock::now();
         S.StepOnce();
-        stepping += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (s > time_from) stepping += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         dump_state(s);
       }
       if (!job_str("write_restart").empty()) {
@@ -958,7 +991,7 @@ int main(int argc, char **argv) {
           const Int3 h = U.inner_hi();
           cells += (long)h.i * h.j * h.k;
         }
-        const double meta[3] = {stepping, (double)steps, (double)cells};
+        const double meta[3] = {stepping, (double)(steps - std::min(steps, time_from)), (double)cells};
         const int l[3] = {0, 0, 0}, h[3] = {1, 1, 3};
         d.rec("timing", -1, l, h, 1, meta);
       }

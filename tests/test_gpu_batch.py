@@ -184,3 +184,56 @@ def test_add_periodic_equals_explicit_tables(cases):
         assert _same(_state(b, slots[1], fields), _state(b, slots[0], fields)), precision
         b.close()
         d.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_nonfinite_solve_retires_alone(cases, precision):
+    """A NaN planted in one owned cell of one solve's uploaded state: that
+    solve retires with MHD_ERR_NONFINITE at its next step, its state is left
+    as it was, and the other solves of the batch finish every requested step
+    with the same result as when run without it."""
+    from mpcns_mercury_b200 import reference_constants
+    from mpcns_mercury_b200 import workloads as W
+    from mpcns_mercury_b200.capi import Batch, SolveDesc
+
+    steps = 4
+    bad_sid, good = 1, (0, 2)
+
+    def add(b, fields, n):
+        d = SolveDesc([n], W.NGHOST, reference_constants(cfl=0.4), precision=precision)
+        slot = b.add(d)
+        W.upload_case(lambda f, a, lo, hi, blk: b.upload(slot, f, a, lo, hi, block=blk), fields)
+        b.sync(slot, "UCELL")
+        b.sync(slot, "BFACE")
+        b.prepare(slot)
+        b.request(slot, steps)
+        return slot, d
+
+    clean = Batch(4, precision)
+    ref = {sid: add(clean, cases[sid], SIZES[sid]) for sid in good}
+    clean.run(steps)
+    ref_state = {sid: _state(clean, ref[sid][0], cases[sid]) for sid in good}
+
+    poisoned = {k: v for k, v in cases[bad_sid].items()}
+    u = poisoned["U_Na"]
+    data = u.data.copy()
+    g = [-v for v in u.lo]
+    data[g[0] + 3, g[1] + 2, g[2] + 5, 4] = np.nan  # energy of one owned cell
+    poisoned["U_Na"] = type(u)(u.lo, u.hi, data)
+
+    b = Batch(4, precision)
+    slots = {sid: add(b, cases[sid] if sid != bad_sid else poisoned, SIZES[sid]) for sid in (0, 1, 2)}
+    b.run(steps)
+    infos = b.poll()
+    from mpcns_mercury_b200.capi import STATUS
+
+    assert STATUS[infos[slots[bad_sid][0]].status] == "ERR_NONFINITE"
+    assert infos[slots[bad_sid][0]].step == 0
+    for sid in good:
+        slot = slots[sid][0]
+        assert infos[slot].status == 0 and infos[slot].step == steps
+        assert _same(_state(b, slot, cases[sid]), ref_state[sid]), sid
+    for bb, ss in ((clean, ref), (b, slots)):
+        for _, d in ss.values():
+            d.close()
+        bb.close()

@@ -18,12 +18,14 @@ def _owned(arr, lo, hi):
     return arr[g[0]:hi[0], g[1]:hi[1], g[2]:hi[2]]
 
 
-@pytest.fixture(scope="module")
-def both(ref_oracle):
+@pytest.fixture(scope="module", params=[6, (5, 7, 9)], ids=["cube6", "box5x7x9"])
+def both(ref_oracle, request):
+    """The 6^3 cube and a non-cubic periodic box (per-axis cell counts, the
+    ensemble's block shapes) set up by both sides."""
     from mpcns_mercury_b200 import setup as S
 
-    n = 6
-    d = ref_oracle.cube_run(n=n, steps=0, dump_at=[0])
+    n = request.param
+    d = ref_oracle.cube_run(n=n if isinstance(n, int) else " ".join(map(str, n)), steps=0, dump_at=[0])
     _, f = S.cube_case(n)
     return d, f
 

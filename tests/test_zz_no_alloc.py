@@ -40,9 +40,9 @@ class HallBlock(ctypes.Structure):
                 ("M_Na", ctypes.c_double), ("M_ref", ctypes.c_double), ("ne_hall_floor", ctypes.c_double)]
 
 
-def _block(ctx, n, consts):
+def _block(ctx, cells, consts):
     blk = HallBlock()
-    blk.n[:] = [n, n, n]
+    blk.n[:] = list(cells)
     blk.nghost = 4
     _, G, si, sj, _ = _view(ctx, "U_H")
     blk.G, blk.si, blk.sj = G, si, sj
@@ -63,7 +63,10 @@ def _block(ctx, n, consts):
     return blk, G, si, sj
 
 
-def test_static_scratch_hall_emf_matches_step():
+@pytest.mark.parametrize("cells", [(16, 16, 16), (12, 16, 20)], ids=["cube16", "box12x16x20"])
+def test_static_scratch_hall_emf_matches_step(cells):
+    """A cube and a block with three different extents (a swapped axis in the
+    scratch or launch indexing would still pass on a cube)."""
     if not has_gpu():
         pytest.skip("no GPU")
     import torch
@@ -75,31 +78,31 @@ def test_static_scratch_hall_emf_matches_step():
     L = capi.lib()
     L.mhd_hall_emf_static_scratch.argtypes = [ctypes.POINTER(HallBlock), ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_void_p]
-    n = 16
-    _, fields = S.cube_case(n)
-    ctx, _ = make_context([(n, n, n)], [fields])
+    L.mhd_last_error.restype = ctypes.c_char_p
+    _, fields = S.cube_case(cells)
+    ctx, _ = make_context([cells], [fields])
     consts = reference_constants(cfl=0.4)
     try:
         _, G, si, sj, ext = _view(ctx, "U_H")
         for call in range(2):
-            blk, G, si, sj = _block(ctx, n, consts)
+            blk, G, si, sj = _block(ctx, cells, consts)
             # the caller's own output buffers (memory the caller already owns)
             outs = [torch.full((ext[0] * si,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(3)]
             torch.cuda.synchronize()
             rc = L.mhd_hall_emf_static_scratch(ctypes.byref(blk), outs[0].data_ptr(), outs[1].data_ptr(),
                                                outs[2].data_ptr(), ctx.stream())
-            assert rc == 0, capi.lib().mhd_last_error()
+            assert rc == 0, L.mhd_last_error()
             ctx.synchronize()
             ctx.step(1)  # the existing entry point computes the same Hall EMF inside the step
             for a, (fld, stag) in enumerate((("EHALL_XI", (0, 1, 1)), ("EHALL_ETA", (1, 0, 1)),
                                              ("EHALL_ZETA", (1, 1, 0)))):
-                hi = tuple(n + s for s in stag)
+                hi = tuple(c + s for c, s in zip(cells, stag))
                 want = ctx.download(fld, (0, 0, 0), hi)[..., 0]
                 box = outs[a].cpu().numpy().reshape(ext[0], ext[1], sj)
                 got = box[G:G + hi[0], G:G + hi[1], G:G + hi[2]]
                 # owned edges that are not periodic aliases (alias edges take
                 # their owner's value in the step's Ehall sync)
-                sl = tuple(slice(0, n) for _ in range(3))
+                sl = tuple(slice(0, c) for c in cells)
                 g, w = got[sl], want[sl]
                 assert np.all(np.isfinite(g)), (call, fld)
                 err = np.linalg.norm((g - w).ravel()) / np.linalg.norm(w.ravel())
@@ -117,8 +120,10 @@ def test_rejects_blocks_beyond_the_static_scratch():
     L.mhd_hall_emf_static_scratch.argtypes = [ctypes.POINTER(HallBlock), ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_void_p]
     blk = HallBlock()
-    blk.n[:] = [200, 200, 200]  # (200 + 8)^3 cells > MHD_HALL_SCRATCH_MAX_CELLS
+    blk.n[:] = [200, 200, 200]  # (200 + 2)^3 scratch cells > MHD_HALL_SCRATCH_MAX_CELLS
     blk.nghost, blk.G = 4, 5
+    blk.sj = 200 + 1 + 2 * 5
+    blk.si = blk.sj * (200 + 1 + 2 * 5)
     dummy = 16  # non-null placeholders: rejected before any device access
     for name in ("rho_H", "rho_Na"):
         setattr(blk, name, dummy)
@@ -127,3 +132,11 @@ def test_rejects_blocks_beyond_the_static_scratch():
         for a in range(3):
             arr[a] = dummy
     assert L.mhd_hall_emf_static_scratch(ctypes.byref(blk), dummy, dummy, dummy, None) == 1  # MHD_ERR_ARG
+    # a block that fits, with strides smaller than its box (k extent
+    # n + 1 + 2G, j extent n + 1 + 2G): rejected, nothing touches the device
+    blk.n[:] = [10, 12, 14]
+    blk.sj, blk.si = 14 + 1 + 2 * 5 - 1, (14 + 1 + 2 * 5) * (12 + 1 + 2 * 5)
+    assert L.mhd_hall_emf_static_scratch(ctypes.byref(blk), dummy, dummy, dummy, None) == 1
+    blk.sj = 14 + 1 + 2 * 5
+    blk.si = blk.sj * (12 + 1 + 2 * 5) - 1
+    assert L.mhd_hall_emf_static_scratch(ctypes.byref(blk), dummy, dummy, dummy, None) == 1
