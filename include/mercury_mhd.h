@@ -89,6 +89,20 @@ enum mhd_location { MHD_CELL = 0, MHD_FACE_XI, MHD_FACE_ETA, MHD_FACE_ZETA, MHD_
 enum mhd_group { MHD_SYNC_UCELL = 0, MHD_SYNC_BFACE, MHD_SYNC_EHALL, MHD_SYNC_EEDGE, MHD_SYNC_B_CELL,
                  MHD_SYNC_JEDGE, MHD_SYNC_J_CELL, MHD_NUM_GROUPS };
 
+/* Indices into mhd_constants.bc (BuildMercuryBackgroundState,
+ * Z4_Mercury/include/0_BackgroundState.h:18-85, and the wall floors of
+ * BC_Solid_Surface_) */
+enum mhd_bc_const {
+  MHD_BC_QINF = 0,        /* 5: upstream H+ conserved state */
+  MHD_BC_QINFS = 5,       /* 5: upstream Na+ conserved state */
+  MHD_BC_BIMF = 10,       /* 3: IMF */
+  MHD_BC_ZERO = 13,       /* 0.0 */
+  MHD_BC_NA_RHO_FLOOR = 14, /* 1e-12 */
+  MHD_BC_NA_E_FLOOR = 15, /* 1e-12 / (gamma - 1) */
+  MHD_BC_UINF = 16,       /* 3: upstream velocity */
+  MHD_NUM_BC = 19
+};
+
 /* Physical constants as calc_physical_constant derives them (Tools.cpp:3-48). */
 typedef struct mhd_constants {
   double gamma, M_H, M_Na, M_ref, T_ref, L_ref, U_ref, B_ref, n_ref, rho_ref, m_Na, k_Boltz, q_e, mu0;
@@ -115,6 +129,8 @@ typedef struct mhd_constants {
   double res_rtol;
   int32_t resistive;  /* is_Mercury_resistance */
   int32_t res_max_it;
+  /* values of the physical boundary operations (mhd_bc_const) */
+  double bc[MHD_NUM_BC];
 } mhd_constants;
 
 /* One DOF reference in the FieldBlock index space. */
@@ -130,10 +146,43 @@ typedef struct mhd_copy {
   double sign;
 } mhd_copy;
 
+/* Physical boundary operations of a sync group (BoundaryCore::ApplyPhysical
+ * with the handlers MercuryBoundary::InstallHandlers registers,
+ * Z4_Mercury/src/boundary/Boundary_Build.cpp:5-300), run before the group's
+ * copies.  The copies of a boundary handler (ghost <- boundary layer) are
+ * ordinary entries of the group's halo table; these are the operations that
+ * compute a value:
+ *   MHD_PHYS_SET   dst <- mhd_constants.bc[arg] (farfield states, IMF, floors, zero)
+ *   MHD_PHYS_WALL  the solid-wall state of BC_Solid_Surface_
+ *                  (Z4_Mercury/src/boundary/Boundary_Condition_Fluid.cpp:37-259) on the
+ *                  five components of cell dst from cell src (one cell deeper
+ *                  in the fluid), then on the nghost ghost cells outward of
+ *                  dst along direction arg (+-1, +-2, +-3), clamped to the
+ *                  allocated range
+ *   MHD_PHYS_EFAR  edge dst <- E_inf . dr(dst), E_inf = -u_inf x B_imf
+ *                  (BC_Farfield_Eedge_set_zerocurl,
+ *                  Z4_Mercury/src/boundary/Boundary_Condition.cpp:573-624) */
+enum mhd_phys_kind { MHD_PHYS_SET = 0, MHD_PHYS_WALL = 1, MHD_PHYS_EFAR = 2 };
+typedef struct mhd_phys_op {
+  int32_t kind, arg;
+  mhd_dof dst, src;
+} mhd_phys_op;
+
+/* A pseudo field of mhd_dof: slot `i` of the solve's staging area.  A sync
+ * copy whose source the same copy phase overwrites (the reference's halo
+ * exchange packs every source before it writes, src/4_halo/component_copy/
+ * HaloExchangeInner.cpp:93-160) goes through a staging slot. */
+#define MHD_STAGING 1000
+
 typedef struct mhd_sync_group {
   int32_t n_halo, n_owner;
   const mhd_copy *halo;
   const mhd_copy *owner;
+  int32_t n_phys, n_stash;
+  const mhd_phys_op *phys;   /* physical boundary operations, run first */
+  const mhd_copy *stash;     /* 2 n_stash entries: n_stash copies staging <- source (after the
+                                physical operations), then n_stash copies destination <- staging
+                                (after the halo copies) */
 } mhd_sync_group;
 
 /* Edge alias classes (global_id order): class c has members
@@ -148,6 +197,37 @@ typedef struct mhd_alias_classes {
   const double *owner_sign;
 } mhd_alias_classes;
 
+/* Singular (valence-3) physical edges of a multi-block grid
+ * (SingularEdgeRegistry, src/7_metric/SingularEdgeRegistry.cpp:78-332): the
+ * owner edge of each, its aliases (for the mean length and the canonical
+ * edge vector), the incident cells (EMF and Hall EMF: weighted by |Jac|) and
+ * the incident owner faces (the current).  Weights, the canonical vector and
+ * the inverse Hodge star are computed on the device from the uploaded
+ * geometry when the solve is prepared. */
+typedef struct mhd_singular_alias {
+  mhd_dof edge;       /* field = edge axis 0/1/2 */
+  int32_t orient, pad_;
+} mhd_singular_alias;
+typedef struct mhd_singular_cell {
+  mhd_dof cell;
+  int32_t axis, orient; /* axis and orientation of the alias the cell was reached from */
+} mhd_singular_cell;
+typedef struct mhd_singular_face {
+  mhd_dof face;         /* field = face axis 0/1/2 */
+  int32_t sign, pad_;   /* incidence sign x alias orientation (0: no contribution) */
+} mhd_singular_face;
+typedef struct mhd_singular_edges {
+  int32_t n_edges;
+  const mhd_dof *owner;             /* field = edge axis 0/1/2 */
+  const double *owner_sign;
+  const int32_t *alias_offset;      /* n_edges + 1 */
+  const mhd_singular_alias *aliases;
+  const int32_t *cell_offset;       /* n_edges + 1 */
+  const mhd_singular_cell *cells;
+  const int32_t *face_offset;       /* n_edges + 1 */
+  const mhd_singular_face *faces;
+} mhd_singular_edges;
+
 typedef struct mhd_desc {
   int32_t n_blocks;
   const int32_t *cells;   /* n_blocks * 3: cells per axis (mx, my, mz) */
@@ -156,6 +236,13 @@ typedef struct mhd_desc {
   mhd_constants constants;
   mhd_sync_group groups[MHD_NUM_GROUPS];
   mhd_alias_classes edge_aliases;
+  /* multi-block grids with physical boundaries (zero / NULL otherwise) */
+  int32_t n_staging;               /* staging slots the groups' stash copies use */
+  int32_t n_wall;
+  const mhd_phys_op *wall;         /* the step's wall EMF: E_t = 0 on solid-wall edges
+                                      (ApplyStationaryWallNonResistiveEMF_,
+                                      Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:5-88) */
+  mhd_singular_edges singular;
 } mhd_desc;
 
 typedef struct mhd_ctx mhd_ctx;
@@ -390,6 +477,48 @@ int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghost, mhd_topo
  * blocks. */
 int mhd_topology_periodic_lattice(const int32_t cells[3], const int32_t blocks[3], int32_t nghost,
                                   mhd_topology **out);
+/* A general multi-block grid: blocks of cells[3 b .. 3 b + 2] cells, their
+ * inner face patches in the reference's topology order
+ * (Topology::inner_patches, TOPO::build_topology,
+ * src/2_topology/TopologyBuilder.cpp:436; node boxes half-open, the node
+ * index map this -> nb: nb[perm[a]] = sign[a] * this[a] + offset[a],
+ * src/2_topology/TopologyOps.cpp:77-230) and physical patches
+ * (Farfield or the solid wall, Coupled-Solid).  The builder derives the edge
+ * and vertex patches as the reference does
+ * (src/2_topology/TopologyEdge.cpp:45-345), replays every sync group of
+ * MercuryBoundary::Sync (physical handlers, the three halo stages with the
+ * reference's exchange rules, owner-to-alias copies;
+ * Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110) on symbolic DOF values and
+ * flattens the result into the descriptor's tables; it also builds the face
+ * and edge equivalence classes (owner = smallest (block, i, j, k), canonical
+ * orientation from the smallest node representatives,
+ * src/2_topology/TopologyQuery.cpp:104-190), the edge alias classes, the
+ * singular-edge lists and the wall-EMF edges.  resistive selects the
+ * handler set of is_Mercury_resistance. */
+typedef struct mhd_patch {
+  int32_t this_block, nb_block, direction, nb_direction;
+  int32_t this_lo[3], this_hi[3], nb_lo[3], nb_hi[3];
+  int32_t perm[3], sign[3], offset[3];
+  int32_t dir3;   /* edge and vertex patches: direction, dir2, dir3 are their face directions */
+} mhd_patch;
+enum mhd_bc_kind { MHD_BC_FARFIELD = 0, MHD_BC_SOLID = 1 };
+typedef struct mhd_physical_patch {
+  int32_t block, direction, bc, pad_;
+  int32_t lo[3], hi[3];
+} mhd_physical_patch;
+int mhd_topology_multiblock(int32_t n_blocks, const int32_t *cells, int32_t nghost, int32_t n_faces,
+                            const mhd_patch *faces, int32_t n_physical, const mhd_physical_patch *physical,
+                            int32_t resistive, mhd_topology **out);
+/* The 6-panel gnomonic cubed-sphere shell of na x na x nr cells per panel
+ * (panel axes: i, j angular, k radial; the panel numbering and patch order
+ * of the oracle's shell case): inner sphere k = 0 a solid wall, outer sphere
+ * k = nr Farfield, eight valence-3 radial lines. */
+int mhd_topology_cubed_sphere(int32_t na, int32_t nr, int32_t nghost, int32_t resistive, mhd_topology **out);
+/* The patches a multi-block builder used: which = 0 inner face patches,
+ * 1 inner edge patches, 2 inner vertex patches (direction/nb_direction/dir3
+ * hold the edge's or vertex's face directions); and the physical patches. */
+int mhd_topology_patches(const mhd_topology *topo, int32_t which, const mhd_patch **patches, int32_t *n);
+int mhd_topology_physical(const mhd_topology *topo, const mhd_physical_patch **patches, int32_t *n);
 int mhd_topology_fill_desc(const mhd_topology *topo, mhd_desc *desc);
 int mhd_topology_destroy(mhd_topology *topo);
 

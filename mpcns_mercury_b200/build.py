@@ -25,6 +25,7 @@ UNITS = [
     ("mhd_kernels.cu", "mhd_kernels_f32.o", FAST32),
     ("mhd_ctx.cu", "mhd_ctx.o", EXACT),
     ("mhd_topology.cpp", "mhd_topology.o", EXACT),
+    ("mhd_multiblock.cpp", "mhd_multiblock.o", EXACT),
     ("mhd_noalloc.cu", "mhd_noalloc.o", EXACT),
     ("mhd_host_setup.cpp", "mhd_host_setup.o", EXACT),
     ("mhd_restart.cpp", "mhd_restart.o", EXACT),

@@ -71,7 +71,14 @@ class MhdConstants(ctypes.Structure):
         "momentum_induce_coeff", "momentum_hall_coeff", "inver_MA2", "ne_hall_floor",
         "arti_eta_max", "arti_J_start", "arti_J_on")] + [
         ("ambipolar", ctypes.c_int32), ("local_arti", ctypes.c_int32), ("res_rtol", ctypes.c_double),
-        ("resistive", ctypes.c_int32), ("res_max_it", ctypes.c_int32)]
+        ("resistive", ctypes.c_int32), ("res_max_it", ctypes.c_int32), ("bc", ctypes.c_double * 19)]
+
+
+# indices into MhdConstants.bc (enum mhd_bc_const)
+BC_QINF, BC_QINFS, BC_BIMF, BC_ZERO, BC_NA_RHO_FLOOR, BC_NA_E_FLOOR, BC_UINF = 0, 5, 10, 13, 14, 15, 16
+MHD_STAGING = 1000  # pseudo field of a staging slot in MhdDof
+PHYS_SET, PHYS_WALL, PHYS_EFAR = 0, 1, 2
+BC_FARFIELD, BC_SOLID = 0, 1
 
 
 class MhdDof(ctypes.Structure):
@@ -82,9 +89,15 @@ class MhdCopy(ctypes.Structure):
     _fields_ = [("dst", MhdDof), ("src", MhdDof), ("sign", ctypes.c_double)]
 
 
+class MhdPhysOp(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("arg", ctypes.c_int32), ("dst", MhdDof), ("src", MhdDof)]
+
+
 class MhdSyncGroup(ctypes.Structure):
     _fields_ = [("n_halo", ctypes.c_int32), ("n_owner", ctypes.c_int32),
-                ("halo", ctypes.POINTER(MhdCopy)), ("owner", ctypes.POINTER(MhdCopy))]
+                ("halo", ctypes.POINTER(MhdCopy)), ("owner", ctypes.POINTER(MhdCopy)),
+                ("n_phys", ctypes.c_int32), ("n_stash", ctypes.c_int32),
+                ("phys", ctypes.POINTER(MhdPhysOp)), ("stash", ctypes.POINTER(MhdCopy))]
 
 
 class MhdAliasClasses(ctypes.Structure):
@@ -93,10 +106,43 @@ class MhdAliasClasses(ctypes.Structure):
                 ("owner", ctypes.POINTER(MhdDof)), ("owner_sign", ctypes.POINTER(ctypes.c_double))]
 
 
+class MhdSingularAlias(ctypes.Structure):
+    _fields_ = [("edge", MhdDof), ("orient", ctypes.c_int32), ("pad_", ctypes.c_int32)]
+
+
+class MhdSingularCell(ctypes.Structure):
+    _fields_ = [("cell", MhdDof), ("axis", ctypes.c_int32), ("orient", ctypes.c_int32)]
+
+
+class MhdSingularFace(ctypes.Structure):
+    _fields_ = [("face", MhdDof), ("sign", ctypes.c_int32), ("pad_", ctypes.c_int32)]
+
+
+class MhdSingularEdges(ctypes.Structure):
+    _fields_ = [("n_edges", ctypes.c_int32), ("owner", ctypes.POINTER(MhdDof)),
+                ("owner_sign", ctypes.POINTER(ctypes.c_double)), ("alias_offset", ctypes.POINTER(ctypes.c_int32)),
+                ("aliases", ctypes.POINTER(MhdSingularAlias)), ("cell_offset", ctypes.POINTER(ctypes.c_int32)),
+                ("cells", ctypes.POINTER(MhdSingularCell)), ("face_offset", ctypes.POINTER(ctypes.c_int32)),
+                ("faces", ctypes.POINTER(MhdSingularFace))]
+
+
 class MhdDesc(ctypes.Structure):
     _fields_ = [("n_blocks", ctypes.c_int32), ("cells", ctypes.POINTER(ctypes.c_int32)),
                 ("nghost", ctypes.c_int32), ("precision", ctypes.c_int32), ("constants", MhdConstants),
-                ("groups", MhdSyncGroup * 7), ("edge_aliases", MhdAliasClasses)]
+                ("groups", MhdSyncGroup * 7), ("edge_aliases", MhdAliasClasses),
+                ("n_staging", ctypes.c_int32), ("n_wall", ctypes.c_int32), ("wall", ctypes.POINTER(MhdPhysOp)),
+                ("singular", MhdSingularEdges)]
+
+
+class MhdPatch(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("this_block", "nb_block", "direction", "nb_direction")] + [
+        (n, ctypes.c_int32 * 3) for n in ("this_lo", "this_hi", "nb_lo", "nb_hi", "perm", "sign", "offset")] + [
+        ("dir3", ctypes.c_int32)]
+
+
+class MhdPhysicalPatch(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("block", "direction", "bc", "pad_")] + [
+        ("lo", ctypes.c_int32 * 3), ("hi", ctypes.c_int32 * 3)]
 
 
 class MhdInfo(ctypes.Structure):
@@ -131,6 +177,7 @@ EXPORTS = [
     "mhd_ctx_create", "mhd_ctx_destroy", "mhd_upload_field", "mhd_download_field", "mhd_prepare", "mhd_step",
     "mhd_step_async", "mhd_synchronize", "mhd_sync", "mhd_get_info", "mhd_get_status", "mhd_field_info", "mhd_stream",
     "mhd_kernels_per_step", "mhd_device_view", "mhd_last_error", "mhd_topology_periodic_block", "mhd_topology_periodic_lattice",
+    "mhd_topology_multiblock", "mhd_topology_cubed_sphere", "mhd_topology_patches", "mhd_topology_physical",
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
     "mhd_save_restart", "mhd_load_restart", "mhd_tecplot_write", "mhd_rundata_write", "mhd_rundata_read", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
@@ -179,6 +226,14 @@ def lib() -> ctypes.CDLL:
     L.mhd_device_view.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                   i32p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), i32p]
     L.mhd_last_error.restype = ctypes.c_char_p
+    L.mhd_topology_cubed_sphere.argtypes = [ctypes.c_int32] * 4 + [ctypes.POINTER(P)]
+    L.mhd_topology_multiblock.argtypes = [ctypes.c_int32, i32p, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.POINTER(MhdPatch), ctypes.c_int32, ctypes.POINTER(MhdPhysicalPatch),
+                                          ctypes.c_int32, ctypes.POINTER(P)]
+    L.mhd_topology_patches.argtypes = [P, ctypes.c_int32, ctypes.POINTER(ctypes.POINTER(MhdPatch)),
+                                       ctypes.POINTER(ctypes.c_int32)]
+    L.mhd_topology_physical.argtypes = [P, ctypes.POINTER(ctypes.POINTER(MhdPhysicalPatch)),
+                                        ctypes.POINTER(ctypes.c_int32)]
     L.mhd_topology_periodic_block.argtypes = [i32p, ctypes.c_int32, ctypes.POINTER(P)]
     L.mhd_topology_periodic_lattice.argtypes = [i32p, i32p, ctypes.c_int32, ctypes.POINTER(P)]
     L.mhd_topology_fill_desc.argtypes = [P, ctypes.POINTER(MhdDesc)]

@@ -15,7 +15,9 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
                         M_H: float = 0.001, M_Na: float = 0.023, arti_eta_max: float = 0.0,
                         arti_J_start: float = 800.0, arti_J_on: float = 3000.0,
                         local_arti: bool = False, resistive: bool = False, res_rtol: float = 1e-13,
-                        res_max_it: int = 500) -> MhdConstants:
+                        res_max_it: int = 500, initial=None) -> MhdConstants:
+    if initial is None:
+        initial = DEFAULT_INITIAL
     c = MhdConstants()
     c.gamma = gamma
     c.q_e = q_e
@@ -50,4 +52,37 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
     c.resistive = 1 if resistive else 0
     c.res_rtol = res_rtol
     c.res_max_it = res_max_it
+    set_boundary(c, gamma=gamma, NA=NA, R_uni=R_uni, U_ref=U_ref, T_ref=T_ref, n_ref=n_ref, M_ref=M_ref,
+                 B_ref=B_ref, initial=initial)
+    return c
+
+
+# The reference's default INITIAL list (Z4_Mercury/9999setup/1_Initial_condition.txt):
+# U, T, n, Molecular_mass, c_y, c_z, Bx, By, Bz (SI)
+DEFAULT_INITIAL = (4.03112887e5, 1.7407e5, 4e7, 0.001, 1.240347346e-1, 0.0, 0.0, 0.0, 0.0)
+
+
+def set_boundary(c, gamma=1.6667, NA=6.02e23, R_uni=8.314, U_ref=4.031e5, T_ref=1.7407e5, n_ref=4e7,
+                 M_ref=0.001, B_ref=1e-9, initial=DEFAULT_INITIAL, rho_small=1e-6):
+    """The values of the physical boundary operations (mhd_constants.bc):
+    the upstream states of both species, the IMF and the upstream velocity as
+    BuildMercuryBackgroundState derives them from the INITIAL and REF lists
+    (Z4_Mercury/include/0_BackgroundState.h:18-85), zero, and the Na+ floor
+    state of the solid wall (Z4_Mercury/src/boundary/Boundary_Condition_Fluid.cpp:59-170)."""
+    import math
+
+    U, T, n, Mm, c_y, c_z, Bx, By, Bz = initial
+    k_B = R_uni / NA
+    rho_ref = M_ref / NA * n_ref
+    rho0 = (n / n_ref) * (Mm / M_ref)
+    c_x = -math.sqrt(1.0 - c_y * c_y - c_z * c_z)
+    u0, v0, w0 = c_x * U / U_ref, c_y * U / U_ref, c_z * U / U_ref
+    p0 = n * k_B * T / (rho_ref * U_ref * U_ref)
+    qinf = [rho0, rho0 * u0, rho0 * v0, rho0 * w0, 0.5 * rho0 * (u0 * u0 + v0 * v0 + w0 * w0) + p0 / (gamma - 1.0)]
+    pN = p0 * rho_small / 23.0
+    rhoN = rho_small * rho0
+    qinfs = [rhoN, 0.0, 0.0, 0.0, pN / (gamma - 1.0) + 0.5 * rhoN * (0.0 * 0.0 + 0.0 * 0.0 + 0.0 * 0.0)]
+    vals = qinf + qinfs + [Bx / B_ref, By / B_ref, Bz / B_ref, 0.0, 1.0e-12, 1.0e-12 / (gamma - 1.0), u0, v0, w0]
+    for q, v in enumerate(vals):
+        c.bc[q] = v
     return c

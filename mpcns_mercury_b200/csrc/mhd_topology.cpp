@@ -3,7 +3,6 @@
 // periodic in every direction, or for a periodic box cut into a lattice of
 // aligned blocks, from the walks of mhd_periodic.h.
 #include <cstdint>
-#include <memory>
 #include <new>
 #include <vector>
 
@@ -12,25 +11,7 @@
 #include "mhd_parallel.h"
 #include "mhd_periodic.h"
 
-// A copy table whose entries are written once, by the building threads (no
-// zero-fill of a freshly allocated table).
-struct CopyTable {
-  std::unique_ptr<mhd_copy[]> p;
-  size_t n = 0;
-  void allocate(size_t count) {
-    p.reset(count ? new mhd_copy[count] : nullptr);
-    n = count;
-  }
-  mhd_copy *data() const { return p.get(); }
-  size_t size() const { return n; }
-};
-
-struct mhd_topology {
-  CopyTable halo[MHD_NUM_GROUPS], owner[MHD_NUM_GROUPS];
-  std::vector<int32_t> alias_offset;
-  std::vector<mhd_dof> alias_member, alias_owner;
-  std::vector<double> alias_msign, alias_osign;
-};
+#include "mhd_topology_impl.h"
 
 namespace {
 
@@ -162,7 +143,24 @@ extern "C" int mhd_topology_fill_desc(const mhd_topology *t, mhd_desc *d) {
     d->groups[g].halo = t->halo[g].data();
     d->groups[g].n_owner = (int32_t)t->owner[g].size();
     d->groups[g].owner = t->owner[g].data();
+    d->groups[g].n_phys = (int32_t)t->phys[g].size();
+    d->groups[g].phys = t->phys[g].data();
+    d->groups[g].n_stash = (int32_t)(t->stash[g].size() / 2);
+    d->groups[g].stash = t->stash[g].data();
   }
+  d->n_staging = t->n_staging;
+  d->n_wall = (int32_t)t->wall.size();
+  d->wall = t->wall.data();
+  mhd_singular_edges &s = d->singular;
+  s.n_edges = (int32_t)t->sing_owner.size();
+  s.owner = t->sing_owner.data();
+  s.owner_sign = t->sing_owner_sign.data();
+  s.alias_offset = t->sing_alias_offset.data();
+  s.aliases = t->sing_aliases.data();
+  s.cell_offset = t->sing_cell_offset.data();
+  s.cells = t->sing_cells.data();
+  s.face_offset = t->sing_face_offset.data();
+  s.faces = t->sing_faces.data();
   d->edge_aliases.n_classes = (int32_t)t->alias_owner.size();
   d->edge_aliases.offset = t->alias_offset.data();
   d->edge_aliases.member = t->alias_member.data();

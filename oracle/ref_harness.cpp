@@ -856,6 +856,68 @@ void dump_edge_classes(TOPO::Topology &topo, Dumper &d) {
   d.rec("edge_alias_classes", -1, l, h, 1, buf.data());
 }
 
+// The reference's topology patch lists (TOPO::Topology, built by
+// TOPO::build_topology, src/2_topology/TopologyBuilder.cpp:436) as int32
+// records, so that a multi-block table builder can be pinned patch for patch:
+//   record "topo_faces":    per inner patch  this_block nb_block direction nb_direction
+//                           this_box_node lo[3] hi[3]  nb_box_node lo[3] hi[3]  perm[3] sign[3] offset[3]
+//   record "topo_edges":    per inner edge patch  this_block nb_block dir1 dir2 this lo/hi nb lo/hi perm sign offset
+//   record "topo_vertices": per inner vertex patch  this_block nb_block dir1 dir2 dir3 this lo/hi nb lo/hi perm sign offset
+//   record "topo_physical": per physical patch  this_block direction bc_id this lo/hi
+//   record "topo_phys_edges" / "topo_phys_vertices": physical edge / vertex patches (block dir1 dir2 [dir3] lo/hi)
+void dump_topology(TOPO::Topology &t, Dumper &d) {
+  auto box = [](std::vector<double> &b, const Box3 &x) {
+    for (int v : {x.lo.i, x.lo.j, x.lo.k, x.hi.i, x.hi.j, x.hi.k}) b.push_back(v);
+  };
+  auto tr = [](std::vector<double> &b, const TOPO::IndexTransform &x) {
+    for (int a = 0; a < 3; ++a) b.push_back(x.perm[a]);
+    for (int a = 0; a < 3; ++a) b.push_back(x.sign[a]);
+    for (int v : {x.offset.i, x.offset.j, x.offset.k}) b.push_back(v);
+  };
+  auto emit = [&](const char *name, std::vector<double> &b) {
+    if (b.empty()) b.push_back(-1.0);
+    const int l[3] = {0, 0, 0}, h[3] = {(int)b.size(), 1, 1};
+    d.rec(name, -1, l, h, 1, b.data());
+  };
+  std::vector<double> f, e, v, p, pe, pv;
+  for (const auto &x : t.inner_patches) {
+    for (int q : {x.this_block, x.nb_block, x.direction, x.nb_direction, (int)x.is_coupling}) f.push_back(q);
+    box(f, x.this_box_node);
+    box(f, x.nb_box_node);
+    tr(f, x.trans);
+  }
+  for (const auto &x : t.inner_edge_patches) {
+    for (int q : {x.this_block, x.nb_block, x.dir1, x.dir2, (int)x.is_coupling}) e.push_back(q);
+    box(e, x.this_box_node);
+    box(e, x.nb_box_node);
+    tr(e, x.trans);
+  }
+  for (const auto &x : t.inner_vertex_patches) {
+    for (int q : {x.this_block, x.nb_block, x.dir1, x.dir2, x.dir3, (int)x.is_coupling}) v.push_back(q);
+    box(v, x.this_box_node);
+    box(v, x.nb_box_node);
+    tr(v, x.trans);
+  }
+  for (const auto &x : t.physical_patches) {
+    for (int q : {x.this_block, x.direction, x.bc_id}) p.push_back(q);
+    box(p, x.this_box_node);
+  }
+  for (const auto &x : t.physical_edge_patches) {
+    for (int q : {x.this_block, x.dir1, x.dir2}) pe.push_back(q);
+    box(pe, x.this_box_node);
+  }
+  for (const auto &x : t.physical_vertex_patches) {
+    for (int q : {x.this_block, x.dir1, x.dir2, x.dir3}) pv.push_back(q);
+    box(pv, x.this_box_node);
+  }
+  emit("topo_faces", f);
+  emit("topo_edges", e);
+  emit("topo_vertices", v);
+  emit("topo_physical", p);
+  emit("topo_phys_edges", pe);
+  emit("topo_phys_vertices", pv);
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -909,6 +971,9 @@ int main(int argc, char **argv) {
       if (job_int("dump_grid", 0)) dump_grid(d, grd);
       probe_group(S, job_str("probe_group"), d);
     } else if (mode == "classes") {
+      dump_edge_classes(topology, d);
+    } else if (mode == "topology") {
+      dump_topology(topology, d);
       dump_edge_classes(topology, d);
     } else {
       const std::string init = job_str("init", "ot");
