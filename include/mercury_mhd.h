@@ -74,6 +74,7 @@ enum mhd_field {
   MHD_BCELL_W, MHD_JCELL_W, MHD_BADD_XI, MHD_BADD_ETA, MHD_BADD_ZETA, MHD_PHOTO,
   MHD_CELL_X, MHD_CELL_Y, MHD_CELL_Z,                              /* cell centres */
   MHD_TAPER_XI, MHD_TAPER_ETA, MHD_TAPER_ZETA,                     /* Hall radial taper per edge */
+  MHD_TAPER_CELL,                                                  /* Hall radial taper at cell centres (singular edges) */
   MHD_LOCAL_ETA_XI, MHD_LOCAL_ETA_ETA, MHD_LOCAL_ETA_ZETA,         /* local artificial resistivity per edge */
   MHD_ETA_RES_XI, MHD_ETA_RES_ETA, MHD_ETA_RES_ZETA,               /* implicit resistivity per owned edge */
   /* work of the implicit resistive solve (3 components: xi, eta, zeta edges;
@@ -338,6 +339,16 @@ int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base,
  * workload definition states, so that host-generated initial states are
  * byte-identical to the ones the CPU oracle generates. */
 int mhd_seeded_uniform(uint64_t seed, int64_t count, double a, double *out);
+
+/* Host helpers of the cubed-sphere shell case (no counterpart in the
+ * reference solver, which reads its grid from files): the nodes of panel
+ * `panel` over [-G, n + 1 + G) per axis (AoS, k fastest; the owned nodes are
+ * the oracle shell case's, the ghost nodes continue the panel mapping; the
+ * ghost angles must stay below 90 degrees: na > 2 G), and the Hall radial
+ * taper (HallRadialTaper_, Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:6-13)
+ * at n points. */
+int mhd_shell_nodes(int32_t na, int32_t nr, double r_out, int32_t panel, int32_t G, double *out);
+int mhd_hall_taper(double r_min, double r_max, int64_t n, const double *xyz, double *out);
 
 /* ---- Hall edge EMF without device allocation ----
  * No counterpart in the reference: it exists for callers that may not call

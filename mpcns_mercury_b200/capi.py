@@ -27,7 +27,7 @@ FIELDS = [
     "HODGE_FACE_XI", "HODGE_FACE_ETA", "HODGE_FACE_ZETA",
     "HODGE_EDGE_XI", "HODGE_EDGE_ETA", "HODGE_EDGE_ZETA",
     "BCELL_W", "JCELL_W", "BADD_XI", "BADD_ETA", "BADD_ZETA", "PHOTO",
-    "CELL_X", "CELL_Y", "CELL_Z", "TAPER_XI", "TAPER_ETA", "TAPER_ZETA",
+    "CELL_X", "CELL_Y", "CELL_Z", "TAPER_XI", "TAPER_ETA", "TAPER_ZETA", "TAPER_CELL",
     "LOCAL_ETA_XI", "LOCAL_ETA_ETA", "LOCAL_ETA_ZETA", "ETA_RES_XI", "ETA_RES_ETA", "ETA_RES_ZETA",
     "RES_W", "RES_X", "RES_R", "RES_P", "RES_Q", "RES_BSTAR",
 ]
@@ -55,6 +55,7 @@ REF_FIELD = {
     "Bcell_from_Bface_w": "BCELL_W", "Jcell_from_Jedge_w": "JCELL_W",
     "Badd_xi": "BADD_XI", "Badd_eta": "BADD_ETA", "Badd_zeta": "BADD_ZETA", "Photo_rate": "PHOTO",
     "divB": "DIVB", "taper_xi": "TAPER_XI", "taper_eta": "TAPER_ETA", "taper_zeta": "TAPER_ZETA",
+    "taper_cell": "TAPER_CELL",
     "eta_res_xi": "ETA_RES_XI", "eta_res_eta": "ETA_RES_ETA", "eta_res_zeta": "ETA_RES_ZETA",
     "local_arti_eta_xi": "LOCAL_ETA_XI", "local_arti_eta_eta": "LOCAL_ETA_ETA", "local_arti_eta_zeta": "LOCAL_ETA_ZETA",
 }
@@ -431,13 +432,17 @@ class Context:
         self.desc.precision = precision
         self.desc.constants = constants
         self._topo = ctypes.c_void_p()
-        if topology is None and lattice is not None:
+        self._owns_topo = topology is None
+        if topology is not None:  # a topology handle (mhd_topology_*) that fills the descriptor's tables
+            self._topo = topology
+            check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
+        elif lattice is not None:
             if len(cells) != lattice[0] * lattice[1] * lattice[2] or any(tuple(c) != tuple(cells[0]) for c in cells):
                 raise ValueError("a lattice has bx * by * bz blocks of equal cells")
             check(L.mhd_topology_periodic_lattice(_i3(cells[0]), _i3(lattice), nghost, ctypes.byref(self._topo)),
                   "mhd_topology_periodic_lattice")
             check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
-        elif topology is None and len(cells) == 1:
+        elif len(cells) == 1:
             check(L.mhd_topology_periodic_block(_i3(cells[0]), nghost, ctypes.byref(self._topo)),
                   "mhd_topology_periodic_block")
             check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")

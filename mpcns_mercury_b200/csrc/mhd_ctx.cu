@@ -117,8 +117,18 @@ struct Tables {
   int users = 0;
   int *dtile_prefix[kNumRanges] = {};
   int tiles[kNumRanges] = {};
-  int64_t *tab_seg[kMaxGroups][3] = {};
-  int tab_n[kMaxGroups][3] = {};  // segments; phase 0 halo (step depth), 1 owner, 2 halo (all)
+  int64_t *tab_seg[kMaxGroups][kNumPhases] = {};
+  int tab_n[kMaxGroups][kNumPhases] = {};  // segments per CopyPhase
+  // physical boundary operations (per group, then the wall EMF)
+  int64_t *ph_set[kNumPhys] = {};
+  DevPhysOp *ph_op[kNumPhys] = {};
+  int ph_nset[kNumPhys] = {}, ph_nop[kNumPhys] = {};
+  // singular edges (the geometric data is per solve)
+  int sg_n = 0, sg_ncell = 0;
+  int64_t *sg_owner = nullptr;
+  double *sg_osign = nullptr;
+  int *sg_aoff = nullptr, *sg_alias = nullptr, *sg_coff = nullptr, *sg_cell = nullptr, *sg_foff = nullptr,
+      *sg_face = nullptr;
   int32_t *al_off = nullptr;
   int64_t *al_memE = nullptr, *al_ownE = nullptr, *al_memJ = nullptr, *al_ownJ = nullptr;
   double *al_msign = nullptr, *al_osign = nullptr;
@@ -133,6 +143,9 @@ struct Solve {
   std::vector<Box> boxes;
   std::vector<int64_t> ubase, mbase;  // bytes
   int64_t ubuf = 0, main_off = 0, arena_bytes = 0;
+  int64_t staging_off = 0;  // the sync staging slots (real), after the fields
+  int n_staging = 0;
+  double *sg_geo = nullptr, *sg_w = nullptr;  // singular-edge geometry (k_sing_setup)
   char *arena = nullptr;
   DevBlock *dblocks = nullptr;
   Tables *T = nullptr;
@@ -157,6 +170,11 @@ struct Solve {
   // Arena code of a DOF (kCodeOffMask / kCodeUFlag in mhd_engine.cuh).
   int64_t code(const mhd_dof &d, bool *ok) const {
     *ok = false;
+    if (d.field == MHD_STAGING) {  // a staging slot
+      if (d.i < 0 || d.i >= n_staging) return 0;
+      *ok = true;
+      return staging_off + (int64_t)d.i * es;
+    }
     if (d.field < 0 || d.field >= MHD_NUM_FIELDS || d.block < 0 || d.block >= nblocks) return 0;
     if (d.comp < 0 || d.comp >= kFieldSpec[d.field].ncomp) return 0;
     const Box &bx = boxes[d.block];
@@ -188,14 +206,19 @@ struct mhd_batch {
   DevSolve *dsolves = nullptr;
   SolveState *dstate = nullptr;
   int *dprefix_tiles[kNumRanges] = {};
-  int *dprefix_copy[kMaxGroups][3] = {};
+  int *dprefix_copy[kMaxGroups][kNumPhases] = {};
+  int *dprefix_phys[kNumPhys] = {};
+  int *dprefix_sing = nullptr;
   int *dprefix_aliasE = nullptr, *dprefix_aliasJ = nullptr;
   cudaGraphExec_t graph = nullptr;
   cudaGraphExec_t graph_a = nullptr, graph_b = nullptr;  // the step split around implicit resistive solves
   cudaGraphExec_t graph_cg = nullptr;                   // the CG iteration loop of the masked solve
-  // solves whose pruned-halo (0) / owner (1) table of a group has entries:
-  // sync phases empty in every solve get no launch in the step
-  int live_tables[kMaxGroups][2] = {};
+  // solves whose table of a group's copy phase has entries: sync phases
+  // empty in every solve get no launch in the step (likewise the physical
+  // operations and the singular edges)
+  int live_tables[kMaxGroups][kNumPhases] = {};
+  int live_phys[kNumPhys] = {};
+  int live_sing = 0;
   int n_res = 0;                                        // slots whose solve has the implicit resistive substep
   // FP64 batch of the companions of mixed-precision resistive solves, which
   // runs on this batch's stream and pool (borrowed = true in the companion)
@@ -226,9 +249,11 @@ struct mhd_batch {
     d.mode = mode;
     for (int r = 0; r < kNumRanges; ++r) d.solve_tile_prefix[r] = dprefix_tiles[r];
     for (int g = 0; g < kMaxGroups; ++g)
-      for (int p = 0; p < 3; ++p) d.copy_prefix[g][p] = dprefix_copy[g][p];
+      for (int p = 0; p < kNumPhases; ++p) d.copy_prefix[g][p] = dprefix_copy[g][p];
     d.aliasE_prefix = dprefix_aliasE;
     d.aliasJ_prefix = dprefix_aliasJ;
+    for (int q = 0; q < kNumPhys; ++q) d.phys_prefix[q] = dprefix_phys[q];
+    d.sing_prefix = dprefix_sing;
     return d;
   }
 };
@@ -258,15 +283,15 @@ void launch(mhd_batch *b, int mode, StepKernel k, int *nk, const SyncOps *ops = 
   mark(b, step_kernel_name(k));
 }
 
-SyncOp copy_op(int g, int phase) { return SyncOp{SYNC_COPY, g, phase}; }
-SyncOp alias_op(int which) { return SyncOp{SYNC_ALIAS, which, 0}; }
+SyncOp copy_op(int g, int phase, int prev = 0) { return SyncOp{SYNC_COPY, g, phase, prev}; }
+SyncOp alias_op(int which) { return SyncOp{SYNC_ALIAS, which, 0, 0}; }
 
 // A sync operation some solve of the batch has work for (a copy phase whose
 // table is empty in every solve is left out: the depth-0 halos of E, E_Hall
 // and the J edges, and the owner phases of cell fields, which have no alias
 // DOFs).
 bool op_live(const mhd_batch *b, const SyncOp &o) {
-  return o.kind != SYNC_COPY || o.phase == 2 || b->live_tables[o.arg][o.phase] > 0;
+  return o.kind != SYNC_COPY || o.phase == kPhHaloFull || b->live_tables[o.arg][o.phase] > 0;
 }
 
 // One k_sync launch running one or two independent sync operations.
@@ -282,6 +307,21 @@ void sync2(mhd_batch *b, int mode, SyncOp a, SyncOp c, int *nk) {
   launch(b, mode, SK_SYNC, nk, &ops);
 }
 
+// The physical boundary operations of table `which` (a group, or the wall
+// EMF), when some solve has them.
+void phys1(mhd_batch *b, int mode, int which, int *nk) {
+  if (b->live_phys[which] > 0) launch(b, mode, SK_PHYS, nk, nullptr, which);
+}
+// Before a group's halo copies: its physical operations, then the staging of
+// the sources its halo copies overwrite; after them: the staged copies.
+// prev: the group's U ghosts hold their last synced values in the other
+// buffer (Sync(U) right after the step's buffer flip).
+void sync_pre(mhd_batch *b, int mode, int g, int *nk, int prev = 0) {
+  phys1(b, mode, g, nk);
+  sync1(b, mode, copy_op(g, kPhStash, prev), nk);
+}
+void sync_post(mhd_batch *b, int mode, int g, int *nk) { sync1(b, mode, copy_op(g, kPhUnstash), nk); }
+
 // Adds (d = +1) or removes (d = -1) a solve's step tables from the batch's
 // counts; true when a phase that no solve had entries for gains some (the
 // step graphs, which leave that phase out, must be captured anew).
@@ -289,22 +329,32 @@ bool count_tables(mhd_batch *b, const Solve *S, int d);
 void drop_graphs(mhd_batch *b);
 
 // MercuryBoundary::Sync(group) (Z4_Mercury/src/boundary/Boundary_Sync_.cpp:4-110):
-// the group's halo copies, then its owner copies.  full: every ghost layer
-// (mhd_sync); otherwise the layers the step reads (kHaloDepth).
+// the group's physical operations, halo copies (staged where a source is
+// overwritten by the same phase), then its owner copies.  full: every ghost
+// layer (mhd_sync); otherwise the layers the step reads (kHaloDepth).
 void enqueue_sync(mhd_batch *b, int mode, int g, int *nk, bool full = false) {
-  sync1(b, mode, copy_op(g, full ? 2 : 0), nk);
-  sync1(b, mode, copy_op(g, 1), nk);
+  sync_pre(b, mode, g, nk);
+  sync1(b, mode, copy_op(g, full ? kPhHaloFull : kPhHalo), nk);
+  sync_post(b, mode, g, nk);
+  sync1(b, mode, copy_op(g, kPhOwner), nk);
 }
 
 // UpdateDerivedFields_ (Z4_Mercury/src/physics/MercurySolver_Tools.cpp:309-321) plus the
 // contravariant velocities and the next step's CFL dt.  Independent sync
 // stages share a launch: Sync(B_cell) runs beside the J alias reduction and
-// Sync(Jedge), in the same order per field as the reference.
+// Sync(Jedge), in the same order per field as the reference; the singular
+// edges' current replaces their owners' after the alias reduction
+// (Calc_J_Edge, Z4_Mercury/src/physics/MercurySolver_Current.cpp:140-201).
 void enqueue_derived(mhd_batch *b, int mode, int *nk) {
   launch(b, mode, SK_BCELL_JEDGE, nk);
-  sync2(b, mode, copy_op(MHD_SYNC_B_CELL, 0), alias_op(1), nk);
-  sync2(b, mode, copy_op(MHD_SYNC_B_CELL, 1), copy_op(MHD_SYNC_JEDGE, 0), nk);
-  sync1(b, mode, copy_op(MHD_SYNC_JEDGE, 1), nk);
+  sync_pre(b, mode, MHD_SYNC_B_CELL, nk);
+  sync2(b, mode, copy_op(MHD_SYNC_B_CELL, kPhHalo), alias_op(1), nk);
+  sync_post(b, mode, MHD_SYNC_B_CELL, nk);
+  if (b->live_sing > 0) launch(b, mode, SK_SING_J, nk);
+  sync_pre(b, mode, MHD_SYNC_JEDGE, nk);
+  sync2(b, mode, copy_op(MHD_SYNC_B_CELL, kPhOwner), copy_op(MHD_SYNC_JEDGE, kPhHalo), nk);
+  sync_post(b, mode, MHD_SYNC_JEDGE, nk);
+  sync1(b, mode, copy_op(MHD_SYNC_JEDGE, kPhOwner), nk);
   launch(b, mode, SK_JCELL, nk);
   enqueue_sync(b, mode, MHD_SYNC_J_CELL, nk);
   launch(b, mode, SK_PV_UPLUS, nk);
@@ -316,22 +366,36 @@ void enqueue_derived(mhd_batch *b, int mode, int *nk) {
 // (Driver.cpp:33-38) runs between A and B and B starts with Sync(B faces).
 void enqueue_step_a(mhd_batch *b, int *nk) {
   const int m = 0;
-  // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171);
-  // the E alias reduction (ideal EMF) and Sync(Ehall) touch different fields
+  // AssembleRHS_Induction_CT_ (Z4_Mercury/src/physics/MercurySolver_MagneticRHS.cpp:90-171)
   launch(b, m, SK_FACE_EMF, nk);
   launch(b, m, SK_EDGE_EMF, nk);
   launch(b, m, SK_HALL_EDGE, nk);
-  sync2(b, m, alias_op(0), copy_op(MHD_SYNC_EHALL, 0), nk);
-  sync1(b, m, copy_op(MHD_SYNC_EHALL, 1), nk);
+  if (b->live_sing > 0 || b->live_phys[MHD_SYNC_EHALL] > 0 || b->live_tables[MHD_SYNC_EHALL][kPhStash] > 0) {
+    // the E alias reduction, the singular edges' EMF and Hall EMF, Sync(Ehall)
+    sync1(b, m, alias_op(0), nk);
+    if (b->live_sing > 0) launch(b, m, SK_SING_EMF, nk);
+    enqueue_sync(b, m, MHD_SYNC_EHALL, nk);
+  } else {  // the E alias reduction and Sync(Ehall) touch different fields
+    sync2(b, m, alias_op(0), copy_op(MHD_SYNC_EHALL, kPhHalo), nk);
+    sync1(b, m, copy_op(MHD_SYNC_EHALL, kPhOwner), nk);
+  }
   launch(b, m, SK_ADD_HALL, nk);
+  phys1(b, m, kMaxGroups, nk);  // the wall EMF: E_t = 0 on solid-wall edges
   enqueue_sync(b, m, MHD_SYNC_EEDGE, nk);
   // AssembleRHS_Fluid_ + ApplyUpdate_Euler_ (state into the other buffer) and
   // the constrained-transport face update (Z4_Mercury/src/physics/MercurySolver_Advance.cpp:73-147)
   launch(b, m, SK_FLUID, nk);
   launch(b, m, SK_BFACE, nk);
   launch(b, m, SK_FLIP, nk);
-  sync2(b, m, copy_op(MHD_SYNC_UCELL, 0), copy_op(MHD_SYNC_BFACE, 0), nk);
-  sync2(b, m, copy_op(MHD_SYNC_UCELL, 1), copy_op(MHD_SYNC_BFACE, 1), nk);
+  // the reference's Sync(Ucell) reads ghosts it does not overwrite first at
+  // their values from the previous sync, which after the flip are in the
+  // other buffer
+  sync_pre(b, m, MHD_SYNC_UCELL, nk, 1);
+  sync_pre(b, m, MHD_SYNC_BFACE, nk);
+  sync2(b, m, copy_op(MHD_SYNC_UCELL, kPhHalo), copy_op(MHD_SYNC_BFACE, kPhHalo), nk);
+  sync_post(b, m, MHD_SYNC_UCELL, nk);
+  sync_post(b, m, MHD_SYNC_BFACE, nk);
+  sync2(b, m, copy_op(MHD_SYNC_UCELL, kPhOwner), copy_op(MHD_SYNC_BFACE, kPhOwner), nk);
 }
 void enqueue_step_b(mhd_batch *b, int *nk, bool resync_b) {
   const int m = 0;
@@ -370,10 +434,13 @@ int publish(mhd_batch *b) {
   for (int r = 0; r < kNumRanges; ++r)
     if ((rc = put(b->dprefix_tiles[r], [&](const Solve *S) { return S->T->tiles[r]; }))) return rc;
   for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 3; ++p)
+    for (int p = 0; p < kNumPhases; ++p)
       if ((rc = put(b->dprefix_copy[g][p], [&](const Solve *S) { return S->T->tab_n[g][p]; }))) return rc;
   if ((rc = put(b->dprefix_aliasE, [](const Solve *S) { return (S->T->al_n + 7) / 8; }))) return rc;
   if ((rc = put(b->dprefix_aliasJ, [](const Solve *S) { return (S->T->al_n + 7) / 8; }))) return rc;
+  for (int q = 0; q < kNumPhys; ++q)
+    if ((rc = put(b->dprefix_phys[q], [&](const Solve *S) { return S->T->ph_nset[q] + S->T->ph_nop[q]; }))) return rc;
+  if ((rc = put(b->dprefix_sing, [](const Solve *S) { return S->T->sg_n; }))) return rc;
   std::vector<DevSolve> ds((size_t)C);
   for (int s = 0; s < C; ++s) {
     DevSolve &d = ds[s];
@@ -387,11 +454,13 @@ int publish(mhd_batch *b) {
     d.ubuf = S->ubuf;
     d.nblocks = S->nblocks;
     for (int r = 0; r < kNumRanges; ++r) d.tile_prefix[r] = S->T->dtile_prefix[r];
-    for (int g = 0; g < kMaxGroups; ++g) {
-      d.halo[g] = DevTable{S->T->tab_seg[g][0], S->T->tab_n[g][0]};
-      d.owner[g] = DevTable{S->T->tab_seg[g][1], S->T->tab_n[g][1]};
-      d.halo_full[g] = DevTable{S->T->tab_seg[g][2], S->T->tab_n[g][2]};
-    }
+    for (int g = 0; g < kMaxGroups; ++g)
+      for (int p = 0; p < kNumPhases; ++p) d.tab[g][p] = DevTable{S->T->tab_seg[g][p], S->T->tab_n[g][p]};
+    for (int q = 0; q < kNumPhys; ++q)
+      d.phys[q] = DevPhys{S->T->ph_set[q], S->T->ph_op[q], S->T->ph_nset[q], S->T->ph_nop[q]};
+    const Tables &T = *S->T;
+    d.sing = DevSingular{T.sg_n, T.sg_owner, T.sg_osign, T.sg_aoff, T.sg_alias, T.sg_coff, T.sg_cell, T.sg_foff,
+                         T.sg_face, S->sg_geo, S->sg_w};
     d.aliasE = DevAlias{S->T->al_off, S->T->al_memE, S->T->al_msign, S->T->al_ownE, S->T->al_osign, S->T->al_n};
     d.aliasJ = DevAlias{S->T->al_off, S->T->al_memJ, S->T->al_msign, S->T->al_ownJ, S->T->al_osign, S->T->al_n};
   }
@@ -448,7 +517,7 @@ void encode_chunk(const Solve *S, const mhd_copy *tab, int t0, int t1, Encoded *
     e->dst[t] = dc;
     e->src[t] = sc;
     e->neg[t] = tab[t].sign < 0.0;
-    const int d = dof_depth(S, tab[t].dst);
+    const int d = tab[t].dst.field == MHD_STAGING ? 0 : dof_depth(S, tab[t].dst);
     e->depth[t] = (uint8_t)(d > 255 ? 255 : d);
     if (t > t0 && dc <= e->dst[t - 1]) *asc = 0;
   }
@@ -467,12 +536,12 @@ void encode_chunk(const Solve *S, const mhd_copy *tab, int t0, int t1, Encoded *
 // of one phase are distinct and no copy of a phase reads a value the phase
 // writes, so the order of application does not change the result.  Signs
 // must be +1 or -1 (orientation flips).
-std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth) {
+std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth, const std::vector<char> *keep = nullptr) {
   const int n0 = (int)e.dst.size();
   std::vector<int> order;
   order.reserve(n0);
   for (int t = 0; t < n0; ++t)
-    if (max_depth < 0 || e.depth[t] <= max_depth) order.push_back(t);
+    if (keep ? (*keep)[t] != 0 : (max_depth < 0 || e.depth[t] <= max_depth)) order.push_back(t);
   const int n = (int)order.size();
   if (!e.ascending)
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return e.dst[a] < e.dst[c]; });
@@ -549,14 +618,60 @@ std::vector<int64_t> build_segments(const Encoded &e, int es, int max_depth) {
 // The three phases of every group (pruned halo, owner, full halo) segmented
 // on the host threads from the encoded halo (2 g) and owner (2 g + 1)
 // tables, and uploaded.
-int upload_encoded(Solve *S, const std::vector<Encoded> &enc, cudaStream_t st) {
-  std::vector<std::vector<int64_t>> seg(3 * MHD_NUM_GROUPS);
-  mhd::parallel_for(3 * MHD_NUM_GROUPS, [&](int q) {
-    const int g = q / 3, phase = q % 3;
-    seg[q] = build_segments(enc[2 * g + (phase == 1)], S->es, phase == 0 ? kHaloDepth[g] : -1);
+// The halo copies the step keeps: those whose destination lies within the
+// group's step depth, and (transitively) every halo copy that writes a
+// source of a kept copy, of a staged copy or of an owner copy -- a ghost
+// beyond the step depth that such a copy reads must hold its value from the
+// previous sync, as in the reference.
+std::vector<char> step_halo_mask(const Encoded &h, const Encoded *owner, const Encoded *stash, int max_depth) {
+  const size_t n = h.dst.size();
+  std::vector<char> keep(n, 0);
+  std::unordered_map<int64_t, size_t> by_dst;
+  by_dst.reserve(n * 2);
+  for (size_t t = 0; t < n; ++t) by_dst[h.dst[t]] = t;  // the later entry wins a destination written twice
+  std::vector<int64_t> todo;
+  for (size_t t = 0; t < n; ++t)
+    if (h.depth[t] <= max_depth) {
+      keep[t] = 1;
+      todo.push_back(h.src[t]);
+    }
+  for (const Encoded *o : {owner, stash})
+    if (o) todo.insert(todo.end(), o->src.begin(), o->src.end());
+  while (!todo.empty()) {
+    const int64_t c = todo.back();
+    todo.pop_back();
+    auto it = by_dst.find(c);
+    if (it == by_dst.end() || keep[it->second]) continue;
+    keep[it->second] = 1;
+    todo.push_back(h.src[it->second]);
+  }
+  return keep;
+}
+
+// Every group's phases (CopyPhase) segmented on the host threads from its
+// encoded tables, enc[per_group * g + q]: q = 0 halo, 1 owner, 2 staging
+// (per_group 4: the stash copies, then the copies from the staging slots).
+int upload_encoded(Solve *S, const std::vector<Encoded> &enc, cudaStream_t st, int per_group = 2) {
+  std::vector<std::vector<int64_t>> seg(kNumPhases * MHD_NUM_GROUPS);
+  mhd::parallel_for(kNumPhases * MHD_NUM_GROUPS, [&](int q) {
+    const int g = q / kNumPhases, phase = q % kNumPhases;
+    const Encoded &h = enc[per_group * g], &o = enc[per_group * g + 1];
+    const Encoded *stash = per_group > 2 ? &enc[per_group * g + 2] : nullptr;
+    const Encoded *unstash = per_group > 2 ? &enc[per_group * g + 3] : nullptr;
+    switch (phase) {
+      case kPhHalo: {
+        const std::vector<char> keep = step_halo_mask(h, &o, stash, kHaloDepth[g]);
+        seg[q] = build_segments(h, S->es, -1, &keep);
+        break;
+      }
+      case kPhOwner: seg[q] = build_segments(o, S->es, -1); break;
+      case kPhHaloFull: seg[q] = build_segments(h, S->es, -1); break;
+      case kPhStash: if (stash) seg[q] = build_segments(*stash, S->es, -1); break;
+      default: if (unstash) seg[q] = build_segments(*unstash, S->es, -1); break;
+    }
   });
-  for (int q = 0; q < 3 * MHD_NUM_GROUPS; ++q) {
-    const int g = q / 3, phase = q % 3;
+  for (int q = 0; q < kNumPhases * MHD_NUM_GROUPS; ++q) {
+    const int g = q / kNumPhases, phase = q % kNumPhases;
     S->T->tab_n[g][phase] = (int)(seg[q].size() / kSegWords);
     S->T->table_bytes += (int64_t)seg[q].size() * 8;
     const int rc = dev_upload(S->pool, seg[q], &S->T->tab_seg[g][phase], st);
@@ -664,15 +779,18 @@ int upload_aliases_periodic(Solve *S, cudaStream_t st) {
 // threads, then segmented and uploaded.
 int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
   // every table's chunks on one pool of host threads
-  constexpr int NT = 2 * MHD_NUM_GROUPS;
+  // per group: halo, owner, staging in, staging out
+  constexpr int NT = 4 * MHD_NUM_GROUPS;
   std::vector<Encoded> enc(NT);
   const mhd_copy *tabs[NT];
   int ntab[NT], first_chunk[NT + 1];
   first_chunk[0] = 0;
   for (int q = 0; q < NT; ++q) {
-    const int g = q / 2, p = q % 2;
-    tabs[q] = p ? groups[g].owner : groups[g].halo;
-    ntab[q] = p ? groups[g].n_owner : groups[g].n_halo;
+    const int g = q / 4, p = q % 4;
+    const mhd_sync_group &G = groups[g];
+    if (G.n_stash < 0 || (G.n_stash > 0 && !G.stash)) return fail(MHD_ERR_ARG, "group %d: bad staging table", g);
+    tabs[q] = p == 0 ? G.halo : p == 1 ? G.owner : p == 2 ? G.stash : G.stash + G.n_stash;
+    ntab[q] = p == 0 ? G.n_halo : p == 1 ? G.n_owner : G.n_stash;
     if (ntab[q] < 0 || (ntab[q] > 0 && !tabs[q])) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, p);
     Encoded &e = enc[q];
     e.dst.resize(ntab[q]);
@@ -693,7 +811,7 @@ int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
     encode_chunk(S, tabs[q], t0, t1, &enc[q], &bad[c], &kind[c], &asc[c]);
   });
   for (int q = 0; q < NT; ++q) {
-    const int g = q / 2, p = q % 2;
+    const int g = q / 4, p = q % 4;
     Encoded &e = enc[q];
     e.ascending = true;
     for (int c = first_chunk[q]; c < first_chunk[q + 1]; ++c) {
@@ -706,7 +824,7 @@ int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
       if (!asc[c] || (t0 && e.dst[t0] <= e.dst[t0 - 1])) e.ascending = false;
     }
   }
-  return upload_encoded(S, enc, st);
+  return upload_encoded(S, enc, st, 4);
 }
 
 int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
@@ -753,13 +871,21 @@ void free_solve(Solve *S, cudaStream_t st) {
   };
   f(S->arena);
   f(S->dblocks);
+  f(S->sg_geo);
+  f(S->sg_w);
   Tables *T = S->T;
   if (T && --T->users == 0) {
     for (int r = 0; r < kNumRanges; ++r) f(T->dtile_prefix[r]);
     for (int g = 0; g < kMaxGroups; ++g)
-      for (int p = 0; p < 3; ++p) f(T->tab_seg[g][p]);
+      for (int p = 0; p < kNumPhases; ++p) f(T->tab_seg[g][p]);
+    for (int q = 0; q < kNumPhys; ++q) {
+      f(T->ph_set[q]);
+      f(T->ph_op[q]);
+    }
     for (void *p : {(void *)T->al_off, (void *)T->al_memE, (void *)T->al_ownE, (void *)T->al_memJ, (void *)T->al_ownJ,
-                    (void *)T->al_msign, (void *)T->al_osign})
+                    (void *)T->al_msign, (void *)T->al_osign, (void *)T->sg_owner, (void *)T->sg_osign,
+                    (void *)T->sg_aoff, (void *)T->sg_alias, (void *)T->sg_coff, (void *)T->sg_cell,
+                    (void *)T->sg_foff, (void *)T->sg_face})
       f(p);
     delete T;
   }
@@ -818,11 +944,20 @@ int build_graph(mhd_batch *b) {
 bool count_tables(mhd_batch *b, const Solve *S, int d) {
   bool grew = false;
   for (int g = 0; g < MHD_NUM_GROUPS; ++g)
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < kNumPhases; ++p)
       if (S->T->tab_n[g][p] > 0) {
         grew = grew || (d > 0 && b->live_tables[g][p] == 0);
         b->live_tables[g][p] += d;
       }
+  for (int q = 0; q < kNumPhys; ++q)
+    if (S->T->ph_nset[q] + S->T->ph_nop[q] > 0) {
+      grew = grew || (d > 0 && b->live_phys[q] == 0);
+      b->live_phys[q] += d;
+    }
+  if (S->T->sg_n > 0) {
+    grew = grew || (d > 0 && b->live_sing == 0);
+    b->live_sing += d;
+  }
   return grew;
 }
 
@@ -1117,8 +1252,11 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
   for (int r = 0; r < kNumRanges; ++r)
     if (cudaMalloc(&b->dprefix_tiles[r], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
   for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 3; ++p)
+    for (int p = 0; p < kNumPhases; ++p)
       if (cudaMalloc(&b->dprefix_copy[g][p], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
+  for (int q = 0; q < kNumPhys; ++q)
+    if (cudaMalloc(&b->dprefix_phys[q], sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
+  if (cudaMalloc(&b->dprefix_sing, sizeof(int) * C1) != cudaSuccess) return bail(fail(MHD_ERR_OOM, "prefix"));
   if (cudaMalloc(&b->dprefix_aliasE, sizeof(int) * C1) != cudaSuccess ||
       cudaMalloc(&b->dprefix_aliasJ, sizeof(int) * C1) != cudaSuccess)
     return bail(fail(MHD_ERR_OOM, "prefix"));
@@ -1163,7 +1301,9 @@ int mhd_batch_destroy(mhd_batch *b) {
   }
   for (int r = 0; r < kNumRanges; ++r) cudaFree(b->dprefix_tiles[r]);
   for (int g = 0; g < kMaxGroups; ++g)
-    for (int p = 0; p < 3; ++p) cudaFree(b->dprefix_copy[g][p]);
+    for (int p = 0; p < kNumPhases; ++p) cudaFree(b->dprefix_copy[g][p]);
+  for (int q = 0; q < kNumPhys; ++q) cudaFree(b->dprefix_phys[q]);
+  cudaFree(b->dprefix_sing);
   cudaFree(b->dprefix_aliasE);
   cudaFree(b->dprefix_aliasJ);
   for (auto e : b->prof_events) cudaEventDestroy(e);
@@ -1198,7 +1338,10 @@ int64_t mhd_desc_device_bytes(const mhd_desc *desc) {
     bytes += ((int64_t)kNumMetric * 8 + (nr + 2 * kNumUComps) * es) * bx.total;
   }
   for (int g = 0; g < MHD_NUM_GROUPS; ++g)
-    bytes += (int64_t)(desc->groups[g].n_halo + desc->groups[g].n_owner) * 24;
+    bytes += (int64_t)(desc->groups[g].n_halo + desc->groups[g].n_owner + 2 * desc->groups[g].n_stash) * 24 +
+             (int64_t)desc->groups[g].n_phys * sizeof(DevPhysOp);
+  bytes += (int64_t)desc->n_staging * (desc->precision == kMixed ? 4 : 8) + 256 +
+           (int64_t)desc->n_wall * 8 + (int64_t)desc->singular.n_edges * 128;
   if (desc->edge_aliases.n_classes > 0 && desc->edge_aliases.offset)
     bytes += (int64_t)desc->edge_aliases.offset[desc->edge_aliases.n_classes] * 24 +
              (int64_t)desc->edge_aliases.n_classes * 28;
@@ -1224,6 +1367,175 @@ static int ensure_shadow(mhd_batch *b) {
   sh->pool = b->pool;
   sh->borrowed = true;
   b->shadow = sh;
+  return MHD_OK;
+}
+
+// Per-solve constants from the descriptor's (calc_physical_constant values
+// and the boundary-operation values).
+static Consts make_consts(const mhd_constants &k, int nghost) {
+  Consts c = Consts{k.gamma,         k.M_H,       k.M_Na,        k.M_ref,
+                    k.T_ref,         k.L_ref,     k.U_ref,       k.B_ref,
+                    k.n_ref,         k.rho_ref,   k.m_Na,        k.k_Boltz,
+                    k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
+                    k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
+                    k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
+                    k.ambipolar,     k.local_arti, nghost, k.resistive, {}};
+  for (int q = 0; q < MHD_NUM_BC; ++q) c.bc[q] = k.bc[q];
+  return c;
+}
+
+// The physical boundary operations of every group and the wall EMF, encoded
+// as arena codes (MHD_PHYS_SET: one word; the others DevPhysOp).
+static int upload_phys(Solve *S, const mhd_desc *desc, cudaStream_t st) {
+  for (int q = 0; q < kNumPhys; ++q) {
+    const mhd_phys_op *ops = q < kMaxGroups ? desc->groups[q].phys : desc->wall;
+    const int n = q < kMaxGroups ? desc->groups[q].n_phys : desc->n_wall;
+    if (n < 0 || (n > 0 && !ops)) return fail(MHD_ERR_ARG, "physical operations %d: bad table", q);
+    std::vector<int64_t> set;
+    std::vector<DevPhysOp> other;
+    for (int t = 0; t < n; ++t) {
+      const mhd_phys_op &o = ops[t];
+      bool ok1 = false, ok2 = true;
+      const int64_t dc = S->code(o.dst, &ok1);
+      if (!ok1) return fail(MHD_ERR_ARG, "physical operation %d of table %d: destination out of range", t, q);
+      if (o.kind == MHD_PHYS_SET) {
+        if (o.arg < 0 || o.arg >= MHD_NUM_BC) return fail(MHD_ERR_ARG, "physical operation %d: value index %d", t, o.arg);
+        set.push_back(dc | ((int64_t)o.arg << kPhysArgShift));
+        continue;
+      }
+      DevPhysOp d{};
+      d.kind = o.kind;
+      d.dst = dc;
+      const Box &bx = S->boxes[o.dst.block];
+      d.cstride = bx.total * S->es;
+      if (o.kind == MHD_PHYS_WALL) {
+        if (o.dst.field != MHD_U_H || o.dst.comp != 0 || o.src.field != MHD_U_H || o.src.block != o.dst.block)
+          return fail(MHD_ERR_ARG, "wall operation %d: cells of U_H of one block", t);
+        d.src = S->code(o.src, &ok2);
+        const int ax = std::abs(o.arg) - 1, sg = o.arg > 0 ? 1 : -1;
+        if (ax < 0 || ax > 2 || S->nghost > kMaxWallGhosts) return fail(MHD_ERR_ARG, "wall operation %d: direction", t);
+        d.nghost = S->nghost;
+        for (int g = 1; g <= S->nghost; ++g) {
+          mhd_dof c = o.dst;
+          int *q3[3] = {&c.i, &c.j, &c.k};
+          *q3[ax] += g * sg;
+          for (int a = 0; a < 3; ++a)  // clamped to the allocated cell range
+            *q3[a] = std::min(std::max(*q3[a], -S->nghost), bx.n[a] + S->nghost - 1);
+          bool okg = false;
+          d.ghost[g - 1] = S->code(c, &okg);
+          ok2 = ok2 && okg;
+        }
+      } else if (o.kind == MHD_PHYS_EFAR) {
+        if (o.dst.field < MHD_E_XI || o.dst.field > MHD_E_ZETA) return fail(MHD_ERR_ARG, "farfield EMF %d: not an E edge", t);
+        mhd_dof dr = o.dst;
+        dr.field = MHD_DR_XI + (o.dst.field - MHD_E_XI);
+        dr.comp = 0;
+        d.src = S->code(dr, &ok2);
+      } else {
+        return fail(MHD_ERR_ARG, "physical operation %d: kind %d", t, o.kind);
+      }
+      if (!ok2) return fail(MHD_ERR_ARG, "physical operation %d of table %d: source out of range", t, q);
+      other.push_back(d);
+    }
+    S->T->ph_nset[q] = (int)set.size();
+    S->T->ph_nop[q] = (int)other.size();
+    S->T->table_bytes += (int64_t)set.size() * 8 + (int64_t)other.size() * sizeof(DevPhysOp);
+    int rc;
+    if ((rc = dev_upload(S->pool, set, &S->T->ph_set[q], st)) || (rc = dev_upload(S->pool, other, &S->T->ph_op[q], st)))
+      return rc;
+  }
+  return MHD_OK;
+}
+
+// Per-solve geometric data of the singular edges (written by k_sing_setup).
+static int alloc_singular_geo(Solve *S, cudaStream_t st) {
+  if (S->T->sg_n <= 0) return MHD_OK;
+  CUDA_TRY(cudaMallocFromPoolAsync((void **)&S->sg_geo, sizeof(double) * 4 * S->T->sg_n, S->pool, st));
+  CUDA_TRY(cudaMallocFromPoolAsync((void **)&S->sg_w, sizeof(double) * std::max(1, S->T->sg_ncell), S->pool, st));
+  CUDA_TRY(cudaMemsetAsync(S->sg_geo, 0, sizeof(double) * 4 * S->T->sg_n, st));
+  CUDA_TRY(cudaMemsetAsync(S->sg_w, 0, sizeof(double) * std::max(1, S->T->sg_ncell), st));
+  return MHD_OK;
+}
+
+// The singular-edge lists as device records (mhd_singular_edges).
+static int upload_singular(Solve *S, const mhd_singular_edges &g, cudaStream_t st) {
+  if (g.n_edges <= 0) return MHD_OK;
+  if (!g.owner || !g.owner_sign || !g.alias_offset || !g.aliases || !g.cell_offset || !g.cells || !g.face_offset ||
+      !g.faces)
+    return fail(MHD_ERR_ARG, "singular edges: null table");
+  const int n = g.n_edges;
+  std::vector<int64_t> owner(3 * n);
+  std::vector<double> osign(g.owner_sign, g.owner_sign + n);
+  auto inside = [&](int field, int block, int i, int j, int k) {
+    const mhd_dof d{field, block, i, j, k, 0};
+    bool ok = false;
+    S->code(d, &ok);
+    return ok;
+  };
+  for (int e = 0; e < n; ++e) {
+    const mhd_dof &o = g.owner[e];
+    if (o.field < 0 || o.field > 2) return fail(MHD_ERR_ARG, "singular edge %d: owner axis %d", e, o.field);
+    const int fl[3] = {MHD_E_XI + o.field, MHD_EHALL_XI + o.field, MHD_J_XI + o.field};
+    for (int q = 0; q < 3; ++q) {
+      mhd_dof d = o;
+      d.field = fl[q];
+      d.comp = 0;
+      bool ok = false;
+      owner[3 * e + q] = S->code(d, &ok);
+      if (!ok) return fail(MHD_ERR_ARG, "singular edge %d: owner out of range", e);
+    }
+  }
+  auto records = [&](const int32_t *off, auto get, int per, std::vector<int> &offs, std::vector<int> &rec,
+                     const char *what) -> int {
+    offs.assign(off, off + n + 1);
+    for (int q = off[0]; q < off[n]; ++q) {
+      int r[6];
+      get(q, r);
+      const int fld = per == 0 ? MHD_CELL : per;
+      (void)fld;
+      rec.insert(rec.end(), r, r + 6);
+    }
+    return MHD_OK;
+    (void)what;
+  };
+  std::vector<int> aoff, alias, coff, cell, foff, face;
+  records(g.alias_offset, [&](int q, int *r) {
+    const mhd_singular_alias &a = g.aliases[q];
+    r[0] = a.edge.block; r[1] = a.edge.field; r[2] = a.edge.i; r[3] = a.edge.j; r[4] = a.edge.k; r[5] = a.orient;
+  }, 1, aoff, alias, "alias");
+  records(g.cell_offset, [&](int q, int *r) {
+    const mhd_singular_cell &c = g.cells[q];
+    r[0] = c.cell.block; r[1] = c.axis; r[2] = c.cell.i; r[3] = c.cell.j; r[4] = c.cell.k; r[5] = c.orient;
+  }, 0, coff, cell, "cell");
+  records(g.face_offset, [&](int q, int *r) {
+    const mhd_singular_face &f = g.faces[q];
+    r[0] = f.face.block; r[1] = f.face.field; r[2] = f.face.i; r[3] = f.face.j; r[4] = f.face.k; r[5] = f.sign;
+  }, 2, foff, face, "face");
+  // every record inside its block's box (the kernels read +-1 cell around incident cells)
+  for (size_t q = 0; q < alias.size(); q += 6)
+    if (alias[q + 1] < 0 || alias[q + 1] > 2 || !inside(MHD_E_XI + alias[q + 1], alias[q], alias[q + 2], alias[q + 3], alias[q + 4]))
+      return fail(MHD_ERR_ARG, "singular edges: alias %zu out of range", q / 6);
+  for (size_t q = 0; q < cell.size(); q += 6) {
+    if (cell[q + 1] < 0 || cell[q + 1] > 2 || cell[q] < 0 || cell[q] >= S->nblocks)
+      return fail(MHD_ERR_ARG, "singular edges: cell %zu out of range", q / 6);
+    const Box &bx = S->boxes[cell[q]];
+    for (int a = 0; a < 3; ++a)
+      if (cell[q + 2 + a] < 1 - bx.G || cell[q + 2 + a] >= bx.n[a] + bx.G)
+        return fail(MHD_ERR_ARG, "singular edges: cell %zu out of range", q / 6);
+  }
+  for (size_t q = 0; q < face.size(); q += 6)
+    if (face[q + 1] < 0 || face[q + 1] > 2 || !inside(MHD_B_XI + face[q + 1], face[q], face[q + 2], face[q + 3], face[q + 4]))
+      return fail(MHD_ERR_ARG, "singular edges: face %zu out of range", q / 6);
+  Tables &T = *S->T;
+  T.sg_n = n;
+  T.sg_ncell = (int)(cell.size() / 6);
+  T.table_bytes += (int64_t)(owner.size() + osign.size()) * 8 + (int64_t)(alias.size() + cell.size() + face.size()) * 4;
+  int rc;
+  if ((rc = dev_upload(S->pool, owner, &T.sg_owner, st)) || (rc = dev_upload(S->pool, osign, &T.sg_osign, st)) ||
+      (rc = dev_upload(S->pool, aoff, &T.sg_aoff, st)) || (rc = dev_upload(S->pool, alias, &T.sg_alias, st)) ||
+      (rc = dev_upload(S->pool, coff, &T.sg_coff, st)) || (rc = dev_upload(S->pool, cell, &T.sg_cell, st)) ||
+      (rc = dev_upload(S->pool, foff, &T.sg_foff, st)) || (rc = dev_upload(S->pool, face, &T.sg_face, st)))
+    return rc;
   return MHD_OK;
 }
 
@@ -1284,15 +1596,15 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
   }
   S->ubuf = u;
   S->main_off = 2 * u;
-  S->arena_bytes = 2 * u + m;
+  if (desc->n_staging < 0) return bail(fail(MHD_ERR_ARG, "n_staging %d", desc->n_staging));
+  S->n_staging = periodic ? 0 : desc->n_staging;
+  S->staging_off = 2 * u + m;
+  S->arena_bytes = 2 * u + m + ((int64_t)S->n_staging * S->es + 255) / 256 * 256;
   const mhd_constants &k = desc->constants;
-  S->consts = Consts{k.gamma,         k.M_H,       k.M_Na,        k.M_ref,
-                     k.T_ref,         k.L_ref,     k.U_ref,       k.B_ref,
-                     k.n_ref,         k.rho_ref,   k.m_Na,        k.k_Boltz,
-                     k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
-                     k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
-                     k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
-                     k.ambipolar,     k.local_arti, desc->nghost, k.resistive};
+  S->consts = make_consts(k, desc->nghost);
+  if (!periodic && k.resistive && (desc->singular.n_edges > 0 || desc->n_wall > 0 || desc->n_staging > 0))
+    return bail(fail(MHD_ERR_ARG, "the implicit resistive substep is not supported on grids with physical boundaries "
+                                  "or singular edges"));
   if (cudaMallocFromPoolAsync((void **)&S->arena, S->arena_bytes, b->pool, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
@@ -1325,6 +1637,8 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
     } else {
       if ((rc = upload_groups(S, desc->groups, st))) return bail(rc);
       if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
+      if ((rc = upload_phys(S, desc, st))) return bail(rc);
+      if ((rc = upload_singular(S, desc->singular, st)) || (rc = alloc_singular_geo(S, st))) return bail(rc);
     }
   } catch (...) {  // host allocation or thread creation failed
     return bail(fail(MHD_ERR_OOM, "host memory for the copy tables"));
@@ -1400,23 +1714,17 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   S->ubuf = src->ubuf;
   S->main_off = src->main_off;
   S->arena_bytes = src->arena_bytes;
+  S->staging_off = src->staging_off;
+  S->n_staging = src->n_staging;
   S->T = src->T;
   S->T->users += 1;
   S->consts = src->consts;
-  if (constants) {
-    const mhd_constants &k = *constants;
-    S->consts = Consts{k.gamma,         k.M_H,       k.M_Na,        k.M_ref,
-                       k.T_ref,         k.L_ref,     k.U_ref,       k.B_ref,
-                       k.n_ref,         k.rho_ref,   k.m_Na,        k.k_Boltz,
-                       k.q_e,           k.mu0,       k.state_coeff_H, k.state_coeff_Na,
-                       k.CFL,           k.hall_coef, k.momentum_induce_coeff, k.momentum_hall_coeff,
-                       k.inver_MA2,     k.ne_hall_floor, k.arti_eta_max, k.arti_J_start, k.arti_J_on,
-                       k.ambipolar,     k.local_arti, S->nghost, k.resistive};
-  }
+  if (constants) S->consts = make_consts(*constants, S->nghost);
   auto bail = [&](int code) {
     free_solve(S, st);
     return code;
   };
+  if ((rc = alloc_singular_geo(S, st))) return bail(rc);
   if (cudaMallocFromPoolAsync((void **)&S->arena, S->arena_bytes, b->pool, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
@@ -1558,7 +1866,9 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   // reset everything before the buffer index (dt, time, step, remaining, status); keep cur
   if ((rc = set_state_field(b, slot, 0, &s0, offsetof(SolveState, cur)))) return rc;
   const bool res = b->slots[slot]->consts.resistive != 0;
+  const bool sing = b->slots[slot]->T->sg_n > 0;
   rc = targeted(b, slot, [&](int *nk) {
+    if (sing) launch(b, 1, SK_SING_SETUP, nk);  // before anything reads the edge Hodge field it updates
     launch(b, 1, SK_FACE_NORMALS, nk);
     if (res) {  // unknowns of the implicit resistive substep: W = 1 / (eta alpha) on them
       launch(b, 1, SK_RES_SEED, nk);

@@ -85,16 +85,19 @@ struct ConstsT {
   int local_arti;
   int nghost;
   int resistive;
+  T bc[MHD_NUM_BC];  // values of the physical boundary operations (mhd_bc_const)
 };
 using Consts = ConstsT<double>;
 inline ConstsT<float> to_float(const Consts &c) {
-  return ConstsT<float>{(float)c.gamma, (float)c.M_H, (float)c.M_Na, (float)c.M_ref, (float)c.T_ref,
-                        (float)c.L_ref, (float)c.U_ref, (float)c.B_ref, (float)c.n_ref, (float)c.rho_ref,
-                        (float)c.m_Na, (float)c.k_Boltz, (float)c.q_e, (float)c.mu0, (float)c.state_coeff_H,
-                        (float)c.state_coeff_Na, (float)c.CFL, (float)c.hall_coef, (float)c.momentum_induce_coeff,
-                        (float)c.momentum_hall_coeff, (float)c.inver_MA2, (float)c.ne_hall_floor,
-                        (float)c.arti_eta_max, (float)c.arti_J_start, (float)c.arti_J_on, c.ambipolar,
-                        c.local_arti, c.nghost, c.resistive};
+  ConstsT<float> f{(float)c.gamma, (float)c.M_H, (float)c.M_Na, (float)c.M_ref, (float)c.T_ref,
+                   (float)c.L_ref, (float)c.U_ref, (float)c.B_ref, (float)c.n_ref, (float)c.rho_ref,
+                   (float)c.m_Na, (float)c.k_Boltz, (float)c.q_e, (float)c.mu0, (float)c.state_coeff_H,
+                   (float)c.state_coeff_Na, (float)c.CFL, (float)c.hall_coef, (float)c.momentum_induce_coeff,
+                   (float)c.momentum_hall_coeff, (float)c.inver_MA2, (float)c.ne_hall_floor,
+                   (float)c.arti_eta_max, (float)c.arti_J_start, (float)c.arti_J_on, c.ambipolar,
+                   c.local_arti, c.nghost, c.resistive, {}};
+  for (int q = 0; q < MHD_NUM_BC; ++q) f.bc[q] = (float)c.bc[q];
+  return f;
 }
 
 // Per-solve device state.
@@ -145,6 +148,44 @@ struct DevAlias {
 };
 
 constexpr int kMaxGroups = MHD_NUM_GROUPS;
+// Copy phases of a group: 0 halo copies to the step's depth, 1 owner copies,
+// 2 every halo copy, 3 staging <- sources the halo phase overwrites, 4
+// destinations <- staging.
+constexpr int kNumPhases = 5;
+enum CopyPhase : int { kPhHalo = 0, kPhOwner = 1, kPhHaloFull = 2, kPhStash = 3, kPhUnstash = 4 };
+
+// Physical boundary operations (mhd_phys_op) of one solve: per group, and
+// the step's wall EMF as table kMaxGroups.  MHD_PHYS_SET operations are one
+// word each: the destination code with the value index in bits 55..59; the
+// others are DevPhysOp.
+constexpr int kNumPhys = kMaxGroups + 1;
+constexpr int kPhysArgShift = 55;
+constexpr int kMaxWallGhosts = 8;
+struct DevPhysOp {
+  int64_t dst, src;                // codes of component 0 (WALL: cells; EFAR: the edge and its dr vector)
+  int64_t cstride;                 // bytes between the components of dst / src
+  int64_t ghost[kMaxWallGhosts];   // WALL: codes of the ghost cells it fills (component 0)
+  int kind, nghost;
+};
+struct DevPhys {
+  const int64_t *set = nullptr;
+  const DevPhysOp *op = nullptr;
+  int nset = 0, nop = 0;
+};
+// Singular (valence-3) edges of one solve: owner edges (codes in E, E_Hall,
+// J), aliases, incident cells and faces as (block, axis, i, j, k, sign)
+// records, and the geometric data the prepare pass computes (per edge the
+// canonical edge vector and the inverse Hodge star, per cell its weight).
+struct DevSingular {
+  int n = 0;
+  const int64_t *owner = nullptr;   // 3 per edge
+  const double *osign = nullptr;
+  const int *aoff = nullptr, *alias = nullptr;  // 6 ints per alias: block axis i j k orient
+  const int *coff = nullptr, *cell = nullptr;   // 6 ints per cell: block axis i j k orient
+  const int *foff = nullptr, *face = nullptr;   // 6 ints per face: block axis i j k sign
+  double *geo = nullptr;                        // 4 per edge: canonical vector, inverse Hodge star
+  double *w = nullptr;                          // per incident cell
+};
 
 // Directory entry of one solve (device).
 struct DevSolve {
@@ -155,8 +196,10 @@ struct DevSolve {
   int64_t ubuf;                       // bytes per U buffer
   int nblocks;
   const int *tile_prefix[kNumRanges]; // per range: nblocks + 1 prefix sums of tile counts
-  DevTable halo[kMaxGroups], owner[kMaxGroups], halo_full[kMaxGroups];
+  DevTable tab[kMaxGroups][kNumPhases];
   DevAlias aliasE, aliasJ;
+  DevPhys phys[kNumPhys];
+  DevSingular sing;
 };
 
 // The directory handed to every kernel (by value).
@@ -169,8 +212,12 @@ struct Dir {
   // sync tables: per group and phase (0 halo to the step's depth, 1 owner,
   // 2 every halo copy) prefix sums over the solves of their segment counts;
   // alias tables: of their 8-class groups
-  const int *copy_prefix[kMaxGroups][3];
+  const int *copy_prefix[kMaxGroups][kNumPhases];
   const int *aliasE_prefix, *aliasJ_prefix;
+  // physical operations (SET words, then the others) and singular edges:
+  // prefix sums over the solves
+  const int *phys_prefix[kNumPhys];
+  const int *sing_prefix;
 };
 
 template <class R>

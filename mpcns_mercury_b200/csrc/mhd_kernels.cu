@@ -59,6 +59,7 @@ static_assert(cBFY == cBFX + 1 && cBFZ == cBFX + 2 && cALY == cALX + 1 && cALZ =
 constexpr int cBAX = kComp.first[MHD_BADD_XI], cBAY = kComp.first[MHD_BADD_ETA], cBAZ = kComp.first[MHD_BADD_ZETA];
 constexpr int cPHOTO = kComp.first[MHD_PHOTO], cCX = kComp.first[MHD_CELL_X];  // CELL_Y, CELL_Z follow
 constexpr int cTPX = kComp.first[MHD_TAPER_XI], cTPY = kComp.first[MHD_TAPER_ETA], cTPZ = kComp.first[MHD_TAPER_ZETA];
+constexpr int cTPC = kComp.first[MHD_TAPER_CELL];
 constexpr int cLEX = kComp.first[MHD_LOCAL_ETA_XI];  // LOCAL_ETA_ETA, LOCAL_ETA_ZETA follow
 
 // std::max / std::min semantics (first argument wins ties, incl. signed zeros).
@@ -1438,12 +1439,15 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
     bool bad = false;
     if (it.in) {
       R vel[2][3];
+      R chk = R(0.0);  // sum of the conserved components: non-finite if any of them is
       for (int s = 0; s < 2; ++s) {
         const int u0 = s ? cUN : cUH, pv0 = s ? cPVN : cPVH;
         const R coeff = s ? c.state_coeff_Na : c.state_coeff_H;
-        const R rho = dmax(LD(u0, i, j, k), R(1e-12));
-        const R u = LD(u0 + 1, i, j, k) / rho, v = LD(u0 + 2, i, j, k) / rho, w = LD(u0 + 3, i, j, k) / rho;
+        const R r0 = LD(u0, i, j, k), m1 = LD(u0 + 1, i, j, k), m2 = LD(u0 + 2, i, j, k), m3 = LD(u0 + 3, i, j, k);
+        const R rho = dmax(r0, R(1e-12));
+        const R u = m1 / rho, v = m2 / rho, w = m3 / rho;
         const R E = LD(u0 + 4, i, j, k);
+        chk += ((r0 + m1) + (m2 + m3)) + E;
         const R ke = R(0.5) * rho * (u * u + v * v + w * w);
         R eint = E - ke;
         if (eint < R(0.0)) eint = R(0.0);
@@ -1495,7 +1499,9 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_PV) k_pv_uplus(Dir 
       }
       if (i >= 0 && i < B.n0 && j >= 0 && j < B.n1 && k >= 0 && k < B.n2) {
         dtl = cell_dt(B, c, i, j, k);
-        bad = !isfinite(dtl);  // a NaN drops out of the minimum below: record it instead
+        // a NaN drops out of the minimum below (and the pressure floors can
+        // hide a non-finite energy from it): record it instead
+        bad = !isfinite(dtl) || !isfinite(chk);
       }
     }
     // warp minimum, one atomicMin per warp (min is exact in any order)
@@ -1555,14 +1561,14 @@ __global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
     const int q = e - pre[s];
     const int cur = D.state[s].cur;
     if (op.kind == SYNC_COPY) {
-      const DevTable &T = op.phase == 1 ? S.owner[op.arg] : op.phase == 2 ? S.halo_full[op.arg] : S.halo[op.arg];
+      const DevTable &T = S.tab[op.arg][op.phase];
       const int64_t *w = T.seg + kSegWords * (int64_t)q;
       const int64_t dcode = w[0], scode = w[1], rw = w[2];
       const int len = (int)((dcode >> kSegLenShift) & 31) + 1;
       const int n = len * ((int)(rw & 0xffff) + 1);
       const int64_t stride = rw >> kSegStrideShift;  // bytes between runs
       const bool neg = (dcode >> kSegNegBit) & 1;
-      const char *src = (const char *)at_code<R>(S, cur, scode);
+      const char *src = (const char *)at_code<R>(S, cur ^ op.prev, scode);
       char *dst = (char *)at_code<R>(S, cur, dcode);
       // element e of the segment: run e / len, offset e % len (e < 64, so
       // e * ceil(2^16 / len) >> 16 is the exact quotient)
@@ -1590,6 +1596,276 @@ __global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
     }
   }
 }
+
+#define AT(cc, i, j, k) (B.c(cc)[B.off((i), (j), (k))])
+#define ATM(cc, i, j, k) (B.m(cc)[B.off((i), (j), (k))])
+
+// A block's view outside the tile loop (the singular-edge passes).
+template <class R>
+__device__ __forceinline__ V<R> block_view(const Dir &D, int s, int b) {
+  const DevBlock &DB = D.solves[s].blocks[b];
+  V<R> B;
+  const int cur = D.state[s].cur;
+  B.U = (R *)DB.U[cur];
+  B.Un = (R *)DB.U[cur ^ 1];
+  B.M = DB.M;
+  B.total = (int)DB.total;
+  B.si = (int)DB.si;
+  B.sj = (int)DB.sj;
+  B.G = DB.G;
+  B.n0 = DB.n[0];
+  B.n1 = DB.n[1];
+  B.n2 = DB.n[2];
+  return B;
+}
+
+// Physical boundary operations of table `which` (a sync group, or the wall
+// EMF) for every active solve (mhd_phys_op; BoundaryCore::ApplyPhysical with
+// MercuryBoundary's handlers, Z4_Mercury/src/boundary/Boundary_Build.cpp:5-300).
+// The operations of one table write distinct DOFs and read none another
+// writes, so they run in any order.
+template <class R>
+__global__ void __launch_bounds__(256) k_phys(Dir D, int which) {
+  const int *pre = D.phys_prefix[which];
+  const int total = pre[D.nsolves];
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int s = find_solve(pre, D.nsolves, e);
+    if (!solve_active(D, s)) continue;
+    const DevSolve &S = D.solves[s];
+    const DevPhys &P = S.phys[which];
+    const ConstsT<R> &c = consts_of<R>(S);
+    const int cur = D.state[s].cur;
+    const int q = e - pre[s];
+    if (q < P.nset) {  // dst <- bc[arg]
+      const int64_t w = P.set[q];
+      const int arg = (int)((w >> kPhysArgShift) & 31);
+      *at_code<R>(S, cur, w & ~(int64_t(31) << kPhysArgShift)) = c.bc[arg];
+      continue;
+    }
+    const DevPhysOp &op = P.op[q - P.nset];
+    if (op.kind == MHD_PHYS_WALL) {
+      // BC_Solid_Surface_ (Z4_Mercury/src/boundary/Boundary_Condition_Fluid.cpp:37-259), H+:
+      // the boundary cell from the cell one deeper (density floor 2.5e-3,
+      // no-slip, pressure from the conserved state with its floors), then
+      // the ghost cells from the boundary cell's new state
+      const R floor = R(2.5e-3), g1 = c.gamma - R(1.0);
+      auto wall = [&](const R *U, R *out) {
+        const R rho_r = dmax(U[0], floor);
+        const R rho = dmax(rho_r, floor);
+        const R ke = R(0.5) * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / rho;
+        R eint = U[4] - ke;
+        if (eint < R(0.0)) eint = R(0.0);
+        const R p = dmax(g1 * eint, R(1.0e-12));
+        out[0] = rho_r;
+        out[1] = out[2] = out[3] = rho_r * R(0.0);
+        out[4] = p / g1 + R(0.5) * rho_r * R(0.0);
+      };
+      R u[5], w1[5], w2[5];
+      for (int m = 0; m < 5; ++m) u[m] = *at_code<R>(S, cur, op.src + m * op.cstride);
+      wall(u, w1);
+      wall(w1, w2);
+      for (int m = 0; m < 5; ++m) *at_code<R>(S, cur, op.dst + m * op.cstride) = w1[m];
+      for (int g = 0; g < op.nghost; ++g)
+        for (int m = 0; m < 5; ++m) *at_code<R>(S, cur, op.ghost[g] + m * op.cstride) = w2[m];
+    } else {
+      // BC_Farfield_Eedge_set_zerocurl (Z4_Mercury/src/boundary/Boundary_Condition.cpp:573-624):
+      // E = E_inf . dr with E_inf = -u_inf x B_imf
+      const R *u = c.bc + MHD_BC_UINF, *Bi = c.bc + MHD_BC_BIMF;
+      const R E0 = Bi[1] * u[2] - Bi[2] * u[1], E1 = Bi[2] * u[0] - Bi[0] * u[2], E2 = Bi[0] * u[1] - Bi[1] * u[0];
+      const R d0 = *at_code<R>(S, cur, op.src), d1 = *at_code<R>(S, cur, op.src + op.cstride),
+              d2 = *at_code<R>(S, cur, op.src + 2 * op.cstride);
+      *at_code<R>(S, cur, op.dst) = E0 * d0 + E1 * d1 + E2 * d2;
+    }
+  }
+}
+
+// One thread per singular edge of every active solve.
+template <class F>
+__device__ __forceinline__ void for_singular(const Dir &D, F &&f) {
+  const int total = D.sing_prefix[D.nsolves];
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int s = find_solve(D.sing_prefix, D.nsolves, e);
+    if (!solve_active(D, s)) continue;
+    f(s, D.solves[s].sing, e - D.sing_prefix[s]);
+  }
+}
+
+// The geometric data of the singular edges (SingularEdgeRegistry::build,
+// src/7_metric/SingularEdgeRegistry.cpp:78-300) from the uploaded geometry,
+// in the reference's operation order: the mean primal length and the
+// canonical edge vector over the aliases, the |Jac| weights of the incident
+// cells, the dual polygon through their centres (sorted by angle about the
+// edge) and its area, the inverse Hodge star, which also replaces the edge
+// Hodge field of every alias.  Computed in FP64 from the double metric and
+// the real-typed edge fields.
+template <class R>
+__global__ void k_sing_setup(Dir D) {
+  for_singular(D, [&](int s, const DevSingular &G, int e) {
+    double len = 0.0, dr[3] = {0.0, 0.0, 0.0};
+    int nlen = 0;
+    for (int a = G.aoff[e]; a < G.aoff[e + 1]; ++a) {
+      const int *r = G.alias + 6 * a;
+      const V<R> B = block_view<R>(D, s, r[0]);
+      const int ax = r[1];
+      const double L = (double)AT(cDLX + ax, r[2], r[3], r[4]);
+      if (isfinite(L) && L > 0.0) {
+        len += L;
+        ++nlen;
+      }
+      for (int q = 0; q < 3; ++q) dr[q] += r[5] * (double)AT((ax == 0 ? cDRX : ax == 1 ? cDRY : cDRZ) + q, r[2], r[3], r[4]);
+    }
+    double gv = 0.0;
+    constexpr int kMaxCells = 16;
+    double pts[kMaxCells][3];
+    int np = 0;
+    for (int q = G.coff[e]; q < G.coff[e + 1]; ++q) {
+      const int *r = G.cell + 6 * q;
+      const V<R> B = block_view<R>(D, s, r[0]);
+      const double v = fabs(ATM(cJAC, r[2], r[3], r[4]));
+      if (isfinite(v) && v > 1.e-30) {
+        gv += v;
+        if (np < kMaxCells) {
+          for (int c = 0; c < 3; ++c) pts[np][c] = (double)AT(cCX + c, r[2], r[3], r[4]);
+          ++np;
+        }
+      }
+    }
+    for (int q = G.coff[e]; q < G.coff[e + 1]; ++q) {
+      const int *r = G.cell + 6 * q;
+      const V<R> B = block_view<R>(D, s, r[0]);
+      const double v = fabs(ATM(cJAC, r[2], r[3], r[4]));
+      G.w[q] = (isfinite(v) && v > 1.e-30 && gv > 0.0) ? v / gv : 0.0;
+    }
+    const double primal = nlen ? len / nlen : 0.0;
+    double dual = 0.0;
+    if (np >= 3) {
+      double cen[3] = {0.0, 0.0, 0.0};
+      for (int n = 0; n < np; ++n)
+        for (int c = 0; c < 3; ++c) cen[c] += pts[n][c];
+      for (int c = 0; c < 3; ++c) cen[c] /= np;
+      double t[3] = {dr[0], dr[1], dr[2]};
+      const double tn = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+      if (tn > 0.0)
+        for (double &x : t) x /= tn;
+      const double ref[3] = {fabs(t[0]) < 0.9 ? 1.0 : 0.0, fabs(t[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+      double u[3] = {t[1] * ref[2] - t[2] * ref[1], t[2] * ref[0] - t[0] * ref[2], t[0] * ref[1] - t[1] * ref[0]};
+      const double un = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      if (un > 0.0)
+        for (double &x : u) x /= un;
+      const double v[3] = {t[1] * u[2] - t[2] * u[1], t[2] * u[0] - t[0] * u[2], t[0] * u[1] - t[1] * u[0]};
+      double ang[kMaxCells];
+      for (int n = 0; n < np; ++n) {
+        double du = 0.0, dv = 0.0;
+        for (int c = 0; c < 3; ++c) {
+          du += (pts[n][c] - cen[c]) * u[c];
+          dv += (pts[n][c] - cen[c]) * v[c];
+        }
+        ang[n] = atan2(dv, du);
+      }
+      int ord[kMaxCells];
+      for (int n = 0; n < np; ++n) ord[n] = n;
+      for (int n = 1; n < np; ++n)  // insertion sort by angle (the points are few and their angles distinct)
+        for (int m = n; m > 0 && ang[ord[m]] < ang[ord[m - 1]]; --m) {
+          const int tmp = ord[m];
+          ord[m] = ord[m - 1];
+          ord[m - 1] = tmp;
+        }
+      double av[3] = {0.0, 0.0, 0.0};
+      for (int n = 0; n < np; ++n) {
+        const double *a = pts[ord[n]], *b = pts[ord[(n + 1) % np]];
+        av[0] += a[1] * b[2] - a[2] * b[1];
+        av[1] += a[2] * b[0] - a[0] * b[2];
+        av[2] += a[0] * b[1] - a[1] * b[0];
+      }
+      dual = 0.5 * sqrt(av[0] * av[0] + av[1] * av[1] + av[2] * av[2]);
+    }
+    if (!(dual > 0.0)) dual = primal > 0.0 ? gv / primal : 0.0;
+    const double ih = dual > 0.0 ? primal / dual : 0.0;
+    double *geo = G.geo + 4 * e;
+    for (int q = 0; q < 3; ++q) geo[q] = nlen > 0 ? dr[q] / nlen : 0.0;
+    geo[3] = ih;
+    for (int a = G.aoff[e]; a < G.aoff[e + 1]; ++a) {  // the registry publishes it to every alias
+      const int *r = G.alias + 6 * a;
+      const V<R> B = block_view<R>(D, s, r[0]);
+      AT(cALX + r[1], r[2], r[3], r[4]) = (R)ih;
+    }
+  });
+}
+
+// The EMF and the Hall EMF of the singular edges' owners:
+// AssembleSingularEdgeEMF_NonHall_ (Z4_Mercury/src/physics/MercurySolver_MagExplicit_Ideal.cpp:57-130) and
+// AssembleSingularEdgeEMF_HallExplicit_ (MercurySolver_MagExplicit_Hall.cpp:32-56): the |Jac|-weighted
+// sum over the incident cells of the cell field projected on the canonical
+// edge vector, times the owner's orientation.  (The local artificial
+// resistivity term of the non-Hall EMF is not included.)
+template <class R>
+__global__ void k_sing_emf(Dir D) {
+  for_singular(D, [&](int s, const DevSingular &G, int e) {
+    const ConstsT<R> &c = consts_of<R>(D.solves[s]);
+    const double *geo = G.geo + 4 * e;
+    const R cv[3] = {(R)geo[0], (R)geo[1], (R)geo[2]};
+    R sumE = R(0.0), sumH = R(0.0);
+    for (int q = G.coff[e]; q < G.coff[e + 1]; ++q) {
+      const int *r = G.cell + 6 * q;
+      const V<R> B = block_view<R>(D, s, r[0]);
+      const int i = r[2], j = r[3], k = r[4];
+      const R u0 = AT(cUP, i, j, k), u1 = AT(cUP + 1, i, j, k), u2 = AT(cUP + 2, i, j, k);
+      const R b0 = AT(cBC, i, j, k), b1 = AT(cBC + 1, i, j, k), b2 = AT(cBC + 2, i, j, k);
+      const R ex = -(u1 * b2 - u2 * b1), ey = -(u2 * b0 - u0 * b2), ez = -(u0 * b1 - u1 * b0);
+      R emf = ex * cv[0] + ey * cv[1] + ez * cv[2];
+      const Num<R> num = num_limiter<R>(c, AT(cUH, i, j, k), AT(cUN, i, j, k));
+      if (c.ambipolar) {
+        const int ax = r[1];
+        const int im = i - (ax == 0), jm = j - (ax == 1), km = k - (ax == 2);
+        const int ip = i + (ax == 0), jp = j + (ax == 1), kp = k + (ax == 2);
+        const R dp = R(0.5) * ((AT(cPVH + 3, ip, jp, kp) + AT(cPVN + 3, ip, jp, kp)) -
+                               (AT(cPVH + 3, im, jm, km) + AT(cPVN + 3, im, jm, km)));
+        const R pressure_coef = (c.rho_ref * c.U_ref) / (c.q_e * c.L_ref * c.B_ref * c.n_ref);
+        emf -= pressure_coef * R(r[5]) * dp / num.ne_eff;
+      }
+      const R j0 = AT(cJC, i, j, k), j1 = AT(cJC + 1, i, j, k), j2 = AT(cJC + 2, i, j, k);
+      if (c.arti_eta_max > R(0.0)) {
+        const R jedge = j0 * cv[0] + j1 * cv[1] + j2 * cv[2];
+        const R jmag = sqrt(j0 * j0 + j1 * j1 + j2 * j2);
+        R qq = (jmag - c.arti_J_start) / dmax(c.arti_J_on - c.arti_J_start, R(1.e-30));
+        qq = dmax(R(0.0), dmin(R(1.0), qq));
+        emf += c.arti_eta_max * qq * qq * (R(3.0) - R(2.0) * qq) * jedge;
+      }
+      const R w = (R)G.w[q];
+      sumE += w * emf;
+      // Hall: alpha (J x B) at the cell, times the radial taper at its centre
+      const R alpha = c.hall_coef / num.ne_eff;
+      const R hx = alpha * (j1 * b2 - j2 * b1), hy = alpha * (j2 * b0 - j0 * b2), hz = alpha * (j0 * b1 - j1 * b0);
+      sumH += w * (AT(cTPC, i, j, k) * (hx * cv[0] + hy * cv[1] + hz * cv[2]));
+    }
+    const R os = (R)G.osign[e];
+    *at_code<R>(D.solves[s], D.state[s].cur, G.owner[3 * e]) = os * sumE;
+    *at_code<R>(D.solves[s], D.state[s].cur, G.owner[3 * e + 1]) = os * sumH;
+  });
+}
+
+// The current of the singular edges' owners (AssembleSingularEdgeCurrent_,
+// Z4_Mercury/src/physics/MercurySolver_Current.cpp:59-138): the inverse Hodge star times the sum
+// over the incident owner faces of the signed beta B, times the owner's
+// orientation.
+template <class R>
+__global__ void k_sing_j(Dir D) {
+  for_singular(D, [&](int s, const DevSingular &G, int e) {
+    const R ih = (R)G.geo[4 * e + 3];
+    R sum = R(0.0);
+    for (int q = G.foff[e]; q < G.foff[e + 1]; ++q) {
+      const int *r = G.face + 6 * q;
+      if (r[5] == 0) continue;
+      const V<R> B = block_view<R>(D, s, r[0]);
+      const int ax = r[1];
+      sum += ih * R(r[5]) * AT(cBFX + ax, r[2], r[3], r[4]) * AT((ax == 0 ? cBX : ax == 1 ? cBY : cBZ), r[2], r[3], r[4]);
+    }
+    *at_code<R>(D.solves[s], D.state[s].cur, G.owner[3 * e + 2]) = R(G.osign[e]) * sum;
+  });
+}
+
+#undef AT
+#undef ATM
 
 // After the updates: flip the state buffer, account time/step
 // (Z4_Mercury/src/MercurySolver_Driver.cpp:40-45), record a dt failure (the
@@ -1660,6 +1936,7 @@ static const void *kernel_fn(StepKernel k) {
     case SK_RES_BUPDATE: return (const void *)k_res_bupdate<R>;
     case SK_RES_CG: return (const void *)k_res_cg<R>;
     case SK_RES_PUPD_E: return (const void *)k_res_pupd_e<R>;
+    case SK_PHYS: return (const void *)k_phys<R>;
     default: return nullptr;
   }
 }
@@ -1720,6 +1997,10 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_RES_PUPD_E: k_res_pupd_e<R><<<G, kTileThreads, 0, st>>>(D, rs.cg); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
+    case SK_PHYS: k_phys<R><<<G, 256, 0, st>>>(D, iarg); break;
+    case SK_SING_SETUP: k_sing_setup<R><<<8, 64, 0, st>>>(D); break;
+    case SK_SING_EMF: k_sing_emf<R><<<8, 64, 0, st>>>(D); break;
+    case SK_SING_J: k_sing_j<R><<<8, 64, 0, st>>>(D); break;
     default: break;
   }
 }
@@ -1812,7 +2093,8 @@ const char *step_kernel_name(StepKernel k) {
                                 "k_sync",     "k_flip",     "k_retire",      "k_face_normals", "k_div_b",
                                 "k_res_seed", "k_res_w",    "k_res_vec",     "k_res_db",   "k_res_dj",
                                 "k_res_q",    "k_res_dot",  "k_res_sum",     "k_res_copyb", "k_res_bupdate",
-                                "k_res_cg",   "k_res_pupd_e"};
+                                "k_res_cg",   "k_res_pupd_e", "k_phys",      "k_sing_setup", "k_sing_emf",
+                                "k_sing_j"};
   static_assert(sizeof(names) / sizeof(names[0]) == SK_COUNT, "a name per kernel");
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }

@@ -11,7 +11,9 @@ enum StepKernel {
   SK_JCELL, SK_PV_UPLUS, SK_SYNC, SK_FLIP, SK_RETIRE, SK_FACE_NORMALS, SK_DIVB,
   // implicit resistive substep
   SK_RES_SEED, SK_RES_W, SK_RES_VEC, SK_RES_DB, SK_RES_DJ, SK_RES_Q, SK_RES_DOT, SK_RES_SUM, SK_RES_COPYB,
-  SK_RES_BUPDATE, SK_RES_CG, SK_RES_PUPD_E, SK_COUNT
+  SK_RES_BUPDATE, SK_RES_CG, SK_RES_PUPD_E,
+  // grids with physical boundaries and singular edges
+  SK_PHYS, SK_SING_SETUP, SK_SING_EMF, SK_SING_J, SK_COUNT
 };
 
 // One launch of k_sync runs up to two independent sync operations: a copy
@@ -20,7 +22,9 @@ enum SyncKind { SYNC_COPY = 0, SYNC_ALIAS = 1 };
 struct SyncOp {
   int kind;   // SyncKind
   int arg;    // SYNC_COPY: group; SYNC_ALIAS: 0 = E, 1 = J
-  int phase;  // SYNC_COPY: 0 halo copies to the step's depth, 1 owner copies, 2 every halo copy
+  int phase;  // SYNC_COPY: a CopyPhase (mhd_engine.cuh)
+  int prev;   // SYNC_COPY: read U components from the other buffer (1) -- the staged
+              // ghosts of Sync(U) inside the step, whose last synced values are there
 };
 struct SyncOps {
   SyncOp op[2];

@@ -47,7 +47,8 @@ constexpr FieldSpec kFieldSpec[MHD_NUM_FIELDS] = {
     {1, MHD_FACE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA}, {18, MHD_CELL},
     {36, MHD_CELL},     {1, MHD_FACE_XI},   {1, MHD_FACE_ETA},  {1, MHD_FACE_ZETA}, {1, MHD_CELL},
     {1, MHD_CELL},      {1, MHD_CELL},      {1, MHD_CELL},      {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},
-    {1, MHD_EDGE_ZETA}, {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA} /* LOCAL_ETA */,
+    {1, MHD_EDGE_ZETA}, {1, MHD_CELL} /* TAPER_CELL */,
+    {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA} /* LOCAL_ETA */,
     {1, MHD_EDGE_XI},   {1, MHD_EDGE_ETA},  {1, MHD_EDGE_ZETA} /* ETA_RES */,
     {3, MHD_EDGE_XI},   {3, MHD_EDGE_XI},   {3, MHD_EDGE_XI},   {3, MHD_EDGE_XI},   {3, MHD_EDGE_XI},
     {3, MHD_FACE_XI} /* RES_W, RES_X, RES_R, RES_P, RES_Q, RES_BSTAR */};

@@ -194,3 +194,18 @@ SHELL_JOB = {
     "initial_line": SHELL_UPSTREAM,
     "farfield_line": "1612400.0 1954409.5501563628 4E7 0.0 0.0",
 }
+
+
+def shell_run(na=8, nr=16, steps=5, dump_at=None, extra=None, workdir=None):
+    """Run the cubed-sphere shell case (SHELL_JOB with na x na x nr cells per
+    panel) on the reference build; returns the dump with the static inputs,
+    the Hall taper (edges and cell centres), the grid and the state, derived
+    and work fields at the requested steps (0 = after the preamble)."""
+    job = dict(SHELL_JOB)
+    job.update(na=na, nr=nr, steps=steps, dump_grid=1, dump_taper=1,
+               dump_static=" ".join(STATIC_FIELDS),
+               dump_fields=" ".join(STATE_FIELDS + DERIVED_FIELDS + WORK_FIELDS),
+               dump_at=" ".join(str(s) for s in (dump_at or [0, steps])))
+    if extra:
+        job.update(extra)
+    return run_job(job, workdir=workdir)

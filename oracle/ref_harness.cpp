@@ -770,6 +770,23 @@ void dump_taper(MercurySolver &S, Dumper &d) {
       const int l[3] = {lo.i, lo.j, lo.k}, h[3] = {hi.i, hi.j, hi.k};
       d.rec(std::string("static:") + names[a], ib, l, h, 1, t.data());
     }
+  // and at the owned cell centres (HallRadialTaper_ of the singular-edge Hall
+  // EMF, Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:51), zero elsewhere
+  for (int ib = 0; ib < fld->num_blocks(); ++ib) {
+    FieldBlock &U = fld->field(S.fid_.fid_U_H, ib);
+    Block &blk = S.grd_->grids(ib);
+    const Int3 lo = U.get_lo(), hi = U.get_hi(), ilo = U.inner_lo(), ihi = U.inner_hi();
+    const int ni = hi.i - lo.i, nj = hi.j - lo.j, nk = hi.k - lo.k;
+    std::vector<double> t((size_t)ni * nj * nk, 0.0);
+    for (int i = ilo.i; i < ihi.i; ++i)
+      for (int j = ilo.j; j < ihi.j; ++j)
+        for (int k = ilo.k; k < ihi.k; ++k)
+          t[((size_t)(i - lo.i) * nj + (j - lo.j)) * nk + (k - lo.k)] =
+              S.HallRadialTaper_(blk.dual_x(i + 1, j + 1, k + 1), blk.dual_y(i + 1, j + 1, k + 1),
+                                 blk.dual_z(i + 1, j + 1, k + 1));
+    const int l[3] = {lo.i, lo.j, lo.k}, h[3] = {hi.i, hi.j, hi.k};
+    d.rec("static:taper_cell", ib, l, h, 1, t.data());
+  }
 }
 
 // Local artificial resistivity per edge as the reference fills it on its first

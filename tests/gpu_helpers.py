@@ -26,6 +26,9 @@ def upload_from_dump(upload, dump, tag="step0:"):
         for name in mo.STATIC_FIELDS + ["taper_xi", "taper_eta", "taper_zeta"]:
             r = dump[("static:" + name, b)]
             up(REF_FIELD[name], r.data, r.lo, r.hi)
+        if ("static:taper_cell", b) in dump:
+            r = dump[("static:taper_cell", b)]
+            up("TAPER_CELL", r.data, r.lo, r.hi)
         for name in ("local_arti_eta_xi", "local_arti_eta_eta", "local_arti_eta_zeta", "eta_res_xi", "eta_res_eta",
                      "eta_res_zeta"):
             if ("static:" + name, b) in dump:
@@ -89,3 +92,26 @@ def div_b(ctx, n):
     d = (B[0][p, o, o] - B[0][o, o, o]) + (B[1][o, p, o] - B[1][o, o, o]) + (B[2][o, o, p] - B[2][o, o, o])
     scale = max(float(np.abs(b[o, o, o]).max()) for b in B)
     return float(np.abs(d).max()) / scale
+
+
+def shell_constants(precision=0):
+    """The shell case's constants: the reference's REF list with the shell
+    job's upstream (INITIAL list), as the oracle harness writes them."""
+    from mpcns_mercury_b200 import reference_constants
+
+    initial = tuple(float(v) for v in mo.SHELL_UPSTREAM.split())
+    return reference_constants(cfl=mo.SHELL_JOB["cfl"], initial=initial)
+
+
+def shell_context(dump, na, nr, precision=0, constants=None):
+    """A context of the 6-panel shell (tables from mhd_topology_cubed_sphere)
+    with the reference's step-0 state and static inputs uploaded."""
+    import ctypes
+
+    from mpcns_mercury_b200 import capi
+
+    t = ctypes.c_void_p()
+    capi.check(capi.lib().mhd_topology_cubed_sphere(na, nr, NGHOST, 0, ctypes.byref(t)), "mhd_topology_cubed_sphere")
+    ctx = Context([(na, na, nr)] * 6, NGHOST, constants or shell_constants(), topology=t, precision=precision)
+    upload_from_dump(ctx.upload, dump)
+    return ctx
