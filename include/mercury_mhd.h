@@ -86,9 +86,16 @@ enum mhd_field {
 enum mhd_location { MHD_CELL = 0, MHD_FACE_XI, MHD_FACE_ETA, MHD_FACE_ZETA, MHD_EDGE_XI, MHD_EDGE_ETA, MHD_EDGE_ZETA,
                     MHD_NODE };
 
-/* Sync groups: MercuryBoundary::Sync names (Z4_Mercury/src/boundary/Boundary_Build.cpp:564-703). */
+/* Sync groups: MercuryBoundary::Sync names (Z4_Mercury/src/boundary/Boundary_Build.cpp:564-703).
+ * MHD_SYNC_ERES and MHD_SYNC_DB are the implicit resistive substep's Sync("Eres")
+ * and Sync("dB") (Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:321,440): the
+ * engine keeps E_res in the E edge arrays and dB in the B face arrays, so their
+ * tables address those fields; they differ from MHD_SYNC_EEDGE and MHD_SYNC_BFACE
+ * only in the physical handlers (Farfield: copy, Coupled-Solid: nothing).  dJ
+ * (in the J edge arrays) shares MHD_SYNC_JEDGE's handlers and tables.  Only
+ * solves with the implicit resistive substep read them. */
 enum mhd_group { MHD_SYNC_UCELL = 0, MHD_SYNC_BFACE, MHD_SYNC_EHALL, MHD_SYNC_EEDGE, MHD_SYNC_B_CELL,
-                 MHD_SYNC_JEDGE, MHD_SYNC_J_CELL, MHD_NUM_GROUPS };
+                 MHD_SYNC_JEDGE, MHD_SYNC_J_CELL, MHD_SYNC_ERES, MHD_SYNC_DB, MHD_NUM_GROUPS };
 
 /* Indices into mhd_constants.bc (BuildMercuryBackgroundState,
  * Z4_Mercury/include/0_BackgroundState.h:18-85, and the wall floors of

@@ -60,7 +60,7 @@ REF_FIELD = {
     "local_arti_eta_xi": "LOCAL_ETA_XI", "local_arti_eta_eta": "LOCAL_ETA_ETA", "local_arti_eta_zeta": "LOCAL_ETA_ZETA",
 }
 
-GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL"]
+GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL", "ERES", "DB"]
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_DT", 5: "ERR_NONFINITE", 6: "ERR_SOLVE",
           7: "ERR_STATE"}
 
@@ -130,7 +130,7 @@ class MhdSingularEdges(ctypes.Structure):
 class MhdDesc(ctypes.Structure):
     _fields_ = [("n_blocks", ctypes.c_int32), ("cells", ctypes.POINTER(ctypes.c_int32)),
                 ("nghost", ctypes.c_int32), ("precision", ctypes.c_int32), ("constants", MhdConstants),
-                ("groups", MhdSyncGroup * 7), ("edge_aliases", MhdAliasClasses),
+                ("groups", MhdSyncGroup * len(GROUPS)), ("edge_aliases", MhdAliasClasses),
                 ("n_staging", ctypes.c_int32), ("n_wall", ctypes.c_int32), ("wall", ctypes.POINTER(MhdPhysOp)),
                 ("singular", MhdSingularEdges)]
 

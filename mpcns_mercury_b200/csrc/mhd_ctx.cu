@@ -283,8 +283,8 @@ void launch(mhd_batch *b, int mode, StepKernel k, int *nk, const SyncOps *ops = 
   mark(b, step_kernel_name(k));
 }
 
-SyncOp copy_op(int g, int phase, int prev = 0) { return SyncOp{SYNC_COPY, g, phase, prev}; }
-SyncOp alias_op(int which) { return SyncOp{SYNC_ALIAS, which, 0, 0}; }
+SyncOp copy_op(int g, int phase, int prev = 0, int mark = 0) { return SyncOp{SYNC_COPY, g, phase, prev, mark}; }
+SyncOp alias_op(int which) { return SyncOp{SYNC_ALIAS, which, 0, 0, 0}; }
 
 // A sync operation some solve of the batch has work for (a copy phase whose
 // table is empty in every solve is left out: the depth-0 halos of E, E_Hall
@@ -472,9 +472,10 @@ int publish(mhd_batch *b) {
 // ghost layer any kernel of the step reads it at (U and the face fluxes: the
 // face EMF candidates and contravariant velocities two layers out; B_cell and
 // J_cell: the Hall cell field one layer out; E, E_Hall and J edges are read
-// only at owned and alias positions).  Explicit syncs (mhd_sync) fill every
+// only at owned and alias positions; in the implicit resistive substep E_res
+// only there and dB one layer out).  Explicit syncs (mhd_sync) fill every
 // layer.
-constexpr int kHaloDepth[MHD_NUM_GROUPS] = {2, 2, 0, 0, 1, 0, 1};
+constexpr int kHaloDepth[MHD_NUM_GROUPS] = {2, 2, 0, 0, 1, 0, 1, 0, 1};
 
 // Ghost depth of a DOF: how far outside its owned range [0, n + stagger) it lies.
 int dof_depth(const Solve *S, const mhd_dof &d) {
@@ -752,6 +753,13 @@ int upload_groups_periodic(Solve *S, cudaStream_t st) {
         break;
       }
   }
+  // Sync(Eres) and Sync(dB) of a periodic block: the E edge and B face
+  // copies (no physical boundary tells them apart)
+  if (S->consts.resistive)
+    for (int p = 0; p < 2; ++p) {
+      enc[2 * MHD_SYNC_ERES + p] = enc[2 * MHD_SYNC_EEDGE + p];
+      enc[2 * MHD_SYNC_DB + p] = enc[2 * MHD_SYNC_BFACE + p];
+    }
   return upload_encoded(S, enc, st);
 }
 
@@ -792,6 +800,7 @@ int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
     tabs[q] = p == 0 ? G.halo : p == 1 ? G.owner : p == 2 ? G.stash : G.stash + G.n_stash;
     ntab[q] = p == 0 ? G.n_halo : p == 1 ? G.n_owner : G.n_stash;
     if (ntab[q] < 0 || (ntab[q] > 0 && !tabs[q])) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, p);
+    if (g >= MHD_SYNC_ERES && !S->consts.resistive) ntab[q] = 0;  // read only by the implicit substep
     Encoded &e = enc[q];
     e.dst.resize(ntab[q]);
     e.src.resize(ntab[q]);
@@ -985,13 +994,37 @@ int res_dot(mhd_batch *b, int op) {
 // q = A p (MatMultImplicitResistive_, Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:420-472):
 // E_res from p, its owner copies, dB = -dt curl E_res, Sync(dB), dJ, its
 // alias reduction and owner copies, q = E_res - eta dJ.
+// On grids with physical boundaries or rotated seams the full Sync(Eres),
+// Sync(dB) and Sync(dJ) run, in the reference's order, with the singular
+// edges' current between the dJ alias reduction and its owner copies; the
+// unknowns read only owned values (no copy of these groups writes an owned
+// position from a ghost one), so of Sync(Eres) and Sync(dJ) only the owner
+// copies change q, and dB is read one ghost layer out.
+bool open_grids(const mhd_batch *b) {
+  if (b->live_sing > 0) return true;
+  for (int q = 0; q < kNumPhys; ++q)
+    if (b->live_phys[q] > 0) return true;
+  for (int g = 0; g < kMaxGroups; ++g)
+    if (b->live_tables[g][kPhStash] > 0) return true;
+  return false;
+}
+// Sync(group) after its owner copies already ran: the owner copies again
+// only when the halo phase may have changed a source of them.
+void sync_after_owner(mhd_batch *b, int mode, int g, int *nk) {
+  if (b->live_phys[g] == 0 && b->live_tables[g][kPhHalo] == 0 && b->live_tables[g][kPhStash] == 0) return;
+  enqueue_sync(b, mode, g, nk);
+}
 void res_apply_core(mhd_batch *b, int *nk) {  // from E_res (set) to dJ (synced)
-  sync1(b, 1, copy_op(MHD_SYNC_EEDGE, 1), nk);
+  sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner), nk);  // HALO_OWNER::sync_edge_1form
+  sync_after_owner(b, 1, MHD_SYNC_ERES, nk);           // Sync("Eres")
   launch(b, 1, SK_RES_DB, nk);
-  enqueue_sync(b, 1, MHD_SYNC_BFACE, nk);
+  if (open_grids(b)) launch(b, 1, SK_RES_CLEARB, nk);
+  enqueue_sync(b, 1, MHD_SYNC_DB, nk);
   launch(b, 1, SK_RES_DJ, nk);
   sync1(b, 1, alias_op(1), nk);
-  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, 1), nk);
+  if (b->live_sing > 0) launch(b, 1, SK_SING_J, nk);  // AssembleSingularEdgeCurrent_(dB, dJ)
+  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), nk);
+  sync_after_owner(b, 1, MHD_SYNC_JEDGE, nk);         // Sync("dJ")
 }
 void res_apply(mhd_batch *b, int *nk) {
   launch(b, 1, SK_RES_VEC, nk, nullptr, RES_E_FROM_P);
@@ -1151,7 +1184,9 @@ int res_solve(mhd_batch *b, int slot) {
   launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_SNAPSHOT);
   launch(b, 1, SK_BCELL_JEDGE, &nk);  // Calc_J_Edge on B* (B_cell is refreshed again after the substep)
   sync1(b, 1, alias_op(1), &nk);
-  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, 1), &nk);
+  if (b->live_sing > 0) launch(b, 1, SK_SING_J, &nk);
+  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), &nk);
+  sync_after_owner(b, 1, MHD_SYNC_JEDGE, &nk);
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_INIT);
   bool converged = false;
   if (S->shadow_slot >= 0) {
@@ -1169,7 +1204,8 @@ int res_solve(mhd_batch *b, int slot) {
   }
   // E_res = x, its owner copies; B = B* + dt (-curl E_res) on the owned faces
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_E_FROM_X);
-  sync1(b, 1, copy_op(MHD_SYNC_EEDGE, 1), &nk);
+  sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner), &nk);
+  sync_after_owner(b, 1, MHD_SYNC_ERES, &nk);
   launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_RESTORE);
   launch(b, 1, SK_RES_BUPDATE, &nk);
   CUDA_TRY(cudaGetLastError());
@@ -1389,8 +1425,9 @@ static Consts make_consts(const mhd_constants &k, int nghost) {
 static int upload_phys(Solve *S, const mhd_desc *desc, cudaStream_t st) {
   for (int q = 0; q < kNumPhys; ++q) {
     const mhd_phys_op *ops = q < kMaxGroups ? desc->groups[q].phys : desc->wall;
-    const int n = q < kMaxGroups ? desc->groups[q].n_phys : desc->n_wall;
+    int n = q < kMaxGroups ? desc->groups[q].n_phys : desc->n_wall;
     if (n < 0 || (n > 0 && !ops)) return fail(MHD_ERR_ARG, "physical operations %d: bad table", q);
+    if (q >= MHD_SYNC_ERES && q < kMaxGroups && !S->consts.resistive) n = 0;  // the implicit substep's groups
     std::vector<int64_t> set;
     std::vector<DevPhysOp> other;
     for (int t = 0; t < n; ++t) {
@@ -1602,9 +1639,10 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
   S->arena_bytes = 2 * u + m + ((int64_t)S->n_staging * S->es + 255) / 256 * 256;
   const mhd_constants &k = desc->constants;
   S->consts = make_consts(k, desc->nghost);
-  if (!periodic && k.resistive && (desc->singular.n_edges > 0 || desc->n_wall > 0 || desc->n_staging > 0))
-    return bail(fail(MHD_ERR_ARG, "the implicit resistive substep is not supported on grids with physical boundaries "
-                                  "or singular edges"));
+  if (!periodic && k.resistive && desc->precision == kMixed &&
+      (desc->singular.n_edges > 0 || desc->n_wall > 0 || desc->n_staging > 0))
+    return bail(fail(MHD_ERR_ARG, "the mixed-precision implicit resistive substep is not supported on grids with "
+                                  "physical boundaries or singular edges (FP64 is)"));
   if (cudaMallocFromPoolAsync((void **)&S->arena, S->arena_bytes, b->pool, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
@@ -1872,7 +1910,7 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
     launch(b, 1, SK_FACE_NORMALS, nk);
     if (res) {  // unknowns of the implicit resistive substep: W = 1 / (eta alpha) on them
       launch(b, 1, SK_RES_SEED, nk);
-      sync1(b, 1, copy_op(MHD_SYNC_EEDGE, 1), nk);
+      sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner, 0, 1), nk);  // zero the non-owner aliases
       launch(b, 1, SK_RES_W, nk);
     }
     enqueue_derived(b, 1, nk);

@@ -957,15 +957,15 @@ __device__ __forceinline__ bool edge_owned(int a, int i, int j, int k, int n0, i
   return a == 0 ? (i < n0 && j <= n1 && k <= n2) : a == 1 ? (i <= n0 && j < n1 && k <= n2) : (i <= n0 && j <= n1 && k < n2);
 }
 
-// E = the element offset of each edge (owned range and alias layer): after
-// the owner copies, an edge still holding its own offset is not a
-// non-owner alias (its own unknown).
+// E = 1 on every edge of the owned range; the owner phase of Sync(E_res)
+// run in mark mode then zeros its destinations, the non-owner aliases, so
+// an edge still at 1 is its own unknown.
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_seed(Dir D) {
   for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int o = B.off(it.i, it.j, it.k);
-    for (int a = 0; a < 3; ++a) B.c(cEX + a)[o] = R((double)o);
+    for (int a = 0; a < 3; ++a) B.c(cEX + a)[o] = R(1.0);
   });
 }
 
@@ -978,7 +978,7 @@ __global__ void __launch_bounds__(kTileThreads) k_res_w(Dir D) {
     const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       R w = R(0.0);
-      if (edge_owned(a, it.i, it.j, it.k, B.n0, B.n1, B.n2) && B.c(cEX + a)[o] == R((double)o)) {
+      if (edge_owned(a, it.i, it.j, it.k, B.n0, B.n1, B.n2) && B.c(cEX + a)[o] != R(0.0)) {
         const R eta = B.c(cETAR + a)[o], alpha = B.c(cALX + a)[o];
         if (eta > R(0.0) && alpha > R(0.0)) w = R(1.0) / (eta * alpha);
       }
@@ -1067,6 +1067,23 @@ __global__ void __launch_bounds__(kTileThreads) k_res_dj(Dir D) {
                    (AT(cBFY, i, j, k) * AT(cBY, i, j, k) - AT(cBFY, i - 1, j, k) * AT(cBY, i - 1, j, k))) * R(1.0);
       AT(cJZ, i, j, k) = v * AT(cALZ, i, j, k);
     }
+  });
+}
+
+// dB = 0 on every face of the block outside the owned range: the reference
+// clears dB before the curl (clear_triplet, Mercury_ImplicitResistive.cpp:428),
+// so Sync(dB) starts from zero ghosts; a Coupled-Solid boundary leaves them
+// at zero and the halo copies of a rotated seam can read them.
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_clearb(Dir D) {
+  for_items<R, kFull>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    if (!it.in) return;
+    const int i = it.i, j = it.j, k = it.k;
+    const bool ci = i >= 0 && i < B.n0, cj = j >= 0 && j < B.n1, ck = k >= 0 && k < B.n2;
+    const int o = B.off(i, j, k);
+    if (!(i >= 0 && i <= B.n0 && cj && ck)) B.c(cBX)[o] = R(0.0);
+    if (!(ci && j >= 0 && j <= B.n1 && ck)) B.c(cBY)[o] = R(0.0);
+    if (!(ci && cj && k >= 0 && k <= B.n2)) B.c(cBZ)[o] = R(0.0);
   });
 }
 
@@ -1584,7 +1601,7 @@ __global__ void __launch_bounds__(256) k_sync(Dir D, SyncOps ops) {
       }
 #pragma unroll
       for (int u = 0; u < kSegElems / 8; ++u)
-        if (lane + 8 * u < n) *(R *)(dst + off[u]) = neg ? -v[u] : v[u];
+        if (lane + 8 * u < n) *(R *)(dst + off[u]) = op.mark ? R(0.0) : (neg ? -v[u] : v[u]);
     } else {
       const DevAlias &A = op.arg ? S.aliasJ : S.aliasE;
       const int c = q * 8 + lane;
@@ -1937,6 +1954,7 @@ static const void *kernel_fn(StepKernel k) {
     case SK_RES_CG: return (const void *)k_res_cg<R>;
     case SK_RES_PUPD_E: return (const void *)k_res_pupd_e<R>;
     case SK_PHYS: return (const void *)k_phys<R>;
+    case SK_RES_CLEARB: return (const void *)k_res_clearb<R>;
     default: return nullptr;
   }
 }
@@ -2001,6 +2019,7 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_SING_SETUP: k_sing_setup<R><<<8, 64, 0, st>>>(D); break;
     case SK_SING_EMF: k_sing_emf<R><<<8, 64, 0, st>>>(D); break;
     case SK_SING_J: k_sing_j<R><<<8, 64, 0, st>>>(D); break;
+    case SK_RES_CLEARB: k_res_clearb<R><<<G, kTileThreads, 0, st>>>(D); break;
     default: break;
   }
 }
@@ -2094,7 +2113,7 @@ const char *step_kernel_name(StepKernel k) {
                                 "k_res_seed", "k_res_w",    "k_res_vec",     "k_res_db",   "k_res_dj",
                                 "k_res_q",    "k_res_dot",  "k_res_sum",     "k_res_copyb", "k_res_bupdate",
                                 "k_res_cg",   "k_res_pupd_e", "k_phys",      "k_sing_setup", "k_sing_emf",
-                                "k_sing_j"};
+                                "k_sing_j",   "k_res_clearb"};
   static_assert(sizeof(names) / sizeof(names[0]) == SK_COUNT, "a name per kernel");
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }

@@ -13,7 +13,9 @@ enum StepKernel {
   SK_RES_SEED, SK_RES_W, SK_RES_VEC, SK_RES_DB, SK_RES_DJ, SK_RES_Q, SK_RES_DOT, SK_RES_SUM, SK_RES_COPYB,
   SK_RES_BUPDATE, SK_RES_CG, SK_RES_PUPD_E,
   // grids with physical boundaries and singular edges
-  SK_PHYS, SK_SING_SETUP, SK_SING_EMF, SK_SING_J, SK_COUNT
+  SK_PHYS, SK_SING_SETUP, SK_SING_EMF, SK_SING_J,
+  // implicit resistive substep on grids with physical boundaries: zero the ghost faces of dB
+  SK_RES_CLEARB, SK_COUNT
 };
 
 // One launch of k_sync runs up to two independent sync operations: a copy
@@ -25,6 +27,8 @@ struct SyncOp {
   int phase;  // SYNC_COPY: a CopyPhase (mhd_engine.cuh)
   int prev;   // SYNC_COPY: read U components from the other buffer (1) -- the staged
               // ghosts of Sync(U) inside the step, whose last synced values are there
+  int mark;   // SYNC_COPY: write 0 to every destination instead of the copy (marks
+              // the phase's destinations, e.g. the non-owner aliases of an owner phase)
 };
 struct SyncOps {
   SyncOp op[2];

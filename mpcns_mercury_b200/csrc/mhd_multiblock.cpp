@@ -361,13 +361,20 @@ const GroupDef kGroupDefs[MHD_NUM_GROUPS] = {
     {MHD_SYNC_B_CELL, kComponent, 3, {MHD_B_CELL, MHD_BIND_CELL}, false},
     {MHD_SYNC_JEDGE, kEdge1, 3, {MHD_J_XI, MHD_J_ETA, MHD_J_ZETA}, true},
     {MHD_SYNC_J_CELL, kComponent, 3, {MHD_J_CELL}, false},
+    // the implicit substep's E_res and dB, kept in the E edge and B face arrays
+    {MHD_SYNC_ERES, kEdge1, 3, {MHD_E_XI, MHD_E_ETA, MHD_E_ZETA}, true},
+    {MHD_SYNC_DB, kFace2, 3, {MHD_B_XI, MHD_B_ETA, MHD_B_ZETA}, true},
 };
 
 // The physical handlers MercuryBoundary::InstallHandlers registers for the
 // fields of these groups (Z4_Mercury/src/boundary/Boundary_Build.cpp:5-300).
 enum Handler { hNop, hCopy, hFarU_H, hFarU_Na, hWallU_H, hWallU_Na, hFarE, hFarBcell, hFarBind, hWallJcell };
-Handler handler(int field, int bc, bool resistive) {
+Handler handler(int group, int field, int bc, bool resistive) {
   const bool far = bc == MHD_BC_FARFIELD;
+  // Eres_*, dB_*, dJ_*: the defaults (Farfield and Pole copy, Coupled-Solid
+  // nothing); BC_Farfield_Eedge_set_zerocurl, registered for Eres_* on
+  // Farfield, falls back to the copy for every field not named E_*
+  if (group == MHD_SYNC_ERES || group == MHD_SYNC_DB) return far ? hCopy : hNop;
   switch (field) {
     case MHD_U_H: return far ? hFarU_H : hWallU_H;
     case MHD_U_NA: return far ? hFarU_Na : hWallU_Na;
@@ -522,7 +529,7 @@ struct Replay {
         const int f = gd.fields[fs], b = pp.b, loc = mhd::kFieldSpec[f].loc;
         const IBox in = inner_slab(b, loc, pp.box, pp.dir);
         const int ax = axis_of(pp.dir), sgn = pp.dir > 0 ? 1 : -1;
-        switch (handler(f, pp.bc, resistive)) {
+        switch (handler(gd.group, f, pp.bc, resistive)) {
           case hNop: break;
           case hCopy: default_copy((int)fs, b, in, pp.dir); break;
           case hFarU_H:
@@ -576,7 +583,7 @@ struct Replay {
             each(ghost_slab(in, pp.dir), [&](const int p[3]) {
               for (int m = 0; m < 3; ++m)
                 set_phys(arr((int)fs, b, m), p, MHD_PHYS_SET,
-                         handler(f, pp.bc, resistive) == hFarBcell ? MHD_BC_BIMF + m : MHD_BC_ZERO);
+                         handler(gd.group, f, pp.bc, resistive) == hFarBcell ? MHD_BC_BIMF + m : MHD_BC_ZERO);
             });
             break;
           case hWallJcell:  // BC_Solid_Surface_Jcell: zero the boundary layer and the next inward, copy out
@@ -1079,6 +1086,7 @@ int build(Grid &G, bool resistive, mhd_topology **out) {
     const Classes ecls = edge_classes(G, N), fcls = face_classes(G, N);
     int staging = 0;
     for (int q = 0; q < MHD_NUM_GROUPS; ++q) {
+      if (q >= MHD_SYNC_ERES && !resistive) continue;  // read only by the implicit substep
       GroupTables T = replay_group(G, kGroupDefs[q], fcls, ecls, resistive, &staging);
       t->halo[q].assign(T.halo);
       t->owner[q].assign(T.owner);

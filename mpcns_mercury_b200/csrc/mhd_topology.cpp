@@ -101,6 +101,7 @@ extern "C" int mhd_topology_periodic_block(const int32_t cells[3], int32_t nghos
   auto *t = new (std::nothrow) mhd_topology();
   if (!t) return MHD_ERR_OOM;
   const int n[3] = {cells[0], cells[1], cells[2]};
+  t->res_groups_alias = true;
   try {
     build_groups(t, n, nghost);
     build_alias(t, n);
@@ -125,6 +126,7 @@ extern "C" int mhd_topology_periodic_lattice(const int32_t cells[3], const int32
   if (!t) return MHD_ERR_OOM;
   const int n[3] = {cells[0], cells[1], cells[2]};
   const Lattice L{{blocks[0], blocks[1], blocks[2]}};
+  t->res_groups_alias = true;
   try {
     build_lattice_groups(t, n, L, nghost);
     alias_classes_lattice(n, L, t->alias_offset, t->alias_member, t->alias_msign, t->alias_owner, t->alias_osign);
@@ -147,6 +149,10 @@ extern "C" int mhd_topology_fill_desc(const mhd_topology *t, mhd_desc *d) {
     d->groups[g].phys = t->phys[g].data();
     d->groups[g].n_stash = (int32_t)(t->stash[g].size() / 2);
     d->groups[g].stash = t->stash[g].data();
+  }
+  if (t->res_groups_alias) {
+    d->groups[MHD_SYNC_ERES] = d->groups[MHD_SYNC_EEDGE];
+    d->groups[MHD_SYNC_DB] = d->groups[MHD_SYNC_BFACE];
   }
   d->n_staging = t->n_staging;
   d->n_wall = (int32_t)t->wall.size();

@@ -47,4 +47,7 @@ struct mhd_topology {
   // the grid's patches as the builder derived them (for inspection)
   std::vector<mhd_patch> faces, edges, vertices;
   std::vector<mhd_physical_patch> physical;
+  // periodic blocks and lattices: Sync(Eres) and Sync(dB) are the E edge and
+  // B face groups' copies (no physical boundary tells them apart)
+  bool res_groups_alias = false;
 };

@@ -162,9 +162,9 @@ std::string setup_mhd() {
   o << job_str("dipole_line", "0.0 0.0 0.0 0.0 0.0 -2.83E19 0.0") << "\n";
   o << "LIST==================================================================\n";
   o << "bool    is_Mercury_resistance " << job_int("resistive", 0) << "\n";
-  o << "double  mercury_eta_r_inner 0.84\n";
-  o << "double  mercury_eta_r_outer 1.04\n";
-  o << "double  mercury_eta_width 0.02\n";
+  o << "double  mercury_eta_r_inner " << job_dbl("eta_r_inner", 0.84) << "\n";
+  o << "double  mercury_eta_r_outer " << job_dbl("eta_r_outer", 1.04) << "\n";
+  o << "double  mercury_eta_width " << job_dbl("eta_width", 0.02) << "\n";
   o << "double  implicit_resistive_ksp_rtol " << job_dbl("ksp_rtol", 5e-3) << "\n";
   o << "double  implicit_resistive_ksp_atol " << job_dbl("ksp_atol", 1e-8) << "\n";
   o << "int     implicit_resistive_ksp_max_it " << job_int("ksp_max_it", 200) << "\n";

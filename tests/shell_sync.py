@@ -14,7 +14,23 @@ from mpcns_mercury_b200.capi import FIELD_ID, REF_FIELD
 GROUPS = {"UCELL": ("Ucell", ["U_H", "U_Na"]), "BFACE": ("Bface", ["B_xi", "B_eta", "B_zeta"]),
           "EHALL": ("Ehall", ["Ehall_xi", "Ehall_eta", "Ehall_zeta"]), "EEDGE": ("Eedge", ["E_xi", "E_eta", "E_zeta"]),
           "B_CELL": ("B_cell", ["B_cell", "Bind_cell"]), "JEDGE": ("Jedge", ["J_xi", "J_eta", "J_zeta"]),
-          "J_CELL": ("J_cell", ["J_cell"])}
+          "J_CELL": ("J_cell", ["J_cell"]),
+          # the implicit resistive substep's groups (a resistive run); the
+          # engine keeps E_res, dB and dJ in the E, B and J arrays, and dJ
+          # uses the J edge group's tables
+          "ERES": ("Eres", ["Eres_xi", "Eres_eta", "Eres_zeta"]), "DB": ("dB", ["dB_xi", "dB_eta", "dB_zeta"]),
+          "DJ": ("dJ", ["dJ_xi", "dJ_eta", "dJ_zeta"])}
+RESISTIVE_GROUPS = {"ERES", "DB", "DJ"}
+TABLES = {"DJ": "JEDGE"}  # probe group -> the descriptor group whose tables apply
+_ARRAY_OF = {"Eres": "E", "dB": "B", "dJ": "J"}
+
+
+def field_key(f):
+    """The mhd_field id whose arrays hold the reference field f."""
+    head, _, tail = f.partition("_")
+    if head in _ARRAY_OF:
+        f = _ARRAY_OF[head] + "_" + tail
+    return FIELD_ID[REF_FIELD[f]]
 # the oracle harness's default upstream (INITIAL list, SI): U T n M c_y c_z Bx By Bz
 INITIAL = (4.03112887e5, 1.7407e5, 4e7, 0.001, 1.240347346e-1, 0.0, -1.52e-8, 8.4e-9, -8.5e-9)
 GAMMA = 1.6667
@@ -130,16 +146,17 @@ def probe_and_apply(ref_oracle, group, na, nr):
     from mpcns_mercury_b200.constants import reference_constants
 
     ref_group, fields = GROUPS[group]
+    res = 1 if group in RESISTIVE_GROUPS else 0
     job = dict(case="shell", na=na, nr=nr, mode="probe", probe_group=ref_group, probe_fields=" ".join(fields),
-               steps=0, dump_grid=1, initial_line=" ".join(repr(v) for v in INITIAL))
+               steps=0, dump_grid=1, initial_line=" ".join(repr(v) for v in INITIAL), resistive=res)
     dump = ref_oracle.run_job(job)
-    L, t, desc = shell_topology(na, nr)
+    L, t, desc = shell_topology(na, nr, resistive=res)
     try:
-        recs = {(FIELD_ID[REF_FIELD[f]], b): dump[("before:" + f, b)] for f in fields for b in range(6)}
+        recs = {(field_key(f), b): dump[("before:" + f, b)] for f in fields for b in range(6)}
         arrays = {k: r.data.copy() for k, r in recs.items()}
         nodes = {b: (dump[("node_x", b)], dump[("node_y", b)], dump[("node_z", b)]) for b in range(6)}
         c = reference_constants(initial=INITIAL)
-        apply_group(desc, GORDER.index(group), arrays, recs, nodes, [c.bc[q] for q in range(19)])
+        apply_group(desc, GORDER.index(TABLES.get(group, group)), arrays, recs, nodes, [c.bc[q] for q in range(19)])
     finally:
         L.mhd_topology_destroy(t)
     return dump, arrays, fields

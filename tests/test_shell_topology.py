@@ -67,12 +67,12 @@ def test_shell_patches_match_reference(ref_oracle, na, nr):
 @pytest.mark.parametrize("na,nr", SIZES)
 @pytest.mark.parametrize("group", list(GROUPS))
 def test_shell_sync_tables_match_reference_probe(ref_oracle, group, na, nr):
-    from mpcns_mercury_b200.capi import FIELD_ID, REF_FIELD
+    from shell_sync import field_key
 
     dump, arrays, fields = probe_and_apply(ref_oracle, group, na, nr)
     for f in fields:
         for b in range(6):
-            got = arrays[(FIELD_ID[REF_FIELD[f]], b)]
+            got = arrays[(field_key(f), b)]
             want = dump[("after:" + f, b)].data
             assert np.array_equal(np.isnan(got), np.isnan(want)), (f, b)
             m = ~np.isnan(want)
