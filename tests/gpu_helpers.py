@@ -94,13 +94,14 @@ def div_b(ctx, n):
     return float(np.abs(d).max()) / scale
 
 
-def shell_constants(precision=0):
+def shell_constants(precision=0, **kw):
     """The shell case's constants: the reference's REF list with the shell
-    job's upstream (INITIAL list), as the oracle harness writes them."""
+    job's upstream (INITIAL list), as the oracle harness writes them; kw:
+    further reference_constants arguments (resistive, res_rtol, ...)."""
     from mpcns_mercury_b200 import reference_constants
 
     initial = tuple(float(v) for v in mo.SHELL_UPSTREAM.split())
-    return reference_constants(cfl=mo.SHELL_JOB["cfl"], initial=initial)
+    return reference_constants(cfl=mo.SHELL_JOB["cfl"], initial=initial, **kw)
 
 
 def shell_context(dump, na, nr, precision=0, constants=None):
@@ -110,8 +111,10 @@ def shell_context(dump, na, nr, precision=0, constants=None):
 
     from mpcns_mercury_b200 import capi
 
+    constants = constants or shell_constants()
     t = ctypes.c_void_p()
-    capi.check(capi.lib().mhd_topology_cubed_sphere(na, nr, NGHOST, 0, ctypes.byref(t)), "mhd_topology_cubed_sphere")
-    ctx = Context([(na, na, nr)] * 6, NGHOST, constants or shell_constants(), topology=t, precision=precision)
+    capi.check(capi.lib().mhd_topology_cubed_sphere(na, nr, NGHOST, int(bool(constants.resistive)), ctypes.byref(t)),
+               "mhd_topology_cubed_sphere")
+    ctx = Context([(na, na, nr)] * 6, NGHOST, constants, topology=t, precision=precision)
     upload_from_dump(ctx.upload, dump)
     return ctx

@@ -122,3 +122,42 @@ def test_config2_shell_matches_reference(config2, precision, tol):
     assert not bad, {k: v for k, v in worst.items() if v > tol}
     assert ctx.info().status == 0
     ctx.close()
+
+
+RES_EXTRA = dict(resistive=1, ksp_rtol=1e-14, ksp_atol=1e-300, ksp_max_it=4000)
+
+
+@pytest.fixture(scope="module")
+def res_shell(ref_oracle):
+    """The shell with the implicit resistive substep (the reference's radial
+    tanh window of eta around the inner wall), solved to 1e-14 by the
+    reference's GMRES."""
+    if not has_gpu():
+        pytest.skip("no GPU")
+    return ref_oracle.shell_run(na=NA, nr=NR, steps=STEPS, dump_at=[0, STEPS], extra=RES_EXTRA)
+
+
+def test_shell_implicit_resistivity_matches_reference(ref_oracle, res_shell):
+    """Sync(Eres)/Sync(dB)/Sync(dJ) with the shell's physical boundaries and
+    the singular edges' current inside the operator, B* restore and update:
+    the state after the steps within 1e-10 relative L2 per field (CG in the
+    1/(eta alpha)-weighted product against the reference's GMRES, both to a
+    relative residual of 1e-14)."""
+    import mercury_oracle as mo
+    from gpu_helpers import compare, shell_constants, shell_context
+
+    k = shell_constants(resistive=True, res_rtol=1e-14, res_max_it=2000)
+    ctx = shell_context(res_shell, NA, NR, constants=k)
+    ctx.prepare()
+    ctx.step(STEPS)
+    worst, bad = compare(ctx, res_shell, f"step{STEPS}:", mo.STATE_FIELDS, 1e-10)
+    print("shell implicit resistivity: max rel L2", max(worst.values()))
+    assert not bad, {k: v for k, v in worst.items() if v > 1e-10}
+    info = ctx.info()
+    assert info.status == 0 and info.res_iters > 0 and info.res_relres <= 1e-14
+    # the substep is active: B differs from the run without it
+    a = res_shell[(f"step{STEPS}:B_xi", 0)].data
+    plain = ref_oracle.shell_run(na=NA, nr=NR, steps=STEPS, dump_at=[STEPS], extra={"dump_fields": "B_xi"})
+    b = plain[(f"step{STEPS}:B_xi", 0)].data
+    assert float(np.abs(a - b).max()) > 1e-9
+    ctx.close()
