@@ -93,9 +93,12 @@ enum mhd_location { MHD_CELL = 0, MHD_FACE_XI, MHD_FACE_ETA, MHD_FACE_ZETA, MHD_
  * tables address those fields; they differ from MHD_SYNC_EEDGE and MHD_SYNC_BFACE
  * only in the physical handlers (Farfield: copy, Coupled-Solid: nothing).  dJ
  * (in the J edge arrays) shares MHD_SYNC_JEDGE's handlers and tables.  Only
- * solves with the implicit resistive substep read them. */
+ * solves with the implicit resistive substep read them.  MHD_SYNC_BADD is
+ * Sync("Badd") of the background field (Z4_Mercury/src/MercurySolver.cpp:141),
+ * run once after the background is set (mhd_setup_geometry_bg); periodic
+ * blocks and lattices have no copies in it. */
 enum mhd_group { MHD_SYNC_UCELL = 0, MHD_SYNC_BFACE, MHD_SYNC_EHALL, MHD_SYNC_EEDGE, MHD_SYNC_B_CELL,
-                 MHD_SYNC_JEDGE, MHD_SYNC_J_CELL, MHD_SYNC_ERES, MHD_SYNC_DB, MHD_NUM_GROUPS };
+                 MHD_SYNC_JEDGE, MHD_SYNC_J_CELL, MHD_SYNC_ERES, MHD_SYNC_DB, MHD_SYNC_BADD, MHD_NUM_GROUPS };
 
 /* Indices into mhd_constants.bc (BuildMercuryBackgroundState,
  * Z4_Mercury/include/0_BackgroundState.h:18-85, and the wall floors of
@@ -347,14 +350,24 @@ int mhd_device_view(mhd_ctx *ctx, int field, int block, int comp, double **base,
  * byte-identical to the ones the CPU oracle generates. */
 int mhd_seeded_uniform(uint64_t seed, int64_t count, double a, double *out);
 
-/* Host helpers of the cubed-sphere shell case (no counterpart in the
- * reference solver, which reads its grid from files): the nodes of panel
- * `panel` over [-G, n + 1 + G) per axis (AoS, k fastest; the owned nodes are
- * the oracle shell case's, the ghost nodes continue the panel mapping; the
- * ghost angles must stay below 90 degrees: na > 2 G), and the Hall radial
+/* Host helpers of the cubed-sphere shell case: the nodes of panel `panel`
+ * over [-G, n + 1 + G) per axis (AoS, k fastest).  The owned
+ * nodes are the equiangular panel directions (panels 0-3 around the z axis,
+ * 4 north, 5 south) at radii r_k = r_out^(k / nr); the reference reads them
+ * from grid files, so they have no counterpart there.  The ghost nodes are
+ * extrapolated as the reference's grid reader adds them (Block::Add_ghostmesh,
+ * src/1_grid/1_MPCNS_Grid.cpp:591-815), so the static fields computed from
+ * them match the reference's on every position it fills.  And the Hall radial
  * taper (HallRadialTaper_, Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:6-13)
  * at n points. */
 int mhd_shell_nodes(int32_t na, int32_t nr, double r_out, int32_t panel, int32_t G, double *out);
+/* All six panels' nodes (panel-major, each as mhd_shell_nodes lays it out)
+ * with the ghost nodes the reference's grid preprocessing leaves on this
+ * grid (Grid::Grid_Preprocess, include/1_grid/1_MPCNS_Grid.h:151-224:
+ * extrapolation, the inner-interface mesh transfer and the corner
+ * treatment): the strips beside a panel edge hold the neighbour panel's
+ * nodes, the corner columns the nodes those strips received.  G <= na. */
+int mhd_shell_grid(int32_t na, int32_t nr, double r_out, int32_t G, double *out);
 int mhd_hall_taper(double r_min, double r_max, int64_t n, const double *xyz, double *out);
 
 /* ---- Hall edge EMF without device allocation ----
@@ -556,6 +569,40 @@ int mhd_topology_destroy(mhd_topology *topo);
  * nodes); mhd_prepare must follow. */
 int mhd_batch_setup_geometry(mhd_batch *batch, int slot, int block, const double *nodes, double L_ref);
 int mhd_setup_geometry(mhd_ctx *ctx, int block, const double *nodes, double L_ref);
+
+/* The inputs of a magnetosphere case that the reference derives from its
+ * parameter lists, for mhd_setup_geometry_bg:
+ *   the background field (DipoleField, Z4_Mercury/include/operators/Dipole.h:26-43,
+ *     load_from_param :46-86, Build_Badd_FaceFlux :89-363): the dipoles'
+ *     vector potential A along the edges [-1, n + stagger] of the block,
+ *     integrated as A(midpoint) . dr, its curl on the faces it reaches, plus
+ *     B0 . JD of the IMF on every face of [-g, n + stagger + g);
+ *   the Hall radial taper (HallRadialTaperEdge_, HallRadialTaper_,
+ *     Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:6-25) at the
+ *     owned edges' midpoints and the owned cells' centres (0 elsewhere);
+ *   the implicit resistivity per owned edge (ImplicitResistiveEtaAtEdge_,
+ *     Z4_Mercury/src/implicit/Mercury_ImplicitResistive.cpp:228-253, with
+ *     MercuryResistivityShape_, Z4_Mercury/src/physics/MercurySolver_Tools.cpp:50-69),
+ *     written when the solve has the implicit substep.
+ * The dipoles, IMF and length / field units are in SI as the reference's
+ * lists hold them and are nondimensionalised as load_from_param does. */
+#define MHD_MAX_DIPOLES 4
+typedef struct mhd_background {
+  int32_t n_dipoles, pad_;
+  double dipole[MHD_MAX_DIPOLES][7]; /* x0 y0 z0 [m], mx my mz [A m^2], a [m]: the Dipole<n> lists */
+  double B_imf[3];                   /* Bx By Bz [T] of the INITIAL list */
+  double L_ref, B_ref, mu_mag;       /* REF list and mu_mag of the constant list */
+  double hall_r_min, hall_r_max;     /* r_min, r_max of the Hall taper (equal: a step at r_min) */
+  double inver_Rem;                  /* eta_max_mercury / (mu_mag U_ref L_ref) (calc_physical_constant) */
+  double eta_r_inner, eta_r_outer, eta_width; /* mercury_eta_r_inner, _outer, _width */
+} mhd_background;
+/* mhd_setup_geometry plus the background, taper and resistivity of `bg` on
+ * the block (bg NULL: mhd_setup_geometry).  Once every block of the solve is
+ * set, mhd_sync / mhd_batch_sync(MHD_SYNC_BADD) completes the background as
+ * the reference's Sync("Badd") does. */
+int mhd_batch_setup_geometry_bg(mhd_batch *batch, int slot, int block, const double *nodes, double L_ref,
+                                const mhd_background *bg);
+int mhd_setup_geometry_bg(mhd_ctx *ctx, int block, const double *nodes, double L_ref, const mhd_background *bg);
 
 /* ---- Restart files ----
  * The reference's checkpoint format, MPCNSRST version 1

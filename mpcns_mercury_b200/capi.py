@@ -60,7 +60,7 @@ REF_FIELD = {
     "local_arti_eta_xi": "LOCAL_ETA_XI", "local_arti_eta_eta": "LOCAL_ETA_ETA", "local_arti_eta_zeta": "LOCAL_ETA_ZETA",
 }
 
-GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL", "ERES", "DB"]
+GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL", "ERES", "DB", "BADD"]
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_DT", 5: "ERR_NONFINITE", 6: "ERR_SOLVE",
           7: "ERR_STATE"}
 
@@ -127,6 +127,16 @@ class MhdSingularEdges(ctypes.Structure):
                 ("faces", ctypes.POINTER(MhdSingularFace))]
 
 
+class MhdBackground(ctypes.Structure):
+    """mhd_background: dipoles (x0 y0 z0 mx my mz a, SI), IMF [T], units,
+    Hall taper radii, implicit resistivity window."""
+    _fields_ = [("n_dipoles", ctypes.c_int32), ("pad_", ctypes.c_int32), ("dipole", (ctypes.c_double * 7) * 4),
+                ("B_imf", ctypes.c_double * 3), ("L_ref", ctypes.c_double), ("B_ref", ctypes.c_double),
+                ("mu_mag", ctypes.c_double), ("hall_r_min", ctypes.c_double), ("hall_r_max", ctypes.c_double),
+                ("inver_Rem", ctypes.c_double), ("eta_r_inner", ctypes.c_double), ("eta_r_outer", ctypes.c_double),
+                ("eta_width", ctypes.c_double)]
+
+
 class MhdDesc(ctypes.Structure):
     _fields_ = [("n_blocks", ctypes.c_int32), ("cells", ctypes.POINTER(ctypes.c_int32)),
                 ("nghost", ctypes.c_int32), ("precision", ctypes.c_int32), ("constants", MhdConstants),
@@ -184,7 +194,8 @@ EXPORTS = [
     "mhd_save_restart", "mhd_load_restart", "mhd_tecplot_write", "mhd_rundata_write", "mhd_rundata_read", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
-    "mhd_batch_device_view",
+    "mhd_batch_device_view", "mhd_shell_nodes", "mhd_shell_grid", "mhd_hall_taper", "mhd_setup_geometry_bg",
+    "mhd_batch_setup_geometry_bg",
 ]
 
 _lib = None
@@ -242,6 +253,14 @@ def lib() -> ctypes.CDLL:
     L.mhd_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
     L.mhd_div_b.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
     L.mhd_setup_geometry.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_double]
+    L.mhd_shell_nodes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                                  ctypes.c_void_p]
+    L.mhd_setup_geometry_bg.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
+                                        ctypes.POINTER(MhdBackground)]
+    L.mhd_batch_setup_geometry_bg.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
+                                              ctypes.POINTER(MhdBackground)]
+    L.mhd_shell_grid.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_void_p]
+    L.mhd_hall_taper.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
     L.mhd_batch_setup_geometry.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_double]
     RI = ctypes.POINTER(MhdRestartImage)
     L.mhd_restart_values.argtypes = [RI, ctypes.c_int32]
@@ -505,6 +524,14 @@ class Context:
         a = np.ascontiguousarray(nodes, dtype=np.float64)
         check(lib().mhd_setup_geometry(self.ctx, block, a.ctypes.data, float(L_ref)), "mhd_setup_geometry")
 
+    def setup_background(self, nodes, background, block: int = 0, L_ref: float = 2.44e6):
+        """setup_geometry plus the background field, Hall taper and implicit
+        resistivity of an MhdBackground (mhd_setup_geometry_bg); sync("BADD")
+        once every block is set."""
+        a = np.ascontiguousarray(nodes, dtype=np.float64)
+        check(lib().mhd_setup_geometry_bg(self.ctx, block, a.ctypes.data, float(L_ref), ctypes.byref(background)),
+              "mhd_setup_geometry_bg")
+
     def save_restart(self, path):
         """Write the state as an MPCNSRST restart file (mhd_save_restart)."""
         check(lib().mhd_save_restart(self.ctx, os.fsencode(path)), "mhd_save_restart")
@@ -659,6 +686,13 @@ class Batch:
         check(lib().mhd_batch_setup_geometry(self.b, slot, block, a.ctypes.data, float(L_ref)),
               "mhd_batch_setup_geometry")
 
+    def setup_background(self, slot: int, nodes, background, block: int = 0, L_ref: float = 2.44e6):
+        """setup_geometry plus an MhdBackground (mhd_batch_setup_geometry_bg);
+        sync(slot, "BADD") once every block of the solve is set."""
+        a = np.ascontiguousarray(nodes, dtype=np.float64)
+        check(lib().mhd_batch_setup_geometry_bg(self.b, slot, block, a.ctypes.data, float(L_ref),
+                                                ctypes.byref(background)), "mhd_batch_setup_geometry_bg")
+
     def save_restart(self, slot: int, path):
         """Write a solve's state as an MPCNSRST restart file (mhd_batch_save_restart)."""
         check(lib().mhd_batch_save_restart(self.b, slot, os.fsencode(path)), "mhd_batch_save_restart")
@@ -689,3 +723,29 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def shell_nodes(na: int, nr: int, panel: int, r_out: float = 8.0, G: int = 5) -> np.ndarray:
+    """Nodes of one panel of the cubed-sphere shell over [-G, n + 1 + G) per
+    axis, (ni, nj, nk, 3) (mhd_shell_nodes)."""
+    e0, e2 = na + 1 + 2 * G, nr + 1 + 2 * G
+    out = np.empty((e0, e0, e2, 3), dtype=np.float64)
+    check(lib().mhd_shell_nodes(na, nr, float(r_out), panel, G, out.ctypes.data), "mhd_shell_nodes")
+    return out
+
+
+def shell_grid(na: int, nr: int, r_out: float = 8.0, G: int = 5) -> np.ndarray:
+    """All six panels' nodes with the ghost nodes of the reference's grid
+    preprocessing, (6, ni, nj, nk, 3) (mhd_shell_grid)."""
+    e0, e2 = na + 1 + 2 * G, nr + 1 + 2 * G
+    out = np.empty((6, e0, e0, e2, 3), dtype=np.float64)
+    check(lib().mhd_shell_grid(na, nr, float(r_out), G, out.ctypes.data), "mhd_shell_grid")
+    return out
+
+
+def hall_taper(r_min: float, r_max: float, xyz) -> np.ndarray:
+    """The Hall radial taper at points xyz (..., 3) (mhd_hall_taper)."""
+    a = np.ascontiguousarray(xyz, dtype=np.float64)
+    out = np.empty(a.shape[:-1], dtype=np.float64)
+    check(lib().mhd_hall_taper(float(r_min), float(r_max), out.size, a.ctypes.data, out.ctypes.data), "mhd_hall_taper")
+    return out

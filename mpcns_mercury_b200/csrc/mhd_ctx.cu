@@ -475,7 +475,7 @@ int publish(mhd_batch *b) {
 // only at owned and alias positions; in the implicit resistive substep E_res
 // only there and dB one layer out).  Explicit syncs (mhd_sync) fill every
 // layer.
-constexpr int kHaloDepth[MHD_NUM_GROUPS] = {2, 2, 0, 0, 1, 0, 1, 0, 1};
+constexpr int kHaloDepth[MHD_NUM_GROUPS] = {2, 2, 0, 0, 1, 0, 1, 0, 1, 0};
 
 // Ghost depth of a DOF: how far outside its owned range [0, n + stagger) it lies.
 int dof_depth(const Solve *S, const mhd_dof &d) {
@@ -800,7 +800,7 @@ int upload_groups(Solve *S, const mhd_sync_group *groups, cudaStream_t st) {
     tabs[q] = p == 0 ? G.halo : p == 1 ? G.owner : p == 2 ? G.stash : G.stash + G.n_stash;
     ntab[q] = p == 0 ? G.n_halo : p == 1 ? G.n_owner : G.n_stash;
     if (ntab[q] < 0 || (ntab[q] > 0 && !tabs[q])) return fail(MHD_ERR_ARG, "group %d phase %d: bad table", g, p);
-    if (g >= MHD_SYNC_ERES && !S->consts.resistive) ntab[q] = 0;  // read only by the implicit substep
+    if ((g == MHD_SYNC_ERES || g == MHD_SYNC_DB) && !S->consts.resistive) ntab[q] = 0;  // only the implicit substep
     Encoded &e = enc[q];
     e.dst.resize(ntab[q]);
     e.src.resize(ntab[q]);
@@ -1132,6 +1132,8 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
                            cudaMemcpyDeviceToDevice, st));
   launch_res_cross(Dm, C->dblocks, RES_X_SETUP, st);
   CUDA_TRY(cudaGetLastError());
+  if (S->T->sg_n > 0)  // the singular edges' canonical vectors and inverse Hodge stars (FP64 in both)
+    CUDA_TRY(cudaMemcpyAsync(C->sg_geo, S->sg_geo, sizeof(double) * 4 * S->T->sg_n, cudaMemcpyDeviceToDevice, st));
   if ((rc = set_state_field(sh, cs, offsetof(SolveState, mask), &one, sizeof one))) return rc;
   if ((rc = res_dot(sh, RES_DOT_RR))) return rc;
   const double bnorm = std::sqrt(sh->hres[1]);
@@ -1427,7 +1429,7 @@ static int upload_phys(Solve *S, const mhd_desc *desc, cudaStream_t st) {
     const mhd_phys_op *ops = q < kMaxGroups ? desc->groups[q].phys : desc->wall;
     int n = q < kMaxGroups ? desc->groups[q].n_phys : desc->n_wall;
     if (n < 0 || (n > 0 && !ops)) return fail(MHD_ERR_ARG, "physical operations %d: bad table", q);
-    if (q >= MHD_SYNC_ERES && q < kMaxGroups && !S->consts.resistive) n = 0;  // the implicit substep's groups
+    if ((q == MHD_SYNC_ERES || q == MHD_SYNC_DB) && !S->consts.resistive) n = 0;  // the implicit substep's groups
     std::vector<int64_t> set;
     std::vector<DevPhysOp> other;
     for (int t = 0; t < n; ++t) {
@@ -1639,10 +1641,6 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
   S->arena_bytes = 2 * u + m + ((int64_t)S->n_staging * S->es + 255) / 256 * 256;
   const mhd_constants &k = desc->constants;
   S->consts = make_consts(k, desc->nghost);
-  if (!periodic && k.resistive && desc->precision == kMixed &&
-      (desc->singular.n_edges > 0 || desc->n_wall > 0 || desc->n_staging > 0))
-    return bail(fail(MHD_ERR_ARG, "the mixed-precision implicit resistive substep is not supported on grids with "
-                                  "physical boundaries or singular edges (FP64 is)"));
   if (cudaMallocFromPoolAsync((void **)&S->arena, S->arena_bytes, b->pool, st) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MHD_ERR_OOM, "arena of %lld bytes", (long long)S->arena_bytes));
@@ -2007,11 +2005,48 @@ int mhd_batch_load_restart(mhd_batch *b, int slot, const char *path, int32_t *st
   return MHD_OK;
 }
 
+// The background inputs nondimensionalised as DipoleField::load_from_param
+// (Z4_Mercury/include/operators/Dipole.h:46-86) and Build_Badd_FaceFlux's IMF
+// (:323-325) do it.
+static bool geo_background(const mhd_background &in, GeoBg *out) {
+  if (in.n_dipoles < 0 || in.n_dipoles > MHD_MAX_DIPOLES || !(in.L_ref > 0.0) || !(in.B_ref > 0.0) ||
+      !(in.mu_mag > 0.0))
+    return false;
+  if (in.inver_Rem > 0.0 && !(in.eta_width > 0.0)) return false;
+  GeoBg g{};
+  g.nd = in.n_dipoles;
+  double inver_m = 4 * 3.1415926535 * in.B_ref * in.L_ref * in.L_ref * in.L_ref / in.mu_mag;
+  inver_m = 1.0 / inver_m;
+  for (int d = 0; d < in.n_dipoles; ++d) {
+    for (int q = 0; q < 3; ++q) {
+      g.r0[d][q] = in.dipole[d][q] / in.L_ref;
+      g.m[d][q] = in.dipole[d][3 + q] * inver_m;
+    }
+    g.a[d] = in.dipole[d][6] / in.L_ref;
+  }
+  for (int q = 0; q < 3; ++q) g.B0[q] = in.B_imf[q] / in.B_ref;
+  g.hall_r_min = in.hall_r_min;
+  g.hall_r_max = in.hall_r_max;
+  g.inver_Rem = in.inver_Rem;
+  g.eta_r0 = in.eta_r_inner;
+  g.eta_r1 = in.eta_r_outer;
+  g.eta_w = in.eta_width;
+  *out = g;
+  return true;
+}
+
 int mhd_batch_setup_geometry(mhd_batch *b, int slot, int block, const double *nodes, double L_ref) {
+  return mhd_batch_setup_geometry_bg(b, slot, block, nodes, L_ref, nullptr);
+}
+
+int mhd_batch_setup_geometry_bg(mhd_batch *b, int slot, int block, const double *nodes, double L_ref,
+                                const mhd_background *bgp) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
   Solve *S = b->slots[slot];
   if (block < 0 || block >= S->nblocks || !nodes) return fail(MHD_ERR_ARG, "mhd_batch_setup_geometry: bad arguments");
+  GeoBg bg{};
+  if (bgp && !geo_background(*bgp, &bg)) return fail(MHD_ERR_ARG, "mhd_batch_setup_geometry_bg: bad background");
   const Box &bx = S->boxes[block];
   cudaStream_t st = b->stream;
   // the nodes (x, y, z over the whole box) into a temporary device array
@@ -2023,7 +2058,9 @@ int mhd_batch_setup_geometry(mhd_batch *b, int slot, int block, const double *no
     if (dn) cudaFreeAsync(dn, st);
     if (dtab) cudaFreeAsync(dtab, st);
   };
-  if (cudaMallocFromPoolAsync((void **)&dn, sizeof(double) * 3 * (size_t)bx.total, b->pool, st) != cudaSuccess ||
+  // with a background: 3 more arrays for the edge integrals of A
+  if (cudaMallocFromPoolAsync((void **)&dn, sizeof(double) * (bgp ? 6 : 3) * (size_t)bx.total, b->pool, st) !=
+          cudaSuccess ||
       cudaMallocFromPoolAsync((void **)&dtab, sizeof(void *) * GEO_COUNT, b->pool, st) != cudaSuccess) {
     cudaGetLastError();
     release();
@@ -2051,8 +2088,12 @@ int mhd_batch_setup_geometry(mhd_batch *b, int slot, int block, const double *no
   add(MHD_BCELL_W, 18);
   add(MHD_JCELL_W, 36);
   for (int f : {MHD_BADD_XI, MHD_BADD_ETA, MHD_BADD_ZETA, MHD_PHOTO, MHD_CELL_X, MHD_CELL_Y, MHD_CELL_Z, MHD_TAPER_XI,
-                MHD_TAPER_ETA, MHD_TAPER_ZETA})
+                MHD_TAPER_ETA, MHD_TAPER_ZETA, MHD_TAPER_CELL})
     add(f, 1);
+  for (int f : {MHD_ETA_RES_XI, MHD_ETA_RES_ETA, MHD_ETA_RES_ZETA}) {  // only solves with the implicit substep hold it
+    if (S->consts.resistive) add(f, 1);
+    else tab.push_back(nullptr);
+  }
   if ((int)tab.size() != GEO_COUNT) {
     release();
     return fail(MHD_ERR_ARG, "mhd_batch_setup_geometry: output table of %d components", (int)tab.size());
@@ -2074,7 +2115,8 @@ int mhd_batch_setup_geometry(mhd_batch *b, int slot, int block, const double *no
   k_scatter_aos<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(b->staging, -bx.G, -bx.G, -bx.G, e[0], e[1], e[2], 3,
                                                                  b->comp_ptrs, 1, bx.si, bx.sj, bx.G, 0);
   if ((ce = cudaGetLastError()) != cudaSuccess ||
-      (ce = launch_geometry(dn, gb, dtab, S->es == 4, L_ref, st)) != cudaSuccess) {
+      (ce = launch_geometry(dn, gb, dtab, S->es == 4, L_ref, bgp ? &bg : nullptr, dn + 3 * bx.total, st)) !=
+          cudaSuccess) {
     release();
     return fail(MHD_ERR_CUDA, "mhd_batch_setup_geometry: %s", cudaGetErrorString(ce));
   }
@@ -2350,6 +2392,11 @@ int mhd_div_b(mhd_ctx *ctx, double *max_abs) {
 int mhd_setup_geometry(mhd_ctx *ctx, int block, const double *nodes, double L_ref) {
   if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
   return mhd_batch_setup_geometry(ctx->batch, 0, block, nodes, L_ref);
+}
+
+int mhd_setup_geometry_bg(mhd_ctx *ctx, int block, const double *nodes, double L_ref, const mhd_background *bg) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_setup_geometry_bg(ctx->batch, 0, block, nodes, L_ref, bg);
 }
 
 int mhd_save_restart(mhd_ctx *ctx, const char *path) {

@@ -122,6 +122,7 @@ struct Out {
   bool fp32;
   int64_t o;
   __device__ __forceinline__ void put(int comp, double v) const {
+    if (!p[comp]) return;  // a field the solve does not hold
     if (comp < kGeoMetric || !fp32) ((double *)p[comp])[o] = v;
     else ((float *)p[comp])[o] = (float)v;
   }
@@ -250,6 +251,7 @@ __global__ void k_geometry(Geo g, void *const *outp, bool fp32, double L_ref) {
     const int clo[3] = {-gh, -gh, -gh}, chi[3] = {n[0] + gh, n[1] + gh, n[2] + gh};
     if (!in3(i, j, k, clo, chi)) continue;
     const int olo[3] = {0, 0, 0};
+    out.put(GEO_TAPER_CELL, in3(i, j, k, olo, n) ? 1.0 : 0.0);  // the taper at cell centres (off)
     if (in3(i, j, k, olo, n)) {
       // B_cell weights from the six oriented face area vectors
       P3 s[6];
@@ -365,10 +367,129 @@ __global__ void k_geometry(Geo g, void *const *outp, bool fp32, double L_ref) {
   }
 }
 
+// The Hall radial taper at (x, y, z) (HallRadialTaper_,
+// Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:6-13).
+__device__ double hall_taper(const GeoBg &bg, double x, double y, double z) {
+  const double r = sqrt(x * x + y * y + z * z);
+  const double width = bg.hall_r_max - bg.hall_r_min;
+  if (width <= 0.0) return (r >= bg.hall_r_min) ? 1.0 : 0.0;
+  const double mid = 0.5 * (bg.hall_r_min + bg.hall_r_max);
+  return 0.5 * (1.0 + tanh(2.0 * (r - mid) / width));
+}
+
+// Edge integrals of the dipoles' vector potential, A(midpoint) . dr, on the
+// edges [-1, n + stagger] of every family (Build_Badd_FaceFlux step 1,
+// Z4_Mercury/include/operators/Dipole.h:135-210, with A_of_dipole :26-43);
+// the implicit resistivity and the Hall taper of the owned edges
+// (ImplicitResistiveEtaAtEdge_, HallRadialTaperEdge_) and the taper at the
+// owned cell centres.
+__global__ void k_bg_edges(Geo g, void *const *outp, bool fp32, GeoBg bg, double *scratch) {
+  const GeoBox &b = g.b;
+  const int ei = b.n[0] + 1 + 2 * b.G, ej = b.n[1] + 1 + 2 * b.G, ek = b.n[2] + 1 + 2 * b.G;
+  const int64_t npos = (int64_t)ei * ej * ek;
+  const int gh = b.nghost;
+  const int n[3] = {b.n[0], b.n[1], b.n[2]};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < npos; t += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t % ek) - b.G, j = (int)((t / ek) % ej) - b.G, i = (int)(t / ((int64_t)ek * ej)) - b.G;
+    const Out out{outp, fp32, g.off(i, j, k)};
+    for (int ax = 0; ax < 3; ++ax) {
+      const int di = ax == 0, dj = ax == 1, dk = ax == 2;
+      // A . dr on [-1, n + stagger]; taper and resistivity on [-g, n + stagger + g)
+      const int alo[3] = {-1, -1, -1}, ahi[3] = {n[0] + 1 + (ax != 0), n[1] + 1 + (ax != 1), n[2] + 1 + (ax != 2)};
+      const int elo[3] = {-gh, -gh, -gh}, ehi[3] = {n[0] + gh + (ax != 0), n[1] + gh + (ax != 1), n[2] + gh + (ax != 2)};
+      const bool inA = in3(i, j, k, alo, ahi), inE = in3(i, j, k, elo, ehi);
+      if (!inA && !inE) continue;  // (both ranges keep the edge's far node inside the box)
+      const P3 x1 = g.node(i, j, k), x2 = g.node(i + di, j + dj, k + dk);
+      P3 xm, dr;
+      for (int q = 0; q < 3; ++q) {
+        xm.v[q] = (x1.v[q] + x2.v[q]) * 0.5;
+        dr.v[q] = x2.v[q] - x1.v[q];
+      }
+      if (inA) {
+        double A[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < bg.nd; ++d) {
+          double r[3];
+          for (int q = 0; q < 3; ++q) r[q] = xm.v[q] - bg.r0[d][q];
+          double f = (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) + bg.a[d] * bg.a[d];
+          f = sqrt(f) * f;
+          const double *m = bg.m[d];
+          const double c[3] = {m[1] * r[2] - m[2] * r[1], m[2] * r[0] - m[0] * r[2], m[0] * r[1] - m[1] * r[0]};
+          for (int q = 0; q < 3; ++q) A[q] += c[q] / f;
+        }
+        scratch[ax * b.total + g.off(i, j, k)] = A[0] * dr.v[0] + A[1] * dr.v[1] + A[2] * dr.v[2];
+      }
+      // owned edges: the taper at the midpoint and the resistivity
+      if (!inE) continue;
+      const int olo[3] = {0, 0, 0}, ohi[3] = {n[0] + (ax != 0), n[1] + (ax != 1), n[2] + (ax != 2)};
+      const bool own = in3(i, j, k, olo, ohi);
+      // HallRadialTaperEdge_ averages as 0.5 * (x1 + x2)
+      double hm[3];
+      for (int q = 0; q < 3; ++q) hm[q] = 0.5 * (x1.v[q] + x2.v[q]);
+      out.put(GEO_TAPER + ax, own ? hall_taper(bg, hm[0], hm[1], hm[2]) : 0.0);
+      if (bg.inver_Rem > 0.0) {
+        double eta = 0.0;
+        if (own && !(fabs(norm(dr)) <= 1.0e-12)) {
+          const double r = sqrt(hm[0] * hm[0] + hm[1] * hm[1] + hm[2] * hm[2]);
+          double shape = 0.5 * (tanh((r - bg.eta_r0) / bg.eta_w) - tanh((r - bg.eta_r1) / bg.eta_w));
+          shape = (!isfinite(shape) || shape <= 1.0e-10) ? 0.0 : (shape < 1.0 ? shape : 1.0);
+          eta = bg.inver_Rem * shape;
+        }
+        out.put(GEO_ETA_RES + ax, eta);
+      }
+    }
+    // the taper at the owned cell centres (the centre of cell (i, j, k) is dual point (i + 1, j + 1, k + 1))
+    const int clo[3] = {-gh, -gh, -gh}, chi[3] = {n[0] + gh, n[1] + gh, n[2] + gh};
+    if (in3(i, j, k, clo, chi)) {
+      const int olo[3] = {0, 0, 0};
+      double v = 0.0;
+      if (in3(i, j, k, olo, n)) {
+        const P3 c = g.dual(i + 1, j + 1, k + 1);
+        v = hall_taper(bg, c.v[0], c.v[1], c.v[2]);
+      }
+      out.put(GEO_TAPER_CELL, v);
+    }
+  }
+}
+
+// The background field on the faces of [-g, n + stagger + g): the curl of
+// the edge integrals where they reach (the faces [-1, n + stagger + 1)),
+// plus B0 . JD (Build_Badd_FaceFlux steps 0, 2, 3, Dipole.h:93-123,213-361).
+__global__ void k_bg_faces(Geo g, void *const *outp, bool fp32, GeoBg bg, const double *scratch) {
+  const GeoBox &b = g.b;
+  const int ei = b.n[0] + 1 + 2 * b.G, ej = b.n[1] + 1 + 2 * b.G, ek = b.n[2] + 1 + 2 * b.G;
+  const int64_t npos = (int64_t)ei * ej * ek;
+  const int gh = b.nghost;
+  const int n[3] = {b.n[0], b.n[1], b.n[2]};
+  const double *Ex = scratch, *Ey = scratch + b.total, *Ez = scratch + 2 * b.total;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < npos; t += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t % ek) - b.G, j = (int)((t / ek) % ej) - b.G, i = (int)(t / ((int64_t)ek * ej)) - b.G;
+    const Out out{outp, fp32, g.off(i, j, k)};
+    for (int dir = 0; dir < 3; ++dir) {
+      const int lo[3] = {-gh, -gh, -gh};
+      const int hi[3] = {n[0] + gh + (dir == 0), n[1] + gh + (dir == 1), n[2] + gh + (dir == 2)};
+      if (!in3(i, j, k, lo, hi)) continue;
+      const int clo[3] = {-1, -1, -1};
+      const int chi[3] = {n[0] + 1 + (dir == 0), n[1] + 1 + (dir == 1), n[2] + 1 + (dir == 2)};
+      double v = 0.0;
+      if (in3(i, j, k, clo, chi)) {
+        if (dir == 0)
+          v = 1.0 * ((Ey[g.off(i, j, k)] - Ey[g.off(i, j, k + 1)]) + (Ez[g.off(i, j + 1, k)] - Ez[g.off(i, j, k)]));
+        else if (dir == 1)
+          v = 1.0 * ((Ex[g.off(i, j, k + 1)] - Ex[g.off(i, j, k)]) + (Ez[g.off(i, j, k)] - Ez[g.off(i + 1, j, k)]));
+        else
+          v = 1.0 * ((Ex[g.off(i, j, k)] - Ex[g.off(i, j + 1, k)]) + (Ey[g.off(i + 1, j, k)] - Ey[g.off(i, j, k)]));
+      }
+      const P3 a = face_jd(g, dir, i, j, k);
+      v += (bg.B0[0] * a.v[0] + bg.B0[1] * a.v[1] + bg.B0[2] * a.v[2]);
+      out.put(GEO_BADD + dir, v);
+    }
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_geometry(const double *nodes, const GeoBox &box, void *const *out, bool fp32, double L_ref,
-                            cudaStream_t st) {
+                            const GeoBg *bg, double *scratch, cudaStream_t st) {
   Geo g{nodes, nodes + box.total, nodes + 2 * box.total, box};
   const int64_t npos = (int64_t)(box.n[0] + 1 + 2 * box.G) * (box.n[1] + 1 + 2 * box.G) * (box.n[2] + 1 + 2 * box.G);
   int dev = 0, sms = 148;
@@ -377,6 +498,10 @@ cudaError_t launch_geometry(const double *nodes, const GeoBox &box, void *const 
   const int64_t want = (npos + 127) / 128;
   const int blocks = (int)(want < (int64_t)sms * 16 ? want : (int64_t)sms * 16);
   k_geometry<<<blocks > 0 ? blocks : 1, 128, 0, st>>>(g, out, fp32, L_ref);
+  if (bg) {
+    k_bg_edges<<<blocks > 0 ? blocks : 1, 128, 0, st>>>(g, out, fp32, *bg, scratch);
+    k_bg_faces<<<blocks > 0 ? blocks : 1, 128, 0, st>>>(g, out, fp32, *bg, scratch);
+  }
   return cudaGetLastError();
 }
 

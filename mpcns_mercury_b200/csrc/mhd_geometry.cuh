@@ -24,7 +24,9 @@ enum GeoOut {
   GEO_PHOTO = 88,   // Na+ photo-production rate
   GEO_CELL = 89,    // cell centres x, y, z
   GEO_TAPER = 92,   // Hall radial taper per edge family (off: 1 where read)
-  GEO_COUNT = 95
+  GEO_TAPER_CELL = 95,  // Hall radial taper at the owned cell centres (off: 1)
+  GEO_ETA_RES = 96,     // implicit resistivity per owned edge family (null: the solve has none)
+  GEO_COUNT = 99
 };
 constexpr int kGeoMetric = 10;
 
@@ -36,9 +38,23 @@ struct GeoBox {
   int64_t total;   // positions of the box
 };
 
+// A magnetosphere's background field, Hall taper and implicit resistivity,
+// nondimensional (mhd_background after load_from_param's scaling).
+constexpr int kGeoMaxDipoles = 4;
+struct GeoBg {
+  int nd;                                       // dipoles
+  double r0[kGeoMaxDipoles][3], m[kGeoMaxDipoles][3], a[kGeoMaxDipoles];
+  double B0[3];                                 // IMF
+  double hall_r_min, hall_r_max;
+  double inver_Rem, eta_r0, eta_r1, eta_w;      // inver_Rem <= 0: no resistivity written
+};
+
 // nodes: 3 double arrays (x, y, z) over the box, node (i, j, k) at the box
-// offset of (i, j, k); out: GEO_COUNT component base pointers (box layout).
+// offset of (i, j, k); out: GEO_COUNT component base pointers (box layout;
+// the GEO_ETA_RES ones may be null).  bg (may be null): the background
+// inputs, with `scratch` 3 double arrays over the box for the edge
+// integrals of the dipoles' vector potential.
 cudaError_t launch_geometry(const double *nodes, const GeoBox &box, void *const *out, bool fp32, double L_ref,
-                            cudaStream_t st);
+                            const GeoBg *bg, double *scratch, cudaStream_t st);
 
 }  // namespace mhd

@@ -364,6 +364,8 @@ const GroupDef kGroupDefs[MHD_NUM_GROUPS] = {
     // the implicit substep's E_res and dB, kept in the E edge and B face arrays
     {MHD_SYNC_ERES, kEdge1, 3, {MHD_E_XI, MHD_E_ETA, MHD_E_ZETA}, true},
     {MHD_SYNC_DB, kFace2, 3, {MHD_B_XI, MHD_B_ETA, MHD_B_ZETA}, true},
+    // the background field, synced once after its setup
+    {MHD_SYNC_BADD, kFace2, 3, {MHD_BADD_XI, MHD_BADD_ETA, MHD_BADD_ZETA}, true},
 };
 
 // The physical handlers MercuryBoundary::InstallHandlers registers for the
@@ -375,6 +377,7 @@ Handler handler(int group, int field, int bc, bool resistive) {
   // nothing); BC_Farfield_Eedge_set_zerocurl, registered for Eres_* on
   // Farfield, falls back to the copy for every field not named E_*
   if (group == MHD_SYNC_ERES || group == MHD_SYNC_DB) return far ? hCopy : hNop;
+  if (group == MHD_SYNC_BADD) return far ? hCopy : hNop;  // Badd_*: the defaults
   switch (field) {
     case MHD_U_H: return far ? hFarU_H : hWallU_H;
     case MHD_U_NA: return far ? hFarU_Na : hWallU_Na;
@@ -1086,7 +1089,7 @@ int build(Grid &G, bool resistive, mhd_topology **out) {
     const Classes ecls = edge_classes(G, N), fcls = face_classes(G, N);
     int staging = 0;
     for (int q = 0; q < MHD_NUM_GROUPS; ++q) {
-      if (q >= MHD_SYNC_ERES && !resistive) continue;  // read only by the implicit substep
+      if ((q == MHD_SYNC_ERES || q == MHD_SYNC_DB) && !resistive) continue;  // read only by the implicit substep
       GroupTables T = replay_group(G, kGroupDefs[q], fcls, ecls, resistive, &staging);
       t->halo[q].assign(T.halo);
       t->owner[q].assign(T.owner);

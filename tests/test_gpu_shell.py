@@ -161,3 +161,23 @@ def test_shell_implicit_resistivity_matches_reference(ref_oracle, res_shell):
     b = plain[(f"step{STEPS}:B_xi", 0)].data
     assert float(np.abs(a - b).max()) > 1e-9
     ctx.close()
+
+
+def test_shell_implicit_resistivity_mixed(res_shell):
+    """The mixed form on the shell: residual and its norms in FP64 on the
+    solve's FP64 companion (with the singular edges' geometry), FP32 CG
+    corrections, refined to 1e-10; the state within 1e-5 relative L2."""
+    import mercury_oracle as mo
+    from gpu_helpers import compare, shell_constants, shell_context
+
+    k = shell_constants(resistive=True, res_rtol=1e-10, res_max_it=2000)
+    ctx = shell_context(res_shell, NA, NR, precision=1, constants=k)
+    ctx.prepare()
+    ctx.step(STEPS)
+    worst, bad = compare(ctx, res_shell, f"step{STEPS}:", mo.STATE_FIELDS, 1e-5)
+    info = ctx.info()
+    print("shell mixed implicit: refinements", info.res_refinements, "CG iterations", info.res_iters,
+          "max rel L2", max(worst.values()))
+    assert not bad, {k: v for k, v in worst.items() if v > 1e-5}
+    assert info.status == 0 and info.res_relres <= 1e-10
+    ctx.close()

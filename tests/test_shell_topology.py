@@ -125,3 +125,25 @@ def test_shell_singular_edges_are_the_eight_radial_lines():
             assert s.face_offset[e + 1] - s.face_offset[e] == 3  # three seam faces, one owner each
     finally:
         L.mhd_topology_destroy(t)
+
+
+@pytest.mark.parametrize("na,nr", [(5, 6), (6, 8), (8, 12)])
+def test_shell_grid_matches_reference_grid(ref_oracle, na, nr):
+    """mhd_shell_grid: the owned nodes of the shell case and every ghost node
+    as the reference's grid preprocessing leaves it (extrapolation, interface
+    transfer, corner treatment), bit for bit over the whole node range; and
+    mhd_shell_nodes alone: the owned nodes and the radial ghost layers above
+    the panel (the extrapolation, which no transfer overwrites)."""
+    from mpcns_mercury_b200 import capi
+
+    d = ref_oracle.shell_run(na=na, nr=nr, steps=0, dump_at=[0], extra={"dump_fields": "U_H"})
+    G = -d[("node_x", 0)].lo[0]
+    grid = capi.shell_grid(na, nr, r_out=8.0, G=G)
+    for b in range(6):
+        alone = capi.shell_nodes(na, nr, b, r_out=8.0, G=G)
+        for a, ax in enumerate("xyz"):
+            want = d[("node_" + ax, b)].data[..., 0]
+            assert want.shape == grid.shape[1:4], (want.shape, grid.shape)
+            assert np.array_equal(grid[b, ..., a], want), (b, ax, float(np.abs(grid[b, ..., a] - want).max()))
+            o = slice(G, G + na + 1)
+            assert np.array_equal(alone[o, o, :, a], want[o, o, :]), (b, ax)
