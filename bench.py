@@ -650,6 +650,254 @@ def run_e2e_batch(cells, base_id, W_, K, world):
                     "from page-locked host arrays"}
 
 
+# ------------------------------------------------------------------ magnetosphere shells (batched vs plain)
+SHELL_STATE = (("U_H", (0, 0, 0)), ("U_NA", (0, 0, 0)), ("B_XI", (1, 0, 0)), ("B_ETA", (0, 1, 0)),
+               ("B_ZETA", (0, 0, 1)))
+
+
+def _shell_state(get, case, dtype=np.float64):
+    """Owned DOFs of the state fields of every panel, from get(field, lo, hi, block)."""
+    n = (case.na, case.na, case.nr)
+    out = {}
+    for name, st in SHELL_STATE:
+        hi = tuple(n[a] + st[a] for a in range(3))
+        out[name] = np.concatenate([get(name, (0, 0, 0), hi, b).astype(dtype).ravel() for b in range(6)])
+    return out
+
+
+def _shell_descs(cases, ks, topo, precision):
+    from mpcns_mercury_b200.capi import SolveDesc
+
+    return [SolveDesc(c.cells, 4, k, precision=precision, topology=topo.get(c)) for c, k in zip(cases, ks)]
+
+
+def _shell_batch(cases, ks, topo, precision, steps):
+    """A batch holding the cases, set up on the device, prepared, each with
+    ``steps`` steps requested.  Returns (batch, slots)."""
+    from mpcns_mercury_b200 import magnetosphere as M
+    from mpcns_mercury_b200.capi import Batch
+
+    b = Batch(len(cases), precision)
+    descs = _shell_descs(cases, ks, topo, precision)
+    b.reserve(sum(d.device_bytes() for d in descs))
+    slots = []
+    for c, k, d in zip(cases, ks, descs):
+        s = b.add(d)
+        d.close()
+        M.set_up(b, c, slot=s, k=k)
+        b.prepare(s)
+        b.request(s, steps)
+        slots.append(s)
+    return b, slots
+
+
+def _check_batch(b, slots, steps, what):
+    info = b.poll()
+    for s in slots:
+        if info[s].status != 0 or info[s].step != steps:
+            raise RuntimeError(f"{what} slot {s}: status {info[s].status} step {info[s].step}")
+
+
+def run_shells(args, rank, world, device):
+    """The magnetosphere ensemble (64 cubed-sphere shells of uneven sizes and
+    seeded upstream conditions) advanced together by one mixed-precision
+    batch, against the same solves one by one through the plain FP64 path."""
+    import torch
+    from mpcns_mercury_b200 import magnetosphere as M
+
+    nsol = args.solves
+    cases = M.ensemble(nsol, stream=300000 + 1000 * rank)
+    ks = [M.constants(c) for c in cases]
+    cells = [n for c in cases for n in c.cells]
+    ncell = owned_cells(cells)
+    W_, K = args.warmup, args.steps
+    total = W_ + K
+    err_steps = max(total, args.error_steps)
+    topo = M.TopologyCache()
+    t0 = time.perf_counter()
+    for c in cases:  # the grids' sync tables (host, shared by every solve of one grid; not timed)
+        topo.get(c)
+    topo_s = time.perf_counter() - t0
+
+    # 1) the mixed-precision batch: W untimed steps, K timed (state >> L2), on to err_steps
+    mixed, slots = _shell_batch(cases, ks, topo, 1, err_steps)
+    mixed.run(W_)
+    mixed.poll()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    if rank == 0:
+        sampler.start()
+    mixed_ms = _timed_batch_steps(mixed, K, device)
+    clocks = sampler.stop() if rank == 0 else None
+    if err_steps > total:
+        mixed.run(err_steps - total)
+    _check_batch(mixed, slots, err_steps, "mixed batch")
+    # the mixed state is FP32 on the device: kept as float32 on the host, exactly
+    mixed_state = [_shell_state(lambda f, lo, hi, blk: mixed.download(s, f, lo, hi, block=blk), c, np.float32)
+                   for s, c in zip(slots, cases)]
+    for s in slots:
+        mixed.request(s, 3)  # every solve active for the profiled steps
+    prof = _batch_step_profile(mixed, 3)
+    launches = mixed.kernels_per_step()
+    mixed.close()
+    if getattr(args, "batched_only", False):
+        topo.close()
+        return {"metric": METRIC, "value": round(replicas_value(world, ncell, K, mixed_ms), 3), "unit": UNIT,
+                "n_gpus": world, "steps": K, "warmup": W_, "ms_per_step": round(mixed_ms / K, 5),
+                "config": {"workload": "shells", "solves": nsol, "batched_only": True},
+                "kernel_ms": {k: round(v, 5) for k, v in prof.items()}}
+
+    # 2) plain FP64, one solve at a time: W untimed, K timed, on to err_steps
+    plain_ms = []
+    worst = {}
+    sub_bytes, nsub = 0, 0
+    for c, k in zip(cases, ks):  # the FP64 batch's subset: the first solves within 40 GB
+        d = _shell_descs([c], [k], topo, 0)[0]
+        if sub_bytes + d.device_bytes() > 40e9 and nsub > 0:
+            d.close()
+            break
+        sub_bytes += d.device_bytes()
+        nsub += 1
+        d.close()
+    plain_sub = []
+    for i, (c, k) in enumerate(zip(cases, ks)):
+        ctx = M.context(c, precision=0, k=k, topologies=topo)
+        ctx.step(W_)
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.step_async(K)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms.append(e0.elapsed_time(e1))
+        if err_steps > total:
+            ctx.step_async(err_steps - total)
+        ctx.synchronize()
+        info = ctx.info()
+        if info.status != 0 or info.step != err_steps:
+            raise RuntimeError(f"plain FP64 solve {i}: status {info.status} step {info.step}")
+        st = _shell_state(lambda f, lo, hi, blk: ctx.download(f, lo, hi, block=blk), c)
+        for name in st:
+            worst[name] = max(worst.get(name, 0.0), _rel_l2(mixed_state[i][name].astype(np.float64), st[name]))
+        if i < nsub:
+            plain_sub.append(st)
+        ctx.close()
+    del mixed_state
+
+    # 3) the FP64 batch on the subset: its rate, and bitwise equality with the plain path
+    fp64, fslots = _shell_batch(cases[:nsub], ks[:nsub], topo, 0, err_steps)
+    fp64.run(W_)
+    fp64.poll()
+    fp64_ms = _timed_batch_steps(fp64, K, device)
+    if err_steps > total:
+        fp64.run(err_steps - total)
+    _check_batch(fp64, fslots, err_steps, "FP64 batch")
+    fp64_identical = True
+    for i, (s, c) in enumerate(zip(fslots, cases[:nsub])):
+        got = _shell_state(lambda f, lo, hi, blk: fp64.download(s, f, lo, hi, block=blk), c)
+        fp64_identical = fp64_identical and all(np.array_equal(got[n], plain_sub[i][n]) for n in got)
+    fp64.close()
+    del plain_sub
+    sub_cells = sum(c.cell_count() for c in cases[:nsub])
+    if world > 1:
+        mixed_ms, plain_total, fp64_ms, plain_sub_ms = max_over_ranks(
+            [mixed_ms, sum(plain_ms), fp64_ms, sum(plain_ms[:nsub])], device)
+    else:
+        plain_total, plain_sub_ms = sum(plain_ms), sum(plain_ms[:nsub])
+
+    value = replicas_value(world, ncell, K, mixed_ms)
+    plain = replicas_value(world, ncell, K, plain_total)
+    batched64 = replicas_value(world, sub_cells, K, fp64_ms)
+    plain_sub_rate = replicas_value(world, sub_cells, K, plain_sub_ms)
+    peak, peak_kind = load_peaks()
+    roof = roofline(prof, cells, peak, peak_kind, precision=1, traffic_key="k_fluid_mixed_shells")
+    e2e = run_e2e_shells(cases, ks, topo, err_steps, world)
+    topo.close()
+    cpu = cpu_baseline_sample(args) if (rank == 0 and not args.no_cpu_baseline) else None
+    return {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W_,
+        "ms_per_step": round(mixed_ms / K, 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (metric f64)", "data": "synthetic",
+        "config": {"workload": "shells", "solves": nsol, "description":
+                   f"{nsol} magnetosphere solves: 6-panel cubed-sphere shells r in [1, 8] (r geometric), cells per "
+                   "panel axis log-uniform (na in [24,64], nr in [24,128]), H+ and Na+ (mass 1:23) with Na+ "
+                   "fraction U[1e-4,1e-2], centred dipole, upstream |v| U[2,6], n U[0.5,3], IMF Bz U[-0.4,0.4], "
+                   "Hall (radial taper 1.1-1.2) + electron pressure, solid inner wall, farfield outer sphere, "
+                   "CFL 0.4; set up on the device from these parameters; one batch, one CUDA graph launch per "
+                   "step advancing every solve",
+                   "cells_per_replica": ncell, "blocks_per_replica": len(cells),
+                   "precision": "mixed: FP32 state/work/flux/EMF/update, FP64 Jac/JD",
+                   "l2": "inputs larger than L2 (not flushed)", "parallelism": f"replicas x{world}",
+                   "plain_fp64_one_by_one_mcells": round(plain, 3),
+                   "batched_mixed_vs_plain_fp64": round(value / plain, 3),
+                   "batched_fp64_subset": {"solves": nsub, "cells": sub_cells, "mcells": round(batched64, 3),
+                                           "plain_fp64_same_solves_mcells": round(plain_sub_rate, 3),
+                                           "bitwise_equal_plain": bool(fp64_identical)},
+                   "error_vs_fp64_rel_l2_max_over_solves": {k: float(f"{v:.3e}") for k, v in worst.items()},
+                   "error_steps": err_steps, "host_topology_build_s": round(topo_s, 2)},
+        "roofline": roof, "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches * K, "clocks": clocks,
+        "kernel_ms": {k: round(v, 5) for k, v in prof.items()},
+    }
+
+
+def run_e2e_shells(cases, ks, topo, steps, world):
+    """The mixed batch end to end through the C ABI, one wall-clock region:
+    add every solve (its grid's sync tables, built ahead like a grid file),
+    its static fields and background computed on the device from the
+    page-locked node coordinates, the initial state filled on the device,
+    prepare, ``steps`` steps (the configuration's per-solve count), download
+    of every solve's final state."""
+    import torch
+    from mpcns_mercury_b200 import magnetosphere as M
+    from mpcns_mercury_b200.capi import Batch, shell_grid
+
+    pinned = []
+    for c in cases:
+        g = shell_grid(c.na, c.nr, c.r_out, M.NGHOST + 1)
+        t = torch.empty(g.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = g
+        pinned.append(t.numpy())
+    descs = _shell_descs(cases, ks, topo, 1)
+    b = Batch(len(cases), 1)
+    b.reserve(sum(d.device_bytes() for d in descs))
+    torch.cuda.synchronize()
+    h2d = d2h = 0
+    t0 = time.perf_counter()
+    slots = []
+    for c, k, d, nodes in zip(cases, ks, descs, pinned):
+        s = b.add(d)
+        h2d += M.set_up(b, c, slot=s, k=k, nodes=nodes)
+        b.prepare(s)
+        b.request(s, steps)
+        slots.append(s)
+    b.run(steps)
+    info = b.poll()
+    for s, c in zip(slots, cases):
+        st = _shell_state(lambda f, lo, hi, blk: b.download(s, f, lo, hi, block=blk), c)
+        d2h += sum(v.nbytes for v in st.values())
+    t1 = time.perf_counter()
+    for d in descs:
+        d.close()
+    ok = all(info[s].status == 0 and info[s].step == steps for s in slots)
+    b.close()
+    if not ok:
+        raise RuntimeError("e2e batch: a solve did not finish its steps")
+    ncell = sum(c.cell_count() for c in cases)
+    return {"value": round(world * ncell * steps / (t1 - t0) / 1e6, 3), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / steps), "d2h_bytes_per_step": int(d2h / steps),
+            "wall_s": round(t1 - t0, 4), "steps": steps,
+            "what": "one wall-clock region: add of every solve (its grid's sync tables, built on the host ahead "
+                    "like a grid file), static fields and background computed on the device from page-locked "
+                    "node coordinates (mhd_batch_setup_geometry_bg, Sync(Badd)), initial state filled on the "
+                    "device, Sync(U), Sync(B), prepare, the configuration's steps per solve, download of every "
+                    "final state, all through the C ABI"}
+
+
 # ------------------------------------------------------------------ serving
 def run_serving(args, rank, world, device):
     """Poisson request stream served by the continuous-batching server
@@ -792,30 +1040,50 @@ def run_implicit(args, rank, world, device):
 
 # ------------------------------------------------------------------ reference arm
 def reference_members(args):
-    """Cells per axis of every member of ``args.workload``, exactly as our arm
-    runs them (sizes drawn without loading the CUDA library)."""
+    """Every member of ``args.workload`` as the reference harness job that
+    sets it up exactly as our arm runs it, with its owned cells: [(job, cells)].
+    Sizes and upstream conditions are drawn without loading the CUDA library."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mercury_oracle as mo
     from mpcns_mercury_b200 import workloads as W
+
+    def cube(n, sid):
+        job = dict(mo.CUBE_JOB)
+        job.update(n=" ".join(str(int(v)) for v in n), solve_id=sid)
+        return job, int(n[0]) * int(n[1]) * int(n[2])
 
     if args.workload.startswith("cube"):
         n = int(args.workload[4:])
-        return [(n, n, n)]
+        return [cube((n, n, n), 0)]
     if args.workload == "ensemble":
-        return [tuple(c) for c in W.ensemble_sizes(args.solves)]
+        return [cube(c, s) for s, c in enumerate(W.ensemble_sizes(args.solves))]
     if args.workload == "serve":
-        return [tuple(c) for c in W.ensemble_sizes(args.shapes, stream=200000)]
+        return [cube(c, s) for s, c in enumerate(W.ensemble_sizes(args.shapes, stream=200000))]
+    if args.workload == "shells":
+        from mpcns_mercury_b200 import magnetosphere as M
+
+        out = []
+        for c in M.ensemble(args.solves, stream=300000):
+            up = [float(v) for v in c.upstream]
+            job = dict(mo.SHELL_JOB)
+            job.update(na=c.na, nr=c.nr, na_fraction=float(c.na_fraction),
+                       initial_line=" ".join(repr(v) for v in up),
+                       farfield_line=" ".join(repr(v) for v in (up[0], up[1], up[2], up[4], up[5])))
+            out.append((job, c.cell_count()))
+        return out
     raise SystemExit(f"unknown workload {args.workload}")
 
 
-def run_reference_member(cells, warm, steps, solve_id=0):
+def run_reference_member(job, warm, steps):
     """One member on the reference build (one single-rank process): ``warm``
     untimed StepOnce calls, then ``steps`` timed ones.  Returns (seconds per
     timed step, owned cells)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mercury_oracle as mo
 
-    job = dict(mo.CUBE_JOB)
-    job.update(n=" ".join(str(int(v)) for v in cells), steps=warm + steps, time_from=warm, dump_fields="U_H",
-               dump_at=str(warm + steps), solve_id=solve_id)
+    job = dict(job)
+    job.update(steps=warm + steps, time_from=warm, dump_fields="U_H", dump_at=str(warm + steps), dump_grid=0,
+               dump_taper=0, dump_static="")
     d = mo.run_job(job, timeout=3600)
     secs, nsteps, ncell = d[("timing", -1)].data.ravel()
     return float(secs) / max(1.0, float(nsteps)), int(ncell)
@@ -833,18 +1101,18 @@ def reference_sample(members, warm, steps, procs):
     procs = max(1, min(procs, len(members)))
     load = [0] * procs
     parts = [[] for _ in range(procs)]
-    for sid in sorted(range(len(members)), key=lambda q: -(members[q][0] * members[q][1] * members[q][2])):
+    for sid in sorted(range(len(members)), key=lambda q: -members[q][1]):
         w = load.index(min(load))
         parts[w].append(sid)
-        load[w] += members[sid][0] * members[sid][1] * members[sid][2]
+        load[w] += members[sid][1]
 
     def core(part):
-        return sum(run_reference_member(members[sid], warm, steps, solve_id=sid)[0] for sid in part)
+        return sum(run_reference_member(members[sid][0], warm, steps)[0] for sid in part)
 
     with ThreadPoolExecutor(max_workers=procs) as ex:
         per_core = list(ex.map(core, parts))
     step_s = max(per_core)
-    cells = sum(a * b * c for a, b, c in members)
+    cells = sum(m[1] for m in members)
     return cells / step_s / 1e6, step_s, procs
 
 
@@ -861,11 +1129,13 @@ def cpu_baseline_sample(args, cells=None):
     cores = os.cpu_count() or 1
     sample = members[:min(len(members), cores)]
     rate, step_s, procs = reference_sample(sample, 1, 2, cores)
-    one_step_s, one_cells = run_reference_member((32, 32, 32), 1, 5)
+    cube = dict(mo.CUBE_JOB)
+    cube.update(n="32 32 32", solve_id=0)
+    one_step_s, one_cells = run_reference_member(cube, 1, 5)
     return {"value": round(rate, 4), "unit": UNIT, "cores": procs, "kind": "reference",
-            "sample": f"{args.workload}: the first {len(sample)} members at their own shapes, one single-rank "
-                      f"reference process per member (oracle/_ref, built from the reference sources) spread over "
-                      f"{procs} cores, 1 untimed + 2 timed StepOnce calls each, setup excluded",
+            "sample": f"{args.workload}: the first {len(sample)} members at their own shapes and conditions, one "
+                      f"single-rank reference process per member (oracle/_ref, built from the reference sources) "
+                      f"spread over {procs} cores, 1 untimed + 2 timed StepOnce calls each, setup excluded",
             "one_core_cube32": {"value": round(one_cells / one_step_s / 1e6, 4), "unit": UNIT, "cores": 1,
                                 "ms_per_step": round(1e3 * one_step_s, 3),
                                 "sample": "periodic curvilinear 32^3 cube (Orszag-Tang, 2 ion fluids, Hall + p_e), "
@@ -889,12 +1159,12 @@ def run_reference(args, rank, world):
     t0 = time.perf_counter()
     value, step_s, procs = reference_sample(members, 1, steps, cores)
     wall = time.perf_counter() - t0
-    cells = sum(a * b * c for a, b, c in members)
+    cells = sum(m[1] for m in members)
     return {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": 1, "ms_per_step": round(1e3 * step_s, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "members": len(members), "cells_per_replica": cells,
-                       "blocks": [list(c) for c in members], "wall_s": round(wall, 2),
+                       "wall_s": round(wall, 2),
                        "implementation": "reference solver compiled from its own sources (oracle/_ref), one "
                                          f"single-rank process per member, members spread over {procs} cores",
                        "timing": "per member: 1 untimed StepOnce, then the timed ones (setup excluded); a workload "
@@ -911,7 +1181,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="ensemble", help="ensemble (default), serve, implicit, cube32, cubeN")
+    ap.add_argument("--workload", default="shells",
+                    help="shells (default), ensemble, serve, implicit, cube32, cubeN")
     ap.add_argument("--solves", type=int, default=64, help="ensemble: solves per GPU")
     ap.add_argument("--batched-only", action="store_true",
                     help="ensemble: run only the mixed batch (profiling; no plain/FP64 legs, no error check)")
@@ -949,7 +1220,9 @@ def main():
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.workload == "ensemble":
+        if args.workload == "shells":
+            line = run_shells(args, rank, world, device)
+        elif args.workload == "ensemble":
             line = run_ensemble(args, rank, world, device)
         elif args.workload == "serve":
             line = run_serving(args, rank, world, device)

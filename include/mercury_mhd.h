@@ -272,6 +272,11 @@ int mhd_upload_field(mhd_ctx *ctx, int field, int block, const double *data, con
                      const int32_t hi[3], int ncomp);
 int mhd_download_field(mhd_ctx *ctx, int field, int block, double *data, const int32_t lo[3],
                        const int32_t hi[3], int ncomp);
+/* Sets every position of [lo, hi) to values[m] per component m (ncomp <= 36)
+ * on the device: a uniform state without its host array (Common_Initial,
+ * Z4_Mercury/include/2_Initial.h:134-215, sets U and B that way). */
+int mhd_fill_field(mhd_ctx *ctx, int field, int block, const double *values, const int32_t lo[3],
+                   const int32_t hi[3], int ncomp);
 
 /* The preamble of MercurySolver::Advance (Z4_Mercury/src/MercurySolver_Driver.cpp:6-13):
  * UpdateDerivedFields_ on the uploaded state.  Sets time/step. */
@@ -462,6 +467,8 @@ int mhd_batch_upload_field(mhd_batch *batch, int slot, int field, int block, con
                            const int32_t lo[3], const int32_t hi[3], int ncomp);
 int mhd_batch_download_field(mhd_batch *batch, int slot, int field, int block, double *data,
                              const int32_t lo[3], const int32_t hi[3], int ncomp);
+int mhd_batch_fill_field(mhd_batch *batch, int slot, int field, int block, const double *values,
+                         const int32_t lo[3], const int32_t hi[3], int ncomp);
 int mhd_batch_sync(mhd_batch *batch, int slot, int group);
 int mhd_batch_prepare(mhd_batch *batch, int slot, double time, int64_t step);
 /* Sets the slot's request to nsteps more steps (0 parks it). */

@@ -195,7 +195,7 @@ EXPORTS = [
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view", "mhd_shell_nodes", "mhd_shell_grid", "mhd_hall_taper", "mhd_setup_geometry_bg",
-    "mhd_batch_setup_geometry_bg",
+    "mhd_batch_setup_geometry_bg", "mhd_fill_field", "mhd_batch_fill_field",
 ]
 
 _lib = None
@@ -255,6 +255,9 @@ def lib() -> ctypes.CDLL:
     L.mhd_setup_geometry.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_double]
     L.mhd_shell_nodes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
                                   ctypes.c_void_p]
+    L.mhd_fill_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p, ctypes.c_int]
+    L.mhd_batch_fill_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p,
+                                       ctypes.c_int]
     L.mhd_setup_geometry_bg.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
                                         ctypes.POINTER(MhdBackground)]
     L.mhd_batch_setup_geometry_bg.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
@@ -438,10 +441,12 @@ class Context:
     """One device-resident solve behind the C ABI (mhd_ctx)."""
 
     def __init__(self, cells, nghost: int, constants: MhdConstants, topology=None, precision: int = 0,
-                 lattice=None):
+                 lattice=None, keep_topology: bool = False):
         """cells: cells per block; one block is periodic in every direction,
         lattice=(bx, by, bz) makes bx * by * bz equal blocks tile a periodic
-        box (mhd_topology_periodic_lattice)."""
+        box (mhd_topology_periodic_lattice).  topology: a topology handle
+        (mhd_topology_*) the context destroys at close, unless keep_topology
+        (the caller shares it between solves of one grid)."""
         L = lib()
         self._cells = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
         self.desc = MhdDesc()
@@ -451,7 +456,7 @@ class Context:
         self.desc.precision = precision
         self.desc.constants = constants
         self._topo = ctypes.c_void_p()
-        self._owns_topo = topology is None
+        self._owns_topo = topology is None or not keep_topology
         if topology is not None:  # a topology handle (mhd_topology_*) that fills the descriptor's tables
             self._topo = topology
             check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
@@ -472,6 +477,12 @@ class Context:
         a = np.ascontiguousarray(array, dtype=np.float64)
         check(lib().mhd_upload_field(self.ctx, FIELD_ID[field], block, a.ctypes.data_as(ctypes.c_void_p),
                                      _i3(lo), _i3(hi), a.shape[-1]), f"upload {field}")
+
+    def fill(self, field: str, values, lo, hi, block: int = 0):
+        """Every position of [lo, hi) set to values (one per component) on the device."""
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        check(lib().mhd_fill_field(self.ctx, FIELD_ID[field], block, v.ctypes.data, _i3(lo), _i3(hi), v.size),
+              f"fill {field}")
 
     def download(self, field: str, lo, hi, block: int = 0) -> np.ndarray:
         nc, _ = field_info(field)
@@ -551,9 +562,9 @@ class Context:
         if getattr(self, "ctx", None):
             lib().mhd_ctx_destroy(self.ctx)
             self.ctx = None
-        if getattr(self, "_topo", None):
+        if getattr(self, "_topo", None) and getattr(self, "_owns_topo", True):
             lib().mhd_topology_destroy(self._topo)
-            self._topo = None
+        self._topo = None
 
     def __del__(self):
         try:
@@ -565,10 +576,13 @@ class Context:
 class SolveDesc:
     """A solve descriptor (mhd_desc) with the storage it points to kept alive."""
 
-    def __init__(self, cells, nghost: int, constants: MhdConstants, precision: int = 0, lattice=None):
+    def __init__(self, cells, nghost: int, constants: MhdConstants, precision: int = 0, lattice=None, topology=None):
         """cells: cells per block.  One block: periodic in every direction.
         lattice=(bx, by, bz): the blocks (bx * by * bz equal ones, in the
-        order of mhd_topology_periodic_lattice) tile a periodic box."""
+        order of mhd_topology_periodic_lattice) tile a periodic box.
+        topology: a topology handle (mhd_topology_*) whose tables fill the
+        descriptor; the caller keeps it (and may share it between solves of
+        one grid) and destroys it after the solves are added."""
         L = lib()
         self._cells = (ctypes.c_int32 * (3 * len(cells)))(*[int(x) for b in cells for x in b])
         self.desc = MhdDesc()
@@ -578,7 +592,11 @@ class SolveDesc:
         self.desc.precision = precision
         self.desc.constants = constants
         self._topo = ctypes.c_void_p()
-        if lattice is not None:
+        self._owns_topo = topology is None
+        if topology is not None:
+            self._topo = topology
+            check(L.mhd_topology_fill_desc(self._topo, ctypes.byref(self.desc)), "mhd_topology_fill_desc")
+        elif lattice is not None:
             if len(cells) != lattice[0] * lattice[1] * lattice[2] or any(tuple(c) != tuple(cells[0]) for c in cells):
                 raise ValueError("a lattice has bx * by * bz blocks of equal cells")
             check(L.mhd_topology_periodic_lattice(_i3(cells[0]), _i3(lattice), nghost, ctypes.byref(self._topo)),
@@ -593,9 +611,9 @@ class SolveDesc:
         return int(lib().mhd_desc_device_bytes(ctypes.byref(self.desc)))
 
     def close(self):
-        if getattr(self, "_topo", None):
+        if getattr(self, "_topo", None) and getattr(self, "_owns_topo", True):
             lib().mhd_topology_destroy(self._topo)
-            self._topo = None
+        self._topo = None
 
     def __del__(self):
         try:
@@ -632,6 +650,12 @@ class Batch:
         a = np.ascontiguousarray(array, dtype=np.float64)
         check(lib().mhd_batch_upload_field(self.b, slot, FIELD_ID[field], block, a.ctypes.data_as(ctypes.c_void_p),
                                            _i3(lo), _i3(hi), a.shape[-1]), f"upload {field}")
+
+    def fill(self, slot: int, field: str, values, lo, hi, block: int = 0):
+        """Every position of [lo, hi) of a solve set to values on the device (mhd_batch_fill_field)."""
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        check(lib().mhd_batch_fill_field(self.b, slot, FIELD_ID[field], block, v.ctypes.data, _i3(lo), _i3(hi),
+                                         v.size), f"fill {field}")
 
     def download(self, slot: int, field: str, lo, hi, block: int = 0) -> np.ndarray:
         nc, _ = field_info(field)

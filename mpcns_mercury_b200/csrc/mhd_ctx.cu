@@ -87,6 +87,25 @@ __global__ void k_scatter_aos(const double *__restrict__ aos, int lo0, int lo1, 
     }
   }
 }
+// One value per component over a box range (mhd_batch_fill_field).
+struct FillValues {
+  double v[36];
+};
+__global__ void k_fill(FillValues val, int lo0, int lo1, int lo2, int e0, int e1, int e2, int nc,
+                       void *const *__restrict__ dst_comp, int ndst, int64_t si, int64_t sj, int G, int fp32) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t npts = (int64_t)e0 * e1 * e2;
+  if (t >= npts) return;
+  const int k = (int)(t % e2), j = (int)((t / e2) % e1), i = (int)(t / ((int64_t)e1 * e2));
+  const int64_t off = (int64_t)(i + lo0 + G) * si + (int64_t)(j + lo1 + G) * sj + (k + lo2 + G);
+  for (int m = 0; m < nc; ++m)
+    for (int d = 0; d < ndst; ++d) {
+      if (fp32)
+        ((float *)dst_comp[d * nc + m])[off] = (float)val.v[m];
+      else
+        ((double *)dst_comp[d * nc + m])[off] = val.v[m];
+    }
+}
 __global__ void k_gather_aos(double *__restrict__ aos, int lo0, int lo1, int lo2, int e0, int e1, int e2, int nc,
                              void *const *__restrict__ src_comp, int64_t si, int64_t sj, int G, int fp32) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1860,6 +1879,32 @@ int mhd_batch_upload_field(mhd_batch *b, int slot, int field, int block, const d
   return MHD_OK;
 }
 
+int mhd_batch_fill_field(mhd_batch *b, int slot, int field, int block, const double *values, const int32_t lo[3],
+                         const int32_t hi[3], int ncomp) {
+  Solve *S = nullptr;
+  int rc = xfer(b, slot, field, block, lo, hi, ncomp, &S);
+  if (rc) return rc;
+  if (!values || ncomp > 36) return fail(MHD_ERR_ARG, "fill: bad values");
+  FillValues val{};
+  for (int m = 0; m < ncomp; ++m) val.v[m] = values[m];
+  const int e[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+  const size_t npts = (size_t)e[0] * e[1] * e[2];
+  const int c0 = kComp.first[field];
+  const int ndst = c0 < kNumUComps ? 2 : 1;  // U: both buffers, as an upload
+  void *ptrs[72];
+  for (int d = 0; d < ndst; ++d)
+    for (int m = 0; m < ncomp; ++m) ptrs[d * ncomp + m] = S->comp_ptr(block, c0 + m, d);
+  CUDA_TRY(cudaMemcpyAsync(b->comp_ptrs, ptrs, sizeof(void *) * ndst * ncomp, cudaMemcpyHostToDevice, b->stream));
+  const Box &bx = S->boxes[block];
+  k_fill<<<(unsigned)((npts + 255) / 256), 256, 0, b->stream>>>(val, lo[0], lo[1], lo[2], e[0], e[1], e[2], ncomp,
+                                                                b->comp_ptrs, ndst, bx.si, bx.sj, bx.G,
+                                                                S->comp_bytes(c0) == 4);
+  CUDA_TRY(cudaGetLastError());
+  // the pointer table is pageable: staged before the copy returned
+  S->prepared = false;
+  return MHD_OK;
+}
+
 int mhd_batch_download_field(mhd_batch *b, int slot, int field, int block, double *data, const int32_t lo[3],
                              const int32_t hi[3], int ncomp) {
   Solve *S = nullptr;
@@ -2336,6 +2381,12 @@ int mhd_upload_field(mhd_ctx *ctx, int field, int block, const double *data, con
                      int ncomp) {
   if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
   return mhd_batch_upload_field(ctx->batch, 0, field, block, data, lo, hi, ncomp);
+}
+
+int mhd_fill_field(mhd_ctx *ctx, int field, int block, const double *values, const int32_t lo[3], const int32_t hi[3],
+                   int ncomp) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_fill_field(ctx->batch, 0, field, block, values, lo, hi, ncomp);
 }
 
 int mhd_download_field(mhd_ctx *ctx, int field, int block, double *data, const int32_t lo[3], const int32_t hi[3],

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "mercury_mhd.h"
+#include "mhd_topology_impl.h"
 
 // Seeded multiplicative-noise draws of the synthetic workloads: the engine is
 // std::mt19937_64 seeded with `seed`, each uniform formed as (x >> 11) * 2^-53
@@ -146,18 +147,10 @@ extern "C" int mhd_shell_grid(int32_t na, int32_t nr, double r_out, int32_t G, d
     const int rc = mhd_shell_nodes(na, nr, r_out, p, G, out + p * per);
     if (rc) return rc;
   }
-  mhd_topology *t = nullptr;
-  int rc = mhd_topology_cubed_sphere(na, nr, 1, 0, &t);
+  std::vector<mhd_patch> fp;
+  std::vector<mhd_physical_patch> phys;
+  const int rc = mhd::cubed_sphere_patches(na, nr, &fp, &phys);
   if (rc) return rc;
-  const mhd_patch *faces = nullptr;
-  int32_t nf = 0;
-  rc = mhd_topology_patches(t, 0, &faces, &nf);
-  if (rc) {
-    mhd_topology_destroy(t);
-    return rc;
-  }
-  std::vector<mhd_patch> fp(faces, faces + nf);
-  mhd_topology_destroy(t);
   // the face patch of panel p in direction d (+-1, +-2)
   auto face_of = [&](int p, int d) -> const mhd_patch * {
     for (const auto &f : fp)

@@ -38,6 +38,7 @@
 #include "mercury_mhd.h"
 #include "mhd_error.h"
 #include "mhd_layout.cuh"
+#include "mhd_parallel.h"
 #include "mhd_topology_impl.h"
 
 namespace {
@@ -778,6 +779,13 @@ Classes edge_classes(const Grid &G, const Nodes &N) {
     for (int ax = 0; ax < 3; ++ax) {
       const IBox own = G.owned(b, MHD_EDGE_XI + ax);
       Replay::each(own, [&](const int p[3]) {
+        // only an edge on the block's boundary (in a face plane across
+        // another axis) has nodes another block shares; the rest are classes
+        // of one, which are dropped
+        bool on = false;
+        for (int c = 0; c < 3; ++c)
+          if (c != ax && (p[c] == 0 || p[c] == G.n[b][c])) on = true;
+        if (!on) return;
         int q[3] = {p[0], p[1], p[2]};
         q[ax] += 1;
         const NodeKey a = N.rep_of(b, p[0], p[1], p[2]), c = N.rep_of(b, q[0], q[1], q[2]);
@@ -830,6 +838,7 @@ Classes face_classes(const Grid &G, const Nodes &N) {
       const IBox own = G.owned(b, MHD_FACE_XI + ax);
       const int u = ax == 0 ? 1 : 0, w = ax == 2 ? 1 : 2;  // the face's two in-plane axes (corners order)
       Replay::each(own, [&](const int p[3]) {
+        if (p[ax] != 0 && p[ax] != G.n[b][ax]) return;  // an interior face is a class of one
         std::array<NodeKey, 4> c;
         for (int n = 0; n < 4; ++n) {
           int q[3] = {p[0], p[1], p[2]};
@@ -875,6 +884,7 @@ struct GroupTables {
   std::vector<mhd_phys_op> phys;
   std::vector<mhd_copy> halo, owner, stash;
   int n_stash = 0;
+  int n_staging = 0;  // staging slots, numbered from 0
 };
 
 bool in_owned(const Grid &G, const mhd_dof &d) {
@@ -883,27 +893,16 @@ bool in_owned(const Grid &G, const mhd_dof &d) {
   return o.contains(p);
 }
 
-struct DofHash {
-  size_t operator()(const mhd_dof &d) const {
-    return (((size_t)d.field * 1315423911u ^ (size_t)d.block * 2654435761u) ^ ((size_t)d.i * 97531u)) ^
-           ((size_t)d.j * 8191u) ^ ((size_t)d.k * 131071u) ^ ((size_t)d.comp * 524287u);
-  }
-};
-struct DofEq {
-  bool operator()(const mhd_dof &a, const mhd_dof &b) const {
-    return a.field == b.field && a.block == b.block && a.i == b.i && a.j == b.j && a.k == b.k && a.comp == b.comp;
-  }
-};
 
-GroupTables replay_group(const Grid &G, const GroupDef &gd, const Classes &fcls, const Classes &ecls, bool resistive,
-                         int *staging_base) {
+// The group's tables; its staging slots are numbered from 0 (n_staging of
+// them): the caller shifts them past the other groups'.
+GroupTables replay_group(const Grid &G, const GroupDef &gd, const Classes &fcls, const Classes &ecls, bool resistive) {
   Replay R(G, gd);
   // stage 1: physical handlers, then the face halo; stages 2 and 3: the edge
   // and vertex halos (the grid has no physical edge or vertex patches, so the
   // corner defaults do nothing; checked by the caller)
   R.apply_physical(resistive);
   for (int stage = 1; stage <= 3; ++stage) R.halo(stage);
-  std::vector<mhd_copy> owner_copies;
   if (gd.owner) {
     // owner-to-alias copies (Halo::sync_owner_alias_group): alias <- owner
     // times the product of their canonical signs
@@ -923,40 +922,48 @@ GroupTables replay_group(const Grid &G, const GroupDef &gd, const Classes &fcls,
   GroupTables T;
   T.phys = R.phys;
   // every DOF whose value changed: a copy from its source, unless a physical
-  // operation computed it
-  std::vector<mhd_copy> halo;
+  // operation computed it; halo copies as (destination, source) identities
+  const int64_t nsym = R.arrs.empty() ? 0 : R.arrs.back().base + (int64_t)R.arrs.back().v.size();
+  std::vector<char> phys_w(nsym, 0);
+  for (int64_t id : R.phys_written) phys_w[id] = 1;
+  std::vector<int64_t> hdst, hsrc;
+  std::vector<char> hneg;
   for (const auto &a : R.arrs)
     for (int64_t q = 0; q < (int64_t)a.v.size(); ++q) {
       const int64_t v = a.v[q], self = a.base + q;
       if (v == sym(self, false, false)) continue;
       if (v == sym(self, true, false)) continue;  // kept the value its handler computed
       const int64_t sid = sym_id(v);
-      if (!(v & kPhysBit) && R.phys_written.count(sid))
-        throw std::runtime_error("a copy reads a value the physical handlers overwrite");
-      mhd_copy c;
-      c.dst = R.dof_of(self);
-      c.src = R.dof_of(sid);
-      c.sign = (v & kNegBit) ? -1.0 : 1.0;
-      if (c.dst.field == c.src.field && c.dst.block == c.src.block && c.dst.i == c.src.i && c.dst.j == c.src.j &&
-          c.dst.k == c.src.k && c.dst.comp == c.src.comp && c.sign > 0)
-        continue;
-      (in_owned(G, c.dst) ? T.owner : halo).push_back(c);
+      if (!(v & kPhysBit) && phys_w[sid]) throw std::runtime_error("a copy reads a value the physical handlers overwrite");
+      const bool neg = (v & kNegBit) != 0;
+      if (sid == self && !neg) continue;
+      const mhd_dof d = R.dof_of(self);
+      if (in_owned(G, d)) {
+        T.owner.push_back(mhd_copy{d, R.dof_of(sid), neg ? -1.0 : 1.0});
+      } else {
+        hdst.push_back(self);
+        hsrc.push_back(sid);
+        hneg.push_back(neg);
+      }
     }
   // copies whose source the halo phase itself overwrites go through staging
-  std::unordered_set<mhd_dof, DofHash, DofEq> dsts;
-  for (const auto &c : halo) dsts.insert(c.dst);
+  std::vector<char> is_dst(nsym, 0);
+  for (int64_t id : hdst) is_dst[id] = 1;
   std::vector<mhd_copy> unstash;
-  for (const auto &c : halo) {
-    if (!dsts.count(c.src)) {
-      T.halo.push_back(c);
+  int slots = 0;
+  for (size_t t = 0; t < hdst.size(); ++t) {
+    const mhd_dof d = R.dof_of(hdst[t]), src = R.dof_of(hsrc[t]);
+    const double sign = hneg[t] ? -1.0 : 1.0;
+    if (!is_dst[hsrc[t]]) {
+      T.halo.push_back(mhd_copy{d, src, sign});
       continue;
     }
-    const int slot = (*staging_base)++;
-    const mhd_dof st{MHD_STAGING, 0, slot, 0, 0, 0};
-    T.stash.push_back(mhd_copy{st, c.src, 1.0});
-    unstash.push_back(mhd_copy{c.dst, st, c.sign});
+    const mhd_dof st{MHD_STAGING, 0, slots++, 0, 0, 0};
+    T.stash.push_back(mhd_copy{st, src, 1.0});
+    unstash.push_back(mhd_copy{d, st, sign});
   }
   T.n_stash = (int)unstash.size();
+  T.n_staging = slots;
   T.stash.insert(T.stash.end(), unstash.begin(), unstash.end());
   return T;
 }
@@ -1087,10 +1094,31 @@ int build(Grid &G, bool resistive, mhd_topology **out) {
       throw std::runtime_error("physical patches that meet each other (physical corners) are not supported");
     const Nodes N(G);
     const Classes ecls = edge_classes(G, N), fcls = face_classes(G, N);
+    // the groups replayed on the host threads, their staging slots then
+    // numbered group after group
+    std::vector<int> todo;
+    for (int q = 0; q < MHD_NUM_GROUPS; ++q)
+      if (!((q == MHD_SYNC_ERES || q == MHD_SYNC_DB) && !resistive)) todo.push_back(q);  // implicit substep only
+    std::vector<GroupTables> tabs(MHD_NUM_GROUPS);
+    std::vector<std::string> errs(MHD_NUM_GROUPS);
+    mhd::parallel_for((int)todo.size(), [&](int u) {
+      const int q = todo[u];
+      try {
+        tabs[q] = replay_group(G, kGroupDefs[q], fcls, ecls, resistive);
+      } catch (const std::exception &e) {
+        errs[q] = e.what();
+      }
+    });
+    for (const std::string &e : errs)
+      if (!e.empty()) throw std::runtime_error(e);
     int staging = 0;
-    for (int q = 0; q < MHD_NUM_GROUPS; ++q) {
-      if ((q == MHD_SYNC_ERES || q == MHD_SYNC_DB) && !resistive) continue;  // read only by the implicit substep
-      GroupTables T = replay_group(G, kGroupDefs[q], fcls, ecls, resistive, &staging);
+    for (int q : todo) {
+      GroupTables &T = tabs[q];
+      for (mhd_copy &c : T.stash) {
+        if (c.dst.field == MHD_STAGING) c.dst.i += staging;
+        if (c.src.field == MHD_STAGING) c.src.i += staging;
+      }
+      staging += T.n_staging;
       t->halo[q].assign(T.halo);
       t->owner[q].assign(T.owner);
       t->phys[q] = std::move(T.phys);
@@ -1204,10 +1232,10 @@ extern "C" int mhd_topology_multiblock(int32_t n_blocks, const int32_t *cells, i
   return build(G, resistive != 0, out);
 }
 
-extern "C" int mhd_topology_cubed_sphere(int32_t na, int32_t nr, int32_t nghost, int32_t resistive,
-                                         mhd_topology **out) {
-  if (na < 2 || nr < 2 || nghost < 1 || !out)
-    return mhd::set_error(MHD_ERR_ARG, "mhd_topology_cubed_sphere: need na, nr >= 2 and nghost >= 1");
+// The shell's face patches and physical patches (mhd_topology_cubed_sphere).
+int mhd::cubed_sphere_patches(int na, int nr, std::vector<mhd_patch> *faces_out,
+                              std::vector<mhd_physical_patch> *phys_out) {
+  if (na < 2 || nr < 2) return mhd::set_error(MHD_ERR_ARG, "cubed sphere: need na, nr >= 2");
   // panel edges e: 0 i = 0, 1 i = na, 2 j = 0, 3 j = na; partners found by
   // matching the directions of the edge nodes (tangents of the equiangular
   // grid, +-1 exactly at the panel edges)
@@ -1300,6 +1328,19 @@ extern "C" int mhd_topology_cubed_sphere(int32_t na, int32_t nr, int32_t nghost,
       pp.hi[2] = pp.lo[2] + 1;
       phys.push_back(pp);
     }
+  *faces_out = std::move(faces);
+  *phys_out = std::move(phys);
+  return MHD_OK;
+}
+
+extern "C" int mhd_topology_cubed_sphere(int32_t na, int32_t nr, int32_t nghost, int32_t resistive,
+                                         mhd_topology **out) {
+  if (na < 2 || nr < 2 || nghost < 1 || !out)
+    return mhd::set_error(MHD_ERR_ARG, "mhd_topology_cubed_sphere: need na, nr >= 2 and nghost >= 1");
+  std::vector<mhd_patch> faces;
+  std::vector<mhd_physical_patch> phys;
+  const int rc = mhd::cubed_sphere_patches(na, nr, &faces, &phys);
+  if (rc) return rc;
   std::vector<int32_t> cells;
   for (int p = 0; p < 6; ++p) cells.insert(cells.end(), {na, na, nr});
   return mhd_topology_multiblock(6, cells.data(), nghost, (int32_t)faces.size(), faces.data(), (int32_t)phys.size(),

@@ -51,3 +51,9 @@ struct mhd_topology {
   // B face groups' copies (no physical boundary tells them apart)
   bool res_groups_alias = false;
 };
+
+namespace mhd {
+// The 6-panel cubed-sphere shell's face patches (index maps between panels)
+// and physical patches, in the order mhd_topology_cubed_sphere builds from.
+int cubed_sphere_patches(int na, int nr, std::vector<mhd_patch> *faces, std::vector<mhd_physical_patch> *phys);
+}  // namespace mhd

@@ -109,11 +109,30 @@ def initial_state(case: ShellCase, k=None):
 
 def topology(case: ShellCase):
     """The shell's sync tables (mhd_topology_cubed_sphere); the caller owns
-    the handle (Context / Batch.add take it over)."""
+    the handle (a Context takes it over unless keep_topology)."""
     t = ctypes.c_void_p()
     capi.check(capi.lib().mhd_topology_cubed_sphere(case.na, case.nr, NGHOST, int(case.resistive), ctypes.byref(t)),
                "mhd_topology_cubed_sphere")
     return t
+
+
+class TopologyCache:
+    """Topologies shared by the solves of one grid: they depend only on
+    (na, nr, resistive), not on the upstream parameters."""
+
+    def __init__(self):
+        self._t = {}
+
+    def get(self, case: ShellCase):
+        key = (case.na, case.nr, bool(case.resistive))
+        if key not in self._t:
+            self._t[key] = topology(case)
+        return self._t[key]
+
+    def close(self):
+        for t in self._t.values():
+            capi.lib().mhd_topology_destroy(t)
+        self._t = {}
 
 
 def set_up(target, case: ShellCase, slot=None, nodes=None, k=None) -> int:
@@ -139,33 +158,59 @@ def set_up(target, case: ShellCase, slot=None, nodes=None, k=None) -> int:
     n = (case.na, case.na, case.nr)
     lo = (-NGHOST, -NGHOST, -NGHOST)
     hi = tuple(c + NGHOST for c in n)
-    shape = tuple(h - l for h, l in zip(hi, lo))
-    for b in range(6):
-        for name, vec in (("U_H", uh), ("U_NA", un)):
-            a = np.broadcast_to(vec, shape + (5,))
-            if batch:
-                target.upload(slot, name, a, lo, hi, block=b)
-            else:
-                target.upload(name, a, lo, hi, block=b)
-            nbytes += a.size * 8
+    fill = (lambda *a, **kw: target.fill(slot, *a, **kw)) if batch else target.fill
+    for b in range(6):  # uniform values: filled on the device, nothing but 10 numbers sent
+        fill("U_H", uh, lo, hi, block=b)
+        fill("U_NA", un, lo, hi, block=b)
         for ax, fld in enumerate(("B_XI", "B_ETA", "B_ZETA")):
             fhi = list(hi)
             fhi[ax] += 1
-            z = np.zeros(tuple(h - l for h, l in zip(fhi, lo)) + (1,))
-            if batch:
-                target.upload(slot, fld, z, lo, tuple(fhi), block=b)
-            else:
-                target.upload(fld, z, lo, tuple(fhi), block=b)
-            nbytes += z.size * 8
+            fill(fld, [0.0], lo, tuple(fhi), block=b)
+        nbytes += 13 * 8
     sync("UCELL")
     sync("BFACE")
     return nbytes
 
 
-def context(case: ShellCase, precision: int = 0, k=None):
-    """A Context holding the case, set up on the device and prepared."""
+def context(case: ShellCase, precision: int = 0, k=None, topologies: TopologyCache | None = None, nodes=None):
+    """A Context holding the case, set up on the device and prepared
+    (topologies: a cache to take the grid's tables from)."""
     k = k if k is not None else constants(case)
-    ctx = capi.Context(case.cells, NGHOST, k, topology=topology(case), precision=precision)
-    set_up(ctx, case, k=k)
+    if topologies is not None:
+        ctx = capi.Context(case.cells, NGHOST, k, topology=topologies.get(case), precision=precision,
+                           keep_topology=True)
+    else:
+        ctx = capi.Context(case.cells, NGHOST, k, topology=topology(case), precision=precision)
+    set_up(ctx, case, k=k, nodes=nodes)
     ctx.prepare()
     return ctx
+
+
+def ensemble(nsolves: int, stream: int = 300000, resistive: bool = False):
+    """The magnetosphere ensemble: per solve, cells per panel axis drawn
+    log-uniform (na in [24, 64], nr in [24, 128]: blocks of 24^3 to
+    64 x 64 x 128 cells) and the upstream drawn uniform: speed |v| in [2, 6]
+    and density n in [0.5, 3] (units of the REF list's U and n), IMF Bz in
+    [-0.4, 0.4] (units of B_ref), Na+ fraction in [1e-4, 1e-2]; flow along
+    the INITIAL list's axis, T and M of the base upstream.  Seeded draws
+    (mhd_seeded_uniform's generator, solve_id = stream), computed without
+    the CUDA library."""
+    import math
+
+    from .setup import host_uniform_sym
+
+    u = host_uniform_sym(stream, 0.5, 6 * nsolves) + 0.5
+    U_ref, n_ref, B_ref = 4.031e5, 4e7, 1e-9
+    la, ha, hr = math.log(24.0), math.log(64.0), math.log(128.0)
+    out = []
+    for s in range(nsolves):
+        a, b, c, d, e, f = u[6 * s:6 * s + 6]
+        na = int(round(math.exp(la + a * (ha - la))))
+        nr = int(round(math.exp(la + b * (hr - la))))
+        v = 2.0 + 4.0 * c
+        n = 0.5 + 2.5 * d
+        bz = -0.4 + 0.8 * e
+        frac = 1e-4 + (1e-2 - 1e-4) * f
+        up = (v * U_ref, UPSTREAM[1], n * n_ref, UPSTREAM[3], 0.0, 0.0, 0.0, 0.0, bz * B_ref)
+        out.append(ShellCase(na=na, nr=nr, upstream=up, na_fraction=frac, resistive=resistive))
+    return out
