@@ -818,6 +818,17 @@ def run_shells(args, rank, world, device):
     roof = roofline(prof, cells, peak, peak_kind, precision=1, traffic_key="k_fluid_mixed_shells")
     e2e = run_e2e_shells(cases, ks, topo, err_steps, world)
     topo.close()
+    serving = None
+    if args.serve_requests > 0:  # a short request stream of the same physics: p50/p99 beside the throughput
+        sb, sp, _ = serve_shells(args.serve_requests, args.serve_rate, 8, 48, 96, 50, 100, args.serve_requests,
+                                 args.hbm_budget, rank)
+        serving = {"requests": args.serve_requests, "arrival_rate_per_s": args.serve_rate,
+                   "grids": "8 shell sizes, na log-uniform in [24,48], nr in [24,96]; 50-100 steps per request; "
+                            "upstream conditions per request as the ensemble's",
+                   "batched_mixed": _round_stats(sb), "plain_fp64_one_by_one": _round_stats(sp),
+                   "latency_p50_s": round(sb["latency_p50_s"], 4), "latency_p99_s": round(sb["latency_p99_s"], 4),
+                   "throughput_batched_vs_one_by_one": round(sb["mcell_updates_per_s"] / sp["mcell_updates_per_s"],
+                                                             3)}
     cpu = cpu_baseline_sample(args) if (rank == 0 and not args.no_cpu_baseline) else None
     return {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W_,
@@ -841,7 +852,9 @@ def run_shells(args, rank, world, device):
                    "error_vs_fp64_rel_l2_max_over_solves": {k: float(f"{v:.3e}") for k, v in worst.items()},
                    "error_steps": err_steps, "host_topology_build_s": round(topo_s, 2)},
         "roofline": roof, "cpu_baseline": cpu,
-        "e2e": e2e,
+        "e2e": e2e, "serving": serving,
+        "latency_p50_s": serving["latency_p50_s"] if serving else None,
+        "latency_p99_s": serving["latency_p99_s"] if serving else None,
         "gpu_launches": launches * K, "clocks": clocks,
         "kernel_ms": {k: round(v, 5) for k, v in prof.items()},
     }
@@ -943,6 +956,62 @@ def run_serving(args, rank, world, device):
                 "what": "wall clock of the whole request loop, uploads and downloads included"},
     }
     return line
+
+
+def serve_shells(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, capacity, hbm_budget, rank):
+    """A Poisson stream of magnetosphere requests served by the
+    continuous-batching server (mixed precision) and one by one through the
+    plain FP64 path (one context per grid, each request's fields set up on
+    the device).  Returns (batched stats, plain stats, requests)."""
+    from mpcns_mercury_b200 import capi
+    from mpcns_mercury_b200 import magnetosphere as M
+    from mpcns_mercury_b200 import serving as SV
+
+    stream = M.request_stream(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, stream=500000 + 1000 * rank)
+    reqs = [SV.Request(rid=q, arrival_s=t, cells=None, steps=st, fields={}, case=c)
+            for q, (t, c, st) in enumerate(stream)]
+    # the grids' tables and nodes, prepared ahead for both (host setup, like grid files read ahead)
+    topo, nodes = M.TopologyCache(), {}
+    for r in reqs:
+        topo.get(r.case)
+        key = ("shell", r.case.na, r.case.nr, bool(r.case.resistive))
+        if key not in nodes:
+            nodes[key] = capi.shell_grid(r.case.na, r.case.nr, r.case.r_out, M.NGHOST + 1)
+    srv = SV.Server(capacity=capacity, precision=1, hbm_budget=hbm_budget, max_grids=shapes, topologies=topo,
+                    nodes=nodes)
+    batched = srv.serve(reqs)
+    srv.close()
+    for r in reqs:
+        r.done_s = float("nan")
+    plain = SV.serve_one_by_one(reqs, precision=0, topologies=topo, nodes=nodes)
+    topo.close()
+    return batched, plain, reqs
+
+
+def run_serving_shells(args, rank, world, device):
+    """The serving configuration on magnetosphere requests: a seeded Poisson
+    stream (``--requests``, ``--rate``), sizes log-uniform up to
+    6 x 96 x 96 x 192 from ``--shapes`` grids, 50-500 steps each, served by the
+    continuous-batching server (mixed) and one by one (plain FP64)."""
+    sb, sp, reqs = serve_shells(args.requests, args.rate, args.shapes, 96, 192, 50, 500, args.capacity,
+                                args.hbm_budget, rank)
+    return {
+        "metric": METRIC, "value": round(sb["mcell_updates_per_s"] * world, 3), "unit": UNIT, "n_gpus": world,
+        "steps": int(sum(r.steps for r in reqs)), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (metric f64)", "data": "synthetic",
+        "config": {"workload": "serve-shells", "requests": args.requests, "arrival_rate_per_s": args.rate,
+                   "grids": args.shapes, "capacity": args.capacity, "hbm_budget_bytes": args.hbm_budget,
+                   "batched_mixed": _round_stats(sb), "plain_fp64_one_by_one": _round_stats(sp)},
+        "latency_p50_s": round(sb["latency_p50_s"], 4), "latency_p99_s": round(sb["latency_p99_s"], 4),
+        "roofline": None, "cpu_baseline": None,
+        "e2e": {"value": round(sb["mcell_updates_per_s"] * world, 3), "unit": UNIT,
+                "what": "wall clock of the whole request loop: per request its fields set up on the device from "
+                        "its parameters, its steps, its slot freed"},
+    }
+
+
+def _round_stats(d):
+    return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in d.items()}
 
 
 # ------------------------------------------------------------------ implicit substep
@@ -1198,6 +1267,9 @@ def main():
                     help="ensemble: steps after which the mixed batch's error against FP64 is stated")
     ap.add_argument("--ref-steps", type=int, default=5, help="reference arm: timed steps per member (at most --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=32,
+                    help="shells: requests of the serving leg (p50/p99; 0 leaves it out)")
+    ap.add_argument("--serve-rate", type=float, default=40.0, help="shells: their mean arrivals per second")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -1228,6 +1300,8 @@ def main():
             line = run_ensemble(args, rank, world, device)
         elif args.workload == "serve":
             line = run_serving(args, rank, world, device)
+        elif args.workload == "serve-shells":
+            line = run_serving_shells(args, rank, world, device)
         elif args.workload == "implicit":
             line = run_implicit(args, rank, world, device)
         else:

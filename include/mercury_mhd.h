@@ -277,6 +277,8 @@ int mhd_download_field(mhd_ctx *ctx, int field, int block, double *data, const i
  * Z4_Mercury/include/2_Initial.h:134-215, sets U and B that way). */
 int mhd_fill_field(mhd_ctx *ctx, int field, int block, const double *values, const int32_t lo[3],
                    const int32_t hi[3], int ncomp);
+/* mhd_batch_set_constants of the context's solve. */
+int mhd_set_constants(mhd_ctx *ctx, const mhd_constants *constants);
 
 /* The preamble of MercurySolver::Advance (Z4_Mercury/src/MercurySolver_Driver.cpp:6-13):
  * UpdateDerivedFields_ on the uploaded state.  Sets time/step. */
@@ -469,6 +471,11 @@ int mhd_batch_download_field(mhd_batch *batch, int slot, int field, int block, d
                              const int32_t lo[3], const int32_t hi[3], int ncomp);
 int mhd_batch_fill_field(mhd_batch *batch, int slot, int field, int block, const double *values,
                          const int32_t lo[3], const int32_t hi[3], int ncomp);
+/* Replaces a solve's constants (a new upstream state on the same grid: the
+ * parameter lists calc_physical_constant and BuildMercuryBackgroundState read,
+ * Z4_Mercury/src/physics/MercurySolver_Tools.cpp:3-48); the implicit substep's
+ * presence must not change.  mhd_batch_prepare must follow. */
+int mhd_batch_set_constants(mhd_batch *batch, int slot, const mhd_constants *constants);
 int mhd_batch_sync(mhd_batch *batch, int slot, int group);
 int mhd_batch_prepare(mhd_batch *batch, int slot, double time, int64_t step);
 /* Sets the slot's request to nsteps more steps (0 parks it). */

@@ -195,7 +195,8 @@ EXPORTS = [
     "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view", "mhd_shell_nodes", "mhd_shell_grid", "mhd_hall_taper", "mhd_setup_geometry_bg",
-    "mhd_batch_setup_geometry_bg", "mhd_fill_field", "mhd_batch_fill_field",
+    "mhd_batch_setup_geometry_bg", "mhd_fill_field", "mhd_batch_fill_field", "mhd_set_constants",
+    "mhd_batch_set_constants",
 ]
 
 _lib = None
@@ -255,6 +256,8 @@ def lib() -> ctypes.CDLL:
     L.mhd_setup_geometry.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_double]
     L.mhd_shell_nodes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
                                   ctypes.c_void_p]
+    L.mhd_set_constants.argtypes = [P, ctypes.POINTER(MhdConstants)]
+    L.mhd_batch_set_constants.argtypes = [P, ctypes.c_int, ctypes.POINTER(MhdConstants)]
     L.mhd_fill_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p, ctypes.c_int]
     L.mhd_batch_fill_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p,
                                        ctypes.c_int]
@@ -477,6 +480,11 @@ class Context:
         a = np.ascontiguousarray(array, dtype=np.float64)
         check(lib().mhd_upload_field(self.ctx, FIELD_ID[field], block, a.ctypes.data_as(ctypes.c_void_p),
                                      _i3(lo), _i3(hi), a.shape[-1]), f"upload {field}")
+
+    def set_constants(self, constants: MhdConstants):
+        """A new upstream state on the same grid (mhd_set_constants); prepare must follow."""
+        self.constants = constants
+        check(lib().mhd_set_constants(self.ctx, ctypes.byref(constants)), "mhd_set_constants")
 
     def fill(self, field: str, values, lo, hi, block: int = 0):
         """Every position of [lo, hi) set to values (one per component) on the device."""

@@ -1828,6 +1828,22 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   return MHD_OK;
 }
 
+int mhd_batch_set_constants(mhd_batch *b, int slot, const mhd_constants *constants) {
+  int rc = slot_check(b, slot);
+  if (rc) return rc;
+  if (!constants) return fail(MHD_ERR_ARG, "mhd_batch_set_constants: null constants");
+  Solve *S = b->slots[slot];
+  if ((constants->resistive != 0) != (S->consts.resistive != 0))
+    return fail(MHD_ERR_ARG, "mhd_batch_set_constants: the implicit resistive substep cannot be switched");
+  S->consts = make_consts(*constants, S->nghost);
+  S->res_rtol = constants->res_rtol;
+  S->res_max_it = constants->res_max_it;
+  S->prepared = false;
+  if ((rc = publish(b))) return rc;
+  if (S->shadow_slot >= 0 && b->shadow) return mhd_batch_set_constants(b->shadow, S->shadow_slot, constants);
+  return MHD_OK;
+}
+
 int mhd_batch_remove(mhd_batch *b, int slot) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
@@ -2381,6 +2397,11 @@ int mhd_upload_field(mhd_ctx *ctx, int field, int block, const double *data, con
                      int ncomp) {
   if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
   return mhd_batch_upload_field(ctx->batch, 0, field, block, data, lo, hi, ncomp);
+}
+
+int mhd_set_constants(mhd_ctx *ctx, const mhd_constants *constants) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_set_constants(ctx->batch, 0, constants);
 }
 
 int mhd_fill_field(mhd_ctx *ctx, int field, int block, const double *values, const int32_t lo[3], const int32_t hi[3],

@@ -552,9 +552,9 @@ __device__ __forceinline__ void rusanov(const V<R> &B, R g, int u0, int pv0, R k
 // shared memory (a face's flux has the same inputs and operation order for
 // both cells that share it), then every cell accumulates
 // r[m] -= (F+ - F-) / J, the per-component order of Scheme_U_'s divergence.
-constexpr int cmax3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b > c ? b : c); }
-constexpr int kMaxFaces = cmax3((kTileI + 1) * kTileJ * kTileK, kTileI * (kTileJ + 1) * kTileK,
-                                kTileI * kTileJ * (kTileK + 1));
+constexpr int kNF0 = (kTileI + 1) * kTileJ * kTileK, kNF1 = kTileI * (kTileJ + 1) * kTileK,
+              kNF2 = kTileI * kTileJ * (kTileK + 1);
+constexpr int kTileFaces = kNF0 + kNF1 + kNF2;  // the tile's faces of all three directions
 // Minimum resident CTAs per SM asked of the compiler for the two
 // register-heavy kernels (caps registers at 65536 / (256 * n)).
 #ifndef MHD_MIN_CTAS_FLUID
@@ -562,10 +562,10 @@ constexpr int kMaxFaces = cmax3((kTileI + 1) * kTileJ * kTileK, kTileI * (kTileJ
 #endif
 #ifndef MHD_MIN_CTAS_PV
 #define MHD_MIN_CTAS_PV 4
-#endif  // largest per-direction face count of a tile
+#endif
 template <class R>
 __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir D) {
-  __shared__ R F[5][kMaxFaces];
+  __shared__ R F[5][kTileFaces];
   for_items<R, kCells2>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     const ConstsT<R> &c = consts_of<R>(S);
     const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
@@ -613,53 +613,59 @@ __global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir 
       if constexpr (sizeof(R) == 4) invJ = AT(cFM + 9, i, j, k);  // R(1) / R(Jac), from k_face_normals
       else invJ = R(1.0) / R(ATM(cJAC, i, j, k));
     }
-    // one pass per direction (unrolled: the face grid's extents are constants)
-    auto face_pass = [&](auto dirc) {
-      constexpr int dir = decltype(dirc)::value;
+    // The tile's face fluxes of all three directions in one pass (faces
+    // dealt round-robin over the threads: 912 faces of a 16 x 4 x 4 tile take
+    // four rounds of 256), then every cell takes its six faces' differences
+    // direction by direction, in Scheme_U_'s order.
+#pragma unroll 1
+    for (int gf = tid; gf < kTileFaces; gf += kTileThreads) {
+      const int dir = gf < kNF0 ? 0 : gf < kNF0 + kNF1 ? 1 : 2;
+      const int f = gf - (dir == 0 ? 0 : dir == 1 ? kNF0 : kNF0 + kNF1);
+      const int ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
       // the face's JD: FP32 reads the real-typed copy (k_face_normals), FP64
       // the metric itself (the same values; faster there)
-      constexpr int cm = sizeof(R) == 4 ? cFM + 3 * dir : dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
-      constexpr int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
-      constexpr int ei = kTileI + (dir == 0), ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
-      constexpr int nf = ei * ej * ek;
-#pragma unroll 1
-      for (int f = tid; f < nf; f += kTileThreads) {
-        const int fk = f % ek, fj = (f / ek) % ej, fi = f / (ek * ej);
-        const int x[3] = {it.o[0] + fi, it.o[1] + fj, it.o[2] + fk};
-        bool need = dt_ok;
+      const int cm = sizeof(R) == 4 ? cFM + 3 * dir : dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
+      const int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
+      const int fk = f % ek, fj = (f / ek) % ej, fi = f / (ek * ej);
+      const int x[3] = {it.o[0] + fi, it.o[1] + fj, it.o[2] + fk};
+      bool need = dt_ok;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) need = need && x[a] >= it.lo[a] && x[a] < it.hi[a] + (a == dir);
-        if (need) {
-          int im = x[0], jm = x[1], km = x[2];
-          shift1(dir, im, jm, km, -1);
-          R Fl[5];
-          R k1, k2, k3;
-          if constexpr (sizeof(R) == 4) {
-            k1 = AT(cm, x[0], x[1], x[2]);
-            k2 = AT(cm + 1, x[0], x[1], x[2]);
-            k3 = AT(cm + 2, x[0], x[1], x[2]);
-          } else {
-            k1 = ATM(cm, x[0], x[1], x[2]);
-            k2 = ATM(cm + 1, x[0], x[1], x[2]);
-            k3 = ATM(cm + 2, x[0], x[1], x[2]);
-          }
-          rusanov(B, g, u0, pv0, k1, k2, k3, AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
-#pragma unroll
-          for (int m = 0; m < 5; ++m) F[m][f] = Fl[m];
+      for (int a = 0; a < 3; ++a) need = need && x[a] >= it.lo[a] && x[a] < it.hi[a] + (a == dir);
+      if (need) {
+        int im = x[0], jm = x[1], km = x[2];
+        shift1(dir, im, jm, km, -1);
+        R Fl[5];
+        R k1, k2, k3;
+        if constexpr (sizeof(R) == 4) {
+          k1 = AT(cm, x[0], x[1], x[2]);
+          k2 = AT(cm + 1, x[0], x[1], x[2]);
+          k3 = AT(cm + 2, x[0], x[1], x[2]);
+        } else {
+          k1 = ATM(cm, x[0], x[1], x[2]);
+          k2 = ATM(cm + 1, x[0], x[1], x[2]);
+          k3 = ATM(cm + 2, x[0], x[1], x[2]);
         }
+        rusanov(B, g, u0, pv0, k1, k2, k3, AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) F[m][gf] = Fl[m];
       }
-      __syncthreads();
-      if (it.in && dt_ok) {
-        const int fm = (li * ej + lj) * ek + lk;
+    }
+    __syncthreads();
+    if (it.in && dt_ok) {
+      auto take = [&](auto dirc) {
+        constexpr int dir = decltype(dirc)::value;
+        constexpr int base = dir == 0 ? 0 : dir == 1 ? kNF0 : kNF0 + kNF1;
+        constexpr int ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
+        const int fm = base + (li * ej + lj) * ek + lk;
         const int fp = fm + (dir == 0 ? ej * ek : dir == 1 ? ek : 1);
 #pragma unroll
         for (int m = 0; m < 5; ++m) r[m] -= (F[m][fp] - F[m][fm]) * invJ;
-      }
-      __syncthreads();
-    };
-    face_pass(std::integral_constant<int, 0>{});
-    face_pass(std::integral_constant<int, 1>{});
-    face_pass(std::integral_constant<int, 2>{});
+      };
+      take(std::integral_constant<int, 0>{});
+      take(std::integral_constant<int, 1>{});
+      take(std::integral_constant<int, 2>{});
+    }
+    __syncthreads();  // F is rewritten by the next tile
     if (!it.in || !dt_ok) return;
     // sources (FluidRHS.cpp:206-527)
     const R Tn0 = R(1000.0), sk1 = R(5.0e-5), sk2 = R(1.0e-5);
@@ -1645,8 +1651,14 @@ template <class R>
 __global__ void __launch_bounds__(256) k_phys(Dir D, int which) {
   const int *pre = D.phys_prefix[which];
   const int total = pre[D.nsolves];
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
-    const int s = find_solve(pre, D.nsolves, e);
+  // the CTA takes chunks of kChunk consecutive operations (one solve lookup
+  // per chunk; a thread's solve is found by stepping forward from it)
+  constexpr int kChunk = 2048;
+  for (int c0 = blockIdx.x * kChunk; c0 < total; c0 += gridDim.x * kChunk) {
+  const int s0 = find_solve(pre, D.nsolves, c0);
+  for (int e = c0 + (int)threadIdx.x; e < c0 + kChunk && e < total; e += blockDim.x) {
+    int s = s0;
+    while (s + 1 < D.nsolves && pre[s + 1] <= e) ++s;
     if (!solve_active(D, s)) continue;
     const DevSolve &S = D.solves[s];
     const DevPhys &P = S.phys[which];
@@ -1693,6 +1705,7 @@ __global__ void __launch_bounds__(256) k_phys(Dir D, int which) {
               d2 = *at_code<R>(S, cur, op.src + 2 * op.cstride);
       *at_code<R>(S, cur, op.dst) = E0 * d0 + E1 * d1 + E2 * d2;
     }
+  }
   }
 }
 
@@ -2016,9 +2029,10 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
     case SK_PHYS: k_phys<R><<<G, 256, 0, st>>>(D, iarg); break;
-    case SK_SING_SETUP: k_sing_setup<R><<<8, 64, 0, st>>>(D); break;
-    case SK_SING_EMF: k_sing_emf<R><<<8, 64, 0, st>>>(D); break;
-    case SK_SING_J: k_sing_j<R><<<8, 64, 0, st>>>(D); break;
+    // one thread per singular edge (8 radial lines of nr edges per shell)
+    case SK_SING_SETUP: k_sing_setup<R><<<g_grid_tiles / 2, 64, 0, st>>>(D); break;
+    case SK_SING_EMF: k_sing_emf<R><<<g_grid_tiles / 2, 64, 0, st>>>(D); break;
+    case SK_SING_J: k_sing_j<R><<<g_grid_tiles / 2, 64, 0, st>>>(D); break;
     case SK_RES_CLEARB: k_res_clearb<R><<<G, kTileThreads, 0, st>>>(D); break;
     default: break;
   }

@@ -214,3 +214,33 @@ def ensemble(nsolves: int, stream: int = 300000, resistive: bool = False):
         up = (v * U_ref, UPSTREAM[1], n * n_ref, UPSTREAM[3], 0.0, 0.0, 0.0, 0.0, bz * B_ref)
         out.append(ShellCase(na=na, nr=nr, upstream=up, na_fraction=frac, resistive=resistive))
     return out
+
+
+def request_stream(nreq: int, rate: float, shapes: int = 16, na_max: int = 96, nr_max: int = 192,
+                   steps_min: int = 50, steps_max: int = 500, stream: int = 500000):
+    """A seeded Poisson stream of magnetosphere requests: [(arrival_s,
+    ShellCase, steps)].  The grids come from a pool of ``shapes`` sizes drawn
+    log-uniform (na in [24, na_max], nr in [24, nr_max]); each request has
+    its own upstream conditions (the ensemble's ranges), exponential
+    inter-arrival times of mean 1 / rate and steps uniform in
+    [steps_min, steps_max]."""
+    import math
+
+    from .setup import host_uniform_sym
+
+    u = host_uniform_sym(stream, 0.5, 2 * shapes + 7 * nreq) + 0.5
+    la = math.log(24.0)
+    grid = [(int(round(math.exp(la + u[2 * g] * (math.log(na_max) - la)))),
+             int(round(math.exp(la + u[2 * g + 1] * (math.log(nr_max) - la))))) for g in range(shapes)]
+    U_ref, n_ref, B_ref = 4.031e5, 4e7, 1e-9
+    out, t = [], 0.0
+    for q in range(nreq):
+        a, b, c, d, e, f, h = u[2 * shapes + 7 * q:2 * shapes + 7 * q + 7]
+        t += -math.log(1.0 - a) / rate
+        na, nr = grid[min(int(b * shapes), shapes - 1)]
+        up = (float((2.0 + 4.0 * c) * U_ref), UPSTREAM[1], float((0.5 + 2.5 * d) * n_ref), UPSTREAM[3], 0.0, 0.0,
+              0.0, 0.0, float((-0.4 + 0.8 * e) * B_ref))
+        case = ShellCase(na=na, nr=nr, upstream=up, na_fraction=float(1e-4 + (1e-2 - 1e-4) * f))
+        steps = steps_min + min(int(h * (steps_max - steps_min + 1)), steps_max - steps_min)
+        out.append((t, case, steps))
+    return out

@@ -31,6 +31,8 @@ class Request:
                               # block's "nodes" (statics computed on the device) + initial state
     keep_result: bool = False
     geometry: object = None   # requests with equal keys share their grid and static fields (default: cells)
+    case: object = None       # a magnetosphere.ShellCase: the solve is that shell, set up on the device
+                              # from its parameters (cells and fields unused)
     # filled in by the server
     admitted_s: float = float("nan")
     done_s: float = float("nan")
@@ -43,7 +45,24 @@ def percentile(values, q):
 
 
 def _geometry_key(req: Request):
+    if req.case is not None:
+        return ("shell", req.case.na, req.case.nr, bool(req.case.resistive))
     return req.geometry if req.geometry is not None else tuple(req.cells)
+
+
+def _cell_count(req: Request) -> int:
+    return req.case.cell_count() if req.case is not None else int(np.prod(req.cells))
+
+
+def _shell_result(get, case):
+    """Owned state of every panel of a shell, from get(field, lo, hi, block)."""
+    n = (case.na, case.na, case.nr)
+    out = {}
+    for name, st in (("U_H", (0, 0, 0)), ("U_NA", (0, 0, 0)), ("B_XI", (1, 0, 0)), ("B_ETA", (0, 1, 0)),
+                     ("B_ZETA", (0, 0, 1))):
+        hi = tuple(n[a] + st[a] for a in range(3))
+        out[name] = [get(name, (0, 0, 0), hi, b) for b in range(6)]
+    return out
 
 
 def _upload_state(upload, fields):
@@ -61,7 +80,9 @@ class Server:
     static fields copied on the device) and uploads only its state."""
 
     def __init__(self, capacity: int = 64, precision: int = 1, hbm_budget: float = 100e9, chunk_steps: int = 8,
-                 cfl: float = 0.4, max_grids: int = 16):
+                 cfl: float = 0.4, max_grids: int = 16, topologies=None, nodes=None):
+        """topologies, nodes: a magnetosphere.TopologyCache and a dict of grid
+        nodes to take shell grids from (the caller's, kept open)."""
         self.batch = capi.Batch(capacity + max_grids, precision)
         self.capacity = capacity
         self.max_grids = max_grids
@@ -71,9 +92,24 @@ class Server:
         self.constants = reference_constants(cfl=cfl)
         self.templates = {}     # geometry key -> template slot
         self.grid_bytes = {}    # geometry key -> device bytes of one solve
+        self.topologies = topologies  # shells: their grids' sync tables
+        self._own_topologies = topologies is None
+        self.nodes = nodes if nodes is not None else {}  # shells: their grids' node coordinates
 
     def close(self):
         self.batch.close()
+        if self.topologies is not None and self._own_topologies:
+            self.topologies.close()
+
+    def _shell_grid(self, case):
+        from . import magnetosphere as M
+
+        if self.topologies is None:
+            self.topologies = M.TopologyCache()
+        key = ("shell", case.na, case.nr, bool(case.resistive))
+        if key not in self.nodes:
+            self.nodes[key] = capi.shell_grid(case.na, case.nr, case.r_out, NGHOST + 1)
+        return self.topologies.get(case), self.nodes[key]
 
     # ------------------------------------------------------------------ one solve
     def _template(self, req: Request) -> int:
@@ -81,6 +117,15 @@ class Server:
         if key not in self.templates:
             if len(self.templates) >= self.max_grids:
                 raise RuntimeError(f"more than {self.max_grids} distinct grids")
+            if req.case is not None:  # a shell grid: its tables (every request sets its own fields up)
+                from . import magnetosphere as M
+
+                topo, _ = self._shell_grid(req.case)
+                d = capi.SolveDesc(req.case.cells, NGHOST, M.constants(req.case), precision=self.precision,
+                                   topology=topo)
+                self.templates[key] = self.batch.add(d)
+                d.close()
+                return self.templates[key]
             slot = self.batch.add_periodic(req.cells, NGHOST, self.constants)
             upload_request(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b),
                            lambda nodes: self.batch.setup_geometry(slot, nodes), req.fields)
@@ -88,6 +133,17 @@ class Server:
         return self.templates[key]
 
     def _admit(self, req: Request) -> int:
+        if req.case is not None:
+            from . import magnetosphere as M
+
+            k = M.constants(req.case)
+            slot = self.batch.add_like(self._template(req), constants=k, copy_static=False)
+            _, nodes = self._shell_grid(req.case)
+            M.set_up(self.batch, req.case, slot=slot, k=k, nodes=nodes)
+            self.batch.prepare(slot)
+            self.batch.request(slot, req.steps)
+            req.slot = slot
+            return slot
         slot = self.batch.add_like(self._template(req), copy_static=True)
         _upload_state(lambda f, a, lo, hi, b: self.batch.upload(slot, f, a, lo, hi, block=b), req.fields)
         self.batch.sync(slot, "UCELL")
@@ -98,14 +154,22 @@ class Server:
         return slot
 
     def _retire(self, req: Request):
-        if req.keep_result:
+        if req.keep_result and req.case is not None:
+            req.result = _shell_result(lambda f, lo, hi, b: self.batch.download(req.slot, f, lo, hi, block=b),
+                                       req.case)
+        elif req.keep_result:
             req.result = {name: self.batch.download(req.slot, capi_field(name), req.fields[name].lo,
                                                     req.fields[name].hi) for name in STATE_FIELDS}
         self.batch.remove(req.slot)
 
-    @staticmethod
-    def _bytes(req: Request, precision: int) -> int:
-        d = capi.SolveDesc([req.cells], NGHOST, reference_constants(), precision=precision)
+    def _bytes(self, req: Request, precision: int) -> int:
+        if req.case is not None:
+            from . import magnetosphere as M
+
+            topo, _ = self._shell_grid(req.case)
+            d = capi.SolveDesc(req.case.cells, NGHOST, M.constants(req.case), precision=precision, topology=topo)
+        else:
+            d = capi.SolveDesc([req.cells], NGHOST, reference_constants(), precision=precision)
         b = d.device_bytes()
         d.close()
         return b
@@ -184,20 +248,27 @@ class Server:
         self.batch.poll()
         makespan = clock() - t0
         lat = [r.done_s - r.arrival_s for r in pending]
-        work = sum(int(np.prod(r.cells)) * r.steps for r in pending)
+        work = sum(_cell_count(r) * r.steps for r in pending)
         return {"requests": len(pending), "makespan_s": makespan, "graph_steps": graph_steps,
                 "cell_updates": work, "mcell_updates_per_s": work / makespan / 1e6,
                 "latency_p50_s": percentile(lat, 50), "latency_p99_s": percentile(lat, 99),
                 "latency_mean_s": float(np.mean(lat)) if lat else float("nan")}
 
 
-def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl: float = 0.4):
+def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl: float = 0.4, topologies=None,
+                     nodes=None):
     """The same requests served first-come first-served through the plain
     single-solve path (mhd_ctx, one solve on the GPU at a time).  Like the
     server, it keeps one context per grid (tables and static fields uploaded
-    once) and uploads each request's state."""
+    once) and uploads each request's state; a shell request sets its fields
+    up on its grid's context (topologies / nodes: shell grids prepared
+    ahead, as for the server)."""
     pending = sorted(requests, key=lambda r: r.arrival_s)
     ctxs = {}
+    shells = dict(nodes or {})  # shell grids: nodes per grid, and "topo": the topology cache
+    own_topo = topologies is None
+    if topologies is not None:
+        shells["topo"] = topologies
     t0 = clock()
     for r in pending:
         now = clock() - t0
@@ -206,6 +277,29 @@ def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl:
         r.admitted_s = clock() - t0
         key = _geometry_key(r)
         ctx = ctxs.get(key)
+        if r.case is not None:  # a shell: one context per grid, every request sets its own fields up
+            from . import magnetosphere as M
+
+            if "topo" not in shells:
+                shells["topo"] = M.TopologyCache()
+            k = M.constants(r.case)
+            if key not in shells:
+                shells[key] = capi.shell_grid(r.case.na, r.case.nr, r.case.r_out, NGHOST + 1)
+            if ctx is not None and ctx.info().status != 0:
+                ctx.close()
+                ctx = None
+            if ctx is None:
+                ctx = capi.Context(r.case.cells, NGHOST, k, topology=shells["topo"].get(r.case), precision=precision,
+                                   keep_topology=True)
+                ctxs[key] = ctx
+            ctx.set_constants(k)
+            M.set_up(ctx, r.case, k=k, nodes=shells[key])
+            ctx.prepare()
+            ctx.step(r.steps)
+            if r.keep_result:
+                r.result = _shell_result(lambda f, lo, hi, b: ctx.download(f, lo, hi, block=b), r.case)
+            r.done_s = clock() - t0
+            continue
         if ctx is None:
             ctx = capi.Context([r.cells], NGHOST, reference_constants(cfl=cfl), precision=precision)
             upload_request(lambda f, a, lo, hi, b: ctx.upload(f, a, lo, hi, block=b), ctx.setup_geometry, r.fields)
@@ -223,8 +317,10 @@ def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl:
     makespan = clock() - t0
     for ctx in ctxs.values():
         ctx.close()
+    if "topo" in shells and own_topo:
+        shells["topo"].close()
     lat = [r.done_s - r.arrival_s for r in pending]
-    work = sum(int(np.prod(r.cells)) * r.steps for r in pending)
+    work = sum(_cell_count(r) * r.steps for r in pending)
     return {"requests": len(pending), "makespan_s": makespan, "cell_updates": work,
             "mcell_updates_per_s": work / makespan / 1e6, "latency_p50_s": percentile(lat, 50),
             "latency_p99_s": percentile(lat, 99), "latency_mean_s": float(np.mean(lat)) if lat else float("nan")}

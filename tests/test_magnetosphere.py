@@ -1,0 +1,74 @@
+"""Host side of the magnetosphere case (no GPU): the seeded ensemble and
+request stream, the case's constants and background record, the initial
+state, and the reference arm's jobs for the same members."""
+import math
+
+import numpy as np
+import pytest
+
+
+def test_ensemble_is_seeded_and_in_range():
+    from mpcns_mercury_b200 import magnetosphere as M
+
+    a, b = M.ensemble(64), M.ensemble(64)
+    assert [(c.na, c.nr, c.upstream, c.na_fraction) for c in a] == [(c.na, c.nr, c.upstream, c.na_fraction) for c in b]
+    for c in a:
+        assert 24 <= c.na <= 64 and 24 <= c.nr <= 128
+        U, T, n, Mm, cy, cz, Bx, By, Bz = c.upstream
+        assert 2.0 * 4.031e5 <= U <= 6.0 * 4.031e5 and 0.5 * 4e7 <= n <= 3.0 * 4e7
+        assert abs(Bz) <= 0.4e-9 and Bx == By == 0.0 and cy == cz == 0.0
+        assert 1e-4 <= c.na_fraction <= 1e-2
+    total = sum(c.cell_count() for c in a)
+    assert 20e6 < total < 60e6
+    assert M.ensemble(8, stream=300001)[0].na != a[0].na or M.ensemble(8, stream=300001)[0].nr != a[0].nr
+
+
+def test_request_stream():
+    from mpcns_mercury_b200 import magnetosphere as M
+
+    s = M.request_stream(100, 20.0, shapes=16)
+    t = [x[0] for x in s]
+    assert all(t1 > t0 for t0, t1 in zip(t, t[1:]))
+    assert 2.0 < t[-1] < 10.0  # 100 arrivals at 20/s
+    grids = {(c.na, c.nr) for _, c, _ in s}
+    assert len(grids) <= 16
+    for _, c, st in s:
+        assert 24 <= c.na <= 96 and 24 <= c.nr <= 192 and 50 <= st <= 500
+
+
+def test_initial_state_and_background():
+    from mpcns_mercury_b200 import magnetosphere as M
+
+    case = M.ShellCase(na=8, nr=12)
+    k = M.constants(case)
+    uh, un = M.initial_state(case, k)
+    assert np.array_equal(uh, [k.bc[q] for q in range(5)])
+    g = k.gamma
+    rho = uh[0]
+    p = (g - 1.0) * (uh[4] - 0.5 * rho * ((uh[1] / rho) ** 2 + (uh[2] / rho) ** 2 + (uh[3] / rho) ** 2))
+    assert math.isclose(un[0], 1e-3 * (k.M_Na / k.M_H) * rho, rel_tol=1e-15)
+    pn = (g - 1.0) * (un[4] - 0.5 * un[0] * ((un[1] / un[0]) ** 2 + (un[2] / un[0]) ** 2 + (un[3] / un[0]) ** 2))
+    assert math.isclose(pn, 1e-3 * p, rel_tol=1e-12)
+    bg = M.background(case, k)
+    assert bg.n_dipoles == 1 and bg.dipole[0][5] == M.DIPOLE[5]
+    assert bg.B_imf[2] == M.UPSTREAM[8] and bg.L_ref == k.L_ref and bg.inver_Rem == 0.0
+    res = M.ShellCase(na=8, nr=12, resistive=True)
+    kr = M.constants(res)
+    assert M.background(res, kr).inver_Rem == pytest.approx(1.25e7 / (kr.mu0 * kr.U_ref * kr.L_ref), rel=1e-15)
+
+
+def test_reference_jobs_match_the_members():
+    """The reference arm's harness jobs carry each member's size and upstream."""
+    import bench
+    from mpcns_mercury_b200 import magnetosphere as M
+
+    class A:
+        workload = "shells"
+        solves = 5
+
+    members = bench.reference_members(A())
+    for (job, cells), c in zip(members, M.ensemble(5)):
+        assert job["na"] == c.na and job["nr"] == c.nr and cells == c.cell_count()
+        assert [float(v) for v in job["initial_line"].split()] == [float(v) for v in c.upstream]
+        assert float(job["farfield_line"].split()[0]) == float(c.upstream[0])
+        assert job["na_fraction"] == c.na_fraction
