@@ -721,8 +721,12 @@ def run_shells(args, rank, world, device):
         topo.get(c)
     topo_s = time.perf_counter() - t0
 
-    # 1) the mixed-precision batch: W untimed steps, K timed (state >> L2), on to err_steps
+    # 1) the mixed-precision batch: its fluid tile picked by the autotuner on
+    # the batch itself, W untimed steps, K timed (state >> L2), on to err_steps
+    from mpcns_mercury_b200 import autotune
+
     mixed, slots = _shell_batch(cases, ks, topo, 1, err_steps)
+    tune_mixed = autotune.tune(mixed, 1, cells, reps=3, cache=None)
     mixed.run(W_)
     mixed.poll()
     if world > 1:
@@ -764,8 +768,15 @@ def run_shells(args, rank, world, device):
         nsub += 1
         d.close()
     plain_sub = []
+    # the FP64 fluid tile, picked by the autotuner on the subset's FP64 batch
+    # (used by the plain path and the FP64 batch alike)
+    tb, _ = _shell_batch(cases[:nsub], ks[:nsub], topo, 0, 1)
+    tune64 = autotune.tune(tb, 0, cells, reps=3, cache=None)
+    tb.close()
+    tile64 = tune64["variant"]
     for i, (c, k) in enumerate(zip(cases, ks)):
         ctx = M.context(c, precision=0, k=k, topologies=topo)
+        ctx.fluid_tile(tile64)
         ctx.step(W_)
         stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -791,6 +802,7 @@ def run_shells(args, rank, world, device):
 
     # 3) the FP64 batch on the subset: its rate, and bitwise equality with the plain path
     fp64, fslots = _shell_batch(cases[:nsub], ks[:nsub], topo, 0, err_steps)
+    fp64.fluid_tile(tile64)
     fp64.run(W_)
     fp64.poll()
     fp64_ms = _timed_batch_steps(fp64, K, device)
@@ -816,12 +828,12 @@ def run_shells(args, rank, world, device):
     plain_sub_rate = replicas_value(world, sub_cells, K, plain_sub_ms)
     peak, peak_kind = load_peaks()
     roof = roofline(prof, cells, peak, peak_kind, precision=1, traffic_key="k_fluid_mixed_shells")
-    e2e = run_e2e_shells(cases, ks, topo, err_steps, world)
+    e2e = run_e2e_shells(cases, ks, topo, err_steps, world, tune_mixed["variant"])
     topo.close()
     serving = None
     if args.serve_requests > 0:  # a short request stream of the same physics: p50/p99 beside the throughput
         sb, sp, _ = serve_shells(args.serve_requests, args.serve_rate, 8, 48, 96, 50, 100, args.serve_requests,
-                                 args.hbm_budget, rank)
+                                 args.hbm_budget, rank, fluid_tiles=(tune_mixed["variant"], tile64))
         serving = {"requests": args.serve_requests, "arrival_rate_per_s": args.serve_rate,
                    "grids": "8 shell sizes, na log-uniform in [24,48], nr in [24,96]; 50-100 steps per request; "
                             "upstream conditions per request as the ensemble's",
@@ -850,7 +862,8 @@ def run_shells(args, rank, world, device):
                                            "plain_fp64_same_solves_mcells": round(plain_sub_rate, 3),
                                            "bitwise_equal_plain": bool(fp64_identical)},
                    "error_vs_fp64_rel_l2_max_over_solves": {k: float(f"{v:.3e}") for k, v in worst.items()},
-                   "error_steps": err_steps, "host_topology_build_s": round(topo_s, 2)},
+                   "error_steps": err_steps, "host_topology_build_s": round(topo_s, 2),
+                   "autotune_fluid_tile": {"mixed": _tune_summary(tune_mixed), "fp64": _tune_summary(tune64)}},
         "roofline": roof, "cpu_baseline": cpu,
         "e2e": e2e, "serving": serving,
         "latency_p50_s": serving["latency_p50_s"] if serving else None,
@@ -860,7 +873,16 @@ def run_shells(args, rank, world, device):
     }
 
 
-def run_e2e_shells(cases, ks, topo, steps, world):
+def _tune_summary(t):
+    from mpcns_mercury_b200.capi import fluid_tile_shape
+
+    return {"pick": t["variant"], "shape_k_j_i_ctas": list(t["shape"]),
+            "ms_per_fluid_pass": [round(v, 4) for v in t["ms"]] if t["ms"] else None,
+            "variants": [list(fluid_tile_shape(v)) for v in range(len(t["ms"] or []))],
+            "gain_over_default": round(t["ms"][0] / t["ms"][t["variant"]], 4) if t["ms"] else None}
+
+
+def run_e2e_shells(cases, ks, topo, steps, world, fluid_tile=0):
     """The mixed batch end to end through the C ABI, one wall-clock region:
     add every solve (its grid's sync tables, built ahead like a grid file),
     its static fields and background computed on the device from the
@@ -880,6 +902,7 @@ def run_e2e_shells(cases, ks, topo, steps, world):
     descs = _shell_descs(cases, ks, topo, 1)
     b = Batch(len(cases), 1)
     b.reserve(sum(d.device_bytes() for d in descs))
+    b.fluid_tile(fluid_tile)  # the autotuner's pick for this workload
     torch.cuda.synchronize()
     h2d = d2h = 0
     t0 = time.perf_counter()
@@ -958,7 +981,8 @@ def run_serving(args, rank, world, device):
     return line
 
 
-def serve_shells(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, capacity, hbm_budget, rank):
+def serve_shells(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, capacity, hbm_budget, rank,
+                 fluid_tiles=(0, 0)):
     """A Poisson stream of magnetosphere requests served by the
     continuous-batching server (mixed precision) and one by one through the
     plain FP64 path (one context per grid, each request's fields set up on
@@ -979,11 +1003,12 @@ def serve_shells(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, capac
             nodes[key] = capi.shell_grid(r.case.na, r.case.nr, r.case.r_out, M.NGHOST + 1)
     srv = SV.Server(capacity=capacity, precision=1, hbm_budget=hbm_budget, max_grids=shapes, topologies=topo,
                     nodes=nodes)
+    srv.batch.fluid_tile(fluid_tiles[0])
     batched = srv.serve(reqs)
     srv.close()
     for r in reqs:
         r.done_s = float("nan")
-    plain = SV.serve_one_by_one(reqs, precision=0, topologies=topo, nodes=nodes)
+    plain = SV.serve_one_by_one(reqs, precision=0, topologies=topo, nodes=nodes, fluid_tile=fluid_tiles[1])
     topo.close()
     return batched, plain, reqs
 

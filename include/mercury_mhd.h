@@ -478,6 +478,21 @@ int mhd_batch_fill_field(mhd_batch *batch, int slot, int field, int block, const
 int mhd_batch_set_constants(mhd_batch *batch, int slot, const mhd_constants *constants);
 int mhd_batch_sync(mhd_batch *batch, int slot, int group);
 int mhd_batch_prepare(mhd_batch *batch, int slot, double time, int64_t step);
+/* The fluid kernel's tile variants (Scheme_U_ + sources + update, the
+ * step's largest pass): variant v tiles the owned cells in CTAs of 256
+ * threads, shape[0] x shape[1] x shape[2] cells along k, j, i, compiled for
+ * shape[3] resident CTAs per SM (its register cap).  A batch runs one
+ * (default 0); mhd_batch_time_fluid_tiles times each on the batch's active
+ * solves (the fluid pass alone, `reps` launches after one untimed, writing
+ * only the next-step state buffer, which the next step rewrites: the solves'
+ * results do not change), mhd_batch_fluid_tile sets one (the step graphs are
+ * captured anew).  The choice does not change results: every variant
+ * computes each face flux and cell update with the same operations. */
+#define MHD_NUM_FLUID_TILES 6
+int mhd_fluid_tile_shape(int variant, int32_t shape[4]);
+int mhd_batch_fluid_tile(mhd_batch *batch, int variant);
+int mhd_batch_time_fluid_tiles(mhd_batch *batch, int reps, float ms[MHD_NUM_FLUID_TILES]);
+int mhd_fluid_tile(mhd_ctx *ctx, int variant);  /* mhd_batch_fluid_tile of a context */
 /* Sets the slot's request to nsteps more steps (0 parks it). */
 int mhd_batch_request(mhd_batch *batch, int slot, int64_t nsteps);
 /* Enqueues nsteps graph launches of the batched step (asynchronous).  Each

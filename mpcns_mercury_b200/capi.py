@@ -196,7 +196,8 @@ EXPORTS = [
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view", "mhd_shell_nodes", "mhd_shell_grid", "mhd_hall_taper", "mhd_setup_geometry_bg",
     "mhd_batch_setup_geometry_bg", "mhd_fill_field", "mhd_batch_fill_field", "mhd_set_constants",
-    "mhd_batch_set_constants",
+    "mhd_batch_set_constants", "mhd_fluid_tile_shape", "mhd_batch_fluid_tile", "mhd_batch_time_fluid_tiles",
+    "mhd_fluid_tile",
 ]
 
 _lib = None
@@ -256,6 +257,10 @@ def lib() -> ctypes.CDLL:
     L.mhd_setup_geometry.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_double]
     L.mhd_shell_nodes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
                                   ctypes.c_void_p]
+    L.mhd_fluid_tile_shape.argtypes = [ctypes.c_int, i32p]
+    L.mhd_batch_fluid_tile.argtypes = [P, ctypes.c_int]
+    L.mhd_fluid_tile.argtypes = [P, ctypes.c_int]
+    L.mhd_batch_time_fluid_tiles.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.mhd_set_constants.argtypes = [P, ctypes.POINTER(MhdConstants)]
     L.mhd_batch_set_constants.argtypes = [P, ctypes.c_int, ctypes.POINTER(MhdConstants)]
     L.mhd_fill_field.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, i32p, i32p, ctypes.c_int]
@@ -480,6 +485,10 @@ class Context:
         a = np.ascontiguousarray(array, dtype=np.float64)
         check(lib().mhd_upload_field(self.ctx, FIELD_ID[field], block, a.ctypes.data_as(ctypes.c_void_p),
                                      _i3(lo), _i3(hi), a.shape[-1]), f"upload {field}")
+
+    def fluid_tile(self, variant: int):
+        """Run the fluid kernel's tile variant `variant` (mhd_fluid_tile)."""
+        check(lib().mhd_fluid_tile(self.ctx, int(variant)), "mhd_fluid_tile")
 
     def set_constants(self, constants: MhdConstants):
         """A new upstream state on the same grid (mhd_set_constants); prepare must follow."""
@@ -718,6 +727,16 @@ class Batch:
         check(lib().mhd_batch_setup_geometry(self.b, slot, block, a.ctypes.data, float(L_ref)),
               "mhd_batch_setup_geometry")
 
+    def fluid_tile(self, variant: int):
+        """Run the fluid kernel's tile variant `variant` (mhd_batch_fluid_tile)."""
+        check(lib().mhd_batch_fluid_tile(self.b, int(variant)), "mhd_batch_fluid_tile")
+
+    def time_fluid_tiles(self, reps: int = 5):
+        """ms per fluid pass of every tile variant on the active solves (mhd_batch_time_fluid_tiles)."""
+        ms = (ctypes.c_float * NUM_FLUID_TILES)()
+        check(lib().mhd_batch_time_fluid_tiles(self.b, int(reps), ms), "mhd_batch_time_fluid_tiles")
+        return [float(v) for v in ms]
+
     def setup_background(self, slot: int, nodes, background, block: int = 0, L_ref: float = 2.44e6):
         """setup_geometry plus an MhdBackground (mhd_batch_setup_geometry_bg);
         sync(slot, "BADD") once every block of the solve is set."""
@@ -755,6 +774,16 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+NUM_FLUID_TILES = 6  # MHD_NUM_FLUID_TILES
+
+
+def fluid_tile_shape(variant: int):
+    """(k, j, i, CTAs per SM) of a fluid tile variant (mhd_fluid_tile_shape)."""
+    out = (ctypes.c_int32 * 4)()
+    check(lib().mhd_fluid_tile_shape(int(variant), out), "mhd_fluid_tile_shape")
+    return tuple(int(v) for v in out)
 
 
 def shell_nodes(na: int, nr: int, panel: int, r_out: float = 8.0, G: int = 5) -> np.ndarray:

@@ -256,6 +256,7 @@ struct mhd_batch {
   int snap_next = 0;
   // eager profiling
   bool profiling = false;
+  int fluid_tile = 0;  // the fluid kernel's tile variant (fluid_tile)
   std::vector<cudaEvent_t> prof_events;
   std::vector<const char *> prof_names;
   size_t prof_used = 0;
@@ -403,7 +404,7 @@ void enqueue_step_a(mhd_batch *b, int *nk) {
   enqueue_sync(b, m, MHD_SYNC_EEDGE, nk);
   // AssembleRHS_Fluid_ + ApplyUpdate_Euler_ (state into the other buffer) and
   // the constrained-transport face update (Z4_Mercury/src/physics/MercurySolver_Advance.cpp:73-147)
-  launch(b, m, SK_FLUID, nk);
+  launch(b, m, SK_FLUID, nk, nullptr, b->fluid_tile);
   launch(b, m, SK_BFACE, nk);
   launch(b, m, SK_FLIP, nk);
   // the reference's Sync(Ucell) reads ghosts it does not overwrite first at
@@ -1828,6 +1829,59 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   return MHD_OK;
 }
 
+int mhd_fluid_tile_shape(int variant, int32_t shape[4]) {
+  if (variant < 0 || variant >= kNumFluidTiles || !shape) return fail(MHD_ERR_ARG, "fluid tile variant %d", variant);
+  const FluidTile T = fluid_tile(variant);
+  shape[0] = T.k;
+  shape[1] = T.j;
+  shape[2] = T.i;
+  shape[3] = T.min_ctas;
+  return MHD_OK;
+}
+
+int mhd_batch_fluid_tile(mhd_batch *b, int variant) {
+  if (!b || variant < 0 || variant >= kNumFluidTiles) return fail(MHD_ERR_ARG, "mhd_batch_fluid_tile: bad arguments");
+  if (variant == b->fluid_tile) return MHD_OK;
+  CUDA_TRY(cudaStreamSynchronize(b->stream));  // no step graph in flight
+  b->fluid_tile = variant;
+  drop_graphs(b);
+  return MHD_OK;
+}
+
+int mhd_batch_time_fluid_tiles(mhd_batch *b, int reps, float ms[MHD_NUM_FLUID_TILES]) {
+  if (!b || reps < 1 || !ms) return fail(MHD_ERR_ARG, "mhd_batch_time_fluid_tiles: bad arguments");
+  int rc = read_state(b);
+  if (rc) return rc;
+  bool any = false;
+  for (int s = 0; s < b->capacity; ++s)
+    any = any || (b->slots[s] && b->hstate[s].remaining != 0 && b->hstate[s].status == 0);
+  if (!any) return fail(MHD_ERR_STATE, "mhd_batch_time_fluid_tiles: no solve has steps requested");
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  int nk = 0;
+  for (int v = 0; v < kNumFluidTiles; ++v) {
+    // the fluid pass alone writes only the next state buffer, which the next
+    // step rewrites with the same values: the solves are unchanged
+    launch(b, 0, SK_FLUID, &nk, nullptr, v);  // untimed
+    cudaEventRecord(e0, b->stream);
+    for (int r = 0; r < reps; ++r) launch(b, 0, SK_FLUID, &nk, nullptr, v);
+    cudaEventRecord(e1, b->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(MHD_ERR_CUDA, "mhd_batch_time_fluid_tiles: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    ms[v] = t / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CUDA_TRY(cudaGetLastError());
+  return MHD_OK;
+}
+
 int mhd_batch_set_constants(mhd_batch *b, int slot, const mhd_constants *constants) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
@@ -2397,6 +2451,11 @@ int mhd_upload_field(mhd_ctx *ctx, int field, int block, const double *data, con
                      int ncomp) {
   if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
   return mhd_batch_upload_field(ctx->batch, 0, field, block, data, lo, hi, ncomp);
+}
+
+int mhd_fluid_tile(mhd_ctx *ctx, int variant) {
+  if (!ctx) return fail(MHD_ERR_ARG, "null ctx");
+  return mhd_batch_fluid_tile(ctx->batch, variant);
 }
 
 int mhd_set_constants(mhd_ctx *ctx, const mhd_constants *constants) {

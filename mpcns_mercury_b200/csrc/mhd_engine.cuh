@@ -15,27 +15,44 @@
 
 namespace mhd {
 
+// The fluid kernel's tile variants: cells along k, j, i of one 256-thread
+// CTA, and the resident CTAs per SM asked of the compiler (its register cap,
+// 65536 / (256 n)).  The batch runs one of them (mhd_batch_fluid_tile),
+// picked by timing (mhd_batch_time_fluid_tiles); variant 0 is the default:
+// 16 x 4 x 4 wastes fewer lanes than 32 x 4 x 2 on k extents that are not
+// multiples of 32 and needs 6% fewer face fluxes per tile (912 vs 968).
+struct FluidTile {
+  int k, j, i, min_ctas;
+};
+constexpr int kNumFluidTiles = MHD_NUM_FLUID_TILES;
+__host__ __device__ constexpr FluidTile fluid_tile(int v) {
+  return v == 1 ? FluidTile{32, 4, 2, 3} : v == 2 ? FluidTile{8, 8, 4, 3} : v == 3 ? FluidTile{32, 2, 4, 3}
+         : v == 4 ? FluidTile{16, 4, 4, 2} : v == 5 ? FluidTile{64, 2, 2, 3} : FluidTile{16, 4, 4, 3};
+}
+constexpr int kTileThreads = 256;
+constexpr bool fluid_tiles_ok() {
+  for (int v = 0; v < kNumFluidTiles; ++v)
+    if (fluid_tile(v).k * fluid_tile(v).j * fluid_tile(v).i != kTileThreads) return false;
+  return true;
+}
+static_assert(fluid_tiles_ok(), "fluid tiles of 256 cells");
+
 // Range kinds of the work lists.
 enum RangeKind : int {
   kCells = 0,    // owned cells [0, n)
   kBox = 1,      // [0, n + 1): owned faces and edges of all families
   kExt = 2,      // [-1, n + 2): face EMF candidates incl. one ghost layer
   kAlloc = 3,    // [-gs, n + gs), gs = min(nghost, kStepGhost): the ghost cells the step maintains
-  kCells2 = 4,   // owned cells, two work items per tile (one per ion species)
+  kCells2 = 4,   // owned cells in fluid tiles of variant 0, two work items per tile (one per ion species)
   kFull = 5,     // [-(g + 1), n + g + 2): the whole box
-  kNumRanges = 6
+  // owned cells in fluid tiles of variants 1 .. kNumFluidTiles - 1
+  kNumRanges = 6 + kNumFluidTiles - 1
 };
-
-// Fluid-kernel tile (cells along k, j, i); 256 threads per CTA everywhere.
-// 16 x 4 x 4 wastes fewer lanes than 32 x 4 x 2 on blocks whose k extent is
-// not a multiple of 32 and needs 6% fewer face fluxes per tile (912 vs 968).
-#ifndef MHD_TILE_K
-#define MHD_TILE_K 16
-#define MHD_TILE_J 4
-#define MHD_TILE_I 4
-#endif
-constexpr int kTileK = MHD_TILE_K, kTileJ = MHD_TILE_J, kTileI = MHD_TILE_I, kTileThreads = 256;
-static_assert(kTileK * kTileJ * kTileI == kTileThreads, "fluid tile of 256 cells");
+// The range kind of fluid tile variant v, and the variant of a range kind (-1: none).
+__host__ __device__ constexpr int fluid_kind(int v) { return v == 0 ? (int)kCells2 : (int)kFull + v; }
+__host__ __device__ constexpr int fluid_variant(int kind) {
+  return kind == kCells2 ? 0 : (kind > kFull && kind < kNumRanges ? kind - kFull : -1);
+}
 
 // Ghost depth the step keeps valid between its passes: the widest stencil
 // reach of its kernels (face EMF candidates on [-1, n + 2) read contravariant
@@ -239,30 +256,32 @@ __host__ __device__ inline RangeBox range_of(int kind, const int n[3], int g) {
   RangeBox r;
   for (int a = 0; a < 3; ++a) {
     switch (kind) {
-      case kCells:
-      case kCells2: r.lo[a] = 0; r.hi[a] = n[a]; break;
+      case kCells: r.lo[a] = 0; r.hi[a] = n[a]; break;
       case kBox: r.lo[a] = 0; r.hi[a] = n[a] + 1; break;
       case kExt: r.lo[a] = -1; r.hi[a] = n[a] + 2; break;
       case kFull: r.lo[a] = -(g + 1); r.hi[a] = n[a] + g + 2; break;
-      default: {
+      case kAlloc: {
         const int gs = g < kStepGhost ? g : kStepGhost;
         r.lo[a] = -gs;
         r.hi[a] = n[a] + gs;
         break;
       }
+      default: r.lo[a] = 0; r.hi[a] = n[a]; break;  // the fluid kinds: owned cells
     }
   }
   return r;
 }
-// Work items of a block: kCells2 (the fluid kernel) uses 3-D tiles of
-// 32 k x 4 j x 2 i cells (two per tile, one per species); every other range is
+// Work items of a block: the fluid kinds use 3-D tiles of their variant's
+// shape (two work items per tile, one per species); every other range is
 // cut into runs of kTileThreads consecutive positions of its box (k fastest),
 // so no lane idles at the end of short k rows.
 __host__ __device__ inline int tiles_of(const RangeBox &r, int kind) {
-  if (kind == kCells2) {
-    const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
-    const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
-    const int ti = (r.hi[0] - r.lo[0] + kTileI - 1) / kTileI;
+  const int v = fluid_variant(kind);
+  if (v >= 0) {
+    const FluidTile T = fluid_tile(v);
+    const int tk = (r.hi[2] - r.lo[2] + T.k - 1) / T.k;
+    const int tj = (r.hi[1] - r.lo[1] + T.j - 1) / T.j;
+    const int ti = (r.hi[0] - r.lo[0] + T.i - 1) / T.i;
     return tk * tj * ti * 2;
   }
   const int64_t vol = (int64_t)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);

@@ -150,18 +150,19 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
       it.hi[a] = r.hi[a];
       it.lo[a] = r.lo[a];
     }
-    if (KIND == kCells2) {  // 32 k x 4 j x 2 i tile, one species
+    if constexpr (fluid_variant(KIND) >= 0) {  // a fluid tile, one species
+      constexpr FluidTile T = fluid_tile(fluid_variant(KIND));
       it.species = t & 1;
       t >>= 1;
-      const int tk = (r.hi[2] - r.lo[2] + kTileK - 1) / kTileK;
-      const int tj = (r.hi[1] - r.lo[1] + kTileJ - 1) / kTileJ;
+      const int tk = (r.hi[2] - r.lo[2] + T.k - 1) / T.k;
+      const int tj = (r.hi[1] - r.lo[1] + T.j - 1) / T.j;
       const int bk = t % tk, bj = (t / tk) % tj, bi = t / (tk * tj);
-      it.o[0] = r.lo[0] + bi * kTileI;
-      it.o[1] = r.lo[1] + bj * kTileJ;
-      it.o[2] = r.lo[2] + bk * kTileK;
-      it.k = it.o[2] + (tid % kTileK);
-      it.j = it.o[1] + ((tid / kTileK) % kTileJ);
-      it.i = it.o[0] + (tid / (kTileK * kTileJ));
+      it.o[0] = r.lo[0] + bi * T.i;
+      it.o[1] = r.lo[1] + bj * T.j;
+      it.o[2] = r.lo[2] + bk * T.k;
+      it.k = it.o[2] + (tid % T.k);
+      it.j = it.o[1] + ((tid / T.k) % T.j);
+      it.i = it.o[0] + (tid / (T.k * T.j));
       it.in = it.i < r.hi[0] && it.j < r.hi[1] && it.k < r.hi[2];
     } else {  // a run of kTileThreads consecutive positions of the range box (k fastest)
       const int ek = r.hi[2] - r.lo[2], ej = r.hi[1] - r.lo[1];
@@ -552,21 +553,25 @@ __device__ __forceinline__ void rusanov(const V<R> &B, R g, int u0, int pv0, R k
 // shared memory (a face's flux has the same inputs and operation order for
 // both cells that share it), then every cell accumulates
 // r[m] -= (F+ - F-) / J, the per-component order of Scheme_U_'s divergence.
-constexpr int kNF0 = (kTileI + 1) * kTileJ * kTileK, kNF1 = kTileI * (kTileJ + 1) * kTileK,
-              kNF2 = kTileI * kTileJ * (kTileK + 1);
-constexpr int kTileFaces = kNF0 + kNF1 + kNF2;  // the tile's faces of all three directions
-// Minimum resident CTAs per SM asked of the compiler for the two
-// register-heavy kernels (caps registers at 65536 / (256 * n)).
-#ifndef MHD_MIN_CTAS_FLUID
-#define MHD_MIN_CTAS_FLUID 3
-#endif
+// A tile's faces per direction and in all (variant V).
+template <int VT>
+struct TileFaces {
+  static constexpr FluidTile T = fluid_tile(VT);
+  static constexpr int n0 = (T.i + 1) * T.j * T.k, n1 = T.i * (T.j + 1) * T.k, n2 = T.i * T.j * (T.k + 1);
+  static constexpr int all = n0 + n1 + n2;
+};
+// Minimum resident CTAs per SM asked of the compiler for the primitive pass
+// (caps registers at 65536 / (256 * n)); the fluid kernel's is its tile variant's.
 #ifndef MHD_MIN_CTAS_PV
 #define MHD_MIN_CTAS_PV 4
 #endif
-template <class R>
-__global__ void __launch_bounds__(kTileThreads, MHD_MIN_CTAS_FLUID) k_fluid(Dir D) {
+template <class R, int VT>
+__global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid(Dir D) {
+  constexpr FluidTile T = fluid_tile(VT);
+  constexpr int kNF0 = TileFaces<VT>::n0, kNF1 = TileFaces<VT>::n1, kTileFaces = TileFaces<VT>::all;
+  constexpr int kTileK = T.k, kTileJ = T.j;
   __shared__ R F[5][kTileFaces];
-  for_items<R, kCells2>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, fluid_kind(VT)>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     const ConstsT<R> &c = consts_of<R>(S);
     const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
     // the reference aborts; k_flip records the status (and a solve with a
@@ -1940,6 +1945,32 @@ __global__ void k_retire(Dir D) {
 // residual-dot kernel keeps a fixed grid: its partial sums are indexed by CTA.
 static int g_grid_tiles = 0;
 static int g_grid_kernel[SK_COUNT];
+static int g_grid_fluid[kNumFluidTiles];  // the fluid kernel's, per tile variant
+
+template <class R>
+static const void *fluid_fn(int v) {
+  switch (v) {
+    case 1: return (const void *)k_fluid<R, 1>;
+    case 2: return (const void *)k_fluid<R, 2>;
+    case 3: return (const void *)k_fluid<R, 3>;
+    case 4: return (const void *)k_fluid<R, 4>;
+    case 5: return (const void *)k_fluid<R, 5>;
+    default: return (const void *)k_fluid<R, 0>;
+  }
+}
+static_assert(kNumFluidTiles == 6, "fluid_fn and launch_fluid list every variant");
+template <class R>
+static void launch_fluid(int v, const Dir &D, cudaStream_t st) {
+  const int G = g_grid_fluid[(v >= 0 && v < kNumFluidTiles) ? v : 0];
+  switch (v) {
+    case 1: k_fluid<R, 1><<<G, kTileThreads, 0, st>>>(D); break;
+    case 2: k_fluid<R, 2><<<G, kTileThreads, 0, st>>>(D); break;
+    case 3: k_fluid<R, 3><<<G, kTileThreads, 0, st>>>(D); break;
+    case 4: k_fluid<R, 4><<<G, kTileThreads, 0, st>>>(D); break;
+    case 5: k_fluid<R, 5><<<G, kTileThreads, 0, st>>>(D); break;
+    default: k_fluid<R, 0><<<G, kTileThreads, 0, st>>>(D); break;
+  }
+}
 
 template <class R>
 static const void *kernel_fn(StepKernel k) {
@@ -1948,7 +1979,7 @@ static const void *kernel_fn(StepKernel k) {
     case SK_EDGE_EMF: return (const void *)k_edge_emf<R>;
     case SK_HALL_EDGE: return (const void *)k_hall_edge<R>;
     case SK_ADD_HALL: return (const void *)k_add_hall<R>;
-    case SK_FLUID: return (const void *)k_fluid<R>;
+    case SK_FLUID: return fluid_fn<R>(0);
     case SK_BFACE: return (const void *)k_bface<R>;
     case SK_BCELL_JEDGE: return (const void *)k_bcell_jedge<R>;
     case SK_JCELL: return (const void *)k_jcell<R>;
@@ -1989,6 +2020,15 @@ static void grids_init() {
     }
     g_grid_kernel[k] = sms * (per_sm < 8 ? per_sm : 8);
   }
+  for (int v = 0; v < kNumFluidTiles; ++v) {
+    int per_sm = 8;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fluid_fn<R>(v), kTileThreads, 0) != cudaSuccess ||
+        per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    g_grid_fluid[v] = sms * (per_sm < 8 ? per_sm : 8);
+  }
   g_grid_tiles = sms * 8;
 }
 
@@ -2006,7 +2046,7 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_EDGE_EMF: k_edge_emf<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_HALL_EDGE: k_hall_edge<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_ADD_HALL: k_add_hall<R><<<G, kTileThreads, 0, st>>>(D); break;
-    case SK_FLUID: k_fluid<R><<<G, kTileThreads, 0, st>>>(D); break;
+    case SK_FLUID: launch_fluid<R>(iarg, D, st); break;  // iarg: the tile variant
     case SK_BFACE: k_bface<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_BCELL_JEDGE: k_bcell_jedge<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_JCELL: k_jcell<R><<<G, kTileThreads, 0, st>>>(D); break;

@@ -256,7 +256,7 @@ class Server:
 
 
 def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl: float = 0.4, topologies=None,
-                     nodes=None):
+                     nodes=None, fluid_tile: int = 0):
     """The same requests served first-come first-served through the plain
     single-solve path (mhd_ctx, one solve on the GPU at a time).  Like the
     server, it keeps one context per grid (tables and static fields uploaded
@@ -291,6 +291,7 @@ def serve_one_by_one(requests, precision: int = 0, clock=time.perf_counter, cfl:
             if ctx is None:
                 ctx = capi.Context(r.case.cells, NGHOST, k, topology=shells["topo"].get(r.case), precision=precision,
                                    keep_topology=True)
+                ctx.fluid_tile(fluid_tile)
                 ctxs[key] = ctx
             ctx.set_constants(k)
             M.set_up(ctx, r.case, k=k, nodes=shells[key])

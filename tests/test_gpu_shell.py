@@ -181,3 +181,27 @@ def test_shell_implicit_resistivity_mixed(res_shell):
     assert not bad, {k: v for k, v in worst.items() if v > 1e-5}
     assert info.status == 0 and info.res_relres <= 1e-10
     ctx.close()
+
+
+def test_config2_shell_implicit_resistivity(ref_oracle):
+    """The configuration's shell (6 x 48x48x96) with the implicit resistive
+    substep, 3 steps, FP64: within 1e-10 relative L2 of the reference (CG
+    against GMRES, both to 1e-14)."""
+    if not has_gpu():
+        pytest.skip("no GPU")
+    import mercury_oracle as mo
+    from gpu_helpers import compare, shell_constants, shell_context
+
+    extra = dict(RES_EXTRA, dump_fields="U_H U_Na B_xi B_eta B_zeta")
+    dump = ref_oracle.shell_run(na=48, nr=96, steps=3, dump_at=[0, 3], extra=extra)
+    k = shell_constants(resistive=True, res_rtol=1e-14, res_max_it=4000)
+    ctx = shell_context(dump, 48, 96, constants=k)
+    ctx.prepare()
+    ctx.step(3)
+    worst, bad = compare(ctx, dump, "step3:", mo.STATE_FIELDS, 1e-10)
+    info = ctx.info()
+    print("6 x 48x48x96 shell, implicit resistivity, 3 steps: max rel L2", max(worst.values()),
+          "CG iterations of the last substep", info.res_iters)
+    assert not bad, {k: v for k, v in worst.items() if v > 1e-10}
+    assert info.status == 0 and info.res_relres <= 1e-14
+    ctx.close()

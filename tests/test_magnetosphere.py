@@ -72,3 +72,16 @@ def test_reference_jobs_match_the_members():
         assert [float(v) for v in job["initial_line"].split()] == [float(v) for v in c.upstream]
         assert float(job["farfield_line"].split()[0]) == float(c.upstream[0])
         assert job["na_fraction"] == c.na_fraction
+
+
+def test_fluid_tile_shapes_and_shape_classes():
+    from mpcns_mercury_b200 import autotune, capi
+
+    shapes = [capi.fluid_tile_shape(v) for v in range(capi.NUM_FLUID_TILES)]
+    assert shapes[0] == (16, 4, 4, 3)
+    assert all(k * j * i == 256 and ctas in (2, 3) for k, j, i, ctas in shapes)
+    assert len(set(shapes)) == len(shapes)
+    with pytest.raises(capi.MhdError):
+        capi.fluid_tile_shape(capi.NUM_FLUID_TILES)
+    assert autotune.shape_class([(24, 24, 30)] * 6) == "k<=32-j<=32"
+    assert autotune.shape_class([(48, 48, 96)] * 6) == "k<=128-j<=64"
