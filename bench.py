@@ -832,8 +832,12 @@ def run_shells(args, rank, world, device):
     topo.close()
     serving = None
     if args.serve_requests > 0:  # a short request stream of the same physics: p50/p99 beside the throughput
-        sb, sp, _ = serve_shells(args.serve_requests, args.serve_rate, 8, 48, 96, 50, 100, args.serve_requests,
-                                 args.hbm_budget, rank, fluid_tiles=(tune_mixed["variant"], tile64))
+        items = M.request_stream(args.serve_requests, args.serve_rate, 8, 48, 96, 50, 100,
+                                 stream=500000 + 1000 * rank)
+        sb, sp, _ = serve_shells(items, args.serve_requests, args.hbm_budget,
+                                 fluid_tiles=(tune_mixed["variant"], tile64), shapes=8)
+        sb.pop("latencies")
+        sp.pop("latencies")
         serving = {"requests": args.serve_requests, "arrival_rate_per_s": args.serve_rate,
                    "grids": "8 shell sizes, na log-uniform in [24,48], nr in [24,96]; 50-100 steps per request; "
                             "upstream conditions per request as the ensemble's",
@@ -981,19 +985,18 @@ def run_serving(args, rank, world, device):
     return line
 
 
-def serve_shells(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, capacity, hbm_budget, rank,
-                 fluid_tiles=(0, 0)):
-    """A Poisson stream of magnetosphere requests served by the
+def serve_shells(items, capacity, hbm_budget, fluid_tiles=(0, 0), shapes=16):
+    """Magnetosphere requests [(arrival_s, ShellCase, steps)] served by the
     continuous-batching server (mixed precision) and one by one through the
     plain FP64 path (one context per grid, each request's fields set up on
     the device).  Returns (batched stats, plain stats, requests)."""
+    import torch
     from mpcns_mercury_b200 import capi
     from mpcns_mercury_b200 import magnetosphere as M
     from mpcns_mercury_b200 import serving as SV
 
-    stream = M.request_stream(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, stream=500000 + 1000 * rank)
     reqs = [SV.Request(rid=q, arrival_s=t, cells=None, steps=st, fields={}, case=c)
-            for q, (t, c, st) in enumerate(stream)]
+            for q, (t, c, st) in enumerate(items)]
     # the grids' tables and nodes, prepared ahead for both (host setup, like grid files read ahead)
     topo, nodes = M.TopologyCache(), {}
     for r in reqs:
@@ -1001,14 +1004,22 @@ def serve_shells(nreq, rate, shapes, na_max, nr_max, steps_min, steps_max, capac
         key = ("shell", r.case.na, r.case.nr, bool(r.case.resistive))
         if key not in nodes:
             nodes[key] = capi.shell_grid(r.case.na, r.case.nr, r.case.r_out, M.NGHOST + 1)
-    srv = SV.Server(capacity=capacity, precision=1, hbm_budget=hbm_budget, max_grids=shapes, topologies=topo,
-                    nodes=nodes)
+    srv = SV.Server(capacity=capacity, precision=1, hbm_budget=hbm_budget, max_grids=max(shapes, len(nodes)),
+                    topologies=topo, nodes=nodes)
     srv.batch.fluid_tile(fluid_tiles[0])
+    dist = torch.distributed
+    multi = dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1
+    if multi:
+        dist.barrier()  # the ranks' request clocks start together
     batched = srv.serve(reqs)
     srv.close()
+    batched["latencies"] = [r.done_s - r.arrival_s for r in reqs]
     for r in reqs:
         r.done_s = float("nan")
+    if multi:
+        dist.barrier()
     plain = SV.serve_one_by_one(reqs, precision=0, topologies=topo, nodes=nodes, fluid_tile=fluid_tiles[1])
+    plain["latencies"] = [r.done_s - r.arrival_s for r in reqs]
     topo.close()
     return batched, plain, reqs
 
@@ -1018,18 +1029,26 @@ def run_serving_shells(args, rank, world, device):
     stream (``--requests``, ``--rate``), sizes log-uniform up to
     6 x 96 x 96 x 192 from ``--shapes`` grids, 50-500 steps each, served by the
     continuous-batching server (mixed) and one by one (plain FP64)."""
-    sb, sp, reqs = serve_shells(args.requests, args.rate, args.shapes, 96, 192, 50, 500, args.capacity,
-                                args.hbm_budget, rank)
+    from mpcns_mercury_b200 import magnetosphere as M
+    from mpcns_mercury_b200.distributed import aggregate, partition
+
+    # one stream for the whole job, each rank serving its own partition
+    stream = M.request_stream(args.requests, args.rate, args.shapes, 96, 192, 50, 500, stream=500000)
+    mine = partition([c.cell_count() * st for _, c, st in stream], world)[rank]
+    sb, sp, reqs = serve_shells([stream[q] for q in mine], args.capacity, args.hbm_budget, shapes=args.shapes)
+    sb = aggregate(sb, sb.pop("latencies"))
+    sp = aggregate(sp, sp.pop("latencies"))
     return {
-        "metric": METRIC, "value": round(sb["mcell_updates_per_s"] * world, 3), "unit": UNIT, "n_gpus": world,
+        "metric": METRIC, "value": round(sb["mcell_updates_per_s"], 3), "unit": UNIT, "n_gpus": world,
         "steps": int(sum(r.steps for r in reqs)), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (metric f64)", "data": "synthetic",
         "config": {"workload": "serve-shells", "requests": args.requests, "arrival_rate_per_s": args.rate,
                    "grids": args.shapes, "capacity": args.capacity, "hbm_budget_bytes": args.hbm_budget,
+                   "parallelism": f"request stream partitioned over {world} rank(s) (longest first)",
                    "batched_mixed": _round_stats(sb), "plain_fp64_one_by_one": _round_stats(sp)},
         "latency_p50_s": round(sb["latency_p50_s"], 4), "latency_p99_s": round(sb["latency_p99_s"], 4),
         "roofline": None, "cpu_baseline": None,
-        "e2e": {"value": round(sb["mcell_updates_per_s"] * world, 3), "unit": UNIT,
+        "e2e": {"value": round(sb["mcell_updates_per_s"], 3), "unit": UNIT,
                 "what": "wall clock of the whole request loop: per request its fields set up on the device from "
                         "its parameters, its steps, its slot freed"},
     }
