@@ -64,7 +64,7 @@ def read_dump(path: str) -> dict:
 def run_job(job: dict, timeout: float = 3600.0, workdir: str | None = None) -> dict:
     """Run the reference harness with ``job`` (key -> value) and return its dump."""
     if not available():
-        raise FileNotFoundError(f"{REF_BIN} is not built (make -C oracle)")
+        raise FileNotFoundError(f"{REF_BIN} is not built (make -C oracle REF=<reference sources>)")
     own = workdir is None
     if own:  # a fresh folder under the oracle's own (git-ignored) build directory, removed afterwards
         jobs = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "jobs")

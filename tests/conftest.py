@@ -31,5 +31,5 @@ def ref_oracle():
     import mercury_oracle
 
     if not mercury_oracle.available():
-        pytest.skip("oracle/_ref/mercury_ref not built (make -C oracle)")
+        pytest.skip("oracle/_ref/mercury_ref not built (make -C oracle REF=<reference sources>)")
     return mercury_oracle
