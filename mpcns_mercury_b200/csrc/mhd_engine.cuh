@@ -26,8 +26,8 @@ struct FluidTile {
 };
 constexpr int kNumFluidTiles = MHD_NUM_FLUID_TILES;
 __host__ __device__ constexpr FluidTile fluid_tile(int v) {
-  return v == 1 ? FluidTile{32, 4, 2, 3} : v == 2 ? FluidTile{8, 8, 4, 3} : v == 3 ? FluidTile{32, 2, 4, 3}
-         : v == 4 ? FluidTile{16, 4, 4, 2} : v == 5 ? FluidTile{64, 2, 2, 3} : FluidTile{16, 4, 4, 3};
+  return v == 1 ? FluidTile{8, 8, 4, 4} : v == 2 ? FluidTile{8, 8, 4, 3} : v == 3 ? FluidTile{16, 4, 4, 4}
+         : v == 4 ? FluidTile{16, 4, 4, 2} : v == 5 ? FluidTile{8, 8, 4, 2} : FluidTile{16, 4, 4, 3};
 }
 constexpr int kTileThreads = 256;
 constexpr bool fluid_tiles_ok() {

@@ -525,19 +525,16 @@ __global__ void __launch_bounds__(kTileThreads) k_add_hall(Dir D) {
 }
 
 // ------------------------------------------------------------------ fluid update
-// Rusanov face flux of Scheme_U_ (Z4_Mercury/src/physics/MercurySolver_FluidRHS.cpp:36-104).
+// Rusanov face flux of Scheme_U_ (Z4_Mercury/src/physics/MercurySolver_FluidRHS.cpp:36-104)
+// from the two cells' staged quantities (rho, u, v, w, p and
+// the per-cell terms re = p / (g - 1) + rho |u|^2 / 2, c = sqrt(g p / rho),
+// which Scheme_U_ evaluates per face with the same operations on the same
+// cell values, so staging them once per cell keeps the result bit for bit).
 template <class R>
-__device__ __forceinline__ void rusanov(const V<R> &B, R g, int u0, int pv0, R k1, R k2, R k3,
-                                        R sk, int iL, int jL, int kL, int i, int j, int k, R out[5]) {
-  const R rhoL = AT(u0, iL, jL, kL), uL = AT(pv0, iL, jL, kL), vL = AT(pv0 + 1, iL, jL, kL),
-               wL = AT(pv0 + 2, iL, jL, kL), pL = AT(pv0 + 3, iL, jL, kL);
-  const R rhoR = AT(u0, i, j, k), uR = AT(pv0, i, j, k), vR = AT(pv0 + 1, i, j, k), wR = AT(pv0 + 2, i, j, k),
-               pR = AT(pv0 + 3, i, j, k);
-  const R reL = pL / (g - R(1.0)) + R(0.5) * rhoL * (uL * uL + vL * vL + wL * wL);
-  const R reR = pR / (g - R(1.0)) + R(0.5) * rhoR * (uR * uR + vR * vR + wR * wR);
-  // sk = sqrt(k1 * k1 + k2 * k2 + k3 * k3), the face's |JD| (FNORM component 3)
+__device__ __forceinline__ void rusanov_staged(const R *L, const R *Rr, R k1, R k2, R k3, R sk, R out[5]) {
+  const R rhoL = L[0], uL = L[1], vL = L[2], wL = L[3], pL = L[4], reL = L[5], cL = L[6];
+  const R rhoR = Rr[0], uR = Rr[1], vR = Rr[2], wR = Rr[3], pR = Rr[4], reR = Rr[5], cR = Rr[6];
   const R uvwL = k1 * uL + k2 * vL + k3 * wL, uvwR = k1 * uR + k2 * vR + k3 * wR;
-  const R cL = sqrt(dmax(R(0.0), g * pL / dmax(rhoL, R(1e-30)))), cR = sqrt(dmax(R(0.0), g * pR / dmax(rhoR, R(1e-30))));
   const R rad = dmax(fabs(uvwL) + cL * sk, fabs(uvwR) + cR * sk);
   out[0] = R(0.5) * (rhoL * uvwL + rhoR * uvwR) - R(0.5) * rad * (rhoR - rhoL);
   out[1] = R(0.5) * ((rhoL * uvwL * uL + k1 * pL) + (rhoR * uvwR * uR + k1 * pR)) - R(0.5) * rad * (rhoR * uR - rhoL * uL);
@@ -546,13 +543,6 @@ __device__ __forceinline__ void rusanov(const V<R> &B, R g, int u0, int pv0, R k
   out[4] = R(0.5) * (uvwL * (reL + pL) + uvwR * (reR + pR)) - R(0.5) * rad * (reR - reL);
 }
 
-// ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid (FluidRHS.cpp:206-527) +
-// ApplyUpdate_Euler_ (Z4_Mercury/src/physics/MercurySolver_Advance.cpp:73-147)
-// for one tile of owned cells and one ion species; the state goes to the
-// other buffer.  Per direction, the tile's face fluxes are computed once into
-// shared memory (a face's flux has the same inputs and operation order for
-// both cells that share it), then every cell accumulates
-// r[m] -= (F+ - F-) / J, the per-component order of Scheme_U_'s divergence.
 // A tile's faces per direction and in all (variant V).
 template <int VT>
 struct TileFaces {
@@ -560,6 +550,24 @@ struct TileFaces {
   static constexpr int n0 = (T.i + 1) * T.j * T.k, n1 = T.i * (T.j + 1) * T.k, n2 = T.i * T.j * (T.k + 1);
   static constexpr int all = n0 + n1 + n2;
 };
+
+// Shared memory of the fluid kernel's tile (variant VT): the staged
+// quantities of the tile's cells and their face neighbours (7 values per cell
+// of the tile padded by one layer) and the tile's face fluxes (5 per face).
+template <class R, int VT>
+struct FluidSmem {
+  static constexpr FluidTile T = fluid_tile(VT);
+  static constexpr int PK = T.k + 2, PJ = T.j + 2, PI = T.i + 2, cells = PK * PJ * PI;
+  static constexpr size_t bytes = sizeof(R) * (size_t)(7 * cells + 5 * TileFaces<VT>::all);
+};
+
+// ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid (FluidRHS.cpp:206-527) +
+// ApplyUpdate_Euler_ (Z4_Mercury/src/physics/MercurySolver_Advance.cpp:73-147)
+// for one tile of owned cells and one ion species; the state goes to the
+// other buffer.  Per direction, the tile's face fluxes are computed once into
+// shared memory (a face's flux has the same inputs and operation order for
+// both cells that share it), then every cell accumulates
+// r[m] -= (F+ - F-) / J, the per-component order of Scheme_U_'s divergence.
 // Minimum resident CTAs per SM asked of the compiler for the primitive pass
 // (caps registers at 65536 / (256 * n)); the fluid kernel's is its tile variant's.
 #ifndef MHD_MIN_CTAS_PV
@@ -570,7 +578,10 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
   constexpr FluidTile T = fluid_tile(VT);
   constexpr int kNF0 = TileFaces<VT>::n0, kNF1 = TileFaces<VT>::n1, kTileFaces = TileFaces<VT>::all;
   constexpr int kTileK = T.k, kTileJ = T.j;
-  __shared__ R F[5][kTileFaces];
+  constexpr int PK = FluidSmem<R, VT>::PK, PJ = FluidSmem<R, VT>::PJ, NP = FluidSmem<R, VT>::cells;
+  extern __shared__ __align__(16) unsigned char fluid_smem[];
+  R(*C)[NP] = reinterpret_cast<R(*)[NP]>(fluid_smem);                         // [7][NP]
+  R(*F)[kTileFaces] = reinterpret_cast<R(*)[kTileFaces]>(fluid_smem + sizeof(R) * 7 * NP);  // [5][faces]
   for_items<R, fluid_kind(VT)>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     const ConstsT<R> &c = consts_of<R>(S);
     const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
@@ -618,42 +629,79 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
       if constexpr (sizeof(R) == 4) invJ = AT(cFM + 9, i, j, k);  // R(1) / R(Jac), from k_face_normals
       else invJ = R(1.0) / R(ATM(cJAC, i, j, k));
     }
-    // The tile's face fluxes of all three directions in one pass (faces
-    // dealt round-robin over the threads: 912 faces of a 16 x 4 x 4 tile take
-    // four rounds of 256), then every cell takes its six faces' differences
-    // direction by direction, in Scheme_U_'s order.
+    // Stage the cells the tile's faces read (the tile and one layer beyond
+    // each of its six sides, inside the owned range widened by one): rho,
+    // u, v, w, p and the per-cell terms re and c.
 #pragma unroll 1
-    for (int gf = tid; gf < kTileFaces; gf += kTileThreads) {
-      const int dir = gf < kNF0 ? 0 : gf < kNF0 + kNF1 ? 1 : 2;
-      const int f = gf - (dir == 0 ? 0 : dir == 1 ? kNF0 : kNF0 + kNF1);
-      const int ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
+    for (int q = tid; q < NP; q += kTileThreads) {
+      const int ck = q % PK, cj = (q / PK) % PJ, ci = q / (PK * PJ);
+      const int x0 = it.o[0] - 1 + ci, x1 = it.o[1] - 1 + cj, x2 = it.o[2] - 1 + ck;
+      const int out = (ci == 0 || ci == T.i + 1) + (cj == 0 || cj == T.j + 1) + (ck == 0 || ck == T.k + 1);
+      if (!dt_ok || out > 1 || x0 < it.lo[0] - 1 || x0 > it.hi[0] || x1 < it.lo[1] - 1 || x1 > it.hi[1] ||
+          x2 < it.lo[2] - 1 || x2 > it.hi[2])
+        continue;
+      const R rho = AT(u0, x0, x1, x2), u = AT(pv0, x0, x1, x2), v = AT(pv0 + 1, x0, x1, x2),
+              w = AT(pv0 + 2, x0, x1, x2), p = AT(pv0 + 3, x0, x1, x2);
+      C[0][q] = rho;
+      C[1][q] = u;
+      C[2][q] = v;
+      C[3][q] = w;
+      C[4][q] = p;
+      C[5][q] = p / (g - R(1.0)) + R(0.5) * rho * (u * u + v * v + w * w);
+      C[6][q] = sqrt(dmax(R(0.0), g * p / dmax(rho, R(1e-30))));
+    }
+    __syncthreads();
+    // one face of direction dir (index f among that direction's faces, the
+    // slot gf of the tile's face array): the direction is a compile-time
+    // constant in each of the three instantiations, so the face grid's
+    // extents divide as constants
+    auto face = [&](auto dirc, int f, int gf) {
+      constexpr int dir = decltype(dirc)::value;
+      constexpr int ej = kTileJ + (dir == 1), ek = kTileK + (dir == 2);
       // the face's JD: FP32 reads the real-typed copy (k_face_normals), FP64
       // the metric itself (the same values; faster there)
-      const int cm = sizeof(R) == 4 ? cFM + 3 * dir : dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
-      const int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
+      constexpr int cm = sizeof(R) == 4 ? cFM + 3 * dir : dir == 0 ? cJDX : dir == 1 ? cJDY : cJDZ;
+      constexpr int cn = dir == 0 ? cFNX : dir == 1 ? cFNY : cFNZ;
       const int fk = f % ek, fj = (f / ek) % ej, fi = f / (ek * ej);
       const int x[3] = {it.o[0] + fi, it.o[1] + fj, it.o[2] + fk};
       bool need = dt_ok;
 #pragma unroll
       for (int a = 0; a < 3; ++a) need = need && x[a] >= it.lo[a] && x[a] < it.hi[a] + (a == dir);
-      if (need) {
-        int im = x[0], jm = x[1], km = x[2];
-        shift1(dir, im, jm, km, -1);
-        R Fl[5];
-        R k1, k2, k3;
-        if constexpr (sizeof(R) == 4) {
-          k1 = AT(cm, x[0], x[1], x[2]);
-          k2 = AT(cm + 1, x[0], x[1], x[2]);
-          k3 = AT(cm + 2, x[0], x[1], x[2]);
-        } else {
-          k1 = ATM(cm, x[0], x[1], x[2]);
-          k2 = ATM(cm + 1, x[0], x[1], x[2]);
-          k3 = ATM(cm + 2, x[0], x[1], x[2]);
-        }
-        rusanov(B, g, u0, pv0, k1, k2, k3, AT(cn + 3, x[0], x[1], x[2]), im, jm, km, x[0], x[1], x[2], Fl);
-#pragma unroll
-        for (int m = 0; m < 5; ++m) F[m][gf] = Fl[m];
+      if (!need) return;
+      R k1, k2, k3;
+      if constexpr (sizeof(R) == 4) {
+        k1 = AT(cm, x[0], x[1], x[2]);
+        k2 = AT(cm + 1, x[0], x[1], x[2]);
+        k3 = AT(cm + 2, x[0], x[1], x[2]);
+      } else {
+        k1 = ATM(cm, x[0], x[1], x[2]);
+        k2 = ATM(cm + 1, x[0], x[1], x[2]);
+        k3 = ATM(cm + 2, x[0], x[1], x[2]);
       }
+      // the face's right cell is (fi, fj, fk) of the tile, its left one step back along dir
+      const int qr = ((fi + 1) * PJ + (fj + 1)) * PK + (fk + 1);
+      const int ql = qr - (dir == 0 ? PJ * PK : dir == 1 ? PK : 1);
+      R Lv[7], Rv[7];
+#pragma unroll
+      for (int m = 0; m < 7; ++m) {
+        Lv[m] = C[m][ql];
+        Rv[m] = C[m][qr];
+      }
+      R Fl[5];
+      rusanov_staged(Lv, Rv, k1, k2, k3, AT(cn + 3, x[0], x[1], x[2]), Fl);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) F[m][gf] = Fl[m];
+    };
+    // The tile's face fluxes of all three directions in one pass, dealt
+    // round-robin over the threads (912 faces of a 16 x 4 x 4 tile take four
+    // rounds of 256; a warp straddles a direction change at most twice), then
+    // every cell takes its six faces' differences direction by direction, in
+    // Scheme_U_'s order.
+#pragma unroll 1
+    for (int gf = tid; gf < kTileFaces; gf += kTileThreads) {
+      if (gf < kNF0) face(std::integral_constant<int, 0>{}, gf, gf);
+      else if (gf < kNF0 + kNF1) face(std::integral_constant<int, 1>{}, gf - kNF0, gf);
+      else face(std::integral_constant<int, 2>{}, gf - kNF0 - kNF1, gf);
     }
     __syncthreads();
     if (it.in && dt_ok) {
@@ -1960,15 +2008,26 @@ static const void *fluid_fn(int v) {
 }
 static_assert(kNumFluidTiles == 6, "fluid_fn and launch_fluid list every variant");
 template <class R>
+static size_t fluid_smem(int v) {
+  switch (v) {
+    case 1: return FluidSmem<R, 1>::bytes;
+    case 2: return FluidSmem<R, 2>::bytes;
+    case 3: return FluidSmem<R, 3>::bytes;
+    case 4: return FluidSmem<R, 4>::bytes;
+    case 5: return FluidSmem<R, 5>::bytes;
+    default: return FluidSmem<R, 0>::bytes;
+  }
+}
+template <class R>
 static void launch_fluid(int v, const Dir &D, cudaStream_t st) {
   const int G = g_grid_fluid[(v >= 0 && v < kNumFluidTiles) ? v : 0];
   switch (v) {
-    case 1: k_fluid<R, 1><<<G, kTileThreads, 0, st>>>(D); break;
-    case 2: k_fluid<R, 2><<<G, kTileThreads, 0, st>>>(D); break;
-    case 3: k_fluid<R, 3><<<G, kTileThreads, 0, st>>>(D); break;
-    case 4: k_fluid<R, 4><<<G, kTileThreads, 0, st>>>(D); break;
-    case 5: k_fluid<R, 5><<<G, kTileThreads, 0, st>>>(D); break;
-    default: k_fluid<R, 0><<<G, kTileThreads, 0, st>>>(D); break;
+    case 1: k_fluid<R, 1><<<G, kTileThreads, FluidSmem<R, 1>::bytes, st>>>(D); break;
+    case 2: k_fluid<R, 2><<<G, kTileThreads, FluidSmem<R, 2>::bytes, st>>>(D); break;
+    case 3: k_fluid<R, 3><<<G, kTileThreads, FluidSmem<R, 3>::bytes, st>>>(D); break;
+    case 4: k_fluid<R, 4><<<G, kTileThreads, FluidSmem<R, 4>::bytes, st>>>(D); break;
+    case 5: k_fluid<R, 5><<<G, kTileThreads, FluidSmem<R, 5>::bytes, st>>>(D); break;
+    default: k_fluid<R, 0><<<G, kTileThreads, FluidSmem<R, 0>::bytes, st>>>(D); break;
   }
 }
 
@@ -2022,7 +2081,11 @@ static void grids_init() {
   }
   for (int v = 0; v < kNumFluidTiles; ++v) {
     int per_sm = 8;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fluid_fn<R>(v), kTileThreads, 0) != cudaSuccess ||
+    // the staged cells and face fluxes are dynamic shared memory (above the
+    // 48 KB default in FP64)
+    cudaFuncSetAttribute(fluid_fn<R>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fluid_smem<R>(v));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fluid_fn<R>(v), kTileThreads, fluid_smem<R>(v)) !=
+            cudaSuccess ||
         per_sm < 1) {
       cudaGetLastError();
       per_sm = 1;

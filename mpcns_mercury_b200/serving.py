@@ -162,14 +162,22 @@ class Server:
                                                     req.fields[name].hi) for name in STATE_FIELDS}
         self.batch.remove(req.slot)
 
-    def _bytes(self, req: Request, precision: int) -> int:
+    @staticmethod
+    def _bytes(req: Request, precision: int, topology=None) -> int:
+        """Device bytes of the request's solve (a shell's from its grid's
+        topology: the given handle, else one built and freed here)."""
         if req.case is not None:
             from . import magnetosphere as M
 
-            topo, _ = self._shell_grid(req.case)
+            own = topology is None
+            topo = M.topology(req.case) if own else topology
             d = capi.SolveDesc(req.case.cells, NGHOST, M.constants(req.case), precision=precision, topology=topo)
-        else:
-            d = capi.SolveDesc([req.cells], NGHOST, reference_constants(), precision=precision)
+            b = d.device_bytes()
+            d.close()
+            if own:
+                capi.lib().mhd_topology_destroy(topo)
+            return b
+        d = capi.SolveDesc([req.cells], NGHOST, reference_constants(), precision=precision)
         b = d.device_bytes()
         d.close()
         return b
@@ -177,7 +185,8 @@ class Server:
     def _need(self, req: Request) -> int:
         key = _geometry_key(req)
         if key not in self.grid_bytes:
-            self.grid_bytes[key] = self._bytes(req, self.precision)
+            topo = self._shell_grid(req.case)[0] if req.case is not None else None
+            self.grid_bytes[key] = self._bytes(req, self.precision, topo)
         return self.grid_bytes[key]
 
     # ------------------------------------------------------------------ the loop

@@ -79,7 +79,7 @@ def test_fluid_tile_shapes_and_shape_classes():
 
     shapes = [capi.fluid_tile_shape(v) for v in range(capi.NUM_FLUID_TILES)]
     assert shapes[0] == (16, 4, 4, 3)
-    assert all(k * j * i == 256 and ctas in (2, 3) for k, j, i, ctas in shapes)
+    assert all(k * j * i == 256 and ctas in (2, 3, 4) for k, j, i, ctas in shapes)
     assert len(set(shapes)) == len(shapes)
     with pytest.raises(capi.MhdError):
         capi.fluid_tile_shape(capi.NUM_FLUID_TILES)

@@ -84,7 +84,7 @@ def _server(monkeypatch, capacity, budget, per_solve):
     monkeypatch.setattr(SV.capi, "Batch", FakeBatch)
     monkeypatch.setattr(SV.capi, "SolveDesc", FakeDesc)
     monkeypatch.setattr(SV, "upload_request", lambda *a, **k: 0)
-    monkeypatch.setattr(SV.Server, "_bytes", staticmethod(lambda req, prec: per_solve))
+    monkeypatch.setattr(SV.Server, "_bytes", staticmethod(lambda req, prec, topology=None: per_solve))
     return SV.Server(capacity=capacity, precision=0, hbm_budget=budget, chunk_steps=4)
 
 
