@@ -1496,7 +1496,51 @@ static int upload_phys(Solve *S, const mhd_desc *desc, cudaStream_t st) {
       if (!ok2) return fail(MHD_ERR_ARG, "physical operation %d of table %d: source out of range", t, q);
       other.push_back(d);
     }
-    S->T->ph_nset[q] = (int)set.size();
+    // the constant writes as segments: runs of up to 32 consecutive
+    // destinations of one value, runs of equal length and value whose starts
+    // step by one stride merged up to 32 elements (the ghost rows of a
+    // farfield slab); two words each (start | value index, shape)
+    std::sort(set.begin(), set.end(), [](int64_t a, int64_t b) {
+      const int64_t m = ~(int64_t(31) << kPhysArgShift);
+      return (a & m) < (b & m);
+    });
+    std::vector<int64_t> segs;
+    {
+      const int64_t amask = int64_t(31) << kPhysArgShift, es = S->es;
+      struct Run { int64_t start; int64_t arg; int len; };
+      std::vector<Run> runs;
+      for (int64_t w : set) {
+        const int64_t c = w & ~amask, a = w & amask;
+        if (!runs.empty()) {
+          Run &r = runs.back();
+          if (r.arg == a && r.len < 32 && c == r.start + r.len * es) {
+            ++r.len;
+            continue;
+          }
+        }
+        runs.push_back(Run{c, a, 1});
+      }
+      for (size_t t = 0; t < runs.size();) {
+        const Run &r0 = runs[t];
+        size_t u = t + 1;
+        int64_t stride = 0;
+        while (u < runs.size() && (int)(u - t + 1) * r0.len <= 32 && runs[u].arg == r0.arg && runs[u].len == r0.len) {
+          const int64_t d = runs[u].start - runs[u - 1].start;
+          if (u == t + 1) {
+            if (d <= 0 || d >= (int64_t(1) << 46)) break;
+            stride = d;
+          } else if (d != stride) {
+            break;
+          }
+          ++u;
+        }
+        segs.push_back(r0.start | r0.arg);
+        segs.push_back((int64_t)(r0.len - 1) | ((int64_t)(u - t - 1) << 8) | (stride << 16));
+        t = u;
+      }
+    }
+    set.swap(segs);
+    S->T->ph_nset[q] = (int)set.size() / 2;
     S->T->ph_nop[q] = (int)other.size();
     S->T->table_bytes += (int64_t)set.size() * 8 + (int64_t)other.size() * sizeof(DevPhysOp);
     int rc;

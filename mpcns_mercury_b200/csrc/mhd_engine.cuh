@@ -185,7 +185,7 @@ struct DevPhysOp {
   int kind, nghost;
 };
 struct DevPhys {
-  const int64_t *set = nullptr;
+  const int64_t *set = nullptr;  // nset segments of constant writes, two words each
   const DevPhysOp *op = nullptr;
   int nset = 0, nop = 0;
 };

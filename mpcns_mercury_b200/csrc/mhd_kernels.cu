@@ -1718,10 +1718,15 @@ __global__ void __launch_bounds__(256) k_phys(Dir D, int which) {
     const ConstsT<R> &c = consts_of<R>(S);
     const int cur = D.state[s].cur;
     const int q = e - pre[s];
-    if (q < P.nset) {  // dst <- bc[arg]
-      const int64_t w = P.set[q];
-      const int arg = (int)((w >> kPhysArgShift) & 31);
-      *at_code<R>(S, cur, w & ~(int64_t(31) << kPhysArgShift)) = c.bc[arg];
+    if (q < P.nset) {  // a segment of destinations <- bc[arg]: nr runs of len elements, stride bytes apart
+      const int64_t w0 = P.set[2 * q], w1 = P.set[2 * q + 1];
+      const int arg = (int)((w0 >> kPhysArgShift) & 31);
+      const int len = (int)(w1 & 255) + 1, nr = (int)((w1 >> 8) & 255) + 1;
+      const int64_t stride = w1 >> 16;
+      char *p0 = (char *)at_code<R>(S, cur, w0 & ~(int64_t(31) << kPhysArgShift));
+      const R v = c.bc[arg];
+      for (int r = 0; r < nr; ++r)
+        for (int e = 0; e < len; ++e) *(R *)(p0 + r * stride + (int64_t)e * (int64_t)sizeof(R)) = v;
       continue;
     }
     const DevPhysOp &op = P.op[q - P.nset];
