@@ -133,15 +133,20 @@ typedef struct mhd_constants {
    * Solved to ||A E - b|| <= res_rtol ||b||, else MHD_ERR_SOLVE.  FP64
    * solves: preconditioned CG (at most res_max_it iterations, capped at
    * 100000; res_rtol 0 = 1e-13), its iteration loop run on the device as a
-   * CUDA graph with a conditional loop node.  Mixed-precision solves: iterative refinement with the residual
-   * A E - b and its norms in FP64 and each correction solved by FP32 CG (on
-   * the solve's own FP32 edge fields) to 1e-4 of its right-hand side (at most
-   * res_max_it iterations each, at most 30 refinements; res_rtol 0 = 1e-10). */
+   * CUDA graph with a conditional loop node.  Mixed-precision solves
+   * (res_rtol 0 = 1e-10) on the solve's FP64 companion fields: while the
+   * previous substep took at most res_direct_iters iterations, FP64 CG there;
+   * after a longer one, iterative refinement with the residual A E - b and
+   * its norms in FP64 and each correction solved by FP32 CG (on the solve's
+   * own FP32 edge fields) to 1e-4 of its right-hand side (at most res_max_it
+   * iterations each, at most 30 refinements). */
   double res_rtol;
   int32_t resistive;  /* is_Mercury_resistance */
   int32_t res_max_it;
   /* values of the physical boundary operations (mhd_bc_const) */
   double bc[MHD_NUM_BC];
+  int32_t res_direct_iters; /* 0 = 20; negative: always iterative refinement */
+  int32_t pad_;
 } mhd_constants;
 
 /* One DOF reference in the FieldBlock index space. */

@@ -72,7 +72,8 @@ class MhdConstants(ctypes.Structure):
         "momentum_induce_coeff", "momentum_hall_coeff", "inver_MA2", "ne_hall_floor",
         "arti_eta_max", "arti_J_start", "arti_J_on")] + [
         ("ambipolar", ctypes.c_int32), ("local_arti", ctypes.c_int32), ("res_rtol", ctypes.c_double),
-        ("resistive", ctypes.c_int32), ("res_max_it", ctypes.c_int32), ("bc", ctypes.c_double * 19)]
+        ("resistive", ctypes.c_int32), ("res_max_it", ctypes.c_int32), ("bc", ctypes.c_double * 19),
+        ("res_direct_iters", ctypes.c_int32), ("pad_", ctypes.c_int32)]
 
 
 # indices into MhdConstants.bc (enum mhd_bc_const)

@@ -15,7 +15,7 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
                         M_H: float = 0.001, M_Na: float = 0.023, arti_eta_max: float = 0.0,
                         arti_J_start: float = 800.0, arti_J_on: float = 3000.0,
                         local_arti: bool = False, resistive: bool = False, res_rtol: float = 1e-13,
-                        res_max_it: int = 500, initial=None) -> MhdConstants:
+                        res_max_it: int = 500, res_direct_iters: int = 0, initial=None) -> MhdConstants:
     if initial is None:
         initial = DEFAULT_INITIAL
     c = MhdConstants()
@@ -52,6 +52,9 @@ def reference_constants(cfl: float = 0.4, ambipolar: bool = True, gamma: float =
     c.resistive = 1 if resistive else 0
     c.res_rtol = res_rtol
     c.res_max_it = res_max_it
+    # mixed precision: FP64 CG while the last substep took at most this many
+    # iterations (0: 20), iterative refinement after a longer one (negative: always)
+    c.res_direct_iters = res_direct_iters
     set_boundary(c, gamma=gamma, NA=NA, R_uni=R_uni, U_ref=U_ref, T_ref=T_ref, n_ref=n_ref, M_ref=M_ref,
                  B_ref=B_ref, initial=initial)
     return c

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstddef>
@@ -153,6 +154,10 @@ struct Tables {
   double *al_msign = nullptr, *al_osign = nullptr;
   int al_n = 0;
   int64_t table_bytes = 0;
+  // The implicit substep's k bound: the largest source k of any E / dB / dJ
+  // copy, alias or singular-edge record that carries a value to a lower k
+  // (-1: every one keeps k or raises it; INT_MAX: unknown, no restriction)
+  int res_kdown = INT_MAX;
 };
 
 struct Solve {
@@ -170,12 +175,17 @@ struct Solve {
   Tables *T = nullptr;
   double res_rtol = 0.0;
   int res_max_it = 0;
+  int res_direct = 0;  // mixed precision: FP64 CG while the last substep took at most this many iterations
   // mixed precision with the implicit resistive substep: slot of the FP64
   // companion solve (same blocks and tables) in the batch's companion batch
   int shadow_slot = -1;
   // the last implicit resistive substep (mhd_info)
   double res_relres = 0.0;
   int res_iters = 0, res_refinements = 0;
+  // the implicit substep's work range kResK (set at prepare): its tile
+  // prefix over the blocks and count; null: the whole owned box (kBox)
+  int *dres_prefix = nullptr;
+  int res_tiles = 0;
   Consts consts{};
 
   int comp_bytes(int c) const { return is_metric(c) ? 8 : es; }
@@ -452,7 +462,10 @@ int publish(mhd_batch *b) {
   };
   int rc;
   for (int r = 0; r < kNumRanges; ++r)
-    if ((rc = put(b->dprefix_tiles[r], [&](const Solve *S) { return S->T->tiles[r]; }))) return rc;
+    if ((rc = put(b->dprefix_tiles[r], [&](const Solve *S) {
+           return r == kResK && S->dres_prefix ? S->res_tiles : S->T->tiles[r];
+         })))
+      return rc;
   for (int g = 0; g < kMaxGroups; ++g)
     for (int p = 0; p < kNumPhases; ++p)
       if ((rc = put(b->dprefix_copy[g][p], [&](const Solve *S) { return S->T->tab_n[g][p]; }))) return rc;
@@ -474,6 +487,7 @@ int publish(mhd_batch *b) {
     d.ubuf = S->ubuf;
     d.nblocks = S->nblocks;
     for (int r = 0; r < kNumRanges; ++r) d.tile_prefix[r] = S->T->dtile_prefix[r];
+    if (S->dres_prefix) d.tile_prefix[kResK] = S->dres_prefix;
     for (int g = 0; g < kMaxGroups; ++g)
       for (int p = 0; p < kNumPhases; ++p) d.tab[g][p] = DevTable{S->T->tab_seg[g][p], S->T->tab_n[g][p]};
     for (int q = 0; q < kNumPhys; ++q)
@@ -902,6 +916,7 @@ void free_solve(Solve *S, cudaStream_t st) {
   f(S->dblocks);
   f(S->sg_geo);
   f(S->sg_w);
+  f(S->dres_prefix);
   Tables *T = S->T;
   if (T && --T->users == 0) {
     for (int r = 0; r < kNumRanges; ++r) f(T->dtile_prefix[r]);
@@ -1129,13 +1144,19 @@ int res_cg(mhd_batch *b, double tol_factor, int max_it, double *r0, double *rnor
   return MHD_OK;
 }
 
-// The mixed-precision solve of (I + dt eta alpha C^T beta C) E = b by
-// iterative refinement: the residual r = b - A x and its norms in FP64 on
-// the solve's FP64 companion (widened alpha, beta, eta, W; its own copies of
-// the E / B / J syncs), each correction A d = r solved by FP32 CG on the
-// solve's own arrays to 1e-4 of ||r||, x += d in FP64.  b = eta J(B*) is the
-// FP32 step's current (the state is FP32).  On return the solve's x holds
-// the solution rounded to FP32.
+// The mixed-precision solve of (I + dt eta alpha C^T beta C) E = b on the
+// solve's FP64 companion (widened alpha, beta, eta, W; its own copies of the
+// E / B / J syncs); b = eta J(B*) is the FP32 step's current (the state is
+// FP32).  While the previous substep took at most res_direct iterations
+// the companion runs the CG itself in FP64 (one host round trip); after a
+// longer one, iterative refinement: the residual r = b - A x and its norms in
+// FP64 on the companion, each correction A d = r solved by FP32 CG on the
+// solve's own arrays to 1e-4 of ||r||, x += d in FP64 (half the bytes per
+// iteration, two more round trips and an FP64 operator per refinement).  On
+// return the solve's x holds the solution rounded to FP32.
+constexpr int kDirectIters = 20;
+int direct_iters(const mhd_constants &k) { return k.res_direct_iters == 0 ? kDirectIters : k.res_direct_iters; }
+
 int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
   mhd_batch *sh = b->shadow;
   const int cs = S->shadow_slot;
@@ -1155,9 +1176,20 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
   if (S->T->sg_n > 0)  // the singular edges' canonical vectors and inverse Hodge stars (FP64 in both)
     CUDA_TRY(cudaMemcpyAsync(C->sg_geo, S->sg_geo, sizeof(double) * 4 * S->T->sg_n, cudaMemcpyDeviceToDevice, st));
   if ((rc = set_state_field(sh, cs, offsetof(SolveState, mask), &one, sizeof one))) return rc;
+  const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-10;
+  if (S->res_direct >= 0 && S->res_iters <= S->res_direct) {
+    // a short solve: FP64 CG on the companion from x = 0, p = r = b
+    launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
+    double r0 = 0.0, rn = 0.0;
+    if ((rc = res_cg(sh, rtol, S->res_max_it, &r0, &rn, &S->res_iters, converged))) return rc;
+    S->res_refinements = 0;
+    S->res_relres = r0 > 0.0 ? rn / r0 : 0.0;
+    launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_X, st);
+    CUDA_TRY(cudaGetLastError());
+    return set_state_field(sh, cs, offsetof(SolveState, mask), &zero, sizeof zero);
+  }
   if ((rc = res_dot(sh, RES_DOT_RR))) return rc;
   const double bnorm = std::sqrt(sh->hres[1]);
-  const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-10;
   double rn = bnorm;
   S->res_iters = 0;
   S->res_refinements = 0;
@@ -1444,6 +1476,53 @@ static Consts make_consts(const mhd_constants &k, int nghost) {
 
 // The physical boundary operations of every group and the wall EMF, encoded
 // as arena codes (MHD_PHYS_SET: one word; the others DevPhysOp).
+// The largest k whose value an E_res / dB / dJ copy (halo, owner, or staged
+// through a slot), an edge alias class or a singular-edge record carries to a
+// lower k; -1 when none does (the radial index of a shell: every copy keeps
+// k, the inner boundary's copies reach k < 0 from the first layers).  The
+// implicit substep then computes only k below this bound + 2 and below its
+// unknowns' top + 2: no value it needs comes from above.
+static int res_kdown(const mhd_desc *desc) {
+  int m = -1;
+  auto flow = [&](int src_k, int dst_k) {
+    if (src_k > dst_k) m = std::max(m, src_k);
+  };
+  for (int g : {(int)MHD_SYNC_ERES, (int)MHD_SYNC_DB, (int)MHD_SYNC_JEDGE}) {
+    const mhd_sync_group &G = desc->groups[g];
+    for (int t = 0; t < G.n_halo; ++t) flow(G.halo[t].src.k, G.halo[t].dst.k);
+    for (int t = 0; t < G.n_owner; ++t) flow(G.owner[t].src.k, G.owner[t].dst.k);
+    if (G.n_stash > 0 && G.stash) {
+      std::unordered_map<int, int> slot_k;  // staging slot -> the k it was filled from
+      for (int t = 0; t < G.n_stash; ++t) slot_k[G.stash[t].dst.i] = G.stash[t].src.k;
+      for (int t = 0; t < G.n_stash; ++t) {
+        const mhd_copy &c = G.stash[G.n_stash + t];
+        auto it = slot_k.find(c.src.i);
+        if (it == slot_k.end()) return INT_MAX;
+        flow(it->second, c.dst.k);
+      }
+    }
+  }
+  const mhd_alias_classes &a = desc->edge_aliases;
+  if (a.n_classes > 0 && a.offset && a.member && a.owner)
+    for (int c = 0; c < a.n_classes; ++c) {
+      int lo = a.owner[c].k, hi = lo;
+      for (int q = a.offset[c]; q < a.offset[c + 1]; ++q) {
+        lo = std::min(lo, a.member[q].k);
+        hi = std::max(hi, a.member[q].k);
+      }
+      flow(hi, lo);
+    }
+  const mhd_singular_edges &g = desc->singular;
+  if (g.n_edges > 0 && g.owner && g.alias_offset && g.aliases && g.cell_offset && g.cells && g.face_offset && g.faces)
+    for (int e = 0; e < g.n_edges; ++e) {
+      const int k = g.owner[e].k;
+      for (int q = g.alias_offset[e]; q < g.alias_offset[e + 1]; ++q) flow(g.aliases[q].edge.k, k);
+      for (int q = g.cell_offset[e]; q < g.cell_offset[e + 1]; ++q) flow(g.cells[q].cell.k, k);
+      for (int q = g.face_offset[e]; q < g.face_offset[e + 1]; ++q) flow(g.faces[q].face.k, k);
+    }
+  return m;
+}
+
 static int upload_phys(Solve *S, const mhd_desc *desc, cudaStream_t st) {
   for (int q = 0; q < kNumPhys; ++q) {
     const mhd_phys_op *ops = q < kMaxGroups ? desc->groups[q].phys : desc->wall;
@@ -1724,6 +1803,7 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
     d.G = bx.G;
     for (int a = 0; a < 3; ++a) d.n[a] = bx.n[a];
     d.solve = slot;
+    d.reskhi = bx.n[2] + 1;
   }
   int rc;
   if ((rc = dev_upload(S->pool, blocks, &S->dblocks, st))) return bail(rc);
@@ -1739,6 +1819,7 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
       if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
       if ((rc = upload_phys(S, desc, st))) return bail(rc);
       if ((rc = upload_singular(S, desc->singular, st)) || (rc = alloc_singular_geo(S, st))) return bail(rc);
+      if (S->consts.resistive) S->T->res_kdown = res_kdown(desc);
     }
   } catch (...) {  // host allocation or thread creation failed
     return bail(fail(MHD_ERR_OOM, "host memory for the copy tables"));
@@ -1748,6 +1829,7 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
   S->res_rtol = k.res_rtol;
   S->res_max_it = k.res_max_it;
+  S->res_direct = direct_iters(k);
   b->slots[slot] = S;
   if (S->consts.resistive) ++b->n_res;
   const bool grew = count_tables(b, S, +1);
@@ -1847,6 +1929,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
     d.G = bx.G;
     for (int a = 0; a < 3; ++a) d.n[a] = bx.n[a];
     d.solve = slot;
+    d.reskhi = bx.n[2] + 1;
   }
   if ((rc = dev_upload(S->pool, blocks, &S->dblocks, st))) return bail(rc);
   SolveState s0{};
@@ -1854,6 +1937,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
   if ((rc = set_state_field(b, slot, 0, &s0, sizeof s0))) return bail(rc);
   S->res_rtol = constants ? constants->res_rtol : src->res_rtol;
   S->res_max_it = constants ? constants->res_max_it : src->res_max_it;
+  S->res_direct = constants ? direct_iters(*constants) : src->res_direct;
   b->slots[slot] = S;
   if (S->consts.resistive) ++b->n_res;
   if (count_tables(b, S, +1)) {  // not reached while the template itself is in the batch
@@ -1936,6 +2020,7 @@ int mhd_batch_set_constants(mhd_batch *b, int slot, const mhd_constants *constan
   S->consts = make_consts(*constants, S->nghost);
   S->res_rtol = constants->res_rtol;
   S->res_max_it = constants->res_max_it;
+  S->res_direct = direct_iters(*constants);
   S->prepared = false;
   if ((rc = publish(b))) return rc;
   if (S->shadow_slot >= 0 && b->shadow) return mhd_batch_set_constants(b->shadow, S->shadow_slot, constants);
@@ -2051,6 +2136,64 @@ int mhd_batch_sync(mhd_batch *b, int slot, int group) {
   return targeted(b, slot, [&](int *nk) { enqueue_sync(b, 1, group, nk, true); });  // asynchronous
 }
 
+// The implicit substep's work range of one solve (kResK), after its
+// unknowns are marked: per block k < min(n_k + 1, R), R = 2 + the larger of
+// the unknowns' top k (over the blocks) and the tables' k bound (res_kdown).
+// Every value the substep computes for its unknowns then lies in the range,
+// bit for bit as over the whole box; above it E_res stays 0 and B does not
+// change.  The FP64 companion of a mixed solve takes the same range.  One
+// host round trip (the unknowns are known on the device only).
+static int apply_res_range(mhd_batch *b, Solve *S, const std::vector<int> &hi) {
+  bool whole = true;
+  for (int bi = 0; bi < S->nblocks; ++bi) whole = whole && hi[bi] == S->boxes[bi].n[2] + 1;
+  cudaStream_t st = b->stream;
+  if (S->dres_prefix) {
+    CUDA_TRY(cudaFreeAsync(S->dres_prefix, st));
+    S->dres_prefix = nullptr;
+  }
+  S->res_tiles = 0;
+  std::vector<int> prefix(1, 0);
+  for (int bi = 0; bi < S->nblocks; ++bi) {
+    CUDA_TRY(cudaMemcpyAsync(&S->dblocks[bi].reskhi, &hi[bi], sizeof(int), cudaMemcpyHostToDevice, st));
+    RangeBox r = range_of(kResK, S->boxes[bi].n, S->nghost);
+    r.hi[2] = hi[bi];
+    prefix.push_back(prefix.back() + tiles_of(r, kResK));
+  }
+  if (!whole) {
+    int rc = dev_upload(S->pool, prefix, &S->dres_prefix, st);
+    if (rc) return rc;
+    S->res_tiles = prefix.back();
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));  // the host values above are staged
+  return publish(b);
+}
+
+static int res_range(mhd_batch *b, int slot) {
+  Solve *S = b->slots[slot];
+  int *dk = nullptr;
+  CUDA_TRY(cudaMallocFromPoolAsync((void **)&dk, sizeof(int) * S->nblocks, b->pool, b->stream));
+  CUDA_TRY(cudaMemsetAsync(dk, 0xff, sizeof(int) * S->nblocks, b->stream));  // -1
+  const int one = 1, zero = 0;
+  int rc = set_state_field(b, slot, offsetof(SolveState, mask), &one, sizeof one);
+  if (rc) return rc;
+  launch_res_kmax(b->dir(1), b->precision, dk, b->stream);
+  CUDA_TRY(cudaGetLastError());
+  if ((rc = set_state_field(b, slot, offsetof(SolveState, mask), &zero, sizeof zero))) return rc;
+  std::vector<int> kmax(S->nblocks, -1);
+  CUDA_TRY(cudaMemcpyAsync(kmax.data(), dk, sizeof(int) * S->nblocks, cudaMemcpyDeviceToHost, b->stream));
+  CUDA_TRY(cudaFreeAsync(dk, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  int top = -1;
+  for (int k : kmax) top = std::max(top, k);
+  const int kd = S->T->res_kdown;
+  const int64_t R = kd == INT_MAX ? INT64_MAX : (int64_t)std::max(top, kd) + 2;
+  std::vector<int> hi(S->nblocks);
+  for (int bi = 0; bi < S->nblocks; ++bi) hi[bi] = (int)std::min<int64_t>(S->boxes[bi].n[2] + 1, R);
+  if ((rc = apply_res_range(b, S, hi))) return rc;
+  if (S->shadow_slot >= 0 && b->shadow) return apply_res_range(b->shadow, b->shadow->slots[S->shadow_slot], hi);
+  return MHD_OK;
+}
+
 int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   int rc = slot_check(b, slot);
   if (rc) return rc;
@@ -2073,6 +2216,7 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
     enqueue_derived(b, 1, nk);
   });
   if (rc) return rc;
+  if (res && (rc = res_range(b, slot))) return rc;
   b->slots[slot]->prepared = true;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
 }

@@ -45,13 +45,16 @@ enum RangeKind : int {
   kAlloc = 3,    // [-gs, n + gs), gs = min(nghost, kStepGhost): the ghost cells the step maintains
   kCells2 = 4,   // owned cells in fluid tiles of variant 0, two work items per tile (one per ion species)
   kFull = 5,     // [-(g + 1), n + g + 2): the whole box
-  // owned cells in fluid tiles of variants 1 .. kNumFluidTiles - 1
-  kNumRanges = 6 + kNumFluidTiles - 1
+  // owned cells in fluid tiles of variants 1 .. kNumFluidTiles - 1 (kinds 6 ..)
+  // [0, n + 1) with k below the block's reskhi: the implicit substep's work
+  // (its unknowns and the faces and edges they reach)
+  kResK = 6 + kNumFluidTiles - 1,
+  kNumRanges = kResK + 1
 };
 // The range kind of fluid tile variant v, and the variant of a range kind (-1: none).
 __host__ __device__ constexpr int fluid_kind(int v) { return v == 0 ? (int)kCells2 : (int)kFull + v; }
 __host__ __device__ constexpr int fluid_variant(int kind) {
-  return kind == kCells2 ? 0 : (kind > kFull && kind < kNumRanges ? kind - kFull : -1);
+  return kind == kCells2 ? 0 : (kind > kFull && kind < kResK ? kind - kFull : -1);
 }
 
 // Ghost depth the step keeps valid between its passes: the widest stencil
@@ -88,6 +91,7 @@ struct DevBlock {
   int64_t total, si, sj;
   int G, n[3];
   int solve;          // index of the owning solve in the directory
+  int reskhi;         // the implicit substep's k bound (exclusive) of range kResK; n[2] + 1: the whole box
 };
 
 // Per-solve constants, as calc_physical_constant derives them
@@ -257,7 +261,8 @@ __host__ __device__ inline RangeBox range_of(int kind, const int n[3], int g) {
   for (int a = 0; a < 3; ++a) {
     switch (kind) {
       case kCells: r.lo[a] = 0; r.hi[a] = n[a]; break;
-      case kBox: r.lo[a] = 0; r.hi[a] = n[a] + 1; break;
+      case kBox:
+      case kResK: r.lo[a] = 0; r.hi[a] = n[a] + 1; break;  // kResK: k clamped per block where it is used
       case kExt: r.lo[a] = -1; r.hi[a] = n[a] + 2; break;
       case kFull: r.lo[a] = -(g + 1); r.hi[a] = n[a] + g + 2; break;
       case kAlloc: {

@@ -141,7 +141,8 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
     if (!solve_active(D, s)) continue;  // inactive solve (the whole CTA agrees)
     const DevSolve &S = D.solves[s];
     const DevBlock &DB = S.blocks[b];
-    const RangeBox r = range_of(KIND, DB.n, S.c.nghost);
+    RangeBox r = range_of(KIND, DB.n, S.c.nghost);
+    if constexpr (KIND == kResK) r.hi[2] = DB.reskhi;
     Item it;
     it.s = s;
     it.blk = b;
@@ -1046,10 +1047,25 @@ __global__ void __launch_bounds__(kTileThreads) k_res_w(Dir D) {
   });
 }
 
+// Per block of the masked solve: the largest k of an edge with W > 0 (out
+// starts at -1).  The substep's work range kResK ends two layers above it:
+// the faces below the unknowns' top layer read E_res one layer up, the
+// current on the unknowns reads those faces.
+template <class R>
+__global__ void __launch_bounds__(kTileThreads) k_res_kmax(Dir D, int *out) {
+  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    const int o = it.in ? B.off(it.i, it.j, it.k) : 0;
+    const bool dof = it.in && (B.c(cRW)[o] > R(0.0) || B.c(cRW + 1)[o] > R(0.0) || B.c(cRW + 2)[o] > R(0.0));
+    int k = dof ? it.k : -1;
+    for (int of = 16; of > 0; of >>= 1) k = max(k, __shfl_xor_sync(0xffffffffu, k, of));
+    if ((threadIdx.x & 31) == 0 && k >= 0) atomicMax(out + it.blk, k);
+  });
+}
+
 // Vector operations of the CG on the unknowns (W > 0); other entries stay 0.
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op, double s) {
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
@@ -1091,7 +1107,7 @@ __global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op, double 
 // Z4_Mercury/src/operators/CTOperators.cpp:6-56; MatMultImplicitResistive_, :420-445).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_db(Dir D) {
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const R m = R(-D.state[it.s].dt);
     const int i = it.i, j = it.j, k = it.k;
@@ -1108,7 +1124,7 @@ __global__ void __launch_bounds__(kTileThreads) k_res_db(Dir D) {
 // Mercury_ImplicitResistive.cpp:314-393; CTOperators.cpp:59-110).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_dj(Dir D) {
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int i = it.i, j = it.j, k = it.k;
     if (i < B.n0) {
@@ -1149,7 +1165,7 @@ __global__ void __launch_bounds__(kTileThreads) k_res_clearb(Dir D) {
 // q = A p = E_res - eta dJ on the unknowns (MatMultImplicitResistive_, :446-468).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_q(Dir D) {
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
@@ -1165,7 +1181,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_dot(Dir D, int op, double *partial) {
   __shared__ double sh[2][kTileThreads / 32];
   double acc0 = 0.0, acc1 = 0.0;
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
@@ -1228,7 +1244,7 @@ __global__ void __launch_bounds__(kTileThreads) k_res_cg(Dir D, int op, double *
   const R alpha = R(cg->alpha);
   double acc0 = 0.0, acc1 = 0.0;
   if (!skip)
-    for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+    for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
       if (!it.in) return;
       const int o = B.off(it.i, it.j, it.k);
       for (int a = 0; a < 3; ++a) {
@@ -1341,7 +1357,7 @@ template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_pupd_e(Dir D, const ResCG *cg) {
   if (cg->done) return;
   const R beta = R(cg->beta);
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
@@ -1371,15 +1387,17 @@ __global__ void __launch_bounds__(kTileThreads) k_res_copyb(Dir D, int op) {
 // ApplyUpdate_Euler_BfaceOnly_, Z4_Mercury/src/physics/MercurySolver_MagExplicit_Hall.cpp:435-473).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_bupdate(Dir D) {
-  for_items<R, kBox>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const R dt = R(D.state[it.s].dt);
     const int i = it.i, j = it.j, k = it.k;
-    if (j < B.n1 && k < B.n2) {
+    // the faces whose edges E_res covers (k + 1 below the range's bound);
+    // above them E_res is 0 and B does not change
+    if (j < B.n1 && k + 1 < it.hi[2]) {
       const R rb = R(-1.0) * ((AT(cEY, i, j, k) - AT(cEY, i, j, k + 1)) + (AT(cEZ, i, j + 1, k) - AT(cEZ, i, j, k)));
       AT(cBX, i, j, k) += dt * rb;
     }
-    if (i < B.n0 && k < B.n2) {
+    if (i < B.n0 && k + 1 < it.hi[2]) {
       const R rb = R(-1.0) * ((AT(cEX, i, j, k + 1) - AT(cEX, i, j, k)) + (AT(cEZ, i, j, k) - AT(cEZ, i + 1, j, k)));
       AT(cBY, i, j, k) += dt * rb;
     }
@@ -1704,32 +1722,52 @@ template <class R>
 __global__ void __launch_bounds__(256) k_phys(Dir D, int which) {
   const int *pre = D.phys_prefix[which];
   const int total = pre[D.nsolves];
-  // the CTA takes chunks of kChunk consecutive operations (one solve lookup
-  // per chunk; a thread's solve is found by stepping forward from it)
-  constexpr int kChunk = 2048;
-  for (int c0 = blockIdx.x * kChunk; c0 < total; c0 += gridDim.x * kChunk) {
-  const int s0 = find_solve(pre, D.nsolves, c0);
-  for (int e = c0 + (int)threadIdx.x; e < c0 + kChunk && e < total; e += blockDim.x) {
-    int s = s0;
-    while (s + 1 < D.nsolves && pre[s + 1] <= e) ++s;
-    if (!solve_active(D, s)) continue;
-    const DevSolve &S = D.solves[s];
-    const DevPhys &P = S.phys[which];
-    const ConstsT<R> &c = consts_of<R>(S);
-    const int cur = D.state[s].cur;
-    const int q = e - pre[s];
-    if (q < P.nset) {  // a segment of destinations <- bc[arg]: nr runs of len elements, stride bytes apart
-      const int64_t w0 = P.set[2 * q], w1 = P.set[2 * q + 1];
-      const int arg = (int)((w0 >> kPhysArgShift) & 31);
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  // a warp takes 32 consecutive operations, one per lane; the constant
+  // segments among them are then written by the whole warp, one element per
+  // lane (consecutive destinations to consecutive lanes)
+  for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < total; base += nwarps * 32) {
+    const int e = base + lane;
+    unsigned long long seg_p = 0;  // the segment's first destination (0: not a segment)
+    int64_t seg_w = 0;
+    R seg_v = R(0.0);
+    const DevPhysOp *opp = nullptr;
+    const DevSolve *Sp = nullptr;
+    int cur = 0;
+    if (e < total) {
+      const int s = find_solve(pre, D.nsolves, e);
+      if (solve_active(D, s)) {
+        Sp = &D.solves[s];
+        const DevPhys &P = Sp->phys[which];
+        cur = D.state[s].cur;
+        const int q = e - pre[s];
+        if (q < P.nset) {  // destinations <- bc[arg]: nr runs of len elements, stride bytes apart
+          const int64_t w0 = P.set[2 * q];
+          seg_w = P.set[2 * q + 1];
+          seg_v = consts_of<R>(*Sp).bc[(int)((w0 >> kPhysArgShift) & 31)];
+          seg_p = (unsigned long long)at_code<R>(*Sp, cur, w0 & ~(int64_t(31) << kPhysArgShift));
+        } else {
+          opp = &P.op[q - P.nset];
+        }
+      }
+    }
+    for (unsigned m = __ballot_sync(0xffffffffu, seg_p != 0); m; m &= m - 1) {
+      const int src = __ffs(m) - 1;
+      char *p0 = (char *)__shfl_sync(0xffffffffu, seg_p, src);
+      const int64_t w1 = __shfl_sync(0xffffffffu, seg_w, src);
+      const R v = __shfl_sync(0xffffffffu, seg_v, src);
       const int len = (int)(w1 & 255) + 1, nr = (int)((w1 >> 8) & 255) + 1;
       const int64_t stride = w1 >> 16;
-      char *p0 = (char *)at_code<R>(S, cur, w0 & ~(int64_t(31) << kPhysArgShift));
-      const R v = c.bc[arg];
-      for (int r = 0; r < nr; ++r)
-        for (int e = 0; e < len; ++e) *(R *)(p0 + r * stride + (int64_t)e * (int64_t)sizeof(R)) = v;
-      continue;
+      if (lane < len * nr) {
+        const int r = lane / len;
+        *(R *)(p0 + r * stride + (int64_t)(lane - r * len) * (int64_t)sizeof(R)) = v;
+      }
     }
-    const DevPhysOp &op = P.op[q - P.nset];
+    if (!opp) continue;
+    const DevSolve &S = *Sp;
+    const ConstsT<R> &c = consts_of<R>(S);
+    const DevPhysOp &op = *opp;
     if (op.kind == MHD_PHYS_WALL) {
       // BC_Solid_Surface_ (Z4_Mercury/src/boundary/Boundary_Condition_Fluid.cpp:37-259), H+:
       // the boundary cell from the cell one deeper (density floor 2.5e-3,
@@ -1763,7 +1801,6 @@ __global__ void __launch_bounds__(256) k_phys(Dir D, int which) {
               d2 = *at_code<R>(S, cur, op.src + 2 * op.cstride);
       *at_code<R>(S, cur, op.dst) = E0 * d0 + E1 * d1 + E2 * d2;
     }
-  }
   }
 }
 
@@ -2202,7 +2239,23 @@ void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const S
 }
 
 void init_launch_grids_f32() { grids<float>(); }
+
+void launch_res_kmax_f32(const Dir &D, int *out, cudaStream_t st) {
+  grids<float>();
+  k_res_kmax<float><<<g_grid_tiles, kTileThreads, 0, st>>>(D, out);
+}
 #else
+void launch_res_kmax_f32(const Dir &D, int *out, cudaStream_t st);
+
+void launch_res_kmax(const Dir &D, int precision, int *out, cudaStream_t st) {
+  if (precision == kMixed) {
+    launch_res_kmax_f32(D, out, st);
+  } else {
+    grids<double>();
+    k_res_kmax<double><<<g_grid_tiles, kTileThreads, 0, st>>>(D, out);
+  }
+}
+
 void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
                             ResScratch rs);
 

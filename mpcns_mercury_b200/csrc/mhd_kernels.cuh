@@ -77,6 +77,9 @@ int res_dot_grid();
 // are cblocks (k_res_cross, FP32 translation unit).
 enum ResCrossOp { RES_X_SETUP = 0, RES_X_DEMOTE_R, RES_X_ADD_X, RES_X_DEMOTE_X };
 void launch_res_cross(const Dir &D, const DevBlock *cblocks, int op, cudaStream_t st);
+// Per block of the masked solve of D: the largest k of an unknown of the
+// implicit substep into out[block] (atomic max; out starts at -1).
+void launch_res_kmax(const Dir &D, int precision, int *out, cudaStream_t st);
 // Queries every kernel's resident CTAs per SM once (call before any stream capture).
 void init_launch_grids();
 const char *step_kernel_name(StepKernel k);

@@ -58,17 +58,48 @@ def test_implicit_resistivity_matches_reference(ref_oracle, res_dump):
     print("implicit resistivity rel L2 vs reference:", worst)
 
 
-def _mixed_constants():
+def _mixed_constants(direct=0):
     from mpcns_mercury_b200 import reference_constants
 
-    return reference_constants(cfl=0.4, resistive=True, res_rtol=1e-10, res_max_it=500)
+    return reference_constants(cfl=0.4, resistive=True, res_rtol=1e-10, res_max_it=500, res_direct_iters=direct)
+
+
+def test_mixed_precision_implicit_direct(res_dump):
+    """The mixed form's solve as FP64 CG on the companion (no refinement), to
+    1e-10: every substep under a threshold above its iteration count (1000);
+    under the default threshold (20) the first substep only, the next ones
+    switch to iterative refinement (this case takes ~100 iterations)."""
+    import mercury_oracle as mo
+    from gpu_helpers import compare, context_from_dump
+
+    for direct in (1000, 0):
+        ctx = context_from_dump(res_dump, 16, precision=1, constants=_mixed_constants(direct))
+        ctx.prepare()
+        refinements, iters = [], []
+        for _ in range(10):
+            ctx.step(1)
+            info = ctx.info()
+            assert info.status == 0
+            assert info.res_relres <= 1e-10, info.res_relres
+            refinements.append(info.res_refinements)
+            iters.append(info.res_iters)
+        assert refinements[0] == 0 and iters[0] > 20
+        if direct == 1000:
+            assert max(refinements) == 0
+        else:
+            assert min(refinements[1:]) >= 1
+        worst, bad = compare(ctx, res_dump, "step10:", mo.STATE_FIELDS, MIXED_TOL)
+        assert not bad, worst
+        ctx.close()
+        print("mixed implicit, direct threshold", direct, ": refinements", refinements, "CG iterations", iters,
+              "rel L2 vs reference", worst)
 
 
 def test_mixed_precision_implicit_resistivity(res_dump):
     import mercury_oracle as mo
     from gpu_helpers import compare, context_from_dump
 
-    ctx = context_from_dump(res_dump, 16, precision=1, constants=_mixed_constants())
+    ctx = context_from_dump(res_dump, 16, precision=1, constants=_mixed_constants(direct=-1))
     ctx.prepare()
     refinements, iters = [], []
     for _ in range(10):
@@ -127,8 +158,8 @@ def test_mixed_precision_implicit_in_a_batch(res_dump):
     d.close()
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_unconverged_substep_reports_solve_status(res_dump, precision):
+@pytest.mark.parametrize("precision,direct", [(0, 0), (1, 0), (1, -1)], ids=["fp64", "mixed-direct", "mixed-refined"])
+def test_unconverged_substep_reports_solve_status(res_dump, precision, direct):
     """A solve capped below convergence ends its device loop at res_max_it
     and the step returns MHD_ERR_SOLVE (the reference throws there)."""
     from gpu_helpers import context_from_dump
@@ -136,14 +167,14 @@ def test_unconverged_substep_reports_solve_status(res_dump, precision):
     from mpcns_mercury_b200.capi import MhdError
 
     # one CG iteration per solve: the operator needs about 200 to reach 1e-10
-    k = reference_constants(cfl=0.4, resistive=True, res_rtol=1e-14, res_max_it=1)
+    k = reference_constants(cfl=0.4, resistive=True, res_rtol=1e-14, res_max_it=1, res_direct_iters=direct)
     ctx = context_from_dump(res_dump, 16, precision=precision, constants=k)
     ctx.prepare()
     with pytest.raises(MhdError):
         ctx.step(1)
     info = ctx.info()
     assert info.status == 6  # MHD_ERR_SOLVE
-    if precision == 0:
+    if direct == 0:  # FP64 CG (on the FP64 companion in mixed precision)
         assert info.res_iters == 1 and info.res_refinements == 0
     else:  # 30 refinements of one FP32 iteration each
         assert info.res_refinements == 30 and info.res_iters == 30
