@@ -665,6 +665,26 @@ def _shell_state(get, case, dtype=np.float64):
     return out
 
 
+def _flux_divergence(ctx, case):
+    """max over the owned cells of |sum of the induced field's outward face
+    fluxes|, over the largest face flux of the total field (induced + dipole
+    + IMF background): the constrained transport's div B in units of the
+    field it transports."""
+    n0, n1, n2 = case.na, case.na, case.nr
+    worst, big = 0.0, 0.0
+    for blk in range(6):
+        f = {}
+        for ax, name in enumerate(("B_XI", "B_ETA", "B_ZETA")):
+            hi = [n0, n1, n2]
+            hi[ax] += 1
+            f[ax] = ctx.download(name, (0, 0, 0), tuple(hi), block=blk)[..., 0]
+            tot = f[ax] + ctx.download("BADD" + name[1:], (0, 0, 0), tuple(hi), block=blk)[..., 0]
+            big = max(big, float(np.abs(tot).max()))
+        div = (f[0][1:] - f[0][:-1]) + (f[1][:, 1:] - f[1][:, :-1]) + (f[2][:, :, 1:] - f[2][:, :, :-1])
+        worst = max(worst, float(np.abs(div).max()))
+    return worst / max(big, 1e-300)
+
+
 def _shell_descs(cases, ks, topo, precision):
     from mpcns_mercury_b200.capi import SolveDesc
 
@@ -864,8 +884,11 @@ def run_shells(args, rank, world, device):
                    "panel axis log-uniform (na in [24,64], nr in [24,128]), H+ and Na+ (mass 1:23) with Na+ "
                    "fraction U[1e-4,1e-2], centred dipole, upstream |v| U[2,6], n U[0.5,3], IMF Bz U[-0.4,0.4], "
                    "Hall (radial taper 1.1-1.2) + electron pressure, solid inner wall, farfield outer sphere, "
-                   "CFL 0.4; set up on the device from these parameters; one batch, one CUDA graph launch per "
-                   "step advancing every solve",
+                   "implicit resistivity eta = 1e-3 exp(-(r - 1) / 0.2) (the reference's tanh window, outer edge 1, "
+                   "width 0.4), CG to 1e-10, CFL 0.4; set up on the device from these parameters; one batch: per "
+                   "step one CUDA graph for the explicit part of every solve, the implicit substep of every solve "
+                   "at once (one device CG loop; in the mixed batch FP64 CG on the solves' FP64 companions), one "
+                   "graph for the rest",
                    "cells_per_replica": ncell, "blocks_per_replica": len(cells),
                    "precision": "mixed: FP32 state/work/flux/EMF/update, FP64 Jac/JD",
                    "l2": "inputs larger than L2 (not flushed)", "parallelism": f"replicas x{world}",
@@ -906,10 +929,9 @@ def run_config2(args, rank, world, device):
     from mpcns_mercury_b200 import magnetosphere as M
 
     steps = args.config_steps
-    # eta = 1e-3 (units of the REF list) at the surface falling off over ~0.2
-    # planet radii: the reference's tanh window with these parameters
-    case = M.ShellCase(na=48, nr=96, resistive=True, eta_max=1e-3 * 1.256637061e-6 * 4.031e5 * 2.44e6,
-                       eta_r_inner=0.8, eta_r_outer=1.2, eta_width=0.1, res_rtol=1e-10, res_max_it=2000)
+    # eta = 1e-3 exp(-(r - 1) / 0.2) (units of mu0 U_ref L_ref) as the
+    # reference's tanh window (magnetosphere.ETA_CONFIG)
+    case = M.ShellCase(na=48, nr=96, resistive=True, **M.ETA_CONFIG)
     out = {}
     states = {}
     for prec in (0, 1):
@@ -929,10 +951,8 @@ def run_config2(args, rank, world, device):
         if info.status != 0:
             raise RuntimeError(f"config2 precision {prec}: status {info.status}")
         states[prec] = _shell_state(lambda f, lo, hi, blk: ctx.download(f, lo, hi, block=blk), case)
-        divb = ctx.div_b()
-        bmax = max(float(np.abs(states[prec][n]).max()) for n in ("B_XI", "B_ETA", "B_ZETA"))
         out[prec] = {"mcells": round(case.cell_count() * steps / (ms * 1e-3) / 1e6, 3), "ms_per_step": round(ms / steps, 4),
-                     "div_b_max": divb, "div_b_max_over_max_face_flux": divb / max(bmax, 1e-300),
+                     "div_b_max": ctx.div_b(), "div_b_flux_sum_over_max_face_flux": _flux_divergence(ctx, case),
                      "last_substep_cg_iterations": int(info.res_iters),
                      "last_substep_refinements": int(info.res_refinements),
                      "last_substep_relative_residual": float(info.res_relres)}
@@ -945,7 +965,8 @@ def run_config2(args, rank, world, device):
         "config": {"workload": "config2", "description":
                    "one magnetosphere shell, 6 panels of 48x48x96 cells (r in [1, 8], geometric), H+ and Na+ (1e-3), "
                    "centred dipole, upstream |v| 4, n 1, p 0.1, IMF Bz -0.2, Hall + p_e, implicit resistivity "
-                   "eta = 1e-3 near the surface (tanh window 0.8-1.2, width 0.1), CFL 0.4; set up on the device",
+                   "eta = 1e-3 exp(-(r - 1) / 0.2) as the reference's tanh window (outer edge 1, width 0.4, inner 0: "
+                   "equal for r - 1 >> 0.2, half at the surface), CG to 1e-10, CFL 0.4; set up on the device",
                    "cells": case.cell_count(), "fp64": out[0], "mixed": out[1],
                    "mixed_vs_fp64_rel_l2_after_steps": err},
     }
@@ -1249,6 +1270,10 @@ def reference_members(args):
             job.update(na=c.na, nr=c.nr, na_fraction=float(c.na_fraction),
                        initial_line=" ".join(repr(v) for v in up),
                        farfield_line=" ".join(repr(v) for v in (up[0], up[1], up[2], up[4], up[5])))
+            if c.resistive:  # the implicit substep, solved by the reference's GMRES to the same tolerance
+                job.update(resistive=1, eta_max=float(c.eta_max), eta_r_inner=float(c.eta_r_inner),
+                           eta_r_outer=float(c.eta_r_outer), eta_width=float(c.eta_width),
+                           ksp_rtol=float(c.res_rtol), ksp_atol=1e-300, ksp_max_it=int(c.res_max_it))
             out.append((job, c.cell_count()))
         return out
     raise SystemExit(f"unknown workload {args.workload}")

@@ -255,7 +255,8 @@ struct mhd_batch {
   bool borrowed = false;
   ResScratch res{nullptr, nullptr};
   double *hres = nullptr;                               // pinned copy of res.result
-  ResCG *hcg = nullptr;                                 // pinned copy of res.cg
+  ResCG *hcg = nullptr;                                 // pinned copy of res.cg (one per slot)
+  size_t tpart_elems = 0;                               // doubles allocated at res.tpartial
   int kernels_per_step = 0;
   double *staging = nullptr;
   size_t staging_elems = 0;
@@ -497,6 +498,10 @@ int publish(mhd_batch *b) {
                          T.sg_face, S->sg_geo, S->sg_w};
     d.aliasE = DevAlias{S->T->al_off, S->T->al_memE, S->T->al_msign, S->T->al_ownE, S->T->al_osign, S->T->al_n};
     d.aliasJ = DevAlias{S->T->al_off, S->T->al_memJ, S->T->al_msign, S->T->al_ownJ, S->T->al_osign, S->T->al_n};
+    if (S->shadow_slot >= 0 && b->shadow && b->shadow->slots[S->shadow_slot]) {
+      d.companion = b->shadow->slots[S->shadow_slot]->dblocks;
+      d.companion_state = b->shadow->dstate + S->shadow_slot;
+    }
   }
   CUDA_TRY(cudaMemcpyAsync(b->dsolves, ds.data(), sizeof(DevSolve) * C, cudaMemcpyHostToDevice, b->stream));
   return MHD_OK;
@@ -1067,11 +1072,12 @@ void res_apply(mhd_batch *b, int *nk) {
   launch(b, 1, SK_RES_Q, nk);
 }
 
-// The CG iteration loop of the masked solve as one CUDA graph: k_res_cg
-// (CG_INIT) sets the loop condition, then a conditional WHILE node repeats
-// the iteration (operator, q and (p.q)_W, the x / r update and the stop
-// test, the direction update) until the device CG state says it is over.
-// Captured once per batch (again after the tables change).
+// The CG iteration loop of every masked solve as one CUDA graph: k_res_cg
+// and k_res_cg_sum (CG_INIT) set the loop condition, then a conditional
+// WHILE node repeats the iteration (operator, q and (p.q)_W, the x / r update
+// and the stop test, the direction update) while some solve's device CG
+// state says it is still running; a solve whose loop ends leaves the mask.
+// Captured once per batch (again after the tables or the partials change).
 int build_cg_graph(mhd_batch *b) {
   if (b->graph_cg) return MHD_OK;
   cudaGraph_t g = nullptr;
@@ -1092,11 +1098,20 @@ int build_cg_graph(mhd_batch *b) {
       cudaSuccess)
     return fin(e, "capture");
   launch(b, 1, SK_RES_CG, &nk, nullptr, CG_INIT);
+  launch(b, 1, SK_RES_CGSUM, &nk, nullptr, CG_INIT);
   if ((e = cudaStreamEndCapture(b->stream, &g)) != cudaSuccess) return fin(e, "capture");
+  // the loop node follows the chain's last node
+  cudaGraphNode_t nodes[2] = {};
+  size_t n = 2;
+  if ((e = cudaGraphGetNodes(g, nodes, &n)) != cudaSuccess || n != 2)
+    return fin(e != cudaSuccess ? e : cudaErrorUnknown, "init nodes");
   cudaGraphNode_t init = nullptr;
-  size_t n = 1;
-  if ((e = cudaGraphGetNodes(g, &init, &n)) != cudaSuccess || n != 1)
-    return fin(e != cudaSuccess ? e : cudaErrorUnknown, "init node");
+  for (cudaGraphNode_t c : nodes) {
+    size_t nd = 0;
+    if ((e = cudaGraphNodeGetDependentNodes(c, nullptr, &nd)) != cudaSuccess) return fin(e, "init nodes");
+    if (nd == 0) init = c;
+  }
+  if (!init) return fin(cudaErrorUnknown, "init nodes");
   cudaGraphNodeParams p{};
   p.type = cudaGraphNodeTypeConditional;
   p.conditional.handle = h;
@@ -1110,7 +1125,9 @@ int build_cg_graph(mhd_batch *b) {
     return fin(e, "body capture");
   res_apply_core(b, &nk);
   launch(b, 1, SK_RES_CG, &nk, nullptr, CG_PQ);
+  launch(b, 1, SK_RES_CGSUM, &nk, nullptr, CG_PQ);
   launch(b, 1, SK_RES_CG, &nk, nullptr, CG_RR);
+  launch(b, 1, SK_RES_CGSUM, &nk, nullptr, CG_RR);
   launch(b, 1, SK_RES_PUPD_E, &nk);
   if ((e = cudaStreamEndCapture(b->stream, &body)) != cudaSuccess) return fin(e, "body capture");
   e = cudaGraphInstantiate(&b->graph_cg, g, 0);
@@ -1123,25 +1140,72 @@ int build_cg_graph(mhd_batch *b) {
   return MHD_OK;
 }
 
-// CG on the masked solve from x = 0 and r = p = the right-hand side
-// (already set) until ||r|| <= tol_factor ||r_0|| or max_it iterations, the
-// loop on the device (build_cg_graph); one host round trip at the end.
-int res_cg(mhd_batch *b, double tol_factor, int max_it, double *r0, double *rnorm, int *iters, bool *converged) {
-  int rc = build_cg_graph(b);
-  if (rc) return rc;
-  ResCG *h = b->hcg;
-  *h = ResCG{};
-  h->tol_factor = tol_factor;
-  h->max_it = std::max(0, std::min(max_it, 100000));  // the loop runs on the device: a hard bound
-  CUDA_TRY(cudaMemcpyAsync(b->res.cg, h, sizeof(ResCG), cudaMemcpyHostToDevice, b->stream));
-  CUDA_TRY(cudaGraphLaunch(b->graph_cg, b->stream));
-  CUDA_TRY(cudaMemcpyAsync(h, b->res.cg, sizeof(ResCG), cudaMemcpyDeviceToHost, b->stream));
-  CUDA_TRY(cudaStreamSynchronize(b->stream));
-  *r0 = h->r0;
-  *rnorm = h->rnorm;
-  *iters = h->it;
-  *converged = h->converged != 0;
+// The per-warp tile partials of the batched CG: 2 doubles per warp of every
+// kResK tile of the batch's solves (grown on demand; the loop graph holds the
+// pointer, so a new buffer means a new graph).
+int ensure_tpartial(mhd_batch *b) {
+  size_t tiles = 0;
+  for (int s = 0; s < b->capacity; ++s)
+    if (const Solve *S = b->slots[s]) tiles += (size_t)(S->dres_prefix ? S->res_tiles : S->T->tiles[kResK]);
+  const size_t need = std::max<size_t>(tiles, 1) * kWarpsPerTile * 2;
+  if (need <= b->tpart_elems) return MHD_OK;
+  CUDA_TRY(cudaStreamSynchronize(b->stream));  // no loop graph in flight
+  if (b->graph_cg) {
+    cudaGraphExecDestroy(b->graph_cg);
+    b->graph_cg = nullptr;
+  }
+  cudaFree(b->res.tpartial);
+  b->res.tpartial = nullptr;
+  b->tpart_elems = 0;
+  if (cudaMalloc(&b->res.tpartial, sizeof(double) * need) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MHD_ERR_OOM, "CG partials of %zu doubles", need);
+  }
+  b->tpart_elems = need;
   return MHD_OK;
+}
+
+// Sets every slot's mask (one strided copy of the mask fields).
+int apply_masks(mhd_batch *b, const std::vector<int> &on) {
+  CUDA_TRY(cudaMemcpy2DAsync((char *)b->dstate + offsetof(SolveState, mask), sizeof(SolveState), on.data(),
+                             sizeof(int), sizeof(int), (size_t)b->capacity, cudaMemcpyHostToDevice, b->stream));
+  return MHD_OK;
+}
+
+// One CG job of the batched loop: the slot, its stop factor and iteration cap.
+struct CgJob {
+  int slot;
+  double tol_factor;
+  int max_it;
+};
+
+// CG on every job's solve at once, each from x = 0 and r = p = its
+// right-hand side (already set), until ||r|| <= tol_factor ||r_0|| or max_it
+// iterations, the loop on the device (build_cg_graph); the jobs' masks are
+// set here and are all clear on return; one host round trip at the end.
+// Each job's final state is in b->hcg[slot].
+int res_cg_batch(mhd_batch *b, const std::vector<CgJob> &jobs) {
+  int rc;
+  if ((rc = ensure_tpartial(b)) || (rc = build_cg_graph(b))) return rc;
+  std::vector<int> on((size_t)b->capacity, 0);
+  for (int s = 0; s < b->capacity; ++s) {
+    b->hcg[s] = ResCG{};
+    b->hcg[s].done = 1;
+  }
+  for (const CgJob &j : jobs) {
+    ResCG &h = b->hcg[j.slot];
+    h.done = 0;
+    h.tol_factor = j.tol_factor;
+    h.max_it = std::max(0, std::min(j.max_it, 100000));  // the loop runs on the device: a hard bound
+    on[j.slot] = 1;
+  }
+  if ((rc = apply_masks(b, on))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(b->res.cg, b->hcg, sizeof(ResCG) * b->capacity, cudaMemcpyHostToDevice, b->stream));
+  CUDA_TRY(cudaGraphLaunch(b->graph_cg, b->stream));
+  CUDA_TRY(cudaMemcpyAsync(b->hcg, b->res.cg, sizeof(ResCG) * b->capacity, cudaMemcpyDeviceToHost, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  std::fill(on.begin(), on.end(), 0);
+  return apply_masks(b, on);
 }
 
 // The mixed-precision solve of (I + dt eta alpha C^T beta C) E = b on the
@@ -1160,34 +1224,19 @@ int direct_iters(const mhd_constants &k) { return k.res_direct_iters == 0 ? kDir
 int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
   mhd_batch *sh = b->shadow;
   const int cs = S->shadow_slot;
-  const Solve *C = sh->slots[cs];
   const Dir Dm = b->dir(1);
   cudaStream_t st = b->stream;
   constexpr int kMaxRefinements = 30;
   constexpr double kInnerRtol = 1e-4;
-  const int one = 1, zero = 0;
   int rc, nk = 0;
+  std::vector<int> mb((size_t)b->capacity, 0), ms((size_t)sh->capacity, 0);
+  mb[slot] = 1;
+  ms[cs] = 1;
+  if ((rc = apply_masks(b, mb)) || (rc = apply_masks(sh, ms))) return rc;
   // the companion's dt, coefficients, b and x = 0
-  CUDA_TRY(cudaMemcpyAsync((char *)(sh->dstate + cs) + offsetof(SolveState, dt),
-                           (const char *)(b->dstate + slot) + offsetof(SolveState, dt), sizeof(double),
-                           cudaMemcpyDeviceToDevice, st));
-  launch_res_cross(Dm, C->dblocks, RES_X_SETUP, st);
+  launch_res_cross(Dm, RES_X_SETUP, st);
   CUDA_TRY(cudaGetLastError());
-  if (S->T->sg_n > 0)  // the singular edges' canonical vectors and inverse Hodge stars (FP64 in both)
-    CUDA_TRY(cudaMemcpyAsync(C->sg_geo, S->sg_geo, sizeof(double) * 4 * S->T->sg_n, cudaMemcpyDeviceToDevice, st));
-  if ((rc = set_state_field(sh, cs, offsetof(SolveState, mask), &one, sizeof one))) return rc;
   const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-10;
-  if (S->res_direct >= 0 && S->res_iters <= S->res_direct) {
-    // a short solve: FP64 CG on the companion from x = 0, p = r = b
-    launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
-    double r0 = 0.0, rn = 0.0;
-    if ((rc = res_cg(sh, rtol, S->res_max_it, &r0, &rn, &S->res_iters, converged))) return rc;
-    S->res_refinements = 0;
-    S->res_relres = r0 > 0.0 ? rn / r0 : 0.0;
-    launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_X, st);
-    CUDA_TRY(cudaGetLastError());
-    return set_state_field(sh, cs, offsetof(SolveState, mask), &zero, sizeof zero);
-  }
   if ((rc = res_dot(sh, RES_DOT_RR))) return rc;
   const double bnorm = std::sqrt(sh->hres[1]);
   double rn = bnorm;
@@ -1207,32 +1256,36 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
     }
     if (S->res_refinements == kMaxRefinements || !(rn == rn)) break;
     // the correction: FP32 CG on r rounded to FP32, x += d in FP64
-    launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_R, st);
+    launch_res_cross(Dm, RES_X_DEMOTE_R, st);
     launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
-    double r32_0 = 0.0, r32 = 0.0;  // the correction's own residuals: not used (r is checked in FP64)
-    int iters = 0;
-    bool inner = false;
-    if ((rc = res_cg(b, kInnerRtol, S->res_max_it, &r32_0, &r32, &iters, &inner))) return rc;
-    launch_res_cross(Dm, C->dblocks, RES_X_ADD_X, st);
-    S->res_iters += iters;
+    if ((rc = res_cg_batch(b, {CgJob{slot, kInnerRtol, S->res_max_it}}))) return rc;
+    if ((rc = apply_masks(b, mb))) return rc;  // the loop cleared it
+    launch_res_cross(Dm, RES_X_ADD_X, st);
+    S->res_iters += b->hcg[slot].it;
     ++S->res_refinements;
   }
   S->res_relres = bnorm > 0.0 ? rn / bnorm : 0.0;
-  launch_res_cross(Dm, C->dblocks, RES_X_DEMOTE_X, st);
+  launch_res_cross(Dm, RES_X_DEMOTE_X, st);
   CUDA_TRY(cudaGetLastError());
-  return set_state_field(sh, cs, offsetof(SolveState, mask), &zero, sizeof zero);
+  std::fill(ms.begin(), ms.end(), 0);
+  return apply_masks(sh, ms);
 }
 
-// The implicit resistive substep of one solve (SolveImplicitResistiveDiffusion_,
-// Mercury_ImplicitResistive.cpp:475-555), after the explicit update and its
-// Sync(B faces): B* snapshot, J(B*), b = eta J(B*), the solve (FP64: CG in
-// the inner product weighted by 1 / (eta alpha), in which A is self-adjoint;
-// mixed precision: res_refine), then B = B* - dt curl E_res.  The reference
-// solves with GMRES; the solution is the same to the solvers' tolerance.
-int res_solve(mhd_batch *b, int slot) {
-  Solve *S = b->slots[slot];
-  const int one = 1, zero = 0;
-  int rc = set_state_field(b, slot, offsetof(SolveState, mask), &one, sizeof one);
+// The implicit resistive substep (SolveImplicitResistiveDiffusion_,
+// Mercury_ImplicitResistive.cpp:475-555) of every listed solve at once,
+// after the explicit update and its Sync(B faces): B* snapshot, J(B*),
+// b = eta J(B*), the solves (FP64: CG in the inner product weighted by
+// 1 / (eta alpha), in which A is self-adjoint, all solves in one device
+// loop; mixed precision: the short ones as FP64 CG on their companions in
+// one loop, the others by res_refine), then B = B* - dt curl E_res.  The
+// reference solves with GMRES; the solution is the same to the solvers'
+// tolerance.  A solve that did not converge gets MHD_ERR_SOLVE.
+int res_step(mhd_batch *b, const std::vector<int> &slots) {
+  if (slots.empty()) return MHD_OK;
+  cudaStream_t st = b->stream;
+  std::vector<int> on((size_t)b->capacity, 0);
+  for (int s : slots) on[s] = 1;
+  int rc = apply_masks(b, on);
   if (rc) return rc;
   int nk = 0;
   launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_SNAPSHOT);
@@ -1242,20 +1295,58 @@ int res_solve(mhd_batch *b, int slot) {
   sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), &nk);
   sync_after_owner(b, 1, MHD_SYNC_JEDGE, &nk);
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_INIT);
-  bool converged = false;
-  if (S->shadow_slot >= 0) {
-    if ((rc = res_refine(b, slot, S, &converged))) return rc;
-  } else {
-    const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-13;
-    double bnorm = 0.0, rn = 0.0;
-    if ((rc = res_cg(b, rtol, S->res_max_it, &bnorm, &rn, &S->res_iters, &converged))) return rc;
-    S->res_relres = bnorm > 0.0 ? rn / bnorm : 0.0;
+  std::vector<char> conv((size_t)b->capacity, 0);
+  auto take = [&](Solve *S, const ResCG &h, int s) {
+    S->res_iters = h.it;
     S->res_refinements = 0;
+    S->res_relres = h.r0 > 0.0 ? h.rnorm / h.r0 : 0.0;
+    conv[s] = h.converged != 0;
+  };
+  if (b->precision != kMixed) {
+    std::vector<CgJob> jobs;
+    for (int s : slots) {
+      const Solve *S = b->slots[s];
+      jobs.push_back(CgJob{s, S->res_rtol > 0.0 ? S->res_rtol : 1e-13, S->res_max_it});
+    }
+    if ((rc = res_cg_batch(b, jobs))) return rc;
+    for (int s : slots) take(b->slots[s], b->hcg[s], s);
+  } else {
+    mhd_batch *sh = b->shadow;
+    std::vector<int> direct, refine;
+    for (int s : slots) {
+      const Solve *S = b->slots[s];
+      (S->res_direct >= 0 && S->res_iters <= S->res_direct ? direct : refine).push_back(s);
+    }
+    if (!direct.empty()) {
+      // FP64 CG on the companions of the short solves, from x = 0, p = r = b
+      std::vector<int> mb((size_t)b->capacity, 0), ms((size_t)sh->capacity, 0);
+      std::vector<CgJob> jobs;
+      for (int s : direct) {
+        const Solve *S = b->slots[s];
+        mb[s] = 1;
+        ms[S->shadow_slot] = 1;
+        jobs.push_back(CgJob{S->shadow_slot, S->res_rtol > 0.0 ? S->res_rtol : 1e-10, S->res_max_it});
+      }
+      if ((rc = apply_masks(b, mb)) || (rc = apply_masks(sh, ms))) return rc;
+      launch_res_cross(b->dir(1), RES_X_SETUP, st);
+      launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
+      if ((rc = res_cg_batch(sh, jobs))) return rc;
+      launch_res_cross(b->dir(1), RES_X_DEMOTE_X, st);
+      CUDA_TRY(cudaGetLastError());
+      for (int s : direct) take(b->slots[s], sh->hcg[b->slots[s]->shadow_slot], s);
+    }
+    for (int s : refine) {
+      bool c = false;
+      if ((rc = res_refine(b, s, b->slots[s], &c))) return rc;
+      conv[s] = c;
+    }
   }
-  if (!converged) {
-    const int st = MHD_ERR_SOLVE;
-    if ((rc = set_state_field(b, slot, offsetof(SolveState, status), &st, sizeof st))) return rc;
-  }
+  if ((rc = apply_masks(b, on))) return rc;  // the loops left their solves' masks clear
+  for (int s : slots)
+    if (!conv[s]) {
+      const int e = MHD_ERR_SOLVE;
+      if ((rc = set_state_field(b, s, offsetof(SolveState, status), &e, sizeof e))) return rc;
+    }
   // E_res = x, its owner copies; B = B* + dt (-curl E_res) on the owned faces
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_E_FROM_X);
   sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner), &nk);
@@ -1263,7 +1354,8 @@ int res_solve(mhd_batch *b, int slot) {
   launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_RESTORE);
   launch(b, 1, SK_RES_BUPDATE, &nk);
   CUDA_TRY(cudaGetLastError());
-  return set_state_field(b, slot, offsetof(SolveState, mask), &zero, sizeof zero);
+  std::fill(on.begin(), on.end(), 0);
+  return apply_masks(b, on);
 }
 
 int xfer(mhd_batch *b, int slot, int field, int block, const int32_t lo[3], const int32_t hi[3], int ncomp,
@@ -1352,9 +1444,11 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
     return bail(fail(MHD_ERR_OOM, "prefix"));
   if (cudaMalloc(&b->res.partial, sizeof(double) * 2 * res_dot_grid()) != cudaSuccess ||
       cudaMalloc(&b->res.result, sizeof(double) * 2) != cudaSuccess ||
-      cudaMalloc(&b->res.cg, sizeof(ResCG)) != cudaSuccess ||
+      cudaMalloc(&b->res.cg, sizeof(ResCG) * capacity) != cudaSuccess ||
+      cudaMalloc(&b->res.ctl, sizeof(ResCtl)) != cudaSuccess ||
+      cudaMemsetAsync(b->res.ctl, 0, sizeof(ResCtl), b->stream) != cudaSuccess ||
       cudaMallocHost(&b->hres, sizeof(double) * 2) != cudaSuccess ||
-      cudaMallocHost(&b->hcg, sizeof(ResCG)) != cudaSuccess)
+      cudaMallocHost(&b->hcg, sizeof(ResCG) * capacity) != cudaSuccess)
     return bail(fail(MHD_ERR_OOM, "solver scratch"));
   if (cudaMemsetAsync(b->dstate, 0, sizeof(SolveState) * capacity, b->stream) != cudaSuccess)
     return bail(fail(MHD_ERR_CUDA, "state init"));
@@ -1376,6 +1470,8 @@ int mhd_batch_destroy(mhd_batch *b) {
   cudaFree(b->res.partial);
   cudaFree(b->res.result);
   cudaFree(b->res.cg);
+  cudaFree(b->res.ctl);
+  cudaFree(b->res.tpartial);
   if (b->hres) cudaFreeHost(b->hres);
   if (b->hcg) cudaFreeHost(b->hcg);
   for (auto *S : b->slots) free_solve(S, b->stream);
@@ -1850,6 +1946,7 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
       return rc;
     }
     S->shadow_slot = cs;
+    if ((rc = publish(b))) return rc;  // the directory entry's companion
   }
   *slot_out = slot;
   return MHD_OK;
@@ -1952,6 +2049,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
       return rc;
     }
     S->shadow_slot = cs;
+    if ((rc = publish(b))) return rc;  // the directory entry's companion
   }
   *slot_out = slot;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
@@ -2217,6 +2315,10 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   });
   if (rc) return rc;
   if (res && (rc = res_range(b, slot))) return rc;
+  const Solve *S = b->slots[slot];
+  if (res && S->shadow_slot >= 0 && S->T->sg_n > 0)  // the singular edges' geometry, FP64 in both
+    CUDA_TRY(cudaMemcpyAsync(b->shadow->slots[S->shadow_slot]->sg_geo, S->sg_geo, sizeof(double) * 4 * S->T->sg_n,
+                             cudaMemcpyDeviceToDevice, b->stream));
   b->slots[slot]->prepared = true;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
 }
@@ -2468,17 +2570,19 @@ int mhd_batch_run(mhd_batch *b, int nsteps) {
     for (int s = 0; s < nsteps; ++s) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
     return MHD_OK;
   }
-  // with implicit resistive solves: part A, each such solve's substep (host-driven CG), part B
+  // with implicit resistive solves: part A, their substep (all at once, host-driven), part B
   if ((rc = capture(b, &b->graph_a, nullptr, [&](int *nk) { enqueue_step_a(b, nk); }))) return rc;
   if ((rc = capture(b, &b->graph_b, nullptr, [&](int *nk) { enqueue_step_b(b, nk, true); }))) return rc;
+  std::vector<int> slots;
   for (int s = 0; s < nsteps; ++s) {
     CUDA_TRY(cudaGraphLaunch(b->graph_a, b->stream));
     if ((rc = read_state(b))) return rc;
+    slots.clear();
     for (int q = 0; q < b->capacity; ++q) {
       const Solve *S = b->slots[q];
-      if (S && S->consts.resistive && b->hstate[q].remaining > 0 && b->hstate[q].status == 0)
-        if ((rc = res_solve(b, q))) return rc;
+      if (S && S->consts.resistive && b->hstate[q].remaining > 0 && b->hstate[q].status == 0) slots.push_back(q);
     }
+    if ((rc = res_step(b, slots))) return rc;
     CUDA_TRY(cudaGraphLaunch(b->graph_b, b->stream));
   }
   return MHD_OK;

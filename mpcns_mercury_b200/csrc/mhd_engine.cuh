@@ -221,6 +221,10 @@ struct DevSolve {
   DevAlias aliasE, aliasJ;
   DevPhys phys[kNumPhys];
   DevSingular sing;
+  // a mixed-precision solve's FP64 companion (implicit substep): its blocks
+  // and its state in the companion batch (null without one)
+  const DevBlock *companion;
+  SolveState *companion_state;
 };
 
 // The directory handed to every kernel (by value).

@@ -106,11 +106,16 @@ struct Item {
   int lo[3];   // range lower bounds
 };
 
+struct NoTileEnd {
+  __device__ void operator()(int) const {}
+};
+
 // Work-item loop: for every tile of range `KIND` of every active solve, call
-// f(S, B, item).  Tile lookup: two binary searches by thread 0, broadcast
-// through shared memory.
-template <class R, int KIND, class F>
-__device__ __forceinline__ void for_items(const Dir &D, F &&f) {
+// f(S, B, item), then end(w) with the tile's index w over all solves (every
+// thread of the CTA).  Tile lookup: two binary searches by thread 0,
+// broadcast through shared memory.
+template <class R, int KIND, class F, class E = NoTileEnd>
+__device__ __forceinline__ void for_items(const Dir &D, F &&f, E &&end = E{}) {
   __shared__ int sh[3];
   const int total = D.solve_tile_prefix[KIND][D.nsolves];
   const int tid = threadIdx.x;
@@ -188,6 +193,7 @@ __device__ __forceinline__ void for_items(const Dir &D, F &&f) {
     B.n1 = DB.n[1];
     B.n2 = DB.n[2];
     f(S, B, it);
+    end(w);
   }
 }
 
@@ -1227,138 +1233,141 @@ __global__ void k_res_sum(const double *partial, int n, double *result) {
   }
 }
 
-// One step of the CG iteration with its dot product, the scalar update done
-// by the last CTA to finish (no host round trip).  The last CTA sums the
-// per-CTA partials with all its threads in a fixed order (thread t takes
-// CTAs t, t + 256, ...; then a fixed tree), so the sums are deterministic,
-// then sets the loop condition of the graph (CG_INIT, CG_RR); CG_PQ clears
-// it first, so a loop whose stop test did not run ends.
+// One step of the CG iteration of every masked solve with its dot products:
+// each warp writes its sums over each tile to its own slot of tpart (2
+// doubles per warp and tile), k_res_cg_sum then adds a solve's slots in a
+// fixed order (deterministic) and updates its scalars.  CG_PQ first clears
+// the loop condition, so a loop whose stop test did not run ends.
 template <class R>
-__global__ void __launch_bounds__(kTileThreads) k_res_cg(Dir D, int op, double *partial, ResCG *cg,
+__global__ void __launch_bounds__(kTileThreads) k_res_cg(Dir D, int op, double *tpart, const ResCG *cg,
                                                          cudaGraphConditionalHandle handle) {
-  __shared__ double sh[2][kTileThreads / 32];
-  __shared__ unsigned int ticket;
-  __shared__ double tot[2];
   if (op == CG_PQ && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
-  const bool skip = op == CG_RR && cg->done != 0;  // breakdown in CG_PQ
-  const R alpha = R(cg->alpha);
   double acc0 = 0.0, acc1 = 0.0;
-  if (!skip)
-    for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
-      if (!it.in) return;
-      const int o = B.off(it.i, it.j, it.k);
-      for (int a = 0; a < 3; ++a) {
-        const R wr = B.c(cRW + a)[o];
-        const bool dof = wr > R(0.0);
-        const double w = (double)wr;
-        R *x = B.c(cRX + a) + o, *r = B.c(cRR + a) + o, *p = B.c(cRP + a) + o, *q = B.c(cRQ + a) + o;
-        if (op == CG_INIT) {
-          B.c(cEX + a)[o] = dof ? *p : R(0.0);
-          if (w > 0.0) {
-            const double rv = (double)*r;
-            acc0 += w * rv * rv;
-            acc1 += rv * rv;
-          }
-        } else if (op == CG_PQ) {
-          const R qv = dof ? B.c(cEX + a)[o] - B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
-          *q = qv;
-          if (w > 0.0) acc0 += w * (double)*p * (double)qv;
-        } else {
-          if (dof) {
-            *x += alpha * *p;
-            *r -= alpha * *q;
-          }
-          if (w > 0.0) {
-            const double rv = (double)*r;
-            acc0 += w * rv * rv;
-            acc1 += rv * rv;
+  for_items<R, kResK>(
+      D,
+      [&](const DevSolve &S, const V<R> &B, const Item &it) {
+        if (!it.in) return;
+        const R alpha = R(cg[it.s].alpha);
+        const int o = B.off(it.i, it.j, it.k);
+        for (int a = 0; a < 3; ++a) {
+          const R wr = B.c(cRW + a)[o];
+          const bool dof = wr > R(0.0);
+          const double w = (double)wr;
+          R *x = B.c(cRX + a) + o, *r = B.c(cRR + a) + o, *p = B.c(cRP + a) + o, *q = B.c(cRQ + a) + o;
+          if (op == CG_INIT) {
+            B.c(cEX + a)[o] = dof ? *p : R(0.0);
+            if (w > 0.0) {
+              const double rv = (double)*r;
+              acc0 += w * rv * rv;
+              acc1 += rv * rv;
+            }
+          } else if (op == CG_PQ) {
+            const R qv = dof ? B.c(cEX + a)[o] - B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
+            *q = qv;
+            if (w > 0.0) acc0 += w * (double)*p * (double)qv;
+          } else {
+            if (dof) {
+              *x += alpha * *p;
+              *r -= alpha * *q;
+            }
+            if (w > 0.0) {
+              const double rv = (double)*r;
+              acc0 += w * rv * rv;
+              acc1 += rv * rv;
+            }
           }
         }
+      },
+      [&](int w) {  // the warp's sums over this tile
+        for (int of = 16; of > 0; of >>= 1) {
+          acc0 += __shfl_xor_sync(0xffffffffu, acc0, of);
+          acc1 += __shfl_xor_sync(0xffffffffu, acc1, of);
+        }
+        if ((threadIdx.x & 31) == 0) {
+          const int64_t slot = (int64_t)w * kWarpsPerTile + (threadIdx.x >> 5);
+          tpart[2 * slot] = acc0;
+          tpart[2 * slot + 1] = acc1;
+        }
+        acc0 = acc1 = 0.0;
+      });
+}
+
+// The per-solve end of a k_res_cg step: CTA s adds solve s's tile partials
+// (threads stride over them, then a fixed tree) and updates its state; a
+// solve whose loop ends (converged, max_it, breakdown) leaves the mask, so
+// the following kernels skip it.  The last CTA to finish (atomic ticket)
+// sets the loop condition after CG_INIT and CG_RR: some solve still running.
+__global__ void __launch_bounds__(kTileThreads) k_res_cg_sum(Dir D, int op, const double *tpart, ResCG *cg,
+                                                             ResCtl *ctl, cudaGraphConditionalHandle handle) {
+  __shared__ double sh[2][kWarpsPerTile];
+  __shared__ unsigned int ticket;
+  const int s = blockIdx.x;
+  if (s < D.nsolves && solve_active(D, s)) {  // the whole CTA agrees
+    const int *sp = D.solve_tile_prefix[kResK];
+    const int64_t a = (int64_t)sp[s] * kWarpsPerTile, e = (int64_t)sp[s + 1] * kWarpsPerTile;
+    double u0 = 0.0, u1 = 0.0;
+    for (int64_t q = a + threadIdx.x; q < e; q += kTileThreads) {
+      u0 += tpart[2 * q];
+      u1 += tpart[2 * q + 1];
+    }
+    for (int of = 16; of > 0; of >>= 1) {
+      u0 += __shfl_xor_sync(0xffffffffu, u0, of);
+      u1 += __shfl_xor_sync(0xffffffffu, u1, of);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      sh[0][threadIdx.x >> 5] = u0;
+      sh[1][threadIdx.x >> 5] = u1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t0 = 0.0, t1 = 0.0;
+      for (int w = 0; w < kWarpsPerTile; ++w) {
+        t0 += sh[0][w];
+        t1 += sh[1][w];
       }
-    });
-  for (int of = 16; of > 0; of >>= 1) {
-    acc0 += __shfl_xor_sync(0xffffffffu, acc0, of);
-    acc1 += __shfl_xor_sync(0xffffffffu, acc1, of);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sh[0][threadIdx.x >> 5] = acc0;
-    sh[1][threadIdx.x >> 5] = acc1;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s0 = 0.0, s1 = 0.0;
-    for (int w = 0; w < kTileThreads / 32; ++w) {
-      s0 += sh[0][w];
-      s1 += sh[1][w];
+      ResCG &c = cg[s];
+      if (op == CG_INIT) {
+        c.rho = t0;
+        c.r0 = c.rnorm = sqrt(t1);
+        c.tol = c.tol_factor * c.r0;
+        c.it = 0;
+        c.converged = c.rnorm <= c.tol;
+        c.done = c.converged || c.max_it <= 0;
+      } else if (op == CG_PQ) {
+        if (!(t0 > 0.0)) c.done = 1;  // breakdown: not positive definite on these unknowns
+        else c.alpha = c.rho / t0;
+      } else {
+        c.it += 1;
+        c.rnorm = sqrt(t1);
+        if (c.rnorm <= c.tol) c.converged = c.done = 1;
+        else if (c.it >= c.max_it) c.done = 1;
+        c.beta = t0 / c.rho;
+        c.rho = t0;
+      }
+      if (c.done) D.state[s].mask = 0;
+      else atomicAdd(&ctl->running, 1);
     }
-    partial[2 * blockIdx.x] = s0;
-    partial[2 * blockIdx.x + 1] = s1;
+  }
+  if (threadIdx.x == 0) {
     __threadfence();
-    ticket = atomicAdd(&cg->arrivals, 1u);
+    ticket = atomicAdd(&ctl->arrivals, 1u);
   }
   __syncthreads();
-  if (ticket != gridDim.x - 1) return;  // the whole CTA agrees
+  if (threadIdx.x != 0 || ticket != gridDim.x - 1) return;
   __threadfence();
-  double u0 = 0.0, u1 = 0.0;
-  for (unsigned q = threadIdx.x; q < gridDim.x; q += kTileThreads) {
-    u0 += __ldcg(partial + 2 * q);
-    u1 += __ldcg(partial + 2 * q + 1);
-  }
-  for (int of = 16; of > 0; of >>= 1) {
-    u0 += __shfl_xor_sync(0xffffffffu, u0, of);
-    u1 += __shfl_xor_sync(0xffffffffu, u1, of);
-  }
-  __syncthreads();  // sh is reused
-  if ((threadIdx.x & 31) == 0) {
-    sh[0][threadIdx.x >> 5] = u0;
-    sh[1][threadIdx.x >> 5] = u1;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double v0 = 0.0, v1 = 0.0;
-    for (int w = 0; w < kTileThreads / 32; ++w) {
-      v0 += sh[0][w];
-      v1 += sh[1][w];
-    }
-    tot[0] = v0;
-    tot[1] = v1;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  const double t0 = tot[0], t1 = tot[1];
-  cg->arrivals = 0;
-  if (op == CG_INIT) {
-    cg->rho = t0;
-    cg->r0 = cg->rnorm = sqrt(t1);
-    cg->tol = cg->tol_factor * cg->r0;
-    cg->it = 0;
-    cg->converged = cg->rnorm <= cg->tol;
-    cg->done = cg->converged || cg->max_it <= 0;
-    cudaGraphSetConditional(handle, cg->done ? 0u : 1u);
-  } else if (op == CG_PQ) {
-    if (!(t0 > 0.0)) cg->done = 1;  // breakdown: not positive definite on these unknowns
-    else cg->alpha = cg->rho / t0;
-  } else {
-    if (!skip) {
-      cg->it += 1;
-      cg->rnorm = sqrt(t1);
-      if (cg->rnorm <= cg->tol) cg->converged = cg->done = 1;
-      else if (cg->it >= cg->max_it) cg->done = 1;
-      cg->beta = t0 / cg->rho;
-      cg->rho = t0;
-    }
-    cudaGraphSetConditional(handle, cg->done ? 0u : 1u);
-  }
+  const int running = atomicAdd(&ctl->running, 0);
+  ctl->arrivals = 0;
+  ctl->running = 0;
+  if (op != CG_PQ) cudaGraphSetConditional(handle, running > 0 ? 1u : 0u);
 }
 
 // p = r + beta p and E_res = p on the unknowns (the next iteration's
-// operator input), unless the loop is over.
+// operator input) of every solve still iterating (in the mask).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_pupd_e(Dir D, const ResCG *cg) {
-  if (cg->done) return;
-  const R beta = R(cg->beta);
   for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
+    const R beta = R(cg[it.s].beta);
     const int o = B.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       const bool dof = B.c(cRW + a)[o] > R(0.0);
@@ -2100,6 +2109,7 @@ static const void *kernel_fn(StepKernel k) {
     case SK_RES_PUPD_E: return (const void *)k_res_pupd_e<R>;
     case SK_PHYS: return (const void *)k_phys<R>;
     case SK_RES_CLEARB: return (const void *)k_res_clearb<R>;
+    case SK_RES_CGSUM: return (const void *)k_res_cg_sum;
     default: return nullptr;
   }
 }
@@ -2169,7 +2179,8 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_RES_SUM: k_res_sum<<<1, 32, 0, st>>>(rs.partial, g_grid_tiles, rs.result); break;
     case SK_RES_COPYB: k_res_copyb<R><<<G, kTileThreads, 0, st>>>(D, iarg); break;
     case SK_RES_BUPDATE: k_res_bupdate<R><<<G, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_CG: k_res_cg<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.partial, rs.cg, rs.handle); break;
+    case SK_RES_CG: k_res_cg<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.tpartial, rs.cg, rs.handle); break;
+    case SK_RES_CGSUM: k_res_cg_sum<<<D.nsolves, kTileThreads, 0, st>>>(D, iarg, rs.tpartial, rs.cg, rs.ctl, rs.handle); break;
     case SK_RES_PUPD_E: k_res_pupd_e<R><<<G, kTileThreads, 0, st>>>(D, rs.cg); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;
@@ -2189,18 +2200,22 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
 // flags.
 #if MHD_KERNELS_F32
 // Vectors of the mixed-precision implicit substep between a solve's FP32
-// arena (the masked solve of D) and its FP64 companion (cblocks: the
-// companion's blocks, the same boxes), over the whole box:
+// arena (every masked solve of D) and its FP64 companion (DevSolve::companion:
+// the companion's blocks, the same boxes), over the whole box:
 // RES_X_SETUP: companion alpha, beta, eta, W = the solve's (widened); the
 //   companion's b (B* snapshot arrays) and r = the solve's r (the FP32
-//   right-hand side eta J(B*)); companion x = 0.
+//   right-hand side eta J(B*)); companion x = 0; the companion's dt = the step's.
 // RES_X_DEMOTE_R: r = (float) companion r (the next correction's right-hand side).
 // RES_X_ADD_X: companion x += x (the correction).
 // RES_X_DEMOTE_X: x = (float) companion x (the solution).
-__global__ void __launch_bounds__(kTileThreads) k_res_cross(Dir D, const DevBlock *cblocks, int op) {
+__global__ void __launch_bounds__(kTileThreads) k_res_cross(Dir D, int op) {
   for_items<float, kFull>(D, [&](const DevSolve &S, const V<float> &B, const Item &it) {
     if (!it.in) return;
-    const DevBlock &CB = cblocks[it.blk];
+    const DevBlock &CB = S.companion[it.blk];
+    if (op == RES_X_SETUP && it.blk == 0 && it.i == it.lo[0] && it.j == it.lo[1] && it.k == it.lo[2]) {
+      S.companion_state->dt = D.state[it.s].dt;  // the step's dt, once per solve
+      S.companion_state->dt_bits = D.state[it.s].dt_bits;
+    }
     V<double> C;
     C.U = C.Un = nullptr;
     C.M = CB.M;
@@ -2227,9 +2242,9 @@ __global__ void __launch_bounds__(kTileThreads) k_res_cross(Dir D, const DevBloc
   });
 }
 
-void launch_res_cross(const Dir &D, const DevBlock *cblocks, int op, cudaStream_t st) {
+void launch_res_cross(const Dir &D, int op, cudaStream_t st) {
   grids<float>();
-  k_res_cross<<<g_grid_tiles, kTileThreads, 0, st>>>(D, cblocks, op);
+  k_res_cross<<<g_grid_tiles, kTileThreads, 0, st>>>(D, op);
 }
 
 void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,
@@ -2288,7 +2303,7 @@ const char *step_kernel_name(StepKernel k) {
                                 "k_res_seed", "k_res_w",    "k_res_vec",     "k_res_db",   "k_res_dj",
                                 "k_res_q",    "k_res_dot",  "k_res_sum",     "k_res_copyb", "k_res_bupdate",
                                 "k_res_cg",   "k_res_pupd_e", "k_phys",      "k_sing_setup", "k_sing_emf",
-                                "k_sing_j",   "k_res_clearb"};
+                                "k_sing_j",   "k_res_clearb", "k_res_cg_sum"};
   static_assert(sizeof(names) / sizeof(names[0]) == SK_COUNT, "a name per kernel");
   return (k >= 0 && k < SK_COUNT) ? names[k] : "?";
 }

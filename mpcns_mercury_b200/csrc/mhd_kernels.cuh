@@ -15,7 +15,9 @@ enum StepKernel {
   // grids with physical boundaries and singular edges
   SK_PHYS, SK_SING_SETUP, SK_SING_EMF, SK_SING_J,
   // implicit resistive substep on grids with physical boundaries: zero the ghost faces of dB
-  SK_RES_CLEARB, SK_COUNT
+  SK_RES_CLEARB,
+  // the batched CG's per-solve sums
+  SK_RES_CGSUM, SK_COUNT
 };
 
 // One launch of k_sync runs up to two independent sync operations: a copy
@@ -40,29 +42,40 @@ enum ResVecOp { RES_INIT = 0, RES_E_FROM_P, RES_E_FROM_X, RES_AXPY, RES_PUPD, RE
 enum ResDotOp { RES_DOT_PQ = 0, RES_DOT_RR };
 enum ResCopyOp { RES_SNAPSHOT = 0, RES_RESTORE };
 
-// CG state of the masked solve on the device, for the iteration loop run as
-// a CUDA graph (k_res_cg, k_res_pupd_e): the host sets tol_factor and max_it
-// (and zeros the rest) before the graph and reads it back after.
+// CG state of one solve on the device (one per slot), for the iteration
+// loop run as a CUDA graph over every masked solve at once (k_res_cg,
+// k_res_cg_sum, k_res_pupd_e): the host sets tol_factor and max_it (and
+// zeros the rest) before the graph and reads it back after.
 struct ResCG {
   double rho, alpha, beta;  // W-weighted r.r, step length, direction update
   double r0, rnorm, tol;    // ||r|| at the start and now, stop when rnorm <= tol = tol_factor * r0
   double tol_factor;
   int it, max_it;           // iterations taken, at most max_it
   int done, converged;      // loop over (converged, max_it reached, or breakdown)
-  unsigned int arrivals;    // CTAs finished with the current dot product
-  int pad_;
+};
+// The loop's shared counters: CTAs of k_res_cg_sum finished, solves still iterating.
+struct ResCtl {
+  unsigned int arrivals;
+  int running;
 };
 // Steps of k_res_cg: CG_INIT: E = p, (r.r)_W and r.r, sets rho, r0, tol;
 // CG_PQ: q = A p (its last part, E - eta dJ) and (p.q)_W, sets alpha;
 // CG_RR: x += alpha p, r -= alpha q, (r.r)_W and r.r, the stop test and beta.
+// k_res_cg writes one partial pair per warp and tile; k_res_cg_sum (one CTA
+// per slot) sums a solve's pairs in a fixed order and updates its state; a
+// solve whose loop is over leaves the mask.
 enum ResCgOp { CG_INIT = 0, CG_PQ, CG_RR };
+constexpr int kWarpsPerTile = kTileThreads / 32;
 
-// Scratch of the CG dot products: per-CTA partial sums and the two results;
-// the device CG state and the graph's loop condition.
+// Scratch of the CG dot products: per-CTA partial sums and the two results
+// (k_res_dot, one masked solve); the per-slot CG states, the per-warp tile
+// partials of the batched loop, its counters and the graph's loop condition.
 struct ResScratch {
   double *partial;  // 2 * grid
   double *result;   // 2
   ResCG *cg = nullptr;
+  double *tpartial = nullptr;  // 2 per warp of every kResK tile
+  ResCtl *ctl = nullptr;
   unsigned long long handle = 0;  // cudaGraphConditionalHandle of the loop
 };
 
@@ -72,11 +85,11 @@ struct ResScratch {
 void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision, int iarg = 0,
                         double darg = 0.0, ResScratch rs = ResScratch{nullptr, nullptr});
 int res_dot_grid();
-// Mixed-precision implicit substep: moves its vectors between the masked
-// solve of the FP32 directory D and the solve's FP64 companion, whose blocks
-// are cblocks (k_res_cross, FP32 translation unit).
+// Mixed-precision implicit substep: moves its vectors between every masked
+// solve of the FP32 directory D and its FP64 companion (DevSolve::companion;
+// RES_X_SETUP also hands over the step's dt) (k_res_cross, FP32 translation unit).
 enum ResCrossOp { RES_X_SETUP = 0, RES_X_DEMOTE_R, RES_X_ADD_X, RES_X_DEMOTE_X };
-void launch_res_cross(const Dir &D, const DevBlock *cblocks, int op, cudaStream_t st);
+void launch_res_cross(const Dir &D, int op, cudaStream_t st);
 // Per block of the masked solve of D: the largest k of an unknown of the
 // implicit substep into out[block] (atomic max; out starts at -1).
 void launch_res_kmax(const Dir &D, int precision, int *out, cudaStream_t st);

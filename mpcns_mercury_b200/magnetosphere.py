@@ -37,6 +37,17 @@ UPSTREAM = (1612400.0, 1954409.5501563628, 4e7, 0.001, 0.0, 0.0, 0.0, 0.0, -2.00
 DIPOLE = (0.0, 0.0, 0.0, 0.0, 0.0, -1.452678400462402e+17, 0.0)
 
 
+# The configuration's implicit resistivity, eta = 1e-3 exp(-(r - 1) / 0.2) in
+# units of mu0 U_ref L_ref (r in planet radii), written in the reference's one
+# radial profile, the tanh window eta_max (tanh((r - r_in) / w) -
+# tanh((r - r_out) / w)) / 2 (MercurySolver.cpp:173-181 reads its parameters):
+# r_out = 1 and w = 0.4 make its outer flank exp(-2 (r - 1) / 0.4) =
+# exp(-(r - 1) / 0.2) for r - 1 >> 0.2 (half of eta_max at the surface);
+# r_in = 0 puts the inner flank inside the planet.  Solved to 1e-10.
+ETA_CONFIG = dict(eta_max=1e-3 * 1.256637061e-6 * 4.031e5 * 2.44e6, eta_r_inner=0.0, eta_r_outer=1.0,
+                  eta_width=0.4, res_rtol=1e-10, res_max_it=2000)
+
+
 @dataclass
 class ShellCase:
     na: int = 48                 # cells per panel along each angle
@@ -186,13 +197,14 @@ def context(case: ShellCase, precision: int = 0, k=None, topologies: TopologyCac
     return ctx
 
 
-def ensemble(nsolves: int, stream: int = 300000, resistive: bool = False):
+def ensemble(nsolves: int, stream: int = 300000, resistive: bool = True):
     """The magnetosphere ensemble: per solve, cells per panel axis drawn
     log-uniform (na in [24, 64], nr in [24, 128]: blocks of 24^3 to
     64 x 64 x 128 cells) and the upstream drawn uniform: speed |v| in [2, 6]
     and density n in [0.5, 3] (units of the REF list's U and n), IMF Bz in
     [-0.4, 0.4] (units of B_ref), Na+ fraction in [1e-4, 1e-2]; flow along
-    the INITIAL list's axis, T and M of the base upstream.  Seeded draws
+    the INITIAL list's axis, T and M of the base upstream; the implicit
+    resistivity ETA_CONFIG (unless resistive is False).  Seeded draws
     (mhd_seeded_uniform's generator, solve_id = stream), computed without
     the CUDA library."""
     import math
@@ -212,17 +224,21 @@ def ensemble(nsolves: int, stream: int = 300000, resistive: bool = False):
         bz = -0.4 + 0.8 * e
         frac = 1e-4 + (1e-2 - 1e-4) * f
         up = (v * U_ref, UPSTREAM[1], n * n_ref, UPSTREAM[3], 0.0, 0.0, 0.0, 0.0, bz * B_ref)
-        out.append(ShellCase(na=na, nr=nr, upstream=up, na_fraction=frac, resistive=resistive))
+        out.append(ShellCase(na=na, nr=nr, upstream=up, na_fraction=frac, **_res(resistive)))
     return out
 
 
+def _res(resistive: bool) -> dict:
+    return dict(resistive=True, **ETA_CONFIG) if resistive else dict(resistive=False)
+
+
 def request_stream(nreq: int, rate: float, shapes: int = 16, na_max: int = 96, nr_max: int = 192,
-                   steps_min: int = 50, steps_max: int = 500, stream: int = 500000):
+                   steps_min: int = 50, steps_max: int = 500, stream: int = 500000, resistive: bool = True):
     """A seeded Poisson stream of magnetosphere requests: [(arrival_s,
     ShellCase, steps)].  The grids come from a pool of ``shapes`` sizes drawn
     log-uniform (na in [24, na_max], nr in [24, nr_max]); each request has
-    its own upstream conditions (the ensemble's ranges), exponential
-    inter-arrival times of mean 1 / rate and steps uniform in
+    its own upstream conditions (the ensemble's ranges and resistivity),
+    exponential inter-arrival times of mean 1 / rate and steps uniform in
     [steps_min, steps_max]."""
     import math
 
@@ -240,7 +256,7 @@ def request_stream(nreq: int, rate: float, shapes: int = 16, na_max: int = 96, n
         na, nr = grid[min(int(b * shapes), shapes - 1)]
         up = (float((2.0 + 4.0 * c) * U_ref), UPSTREAM[1], float((0.5 + 2.5 * d) * n_ref), UPSTREAM[3], 0.0, 0.0,
               0.0, 0.0, float((-0.4 + 0.8 * e) * B_ref))
-        case = ShellCase(na=na, nr=nr, upstream=up, na_fraction=float(1e-4 + (1e-2 - 1e-4) * f))
+        case = ShellCase(na=na, nr=nr, upstream=up, na_fraction=float(1e-4 + (1e-2 - 1e-4) * f), **_res(resistive))
         steps = steps_min + min(int(h * (steps_max - steps_min + 1)), steps_max - steps_min)
         out.append((t, case, steps))
     return out

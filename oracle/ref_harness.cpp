@@ -99,7 +99,7 @@ std::string setup_general() {
   o << "int     Read_Method 2\n";
   o << "int     max_Nstep " << job_int("steps", 1) << "\n";
   o << "int     corner_treat 2\n";
-  o << "double  eta_max_mercury 1.25E7\n";
+  o << "double  eta_max_mercury " << job_dbl("eta_max", 1.25e7) << "\n";
   o << "int     ns 2\n";
   o << "double  mole_mass1 0.001\n";
   o << "double  mole_mass2 0.023\n";

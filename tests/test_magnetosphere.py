@@ -72,6 +72,27 @@ def test_reference_jobs_match_the_members():
         assert [float(v) for v in job["initial_line"].split()] == [float(v) for v in c.upstream]
         assert float(job["farfield_line"].split()[0]) == float(c.upstream[0])
         assert job["na_fraction"] == c.na_fraction
+        # the configuration's implicit resistivity, solved to the same tolerance
+        assert c.resistive and job["resistive"] == 1 and job["ksp_rtol"] == c.res_rtol == 1e-10
+        assert (job["eta_r_inner"], job["eta_r_outer"], job["eta_width"]) == (0.0, 1.0, 0.4)
+        assert job["eta_max"] == pytest.approx(1e-3 * 1.256637061e-6 * 4.031e5 * 2.44e6, rel=1e-15)
+
+
+def test_resistivity_window_follows_the_stated_profile():
+    """The tanh window of ETA_CONFIG against eta = 1e-3 exp(-(r - 1) / 0.2):
+    within 1.5 % for r >= 2, 9 % at r = 1.5, half of it at the surface."""
+    from mpcns_mercury_b200 import magnetosphere as M
+
+    c = M.ETA_CONFIG
+    k = M.constants(M.ShellCase(resistive=True, **c))
+    inver_Rem = c["eta_max"] / (k.mu0 * k.U_ref * k.L_ref)
+    assert inver_Rem == pytest.approx(1e-3, rel=1e-12)
+    w, r0, r1 = c["eta_width"], c["eta_r_inner"], c["eta_r_outer"]
+    for r in np.linspace(1.5, 4.0, 11):
+        eta = inver_Rem * 0.5 * (math.tanh((r - r0) / w) - math.tanh((r - r1) / w))
+        assert eta == pytest.approx(1e-3 * math.exp(-(r - 1.0) / 0.2), rel=1.5e-2 if r >= 2.0 else 9e-2)
+    eta1 = inver_Rem * 0.5 * (math.tanh((1.0 - r0) / w) - math.tanh(0.0))
+    assert eta1 == pytest.approx(0.5e-3, rel=2e-2)
 
 
 def test_fluid_tile_shapes_and_shape_classes():
