@@ -755,7 +755,9 @@ def run_shells(args, rank, world, device):
     sampler = ClockSampler(device.index if device.index is not None else 0)
     if rank == 0:
         sampler.start()
+    mixed.substep_ms()  # restart the substep's count
     mixed_ms = _timed_batch_steps(mixed, K, device)
+    mixed_substep = mixed.substep_ms()
     clocks = sampler.stop() if rank == 0 else None
     if err_steps > total:
         mixed.run(err_steps - total)
@@ -772,7 +774,8 @@ def run_shells(args, rank, world, device):
         topo.close()
         return {"metric": METRIC, "value": round(replicas_value(world, ncell, K, mixed_ms), 3), "unit": UNIT,
                 "n_gpus": world, "steps": K, "warmup": W_, "ms_per_step": round(mixed_ms / K, 5),
-                "config": {"workload": "shells", "solves": nsol, "batched_only": True},
+                "config": {"workload": "shells", "solves": nsol, "batched_only": True,
+                           "implicit_substep_ms_per_step": round(mixed_substep, 4)},
                 "kernel_ms": {k: round(v, 5) for k, v in prof.items()}}
 
     # 2) plain FP64, one solve at a time: W untimed, K timed, on to err_steps
@@ -899,6 +902,7 @@ def run_shells(args, rank, world, device):
                                            "bitwise_equal_plain": bool(fp64_identical)},
                    "error_vs_fp64_rel_l2_max_over_solves": {k: float(f"{v:.3e}") for k, v in worst.items()},
                    "error_vs_fp64_of_B_relative_to_total_field": {k: float(f"{v:.3e}") for k, v in worst_tot.items()},
+                   "implicit_substep_ms_per_step": {"mixed_batch": round(mixed_substep, 4)},
                    "error_steps": err_steps, "host_topology_build_s": round(topo_s, 2),
                    "autotune_fluid_tile": {"mixed": _tune_summary(tune_mixed), "fp64": _tune_summary(tune64)}},
         "roofline": roof, "cpu_baseline": cpu,

@@ -503,6 +503,11 @@ int mhd_batch_request(mhd_batch *batch, int slot, int64_t nsteps);
 /* Enqueues nsteps graph launches of the batched step (asynchronous).  Each
  * launch advances every slot that still has steps requested by one step. */
 int mhd_batch_run(mhd_batch *batch, int nsteps);
+/* Mean device time per step of the implicit resistive substep (every
+ * resistive solve at once: prologue, CG loop, epilogue) over the steps run
+ * since the previous call, in ms (0 when none ran); waits for the batch's
+ * stream and restarts the count. */
+int mhd_batch_substep_ms(mhd_batch *batch, double *ms_per_step);
 /* Synchronises and fills infos[0 .. capacity) (empty slots read zero). */
 int mhd_batch_poll(mhd_batch *batch, mhd_info *infos);
 /* Asynchronous form: mhd_batch_poll_async enqueues a snapshot of every slot's

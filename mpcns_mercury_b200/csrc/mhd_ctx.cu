@@ -257,6 +257,11 @@ struct mhd_batch {
   double *hres = nullptr;                               // pinned copy of res.result
   ResCG *hcg = nullptr;                                 // pinned copy of res.cg (one per slot)
   size_t tpart_elems = 0;                               // doubles allocated at res.tpartial
+  // device time of the implicit substep: events around the last one, the sum and count so far
+  cudaEvent_t res_ev[2] = {nullptr, nullptr};
+  bool res_ev_pending = false;
+  double res_ms = 0.0;
+  int64_t res_steps = 0;
   int kernels_per_step = 0;
   double *staging = nullptr;
   size_t staging_elems = 0;
@@ -1289,7 +1294,9 @@ int res_step(mhd_batch *b, const std::vector<int> &slots) {
   if (rc) return rc;
   int nk = 0;
   launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_SNAPSHOT);
-  launch(b, 1, SK_BCELL_JEDGE, &nk);  // Calc_J_Edge on B* (B_cell is refreshed again after the substep)
+  // Calc_J_Edge on B* over the substep's range (the formula of k_bcell_jedge's
+  // J part; B_cell is refreshed after the substep)
+  launch(b, 1, SK_RES_DJ, &nk);
   sync1(b, 1, alias_op(1), &nk);
   if (b->live_sing > 0) launch(b, 1, SK_SING_J, &nk);
   sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), &nk);
@@ -1467,6 +1474,8 @@ int mhd_batch_destroy(mhd_batch *b) {
   if (b->graph_a) cudaGraphExecDestroy(b->graph_a);
   if (b->graph_b) cudaGraphExecDestroy(b->graph_b);
   if (b->graph_cg) cudaGraphExecDestroy(b->graph_cg);
+  for (cudaEvent_t e : b->res_ev)
+    if (e) cudaEventDestroy(e);
   cudaFree(b->res.partial);
   cudaFree(b->res.result);
   cudaFree(b->res.cg);
@@ -2316,9 +2325,13 @@ int mhd_batch_prepare(mhd_batch *b, int slot, double time, int64_t step) {
   if (rc) return rc;
   if (res && (rc = res_range(b, slot))) return rc;
   const Solve *S = b->slots[slot];
-  if (res && S->shadow_slot >= 0 && S->T->sg_n > 0)  // the singular edges' geometry, FP64 in both
-    CUDA_TRY(cudaMemcpyAsync(b->shadow->slots[S->shadow_slot]->sg_geo, S->sg_geo, sizeof(double) * 4 * S->T->sg_n,
-                             cudaMemcpyDeviceToDevice, b->stream));
+  if (res && S->shadow_slot >= 0) {
+    if (S->T->sg_n > 0)  // the singular edges' geometry, FP64 in both
+      CUDA_TRY(cudaMemcpyAsync(b->shadow->slots[S->shadow_slot]->sg_geo, S->sg_geo, sizeof(double) * 4 * S->T->sg_n,
+                               cudaMemcpyDeviceToDevice, b->stream));
+    // the operator's coefficients (alpha, beta, eta, W), widened into the companion once
+    if ((rc = targeted(b, slot, [&](int *) { launch_res_cross(b->dir(1), RES_X_STATIC, b->stream); }))) return rc;
+  }
   b->slots[slot]->prepared = true;  // asynchronous: stream-ordered with the batch's other work
   return MHD_OK;
 }
@@ -2562,6 +2575,30 @@ int mhd_batch_request(mhd_batch *b, int slot, int64_t nsteps) {
   return set_state_field(b, slot, offsetof(SolveState, remaining), &n, sizeof n);
 }
 
+// Adds the last substep's event time to the batch's sum (its events have
+// completed: the caller synchronised the stream after them).
+static void fold_substep_time(mhd_batch *b) {
+  if (!b->res_ev_pending) return;
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, b->res_ev[0], b->res_ev[1]) == cudaSuccess) {
+    b->res_ms += ms;
+    ++b->res_steps;
+  } else {
+    cudaGetLastError();
+  }
+  b->res_ev_pending = false;
+}
+
+int mhd_batch_substep_ms(mhd_batch *b, double *ms_per_step) {
+  if (!b || !ms_per_step) return fail(MHD_ERR_ARG, "mhd_batch_substep_ms: bad arguments");
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  fold_substep_time(b);
+  *ms_per_step = b->res_steps > 0 ? b->res_ms / (double)b->res_steps : 0.0;
+  b->res_ms = 0.0;
+  b->res_steps = 0;
+  return MHD_OK;
+}
+
 int mhd_batch_run(mhd_batch *b, int nsteps) {
   if (!b || nsteps < 0) return fail(MHD_ERR_ARG, "mhd_batch_run: bad arguments");
   int rc;
@@ -2573,16 +2610,26 @@ int mhd_batch_run(mhd_batch *b, int nsteps) {
   // with implicit resistive solves: part A, their substep (all at once, host-driven), part B
   if ((rc = capture(b, &b->graph_a, nullptr, [&](int *nk) { enqueue_step_a(b, nk); }))) return rc;
   if ((rc = capture(b, &b->graph_b, nullptr, [&](int *nk) { enqueue_step_b(b, nk, true); }))) return rc;
+  if (!b->res_ev[0]) {
+    CUDA_TRY(cudaEventCreate(&b->res_ev[0]));
+    CUDA_TRY(cudaEventCreate(&b->res_ev[1]));
+  }
   std::vector<int> slots;
   for (int s = 0; s < nsteps; ++s) {
     CUDA_TRY(cudaGraphLaunch(b->graph_a, b->stream));
     if ((rc = read_state(b))) return rc;
+    fold_substep_time(b);  // the previous step's substep is complete
     slots.clear();
     for (int q = 0; q < b->capacity; ++q) {
       const Solve *S = b->slots[q];
       if (S && S->consts.resistive && b->hstate[q].remaining > 0 && b->hstate[q].status == 0) slots.push_back(q);
     }
+    if (!slots.empty()) CUDA_TRY(cudaEventRecord(b->res_ev[0], b->stream));
     if ((rc = res_step(b, slots))) return rc;
+    if (!slots.empty()) {
+      CUDA_TRY(cudaEventRecord(b->res_ev[1], b->stream));
+      b->res_ev_pending = true;
+    }
     CUDA_TRY(cudaGraphLaunch(b->graph_b, b->stream));
   }
   return MHD_OK;

@@ -2201,15 +2201,19 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
 #if MHD_KERNELS_F32
 // Vectors of the mixed-precision implicit substep between a solve's FP32
 // arena (every masked solve of D) and its FP64 companion (DevSolve::companion:
-// the companion's blocks, the same boxes), over the whole box:
-// RES_X_SETUP: companion alpha, beta, eta, W = the solve's (widened); the
-//   companion's b (B* snapshot arrays) and r = the solve's r (the FP32
-//   right-hand side eta J(B*)); companion x = 0; the companion's dt = the step's.
+// the companion's blocks, the same boxes):
+// RES_X_STATIC (the whole box, once at prepare): companion alpha, beta, eta,
+//   W = the solve's (widened).
+// The others over the substep's range (kResK), where its unknowns are:
+// RES_X_SETUP: the companion's b (B* snapshot arrays) and r = the solve's r
+//   (the FP32 right-hand side eta J(B*)); companion x = 0; the companion's
+//   dt = the step's.
 // RES_X_DEMOTE_R: r = (float) companion r (the next correction's right-hand side).
 // RES_X_ADD_X: companion x += x (the correction).
 // RES_X_DEMOTE_X: x = (float) companion x (the solution).
+template <int KIND>
 __global__ void __launch_bounds__(kTileThreads) k_res_cross(Dir D, int op) {
-  for_items<float, kFull>(D, [&](const DevSolve &S, const V<float> &B, const Item &it) {
+  for_items<float, KIND>(D, [&](const DevSolve &S, const V<float> &B, const Item &it) {
     if (!it.in) return;
     const DevBlock &CB = S.companion[it.blk];
     if (op == RES_X_SETUP && it.blk == 0 && it.i == it.lo[0] && it.j == it.lo[1] && it.k == it.lo[2]) {
@@ -2229,8 +2233,10 @@ __global__ void __launch_bounds__(kTileThreads) k_res_cross(Dir D, int op) {
     const int o = B.off(it.i, it.j, it.k), oc = C.off(it.i, it.j, it.k);
     for (int a = 0; a < 3; ++a) {
       switch (op) {
-        case RES_X_SETUP:
+        case RES_X_STATIC:
           for (int c : {cALX, cBFX, cETAR, cRW}) C.c(c + a)[oc] = (double)B.c(c + a)[o];
+          break;
+        case RES_X_SETUP:
           C.c(cRBS + a)[oc] = C.c(cRR + a)[oc] = (double)B.c(cRR + a)[o];
           C.c(cRX + a)[oc] = 0.0;
           break;
@@ -2244,7 +2250,8 @@ __global__ void __launch_bounds__(kTileThreads) k_res_cross(Dir D, int op) {
 
 void launch_res_cross(const Dir &D, int op, cudaStream_t st) {
   grids<float>();
-  k_res_cross<<<g_grid_tiles, kTileThreads, 0, st>>>(D, op);
+  if (op == RES_X_STATIC) k_res_cross<kFull><<<g_grid_tiles, kTileThreads, 0, st>>>(D, op);
+  else k_res_cross<kResK><<<g_grid_tiles, kTileThreads, 0, st>>>(D, op);
 }
 
 void launch_step_kernel_f32(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int iarg, double darg,

@@ -85,10 +85,11 @@ struct ResScratch {
 void launch_step_kernel(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps *ops, int precision, int iarg = 0,
                         double darg = 0.0, ResScratch rs = ResScratch{nullptr, nullptr});
 int res_dot_grid();
-// Mixed-precision implicit substep: moves its vectors between every masked
-// solve of the FP32 directory D and its FP64 companion (DevSolve::companion;
-// RES_X_SETUP also hands over the step's dt) (k_res_cross, FP32 translation unit).
-enum ResCrossOp { RES_X_SETUP = 0, RES_X_DEMOTE_R, RES_X_ADD_X, RES_X_DEMOTE_X };
+// Mixed-precision implicit substep: moves its coefficients (RES_X_STATIC, at
+// prepare) and vectors between every masked solve of the FP32 directory D and
+// its FP64 companion (DevSolve::companion; RES_X_SETUP also hands over the
+// step's dt) (k_res_cross, FP32 translation unit).
+enum ResCrossOp { RES_X_SETUP = 0, RES_X_DEMOTE_R, RES_X_ADD_X, RES_X_DEMOTE_X, RES_X_STATIC };
 void launch_res_cross(const Dir &D, int op, cudaStream_t st);
 // Per block of the masked solve of D: the largest k of an unknown of the
 // implicit substep into out[block] (atomic max; out starts at -1).
