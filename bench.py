@@ -746,6 +746,8 @@ def run_shells(args, rank, world, device):
     from mpcns_mercury_b200 import autotune
 
     mixed, slots = _shell_batch(cases, ks, topo, 1, err_steps)
+    if getattr(args, "cg_host_loop", False):  # profiling: the CG iterations as plain launches
+        mixed.cg_host_loop(True)
     tune_mixed = autotune.tune(mixed, 1, cells, reps=3, cache=None)
     mixed.run(W_)
     mixed.poll()
@@ -1393,6 +1395,9 @@ def main():
     ap.add_argument("--workload", default="shells",
                     help="shells (default), ensemble, serve, implicit, cube32, cubeN")
     ap.add_argument("--solves", type=int, default=64, help="ensemble: solves per GPU")
+    ap.add_argument("--cg-host-loop", action="store_true",
+                    help="shells: launch the implicit substep's CG iterations from the host (for profilers that do "
+                         "not follow conditional graph nodes)")
     ap.add_argument("--batched-only", action="store_true",
                     help="ensemble: run only the mixed batch (profiling; no plain/FP64 legs, no error check)")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests")

@@ -508,6 +508,11 @@ int mhd_batch_run(mhd_batch *batch, int nsteps);
  * since the previous call, in ms (0 when none ran); waits for the batch's
  * stream and restarts the count. */
 int mhd_batch_substep_ms(mhd_batch *batch, double *ms_per_step);
+/* on != 0: the substep's CG iterations are launched one by one from the host
+ * (the same kernels and results, a host round trip per iteration) instead of
+ * the device loop, for profilers that do not follow conditional graph nodes.
+ * Off by default. */
+int mhd_batch_cg_host_loop(mhd_batch *batch, int on);
 /* Synchronises and fills infos[0 .. capacity) (empty slots read zero). */
 int mhd_batch_poll(mhd_batch *batch, mhd_info *infos);
 /* Asynchronous form: mhd_batch_poll_async enqueues a snapshot of every slot's

@@ -193,7 +193,7 @@ EXPORTS = [
     "mhd_topology_fill_desc", "mhd_topology_destroy", "mhd_batch_create", "mhd_batch_destroy", "mhd_batch_reserve",
     "mhd_div_b", "mhd_batch_div_b", "mhd_setup_geometry", "mhd_batch_setup_geometry", "mhd_restart_values", "mhd_restart_write", "mhd_restart_read",
     "mhd_save_restart", "mhd_load_restart", "mhd_tecplot_write", "mhd_rundata_write", "mhd_rundata_read", "mhd_batch_save_restart", "mhd_batch_load_restart", "mhd_desc_device_bytes", "mhd_batch_add", "mhd_batch_add_periodic", "mhd_batch_add_like", "mhd_batch_remove", "mhd_batch_upload_field",
-    "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run", "mhd_batch_substep_ms",
+    "mhd_batch_download_field", "mhd_batch_sync", "mhd_batch_prepare", "mhd_batch_request", "mhd_batch_run", "mhd_batch_substep_ms", "mhd_batch_cg_host_loop",
     "mhd_batch_poll", "mhd_batch_poll_async", "mhd_batch_poll_wait", "mhd_batch_stream", "mhd_batch_kernels_per_step", "mhd_batch_step_profiled",
     "mhd_batch_device_view", "mhd_shell_nodes", "mhd_shell_grid", "mhd_hall_taper", "mhd_setup_geometry_bg",
     "mhd_batch_setup_geometry_bg", "mhd_fill_field", "mhd_batch_fill_field", "mhd_set_constants",
@@ -309,6 +309,7 @@ def lib() -> ctypes.CDLL:
     L.mhd_batch_request.argtypes = [P, ctypes.c_int, ctypes.c_int64]
     L.mhd_batch_run.argtypes = [P, ctypes.c_int]
     L.mhd_batch_substep_ms.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+    L.mhd_batch_cg_host_loop.argtypes = [P, ctypes.c_int]
     L.mhd_batch_poll.argtypes = [P, ctypes.POINTER(MhdInfo)]
     L.mhd_batch_poll_async.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
     L.mhd_batch_poll_wait.argtypes = [P, ctypes.c_int, ctypes.POINTER(MhdInfo)]
@@ -695,6 +696,10 @@ class Batch:
 
     def run(self, nsteps: int):
         check(lib().mhd_batch_run(self.b, nsteps), "mhd_batch_run")
+
+    def cg_host_loop(self, on: bool = True):
+        """Launch the substep's CG iterations from the host (for profilers)."""
+        check(lib().mhd_batch_cg_host_loop(self.b, int(bool(on))), "mhd_batch_cg_host_loop")
 
     def substep_ms(self) -> float:
         """Mean device ms per step of the implicit substep since the last call."""

@@ -257,6 +257,7 @@ struct mhd_batch {
   double *hres = nullptr;                               // pinned copy of res.result
   ResCG *hcg = nullptr;                                 // pinned copy of res.cg (one per slot)
   size_t tpart_elems = 0;                               // doubles allocated at res.tpartial
+  bool cg_host_loop = false;                            // CG iterations launched one by one from the host
   // device time of the implicit substep: events around the last one, the sum and count so far
   cudaEvent_t res_ev[2] = {nullptr, nullptr};
   bool res_ev_pending = false;
@@ -1026,9 +1027,9 @@ void drop_graphs(mhd_batch *b) {
 }
 
 // Dot product of the CG (2 values) into b->hres.
-int res_dot(mhd_batch *b, int op) {
+int res_dot(mhd_batch *b) {
   int nk = 0;
-  launch(b, 1, SK_RES_DOT, &nk, nullptr, op);
+  launch(b, 1, SK_RES_DOT, &nk);
   launch(b, 1, SK_RES_SUM, &nk);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemcpyAsync(b->hres, b->res.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -1091,6 +1092,7 @@ int build_cg_graph(mhd_batch *b) {
   b->profiling = false;  // no event records inside the graph
   auto fin = [&](cudaError_t e, const char *what) {
     b->profiling = prof;
+    b->res.in_graph = 0;
     cudaGraphDestroy(g);
     return fail(MHD_ERR_CUDA, "CG graph, %s: %s", what, cudaGetErrorString(e));
   };
@@ -1098,6 +1100,7 @@ int build_cg_graph(mhd_batch *b) {
   cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
   if (e != cudaSuccess) return fin(e, "condition");
   b->res.handle = h;
+  b->res.in_graph = 1;  // captured launches set the loop condition
   int nk = 0;
   if ((e = cudaStreamBeginCaptureToGraph(b->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
       cudaSuccess)
@@ -1137,6 +1140,7 @@ int build_cg_graph(mhd_batch *b) {
   if ((e = cudaStreamEndCapture(b->stream, &body)) != cudaSuccess) return fin(e, "body capture");
   e = cudaGraphInstantiate(&b->graph_cg, g, 0);
   b->profiling = prof;
+  b->res.in_graph = 0;
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
     b->graph_cg = nullptr;
@@ -1184,14 +1188,14 @@ struct CgJob {
   int max_it;
 };
 
-// CG on every job's solve at once, each from x = 0 and r = p = its
-// right-hand side (already set), until ||r|| <= tol_factor ||r_0|| or max_it
+// CG on every job's solve at once, each from x = 0 and p = r = its
+// right-hand side (r already set), until ||r|| <= tol_factor ||r_0|| or max_it
 // iterations, the loop on the device (build_cg_graph); the jobs' masks are
 // set here and are all clear on return; one host round trip at the end.
 // Each job's final state is in b->hcg[slot].
 int res_cg_batch(mhd_batch *b, const std::vector<CgJob> &jobs) {
   int rc;
-  if ((rc = ensure_tpartial(b)) || (rc = build_cg_graph(b))) return rc;
+  if ((rc = ensure_tpartial(b)) || (!b->cg_host_loop && (rc = build_cg_graph(b)))) return rc;
   std::vector<int> on((size_t)b->capacity, 0);
   for (int s = 0; s < b->capacity; ++s) {
     b->hcg[s] = ResCG{};
@@ -1206,7 +1210,26 @@ int res_cg_batch(mhd_batch *b, const std::vector<CgJob> &jobs) {
   }
   if ((rc = apply_masks(b, on))) return rc;
   CUDA_TRY(cudaMemcpyAsync(b->res.cg, b->hcg, sizeof(ResCG) * b->capacity, cudaMemcpyHostToDevice, b->stream));
-  CUDA_TRY(cudaGraphLaunch(b->graph_cg, b->stream));
+  if (!b->cg_host_loop) {
+    CUDA_TRY(cudaGraphLaunch(b->graph_cg, b->stream));
+  } else {  // the same kernels launched from the host, the states read back after every iteration
+    int nk = 0;
+    launch(b, 1, SK_RES_CG, &nk, nullptr, CG_INIT);
+    launch(b, 1, SK_RES_CGSUM, &nk, nullptr, CG_INIT);
+    for (;;) {
+      CUDA_TRY(cudaMemcpyAsync(b->hcg, b->res.cg, sizeof(ResCG) * b->capacity, cudaMemcpyDeviceToHost, b->stream));
+      CUDA_TRY(cudaStreamSynchronize(b->stream));
+      bool running = false;
+      for (int s = 0; s < b->capacity; ++s) running = running || !b->hcg[s].done;
+      if (!running) break;  // every solve's loop ends by its own max_it at the latest
+      res_apply_core(b, &nk);
+      launch(b, 1, SK_RES_CG, &nk, nullptr, CG_PQ);
+      launch(b, 1, SK_RES_CGSUM, &nk, nullptr, CG_PQ);
+      launch(b, 1, SK_RES_CG, &nk, nullptr, CG_RR);
+      launch(b, 1, SK_RES_CGSUM, &nk, nullptr, CG_RR);
+      launch(b, 1, SK_RES_PUPD_E, &nk);
+    }
+  }
   CUDA_TRY(cudaMemcpyAsync(b->hcg, b->res.cg, sizeof(ResCG) * b->capacity, cudaMemcpyDeviceToHost, b->stream));
   CUDA_TRY(cudaStreamSynchronize(b->stream));
   std::fill(on.begin(), on.end(), 0);
@@ -1242,7 +1265,7 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
   launch_res_cross(Dm, RES_X_SETUP, st);
   CUDA_TRY(cudaGetLastError());
   const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-10;
-  if ((rc = res_dot(sh, RES_DOT_RR))) return rc;
+  if ((rc = res_dot(sh))) return rc;
   const double bnorm = std::sqrt(sh->hres[1]);
   double rn = bnorm;
   S->res_iters = 0;
@@ -1252,7 +1275,7 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
       launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_P_FROM_X);
       res_apply(sh, &nk);
       launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_RESID);
-      if ((rc = res_dot(sh, RES_DOT_RR))) return rc;
+      if ((rc = res_dot(sh))) return rc;
       rn = std::sqrt(sh->hres[1]);
     }
     if (rn <= rtol * bnorm) {
@@ -1262,7 +1285,6 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
     if (S->res_refinements == kMaxRefinements || !(rn == rn)) break;
     // the correction: FP32 CG on r rounded to FP32, x += d in FP64
     launch_res_cross(Dm, RES_X_DEMOTE_R, st);
-    launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
     if ((rc = res_cg_batch(b, {CgJob{slot, kInnerRtol, S->res_max_it}}))) return rc;
     if ((rc = apply_masks(b, mb))) return rc;  // the loop cleared it
     launch_res_cross(Dm, RES_X_ADD_X, st);
@@ -1336,7 +1358,6 @@ int res_step(mhd_batch *b, const std::vector<int> &slots) {
       }
       if ((rc = apply_masks(b, mb)) || (rc = apply_masks(sh, ms))) return rc;
       launch_res_cross(b->dir(1), RES_X_SETUP, st);
-      launch(sh, 1, SK_RES_VEC, &nk, nullptr, RES_RESTART);
       if ((rc = res_cg_batch(sh, jobs))) return rc;
       launch_res_cross(b->dir(1), RES_X_DEMOTE_X, st);
       CUDA_TRY(cudaGetLastError());
@@ -1454,6 +1475,9 @@ int mhd_batch_create(int capacity, int precision, mhd_batch **out) {
       cudaMalloc(&b->res.cg, sizeof(ResCG) * capacity) != cudaSuccess ||
       cudaMalloc(&b->res.ctl, sizeof(ResCtl)) != cudaSuccess ||
       cudaMemsetAsync(b->res.ctl, 0, sizeof(ResCtl), b->stream) != cudaSuccess ||
+      cudaMalloc(&b->res.chunks, sizeof(double) * 2 * kCgChunks * capacity) != cudaSuccess ||
+      cudaMalloc(&b->res.sarrivals, sizeof(unsigned int) * capacity) != cudaSuccess ||
+      cudaMemsetAsync(b->res.sarrivals, 0, sizeof(unsigned int) * capacity, b->stream) != cudaSuccess ||
       cudaMallocHost(&b->hres, sizeof(double) * 2) != cudaSuccess ||
       cudaMallocHost(&b->hcg, sizeof(ResCG) * capacity) != cudaSuccess)
     return bail(fail(MHD_ERR_OOM, "solver scratch"));
@@ -1480,6 +1504,8 @@ int mhd_batch_destroy(mhd_batch *b) {
   cudaFree(b->res.result);
   cudaFree(b->res.cg);
   cudaFree(b->res.ctl);
+  cudaFree(b->res.chunks);
+  cudaFree(b->res.sarrivals);
   cudaFree(b->res.tpartial);
   if (b->hres) cudaFreeHost(b->hres);
   if (b->hcg) cudaFreeHost(b->hcg);
@@ -1561,6 +1587,7 @@ static int ensure_shadow(mhd_batch *b) {
   sh->stream = b->stream;
   sh->pool = b->pool;
   sh->borrowed = true;
+  sh->cg_host_loop = b->cg_host_loop;
   b->shadow = sh;
   return MHD_OK;
 }
@@ -2587,6 +2614,13 @@ static void fold_substep_time(mhd_batch *b) {
     cudaGetLastError();
   }
   b->res_ev_pending = false;
+}
+
+int mhd_batch_cg_host_loop(mhd_batch *b, int on) {
+  if (!b) return fail(MHD_ERR_ARG, "mhd_batch_cg_host_loop: null batch");
+  b->cg_host_loop = on != 0;
+  if (b->shadow) b->shadow->cg_host_loop = on != 0;
+  return MHD_OK;
 }
 
 int mhd_batch_substep_ms(mhd_batch *b, double *ms_per_step) {

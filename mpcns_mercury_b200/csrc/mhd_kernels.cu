@@ -1070,7 +1070,7 @@ __global__ void __launch_bounds__(kTileThreads) k_res_kmax(Dir D, int *out) {
 
 // Vector operations of the CG on the unknowns (W > 0); other entries stay 0.
 template <class R>
-__global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op, double s) {
+__global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op) {
   for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
     if (!it.in) return;
     const int o = B.off(it.i, it.j, it.k);
@@ -1078,32 +1078,16 @@ __global__ void __launch_bounds__(kTileThreads) k_res_vec(Dir D, int op, double 
       const bool dof = B.c(cRW + a)[o] > R(0.0);
       R *x = B.c(cRX + a) + o, *r = B.c(cRR + a) + o, *p = B.c(cRP + a) + o;
       switch (op) {
-        case RES_INIT: {  // b = eta J (PackImplicitJedgeToVec_, :395-418); x = 0, r = p = b
-          const R bv = dof ? R(0.0) + B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
-          *x = R(0.0);
-          *r = bv;
-          *p = bv;
+        case RES_INIT:  // r = b = eta J (PackImplicitJedgeToVec_, :395-418); the CG's start sets x and p
+          *r = dof ? R(0.0) + B.c(cETAR + a)[o] * B.c(cJX + a)[o] : R(0.0);
           break;
-        }
         case RES_E_FROM_P: B.c(cEX + a)[o] = dof ? *p : R(0.0); break;  // UnpackVecToImplicitEres_ (:294-312)
         case RES_E_FROM_X: B.c(cEX + a)[o] = dof ? *x : R(0.0); break;
-        case RES_RESTART:  // CG on the right-hand side already in r: x = 0, p = r
-          *x = R(0.0);
-          *p = dof ? *r : R(0.0);
-          break;
         case RES_P_FROM_X: *p = dof ? *x : R(0.0); break;
         case RES_RESID:  // r = b - q, b kept in the B* snapshot arrays (FP64 companion of a mixed solve)
           *r = dof ? B.c(cRBS + a)[o] - B.c(cRQ + a)[o] : R(0.0);
           break;
-        case RES_AXPY:
-          if (dof) {
-            *x += R(s) * *p;
-            *r -= R(s) * B.c(cRQ + a)[o];
-          }
-          break;
-        default:  // RES_PUPD
-          if (dof) *p = *r + R(s) * *p;
-          break;
+        default: break;
       }
     }
   });
@@ -1181,10 +1165,9 @@ __global__ void __launch_bounds__(kTileThreads) k_res_q(Dir D) {
   });
 }
 
-// Dot products on the unknowns: op RES_DOT_PQ: (sum W p q, 0); RES_DOT_RR:
-// (sum W r r, sum r r).  Per-CTA partial sums in a fixed order (deterministic).
+// Dot products of r on the unknowns of the masked solve: (sum W r r, sum r r).  Per-CTA partial sums in a fixed order (deterministic).
 template <class R>
-__global__ void __launch_bounds__(kTileThreads) k_res_dot(Dir D, int op, double *partial) {
+__global__ void __launch_bounds__(kTileThreads) k_res_dot(Dir D, double *partial) {
   __shared__ double sh[2][kTileThreads / 32];
   double acc0 = 0.0, acc1 = 0.0;
   for_items<R, kResK>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
@@ -1193,13 +1176,9 @@ __global__ void __launch_bounds__(kTileThreads) k_res_dot(Dir D, int op, double 
     for (int a = 0; a < 3; ++a) {
       const double w = (double)B.c(cRW + a)[o];
       if (!(w > 0.0)) continue;
-      if (op == RES_DOT_PQ) {
-        acc0 += w * (double)B.c(cRP + a)[o] * (double)B.c(cRQ + a)[o];
-      } else {
-        const double r = (double)B.c(cRR + a)[o];
-        acc0 += w * r * r;
-        acc1 += r * r;
-      }
+      const double r = (double)B.c(cRR + a)[o];
+      acc0 += w * r * r;
+      acc1 += r * r;
     }
   });
   for (int of = 16; of > 0; of >>= 1) {
@@ -1237,11 +1216,14 @@ __global__ void k_res_sum(const double *partial, int n, double *result) {
 // each warp writes its sums over each tile to its own slot of tpart (2
 // doubles per warp and tile), k_res_cg_sum then adds a solve's slots in a
 // fixed order (deterministic) and updates its scalars.  CG_PQ first clears
-// the loop condition, so a loop whose stop test did not run ends.
+// the loop condition, so a loop whose stop test did not run ends.  Both
+// kernels write the condition of the loop graph they belong to
+// (build_cg_graph) only when launched inside it (in_graph; the host-driven
+// loop of res_cg_batch reads the states instead).
 template <class R>
 __global__ void __launch_bounds__(kTileThreads) k_res_cg(Dir D, int op, double *tpart, const ResCG *cg,
-                                                         cudaGraphConditionalHandle handle) {
-  if (op == CG_PQ && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
+                                                         cudaGraphConditionalHandle handle, int in_graph) {
+  if (in_graph && op == CG_PQ && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
   double acc0 = 0.0, acc1 = 0.0;
   for_items<R, kResK>(
       D,
@@ -1254,8 +1236,11 @@ __global__ void __launch_bounds__(kTileThreads) k_res_cg(Dir D, int op, double *
           const bool dof = wr > R(0.0);
           const double w = (double)wr;
           R *x = B.c(cRX + a) + o, *r = B.c(cRR + a) + o, *p = B.c(cRP + a) + o, *q = B.c(cRQ + a) + o;
-          if (op == CG_INIT) {
-            B.c(cEX + a)[o] = dof ? *p : R(0.0);
+          if (op == CG_INIT) {  // x = 0, p = r (the start), E_res = p
+            const R pv = dof ? *r : R(0.0);
+            *x = R(0.0);
+            *p = pv;
+            B.c(cEX + a)[o] = pv;
             if (w > 0.0) {
               const double rv = (double)*r;
               acc0 += w * rv * rv;
@@ -1292,19 +1277,27 @@ __global__ void __launch_bounds__(kTileThreads) k_res_cg(Dir D, int op, double *
       });
 }
 
-// The per-solve end of a k_res_cg step: CTA s adds solve s's tile partials
-// (threads stride over them, then a fixed tree) and updates its state; a
-// solve whose loop ends (converged, max_it, breakdown) leaves the mask, so
-// the following kernels skip it.  The last CTA to finish (atomic ticket)
-// sets the loop condition after CG_INIT and CG_RR: some solve still running.
+// The per-solve end of a k_res_cg step: kCgChunks CTAs per slot, CTA c of
+// solve s adds chunk c of the solve's tile partials (threads stride over it,
+// then a fixed tree); the last of them (atomic ticket per solve) adds the
+// chunks in order and updates the solve's state; a solve whose loop ends
+// (converged, max_it, breakdown) leaves the mask, so the following kernels
+// skip it.  The last slot to report (atomic ticket) sets the loop condition
+// after CG_INIT and CG_RR: some solve still running.  Every sum has fixed
+// bounds and order (deterministic, and the same for a solve alone or in a
+// batch).
 __global__ void __launch_bounds__(kTileThreads) k_res_cg_sum(Dir D, int op, const double *tpart, ResCG *cg,
-                                                             ResCtl *ctl, cudaGraphConditionalHandle handle) {
+                                                             ResCtl *ctl, double *chunks, unsigned int *sarr,
+                                                             cudaGraphConditionalHandle handle, int in_graph) {
   __shared__ double sh[2][kWarpsPerTile];
-  __shared__ unsigned int ticket;
-  const int s = blockIdx.x;
-  if (s < D.nsolves && solve_active(D, s)) {  // the whole CTA agrees
+  const int s = blockIdx.x / kCgChunks, c = blockIdx.x % kCgChunks;
+  const bool act = s < D.nsolves && solve_active(D, s);  // the whole CTA agrees
+  bool last_of_solve = false;
+  if (act) {
     const int *sp = D.solve_tile_prefix[kResK];
-    const int64_t a = (int64_t)sp[s] * kWarpsPerTile, e = (int64_t)sp[s + 1] * kWarpsPerTile;
+    const int64_t a0 = (int64_t)sp[s] * kWarpsPerTile, n = (int64_t)(sp[s + 1] - sp[s]) * kWarpsPerTile;
+    const int64_t len = (n + kCgChunks - 1) / kCgChunks;
+    const int64_t a = a0 + min(n, (int64_t)c * len), e = a0 + min(n, (int64_t)(c + 1) * len);
     double u0 = 0.0, u1 = 0.0;
     for (int64_t q = a + threadIdx.x; q < e; q += kTileThreads) {
       u0 += tpart[2 * q];
@@ -1325,40 +1318,51 @@ __global__ void __launch_bounds__(kTileThreads) k_res_cg_sum(Dir D, int op, cons
         t0 += sh[0][w];
         t1 += sh[1][w];
       }
-      ResCG &c = cg[s];
-      if (op == CG_INIT) {
-        c.rho = t0;
-        c.r0 = c.rnorm = sqrt(t1);
-        c.tol = c.tol_factor * c.r0;
-        c.it = 0;
-        c.converged = c.rnorm <= c.tol;
-        c.done = c.converged || c.max_it <= 0;
-      } else if (op == CG_PQ) {
-        if (!(t0 > 0.0)) c.done = 1;  // breakdown: not positive definite on these unknowns
-        else c.alpha = c.rho / t0;
-      } else {
-        c.it += 1;
-        c.rnorm = sqrt(t1);
-        if (c.rnorm <= c.tol) c.converged = c.done = 1;
-        else if (c.it >= c.max_it) c.done = 1;
-        c.beta = t0 / c.rho;
-        c.rho = t0;
-      }
-      if (c.done) D.state[s].mask = 0;
-      else atomicAdd(&ctl->running, 1);
+      chunks[2 * (s * kCgChunks + c)] = t0;
+      chunks[2 * (s * kCgChunks + c) + 1] = t1;
+      __threadfence();
+      last_of_solve = atomicAdd(&sarr[s], 1u) == kCgChunks - 1;
     }
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x != 0) return;
+  if (act ? !last_of_solve : c != 0) return;  // one report per slot: its last chunk, or chunk 0 of an idle slot
+  if (act) {  // every chunk of solve s is in
     __threadfence();
-    ticket = atomicAdd(&ctl->arrivals, 1u);
+    sarr[s] = 0;
+    double t0 = 0.0, t1 = 0.0;
+    for (int q = 0; q < kCgChunks; ++q) {
+      t0 += __ldcg(chunks + 2 * (s * kCgChunks + q));
+      t1 += __ldcg(chunks + 2 * (s * kCgChunks + q) + 1);
+    }
+    ResCG &cs = cg[s];
+    if (op == CG_INIT) {
+      cs.rho = t0;
+      cs.r0 = cs.rnorm = sqrt(t1);
+      cs.tol = cs.tol_factor * cs.r0;
+      cs.it = 0;
+      cs.converged = cs.rnorm <= cs.tol;
+      cs.done = cs.converged || cs.max_it <= 0;
+    } else if (op == CG_PQ) {
+      if (!(t0 > 0.0)) cs.done = 1;  // breakdown: not positive definite on these unknowns
+      else cs.alpha = cs.rho / t0;
+    } else {
+      cs.it += 1;
+      cs.rnorm = sqrt(t1);
+      if (cs.rnorm <= cs.tol) cs.converged = cs.done = 1;
+      else if (cs.it >= cs.max_it) cs.done = 1;
+      cs.beta = t0 / cs.rho;
+      cs.rho = t0;
+    }
+    if (cs.done) D.state[s].mask = 0;
+    else atomicAdd(&ctl->running, 1);
   }
-  __syncthreads();
-  if (threadIdx.x != 0 || ticket != gridDim.x - 1) return;
+  __threadfence();
+  if (atomicAdd(&ctl->arrivals, 1u) != (unsigned)(gridDim.x / kCgChunks) - 1) return;  // the last slot to report
   __threadfence();
   const int running = atomicAdd(&ctl->running, 0);
   ctl->arrivals = 0;
   ctl->running = 0;
-  if (op != CG_PQ) cudaGraphSetConditional(handle, running > 0 ? 1u : 0u);
+  if (in_graph && op != CG_PQ) cudaGraphSetConditional(handle, running > 0 ? 1u : 0u);
 }
 
 // p = r + beta p and E_res = p on the unknowns (the next iteration's
@@ -2171,16 +2175,21 @@ static void launch_as(StepKernel k, const Dir &D, cudaStream_t st, const SyncOps
     case SK_DIVB: k_div_b<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_RES_SEED: k_res_seed<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_RES_W: k_res_w<R><<<G, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_VEC: k_res_vec<R><<<G, kTileThreads, 0, st>>>(D, iarg, darg); break;
+    case SK_RES_VEC: k_res_vec<R><<<G, kTileThreads, 0, st>>>(D, iarg); break;
     case SK_RES_DB: k_res_db<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_RES_DJ: k_res_dj<R><<<G, kTileThreads, 0, st>>>(D); break;
     case SK_RES_Q: k_res_q<R><<<G, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_DOT: k_res_dot<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.partial); break;
+    case SK_RES_DOT: k_res_dot<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, rs.partial); break;
     case SK_RES_SUM: k_res_sum<<<1, 32, 0, st>>>(rs.partial, g_grid_tiles, rs.result); break;
     case SK_RES_COPYB: k_res_copyb<R><<<G, kTileThreads, 0, st>>>(D, iarg); break;
     case SK_RES_BUPDATE: k_res_bupdate<R><<<G, kTileThreads, 0, st>>>(D); break;
-    case SK_RES_CG: k_res_cg<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.tpartial, rs.cg, rs.handle); break;
-    case SK_RES_CGSUM: k_res_cg_sum<<<D.nsolves, kTileThreads, 0, st>>>(D, iarg, rs.tpartial, rs.cg, rs.ctl, rs.handle); break;
+    case SK_RES_CG:
+      k_res_cg<R><<<g_grid_tiles, kTileThreads, 0, st>>>(D, iarg, rs.tpartial, rs.cg, rs.handle, rs.in_graph);
+      break;
+    case SK_RES_CGSUM:
+      k_res_cg_sum<<<D.nsolves * kCgChunks, kTileThreads, 0, st>>>(D, iarg, rs.tpartial, rs.cg, rs.ctl, rs.chunks,
+                                                                   rs.sarrivals, rs.handle, rs.in_graph);
+      break;
     case SK_RES_PUPD_E: k_res_pupd_e<R><<<G, kTileThreads, 0, st>>>(D, rs.cg); break;
     case SK_FLIP: k_flip<<<1, 128, 0, st>>>(D); break;
     case SK_RETIRE: k_retire<<<1, 128, 0, st>>>(D); break;

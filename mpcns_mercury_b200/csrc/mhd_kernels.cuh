@@ -38,8 +38,7 @@ struct SyncOps {
 };
 
 // Operations of SK_RES_VEC / SK_RES_DOT / SK_RES_COPYB (the arg of the launch).
-enum ResVecOp { RES_INIT = 0, RES_E_FROM_P, RES_E_FROM_X, RES_AXPY, RES_PUPD, RES_RESTART, RES_P_FROM_X, RES_RESID };
-enum ResDotOp { RES_DOT_PQ = 0, RES_DOT_RR };
+enum ResVecOp { RES_INIT = 0, RES_E_FROM_P, RES_E_FROM_X, RES_P_FROM_X, RES_RESID };
 enum ResCopyOp { RES_SNAPSHOT = 0, RES_RESTORE };
 
 // CG state of one solve on the device (one per slot), for the iteration
@@ -53,19 +52,20 @@ struct ResCG {
   int it, max_it;           // iterations taken, at most max_it
   int done, converged;      // loop over (converged, max_it reached, or breakdown)
 };
-// The loop's shared counters: CTAs of k_res_cg_sum finished, solves still iterating.
+// The loop's shared counters: slots of k_res_cg_sum reported, solves still iterating.
 struct ResCtl {
   unsigned int arrivals;
   int running;
 };
-// Steps of k_res_cg: CG_INIT: E = p, (r.r)_W and r.r, sets rho, r0, tol;
+// Steps of k_res_cg: CG_INIT: x = 0, p = r, E = p, (r.r)_W and r.r, sets rho, r0, tol;
 // CG_PQ: q = A p (its last part, E - eta dJ) and (p.q)_W, sets alpha;
 // CG_RR: x += alpha p, r -= alpha q, (r.r)_W and r.r, the stop test and beta.
-// k_res_cg writes one partial pair per warp and tile; k_res_cg_sum (one CTA
-// per slot) sums a solve's pairs in a fixed order and updates its state; a
-// solve whose loop is over leaves the mask.
+// k_res_cg writes one partial pair per warp and tile; k_res_cg_sum
+// (kCgChunks CTAs per slot) sums a solve's pairs in fixed chunks and a fixed
+// order and updates its state; a solve whose loop is over leaves the mask.
 enum ResCgOp { CG_INIT = 0, CG_PQ, CG_RR };
 constexpr int kWarpsPerTile = kTileThreads / 32;
+constexpr int kCgChunks = 32;
 
 // Scratch of the CG dot products: per-CTA partial sums and the two results
 // (k_res_dot, one masked solve); the per-slot CG states, the per-warp tile
@@ -76,7 +76,10 @@ struct ResScratch {
   ResCG *cg = nullptr;
   double *tpartial = nullptr;  // 2 per warp of every kResK tile
   ResCtl *ctl = nullptr;
+  double *chunks = nullptr;           // 2 per chunk of every slot (k_res_cg_sum)
+  unsigned int *sarrivals = nullptr;  // per slot: its chunks summed so far
   unsigned long long handle = 0;  // cudaGraphConditionalHandle of the loop
+  int in_graph = 0;               // the CG kernels set the loop condition (launched inside the loop graph)
 };
 
 // Launch one engine kernel over the directory D (ops: SK_SYNC only) in the

@@ -180,3 +180,37 @@ def test_unconverged_substep_reports_solve_status(res_dump, precision, direct):
         assert info.res_refinements == 30 and info.res_iters == 30
     assert info.res_relres > 1e-14
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_host_driven_cg_loop_matches_the_device_loop(res_dump, precision):
+    """The substep's CG iterations launched from the host (for profilers)
+    give the device loop's results bit for bit: the same kernels and the
+    same fixed-order sums."""
+    import mercury_oracle as mo
+    from gpu_helpers import NGHOST, upload_from_dump
+    from mpcns_mercury_b200.capi import REF_FIELD, Batch, SolveDesc
+
+    import numpy as np
+
+    k = _mixed_constants()
+    k.res_rtol = 1e-12 if precision == 0 else 1e-10
+    out = []
+    for host in (False, True):
+        d = SolveDesc([(16, 16, 16)], NGHOST, k, precision=precision)
+        b = Batch(1, precision)
+        s = b.add(d)
+        if host:
+            b.cg_host_loop(True)
+        upload_from_dump(lambda f, a, lo, hi: b.upload(s, f, a, lo, hi), res_dump)
+        b.prepare(s)
+        b.request(s, 3)
+        b.run(3)
+        inf = b.poll()[s]
+        assert inf.status == 0 and inf.step == 3 and inf.res_iters > 0
+        out.append({n: b.download(s, REF_FIELD[n], res_dump[("step10:" + n, 0)].lo, res_dump[("step10:" + n, 0)].hi)
+                    for n in mo.STATE_FIELDS})
+        b.close()
+        d.close()
+    for n in mo.STATE_FIELDS:
+        assert np.array_equal(out[0][n], out[1][n]), n
