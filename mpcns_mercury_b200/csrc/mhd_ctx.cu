@@ -20,6 +20,7 @@
 #include <new>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <utility>
 #include <vector>
 
@@ -1063,8 +1064,7 @@ void sync_after_owner(mhd_batch *b, int mode, int g, int *nk) {
 void res_apply_core(mhd_batch *b, int *nk) {  // from E_res (set) to dJ (synced)
   sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner), nk);  // HALO_OWNER::sync_edge_1form
   sync_after_owner(b, 1, MHD_SYNC_ERES, nk);           // Sync("Eres")
-  launch(b, 1, SK_RES_DB, nk);
-  if (open_grids(b)) launch(b, 1, SK_RES_CLEARB, nk);
+  launch(b, 1, SK_RES_DB, nk);  // the ghost faces were cleared at the substep's start (res_step)
   enqueue_sync(b, 1, MHD_SYNC_DB, nk);
   launch(b, 1, SK_RES_DJ, nk);
   sync1(b, 1, alias_op(1), nk);
@@ -1261,8 +1261,9 @@ int res_refine(mhd_batch *b, int slot, Solve *S, bool *converged) {
   mb[slot] = 1;
   ms[cs] = 1;
   if ((rc = apply_masks(b, mb)) || (rc = apply_masks(sh, ms))) return rc;
-  // the companion's dt, coefficients, b and x = 0
+  // the companion's dt, b and x = 0; its dB ghost faces
   launch_res_cross(Dm, RES_X_SETUP, st);
+  if (open_grids(sh)) launch(sh, 1, SK_RES_CLEARB, &nk);
   CUDA_TRY(cudaGetLastError());
   const double rtol = S->res_rtol > 0.0 ? S->res_rtol : 1e-10;
   if ((rc = res_dot(sh))) return rc;
@@ -1320,10 +1321,13 @@ int res_step(mhd_batch *b, const std::vector<int> &slots) {
   // J part; B_cell is refreshed after the substep)
   launch(b, 1, SK_RES_DJ, &nk);
   sync1(b, 1, alias_op(1), &nk);
-  if (b->live_sing > 0) launch(b, 1, SK_SING_J, &nk);
+  if (b->live_sing > 0) launch(b, 1, SK_SING_J, &nk);  // reads B* around the singular edges
   sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), &nk);
   sync_after_owner(b, 1, MHD_SYNC_JEDGE, &nk);
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_INIT);
+  // the B arrays turn into the operator's dB: its ghost faces start at zero
+  // (restored with B* at the end)
+  if (open_grids(b)) launch(b, 1, SK_RES_CLEARB, &nk);
   std::vector<char> conv((size_t)b->capacity, 0);
   auto take = [&](Solve *S, const ResCG &h, int s) {
     S->res_iters = h.it;
@@ -1358,6 +1362,7 @@ int res_step(mhd_batch *b, const std::vector<int> &slots) {
       }
       if ((rc = apply_masks(b, mb)) || (rc = apply_masks(sh, ms))) return rc;
       launch_res_cross(b->dir(1), RES_X_SETUP, st);
+      if (open_grids(sh)) launch(sh, 1, SK_RES_CLEARB, &nk);  // the companions' dB ghost faces
       if ((rc = res_cg_batch(sh, jobs))) return rc;
       launch_res_cross(b->dir(1), RES_X_DEMOTE_X, st);
       CUDA_TRY(cudaGetLastError());
@@ -1706,6 +1711,38 @@ static int upload_phys(Solve *S, const mhd_desc *desc, cudaStream_t st) {
       }
       if (!ok2) return fail(MHD_ERR_ARG, "physical operation %d of table %d: source out of range", t, q);
       other.push_back(d);
+    }
+    if (q == MHD_SYNC_DB && S->consts.resistive) {
+      // The reference clears dB before every Sync(dB) (clear_triplet,
+      // Mercury_ImplicitResistive.cpp:428); the substep clears the ghost
+      // faces once and then, per sync, zeroes here the ghost faces its copies
+      // read (the others keep their zeros or are rewritten by the sync)
+      std::unordered_set<int64_t> written;
+      for (int t = 0; t < n; ++t) {
+        bool ok = false;
+        written.insert(S->code(ops[t].dst, &ok));
+      }
+      const mhd_sync_group &G = desc->groups[q];
+      auto ghost = [&](const mhd_dof &d) {
+        if (d.field < MHD_B_XI || d.field > MHD_B_ZETA || d.block < 0 || d.block >= S->nblocks) return false;
+        const int ax = d.field - MHD_B_XI;
+        const int *nb = S->boxes[d.block].n;
+        const int x[3] = {d.i, d.j, d.k};
+        for (int a = 0; a < 3; ++a)
+          if (x[a] < 0 || x[a] >= nb[a] + (a == ax ? 1 : 0)) return true;
+        return false;
+      };
+      auto zero_src = [&](const mhd_copy *tab, int m) {
+        for (int t = 0; t < m; ++t) {
+          if (!ghost(tab[t].src)) continue;
+          bool ok = false;
+          const int64_t c = S->code(tab[t].src, &ok);
+          if (ok && written.insert(c).second) set.push_back(c | ((int64_t)MHD_BC_ZERO << kPhysArgShift));
+        }
+      };
+      zero_src(G.halo, G.n_halo);
+      zero_src(G.owner, G.n_owner);
+      if (G.n_stash > 0 && G.stash) zero_src(G.stash, G.n_stash);
     }
     // the constant writes as segments: runs of up to 32 consecutive
     // destinations of one value, runs of equal length and value whose starts
