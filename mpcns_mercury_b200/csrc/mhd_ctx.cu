@@ -159,6 +159,9 @@ struct Tables {
   // copy, alias or singular-edge record that carries a value to a lower k
   // (-1: every one keeps k or raises it; INT_MAX: unknown, no restriction)
   int res_kdown = INT_MAX;
+  // Every halo, staged and physical write of Sync(Eres) and Sync(Jedge) lands
+  // on a ghost position (res_light_syncs)
+  bool res_ghost_writes_only = false;
 };
 
 struct Solve {
@@ -250,6 +253,7 @@ struct mhd_batch {
   int live_phys[kNumPhys] = {};
   int live_sing = 0;
   int n_res = 0;                                        // slots whose solve has the implicit resistive substep
+  int n_res_full = 0;                                   // of them, solves whose substep runs the full E / J syncs
   // FP64 batch of the companions of mixed-precision resistive solves, which
   // runs on this batch's stream and pool (borrowed = true in the companion)
   mhd_batch *shadow = nullptr;
@@ -1014,6 +1018,10 @@ bool count_tables(mhd_batch *b, const Solve *S, int d) {
     grew = grew || (d > 0 && b->live_sing == 0);
     b->live_sing += d;
   }
+  if (S->consts.resistive && !S->T->res_ghost_writes_only) {
+    grew = grew || (d > 0 && b->n_res_full == 0);
+    b->n_res_full += d;
+  }
   return grew;
 }
 
@@ -1061,16 +1069,28 @@ void sync_after_owner(mhd_batch *b, int mode, int g, int *nk) {
   if (b->live_phys[g] == 0 && b->live_tables[g][kPhHalo] == 0 && b->live_tables[g][kPhStash] == 0) return;
   enqueue_sync(b, mode, g, nk);
 }
+// With every solve's Sync(Eres) and Sync(Jedge) writing ghosts only (beyond
+// their owner copies; res_ghost_writes_only), the substep runs the owner
+// copies of E_res and the alias reduction of dJ and leaves out the rest of
+// those two syncs: nothing it reads changes.
+bool res_light_syncs(const mhd_batch *b) { return b->n_res_full == 0; }
+void res_sync_eres(mhd_batch *b, int *nk) {
+  sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner), nk);                  // HALO_OWNER::sync_edge_1form
+  if (!res_light_syncs(b)) sync_after_owner(b, 1, MHD_SYNC_ERES, nk);  // Sync("Eres")
+}
+void res_sync_dj(mhd_batch *b, int *nk) {  // after the current's alias reduction and the singular edges
+  if (res_light_syncs(b)) return;
+  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), nk);
+  sync_after_owner(b, 1, MHD_SYNC_JEDGE, nk);  // Sync("dJ")
+}
 void res_apply_core(mhd_batch *b, int *nk) {  // from E_res (set) to dJ (synced)
-  sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner), nk);  // HALO_OWNER::sync_edge_1form
-  sync_after_owner(b, 1, MHD_SYNC_ERES, nk);           // Sync("Eres")
+  res_sync_eres(b, nk);
   launch(b, 1, SK_RES_DB, nk);  // the ghost faces were cleared at the substep's start (res_step)
   enqueue_sync(b, 1, MHD_SYNC_DB, nk);
   launch(b, 1, SK_RES_DJ, nk);
   sync1(b, 1, alias_op(1), nk);
   if (b->live_sing > 0) launch(b, 1, SK_SING_J, nk);  // AssembleSingularEdgeCurrent_(dB, dJ)
-  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), nk);
-  sync_after_owner(b, 1, MHD_SYNC_JEDGE, nk);         // Sync("dJ")
+  res_sync_dj(b, nk);
 }
 void res_apply(mhd_batch *b, int *nk) {
   launch(b, 1, SK_RES_VEC, nk, nullptr, RES_E_FROM_P);
@@ -1322,8 +1342,7 @@ int res_step(mhd_batch *b, const std::vector<int> &slots) {
   launch(b, 1, SK_RES_DJ, &nk);
   sync1(b, 1, alias_op(1), &nk);
   if (b->live_sing > 0) launch(b, 1, SK_SING_J, &nk);  // reads B* around the singular edges
-  sync1(b, 1, copy_op(MHD_SYNC_JEDGE, kPhOwner), &nk);
-  sync_after_owner(b, 1, MHD_SYNC_JEDGE, &nk);
+  res_sync_dj(b, &nk);
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_INIT);
   // the B arrays turn into the operator's dB: its ghost faces start at zero
   // (restored with B* at the end)
@@ -1382,8 +1401,7 @@ int res_step(mhd_batch *b, const std::vector<int> &slots) {
     }
   // E_res = x, its owner copies; B = B* + dt (-curl E_res) on the owned faces
   launch(b, 1, SK_RES_VEC, &nk, nullptr, RES_E_FROM_X);
-  sync1(b, 1, copy_op(MHD_SYNC_ERES, kPhOwner), &nk);
-  sync_after_owner(b, 1, MHD_SYNC_ERES, &nk);
+  res_sync_eres(b, &nk);
   launch(b, 1, SK_RES_COPYB, &nk, nullptr, RES_RESTORE);
   launch(b, 1, SK_RES_BUPDATE, &nk);
   CUDA_TRY(cudaGetLastError());
@@ -1658,6 +1676,34 @@ static int res_kdown(const mhd_desc *desc) {
       for (int q = g.face_offset[e]; q < g.face_offset[e + 1]; ++q) flow(g.faces[q].face.k, k);
     }
   return m;
+}
+
+// Whether every halo, staged and physical write of Sync(Eres) and of
+// Sync(Jedge) lands on a ghost position (outside the owned range of its
+// field).  The substep reads E_res only at owned positions (the curl of the
+// owned faces) and dJ only at its unknowns (owned owner positions), so then
+// those syncs change nothing it reads beyond the owner copies of E_res and
+// the alias reduction of dJ.
+static bool res_ghost_writes_only(const Solve *S, const mhd_desc *desc) {
+  auto ghost = [&](const mhd_dof &d) {
+    if (d.field < 0 || d.field >= MHD_NUM_FIELDS || d.block < 0 || d.block >= S->nblocks) return false;
+    const int *st = kStagger[kFieldSpec[d.field].loc];
+    const int *nb = S->boxes[d.block].n;
+    const int x[3] = {d.i, d.j, d.k};
+    for (int a = 0; a < 3; ++a)
+      if (x[a] < 0 || x[a] >= nb[a] + st[a]) return true;
+    return false;
+  };
+  for (int g : {(int)MHD_SYNC_ERES, (int)MHD_SYNC_JEDGE}) {
+    const mhd_sync_group &G = desc->groups[g];
+    for (int t = 0; t < G.n_halo; ++t)
+      if (!ghost(G.halo[t].dst)) return false;
+    for (int t = 0; t < G.n_stash; ++t)  // the staged copies' destinations (the second half)
+      if (!ghost(G.stash[G.n_stash + t].dst)) return false;
+    for (int t = 0; t < G.n_phys; ++t)
+      if (!ghost(G.phys[t].dst)) return false;
+  }
+  return true;
 }
 
 static int upload_phys(Solve *S, const mhd_desc *desc, cudaStream_t st) {
@@ -1988,7 +2034,10 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
       if ((rc = upload_aliases(S, desc->edge_aliases, st))) return bail(rc);
       if ((rc = upload_phys(S, desc, st))) return bail(rc);
       if ((rc = upload_singular(S, desc->singular, st)) || (rc = alloc_singular_geo(S, st))) return bail(rc);
-      if (S->consts.resistive) S->T->res_kdown = res_kdown(desc);
+      if (S->consts.resistive) {
+        S->T->res_kdown = res_kdown(desc);
+        S->T->res_ghost_writes_only = res_ghost_writes_only(S, desc);
+      }
     }
   } catch (...) {  // host allocation or thread creation failed
     return bail(fail(MHD_ERR_OOM, "host memory for the copy tables"));
