@@ -188,6 +188,14 @@ def make_context(cells, fields, pinned=None):
     return ctx, h2d
 
 
+# Members of the magnetosphere ensemble in the default shells workload: the
+# first 32 of its seeded draws (19.7 M owned cells).  A mixed-precision solve
+# with the implicit resistive substep holds its FP32 fields and an FP64
+# companion for the substep, about 7 KB per owned cell with the ghost layers
+# (139 GB for these 32); all 64 draws (40.2 M cells) would need 283 GB.
+SHELL_SOLVES = 32
+
+
 def owned_cells(cells):
     return sum(a * b * c for a, b, c in cells)
 
@@ -1401,7 +1409,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="shells",
                     help="shells (default), ensemble, serve, implicit, cube32, cubeN")
-    ap.add_argument("--solves", type=int, default=64, help="ensemble: solves per GPU")
+    ap.add_argument("--solves", type=int, default=None,
+                    help="ensemble / shells: solves per GPU (default: 64 periodic boxes; the first "
+                         f"{SHELL_SOLVES} magnetosphere shells, which fit in HBM with their FP64 companions)")
     ap.add_argument("--cg-host-loop", action="store_true",
                     help="shells: launch the implicit substep's CG iterations from the host (for profilers that do "
                          "not follow conditional graph nodes)")
@@ -1424,6 +1434,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.solves is None:
+        args.solves = SHELL_SOLVES if args.workload == "shells" else 64
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
