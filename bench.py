@@ -785,7 +785,8 @@ def run_shells(args, rank, world, device):
         return {"metric": METRIC, "value": round(replicas_value(world, ncell, K, mixed_ms), 3), "unit": UNIT,
                 "n_gpus": world, "steps": K, "warmup": W_, "ms_per_step": round(mixed_ms / K, 5),
                 "config": {"workload": "shells", "solves": nsol, "batched_only": True,
-                           "implicit_substep_ms_per_step": round(mixed_substep, 4)},
+                           "implicit_substep_ms_per_step": round(mixed_substep, 4),
+                           "autotune_fluid_tile": {"mixed": _tune_summary(tune_mixed)}},
                 "kernel_ms": {k: round(v, 5) for k, v in prof.items()}}
 
     # 2) plain FP64, one solve at a time: W untimed, K timed, on to err_steps

@@ -42,7 +42,9 @@ enum mhd_status {
   MHD_ERR_NONFINITE = 5,/* a NaN/Inf in an owned cell's state: the solve is retired
                            at its next step, the batch's other solves go on */
   MHD_ERR_SOLVE = 6,    /* implicit solve did not converge */
-  MHD_ERR_STATE = 7     /* call out of order (e.g. step before prepare) */
+  MHD_ERR_STATE = 7,    /* call out of order (e.g. step before prepare) */
+  MHD_ERR_TIMEOUT = 8   /* a tile's staged copies did not complete within the fluid
+                           kernel's bounded wait (TMA-staged variant): the solve stops */
 };
 
 /* Field identifiers: the reference's catalog names
@@ -492,8 +494,10 @@ int mhd_batch_prepare(mhd_batch *batch, int slot, double time, int64_t step);
  * only the next-step state buffer, which the next step rewrites: the solves'
  * results do not change), mhd_batch_fluid_tile sets one (the step graphs are
  * captured anew).  The choice does not change results: every variant
- * computes each face flux and cell update with the same operations. */
-#define MHD_NUM_FLUID_TILES 6
+ * computes each face flux and cell update with the same operations.
+ * Variant 6 (16 x 4 x 4) stages each tile's cells with TMA tensor copies,
+ * the next tile's while the current one is computed. */
+#define MHD_NUM_FLUID_TILES 7
 int mhd_fluid_tile_shape(int variant, int32_t shape[4]);
 int mhd_batch_fluid_tile(mhd_batch *batch, int variant);
 int mhd_batch_time_fluid_tiles(mhd_batch *batch, int reps, float ms[MHD_NUM_FLUID_TILES]);

@@ -62,7 +62,7 @@ REF_FIELD = {
 
 GROUPS = ["UCELL", "BFACE", "EHALL", "EEDGE", "B_CELL", "JEDGE", "J_CELL", "ERES", "DB", "BADD"]
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_DT", 5: "ERR_NONFINITE", 6: "ERR_SOLVE",
-          7: "ERR_STATE"}
+          7: "ERR_STATE", 8: "ERR_TIMEOUT"}
 
 
 class MhdConstants(ctypes.Structure):
@@ -789,7 +789,7 @@ class Batch:
             pass
 
 
-NUM_FLUID_TILES = 6  # MHD_NUM_FLUID_TILES
+NUM_FLUID_TILES = 7  # MHD_NUM_FLUID_TILES
 
 
 def fluid_tile_shape(variant: int):

@@ -8,6 +8,8 @@
 // stream-ordered copies between graph launches.
 //
 // mhd_ctx (one solve) is a batch of capacity 1.
+#include <cuda.h>  // CUtensorMap and the encoder's enums (the encoder itself is fetched from the driver)
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +19,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <unordered_map>
@@ -176,6 +179,7 @@ struct Solve {
   double *sg_geo = nullptr, *sg_w = nullptr;  // singular-edge geometry (k_sing_setup)
   char *arena = nullptr;
   DevBlock *dblocks = nullptr;
+  void *dtmaps = nullptr;  // the blocks' TMA tensor maps (DevBlock::tmap)
   Tables *T = nullptr;
   double res_rtol = 0.0;
   int res_max_it = 0;
@@ -923,6 +927,62 @@ int upload_aliases(Solve *S, const mhd_alias_classes &a, cudaStream_t st) {
   return MHD_OK;
 }
 
+// The driver's tensor-map encoder (cuTensorMapEncodeTiled), null when the
+// driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// TMA tensor maps of a solve's blocks for the staged fluid variant: per
+// block U buffer 0 and U buffer 1 (4-D: k, j, i over the row pitch and the
+// box extents, and the 10 U components; box tma_box_k x 6 x 6 x 1) and the
+// real-valued M components through the primitive variables (box of 4
+// components: u, v, w, p).  Copies that reach past the arrays read zeros.
+// A block whose maps cannot be encoded keeps tmap null (the kernel then
+// loads its boxes itself).
+int upload_tmaps(Solve *S, std::vector<DevBlock> &blocks, cudaStream_t st) {
+  for (DevBlock &d : blocks) d.tmap = nullptr;
+  const auto enc = tmap_encoder();
+  if (!enc) return MHD_OK;
+  const int es = S->es;
+  std::vector<CUtensorMap> maps(3 * blocks.size());
+  std::vector<char> ok(blocks.size(), 0);
+  for (size_t bi = 0; bi < blocks.size(); ++bi) {
+    const Box &bx = S->boxes[bi];
+    const cuuint64_t strides[3] = {(cuuint64_t)(bx.sj * es), (cuuint64_t)(bx.si * es), (cuuint64_t)(bx.total * es)};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    bool good = true;
+    for (int q = 0; q < 3 && good; ++q) {
+      void *base = q < 2 ? blocks[bi].U[q] : (void *)(blocks[bi].M + (int64_t)kNumMetric * bx.total * 8);
+      const cuuint64_t dims[4] = {(cuuint64_t)bx.sj, (cuuint64_t)bx.ext[1], (cuuint64_t)bx.ext[0],
+                                  (cuuint64_t)(q < 2 ? kNumUComps : kTmaMComps)};
+      const cuuint32_t box[4] = {(cuuint32_t)tma_box_k(es), kTmaBoxJI, kTmaBoxJI, q < 2 ? 1u : 4u};
+      good = enc(&maps[3 * bi + q], es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base,
+                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    ok[bi] = good;
+  }
+  int rc;
+  CUtensorMap *d = nullptr;
+  if ((rc = dev_upload(S->pool, maps, &d, st))) return rc;
+  S->dtmaps = d;
+  if (((uintptr_t)d & 63) != 0) return MHD_OK;  // tensor maps in global memory must be 64-byte aligned
+  for (size_t bi = 0; bi < blocks.size(); ++bi)
+    if (ok[bi]) blocks[bi].tmap = d + 3 * bi;
+  return MHD_OK;
+}
+
 void free_solve(Solve *S, cudaStream_t st) {
   if (!S) return;
   auto f = [&](void *p) {
@@ -930,6 +990,7 @@ void free_solve(Solve *S, cudaStream_t st) {
   };
   f(S->arena);
   f(S->dblocks);
+  f(S->dtmaps);
   f(S->sg_geo);
   f(S->sg_w);
   f(S->dres_prefix);
@@ -2021,6 +2082,7 @@ static int add_solve(mhd_batch *b, const mhd_desc *desc, bool periodic, int *slo
     d.reskhi = bx.n[2] + 1;
   }
   int rc;
+  if ((rc = upload_tmaps(S, blocks, st))) return bail(rc);
   if ((rc = dev_upload(S->pool, blocks, &S->dblocks, st))) return bail(rc);
   for (int r = 0; r < kNumRanges; ++r) {
     S->T->tiles[r] = prefix[r].back();
@@ -2150,6 +2212,7 @@ int mhd_batch_add_like(mhd_batch *b, int src_slot, const mhd_constants *constant
     d.solve = slot;
     d.reskhi = bx.n[2] + 1;
   }
+  if ((rc = upload_tmaps(S, blocks, st))) return bail(rc);
   if ((rc = dev_upload(S->pool, blocks, &S->dblocks, st))) return bail(rc);
   SolveState s0{};
   s0.dt_bits = kDtUnset;

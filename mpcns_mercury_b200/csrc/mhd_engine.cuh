@@ -29,6 +29,17 @@ __host__ __device__ constexpr FluidTile fluid_tile(int v) {
   return v == 1 ? FluidTile{8, 8, 4, 4} : v == 2 ? FluidTile{8, 8, 4, 3} : v == 3 ? FluidTile{16, 4, 4, 4}
          : v == 4 ? FluidTile{16, 4, 4, 2} : v == 5 ? FluidTile{8, 8, 4, 2} : FluidTile{16, 4, 4, 3};
 }
+// Variant 6 stages each tile's cell box (density and u, v, w, p of its
+// species) with TMA tensor copies, the next tile's while the current one is
+// computed (double-buffered, mbarrier-completed).  Its box: the 16 x 4 x 4
+// tile and one cell beyond each side, the k window widened to whole 16-byte
+// units from a 16-byte-aligned start.
+__host__ __device__ constexpr bool fluid_tma(int v) { return v == 6; }
+constexpr int kTmaBoxJI = 6;  // j and i extents of the staged box
+__host__ __device__ constexpr int tma_box_k(int es) { return es == 4 ? 24 : 20; }
+// Components of a block's real-valued M region that its tensor map spans
+// (through the primitive variables of both species).
+constexpr int kTmaMComps = kComp.first[MHD_PV_NA] + 5 - kNumUComps;
 constexpr int kTileThreads = 256;
 constexpr bool fluid_tiles_ok() {
   for (int v = 0; v < kNumFluidTiles; ++v)
@@ -82,12 +93,18 @@ __host__ __device__ constexpr bool is_metric(int comp) { return comp >= kMetricF
 __host__ __device__ constexpr int rslot(int comp) {
   return comp - kNumUComps - (comp >= kMetricFirst + kNumMetric ? kNumMetric : 0);
 }
+static_assert(kTmaMComps == rslot(kComp.first[MHD_PV_NA] + 4) + 1 && kComp.first[MHD_PV_NA] < kMetricFirst,
+              "the primitive variables lie in the first kTmaMComps real-valued M components");
 
 // Per-block descriptor (device).  Block memory: U buffers of 10 real arrays
 // each; M = [10 metric double arrays | kNumRComps real arrays].
 struct DevBlock {
   void *U[2];         // U_H, U_Na components (10) of buffer 0 / 1
   char *M;
+  // TMA tensor maps of the block (U buffer 0, U buffer 1, the real-valued M
+  // components; 128 bytes each, 64-byte aligned), null where none could be
+  // encoded: the staged fluid variant then loads that block's boxes itself
+  const void *tmap;
   int64_t total, si, sj;
   int G, n[3];
   int solve;          // index of the owning solve in the directory

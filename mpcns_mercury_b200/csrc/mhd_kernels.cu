@@ -110,90 +110,249 @@ struct NoTileEnd {
   __device__ void operator()(int) const {}
 };
 
+// The solve s, its block b and the block's tile t of work item w of range
+// KIND (two binary searches over the directory's prefix sums).
+template <int KIND>
+__device__ __forceinline__ void lookup_item(const Dir &D, int w, int &s, int &b, int &t) {
+  const int *sp = D.solve_tile_prefix[KIND];
+  int lo = 0, hi = D.nsolves;  // largest s with sp[s] <= w
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (sp[mid] <= w) lo = mid; else hi = mid;
+  }
+  s = lo;
+  const int lw = w - sp[s];
+  const int *bp = D.solves[s].tile_prefix[KIND];
+  int blo = 0, bhi = D.solves[s].nblocks;
+  while (bhi - blo > 1) {
+    const int mid = (blo + bhi) >> 1;
+    if (bp[mid] <= lw) blo = mid; else bhi = mid;
+  }
+  b = blo;
+  t = lw - bp[blo];
+}
+
+// Origin (i, j, k) and species of tile t of a fluid range over range box r.
+template <int KIND>
+__device__ __forceinline__ void fluid_tile_origin(const RangeBox &r, int t, int o[3], int &species) {
+  constexpr FluidTile T = fluid_tile(fluid_variant(KIND));
+  species = t & 1;
+  t >>= 1;
+  const int tk = (r.hi[2] - r.lo[2] + T.k - 1) / T.k;
+  const int tj = (r.hi[1] - r.lo[1] + T.j - 1) / T.j;
+  const int bk = t % tk, bj = (t / tk) % tj, bi = t / (tk * tj);
+  o[0] = r.lo[0] + bi * T.i;
+  o[1] = r.lo[1] + bj * T.j;
+  o[2] = r.lo[2] + bk * T.k;
+}
+
+// The work item (s, b, t) of range KIND as this thread sees it, and the
+// block's fields of the current step.
+template <class R, int KIND>
+__device__ __forceinline__ void build_item(const Dir &D, int s, int b, int t, Item &it, V<R> &B) {
+  const int tid = threadIdx.x;
+  const DevSolve &S = D.solves[s];
+  const DevBlock &DB = S.blocks[b];
+  RangeBox r = range_of(KIND, DB.n, S.c.nghost);
+  if constexpr (KIND == kResK) r.hi[2] = DB.reskhi;
+  it.s = s;
+  it.blk = b;
+  it.species = 0;
+  for (int a = 0; a < 3; ++a) {
+    it.hi[a] = r.hi[a];
+    it.lo[a] = r.lo[a];
+  }
+  if constexpr (fluid_variant(KIND) >= 0) {  // a fluid tile, one species
+    constexpr FluidTile T = fluid_tile(fluid_variant(KIND));
+    fluid_tile_origin<KIND>(r, t, it.o, it.species);
+    it.k = it.o[2] + (tid % T.k);
+    it.j = it.o[1] + ((tid / T.k) % T.j);
+    it.i = it.o[0] + (tid / (T.k * T.j));
+    it.in = it.i < r.hi[0] && it.j < r.hi[1] && it.k < r.hi[2];
+  } else {  // a run of kTileThreads consecutive positions of the range box (k fastest)
+    const int ek = r.hi[2] - r.lo[2], ej = r.hi[1] - r.lo[1];
+    const int L = t * kTileThreads + tid;
+    const int rest = L / ek;
+    it.k = r.lo[2] + (L - rest * ek);
+    it.j = r.lo[1] + rest % ej;
+    it.i = r.lo[0] + rest / ej;
+    it.in = L < ek * ej * (r.hi[0] - r.lo[0]);
+    it.o[0] = it.o[1] = it.o[2] = 0;
+  }
+  const int cur = D.state[s].cur;
+  B.U = (R *)DB.U[cur];
+  B.Un = (R *)DB.U[cur ^ 1];
+  B.M = DB.M;
+  B.total = (int)DB.total;
+  B.si = (int)DB.si;
+  B.sj = (int)DB.sj;
+  B.G = DB.G;
+  B.n0 = DB.n[0];
+  B.n1 = DB.n[1];
+  B.n2 = DB.n[2];
+}
+
 // Work-item loop: for every tile of range `KIND` of every active solve, call
 // f(S, B, item), then end(w) with the tile's index w over all solves (every
-// thread of the CTA).  Tile lookup: two binary searches by thread 0,
-// broadcast through shared memory.
+// thread of the CTA).  Tile lookup by thread 0, broadcast through shared
+// memory.
 template <class R, int KIND, class F, class E = NoTileEnd>
 __device__ __forceinline__ void for_items(const Dir &D, F &&f, E &&end = E{}) {
   __shared__ int sh[3];
   const int total = D.solve_tile_prefix[KIND][D.nsolves];
   const int tid = threadIdx.x;
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    if (tid == 0) {
-      const int *sp = D.solve_tile_prefix[KIND];
-      int lo = 0, hi = D.nsolves;  // largest s with sp[s] <= w
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (sp[mid] <= w) lo = mid; else hi = mid;
-      }
-      const int s = lo;
-      const int lw = w - sp[s];
-      const int *bp = D.solves[s].tile_prefix[KIND];
-      int blo = 0, bhi = D.solves[s].nblocks;
-      while (bhi - blo > 1) {
-        const int mid = (blo + bhi) >> 1;
-        if (bp[mid] <= lw) blo = mid; else bhi = mid;
-      }
-      sh[0] = s;
-      sh[1] = blo;
-      sh[2] = lw - bp[blo];
-    }
+    if (tid == 0) lookup_item<KIND>(D, w, sh[0], sh[1], sh[2]);
     __syncthreads();
-    const int s = sh[0], b = sh[1];
-    int t = sh[2];
+    const int s = sh[0], b = sh[1], t = sh[2];
     __syncthreads();
     if (!solve_active(D, s)) continue;  // inactive solve (the whole CTA agrees)
-    const DevSolve &S = D.solves[s];
-    const DevBlock &DB = S.blocks[b];
-    RangeBox r = range_of(KIND, DB.n, S.c.nghost);
-    if constexpr (KIND == kResK) r.hi[2] = DB.reskhi;
     Item it;
-    it.s = s;
-    it.blk = b;
-    it.species = 0;
-    for (int a = 0; a < 3; ++a) {
-      it.hi[a] = r.hi[a];
-      it.lo[a] = r.lo[a];
-    }
-    if constexpr (fluid_variant(KIND) >= 0) {  // a fluid tile, one species
-      constexpr FluidTile T = fluid_tile(fluid_variant(KIND));
-      it.species = t & 1;
-      t >>= 1;
-      const int tk = (r.hi[2] - r.lo[2] + T.k - 1) / T.k;
-      const int tj = (r.hi[1] - r.lo[1] + T.j - 1) / T.j;
-      const int bk = t % tk, bj = (t / tk) % tj, bi = t / (tk * tj);
-      it.o[0] = r.lo[0] + bi * T.i;
-      it.o[1] = r.lo[1] + bj * T.j;
-      it.o[2] = r.lo[2] + bk * T.k;
-      it.k = it.o[2] + (tid % T.k);
-      it.j = it.o[1] + ((tid / T.k) % T.j);
-      it.i = it.o[0] + (tid / (T.k * T.j));
-      it.in = it.i < r.hi[0] && it.j < r.hi[1] && it.k < r.hi[2];
-    } else {  // a run of kTileThreads consecutive positions of the range box (k fastest)
-      const int ek = r.hi[2] - r.lo[2], ej = r.hi[1] - r.lo[1];
-      const int L = t * kTileThreads + tid;
-      const int rest = L / ek;
-      it.k = r.lo[2] + (L - rest * ek);
-      it.j = r.lo[1] + rest % ej;
-      it.i = r.lo[0] + rest / ej;
-      it.in = L < ek * ej * (r.hi[0] - r.lo[0]);
-      it.o[0] = it.o[1] = it.o[2] = 0;
-    }
     V<R> B;
-    const int cur = D.state[s].cur;
-    B.U = (R *)DB.U[cur];
-    B.Un = (R *)DB.U[cur ^ 1];
-    B.M = DB.M;
-    B.total = (int)DB.total;
-    B.si = (int)DB.si;
-    B.sj = (int)DB.sj;
-    B.G = DB.G;
-    B.n0 = DB.n[0];
-    B.n1 = DB.n[1];
-    B.n2 = DB.n[2];
-    f(S, B, it);
+    build_item<R, KIND>(D, s, b, t, it, B);
+    f(D.solves[s], B, it);
     end(w);
+  }
+}
+
+// ------------------------------------------------------------------ TMA staging
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for phase `parity` of the barrier to complete, at most about a
+// second: false when it did not (the caller records MHD_ERR_TIMEOUT).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (int n = 0; n < (1 << 24); ++n) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (n >= 16) __nanosleep(64);
+  }
+  return false;
+}
+// One 4-D tiled tensor copy (no multicast) of the box at coordinates
+// (c0 .. c3) into this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Work-item loop of the TMA-staged fluid variant: as for_items, and each
+// item's box of staged cells (density, then u, v, w, p of its species; k
+// window of tma_box_k(sizeof(R)) from the 16-byte unit holding k = o - 1,
+// j and i windows of 6 from o - 1) is in shared memory when f(S, B, item,
+// box) runs.  Thread 0 looks up item w + gridDim.x and starts its copies into
+// the other stage before item w is computed.  A block without tensor maps
+// has its box loaded by the CTA's threads instead.  A copy not complete
+// within the bounded wait records MHD_ERR_TIMEOUT on the solve and ends
+// the kernel.
+template <class R, int KIND, class F>
+__device__ __forceinline__ void for_fluid_items_tma(const Dir &D, R *stage, uint64_t *bars, F &&f) {
+  constexpr int W = tma_box_k(sizeof(R)), BV = W * kTmaBoxJI * kTmaBoxJI;
+  constexpr int kAlign = 16 / (int)sizeof(R);
+  __shared__ int sh[2][4];  // per stage: solve, block, tile, copy state (0 none, 1 TMA, 2 by the threads)
+  const int total = D.solve_tile_prefix[KIND][D.nsolves];
+  const int tid = threadIdx.x;
+  // the box's coordinates in the block's arrays (k, j, i including the ghost offset)
+  auto box_at = [&](const DevBlock &DB, int s, int t, int c[3], int &species) {
+    const DevSolve &S = D.solves[s];
+    const RangeBox r = range_of(KIND, DB.n, S.c.nghost);
+    int o[3];
+    fluid_tile_origin<KIND>(r, t, o, species);
+    c[0] = (o[2] + DB.G - 1) & ~(kAlign - 1);
+    c[1] = o[1] - 1 + DB.G;
+    c[2] = o[0] - 1 + DB.G;
+  };
+  // thread 0: look item w up into stage st and start its copies
+  auto issue = [&](int w, int st) {
+    int s, b, t;
+    lookup_item<KIND>(D, w, s, b, t);
+    sh[st][0] = s;
+    sh[st][1] = b;
+    sh[st][2] = t;
+    sh[st][3] = 0;
+    if (!solve_active(D, s)) return;
+    const DevBlock &DB = D.solves[s].blocks[b];
+    if (!DB.tmap) {
+      sh[st][3] = 2;
+      return;
+    }
+    int c[3], species;
+    box_at(DB, s, t, c, species);
+    const char *maps = (const char *)DB.tmap;
+    R *dst = stage + st * 5 * BV;
+    const int cur = D.state[s].cur;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of this stage, then the copies
+    mbar_expect_tx(&bars[st], (uint32_t)(5 * BV * sizeof(R)));
+    tma_load_4d(dst, maps + 128 * cur, c[0], c[1], c[2], species ? 5 : 0, &bars[st]);
+    tma_load_4d(dst + BV, maps + 256, c[0], c[1], c[2], rslot(species ? cPVN : cPVH),
+                &bars[st]);
+    sh[st][3] = 1;
+  };
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+  uint32_t phase = 0;  // per stage: parity of its next completion
+  int n = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x, ++n) {
+    const int st = n & 1;
+    __syncthreads();  // stage st's item recorded; stage st ^ 1 no longer read
+    const int s = sh[st][0], b = sh[st][1], t = sh[st][2], how = sh[st][3];
+    if (tid == 0 && w + (int)gridDim.x < total) issue(w + gridDim.x, st ^ 1);
+    if (how == 0) continue;  // inactive solve (the whole CTA agrees)
+    R *box = stage + st * 5 * BV;
+    if (how == 1) {
+      const bool ok = mbar_wait_bounded(&bars[st], (phase >> st) & 1u);
+      phase ^= 1u << st;
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicCAS(&D.state[s].status, 0, (int)MHD_ERR_TIMEOUT);
+        // the next item's copies, if started, land before the CTA ends (bounded again)
+        if (w + (int)gridDim.x < total && sh[st ^ 1][3] == 1) mbar_wait_bounded(&bars[st ^ 1], (phase >> (st ^ 1)) & 1u);
+        return;
+      }
+    } else {  // no tensor maps: the same box by plain loads (zeros outside the block's arrays)
+      const DevBlock &DB = D.solves[s].blocks[b];
+      int c[3], species;
+      box_at(DB, s, t, c, species);
+      const int cur = D.state[s].cur;
+      const R *src[5];
+      src[0] = (const R *)DB.U[cur] + (species ? 5 : 0) * DB.total;
+      const R *mr = (const R *)(DB.M + (int64_t)kNumMetric * DB.total * 8);
+      for (int m = 0; m < 4; ++m)
+        src[1 + m] = mr + (int64_t)(rslot(species ? cPVN : cPVH) + m) * DB.total;
+      const int ext1 = DB.n[1] + 1 + 2 * DB.G, ext0 = DB.n[0] + 1 + 2 * DB.G;
+      for (int q = tid; q < 5 * BV; q += kTileThreads) {
+        const int m = q / BV, e = q % BV;
+        const int x = c[0] + e % W, y = c[1] + (e / W) % kTmaBoxJI, z = c[2] + e / (W * kTmaBoxJI);
+        box[q] = (x < DB.sj && y < ext1 && z < ext0) ? src[m][(int64_t)z * DB.si + (int64_t)y * DB.sj + x] : R(0.0);
+      }
+      __syncthreads();
+    }
+    Item it;
+    V<R> B;
+    build_item<R, KIND>(D, s, b, t, it, B);
+    f(D.solves[s], B, it, (const R *)box);
   }
 }
 
@@ -561,11 +720,19 @@ struct TileFaces {
 // Shared memory of the fluid kernel's tile (variant VT): the staged
 // quantities of the tile's cells and their face neighbours (7 values per cell
 // of the tile padded by one layer) and the tile's face fluxes (5 per face).
+// The TMA-staged variant instead holds two stages of its box (5 components
+// each), re and c over the box, the face fluxes, and 128 bytes to align the
+// stages to 128 bytes.
 template <class R, int VT>
 struct FluidSmem {
   static constexpr FluidTile T = fluid_tile(VT);
   static constexpr int PK = T.k + 2, PJ = T.j + 2, PI = T.i + 2, cells = PK * PJ * PI;
-  static constexpr size_t bytes = sizeof(R) * (size_t)(7 * cells + 5 * TileFaces<VT>::all);
+  static constexpr int BV = tma_box_k(sizeof(R)) * kTmaBoxJI * kTmaBoxJI;  // elements of one component's box
+  static constexpr size_t bytes =
+      fluid_tma(VT) ? 128 + sizeof(R) * (size_t)(2 * 5 * BV + 2 * BV + 5 * TileFaces<VT>::all)
+                    : sizeof(R) * (size_t)(7 * cells + 5 * TileFaces<VT>::all);
+  static_assert(!fluid_tma(VT) || (T.k == 16 && T.j == 4 && T.i == 4), "the staged box assumes a 16 x 4 x 4 tile");
+  static_assert((BV * sizeof(R)) % 128 == 0, "stages stay 128-byte aligned");
 };
 
 // ZeroRHS_ + Scheme_U_ + AddSourceToRHS_Fluid (FluidRHS.cpp:206-527) +
@@ -586,10 +753,19 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
   constexpr int kNF0 = TileFaces<VT>::n0, kNF1 = TileFaces<VT>::n1, kTileFaces = TileFaces<VT>::all;
   constexpr int kTileK = T.k, kTileJ = T.j;
   constexpr int PK = FluidSmem<R, VT>::PK, PJ = FluidSmem<R, VT>::PJ, NP = FluidSmem<R, VT>::cells;
+  constexpr bool kTma = fluid_tma(VT);
+  constexpr int W = tma_box_k(sizeof(R)), BV = FluidSmem<R, VT>::BV;
   extern __shared__ __align__(16) unsigned char fluid_smem[];
-  R(*C)[NP] = reinterpret_cast<R(*)[NP]>(fluid_smem);                         // [7][NP]
-  R(*F)[kTileFaces] = reinterpret_cast<R(*)[kTileFaces]>(fluid_smem + sizeof(R) * 7 * NP);  // [5][faces]
-  for_items<R, fluid_kind(VT)>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) {
+  unsigned char *sbase = fluid_smem;
+  if constexpr (kTma) sbase += (128 - (smem_u32(fluid_smem) & 127)) & 127;
+  // the staged variant: [2 stages][5][BV] | RC [2][BV] (re, c) | F
+  R *stage = reinterpret_cast<R *>(sbase);
+  R(*RC)[BV] = reinterpret_cast<R(*)[BV]>(sbase + sizeof(R) * 10 * BV);
+  R(*C)[NP] = reinterpret_cast<R(*)[NP]>(sbase);  // [7][NP]
+  R(*F)[kTileFaces] =
+      reinterpret_cast<R(*)[kTileFaces]>(sbase + sizeof(R) * (kTma ? 12 * BV : 7 * NP));  // [5][faces]
+  __shared__ uint64_t bars[2];
+  auto body = [&](const DevSolve &S, const V<R> &B, const Item &it, const R *box) {
     const ConstsT<R> &c = consts_of<R>(S);
     const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
     // the reference aborts; k_flip records the status (and a solve with a
@@ -639,6 +815,9 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
     // Stage the cells the tile's faces read (the tile and one layer beyond
     // each of its six sides, inside the owned range widened by one): rho,
     // u, v, w, p and the per-cell terms re and c.
+    // the staged variant: the box of this item holds the cells; re and c of
+    // the cells the faces read go to RC (box indexing, k shifted by koff)
+    const int koff = kTma ? (it.o[2] + B.G - 1) & (16 / (int)sizeof(R) - 1) : 0;
 #pragma unroll 1
     for (int q = tid; q < NP; q += kTileThreads) {
       const int ck = q % PK, cj = (q / PK) % PJ, ci = q / (PK * PJ);
@@ -647,6 +826,13 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
       if (!dt_ok || out > 1 || x0 < it.lo[0] - 1 || x0 > it.hi[0] || x1 < it.lo[1] - 1 || x1 > it.hi[1] ||
           x2 < it.lo[2] - 1 || x2 > it.hi[2])
         continue;
+      if constexpr (kTma) {
+        const int e = (ci * kTmaBoxJI + cj) * W + ck + koff;
+        const R rho = box[e], u = box[BV + e], v = box[2 * BV + e], w = box[3 * BV + e], p = box[4 * BV + e];
+        RC[0][e] = p / (g - R(1.0)) + R(0.5) * rho * (u * u + v * v + w * w);
+        RC[1][e] = sqrt(dmax(R(0.0), g * p / dmax(rho, R(1e-30))));
+        continue;
+      }
       const R rho = AT(u0, x0, x1, x2), u = AT(pv0, x0, x1, x2), v = AT(pv0 + 1, x0, x1, x2),
               w = AT(pv0 + 2, x0, x1, x2), p = AT(pv0 + 3, x0, x1, x2);
       C[0][q] = rho;
@@ -686,13 +872,28 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
         k3 = ATM(cm + 2, x[0], x[1], x[2]);
       }
       // the face's right cell is (fi, fj, fk) of the tile, its left one step back along dir
-      const int qr = ((fi + 1) * PJ + (fj + 1)) * PK + (fk + 1);
-      const int ql = qr - (dir == 0 ? PJ * PK : dir == 1 ? PK : 1);
       R Lv[7], Rv[7];
+      if constexpr (kTma) {
+        const int er = ((fi + 1) * kTmaBoxJI + (fj + 1)) * W + (fk + 1) + koff;
+        const int el = er - (dir == 0 ? kTmaBoxJI * W : dir == 1 ? W : 1);
 #pragma unroll
-      for (int m = 0; m < 7; ++m) {
-        Lv[m] = C[m][ql];
-        Rv[m] = C[m][qr];
+        for (int m = 0; m < 5; ++m) {
+          Lv[m] = box[m * BV + el];
+          Rv[m] = box[m * BV + er];
+        }
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          Lv[5 + m] = RC[m][el];
+          Rv[5 + m] = RC[m][er];
+        }
+      } else {
+        const int qr = ((fi + 1) * PJ + (fj + 1)) * PK + (fk + 1);
+        const int ql = qr - (dir == 0 ? PJ * PK : dir == 1 ? PK : 1);
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+          Lv[m] = C[m][ql];
+          Rv[m] = C[m][qr];
+        }
       }
       R Fl[5];
       rusanov_staged(Lv, Rv, k1, k2, k3, AT(cn + 3, x[0], x[1], x[2]), Fl);
@@ -791,7 +992,12 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
     const int o = B.off(i, j, k);
 #pragma unroll
     for (int m = 0; m < 5; ++m) B.Un[(u0 + m) * B.total + o] = CV(12 + m) + dt * r[m];
-  });
+  };
+  if constexpr (kTma) {
+    for_fluid_items_tma<R, fluid_kind(VT)>(D, stage, bars, body);
+  } else {
+    for_items<R, fluid_kind(VT)>(D, [&](const DevSolve &S, const V<R> &B, const Item &it) { body(S, B, it, nullptr); });
+  }
 }
 
 // B_face += dt * (-curl E) on the owned faces (CTOperators.cpp:6-56 with multiplier -1).
@@ -2058,10 +2264,11 @@ static const void *fluid_fn(int v) {
     case 3: return (const void *)k_fluid<R, 3>;
     case 4: return (const void *)k_fluid<R, 4>;
     case 5: return (const void *)k_fluid<R, 5>;
+    case 6: return (const void *)k_fluid<R, 6>;
     default: return (const void *)k_fluid<R, 0>;
   }
 }
-static_assert(kNumFluidTiles == 6, "fluid_fn and launch_fluid list every variant");
+static_assert(kNumFluidTiles == 7, "fluid_fn and launch_fluid list every variant");
 template <class R>
 static size_t fluid_smem(int v) {
   switch (v) {
@@ -2070,6 +2277,7 @@ static size_t fluid_smem(int v) {
     case 3: return FluidSmem<R, 3>::bytes;
     case 4: return FluidSmem<R, 4>::bytes;
     case 5: return FluidSmem<R, 5>::bytes;
+    case 6: return FluidSmem<R, 6>::bytes;
     default: return FluidSmem<R, 0>::bytes;
   }
 }
@@ -2082,6 +2290,7 @@ static void launch_fluid(int v, const Dir &D, cudaStream_t st) {
     case 3: k_fluid<R, 3><<<G, kTileThreads, FluidSmem<R, 3>::bytes, st>>>(D); break;
     case 4: k_fluid<R, 4><<<G, kTileThreads, FluidSmem<R, 4>::bytes, st>>>(D); break;
     case 5: k_fluid<R, 5><<<G, kTileThreads, FluidSmem<R, 5>::bytes, st>>>(D); break;
+    case 6: k_fluid<R, 6><<<G, kTileThreads, FluidSmem<R, 6>::bytes, st>>>(D); break;
     default: k_fluid<R, 0><<<G, kTileThreads, FluidSmem<R, 0>::bytes, st>>>(D); break;
   }
 }

@@ -101,7 +101,8 @@ def test_fluid_tile_shapes_and_shape_classes():
     shapes = [capi.fluid_tile_shape(v) for v in range(capi.NUM_FLUID_TILES)]
     assert shapes[0] == (16, 4, 4, 3)
     assert all(k * j * i == 256 and ctas in (2, 3, 4) for k, j, i, ctas in shapes)
-    assert len(set(shapes)) == len(shapes)
+    # variant 6 is variant 0's tile with its cells staged by TMA tensor copies
+    assert len(set(shapes[:6])) == 6 and shapes[6] == shapes[0]
     with pytest.raises(capi.MhdError):
         capi.fluid_tile_shape(capi.NUM_FLUID_TILES)
     assert autotune.shape_class([(24, 24, 30)] * 6) == "k<=32-j<=32"
