@@ -30,11 +30,14 @@ __host__ __device__ constexpr FluidTile fluid_tile(int v) {
          : v == 4 ? FluidTile{16, 4, 4, 2} : v == 5 ? FluidTile{8, 8, 4, 2} : FluidTile{16, 4, 4, 3};
 }
 // Variant 6 stages each tile's cell box (density and u, v, w, p of its
-// species) with TMA tensor copies, the next tile's while the current one is
-// computed (double-buffered, mbarrier-completed).  Its box: the 16 x 4 x 4
+// species) with TMA tensor copies issued by a producer warp up to two tiles
+// ahead of the compute threads (double-buffered, mbarrier-completed).  Its box: the 16 x 4 x 4
 // tile and one cell beyond each side, the k window widened to whole 16-byte
 // units from a 16-byte-aligned start.
 __host__ __device__ constexpr bool fluid_tma(int v) { return v == 6; }
+// Threads of a fluid CTA: 256 that compute (one per cell of the tile), and
+// for the staged variant a producer warp that issues the copies.
+__host__ __device__ constexpr int fluid_threads(int v) { return fluid_tma(v) ? 256 + 32 : 256; }
 constexpr int kTmaBoxJI = 6;  // j and i extents of the staged box
 __host__ __device__ constexpr int tma_box_k(int es) { return es == 4 ? 24 : 20; }
 // Components of a block's real-valued M region that its tensor map spans

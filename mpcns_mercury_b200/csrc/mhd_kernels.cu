@@ -254,20 +254,38 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const void *map, int c0, 
       : "memory");
 }
 
-// Work-item loop of the TMA-staged fluid variant: as for_items, and each
-// item's box of staged cells (density, then u, v, w, p of its species; k
-// window of tma_box_k(sizeof(R)) from the 16-byte unit holding k = o - 1,
-// j and i windows of 6 from o - 1) is in shared memory when f(S, B, item,
-// box) runs.  Thread 0 looks up item w + gridDim.x and starts its copies into
-// the other stage before item w is computed.  A block without tensor maps
-// has its box loaded by the CTA's threads instead.  A copy not complete
-// within the bounded wait records MHD_ERR_TIMEOUT on the solve and ends
-// the kernel.
+// The staged variant's 256 compute threads synchronise among themselves
+// (named barrier 1; its producer warp takes no part).
+__device__ __forceinline__ void compute_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ bool compute_and(bool v) {
+  uint32_t r;
+  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, 256, p;\n selp.u32 %0, 1, 0, q;\n}"
+               : "=r"(r)
+               : "r"((uint32_t)v)
+               : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Work-item loop of the TMA-staged fluid variant, warp-specialised: the
+// CTA's 256 compute threads run f(S, B, item, box) for its items, while its
+// ninth warp (one lane) looks the items up and stages each one's box
+// (density, then u, v, w, p of its species; k window of
+// tma_box_k(sizeof(R)) from the 16-byte unit holding k = o - 1, j and i
+// windows of 6 from o - 1) with TMA tensor copies into one of two stages,
+// running up to two items ahead.  bars[0..1]: a stage is full (the item's
+// record, and its copies complete); bars[2..3]: the compute threads are done
+// reading it (f arrives once its face fluxes are built).  A block without
+// tensor maps has its box loaded by the compute threads instead.  A wait that
+// does not end within its bound records MHD_ERR_TIMEOUT on the solve of the
+// item waited for and ends the CTA's loop.
 template <class R, int KIND, class F>
 __device__ __forceinline__ void for_fluid_items_tma(const Dir &D, R *stage, uint64_t *bars, F &&f) {
   constexpr int W = tma_box_k(sizeof(R)), BV = W * kTmaBoxJI * kTmaBoxJI;
   constexpr int kAlign = 16 / (int)sizeof(R);
-  __shared__ int sh[2][4];  // per stage: solve, block, tile, copy state (0 none, 1 TMA, 2 by the threads)
+  __shared__ int sh[2][4];  // per stage: solve, block, tile, copy state (0 inactive, 1 TMA, 2 by the threads)
   const int total = D.solve_tile_prefix[KIND][D.nsolves];
   const int tid = threadIdx.x;
   // the box's coordinates in the block's arrays (k, j, i including the ghost offset)
@@ -280,74 +298,77 @@ __device__ __forceinline__ void for_fluid_items_tma(const Dir &D, R *stage, uint
     c[1] = o[1] - 1 + DB.G;
     c[2] = o[0] - 1 + DB.G;
   };
-  // thread 0: look item w up into stage st and start its copies
-  auto issue = [&](int w, int st) {
-    int s, b, t;
-    lookup_item<KIND>(D, w, s, b, t);
-    sh[st][0] = s;
-    sh[st][1] = b;
-    sh[st][2] = t;
-    sh[st][3] = 0;
-    if (!solve_active(D, s)) return;
-    const DevBlock &DB = D.solves[s].blocks[b];
-    if (!DB.tmap) {
-      sh[st][3] = 2;
-      return;
-    }
-    int c[3], species;
-    box_at(DB, s, t, c, species);
-    const char *maps = (const char *)DB.tmap;
-    R *dst = stage + st * 5 * BV;
-    const int cur = D.state[s].cur;
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of this stage, then the copies
-    mbar_expect_tx(&bars[st], (uint32_t)(5 * BV * sizeof(R)));
-    tma_load_4d(dst, maps + 128 * cur, c[0], c[1], c[2], species ? 5 : 0, &bars[st]);
-    tma_load_4d(dst + BV, maps + 256, c[0], c[1], c[2], rslot(species ? cPVN : cPVH),
-                &bars[st]);
-    sh[st][3] = 1;
-  };
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
+    mbar_init(&bars[2], kTileThreads);
+    mbar_init(&bars[3], kTileThreads);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
-  uint32_t phase = 0;  // per stage: parity of its next completion
-  int n = 0;
-  for (int w = blockIdx.x; w < total; w += gridDim.x, ++n) {
-    const int st = n & 1;
-    __syncthreads();  // stage st's item recorded; stage st ^ 1 no longer read
-    const int s = sh[st][0], b = sh[st][1], t = sh[st][2], how = sh[st][3];
-    if (tid == 0 && w + (int)gridDim.x < total) issue(w + gridDim.x, st ^ 1);
-    if (how == 0) continue;  // inactive solve (the whole CTA agrees)
-    R *box = stage + st * 5 * BV;
-    if (how == 1) {
-      const bool ok = mbar_wait_bounded(&bars[st], (phase >> st) & 1u);
-      phase ^= 1u << st;
-      if (!__syncthreads_and(ok)) {
-        if (tid == 0) atomicCAS(&D.state[s].status, 0, (int)MHD_ERR_TIMEOUT);
-        // the next item's copies, if started, land before the CTA ends (bounded again)
-        if (w + (int)gridDim.x < total && sh[st ^ 1][3] == 1) mbar_wait_bounded(&bars[st ^ 1], (phase >> (st ^ 1)) & 1u);
+  if (tid >= kTileThreads) {  // the producer warp
+    if (tid != kTileThreads) return;
+    uint32_t n = 0;
+    for (int w = blockIdx.x; w < total; w += gridDim.x, ++n) {
+      const int st = n & 1;
+      int s, b, t;
+      lookup_item<KIND>(D, w, s, b, t);
+      if (n >= 2 && !mbar_wait_bounded(&bars[2 + st], ((n >> 1) - 1) & 1u)) {
+        atomicCAS(&D.state[s].status, 0, (int)MHD_ERR_TIMEOUT);
         return;
       }
-    } else {  // no tensor maps: the same box by plain loads (zeros outside the block's arrays)
+      sh[st][0] = s;
+      sh[st][1] = b;
+      sh[st][2] = t;
+      const DevBlock &DB = D.solves[s].blocks[b];
+      if (!solve_active(D, s) || !DB.tmap) {
+        sh[st][3] = solve_active(D, s) ? 2 : 0;
+        mbar_arrive(&bars[st]);
+        continue;
+      }
+      sh[st][3] = 1;
+      int c[3], species;
+      box_at(DB, s, t, c, species);
+      const char *maps = (const char *)DB.tmap;
+      R *dst = stage + st * 5 * BV;
+      const int cur = D.state[s].cur;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the stage's earlier reads, then the copies
+      mbar_expect_tx(&bars[st], (uint32_t)(5 * BV * sizeof(R)));
+      tma_load_4d(dst, maps + 128 * cur, c[0], c[1], c[2], species ? 5 : 0, &bars[st]);
+      tma_load_4d(dst + BV, maps + 256, c[0], c[1], c[2], rslot(species ? cPVN : cPVH), &bars[st]);
+    }
+    return;
+  }
+  uint32_t n = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x, ++n) {
+    const int st = n & 1;
+    const bool ok = mbar_wait_bounded(&bars[st], (n >> 1) & 1u);
+    if (!compute_and(ok)) {
+      if (tid == 0) atomicCAS(&D.state[sh[st][0]].status, 0, (int)MHD_ERR_TIMEOUT);
+      return;
+    }
+    const int s = sh[st][0], b = sh[st][1], t = sh[st][2], how = sh[st][3];
+    R *box = stage + st * 5 * BV;
+    if (how == 0) {  // inactive solve (every compute thread agrees)
+      mbar_arrive(&bars[2 + st]);
+      continue;
+    }
+    if (how == 2) {  // no tensor maps: the same box by plain loads (zeros outside the block's arrays)
       const DevBlock &DB = D.solves[s].blocks[b];
       int c[3], species;
       box_at(DB, s, t, c, species);
       const int cur = D.state[s].cur;
-      const R *src[5];
-      src[0] = (const R *)DB.U[cur] + (species ? 5 : 0) * DB.total;
-      const R *mr = (const R *)(DB.M + (int64_t)kNumMetric * DB.total * 8);
-      for (int m = 0; m < 4; ++m)
-        src[1 + m] = mr + (int64_t)(rslot(species ? cPVN : cPVH) + m) * DB.total;
+      const R *u0p = (const R *)DB.U[cur] + (species ? 5 : 0) * DB.total;
+      const R *pvp = (const R *)(DB.M + (int64_t)kNumMetric * DB.total * 8) +
+                     (int64_t)rslot(species ? cPVN : cPVH) * DB.total;
       const int ext1 = DB.n[1] + 1 + 2 * DB.G, ext0 = DB.n[0] + 1 + 2 * DB.G;
       for (int q = tid; q < 5 * BV; q += kTileThreads) {
         const int m = q / BV, e = q % BV;
         const int x = c[0] + e % W, y = c[1] + (e / W) % kTmaBoxJI, z = c[2] + e / (W * kTmaBoxJI);
-        box[q] = (x < DB.sj && y < ext1 && z < ext0) ? src[m][(int64_t)z * DB.si + (int64_t)y * DB.sj + x] : R(0.0);
+        const R *src = m == 0 ? u0p : pvp + (int64_t)(m - 1) * DB.total;
+        box[q] = (x < DB.sj && y < ext1 && z < ext0) ? src[(int64_t)z * DB.si + (int64_t)y * DB.sj + x] : R(0.0);
       }
-      __syncthreads();
+      compute_bar();
     }
     Item it;
     V<R> B;
@@ -748,7 +769,8 @@ struct FluidSmem {
 #define MHD_MIN_CTAS_PV 4
 #endif
 template <class R, int VT>
-__global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid(Dir D) {
+__global__ void __launch_bounds__(fluid_threads(VT), (sizeof(R) == 8 && fluid_tma(VT)) ? 2 : fluid_tile(VT).min_ctas)
+    k_fluid(Dir D) {
   constexpr FluidTile T = fluid_tile(VT);
   constexpr int kNF0 = TileFaces<VT>::n0, kNF1 = TileFaces<VT>::n1, kTileFaces = TileFaces<VT>::all;
   constexpr int kTileK = T.k, kTileJ = T.j;
@@ -764,7 +786,11 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
   R(*C)[NP] = reinterpret_cast<R(*)[NP]>(sbase);  // [7][NP]
   R(*F)[kTileFaces] =
       reinterpret_cast<R(*)[kTileFaces]>(sbase + sizeof(R) * (kTma ? 12 * BV : 7 * NP));  // [5][faces]
-  __shared__ uint64_t bars[2];
+  __shared__ uint64_t bars[4];
+  auto cta_sync = [] {
+    if constexpr (kTma) compute_bar();
+    else __syncthreads();
+  };
   auto body = [&](const DevSolve &S, const V<R> &B, const Item &it, const R *box) {
     const ConstsT<R> &c = consts_of<R>(S);
     const R dt = __longlong_as_double((long long)D.state[it.s].dt_bits);
@@ -843,7 +869,7 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
       C[5][q] = p / (g - R(1.0)) + R(0.5) * rho * (u * u + v * v + w * w);
       C[6][q] = sqrt(dmax(R(0.0), g * p / dmax(rho, R(1e-30))));
     }
-    __syncthreads();
+    cta_sync();
     // one face of direction dir (index f among that direction's faces, the
     // slot gf of the tile's face array): the direction is a compile-time
     // constant in each of the three instantiations, so the face grid's
@@ -911,7 +937,8 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
       else if (gf < kNF0 + kNF1) face(std::integral_constant<int, 1>{}, gf - kNF0, gf);
       else face(std::integral_constant<int, 2>{}, gf - kNF0 - kNF1, gf);
     }
-    __syncthreads();
+    cta_sync();
+    if constexpr (kTma) mbar_arrive(&bars[2 + (box == stage ? 0 : 1)]);  // this stage's box is no longer read
     if (it.in && dt_ok) {
       auto take = [&](auto dirc) {
         constexpr int dir = decltype(dirc)::value;
@@ -926,7 +953,7 @@ __global__ void __launch_bounds__(kTileThreads, fluid_tile(VT).min_ctas) k_fluid
       take(std::integral_constant<int, 1>{});
       take(std::integral_constant<int, 2>{});
     }
-    __syncthreads();  // F is rewritten by the next tile
+    cta_sync();  // F is rewritten by the next tile
     if (!it.in || !dt_ok) return;
     // sources (FluidRHS.cpp:206-527)
     const R Tn0 = R(1000.0), sk1 = R(5.0e-5), sk2 = R(1.0e-5);
@@ -2290,7 +2317,7 @@ static void launch_fluid(int v, const Dir &D, cudaStream_t st) {
     case 3: k_fluid<R, 3><<<G, kTileThreads, FluidSmem<R, 3>::bytes, st>>>(D); break;
     case 4: k_fluid<R, 4><<<G, kTileThreads, FluidSmem<R, 4>::bytes, st>>>(D); break;
     case 5: k_fluid<R, 5><<<G, kTileThreads, FluidSmem<R, 5>::bytes, st>>>(D); break;
-    case 6: k_fluid<R, 6><<<G, kTileThreads, FluidSmem<R, 6>::bytes, st>>>(D); break;
+    case 6: k_fluid<R, 6><<<G, fluid_threads(6), FluidSmem<R, 6>::bytes, st>>>(D); break;
     default: k_fluid<R, 0><<<G, kTileThreads, FluidSmem<R, 0>::bytes, st>>>(D); break;
   }
 }
@@ -2349,7 +2376,7 @@ static void grids_init() {
     // the staged cells and face fluxes are dynamic shared memory (above the
     // 48 KB default in FP64)
     cudaFuncSetAttribute(fluid_fn<R>(v), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fluid_smem<R>(v));
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fluid_fn<R>(v), kTileThreads, fluid_smem<R>(v)) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fluid_fn<R>(v), fluid_threads(v), fluid_smem<R>(v)) !=
             cudaSuccess ||
         per_sm < 1) {
       cudaGetLastError();
