@@ -1316,6 +1316,21 @@ def run_reference_member(job, warm, steps):
     return float(secs) / max(1.0, float(nsteps)), int(ncell)
 
 
+# Host memory of one reference process per owned cell, an upper estimate
+# (its fields with four ghost layers, the implicit solve's matrix and Krylov
+# vectors): concurrent members are capped so that the largest ones fit.
+REF_BYTES_PER_CELL = 16384
+
+
+def _ref_procs_in_memory(members):
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError, AttributeError):
+        return len(members)
+    biggest = max(m[1] for m in members) * REF_BYTES_PER_CELL
+    return max(1, int(0.8 * avail // max(biggest, 1)))
+
+
 def reference_sample(members, warm, steps, procs):
     """Every member on the reference build, the members partitioned over
     ``procs`` host cores (longest first onto the least loaded core), each core
@@ -1325,7 +1340,7 @@ def reference_sample(members, warm, steps, procs):
     seconds per workload step, cores used)."""
     from concurrent.futures import ThreadPoolExecutor
 
-    procs = max(1, min(procs, len(members)))
+    procs = max(1, min(procs, len(members), _ref_procs_in_memory(members)))
     load = [0] * procs
     parts = [[] for _ in range(procs)]
     for sid in sorted(range(len(members)), key=lambda q: -members[q][1]):
